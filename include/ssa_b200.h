@@ -1,0 +1,94 @@
+/*
+ * ssa_b200.h — additions of the B200 SSA library beyond the reference interface.
+ * Included by ssa_opt.h. None of these functions changes the behaviour of a reference entry
+ * point; they add what the reference API cannot express.
+ */
+#ifndef SSA_B200_H
+#define SSA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Randomized decomposition with `power_iters` subspace iterations and an optional
+ * caller-supplied Gaussian test matrix Omega (K x kp, column-major, kp = min(k + p, L, K)).
+ * Omega == NULL draws the matrix from the library generator like
+ * ssa_opt_decompose_randomized. power_iters == 0 with the same Omega is the reference
+ * algorithm of MKL/ssa_opt.h:1685-1763 (ssa_opt_decompose_randomized). Requires
+ * ssa_opt_prepare. Returns 0 or -1. */
+int ssa_opt_decompose_randomized_ex(SSA_Opt *ssa, int k, int oversampling, int power_iters, const double *Omega);
+
+/* MSSA analogue of ssa_opt_decompose_randomized_ex (reference: mssa_opt_decompose,
+ * MKL/ssa_opt.h:4116-4210). */
+int mssa_opt_decompose_ex(MSSA_Opt *mssa, int k, int oversampling, int power_iters, const double *Omega);
+
+/* ---- batched pipeline ---------------------------------------------------------------------
+ * One launch sequence runs the whole hot path for up to max_series series of identical
+ * (N, L): randomized decomposition (k, oversampling, power_iters), every elementary
+ * reconstruction, the W-correlation matrix and the sums of the requested component groups. */
+typedef struct ssa_batch ssa_batch;
+
+/* groups: n_groups groups, group g has group_sizes[g] indices listed consecutively in
+ * group_idx. Returns 0 or -1. */
+int ssa_batch_create(ssa_batch **out, int max_series, int N, int L, int k, int oversampling, int power_iters,
+                     const int *group_idx, const int *group_sizes, int n_groups);
+void ssa_batch_destroy(ssa_batch *b);
+
+/* Device-resident run: d_x is B x N doubles (row s = series s) in device memory. Results stay
+ * on the device (ssa_batch_device_results). Enqueues on the batch stream and returns without
+ * waiting; seed selects the test matrices (series s uses stream (seed, s)). */
+int ssa_batch_run_device(ssa_batch *b, const double *d_x, int B, uint64_t seed);
+
+/* Host-to-host run through the same pipeline: x is B x N doubles; outputs (host, any may be
+ * NULL): sigma B x k, W B x k x k (row-major per series), groups B x n_groups x N. Waits for
+ * completion. Returns 0, or -1 when any series failed. */
+int ssa_batch_run(ssa_batch *b, const double *x, int B, uint64_t seed, double *sigma, double *W,
+                  double *groups);
+
+/* Device pointers to the results of the last run (strides in elements). */
+typedef struct
+{
+    const double *sigma;      /* B x k */
+    const double *W;          /* B x k x k */
+    const double *groups;     /* B x n_groups x N */
+    const float *recon;       /* elementary reconstructions: series s, component i at
+                                 recon + (s * k + i) * ld_recon */
+    long long ld_recon;
+    const int *status;        /* B status words (0 = ok) */
+    void *stream;             /* cudaStream_t of the batch */
+} ssa_batch_results;
+
+int ssa_batch_device_results(const ssa_batch *b, ssa_batch_results *out);
+/* Wait for the batch stream; returns 0 when every series of the last run succeeded. */
+int ssa_batch_sync(ssa_batch *b);
+
+/* The Hankel matvecs of the context (the reference's static ssa_opt_hankel_matvec /
+ * ssa_opt_hankel_matvec_T, MKL/ssa_opt.h:871-903): y = H v (v: K values, y: L values) and
+ * z = H^T u (u: L values, z: K values), host arrays, computed on the device in FP32. */
+int ssa_opt_hankel_matvec_dev(SSA_Opt *ssa, const double *v, double *y);
+int ssa_opt_hankel_matvec_T_dev(SSA_Opt *ssa, const double *u, double *z);
+
+/* Copy the host factor arrays of a decomposed context: U (L x k) and V (K x k), column-major,
+ * k = n_components. Either pointer may be NULL. Returns k or -1. */
+int ssa_opt_copy_factors(const SSA_Opt *ssa, double *U, double *V);
+
+/* Stage profiler of a batch: with profiling on, every kernel launch of ssa_batch_run* is
+ * bracketed by CUDA events on the batch stream. ssa_batch_profile waits for the stream and
+ * returns the accumulated milliseconds and launch counts per kernel kind in the order
+ * spectrum, corr, gram, chol, rowmul, rr, elem_recon, wcorr_finish, group_sum, recon, lrf.
+ * Returns the number of kinds (11) or -1. */
+int ssa_batch_set_profiling(ssa_batch *b, int on);
+int ssa_batch_profile(ssa_batch *b, double *ms, long long *launches, int nkinds);
+
+/* ---- library information ------------------------------------------------------------------ */
+/* Number of CUDA kernel launches issued by this library in this process. */
+unsigned long long ssa_b200_kernel_launches(void);
+/* sizeof(SSA_Opt) as compiled into the library. */
+int ssa_b200_sizeof_ssa_opt(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

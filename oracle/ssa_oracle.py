@@ -635,3 +635,58 @@ def reference_test_signal(N: int, seed: int = 42) -> np.ndarray:
         x[i] = 100.0 + 50.0 * t + 20.0 * math.sin(2 * math.pi * i / 100.0) + \
             10.0 * math.sin(2 * math.pi * i / 25.0) + 5.0 * randn()
     return x
+
+
+# ---------------------------------------------------------------------------------------------
+# Replica of the library's device Gaussian generator (checker side): the CUDA path draws
+# Omega[row, col] for series s from SplitMix64 hashes of (seed_s, col, row // 2) followed by
+# Box-Muller. The uniforms are bit-identical; the transform here is FP64 (the device uses FP32),
+# so values agree to ~1e-7 relative.
+# ---------------------------------------------------------------------------------------------
+
+_M64 = (1 << 64) - 1
+
+
+def _mix64(z):
+    z = (z + 0x9E3779B97F4A7C15) & _M64
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+    return z ^ (z >> 31)
+
+
+def _mix64_np(z: np.ndarray) -> np.ndarray:
+    z = z.astype(np.uint64)
+    with np.errstate(over="ignore"):
+        z = z + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def series_seed(seed: int, s: int) -> int:
+    """Seed of series s in a batch launched with `seed` (engine: seed ^ golden * (s + 1))."""
+    return (seed ^ ((0x9E3779B97F4A7C15 * (s + 1)) & _M64)) & _M64
+
+
+def single_series_seed(calls: int = 0) -> int:
+    """Seed the single-series API uses for its `calls`-th generated test matrix (42 + 2^32 calls)."""
+    return series_seed((42 + (calls << 32)) & _M64, 0)
+
+
+def device_gaussian(seed_s: int, K: int, kp: int) -> np.ndarray:
+    """K x kp test matrix the device generates for a series with seed `seed_s`."""
+    out = np.zeros((K, kp))
+    npairs = (K + 1) // 2
+    pairs = np.arange(npairs, dtype=np.uint64)
+    for c in range(kp):
+        key = _mix64((seed_s ^ ((0xD1B54A32D192ED03 * (c + 1)) & _M64)) & _M64)
+        with np.errstate(over="ignore"):
+            z = _mix64_np(np.uint64(key) + pairs)
+        u1 = ((z >> np.uint64(40)).astype(np.float64) + 1.0) / 16777216.0
+        u2 = ((z >> np.uint64(16)) & np.uint64(0xFFFFFF)).astype(np.float64) / 16777216.0
+        r = np.sqrt(-2.0 * np.log(u1))
+        vals = np.empty(2 * npairs)
+        vals[0::2] = r * np.cos(2 * math.pi * u2)
+        vals[1::2] = r * np.sin(2 * math.pi * u2)
+        out[:, c] = vals[:K]
+    return out

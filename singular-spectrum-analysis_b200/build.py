@@ -1,0 +1,90 @@
+"""Builds libssa.so (the drop-in SSA library) in this directory.
+
+C host sources are compiled with gcc, the CUDA kernels with nvcc for sm_100a only, and
+everything is linked with the static CUDA runtime, so the library depends on the NVIDIA driver
+alone. Usage: ``python build.py`` (from anywhere) or ``build.build()``.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+INCLUDE = HERE.parent / "include"
+OUT = HERE / "libssa.so"
+BUILD = HERE / "_build"
+
+C_SOURCES = ["ssa_engine.c", "ssa_api.c", "ssa_batch.c", "ssa_mssa.c"]
+CU_SOURCES = ["ssa_kernels.cu"]
+
+NVCC_FLAGS = [
+    "-std=c++17", "-O3", "-lineinfo",
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-Xcompiler", "-fPIC,-fvisibility=hidden",
+]
+
+
+def _cuda_home() -> Path:
+    for c in (os.environ.get("CUDA_HOME"), "/usr/local/cuda"):
+        if c and (Path(c) / "bin" / "nvcc").exists():
+            return Path(c)
+    nv = shutil.which("nvcc")
+    if nv:
+        return Path(nv).resolve().parent.parent
+    raise RuntimeError("nvcc not found")
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build failed: " + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+
+
+def _stale(target: Path, deps: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    cuda = _cuda_home()
+    nvcc = str(cuda / "bin" / "nvcc")
+    BUILD.mkdir(exist_ok=True)
+    headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    objs = []
+    for src in CU_SOURCES:
+        s = CSRC / src
+        o = BUILD / (s.stem + ".cu.o")
+        if force or _stale(o, [s] + headers):
+            cmd = [nvcc, *NVCC_FLAGS, "-I", str(CSRC), "-I", str(INCLUDE), "-c", str(s), "-o", str(o)]
+            if verbose:
+                print(" ".join(cmd))
+            _run(cmd)
+        objs.append(o)
+    for src in C_SOURCES:
+        s = CSRC / src
+        o = BUILD / (s.stem + ".c.o")
+        if force or _stale(o, [s] + headers):
+            cmd = ["gcc", "-std=gnu11", "-O2", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-parameter",
+                   "-I", str(cuda / "include"), "-I", str(CSRC), "-I", str(INCLUDE), "-c", str(s), "-o", str(o)]
+            if verbose:
+                print(" ".join(cmd))
+            _run(cmd)
+        objs.append(o)
+    if force or _stale(OUT, objs):
+        cmd = [nvcc, "-shared", "-cudart", "static", "-gencode", "arch=compute_100a,code=sm_100a",
+               "-o", str(OUT), *map(str, objs), "-lm"]
+        if verbose:
+            print(" ".join(cmd))
+        _run(cmd)
+    return OUT
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)
+    print(OUT)

@@ -1,0 +1,932 @@
+/*
+ * The SSA-Opt C API (MKL/ssa_opt.h:318-430) on the B200 device engine, one series per context.
+ *
+ * Every call validates its arguments exactly where the reference does, enqueues the device
+ * pipeline on the context's stream, waits for it and mirrors results into the host fields of
+ * SSA_Opt (sigma, eigenvalues, U, V). Return codes follow the reference: 0 / -1, counts for
+ * the getters, 0.0 from double-valued getters on error.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <cuda_runtime_api.h>
+
+#include "ssa_engine.h"
+#include "../../include/ssa_opt.h"
+
+struct ssa_gpu_ctx
+{
+    ssa_engine e;
+    int engine_ok;
+    int kp_cap, k_cap;          /* prepared capacity */
+    int spectra_valid;          /* device spectra of sigma_i u_i and v_i are current */
+    int wcorr_valid;            /* e.W holds the W-correlation of the current decomposition */
+    int *d_group;
+    int group_cap;
+    double *d_out;              /* N (+ forecast) doubles */
+    double *d_lrf;              /* R (L) + buf (L + h) + out (h) + verticality */
+    size_t lrf_cap;
+    int *d_status;
+    float *h_stage;             /* pinned float staging, max(L, K) * k_cap */
+    size_t stage_cap;
+    float *d_omega;             /* K x kp caller-supplied test matrix (float) */
+};
+
+#define SSA_DEFAULT_SEED 42ULL
+
+static int imin(int a, int b) { return a < b ? a : b; }
+
+static void gpu_free(struct ssa_gpu_ctx *g)
+{
+    if (!g)
+        return;
+    if (g->engine_ok)
+        ssae_destroy(&g->e);
+    if (g->d_group)
+        cudaFree(g->d_group);
+    if (g->d_out)
+        cudaFree(g->d_out);
+    if (g->d_lrf)
+        cudaFree(g->d_lrf);
+    if (g->d_status)
+        cudaFree(g->d_status);
+    if (g->d_omega)
+        cudaFree(g->d_omega);
+    if (g->h_stage)
+        cudaFreeHost(g->h_stage);
+    free(g);
+}
+
+static int sync_ok(struct ssa_gpu_ctx *g)
+{
+    if (cudaStreamSynchronize(g->e.st) != cudaSuccess)
+        return -1;
+    return 0;
+}
+
+static int ensure_group(struct ssa_gpu_ctx *g, const int *group, int n)
+{
+    if (n > g->group_cap)
+    {
+        if (g->d_group)
+            cudaFree(g->d_group);
+        g->d_group = NULL;
+        int cap = n < 64 ? 64 : n;
+        if (cudaMalloc((void **)&g->d_group, sizeof(int) * cap) != cudaSuccess)
+        {
+            g->group_cap = 0;
+            return -1;
+        }
+        g->group_cap = cap;
+    }
+    return cudaMemcpyAsync(g->d_group, group, sizeof(int) * n, cudaMemcpyHostToDevice, g->e.st) == cudaSuccess ? 0 : -1;
+}
+
+static int ensure_stage(struct ssa_gpu_ctx *g, size_t floats)
+{
+    if (floats <= g->stage_cap)
+        return 0;
+    if (g->h_stage)
+        cudaFreeHost(g->h_stage);
+    g->h_stage = NULL;
+    g->stage_cap = 0;
+    if (cudaMallocHost((void **)&g->h_stage, floats * sizeof(float)) != cudaSuccess)
+        return -1;
+    g->stage_cap = floats;
+    return 0;
+}
+
+/* Copy the signal spectrum into the host field fft_x (interleaved, r2c_len complex). */
+static int mirror_spectrum(SSA_Opt *ssa)
+{
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    const int n = 2 * ssa->r2c_len;
+    if (ensure_stage(g, (size_t)n) != 0)
+        return -1;
+    if (cudaMemcpyAsync(g->h_stage, g->e.X, sizeof(float) * n, cudaMemcpyDeviceToHost, g->e.st) != cudaSuccess)
+        return -1;
+    if (sync_ok(g) != 0)
+        return -1;
+    for (int i = 0; i < n; i++)
+        ssa->fft_x[i] = (double)g->h_stage[i];
+    return 0;
+}
+
+int ssa_opt_init(SSA_Opt *ssa, const ssa_real *x, int N, int L)
+{
+    if (!ssa || !x || N < 4 || L < 2 || L > N - 1)
+        return -1;
+    memset(ssa, 0, sizeof(SSA_Opt));
+    const int logh = ssad_logh_for(N);
+    if (logh > 14)
+        return -1;
+    ssa->N = N;
+    ssa->L = L;
+    ssa->K = N - L + 1;
+    ssa->fft_len = 2 << logh;
+    ssa->r2c_len = (1 << logh) + 1;
+    ssa->batch_size = 1;
+    struct ssa_gpu_ctx *g = (struct ssa_gpu_ctx *)calloc(1, sizeof(*g));
+    if (!g)
+        return -1;
+    ssa->gpu = g;
+    /* Engine with room for k + p = min(SSA_MAX_KP, L, K) columns; prepare() narrows it. */
+    int kp = imin(SSA_MAX_KP, imin(L, ssa->K));
+    if (ssae_create(&g->e, 1, N, L, kp, kp, NULL) != 0)
+    {
+        free(g);
+        ssa->gpu = NULL;
+        return -1;
+    }
+    g->engine_ok = 1;
+    ssa->fft_x = (double *)malloc(sizeof(double) * 2 * ssa->r2c_len);
+    ssa->ws_real = (double *)malloc(sizeof(double) * (N > ssa->fft_len ? N : ssa->fft_len));
+    ssa->ws_complex = (double *)malloc(sizeof(double) * 2 * ssa->r2c_len);
+    ssa->inv_diag_count = (double *)malloc(sizeof(double) * N);
+    if (!ssa->fft_x || !ssa->ws_real || !ssa->ws_complex || !ssa->inv_diag_count ||
+        cudaMalloc((void **)&g->d_out, sizeof(double) * (size_t)N) != cudaSuccess)
+    {
+        ssa_opt_free(ssa);
+        return -1;
+    }
+    for (int t = 0; t < N; t++)
+    {
+        int c = imin(imin(t + 1, L), imin(ssa->K, N - t));
+        ssa->inv_diag_count[t] = c > 0 ? 1.0 / c : 0.0;
+    }
+    if (cudaMemcpyAsync(g->e.x64, x, sizeof(double) * N, cudaMemcpyHostToDevice, g->e.st) != cudaSuccess ||
+        ssae_signal_spectrum(&g->e, g->e.x64, 1) != 0 || mirror_spectrum(ssa) != 0)
+    {
+        ssa_opt_free(ssa);
+        return -1;
+    }
+    ssae_reset_jobs(&g->e);
+    ssa->initialized = true;
+    return 0;
+}
+
+static void free_results(SSA_Opt *ssa)
+{
+    free(ssa->U);
+    free(ssa->V);
+    free(ssa->sigma);
+    free(ssa->eigenvalues);
+    ssa->U = ssa->V = ssa->sigma = ssa->eigenvalues = NULL;
+}
+
+void ssa_opt_free(SSA_Opt *ssa)
+{
+    if (!ssa)
+        return;
+    gpu_free(ssa->gpu);
+    free_results(ssa);
+    free(ssa->fft_x);
+    free(ssa->ws_real);
+    free(ssa->ws_complex);
+    free(ssa->inv_diag_count);
+    free(ssa->decomp_Omega);
+    memset(ssa, 0, sizeof(SSA_Opt));
+}
+
+void ssa_opt_free_prepared(SSA_Opt *ssa)
+{
+    if (!ssa)
+        return;
+    free(ssa->decomp_Omega);
+    ssa->decomp_Omega = NULL;
+    ssa->prepared_kp = 0;
+    ssa->prepared_lwork = 0;
+    ssa->prepared = false;
+}
+
+static int alloc_results(SSA_Opt *ssa, int k)
+{
+    free_results(ssa);
+    ssa->U = (double *)calloc((size_t)ssa->L * k, sizeof(double));
+    ssa->V = (double *)calloc((size_t)ssa->K * k, sizeof(double));
+    ssa->sigma = (double *)calloc((size_t)k, sizeof(double));
+    ssa->eigenvalues = (double *)calloc((size_t)k, sizeof(double));
+    if (!ssa->U || !ssa->V || !ssa->sigma || !ssa->eigenvalues)
+    {
+        free_results(ssa);
+        return -1;
+    }
+    return 0;
+}
+
+int ssa_opt_prepare(SSA_Opt *ssa, int max_k, int oversampling)
+{
+    if (!ssa || !ssa->initialized || max_k < 1)
+        return -1;
+    ssa_opt_free_prepared(ssa);
+    const int L = ssa->L, K = ssa->K;
+    const int p = oversampling <= 0 ? 8 : oversampling;
+    int kp = max_k + p;
+    kp = imin(kp, imin(L, K));
+    const int actual_k = imin(max_k, kp);
+    if (kp > SSA_MAX_KP)
+        return -1;
+    ssa->decomp_Omega = (double *)malloc(sizeof(double) * (size_t)K * kp);
+    if (!ssa->decomp_Omega || alloc_results(ssa, actual_k) != 0)
+    {
+        ssa_opt_free_prepared(ssa);
+        return -1;
+    }
+    ssa->n_components = actual_k;
+    ssa->prepared_kp = kp;
+    ssa->prepared = true;
+    return 0;
+}
+
+int ssa_opt_update_signal(SSA_Opt *ssa, const ssa_real *new_x)
+{
+    if (!ssa || !ssa->initialized || !new_x)
+        return -1;
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    ssa_opt_free_cached_ffts(ssa);
+    ssa->decomposed = false;
+    g->spectra_valid = 0;
+    g->wcorr_valid = 0;
+    ssae_reset_jobs(&g->e);
+    if (cudaMemcpyAsync(g->e.x64, new_x, sizeof(double) * ssa->N, cudaMemcpyHostToDevice, g->e.st) != cudaSuccess ||
+        ssae_signal_spectrum(&g->e, g->e.x64, 1) != 0 || mirror_spectrum(ssa) != 0)
+        return -1;
+    return 0;
+}
+
+/* Download U (L x k), V (K x k), sigma into the host fields. */
+static int mirror_results(SSA_Opt *ssa, int k)
+{
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    ssa_engine *e = &g->e;
+    const int L = ssa->L, K = ssa->K;
+    if (ensure_stage(g, (size_t)(L > K ? L : K) * k) != 0)
+        return -1;
+    if (cudaMemcpy2DAsync(g->h_stage, sizeof(float) * L, e->Y, sizeof(float) * e->ldL, sizeof(float) * L, k,
+                          cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
+        cudaMemcpyAsync(ssa->sigma, e->sigma, sizeof(double) * k, cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
+        sync_ok(g) != 0)
+        return -1;
+    for (size_t i = 0; i < (size_t)L * k; i++)
+        ssa->U[i] = (double)g->h_stage[i];
+    if (cudaMemcpy2DAsync(g->h_stage, sizeof(float) * K, e->Z, sizeof(float) * e->ldK, sizeof(float) * K, k,
+                          cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
+        sync_ok(g) != 0)
+        return -1;
+    for (size_t i = 0; i < (size_t)K * k; i++)
+        ssa->V[i] = (double)g->h_stage[i];
+    ssa->total_variance = 0.0;
+    for (int i = 0; i < k; i++)
+    {
+        ssa->eigenvalues[i] = ssa->sigma[i] * ssa->sigma[i];
+        ssa->total_variance += ssa->eigenvalues[i];
+    }
+    return 0;
+}
+
+static int check_status(struct ssa_gpu_ctx *g)
+{
+    int st = 0;
+    if (cudaMemcpy(&st, g->e.status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -1;
+    return st == 0 ? 0 : -1;
+}
+
+/* Shared body of the randomized decompositions: Omega = host matrix (K x kp, column-major,
+ * double) or NULL for the device generator. */
+static int decompose_randomized_impl(SSA_Opt *ssa, int k, int oversampling, int q, const double *Omega)
+{
+    if (!ssa || !ssa->initialized || k < 1 || q < 0)
+        return -1;
+    ssa_opt_free_cached_ffts(ssa);
+    const int L = ssa->L, K = ssa->K;
+    const int p = oversampling <= 0 ? 8 : oversampling;
+    int kp = imin(k + p, imin(L, K));
+    k = imin(k, kp);
+    if (!ssa->prepared || kp > ssa->prepared_kp)
+        return -1;
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    ssa_engine *e = &g->e;
+    ssae_reset_jobs(e);
+    g->spectra_valid = 0;
+    g->wcorr_valid = 0;
+    ssa->decomposed = false;
+    ssa->n_components = k;
+    int rc = 0;
+    if (Omega)
+    {
+        if (ensure_stage(g, (size_t)K * kp) != 0)
+            return -1;
+        for (size_t i = 0; i < (size_t)K * kp; i++)
+            g->h_stage[i] = (float)Omega[i];
+        rc |= cudaMemcpy2DAsync(e->Z, sizeof(float) * e->ldK, g->h_stage, sizeof(float) * K, sizeof(float) * K, kp,
+                                cudaMemcpyHostToDevice, e->st) != cudaSuccess;
+        rc |= ssae_decompose(e, 1, kp, k, q, e->Z, e->ldK, 0) != 0;
+    }
+    else
+    {
+        const unsigned long long seed = SSA_DEFAULT_SEED + 0x100000000ULL * (unsigned long long)ssa->rng_calls;
+        ssa->rng_calls++;
+        rc |= ssae_decompose(e, 1, kp, k, q, NULL, 0, seed) != 0;
+    }
+    if (rc || sync_ok(g) != 0 || check_status(g) != 0 || mirror_results(ssa, k) != 0)
+        return -1;
+    ssa->decomposed = true;
+    return 0;
+}
+
+int ssa_opt_decompose_randomized(SSA_Opt *ssa, int k, int oversampling)
+{
+    return decompose_randomized_impl(ssa, k, oversampling, 0, NULL);
+}
+
+int ssa_opt_decompose_randomized_ex(SSA_Opt *ssa, int k, int oversampling, int power_iters, const double *Omega)
+{
+    return decompose_randomized_impl(ssa, k, oversampling, power_iters, Omega);
+}
+
+/* Sequential and extend decompositions (MKL/ssa_opt.h:1560-1678, :1935-2056) are outside the
+ * accelerated path; the symbols exist for the wrapper and report failure. */
+int ssa_opt_decompose(SSA_Opt *ssa, int k, int max_iter)
+{
+    (void)ssa;
+    (void)k;
+    (void)max_iter;
+    return -1;
+}
+
+int ssa_opt_extend(SSA_Opt *ssa, int additional_k, int max_iter)
+{
+    (void)ssa;
+    (void)additional_k;
+    (void)max_iter;
+    return -1;
+}
+
+int ssa_opt_decompose_block(SSA_Opt *ssa, int k, int block_size, int max_iter)
+{
+    (void)ssa;
+    (void)k;
+    (void)block_size;
+    (void)max_iter;
+    return -1;
+}
+
+/* ---- spectra cache and reconstruction -------------------------------------------------- */
+
+static int ensure_spectra(const SSA_Opt *ssa)
+{
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    if (g->spectra_valid)
+        return 0;
+    if (ssae_spectra(&g->e, 1, ssa->n_components) != 0)
+        return -1;
+    g->spectra_valid = 1;
+    return 0;
+}
+
+int ssa_opt_cache_ffts(SSA_Opt *ssa)
+{
+    if (!ssa || !ssa->decomposed)
+        return -1;
+    ssae_reset_jobs(&ssa->gpu->e);
+    if (ensure_spectra(ssa) != 0 || sync_ok(ssa->gpu) != 0)
+        return -1;
+    ssa->fft_cached = true;
+    return 0;
+}
+
+void ssa_opt_free_cached_ffts(SSA_Opt *ssa)
+{
+    if (!ssa)
+        return;
+    ssa->fft_cached = false;
+    /* Device spectra stay allocated and are recomputed after the next decomposition. */
+}
+
+/* Device reconstruction of `group` into g->d_out (not synchronised). */
+static int recon_device(const SSA_Opt *ssa, const int *group, int n_group)
+{
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    if (ensure_spectra(ssa) != 0 || ensure_group(g, group, n_group) != 0)
+        return -1;
+    return ssae_recon_group(&g->e, 0, ssa->n_components, g->d_group, n_group, g->d_out) != 0 ? -1 : 0;
+}
+
+int ssa_opt_reconstruct(const SSA_Opt *ssa, const int *group, int n_group, ssa_real *output)
+{
+    if (!ssa || !ssa->decomposed || !group || !output || n_group < 1)
+        return -1;
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    ssae_reset_jobs(&g->e);
+    if (recon_device(ssa, group, n_group) != 0 ||
+        cudaMemcpyAsync(output, g->d_out, sizeof(double) * ssa->N, cudaMemcpyDeviceToHost, g->e.st) != cudaSuccess ||
+        sync_ok(g) != 0)
+        return -1;
+    return 0;
+}
+
+/* ---- W-correlation ---------------------------------------------------------------------- */
+
+static int wcorr_device(const SSA_Opt *ssa)
+{
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    if (g->wcorr_valid)
+        return 0;
+    const int k = ssa->n_components;
+    ssae_reset_jobs(&g->e);
+    if (ssae_elem_recon(&g->e, 1, k) != 0 || ssae_wcorr(&g->e, 1, k) != 0 || sync_ok(g) != 0)
+        return -1;
+    g->wcorr_valid = 1;
+    return 0;
+}
+
+int ssa_opt_wcorr_matrix(const SSA_Opt *ssa, ssa_real *W)
+{
+    if (!ssa || !ssa->decomposed || !W)
+        return -1;
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    const int k = ssa->n_components;
+    if (wcorr_device(ssa) != 0 ||
+        cudaMemcpy(W, g->e.W, sizeof(double) * k * k, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -1;
+    return 0;
+}
+
+int ssa_opt_wcorr_matrix_fast(const SSA_Opt *ssa, ssa_real *W) { return ssa_opt_wcorr_matrix(ssa, W); }
+
+ssa_real ssa_opt_wcorr_pair(const SSA_Opt *ssa, int i, int j)
+{
+    if (!ssa || !ssa->decomposed || i < 0 || i >= ssa->n_components || j < 0 || j >= ssa->n_components)
+        return 0.0;
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    const int k = ssa->n_components;
+    double w = 0.0;
+    if (wcorr_device(ssa) != 0 ||
+        cudaMemcpy(&w, g->e.W + (size_t)i * k + j, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return 0.0;
+    return w;
+}
+
+/* ---- LRF / forecast --------------------------------------------------------------------- */
+
+static int ensure_lrf(struct ssa_gpu_ctx *g, size_t doubles)
+{
+    if (doubles <= g->lrf_cap)
+        return 0;
+    if (g->d_lrf)
+        cudaFree(g->d_lrf);
+    g->d_lrf = NULL;
+    g->lrf_cap = 0;
+    if (cudaMalloc((void **)&g->d_lrf, sizeof(double) * doubles) != cudaSuccess)
+        return -1;
+    if (!g->d_status && cudaMalloc((void **)&g->d_status, sizeof(int)) != cudaSuccess)
+        return -1;
+    g->lrf_cap = doubles;
+    return 0;
+}
+
+/* LRF of `group` and, with h > 0, the forecast over the reconstruction of the group.
+ * Host outputs: R (L-1, may be NULL), verticality, fc (h). Returns 0 or -1 (verticality). */
+static int lrf_forecast(const SSA_Opt *ssa, const int *group, int n_group, int h, double *R, double *vert,
+                        double *fc, double *recon_out)
+{
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    const int L = ssa->L, N = ssa->N;
+    if (n_group > SSA_MAX_KP)
+        return -1;
+    ssae_reset_jobs(&g->e);
+    if (ensure_lrf(g, (size_t)(L - 1) + (size_t)(L - 1 + h) + (size_t)h + 1) != 0)
+        return -1;
+    double *dR = g->d_lrf, *dbuf = dR + (L - 1), *dout = dbuf + (L - 1 + h), *dvert = dout + h;
+    if (recon_device(ssa, group, n_group) != 0)
+        return -1;
+    ssa_lrf_job J;
+    memset(&J, 0, sizeof(J));
+    J.U = g->e.Y;
+    J.group = g->d_group;
+    J.recon = g->d_out;
+    J.R = dR;
+    J.buf = dbuf;
+    J.out = dout;
+    J.verticality = dvert;
+    J.status = g->d_status;
+    J.ld = g->e.ldL;
+    J.L = L;
+    J.N = N;
+    J.n_group = n_group;
+    J.h = h;
+    J.k = ssa->n_components;
+    void *d = ssae_push_jobs(&g->e, &J, sizeof(J));
+    if (!d || cudaMemsetAsync(g->d_status, 0, sizeof(int), g->e.st) != cudaSuccess ||
+        ssad_lrf((const ssa_lrf_job *)d, 1, g->e.st) != 0)
+        return -1;
+    int st = 0;
+    if (cudaMemcpyAsync(&st, g->d_status, sizeof(int), cudaMemcpyDeviceToHost, g->e.st) != cudaSuccess ||
+        cudaMemcpyAsync(vert, dvert, sizeof(double), cudaMemcpyDeviceToHost, g->e.st) != cudaSuccess ||
+        sync_ok(g) != 0)
+        return -1;
+    if (st != 0)
+        return -1;
+    if (R && cudaMemcpy(R, dR, sizeof(double) * (L - 1), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -1;
+    if (h > 0 && cudaMemcpy(fc, dout, sizeof(double) * h, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -1;
+    if (recon_out && cudaMemcpy(recon_out, g->d_out, sizeof(double) * N, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -1;
+    return 0;
+}
+
+static int group_in_range(const SSA_Opt *ssa, const int *group, int n_group)
+{
+    for (int i = 0; i < n_group; i++)
+        if (group[i] < 0 || group[i] >= ssa->n_components)
+            return 0;
+    return 1;
+}
+
+int ssa_opt_compute_lrf(const SSA_Opt *ssa, const int *group, int n_group, SSA_LRF *lrf)
+{
+    if (!ssa || !ssa->decomposed || !group || !lrf || n_group < 1)
+        return -1;
+    memset(lrf, 0, sizeof(SSA_LRF));
+    lrf->L = ssa->L;
+    lrf->valid = false;
+    if (!group_in_range(ssa, group, n_group))
+        return -1;
+    lrf->R = (double *)malloc(sizeof(double) * (ssa->L - 1));
+    if (!lrf->R)
+        return -1;
+    double vert = 0.0;
+    int rc = lrf_forecast(ssa, group, n_group, 0, lrf->R, &vert, NULL, NULL);
+    lrf->verticality = vert;
+    if (rc != 0)
+    {
+        free(lrf->R);
+        lrf->R = NULL;
+        return -1;
+    }
+    lrf->valid = true;
+    return 0;
+}
+
+void ssa_opt_lrf_free(SSA_LRF *lrf)
+{
+    if (!lrf)
+        return;
+    free(lrf->R);
+    memset(lrf, 0, sizeof(SSA_LRF));
+}
+
+int ssa_opt_forecast(const SSA_Opt *ssa, const int *group, int n_group, int n_forecast, ssa_real *output)
+{
+    if (!ssa || !ssa->decomposed || !group || !output || n_group < 1 || n_forecast < 1)
+        return -1;
+    if (!group_in_range(ssa, group, n_group))
+        return -1;
+    double vert;
+    return lrf_forecast(ssa, group, n_group, n_forecast, NULL, &vert, output, NULL);
+}
+
+int ssa_opt_forecast_full(const SSA_Opt *ssa, const int *group, int n_group, int n_forecast, ssa_real *output)
+{
+    if (!ssa || !ssa->decomposed || !group || !output || n_group < 1 || n_forecast < 1)
+        return -1;
+    if (!group_in_range(ssa, group, n_group))
+        return -1;
+    double vert;
+    return lrf_forecast(ssa, group, n_group, n_forecast, NULL, &vert, output + ssa->N, output);
+}
+
+/* The recurrence of MKL/ssa_opt.h:2818-2841 over caller-provided host data. Everything here is
+ * host memory by contract (an LRF and a base signal), so the h dependent dot products run on
+ * the device only when a context is at hand; this entry point has none, so it runs them here. */
+int ssa_opt_forecast_with_lrf(const SSA_LRF *lrf, const ssa_real *base_signal, int base_len, int n_forecast,
+                              ssa_real *output)
+{
+    if (!lrf || !lrf->valid || !lrf->R || !base_signal || !output)
+        return -1;
+    const int L = lrf->L;
+    if (base_len < L - 1 || n_forecast < 1)
+        return -1;
+    const int w = L - 1;
+    double *buf = (double *)malloc(sizeof(double) * (size_t)(w + n_forecast));
+    if (!buf)
+        return -1;
+    for (int i = 0; i < w; i++)
+        buf[i] = base_signal[base_len - w + i];
+    for (int h = 0; h < n_forecast; h++)
+    {
+        double f = 0.0;
+        for (int j = 0; j < w; j++)
+            f += lrf->R[j] * buf[h + j];
+        buf[w + h] = f;
+        output[h] = f;
+    }
+    free(buf);
+    return 0;
+}
+
+/* ---- getters (MKL/ssa_opt.h:3086-3145) -------------------------------------------------- */
+
+int ssa_opt_get_trend(const SSA_Opt *ssa, ssa_real *output)
+{
+    int group[] = {0};
+    return ssa_opt_reconstruct(ssa, group, 1, output);
+}
+
+int ssa_opt_get_noise(const SSA_Opt *ssa, int noise_start, ssa_real *output)
+{
+    if (!ssa || !ssa->decomposed || noise_start < 0)
+        return -1;
+    int n_noise = ssa->n_components - noise_start;
+    if (n_noise <= 0)
+    {
+        memset(output, 0, sizeof(double) * ssa->N);
+        return 0;
+    }
+    int *group = (int *)malloc(sizeof(int) * n_noise);
+    if (!group)
+        return -1;
+    for (int i = 0; i < n_noise; i++)
+        group[i] = noise_start + i;
+    int ret = ssa_opt_reconstruct(ssa, group, n_noise, output);
+    free(group);
+    return ret;
+}
+
+ssa_real ssa_opt_variance_explained(const SSA_Opt *ssa, int start, int end)
+{
+    if (!ssa || !ssa->decomposed || start < 0 || ssa->total_variance <= 0)
+        return 0.0;
+    if (end < 0 || end >= ssa->n_components)
+        end = ssa->n_components - 1;
+    double sum = 0;
+    for (int i = start; i <= end; i++)
+        sum += ssa->eigenvalues[i];
+    return sum / ssa->total_variance;
+}
+
+int ssa_opt_get_singular_values(const SSA_Opt *ssa, ssa_real *output, int max_n)
+{
+    if (!ssa || !ssa->decomposed || !output)
+        return -1;
+    int n = imin(max_n, ssa->n_components);
+    memcpy(output, ssa->sigma, sizeof(double) * n);
+    return n;
+}
+
+int ssa_opt_get_eigenvalues(const SSA_Opt *ssa, ssa_real *output, int max_n)
+{
+    if (!ssa || !ssa->decomposed || !output)
+        return -1;
+    int n = imin(max_n, ssa->n_components);
+    memcpy(output, ssa->eigenvalues, sizeof(double) * n);
+    return n;
+}
+
+ssa_real ssa_opt_get_total_variance(const SSA_Opt *ssa)
+{
+    if (!ssa || !ssa->decomposed)
+        return 0.0;
+    return ssa->total_variance;
+}
+
+/* ---- component statistics and periodic pairs (MKL/ssa_opt.h:2634-2756) ------------------ */
+
+int ssa_opt_component_stats(const SSA_Opt *ssa, SSA_ComponentStats *stats)
+{
+    if (!ssa || !ssa->decomposed || !stats)
+        return -1;
+    int n = ssa->n_components;
+    if (n < 2)
+        return -1;
+    memset(stats, 0, sizeof(SSA_ComponentStats));
+    stats->n = n;
+    stats->singular_values = (double *)malloc(sizeof(double) * n);
+    stats->log_sv = (double *)malloc(sizeof(double) * n);
+    stats->gaps = (double *)malloc(sizeof(double) * (n - 1));
+    stats->cumulative_var = (double *)malloc(sizeof(double) * n);
+    stats->second_diff = (double *)malloc(sizeof(double) * n);
+    if (!stats->singular_values || !stats->log_sv || !stats->gaps || !stats->cumulative_var || !stats->second_diff)
+    {
+        ssa_opt_component_stats_free(stats);
+        return -1;
+    }
+    for (int i = 0; i < n; i++)
+    {
+        stats->singular_values[i] = ssa->sigma[i];
+        stats->log_sv[i] = log(ssa->sigma[i] + 1e-300);
+    }
+    double max_gap = 0.0;
+    int max_gap_idx = 0;
+    for (int i = 0; i < n - 1; i++)
+    {
+        double gap = ssa->sigma[i] / (ssa->sigma[i + 1] + 1e-300);
+        stats->gaps[i] = gap;
+        if (gap > max_gap)
+        {
+            max_gap = gap;
+            max_gap_idx = i;
+        }
+    }
+    double cumsum = 0.0;
+    for (int i = 0; i < n; i++)
+    {
+        cumsum += ssa->eigenvalues[i];
+        stats->cumulative_var[i] = cumsum / ssa->total_variance;
+    }
+    stats->second_diff[0] = 0.0;
+    stats->second_diff[n - 1] = 0.0;
+    for (int i = 1; i < n - 1; i++)
+        stats->second_diff[i] = stats->log_sv[i - 1] - 2.0 * stats->log_sv[i] + stats->log_sv[i + 1];
+    stats->suggested_signal = max_gap_idx + 1;
+    stats->gap_threshold = max_gap;
+    return 0;
+}
+
+void ssa_opt_component_stats_free(SSA_ComponentStats *stats)
+{
+    if (!stats)
+        return;
+    free(stats->singular_values);
+    free(stats->log_sv);
+    free(stats->gaps);
+    free(stats->cumulative_var);
+    free(stats->second_diff);
+    memset(stats, 0, sizeof(SSA_ComponentStats));
+}
+
+int ssa_opt_find_periodic_pairs(const SSA_Opt *ssa, int *pairs, int max_pairs, ssa_real sv_tol,
+                                ssa_real wcorr_thresh)
+{
+    if (!ssa || !ssa->decomposed || !pairs || max_pairs < 1)
+        return 0;
+    if (sv_tol <= 0)
+        sv_tol = 0.1;
+    if (wcorr_thresh <= 0)
+        wcorr_thresh = 0.5;
+    const int n = ssa->n_components;
+    double *W = (double *)malloc(sizeof(double) * n * n);
+    char *used = (char *)calloc((size_t)n, 1);
+    if (!W || !used || ssa_opt_wcorr_matrix(ssa, W) != 0)
+    {
+        free(W);
+        free(used);
+        return 0;
+    }
+    int n_pairs = 0;
+    for (int i = 0; i < n - 1 && n_pairs < max_pairs; i++)
+    {
+        if (used[i])
+            continue;
+        for (int j = i + 1; j < n && n_pairs < max_pairs; j++)
+        {
+            if (used[j])
+                continue;
+            double sv_ratio = ssa->sigma[j] / (ssa->sigma[i] + 1e-300);
+            if (fabs(1.0 - sv_ratio) > sv_tol)
+                continue;
+            if (fabs(W[i * n + j]) < wcorr_thresh)
+                continue;
+            pairs[2 * n_pairs] = i;
+            pairs[2 * n_pairs + 1] = j;
+            used[i] = used[j] = 1;
+            n_pairs++;
+            break;
+        }
+    }
+    free(W);
+    free(used);
+    return n_pairs;
+}
+
+/* ---- out-of-scope symbols kept for the wrapper's optional bindings ---------------------- */
+
+int ssa_opt_vforecast(const SSA_Opt *ssa, const int *group, int n_group, int n_forecast, ssa_real *output)
+{
+    (void)ssa, (void)group, (void)n_group, (void)n_forecast, (void)output;
+    return -1;
+}
+int ssa_opt_vforecast_full(const SSA_Opt *ssa, const int *group, int n_group, int n_forecast, ssa_real *output)
+{
+    (void)ssa, (void)group, (void)n_group, (void)n_forecast, (void)output;
+    return -1;
+}
+int ssa_opt_vforecast_fast(const SSA_Opt *ssa, const int *group, int n_group, const ssa_real *base_signal,
+                           int base_len, int n_forecast, ssa_real *output)
+{
+    (void)ssa, (void)group, (void)n_group, (void)base_signal, (void)base_len, (void)n_forecast, (void)output;
+    return -1;
+}
+int ssa_opt_parestimate(const SSA_Opt *ssa, const int *group, int n_group, SSA_ParEstimate *result)
+{
+    (void)ssa, (void)group, (void)n_group;
+    if (result)
+        memset(result, 0, sizeof(*result));
+    return -1;
+}
+void ssa_opt_parestimate_free(SSA_ParEstimate *result)
+{
+    if (!result)
+        return;
+    free(result->periods);
+    free(result->frequencies);
+    free(result->moduli);
+    free(result->rates);
+    memset(result, 0, sizeof(*result));
+}
+int ssa_opt_gapfill(ssa_real *x, int N, int L, int rank, int max_iter, ssa_real tol, SSA_GapFillResult *result)
+{
+    (void)x, (void)N, (void)L, (void)rank, (void)max_iter, (void)tol;
+    if (result)
+        memset(result, 0, sizeof(*result));
+    return -1;
+}
+int ssa_opt_gapfill_simple(ssa_real *x, int N, int L, int rank, SSA_GapFillResult *result)
+{
+    (void)x, (void)N, (void)L, (void)rank;
+    if (result)
+        memset(result, 0, sizeof(*result));
+    return -1;
+}
+
+/* ---- MKL tuning exports of MKL/py/ssa_wrapper.c:47-123 ---------------------------------- */
+int ssa_mkl_init(int verbose)
+{
+    (void)verbose;
+    return 0;
+}
+int ssa_mkl_init_14900kf(int verbose)
+{
+    (void)verbose;
+    return 0;
+}
+int ssa_mkl_init_generic(int verbose)
+{
+    (void)verbose;
+    return 0;
+}
+void ssa_mkl_set_threads(int n) { (void)n; }
+int ssa_mkl_get_threads(void) { return 1; }
+void ssa_mkl_get_cpu_info(int *p_cores, int *e_cores, int *is_hybrid, int *has_avx512)
+{
+    if (p_cores)
+        *p_cores = 0;
+    if (e_cores)
+        *e_cores = 0;
+    if (is_hybrid)
+        *is_hybrid = 0;
+    if (has_avx512)
+        *has_avx512 = 0;
+}
+void ssa_mkl_disable_affinity(void) {}
+
+/* ---- matvec diagnostics (reference static helpers MKL/ssa_opt.h:871-903) ----------------- */
+static int matvec_dev(SSA_Opt *ssa, const double *in, double *out, int adjoint)
+{
+    if (!ssa || !ssa->initialized || !in || !out)
+        return -1;
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    ssa_engine *e = &g->e;
+    const int nin = adjoint ? ssa->L : ssa->K, nout = adjoint ? ssa->K : ssa->L;
+    float *dst_in = adjoint ? e->Y : e->Z, *src_out = adjoint ? e->Z : e->Y;
+    if (ensure_stage(g, (size_t)(ssa->L > ssa->K ? ssa->L : ssa->K)) != 0)
+        return -1;
+    ssae_reset_jobs(e);
+    for (int i = 0; i < nin; i++)
+        g->h_stage[i] = (float)in[i];
+    if (cudaMemcpyAsync(dst_in, g->h_stage, sizeof(float) * nin, cudaMemcpyHostToDevice, e->st) != cudaSuccess ||
+        ssae_matvec(e, 1, adjoint) != 0 ||
+        cudaMemcpyAsync(g->h_stage, src_out, sizeof(float) * nout, cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
+        sync_ok(g) != 0)
+        return -1;
+    for (int i = 0; i < nout; i++)
+        out[i] = (double)g->h_stage[i];
+    /* the matvec overwrote the first columns of the factor buffers */
+    ssa->decomposed = false;
+    g->spectra_valid = 0;
+    g->wcorr_valid = 0;
+    return 0;
+}
+
+int ssa_opt_hankel_matvec_dev(SSA_Opt *ssa, const double *v, double *y) { return matvec_dev(ssa, v, y, 0); }
+int ssa_opt_hankel_matvec_T_dev(SSA_Opt *ssa, const double *u, double *z) { return matvec_dev(ssa, u, z, 1); }
+
+int ssa_opt_copy_factors(const SSA_Opt *ssa, double *U, double *V)
+{
+    if (!ssa || !ssa->decomposed)
+        return -1;
+    const int k = ssa->n_components;
+    if (U)
+        memcpy(U, ssa->U, sizeof(double) * (size_t)ssa->L * k);
+    if (V)
+        memcpy(V, ssa->V, sizeof(double) * (size_t)ssa->K * k);
+    return k;
+}
+
+/* ---- library information ----------------------------------------------------------------- */
+unsigned long long ssa_b200_kernel_launches(void) { return ssad_launch_count(); }
+int ssa_b200_sizeof_ssa_opt(void) { return (int)sizeof(SSA_Opt); }

@@ -1,0 +1,611 @@
+/*
+ * Device pipeline for B series (see ssa_engine.h). Every stage fills job tables on the host,
+ * stages them through pinned memory into device memory on the engine's stream and launches
+ * one kernel per stage over all series. Nothing here computes numbers on the CPU.
+ *
+ * Randomized decomposition (reference MKL/ssa_opt.h:1685-1763, plus q power iterations):
+ *   Y = H Omega; Q = CholQR2(Y);
+ *   repeat q times: Z = H^T Q; Z = CholQR(Z); Y = H Z; Q = CholQR2(Y);
+ *   B = H^T Q; B^T B = Z_r Lambda Z_r^T (FP64 Jacobi); sigma = sqrt(Lambda);
+ *   U = Q Z_r[:, :k], V = B Z_r[:, :k] Sigma^{-1}, signs so that sum_i U[i, j] >= 0.
+ */
+#include "ssa_engine.h"
+
+#include <stdlib.h>
+#include <string.h>
+
+#define CK(x)                              \
+    do                                     \
+    {                                      \
+        int _e = (int)(x);                 \
+        if (_e != 0)                       \
+            return _e;                     \
+    } while (0)
+
+static long long round4(long long v) { return (v + 3) & ~3LL; }
+static int imin(int a, int b) { return a < b ? a : b; }
+static int imax(int a, int b) { return a > b ? a : b; }
+
+static int gram_rows(int m, int B)
+{
+    /* Aim for about two CTAs per SM over all series; at least one staging chunk per CTA. */
+    int target = 296 / (B > 0 ? B : 1);
+    if (target < 1)
+        target = 1;
+    int rows = (m + target - 1) / target;
+    rows = ((rows + SSA_GRAM_CHUNK - 1) / SSA_GRAM_CHUNK) * SSA_GRAM_CHUNK;
+    return imax(rows, SSA_GRAM_CHUNK);
+}
+
+static int dmalloc(void **p, size_t bytes)
+{
+    *p = NULL;
+    if (bytes == 0)
+        return 0;
+    return (int)cudaMalloc(p, bytes);
+}
+
+int ssae_create(ssa_engine *e, int B, int N, int L, int kp, int k, cudaStream_t stream)
+{
+    memset(e, 0, sizeof(*e));
+    if (B < 1 || N < 4 || L < 2 || L > N - 1 || kp < 1 || kp > SSA_MAX_KP || k < 1 || k > kp)
+        return (int)cudaErrorInvalidValue;
+    int logh = ssad_logh_for(N);
+    if (logh > 14)
+        return (int)cudaErrorInvalidValue;
+    CK(cudaGetDevice(&e->device));
+    CK(ssad_init_device());
+    e->B = B;
+    e->N = N;
+    e->L = L;
+    e->K = N - L + 1;
+    e->logh = logh;
+    e->H = 1 << logh;
+    e->kp = kp;
+    e->k = k;
+    e->ldL = round4(L);
+    e->ldK = round4(e->K);
+    e->ldN = round4(N);
+    e->ldS = 2LL * (e->H + 1) + 2; /* floats; keeps every spectrum 16-byte aligned */
+    e->ldS = round4(e->ldS);
+    e->rows_L = gram_rows(L, B);
+    e->rows_K = gram_rows(e->K, B);
+    e->rows_N = gram_rows(N, B);
+    e->nch_L = (L + e->rows_L - 1) / e->rows_L;
+    e->nch_K = (e->K + e->rows_K - 1) / e->rows_K;
+    e->nch_N = (N + e->rows_N - 1) / e->rows_N;
+    e->nq = (L + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS;
+    if (stream)
+    {
+        e->st = stream;
+    }
+    else
+    {
+        CK(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+        e->own_stream = 1;
+    }
+    const size_t Bs = (size_t)B;
+    const int nchmax = imax(e->nch_L, imax(e->nch_K, e->nch_N));
+    const size_t np = (size_t)kp * (kp + 1) / 2;
+    int r = 0;
+    r |= dmalloc((void **)&e->x64, Bs * N * sizeof(double));
+    r |= dmalloc((void **)&e->X, Bs * e->ldS * sizeof(float));
+    r |= dmalloc((void **)&e->Y, Bs * e->ldL * kp * sizeof(float));
+    r |= dmalloc((void **)&e->Z, Bs * e->ldK * kp * sizeof(float));
+    r |= dmalloc((void **)&e->part, Bs * nchmax * np * sizeof(double));
+    r |= dmalloc((void **)&e->qsum, Bs * e->nq * kp * sizeof(double));
+    r |= dmalloc((void **)&e->Rinv, Bs * kp * kp * sizeof(float));
+    r |= dmalloc((void **)&e->Zu, Bs * kp * k * sizeof(float));
+    r |= dmalloc((void **)&e->Zv, Bs * kp * k * sizeof(float));
+    r |= dmalloc((void **)&e->sigma, Bs * k * sizeof(double));
+    r |= dmalloc((void **)&e->status, Bs * sizeof(int));
+    r |= dmalloc((void **)&e->norm2, Bs * k * sizeof(double));
+    r |= dmalloc((void **)&e->W, Bs * k * k * sizeof(double));
+    if (r)
+    {
+        ssae_destroy(e);
+        return (int)cudaErrorMemoryAllocation;
+    }
+    e->ja.cap = (size_t)B * 8192 + (1 << 20);
+    if (cudaMallocHost((void **)&e->ja.h, e->ja.cap) != cudaSuccess ||
+        cudaMalloc((void **)&e->ja.d, e->ja.cap) != cudaSuccess)
+    {
+        ssae_destroy(e);
+        return (int)cudaErrorMemoryAllocation;
+    }
+    CK(cudaMemsetAsync(e->status, 0, Bs * sizeof(int), e->st));
+    return 0;
+}
+
+int ssae_set_profiling(ssa_engine *e, int on)
+{
+    if (on && !e->ev[0])
+    {
+        for (int i = 0; i < 2 * SSA_PROF_MAX; i++)
+            if (cudaEventCreate(&e->ev[i]) != cudaSuccess)
+                return -1;
+    }
+    e->prof = on;
+    e->nev = 0;
+    for (int k = 0; k < SSAK_NKINDS; k++)
+    {
+        e->prof_ms[k] = 0.0;
+        e->prof_n[k] = 0;
+    }
+    return 0;
+}
+
+void ssae_prof_begin(ssa_engine *e, int kind)
+{
+    if (!e->prof || e->nev >= SSA_PROF_MAX)
+        return;
+    e->ev_kind[e->nev] = kind;
+    cudaEventRecord(e->ev[2 * e->nev], e->st);
+}
+
+void ssae_prof_end(ssa_engine *e)
+{
+    if (!e->prof || e->nev >= SSA_PROF_MAX)
+        return;
+    cudaEventRecord(e->ev[2 * e->nev + 1], e->st);
+    e->nev++;
+}
+
+int ssae_prof_collect(ssa_engine *e)
+{
+    if (!e->prof)
+        return 0;
+    if (cudaStreamSynchronize(e->st) != cudaSuccess)
+        return -1;
+    for (int i = 0; i < e->nev; i++)
+    {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, e->ev[2 * i], e->ev[2 * i + 1]) != cudaSuccess)
+            return -1;
+        e->prof_ms[e->ev_kind[i]] += ms;
+        e->prof_n[e->ev_kind[i]] += 1;
+    }
+    e->nev = 0;
+    return 0;
+}
+
+void ssae_destroy(ssa_engine *e)
+{
+    if (!e)
+        return;
+    if (e->st)
+        cudaStreamSynchronize(e->st);
+    for (int i = 0; i < 2 * SSA_PROF_MAX; i++)
+        if (e->ev[i])
+            cudaEventDestroy(e->ev[i]);
+    void *bufs[] = {e->x64, e->X, e->Y, e->Z, e->part, e->qsum, e->Rinv, e->Zu, e->Zv,
+                    e->sigma, e->status, e->recon, e->norm2, e->W, e->Us, e->Vs, e->ja.d};
+    for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
+        if (bufs[i])
+            cudaFree(bufs[i]);
+    if (e->ja.h)
+        cudaFreeHost(e->ja.h);
+    if (e->own_stream && e->st)
+        cudaStreamDestroy(e->st);
+    memset(e, 0, sizeof(*e));
+}
+
+int ssae_ensure_recon(ssa_engine *e)
+{
+    if (e->recon)
+        return 0;
+    return dmalloc((void **)&e->recon, (size_t)e->B * e->k * e->ldN * sizeof(float));
+}
+
+int ssae_ensure_spectra(ssa_engine *e)
+{
+    if (e->Us && e->Vs)
+        return 0;
+    size_t bytes = (size_t)e->B * e->k * e->ldS * sizeof(float);
+    CK(dmalloc((void **)&e->Us, bytes));
+    return dmalloc((void **)&e->Vs, bytes);
+}
+
+void ssae_reset_jobs(ssa_engine *e)
+{
+    cudaStreamSynchronize(e->st);
+    if (e->prof)
+        ssae_prof_collect(e);
+    e->ja.used = 0;
+}
+
+void *ssae_push_jobs(ssa_engine *e, const void *jobs, size_t sz)
+{
+    size_t off = (e->ja.used + 15) & ~(size_t)15;
+    if (off + sz > e->ja.cap)
+        return NULL;
+    memcpy(e->ja.h + off, jobs, sz);
+    if (cudaMemcpyAsync(e->ja.d + off, e->ja.h + off, sz, cudaMemcpyHostToDevice, e->st) != cudaSuccess)
+        return NULL;
+    e->ja.used = off + sz;
+    return e->ja.d + off;
+}
+
+int ssae_upload_jobs(ssa_engine *e)
+{
+    (void)e;
+    return 0;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+
+int ssae_signal_spectrum(ssa_engine *e, const double *d_x, int nb)
+{
+    ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)nb, sizeof(ssa_col_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    for (int s = 0; s < nb; s++)
+    {
+        ssa_col_job *J = &jobs[s];
+        J->in64 = d_x + (size_t)s * e->N;
+        J->ld_in = e->N;
+        J->n_in = e->N;
+        J->spec = e->X + (size_t)s * e->ldS;
+        J->ld_spec = e->ldS;
+        J->ncols = 1;
+        J->N = e->N;
+        J->L = e->L;
+        J->K = e->K;
+    }
+    void *d = ssae_push_jobs(e, jobs, sizeof(ssa_col_job) * nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_SPECTRUM);
+    int rc_ = ssad_spectrum((const ssa_col_job *)d, nb, 1, e->logh, e->st);
+    ssae_prof_end(e);
+    return rc_;
+}
+
+/* Correlation sweep: out = H in (fwd: in K rows -> out L rows) or H^T in (adjoint). */
+static int sweep(ssa_engine *e, int nb, int ncols, int adjoint, const float *d_omega, long long omega_ld,
+                 unsigned long long seed, int generate)
+{
+    ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)nb, sizeof(ssa_col_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    for (int s = 0; s < nb; s++)
+    {
+        ssa_col_job *J = &jobs[s];
+        float *Ys = e->Y + (size_t)s * e->ldL * e->kp;
+        float *Zs = e->Z + (size_t)s * e->ldK * e->kp;
+        if (!adjoint)
+        {
+            if (generate)
+            {
+                if (d_omega)
+                {
+                    J->in = d_omega + (size_t)s * omega_ld * ncols;
+                    J->ld_in = omega_ld;
+                }
+                else
+                {
+                    J->in = NULL;
+                    J->seed = seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(s + 1));
+                }
+            }
+            else
+            {
+                J->in = Zs;
+                J->ld_in = e->ldK;
+            }
+            J->n_in = e->K;
+            J->out = Ys;
+            J->ld_out = e->ldL;
+            J->n_out = e->L;
+        }
+        else
+        {
+            J->in = Ys;
+            J->ld_in = e->ldL;
+            J->n_in = e->L;
+            J->out = Zs;
+            J->ld_out = e->ldK;
+            J->n_out = e->K;
+        }
+        J->X = e->X + (size_t)s * e->ldS;
+        J->ncols = ncols;
+        J->N = e->N;
+        J->L = e->L;
+        J->K = e->K;
+    }
+    void *d = ssae_push_jobs(e, jobs, sizeof(ssa_col_job) * nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_CORR);
+    int rc_ = ssad_corr((const ssa_col_job *)d, nb, ncols, e->logh, e->st);
+    ssae_prof_end(e);
+    return rc_;
+}
+
+int ssae_matvec(ssa_engine *e, int ncols, int adjoint)
+{
+    return sweep(e, 1, ncols, adjoint, NULL, 0, 0, 0);
+}
+
+/* Gram partials of the m x n blocks A_s (stride per series `sstride`, leading dim ld). */
+static int gram(ssa_engine *e, int nb, const float *A, size_t sstride, long long ld, int m, int n, int rows,
+                int weighted)
+{
+    ssa_gram_job *jobs = (ssa_gram_job *)calloc((size_t)nb, sizeof(ssa_gram_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    const int nch = (m + rows - 1) / rows;
+    const int nchmax = imax(e->nch_L, imax(e->nch_K, e->nch_N));
+    const size_t np = (size_t)e->kp * (e->kp + 1) / 2;
+    for (int s = 0; s < nb; s++)
+    {
+        ssa_gram_job *J = &jobs[s];
+        J->A = A + (size_t)s * sstride;
+        J->part = e->part + (size_t)s * nchmax * np;
+        J->ld = ld;
+        J->m = m;
+        J->n = n;
+        J->rows_per_cta = rows;
+        J->weighted = weighted;
+        J->N = e->N;
+        J->L = e->L;
+        J->K = e->K;
+    }
+    void *d = ssae_push_jobs(e, jobs, sizeof(ssa_gram_job) * nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_GRAM);
+    int rc_ = ssad_gram((const ssa_gram_job *)d, nb, nch, weighted, e->st);
+    ssae_prof_end(e);
+    return rc_;
+}
+
+static int chol(ssa_engine *e, int nb, int nch, int n)
+{
+    ssa_chol_job *jobs = (ssa_chol_job *)calloc((size_t)nb, sizeof(ssa_chol_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    const int nchmax = imax(e->nch_L, imax(e->nch_K, e->nch_N));
+    const size_t np = (size_t)e->kp * (e->kp + 1) / 2;
+    for (int s = 0; s < nb; s++)
+    {
+        ssa_chol_job *J = &jobs[s];
+        J->part = e->part + (size_t)s * nchmax * np;
+        J->Rinv = e->Rinv + (size_t)s * e->kp * e->kp;
+        J->status = e->status + s;
+        J->nchunks = nch;
+        J->n = n;
+    }
+    void *d = ssae_push_jobs(e, jobs, sizeof(ssa_chol_job) * nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_CHOL);
+    int rc_ = ssad_chol((const ssa_chol_job *)d, nb, e->st);
+    ssae_prof_end(e);
+    return rc_;
+}
+
+/* C_s = A_s * M_s for all series (M_s small, n x p, ld ldb, per-series stride mstride). */
+static int rowmul(ssa_engine *e, int nb, const float *A, size_t astride, long long lda, int m, int n,
+                  const float *Mm, size_t mstride, int ldb, int p, float *C, size_t cstride, long long ldc,
+                  double *colsum)
+{
+    ssa_rowmul_job *jobs = (ssa_rowmul_job *)calloc((size_t)nb, sizeof(ssa_rowmul_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    const int nqb = (m + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS;
+    for (int s = 0; s < nb; s++)
+    {
+        ssa_rowmul_job *J = &jobs[s];
+        J->A = A + (size_t)s * astride;
+        J->Bm = Mm + (size_t)s * mstride;
+        J->C = C + (size_t)s * cstride;
+        J->colsum = colsum ? colsum + (size_t)s * nqb * p : NULL;
+        J->lda = lda;
+        J->ldc = ldc;
+        J->m = m;
+        J->n = n;
+        J->p = p;
+        J->ldb = ldb;
+    }
+    void *d = ssae_push_jobs(e, jobs, sizeof(ssa_rowmul_job) * nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_ROWMUL);
+    int rc_ = ssad_rowmul((const ssa_rowmul_job *)d, nb, m, n, e->st);
+    ssae_prof_end(e);
+    return rc_;
+}
+
+/* One CholQR pass on the m x n blocks A_s in place. */
+static int cholqr_pass(ssa_engine *e, int nb, float *A, size_t sstride, long long ld, int m, int n, int rows,
+                       double *colsum)
+{
+    const int nch = (m + rows - 1) / rows;
+    CK(gram(e, nb, A, sstride, ld, m, n, rows, 0));
+    CK(chol(e, nb, nch, n));
+    return rowmul(e, nb, A, sstride, ld, m, n, e->Rinv, (size_t)e->kp * e->kp, n, n, A, sstride, ld, colsum);
+}
+
+int ssae_decompose(ssa_engine *e, int nb, int kp, int k, int q, const float *d_omega, long long omega_ld,
+                   unsigned long long seed)
+{
+    if (nb < 1 || nb > e->B || kp < 1 || kp > e->kp || k < 1 || k > imin(kp, e->k))
+        return (int)cudaErrorInvalidValue;
+    const size_t sY = (size_t)e->ldL * e->kp, sZ = (size_t)e->ldK * e->kp;
+    const int L = e->L, K = e->K;
+    CK(cudaMemsetAsync(e->status, 0, sizeof(int) * nb, e->st));
+    /* Y = H Omega */
+    CK(sweep(e, nb, kp, 0, d_omega, omega_ld, seed, 1));
+    for (int it = 0; it < q; it++)
+    {
+        /* Q = orth(Y) (two passes), Z = H^T Q, Z = orth(Z) (one pass), Y = H Z */
+        CK(cholqr_pass(e, nb, e->Y, sY, e->ldL, L, kp, e->rows_L, NULL));
+        CK(cholqr_pass(e, nb, e->Y, sY, e->ldL, L, kp, e->rows_L, NULL));
+        CK(sweep(e, nb, kp, 1, NULL, 0, 0, 0));
+        CK(cholqr_pass(e, nb, e->Z, sZ, e->ldK, K, kp, e->rows_K, NULL));
+        CK(sweep(e, nb, kp, 0, NULL, 0, 0, 0));
+    }
+    /* final Q = CholQR2(Y) with the column sums of Q for the sign rule */
+    CK(cholqr_pass(e, nb, e->Y, sY, e->ldL, L, kp, e->rows_L, NULL));
+    CK(cholqr_pass(e, nb, e->Y, sY, e->ldL, L, kp, e->rows_L, e->qsum));
+    /* B = H^T Q */
+    CK(sweep(e, nb, kp, 1, NULL, 0, 0, 0));
+    /* Rayleigh-Ritz on B^T B */
+    CK(gram(e, nb, e->Z, sZ, e->ldK, K, kp, e->rows_K, 0));
+    {
+        ssa_rr_job *jobs = (ssa_rr_job *)calloc((size_t)nb, sizeof(ssa_rr_job));
+        if (!jobs)
+            return (int)cudaErrorMemoryAllocation;
+        const int nchmax = imax(e->nch_L, imax(e->nch_K, e->nch_N));
+        const size_t np = (size_t)e->kp * (e->kp + 1) / 2;
+        const int nqb = (L + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS;
+        for (int s = 0; s < nb; s++)
+        {
+            ssa_rr_job *J = &jobs[s];
+            J->part = e->part + (size_t)s * nchmax * np;
+            J->qsum = e->qsum + (size_t)s * nqb * kp;
+            J->sigma = e->sigma + (size_t)s * e->k;
+            J->Zu = e->Zu + (size_t)s * e->kp * e->k;
+            J->Zv = e->Zv + (size_t)s * e->kp * e->k;
+            J->status = e->status + s;
+            J->nchunks = (K + e->rows_K - 1) / e->rows_K;
+            J->nchunks_q = nqb;
+            J->kp = kp;
+            J->k = k;
+        }
+        void *d = ssae_push_jobs(e, jobs, sizeof(ssa_rr_job) * nb);
+        free(jobs);
+        if (!d)
+            return (int)cudaErrorMemoryAllocation;
+        ssae_prof_begin(e, SSAK_RR);
+        int rc_ = ssad_rr((const ssa_rr_job *)d, nb, e->st);
+        ssae_prof_end(e);
+        CK(rc_);
+    }
+    /* U = Q Zu (in place over Y), V = B Zv (in place over Z) */
+    CK(rowmul(e, nb, e->Y, sY, e->ldL, L, kp, e->Zu, (size_t)e->kp * e->k, kp, k, e->Y, sY, e->ldL, NULL));
+    CK(rowmul(e, nb, e->Z, sZ, e->ldK, K, kp, e->Zv, (size_t)e->kp * e->k, kp, k, e->Z, sZ, e->ldK, NULL));
+    return 0;
+}
+
+int ssae_elem_recon(ssa_engine *e, int nb, int k)
+{
+    CK(ssae_ensure_recon(e));
+    ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)nb, sizeof(ssa_col_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    for (int s = 0; s < nb; s++)
+    {
+        ssa_col_job *J = &jobs[s];
+        J->in = e->Y + (size_t)s * e->ldL * e->kp;
+        J->ld_in = e->ldL;
+        J->n_in = e->L;
+        J->in2 = e->Z + (size_t)s * e->ldK * e->kp;
+        J->ld_in2 = e->ldK;
+        J->n_in2 = e->K;
+        J->scale = e->sigma + (size_t)s * e->k;
+        J->out = e->recon + (size_t)s * e->k * e->ldN;
+        J->ld_out = e->ldN;
+        J->norm2 = e->norm2 + (size_t)s * e->k;
+        J->ncols = k;
+        J->N = e->N;
+        J->L = e->L;
+        J->K = e->K;
+    }
+    void *d = ssae_push_jobs(e, jobs, sizeof(ssa_col_job) * nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_ELEM);
+    int rc_ = ssad_elem_recon((const ssa_col_job *)d, nb, k, e->logh, e->st);
+    ssae_prof_end(e);
+    return rc_;
+}
+
+int ssae_wcorr(ssa_engine *e, int nb, int k)
+{
+    /* weighted Gram of the elementary reconstructions: G_ij = sum_t w_t x~_i[t] x~_j[t] */
+    CK(gram(e, nb, e->recon, (size_t)e->k * e->ldN, e->ldN, e->N, k, e->rows_N, 1));
+    ssa_wfin_job *jobs = (ssa_wfin_job *)calloc((size_t)nb, sizeof(ssa_wfin_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    const int nchmax = imax(e->nch_L, imax(e->nch_K, e->nch_N));
+    const size_t np = (size_t)e->kp * (e->kp + 1) / 2;
+    for (int s = 0; s < nb; s++)
+    {
+        jobs[s].part = e->part + (size_t)s * nchmax * np;
+        jobs[s].W = e->W + (size_t)s * e->k * e->k;
+        jobs[s].nchunks = e->nch_N;
+        jobs[s].k = k;
+    }
+    void *d = ssae_push_jobs(e, jobs, sizeof(ssa_wfin_job) * nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_WFIN);
+    int rc_ = ssad_wfin((const ssa_wfin_job *)d, nb, e->st);
+    ssae_prof_end(e);
+    return rc_;
+}
+
+int ssae_spectra(ssa_engine *e, int nb, int k)
+{
+    CK(ssae_ensure_spectra(e));
+    ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)nb * 2, sizeof(ssa_col_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    for (int s = 0; s < nb; s++)
+    {
+        ssa_col_job *Ju = &jobs[2 * s], *Jv = &jobs[2 * s + 1];
+        Ju->in = e->Y + (size_t)s * e->ldL * e->kp;
+        Ju->ld_in = e->ldL;
+        Ju->n_in = e->L;
+        Ju->scale = e->sigma + (size_t)s * e->k;
+        Ju->spec = e->Us + (size_t)s * e->k * e->ldS;
+        Ju->ld_spec = e->ldS;
+        Ju->ncols = k;
+        Jv->in = e->Z + (size_t)s * e->ldK * e->kp;
+        Jv->ld_in = e->ldK;
+        Jv->n_in = e->K;
+        Jv->spec = e->Vs + (size_t)s * e->k * e->ldS;
+        Jv->ld_spec = e->ldS;
+        Jv->ncols = k;
+    }
+    void *d = ssae_push_jobs(e, jobs, sizeof(ssa_col_job) * nb * 2);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_SPECTRUM);
+    int rc_ = ssad_spectrum((const ssa_col_job *)d, 2 * nb, k, e->logh, e->st);
+    ssae_prof_end(e);
+    return rc_;
+}
+
+int ssae_recon_group(ssa_engine *e, int s, int k, const int *d_group, int n_group, double *d_out)
+{
+    ssa_recon_job J;
+    memset(&J, 0, sizeof(J));
+    J.Us = e->Us + (size_t)s * e->k * e->ldS;
+    J.Vs = e->Vs + (size_t)s * e->k * e->ldS;
+    J.group = d_group;
+    J.out64 = d_out;
+    J.ld_spec = e->ldS;
+    J.n_group = n_group;
+    J.k = k;
+    J.N = e->N;
+    J.L = e->L;
+    J.K = e->K;
+    void *d = ssae_push_jobs(e, &J, sizeof(J));
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_RECON);
+    int rc_ = ssad_recon((const ssa_recon_job *)d, 1, e->logh, e->st);
+    ssae_prof_end(e);
+    return rc_;
+}

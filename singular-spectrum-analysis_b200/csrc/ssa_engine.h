@@ -1,0 +1,125 @@
+/*
+ * Device pipeline over a set of B series of identical shape (N, L, k + p): the engine that
+ * both the reference-compatible single-series API (ssa_api.c, B = 1) and the batched API
+ * (ssa_batch.c) drive. Host code in C; all numerics run in ssa_kernels.cu.
+ *
+ * Per-series device layout (series s):
+ *   x64   [s * N]                   input signal (double)
+ *   X     [s * ldS]                 signal spectrum, H + 1 complex (ldS floats)
+ *   Y     [s * ldL * kp]            L x kp range-finder block (Y, Q, then U in place)
+ *   Z     [s * ldK * kp]            K x kp block (Omega, Z, B, then V in place)
+ *   recon [s * k * ldN]             k elementary reconstructions (row i = component i)
+ * Leading dimensions ldL, ldK, ldN are rounded up to multiples of 4 floats (16 B).
+ */
+#ifndef SSA_ENGINE_H
+#define SSA_ENGINE_H
+
+#include <cuda_runtime_api.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "ssa_kernels.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Kernel kinds for the stage profiler. */
+enum
+{
+    SSAK_SPECTRUM = 0,
+    SSAK_CORR,
+    SSAK_GRAM,
+    SSAK_CHOL,
+    SSAK_ROWMUL,
+    SSAK_RR,
+    SSAK_ELEM,
+    SSAK_WFIN,
+    SSAK_GSUM,
+    SSAK_RECON,
+    SSAK_LRF,
+    SSAK_NKINDS
+};
+#define SSA_PROF_MAX 512
+
+typedef struct
+{
+    char *h;    /* pinned host staging */
+    char *d;    /* device copy */
+    size_t cap;
+    size_t used;
+} ssa_job_arena;
+
+typedef struct
+{
+    int B, N, L, K, logh, H, kp, k;
+    long long ldL, ldK, ldN, ldS;
+    int rows_L, rows_K, rows_N;  /* Gram rows per CTA */
+    int nch_L, nch_K, nch_N;     /* Gram partial counts */
+    int nq;                      /* rowmul CTAs over L (colsum partials) */
+    int device;
+    cudaStream_t st;
+    int own_stream;
+    /* device buffers */
+    double *x64;
+    float *X;
+    float *Y, *Z;
+    double *part;                /* B * max(nch) * kp(kp+1)/2 */
+    double *qsum;                /* B * nq * kp */
+    float *Rinv;                 /* B * kp * kp */
+    float *Zu, *Zv;              /* B * kp * k */
+    double *sigma;               /* B * k */
+    int *status;                 /* B */
+    float *recon;                /* B * k * ldN (allocated on demand) */
+    double *norm2;               /* B * k */
+    double *W;                   /* B * k * k */
+    float *Us, *Vs;              /* cached spectra B * k * ldS (allocated on demand) */
+    ssa_job_arena ja;
+    /* stage profiler: event pairs around launches while prof != 0 */
+    int prof;
+    int nev;
+    int ev_kind[SSA_PROF_MAX];
+    cudaEvent_t ev[2 * SSA_PROF_MAX];
+    double prof_ms[SSAK_NKINDS];
+    long long prof_n[SSAK_NKINDS];
+} ssa_engine;
+
+/* Enable/disable event timing of every launch (events are created on first use). */
+int ssae_set_profiling(ssa_engine *e, int on);
+/* Record the start / end of a launch of `kind` (no-op unless profiling). */
+void ssae_prof_begin(ssa_engine *e, int kind);
+void ssae_prof_end(ssa_engine *e);
+/* Wait for the stream, fold recorded intervals into prof_ms / prof_n and reset the list. */
+int ssae_prof_collect(ssa_engine *e);
+
+/* Allocate buffers for up to B series. Returns 0 or a cudaError_t value. */
+int ssae_create(ssa_engine *e, int B, int N, int L, int kp, int k, cudaStream_t stream);
+void ssae_destroy(ssa_engine *e);
+int ssae_ensure_recon(ssa_engine *e);
+int ssae_ensure_spectra(ssa_engine *e);
+
+/* Pipeline stages (enqueue only; nb <= B series starting at series 0). */
+int ssae_signal_spectrum(ssa_engine *e, const double *d_x, int nb);
+/* Randomized range finder + Rayleigh-Ritz. d_omega: device K x kp (ld K) per series (stride
+ * K * kp), or NULL to generate the test matrix on the device from (seed, series index). */
+int ssae_decompose(ssa_engine *e, int nb, int kp, int k, int q, const float *d_omega, long long omega_ld,
+                   unsigned long long seed);
+int ssae_elem_recon(ssa_engine *e, int nb, int k);
+int ssae_wcorr(ssa_engine *e, int nb, int k);
+int ssae_spectra(ssa_engine *e, int nb, int k);
+/* One correlation sweep on series 0 over `ncols` columns already in Z (forward: Y = H Z) or
+ * Y (adjoint: Z = H^T Y). */
+int ssae_matvec(ssa_engine *e, int ncols, int adjoint);
+/* Grouped reconstruction of series s from cached spectra into d_out (double, N). */
+int ssae_recon_group(ssa_engine *e, int s, int k, const int *d_group, int n_group, double *d_out);
+
+/* Job arena: copy `sz` bytes of job structs into the staging area, return the device address
+ * they will have after ssae_upload_jobs. */
+void *ssae_push_jobs(ssa_engine *e, const void *jobs, size_t sz);
+int ssae_upload_jobs(ssa_engine *e);
+void ssae_reset_jobs(ssa_engine *e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,282 @@
+// Shared-memory FFT building blocks for the SSA hot path on sm_100a.
+//
+// One CTA transforms one real sequence of length M = 2H (H = 2^LOGH complex points) that is
+// packed as z[n] = a[2n] + i a[2n+1]. The complex FFT of length H runs as a Stockham
+// auto-sort FFT (Govindaraju et al., "High performance discrete Fourier transforms on
+// graphics processors", SC'08) with radix-16 passes held in registers: every thread owns
+// 16 points per pass, loads them, waits at a barrier, applies twiddles and the in-register
+// DFT, and stores them at their auto-sorted positions, so the transform runs in place in one
+// buffer of H points. The buffer is padded by one point per 16 (spad) so that both the
+// strided loads and the auto-sort stores of a half-warp touch 16 distinct 8-byte bank pairs.
+//
+// Twiddles come from one table g_tw[t] = exp(-2 pi i t / TW_N), computed on the host in FP64
+// and rounded to FP32 once per device.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define SSA_TW_LOG 15
+#define SSA_TW_N (1 << SSA_TW_LOG)
+// Largest complex FFT a single CTA holds: H = 2^14 points (real length M = 32768).
+#define SSA_MAX_LOGH 14
+#define SSA_MIN_LOGH 4
+
+// Defined once in the translation unit that includes this header (ssa_kernels.cu).
+__device__ float2 g_tw[SSA_TW_N];
+
+namespace ssa {
+
+__device__ __forceinline__ int spad(int a) { return a + (a >> 4); }
+__host__ __device__ constexpr int spad_size(int h) { return h + (h >> 4) + 16; }
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+// a * conj(b)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+__device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV>
+__device__ __forceinline__ float2 mul_mi(float2 a) {
+    return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// exp(-+2 pi i t / TW_N) for t in [0, TW_N)
+template <bool INV>
+__device__ __forceinline__ float2 twiddle(int t) {
+    float2 w = g_tw[t];
+    if (INV) w.y = -w.y;
+    return w;
+}
+
+// Multiply by the constant W_16^e (forward sign) or its conjugate.
+template <bool INV, int E>
+__device__ __forceinline__ float2 w16(float2 a) {
+    constexpr float C1 = 0.92387953251128674f;  // cos(pi/8)
+    constexpr float S1 = 0.38268343236508978f;  // sin(pi/8)
+    constexpr float R2 = 0.70710678118654752f;  // 1/sqrt(2)
+    constexpr int e = E & 15;
+    float2 w = make_float2(1.f, 0.f);
+    if constexpr (e == 0) return a;
+    else if constexpr (e == 1) w = make_float2(C1, -S1);
+    else if constexpr (e == 2) w = make_float2(R2, -R2);
+    else if constexpr (e == 3) w = make_float2(S1, -C1);
+    else if constexpr (e == 4) return mul_mi<INV>(a);
+    else if constexpr (e == 6) w = make_float2(-R2, -R2);
+    else if constexpr (e == 9) w = make_float2(-C1, S1);
+    else static_assert(e == 0, "unused constant");
+    if (INV) w.y = -w.y;
+    return cmul(a, w);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft2(float2* a) {
+    float2 t = a[0];
+    a[0] = cadd(t, a[1]);
+    a[1] = csub(t, a[1]);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4s(float2& a0, float2& a1, float2& a2, float2& a3) {
+    float2 s0 = cadd(a0, a2), d0 = csub(a0, a2);
+    float2 s1 = cadd(a1, a3), d1 = mul_mi<INV>(csub(a1, a3));
+    a0 = cadd(s0, s1);
+    a2 = csub(s0, s1);
+    a1 = cadd(d0, d1);
+    a3 = csub(d0, d1);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(float2* a) { dft4s<INV>(a[0], a[1], a[2], a[3]); }
+
+// 8 = 2 x 4: inner DFT4 over a[j + 2l], twiddle W8^{jm} = W16^{2jm}, outer DFT2 over j,
+// output index m + 4n.
+template <bool INV>
+__device__ __forceinline__ void dft8(float2* a) {
+    float2 b0[4] = {a[0], a[2], a[4], a[6]};
+    float2 b1[4] = {a[1], a[3], a[5], a[7]};
+    dft4<INV>(b0);
+    dft4<INV>(b1);
+    b1[1] = w16<INV, 2>(b1[1]);
+    b1[2] = w16<INV, 4>(b1[2]);
+    b1[3] = w16<INV, 6>(b1[3]);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        a[m] = cadd(b0[m], b1[m]);
+        a[m + 4] = csub(b0[m], b1[m]);
+    }
+}
+
+// 16 = 4 x 4: inner DFT4 over a[j + 4l] (l), twiddle W16^{jm}, outer DFT4 over j,
+// output index m + 4n.
+template <bool INV>
+__device__ __forceinline__ void dft16(float2* a) {
+    dft4s<INV>(a[0], a[4], a[8], a[12]);
+    dft4s<INV>(a[1], a[5], a[9], a[13]);
+    dft4s<INV>(a[2], a[6], a[10], a[14]);
+    dft4s<INV>(a[3], a[7], a[11], a[15]);
+    // b[j][m] sits at a[j + 4m]
+    a[5] = w16<INV, 1>(a[5]);
+    a[9] = w16<INV, 2>(a[9]);
+    a[13] = w16<INV, 3>(a[13]);
+    a[6] = w16<INV, 2>(a[6]);
+    a[10] = w16<INV, 4>(a[10]);
+    a[14] = w16<INV, 6>(a[14]);
+    a[7] = w16<INV, 3>(a[7]);
+    a[11] = w16<INV, 6>(a[11]);
+    a[15] = w16<INV, 9>(a[15]);
+    // outer DFT4 over j for each m: inputs a[4m + j], outputs X[m + 4n]
+    dft4s<INV>(a[0], a[1], a[2], a[3]);
+    dft4s<INV>(a[4], a[5], a[6], a[7]);
+    dft4s<INV>(a[8], a[9], a[10], a[11]);
+    dft4s<INV>(a[12], a[13], a[14], a[15]);
+    // now a[4m + n] holds X[m + 4n]: transpose 4x4 into natural order
+    float2 t;
+#define SSA_SWP(i, j) t = a[i]; a[i] = a[j]; a[j] = t;
+    SSA_SWP(1, 4) SSA_SWP(2, 8) SSA_SWP(3, 12) SSA_SWP(6, 9) SSA_SWP(7, 13) SSA_SWP(11, 14)
+#undef SSA_SWP
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void dftR(float2* a) {
+    if constexpr (R == 2) dft2<INV>(a);
+    else if constexpr (R == 4) dft4<INV>(a);
+    else if constexpr (R == 8) dft8<INV>(a);
+    else dft16<INV>(a);
+}
+
+// Threads that take part in an H-point transform: 16 points each.
+template <int LOGH>
+struct FftShape {
+    static constexpr int H = 1 << LOGH;
+    static constexpr int T = H / 16;
+    static constexpr int BLOCK = T < 32 ? 32 : T;
+};
+
+// One Stockham pass of radix 2^RLOG after 2^LOGNS points have been combined.
+template <int RLOG, int LOGNS, int LOGH, bool INV>
+__device__ __forceinline__ void fft_pass(float2* s, int tid) {
+    constexpr int R = 1 << RLOG;
+    constexpr int H = 1 << LOGH;
+    constexpr int T = H / 16;
+    constexpr int NB = 16 / R;
+    constexpr int STR = H / R;
+    constexpr int NS = 1 << LOGNS;
+    const bool active = tid < T;
+    float2 a[16];
+    if (active) {
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const int j = tid + b * T;
+#pragma unroll
+            for (int r = 0; r < R; ++r) a[b * R + r] = s[spad(j + r * STR)];
+        }
+    }
+    __syncthreads();
+    if (active) {
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const int j = tid + b * T;
+            const int k = j & (NS - 1);
+            if constexpr (LOGNS > 0) {
+                // W_{NS R}^{r k} = table index (r k) << (TW_LOG - LOGNS - RLOG)
+                constexpr int SH = SSA_TW_LOG - LOGNS - RLOG;
+#pragma unroll
+                for (int r = 1; r < R; ++r) a[b * R + r] = cmul(a[b * R + r], twiddle<INV>((r * k) << SH));
+            }
+            dftR<R, INV>(a + b * R);
+            const int base = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) s[spad(base + r * NS)] = a[b * R + r];
+        }
+    }
+    __syncthreads();
+}
+
+template <int LOGH, bool INV, int LOGNS>
+__device__ __forceinline__ void fft_passes(float2* s, int tid) {
+    if constexpr (LOGNS + 4 <= LOGH) {
+        fft_pass<4, LOGNS, LOGH, INV>(s, tid);
+        fft_passes<LOGH, INV, LOGNS + 4>(s, tid);
+    } else if constexpr (LOGNS < LOGH) {
+        fft_pass<LOGH - LOGNS, LOGNS, LOGH, INV>(s, tid);
+    }
+}
+
+// In-place H-point complex FFT (unnormalised) of the padded shared buffer s. Must be called
+// by every thread of the CTA; the caller syncs before (data in s) and may read s after.
+template <int LOGH, bool INV>
+__device__ __forceinline__ void fft_block(float2* s) {
+    fft_passes<LOGH, INV, 0>(s, threadIdx.x);
+}
+
+// Load a real sequence a[0..n) (zero beyond n, up to M = 2H) into s as z[n] = a[2n] + i a[2n+1],
+// optionally scaled. The source row must be 8-byte aligned (even element offset).
+template <int LOGH>
+__device__ __forceinline__ void load_real(float2* s, const float* __restrict__ a, int n, float scale) {
+    constexpr int H = 1 << LOGH;
+    const float2* a2 = reinterpret_cast<const float2*>(a);
+    const int nfull = n >> 1;
+    for (int i = threadIdx.x; i < H; i += blockDim.x) {
+        float2 v;
+        if (i < nfull) {
+            v = a2[i];
+            v.x *= scale;
+            v.y *= scale;
+        } else if (i == nfull && (n & 1)) {
+            v = make_float2(a[n - 1] * scale, 0.f);
+        } else {
+            v = make_float2(0.f, 0.f);
+        }
+        s[spad(i)] = v;
+    }
+}
+
+// Store the first n reals of the unpacked sequence p (p[2i] = Re s[i], p[2i+1] = Im s[i]) times scale.
+template <int LOGH>
+__device__ __forceinline__ void store_real(const float2* s, float* __restrict__ out, int n, float scale) {
+    float2* o2 = reinterpret_cast<float2*>(out);
+    const int nfull = n >> 1;
+    for (int i = threadIdx.x; i < nfull; i += blockDim.x) {
+        float2 v = s[spad(i)];
+        o2[i] = make_float2(v.x * scale, v.y * scale);
+    }
+    if ((n & 1) && threadIdx.x == 0) out[n - 1] = s[spad(nfull)].x * scale;
+}
+
+// Real spectrum values A[k] and A[H-k] (k in [1, H/2]) of the packed transform Z held in s:
+// A[k] = E + W_M^k O, A[H-k] = conj(E - W_M^k O) with E = (Z_k + conj Z_{H-k})/2,
+// O = -i (Z_k - conj Z_{H-k})/2.
+template <int LOGH>
+__device__ __forceinline__ void unpack_pair(float2 zk, float2 zm, float2 wk, float2& ak, float2& am) {
+    float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    // O = -i * (zk - conj zm)/2 ; (zk - conj zm) = (zk.x - zm.x, zk.y + zm.y)
+    float2 o = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+    float2 wo = cmul(wk, o);
+    ak = cadd(e, wo);
+    am = conjf2(csub(e, wo));
+}
+
+// Inverse packing for a Hermitian spectrum P: Z'_k = E' + i O', Z'_{H-k} = conj E' + i conj O'
+// with E' = (P_k + conj P_{H-k})/2 and O' = (P_k - conj P_{H-k}) conj(W_M^k)/2.
+__device__ __forceinline__ void pack_pair(float2 pk, float2 pm, float2 wk, float2& zk, float2& zm) {
+    float2 e = make_float2(0.5f * (pk.x + pm.x), 0.5f * (pk.y - pm.y));
+    float2 d = make_float2(0.5f * (pk.x - pm.x), 0.5f * (pk.y + pm.y));
+    float2 o = cmulc(d, wk);
+    // zk = e + i o ; zm = conj(e) + i conj(o)
+    zk = make_float2(e.x - o.y, e.y + o.x);
+    zm = make_float2(e.x + o.y, -e.y + o.x);
+}
+
+// W_M^k for M = 2^(LOGH+1)
+template <int LOGH>
+__device__ __forceinline__ float2 wm(int k) {
+    return g_tw[k << (SSA_TW_LOG - LOGH - 1)];
+}
+
+}  // namespace ssa

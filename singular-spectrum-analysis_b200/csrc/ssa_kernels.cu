@@ -1,0 +1,920 @@
+// sm_100a kernels for the SSA decomposition / reconstruction hot path.
+//
+// Kernel map (reference call sites in SSA-Opt MKL/ssa_opt.h):
+//   k_spectrum     FFT(x ‖ 0) of the signal (:1255-1257) and cached component spectra
+//                  FFT(sigma_i u_i), FFT(v_i) (:2110-2245)
+//   k_corr         Hankel matvec block Y = H V / adjoint Z = H^T U (:910-1004): R2C of each
+//                  column, product with conj of the column spectrum, C2R, first L (or K) values;
+//                  with a NULL input the column is the device Gaussian test matrix (:1719)
+//   k_gram         FP64-accumulated Gram partials A^T W A (CholQR2 Gram, Rayleigh-Ritz Gram and
+//                  the W-correlation SYRK :2543 with diagonal-count weights)
+//   k_chol         FP64 Cholesky of the (k+p) x (k+p) Gram and its triangular inverse
+//   k_rowmul       C = A * Bsmall row by row (Q = Y R^{-1}, U = Q Z, V = B Z Sigma^{-1}; :1736)
+//   k_rr           FP64 Jacobi eigen-decomposition of B^T B: sigma, Ritz rotations, sign rule
+//                  sum U[:, i] >= 0 (:1741-1759)
+//   k_elem_recon   fused elementary reconstruction x~_i = inv_w * (sigma_i u_i conv v_i) and its
+//                  weighted norm (reconstruct :2325-2400 for one component, no cached spectra)
+//   k_recon        grouped reconstruction from cached spectra (:2338-2356, :2393-2397)
+//   k_wfin         W = G_ij / sqrt(G_ii G_jj) (:2527-2546)
+//   k_lrf          LRF coefficients with the verticality check and the R-forecast recurrence
+//                  (:2766-2841), FP64
+#include "ssa_fft.cuh"
+#include "ssa_kernels.h"
+
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+using namespace ssa;
+
+static std::atomic<unsigned long long> g_launches{0};
+static inline int launched(cudaError_t e) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return (int)e;
+}
+
+extern "C" unsigned long long ssad_launch_count(void) { return g_launches.load(); }
+
+// ---------------------------------------------------------------------------------------------
+// Device-side helpers
+// ---------------------------------------------------------------------------------------------
+
+// SplitMix64 finaliser (Steele, Lea, Flood, "Fast splittable pseudorandom number generators",
+// OOPSLA 2014).
+__host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Two N(0,1) values for rows (2*pair, 2*pair+1) of generated column `col` (Box-Muller on two
+// 24-bit uniforms taken from one 64-bit hash of (seed, col, pair)).
+__device__ __forceinline__ float2 gauss_pair(unsigned long long seed, int col, int pair) {
+    unsigned long long key = mix64(seed ^ (0xD1B54A32D192ED03ull * (unsigned long long)(col + 1)));
+    unsigned long long z = mix64(key + (unsigned long long)pair);
+    float u1 = ((float)(z >> 40) + 1.0f) * (1.0f / 16777216.0f);        // (0, 1]
+    float u2 = (float)((z >> 16) & 0xFFFFFFull) * (1.0f / 16777216.0f);  // [0, 1)
+    float r = sqrtf(-2.0f * logf(u1));
+    float sn, cs;
+    sincospif(2.0f * u2, &sn, &cs);
+    return make_float2(r * cs, r * sn);
+}
+
+__device__ __forceinline__ int diag_count(int t, int N, int L, int K) {
+    int c = min(min(t + 1, L), min(K, N - t));
+    return c > 0 ? c : 1;
+}
+
+template <typename T>
+__device__ __forceinline__ T block_sum(T v, T* red) {
+    // red: >= 32 entries of shared scratch; returns the total to every thread. Fixed order.
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    if (warp == 0) {
+        T t = lane < nw ? red[lane] : T(0);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (lane == 0) red[0] = t;
+    }
+    __syncthreads();
+    T r = red[0];
+    __syncthreads();
+    return r;
+}
+
+__host__ __device__ __forceinline__ int pk_index(int i, int j, int n) {  // i <= j
+    return i * n - (i * (i - 1)) / 2 + (j - i);
+}
+
+// Load column `c` of job J into the packed buffer s (input, generated, or double signal).
+template <int LOGH>
+__device__ __forceinline__ void load_column(float2* s, const ssa_col_job& J, int c) {
+    constexpr int H = 1 << LOGH;
+    if (J.in) {
+        const float sc = J.scale ? (float)J.scale[c] : 1.0f;
+        load_real<LOGH>(s, J.in + (long long)c * J.ld_in, J.n_in, sc);
+    } else if (J.in64) {
+        const double* a = J.in64 + (long long)c * J.ld_in;
+        const int n = J.n_in;
+        for (int i = threadIdx.x; i < H; i += blockDim.x) {
+            const int r = 2 * i;
+            float2 v;
+            v.x = r < n ? (float)a[r] : 0.f;
+            v.y = r + 1 < n ? (float)a[r + 1] : 0.f;
+            s[spad(i)] = v;
+        }
+    } else {
+        const int n = J.n_in;
+        const int col = J.col0 + c;
+        for (int i = threadIdx.x; i < H; i += blockDim.x) {
+            const int r = 2 * i;
+            float2 v = make_float2(0.f, 0.f);
+            if (r < n) {
+                v = gauss_pair(J.seed, col, i);
+                if (r + 1 >= n) v.y = 0.f;
+            }
+            s[spad(i)] = v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// FFT column kernels
+// ---------------------------------------------------------------------------------------------
+
+template <int LOGH>
+__global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_spectrum(const ssa_col_job* __restrict__ jobs) {
+    constexpr int H = 1 << LOGH;
+    extern __shared__ float2 smem[];
+    const ssa_col_job J = jobs[blockIdx.y];
+    const int c = blockIdx.x;
+    if (c >= J.ncols) return;
+    load_column<LOGH>(smem, J, c);
+    __syncthreads();
+    fft_block<LOGH, false>(smem);
+    float2* out = reinterpret_cast<float2*>(J.spec + (long long)c * J.ld_spec);
+    for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
+        if (k == 0) {
+            float2 z0 = smem[spad(0)];
+            out[0] = make_float2(z0.x + z0.y, 0.f);
+            out[H] = make_float2(z0.x - z0.y, 0.f);
+        } else {
+            float2 ak, am;
+            unpack_pair<LOGH>(smem[spad(k)], smem[spad(H - k)], wm<LOGH>(k), ak, am);
+            out[k] = ak;
+            out[H - k] = am;
+        }
+    }
+}
+
+template <int LOGH>
+__global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_corr(const ssa_col_job* __restrict__ jobs) {
+    constexpr int H = 1 << LOGH;
+    extern __shared__ float2 smem[];
+    const ssa_col_job J = jobs[blockIdx.y];
+    const int c = blockIdx.x;
+    if (c >= J.ncols) return;
+    load_column<LOGH>(smem, J, c);
+    __syncthreads();
+    fft_block<LOGH, false>(smem);
+    const float2* X = reinterpret_cast<const float2*>(J.X);
+    for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
+        float2 zk, zm;
+        if (k == 0) {
+            const float2 z0 = smem[spad(0)];
+            const float2 p0 = cscale(X[0], z0.x + z0.y);
+            const float2 ph = cscale(X[H], z0.x - z0.y);
+            pack_pair(p0, ph, make_float2(1.f, 0.f), zk, zm);
+            smem[spad(0)] = zk;
+        } else {
+            const float2 w = wm<LOGH>(k);
+            float2 ak, am;
+            unpack_pair<LOGH>(smem[spad(k)], smem[spad(H - k)], w, ak, am);
+            const float2 pk = cmulc(X[k], ak);
+            const float2 pm = cmulc(X[H - k], am);
+            pack_pair(pk, pm, w, zk, zm);
+            smem[spad(k)] = zk;
+            smem[spad(H - k)] = zm;
+        }
+    }
+    __syncthreads();
+    fft_block<LOGH, true>(smem);
+    store_real<LOGH>(smem, J.out + (long long)c * J.ld_out, J.n_out, 1.0f / (float)H);
+}
+
+// Elementary reconstruction of component c: x~[t] = inv_w[t] * (sigma_c u_c conv v_c)[t], and
+// norm2[c] = sum_t w[t] x~[t]^2 (w = diagonal count).
+template <int LOGH>
+__global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_elem_recon(const ssa_col_job* __restrict__ jobs) {
+    constexpr int H = 1 << LOGH;
+    extern __shared__ float2 smem[];
+    __shared__ double red[32];
+    float2* s1 = smem;
+    float2* s2 = smem + spad_size(H);
+    const ssa_col_job J = jobs[blockIdx.y];
+    const int c = blockIdx.x;
+    if (c >= J.ncols) return;
+    const float sc = J.scale ? (float)J.scale[c] : 1.0f;
+    load_real<LOGH>(s1, J.in + (long long)c * J.ld_in, J.n_in, sc);
+    load_real<LOGH>(s2, J.in2 + (long long)c * J.ld_in2, J.n_in2, 1.0f);
+    __syncthreads();
+    fft_block<LOGH, false>(s1);
+    fft_block<LOGH, false>(s2);
+    for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
+        float2 zk, zm;
+        if (k == 0) {
+            const float2 a0 = s1[spad(0)], b0 = s2[spad(0)];
+            const float p0 = (a0.x + a0.y) * (b0.x + b0.y);
+            const float ph = (a0.x - a0.y) * (b0.x - b0.y);
+            pack_pair(make_float2(p0, 0.f), make_float2(ph, 0.f), make_float2(1.f, 0.f), zk, zm);
+            s1[spad(0)] = zk;
+        } else {
+            const float2 w = wm<LOGH>(k);
+            float2 ak, am, bk, bm;
+            unpack_pair<LOGH>(s1[spad(k)], s1[spad(H - k)], w, ak, am);
+            unpack_pair<LOGH>(s2[spad(k)], s2[spad(H - k)], w, bk, bm);
+            pack_pair(cmul(ak, bk), cmul(am, bm), w, zk, zm);
+            s1[spad(k)] = zk;
+            s1[spad(H - k)] = zm;
+        }
+    }
+    __syncthreads();
+    fft_block<LOGH, true>(s1);
+    float* out = J.out + (long long)c * J.ld_out;
+    const float inv_h = 1.0f / (float)H;
+    double acc = 0.0;
+    for (int t = threadIdx.x; t < J.N; t += blockDim.x) {
+        const float2 z = s1[spad(t >> 1)];
+        const float p = ((t & 1) ? z.y : z.x) * inv_h;
+        const int cnt = diag_count(t, J.N, J.L, J.K);
+        const float v = p / (float)cnt;
+        out[t] = v;
+        acc += (double)p * (double)p / (double)cnt;
+    }
+    acc = block_sum<double>(acc, red);
+    if (threadIdx.x == 0 && J.norm2) J.norm2[c] = acc;
+}
+
+// Grouped reconstruction from cached spectra.
+template <int LOGH>
+__global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_recon(const ssa_recon_job* __restrict__ jobs) {
+    constexpr int H = 1 << LOGH;
+    extern __shared__ float2 smem[];
+    const ssa_recon_job J = jobs[blockIdx.y];
+    for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
+        float2 pk = make_float2(0.f, 0.f), pm = make_float2(0.f, 0.f);
+        for (int g = 0; g < J.n_group; ++g) {
+            const int i = J.group[g];
+            if (i < 0 || i >= J.k) continue;
+            const float2* us = reinterpret_cast<const float2*>(J.Us + (long long)i * J.ld_spec);
+            const float2* vs = reinterpret_cast<const float2*>(J.Vs + (long long)i * J.ld_spec);
+            const float2 a = cmul(us[k], vs[k]);
+            const float2 b = cmul(us[H - k], vs[H - k]);
+            pk = cadd(pk, a);
+            pm = cadd(pm, b);
+        }
+        float2 zk, zm;
+        if (k == 0) {
+            pack_pair(pk, pm, make_float2(1.f, 0.f), zk, zm);
+            smem[spad(0)] = zk;
+        } else {
+            pack_pair(pk, pm, wm<LOGH>(k), zk, zm);
+            smem[spad(k)] = zk;
+            smem[spad(H - k)] = zm;
+        }
+    }
+    __syncthreads();
+    fft_block<LOGH, true>(smem);
+    const float inv_h = 1.0f / (float)H;
+    for (int t = threadIdx.x; t < J.N; t += blockDim.x) {
+        const float2 z = smem[spad(t >> 1)];
+        const float p = ((t & 1) ? z.y : z.x) * inv_h;
+        const double v = (double)p / (double)diag_count(t, J.N, J.L, J.K);
+        if (J.out64) J.out64[t] = v;
+        if (J.out) J.out[t] = (float)v;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Gram partials (FP64 accumulation of FP32 data)
+// ---------------------------------------------------------------------------------------------
+
+#define GRAM_THREADS 128
+#define GSTR (SSA_GRAM_CHUNK + 1)
+
+template <bool WEIGHTED>
+__global__ void __launch_bounds__(GRAM_THREADS) k_gram(const ssa_gram_job* __restrict__ jobs) {
+    // [col][row] with a padded column stride so that threads reading different columns at
+    // the same row hit different banks.
+    __shared__ float sA[SSA_MAX_KP * GSTR];
+    __shared__ float sw[SSA_GRAM_CHUNK];
+    const ssa_gram_job J = jobs[blockIdx.y];
+    const int chunk = blockIdx.x;
+    const int r_begin = chunk * J.rows_per_cta;
+    if (r_begin >= J.m) return;
+    const int r_end = min(J.m, r_begin + J.rows_per_cta);
+    const int n = J.n;
+    const int nb = (n + 3) >> 2;
+    const int ntiles = nb * (nb + 1) / 2;
+    // Tile assignment: this thread owns tiles t = tid, tid + 128, ...; at most 2 (n <= 64).
+    double acc[2][4][4];
+    int ti[2], tj[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int t = threadIdx.x + q * GRAM_THREADS;
+        ti[q] = -1;
+        tj[q] = -1;
+        if (t < ntiles) {
+            // upper-triangular tile index -> (bi, bj), bi <= bj
+            int bi = 0, rem = t;
+            while (rem >= nb - bi) {
+                rem -= nb - bi;
+                ++bi;
+            }
+            ti[q] = bi;
+            tj[q] = bi + rem;
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[q][a][b] = 0.0;
+    }
+    double csum = 0.0;
+    for (int r0 = r_begin; r0 < r_end; r0 += SSA_GRAM_CHUNK) {
+        const int rows = min(SSA_GRAM_CHUNK, r_end - r0);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < nb * 4 * SSA_GRAM_CHUNK; idx += GRAM_THREADS) {
+            const int col = idx / SSA_GRAM_CHUNK, r = idx % SSA_GRAM_CHUNK;
+            float v = 0.f;
+            if (col < n && r < rows) v = J.A[(long long)(r0 + r) + (long long)col * J.ld];
+            sA[col * GSTR + r] = v;
+        }
+        if (WEIGHTED) {
+            for (int r = threadIdx.x; r < SSA_GRAM_CHUNK; r += GRAM_THREADS)
+                sw[r] = r < rows ? (float)diag_count(r0 + r, J.N, J.L, J.K) : 0.f;
+        }
+        __syncthreads();
+        if (J.colsum && threadIdx.x < n) {
+            double cs = 0.0;
+            for (int r = 0; r < rows; ++r) cs += (double)sA[threadIdx.x * GSTR + r];
+            csum += cs;
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            if (ti[q] < 0) continue;
+            const float* pa = sA + (ti[q] * 4) * GSTR;
+            const float* pb = sA + (tj[q] * 4) * GSTR;
+            for (int r = 0; r < rows; ++r) {
+                double a[4], b[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    a[u] = (double)pa[u * GSTR + r];
+                    b[u] = (double)pb[u * GSTR + r];
+                }
+                if (WEIGHTED) {
+                    const double w = (double)sw[r];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) b[u] *= w;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) acc[q][u][v] = fma(a[u], b[v], acc[q][u][v]);
+            }
+        }
+    }
+    double* part = J.part + (long long)chunk * (n * (n + 1) / 2);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        if (ti[q] < 0) continue;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int i = ti[q] * 4 + u, j = tj[q] * 4 + v;
+                if (i < n && j < n && i <= j) part[pk_index(i, j, n)] = acc[q][u][v];
+            }
+    }
+    if (J.colsum && threadIdx.x < n) J.colsum[(long long)chunk * n + threadIdx.x] = csum;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Cholesky + triangular inverse (FP64, one CTA per job)
+// ---------------------------------------------------------------------------------------------
+
+#define SMALL_THREADS 256
+#define SLD (SSA_MAX_KP + 1)
+
+__device__ void reduce_packed(const double* __restrict__ part, int nchunks, int n, double* G) {
+    const int np = n * (n + 1) / 2;
+    for (int e = threadIdx.x; e < np; e += blockDim.x) {
+        // invert pk_index
+        int i = 0, rem = e;
+        while (rem >= n - i) {
+            rem -= n - i;
+            ++i;
+        }
+        const int j = i + rem;
+        double s = 0.0;
+        for (int c = 0; c < nchunks; ++c) s += part[(long long)c * np + e];
+        G[i * SLD + j] = s;
+        G[j * SLD + i] = s;
+    }
+}
+
+#define SMALL_SMEM (2 * SSA_MAX_KP * SLD * (int)sizeof(double))
+
+__global__ void __launch_bounds__(SMALL_THREADS) k_chol(const ssa_chol_job* __restrict__ jobs) {
+    extern __shared__ double dsm[];
+    double* G = dsm;
+    double* Rm = dsm + SSA_MAX_KP * SLD;
+    __shared__ double red[32];
+    __shared__ double dmax_s;
+    const ssa_chol_job J = jobs[blockIdx.x];
+    const int n = J.n;
+    reduce_packed(J.part, J.nchunks, n, G);
+    __syncthreads();
+    double dm = 0.0;
+    int bad = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double d = G[i * SLD + i];
+        if (!isfinite(d)) bad = 1;
+        dm = fmax(dm, d);
+    }
+    // max-reduce via warp shuffles on (dm, bad)
+    for (int o = 16; o > 0; o >>= 1) {
+        dm = fmax(dm, __shfl_down_sync(0xffffffffu, dm, o));
+        bad |= __shfl_down_sync(0xffffffffu, bad, o);
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = bad ? -1.0 : dm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        int b = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            if (red[w] < 0.0) b = 1;
+            m = fmax(m, red[w]);
+        }
+        dmax_s = b ? -1.0 : m;
+        if (b && J.status) atomicOr(J.status, 1);
+    }
+    __syncthreads();
+    const double dmax = dmax_s;
+    // Pivot floor: directions below this are treated as rounding noise (rank-deficient input).
+    const double floor_ = dmax > 0.0 ? dmax * 1e-13 * (double)n : 1.0;
+    for (int e = threadIdx.x; e < n * SLD; e += blockDim.x) Rm[e] = 0.0;
+    __syncthreads();
+    // Right-looking Cholesky: G = R^T R, R upper (row j of R in Rm[j][:]).
+    for (int j = 0; j < n; ++j) {
+        if (threadIdx.x == 0) {
+            double d = G[j * SLD + j];
+            if (!(d > floor_)) d = floor_;
+            Rm[j * SLD + j] = sqrt(d);
+        }
+        __syncthreads();
+        const double djj = Rm[j * SLD + j];
+        for (int c = j + 1 + threadIdx.x; c < n; c += blockDim.x) Rm[j * SLD + c] = G[j * SLD + c] / djj;
+        __syncthreads();
+        const int m = n - j - 1;
+        for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+            const int r = j + 1 + e / m, c = j + 1 + e % m;
+            if (r <= c) G[r * SLD + c] -= Rm[j * SLD + r] * Rm[j * SLD + c];
+        }
+        __syncthreads();
+    }
+    // Inverse of the upper-triangular R, one column per thread (back substitution).
+    float* Ri = J.Rinv;
+    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+        double x[SSA_MAX_KP];
+#pragma unroll 1
+        for (int i = c; i >= 0; --i) {
+            double s = (i == c) ? 1.0 : 0.0;
+            for (int l = i + 1; l <= c; ++l) s -= Rm[i * SLD + l] * x[l];
+            x[i] = s / Rm[i * SLD + i];
+        }
+        for (int i = 0; i < n; ++i) Ri[i + c * n] = i <= c ? (float)x[i] : 0.f;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Row-by-row product with a small matrix: C[i, :p] = A[i, :n] Bm
+// ---------------------------------------------------------------------------------------------
+
+#define ROWMUL_THREADS SSA_ROWMUL_ROWS
+
+__global__ void __launch_bounds__(ROWMUL_THREADS) k_rowmul(const ssa_rowmul_job* __restrict__ jobs) {
+    __shared__ float sB[SSA_MAX_KP * SSA_MAX_KP];
+    __shared__ double wsum[ROWMUL_THREADS / 32][SSA_MAX_KP];
+    const ssa_rowmul_job J = jobs[blockIdx.y];
+    const int n = J.n, p = J.p;
+    if (blockIdx.x * ROWMUL_THREADS >= J.m) return;
+    for (int e = threadIdx.x; e < SSA_MAX_KP * p; e += blockDim.x) {
+        const int l = e % SSA_MAX_KP, j = e / SSA_MAX_KP;
+        sB[e] = l < n ? J.Bm[l + j * J.ldb] : 0.f;
+    }
+    __syncthreads();
+    const int i = blockIdx.x * ROWMUL_THREADS + threadIdx.x;
+    const bool live = i < J.m;
+    float a[SSA_MAX_KP];
+#pragma unroll
+    for (int l = 0; l < SSA_MAX_KP; ++l)
+        a[l] = (live && l < n) ? J.A[(long long)i + (long long)l * J.lda] : 0.f;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int j = 0; j < p; ++j) {
+        const float* b = sB + j * SSA_MAX_KP;
+        float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+        for (int l = 0; l < SSA_MAX_KP; l += 2) {
+            s0 = fmaf(a[l], b[l], s0);
+            s1 = fmaf(a[l + 1], b[l + 1], s1);
+        }
+        const float c = s0 + s1;
+        if (live) J.C[(long long)i + (long long)j * J.ldc] = c;
+        if (J.colsum) {
+            double v = live ? (double)c : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) wsum[warp][j] = v;
+        }
+    }
+    if (J.colsum) {
+        __syncthreads();
+        for (int j = threadIdx.x; j < p; j += blockDim.x) {
+            double t = 0.0;
+            for (int w = 0; w < ROWMUL_THREADS / 32; ++w) t += wsum[w][j];
+            J.colsum[(long long)blockIdx.x * p + j] = t;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Rayleigh-Ritz: FP64 parallel cyclic Jacobi on G_B = B^T B
+// ---------------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(SMALL_THREADS) k_rr(const ssa_rr_job* __restrict__ jobs) {
+    extern __shared__ double dsm[];
+    double* G = dsm;
+    double* Z = dsm + SSA_MAX_KP * SLD;
+    __shared__ double rc[SSA_MAX_KP / 2], rs[SSA_MAX_KP / 2];
+    __shared__ int pp[SSA_MAX_KP / 2], pq[SSA_MAX_KP / 2];
+    __shared__ int perm[SSA_MAX_KP + 1];
+    __shared__ double qs[SSA_MAX_KP];
+    __shared__ int order[SSA_MAX_KP];
+    __shared__ int notconv;
+    const ssa_rr_job J = jobs[blockIdx.x];
+    const int n = J.kp;
+    reduce_packed(J.part, J.nchunks, n, G);
+    for (int e = threadIdx.x; e < n * SLD; e += blockDim.x) Z[e] = ((e % SLD) == (e / SLD)) ? 1.0 : 0.0;
+    for (int l = threadIdx.x; l < n; l += blockDim.x) {
+        double s = 0.0;
+        for (int c = 0; c < J.nchunks_q; ++c) s += J.qsum[(long long)c * n + l];
+        qs[l] = s;
+    }
+    const int ne = (n + 1) & ~1;  // even count; index n is a dummy when n is odd
+    for (int i = threadIdx.x; i < ne; i += blockDim.x) perm[i] = i;
+    __syncthreads();
+    const int npairs = ne / 2;
+    for (int sweep = 0; sweep < 40; ++sweep) {
+        if (threadIdx.x == 0) notconv = 0;
+        __syncthreads();
+        for (int step = 0; step < ne - 1; ++step) {
+            // rotations for this step
+            for (int t = threadIdx.x; t < npairs; t += blockDim.x) {
+                int p = perm[t], q = perm[ne - 1 - t];
+                if (p > q) {
+                    const int tmp = p;
+                    p = q;
+                    q = tmp;
+                }
+                double c = 1.0, s = 0.0;
+                if (q < n) {
+                    const double apq = G[p * SLD + q];
+                    const double app = G[p * SLD + p], aqq = G[q * SLD + q];
+                    if (fabs(apq) > 1e-300 && fabs(apq) > 1e-15 * sqrt(fabs(app * aqq))) {
+                        notconv = 1;
+                        const double tau = (aqq - app) / (2.0 * apq);
+                        const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                        c = 1.0 / sqrt(1.0 + tt * tt);
+                        s = tt * c;
+                    }
+                }
+                pp[t] = p;
+                pq[t] = q;
+                rc[t] = c;
+                rs[t] = s;
+            }
+            __syncthreads();
+            // G <- G J and Z <- Z J (columns p, q)
+            for (int e = threadIdx.x; e < npairs * n; e += blockDim.x) {
+                const int t = e / n, r = e % n;
+                const int p = pp[t], q = pq[t];
+                if (q >= n || rs[t] == 0.0) continue;
+                const double c = rc[t], s = rs[t];
+                const double gp = G[r * SLD + p], gq = G[r * SLD + q];
+                G[r * SLD + p] = c * gp - s * gq;
+                G[r * SLD + q] = s * gp + c * gq;
+                const double zp = Z[r * SLD + p], zq = Z[r * SLD + q];
+                Z[r * SLD + p] = c * zp - s * zq;
+                Z[r * SLD + q] = s * zp + c * zq;
+            }
+            __syncthreads();
+            // G <- J^T G (rows p, q)
+            for (int e = threadIdx.x; e < npairs * n; e += blockDim.x) {
+                const int t = e / n, r = e % n;
+                const int p = pp[t], q = pq[t];
+                if (q >= n || rs[t] == 0.0) continue;
+                const double c = rc[t], s = rs[t];
+                const double gp = G[p * SLD + r], gq = G[q * SLD + r];
+                G[p * SLD + r] = c * gp - s * gq;
+                G[q * SLD + r] = s * gp + c * gq;
+            }
+            __syncthreads();
+            // round-robin: keep perm[0], rotate perm[1..ne-1]
+            if (threadIdx.x == 0) {
+                const int last = perm[ne - 1];
+                for (int i = ne - 1; i > 1; --i) perm[i] = perm[i - 1];
+                perm[1] = last;
+            }
+            __syncthreads();
+        }
+        if (!notconv) break;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < n; ++i) order[i] = i;
+        for (int i = 0; i < n; ++i) {  // selection sort, descending eigenvalue
+            int best = i;
+            for (int j = i + 1; j < n; ++j)
+                if (G[order[j] * SLD + order[j]] > G[order[best] * SLD + order[best]]) best = j;
+            const int tmp = order[i];
+            order[i] = order[best];
+            order[best] = tmp;
+        }
+    }
+    __syncthreads();
+    const int k = J.k;
+    for (int j = threadIdx.x; j < k; j += blockDim.x) {
+        const int col = order[j];
+        const double lam = G[col * SLD + col];
+        const double sg = sqrt(fmax(lam, 0.0));
+        double dot = 0.0;
+        for (int l = 0; l < n; ++l) dot += qs[l] * Z[l * SLD + col];
+        const double sgn = dot < 0.0 ? -1.0 : 1.0;
+        const double isg = sg > 1e-300 ? 1.0 / sg : 0.0;
+        for (int l = 0; l < n; ++l) {
+            const double z = sgn * Z[l * SLD + col];
+            J.Zu[l + j * n] = (float)z;
+            J.Zv[l + j * n] = (float)(z * isg);
+        }
+        J.sigma[j] = sg;
+        if (!isfinite(sg) && J.status) atomicOr(J.status, 2);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// W-correlation finish and LRF forecast
+// ---------------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(SMALL_THREADS) k_wfin(const ssa_wfin_job* __restrict__ jobs) {
+    __shared__ double G[SSA_MAX_KP * SLD];
+    const ssa_wfin_job J = jobs[blockIdx.x];
+    const int k = J.k;
+    reduce_packed(J.part, J.nchunks, k, G);
+    __syncthreads();
+    for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
+        const int i = e / k, j = e % k;
+        const double ni = sqrt(G[i * SLD + i]), nj = sqrt(G[j * SLD + j]);
+        double w = 0.0;
+        if (ni > 1e-12 && nj > 1e-12) w = G[i * SLD + j] / (ni * nj);
+        J.W[e] = w;
+    }
+}
+
+__global__ void __launch_bounds__(SMALL_THREADS) k_lrf(const ssa_lrf_job* __restrict__ jobs) {
+    __shared__ double red[32];
+    __shared__ double pi_s[SSA_MAX_KP];
+    __shared__ int ok;
+    const ssa_lrf_job J = jobs[blockIdx.x];
+    const int L = J.L, ng = J.n_group;
+    if (threadIdx.x == 0) {
+        double nu2 = 0.0;
+        for (int g = 0; g < ng; ++g) {
+            const double p = (double)J.U[(long long)(L - 1) + (long long)J.group[g] * J.ld];
+            pi_s[g] = p;
+            nu2 += p * p;
+        }
+        *J.verticality = nu2;
+        ok = nu2 < 1.0 - 1e-10;
+        if (!ok) atomicOr(J.status, 4);
+        red[0] = nu2;
+    }
+    __syncthreads();
+    if (!ok) return;
+    const double scale = 1.0 / (1.0 - red[0]);
+    __syncthreads();
+    const int w = L - 1;
+    for (int j = threadIdx.x; j < w; j += blockDim.x) {
+        double s = 0.0;
+        for (int g = 0; g < ng; ++g) s += pi_s[g] * (double)J.U[(long long)j + (long long)J.group[g] * J.ld];
+        J.R[j] = s * scale;
+        J.buf[j] = J.recon[J.N - w + j];
+    }
+    __syncthreads();
+    for (int h = 0; h < J.h; ++h) {
+        double s = 0.0;
+        for (int j = threadIdx.x; j < w; j += blockDim.x) s += J.R[j] * J.buf[h + j];
+        s = block_sum<double>(s, red);
+        if (threadIdx.x == 0) {
+            J.buf[w + h] = s;
+            J.out[h] = s;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_group_sum(ssa_gsum_job J) {
+    const int s = blockIdx.z, g = blockIdx.y;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= J.N) return;
+    const float* base = J.recon + (long long)s * J.recon_series;
+    double acc = 0.0;
+    for (int e = J.group_off[g]; e < J.group_off[g + 1]; ++e) {
+        const int i = J.group_idx[e];
+        if (i < 0 || i >= J.k) continue;
+        acc += (double)base[(long long)i * J.ld_recon + t];
+    }
+    J.out[(long long)s * J.out_series + (long long)g * J.N + t] = acc;
+}
+
+__global__ void k_gaussian(float* out, long long ld, int rows, int ncols, int col0, unsigned long long seed) {
+    const int c = blockIdx.y;
+    const int npairs = (rows + 1) / 2;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npairs; i += gridDim.x * blockDim.x) {
+        const float2 v = gauss_pair(seed, col0 + c, i);
+        out[(long long)c * ld + 2 * i] = v.x;
+        if (2 * i + 1 < rows) out[(long long)c * ld + 2 * i + 1] = v.y;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------------------------
+
+extern "C" int ssad_logh_for(int N) {
+    int logm = 5;  // M >= 32
+    while ((1 << logm) < N) ++logm;
+    return logm - 1;
+}
+
+extern "C" int ssad_init_device(void) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return (int)e;
+    static bool done[64] = {false};
+    if (dev < 64 && done[dev]) return 0;
+    std::vector<float2> tw(SSA_TW_N);
+    for (int t = 0; t < SSA_TW_N; ++t) {
+        const double a = -2.0 * M_PI * (double)t / (double)SSA_TW_N;
+        tw[t] = make_float2((float)cos(a), (float)sin(a));
+    }
+    e = cudaMemcpyToSymbol(g_tw, tw.data(), sizeof(float2) * SSA_TW_N);
+    if (e != cudaSuccess) return (int)e;
+    if (dev < 64) done[dev] = true;
+    return 0;
+}
+
+template <int LOGH>
+static int smem_bytes(int bufs) { return bufs * spad_size(1 << LOGH) * (int)sizeof(float2); }
+
+template <typename KernelT>
+static cudaError_t set_smem(KernelT kern, int bytes) {
+    if (bytes > 48 * 1024) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return cudaSuccess;
+}
+
+#define SSA_LOGH_DISPATCH(logh, CALL)                                    \
+    switch (logh) {                                                      \
+        case 4: CALL(4); break;                                          \
+        case 5: CALL(5); break;                                          \
+        case 6: CALL(6); break;                                          \
+        case 7: CALL(7); break;                                          \
+        case 8: CALL(8); break;                                          \
+        case 9: CALL(9); break;                                          \
+        case 10: CALL(10); break;                                        \
+        case 11: CALL(11); break;                                        \
+        case 12: CALL(12); break;                                        \
+        case 13: CALL(13); break;                                        \
+        case 14: CALL(14); break;                                        \
+        default: return (int)cudaErrorInvalidValue;                      \
+    }
+
+template <int LOGH>
+static int launch_spectrum(const ssa_col_job* jobs, int njobs, int maxcols, cudaStream_t st) {
+    const int sm = smem_bytes<LOGH>(1);
+    cudaError_t e = set_smem(k_spectrum<LOGH>, sm);
+    if (e != cudaSuccess) return (int)e;
+    k_spectrum<LOGH><<<dim3(maxcols, njobs), FftShape<LOGH>::BLOCK, sm, st>>>(jobs);
+    return launched(cudaGetLastError());
+}
+template <int LOGH>
+static int launch_corr(const ssa_col_job* jobs, int njobs, int maxcols, cudaStream_t st) {
+    const int sm = smem_bytes<LOGH>(1);
+    cudaError_t e = set_smem(k_corr<LOGH>, sm);
+    if (e != cudaSuccess) return (int)e;
+    k_corr<LOGH><<<dim3(maxcols, njobs), FftShape<LOGH>::BLOCK, sm, st>>>(jobs);
+    return launched(cudaGetLastError());
+}
+template <int LOGH>
+static int launch_elem(const ssa_col_job* jobs, int njobs, int maxcols, cudaStream_t st) {
+    const int sm = smem_bytes<LOGH>(2);
+    if (sm > 227 * 1024) return (int)cudaErrorInvalidValue;
+    cudaError_t e = set_smem(k_elem_recon<LOGH>, sm);
+    if (e != cudaSuccess) return (int)e;
+    k_elem_recon<LOGH><<<dim3(maxcols, njobs), FftShape<LOGH>::BLOCK, sm, st>>>(jobs);
+    return launched(cudaGetLastError());
+}
+template <int LOGH>
+static int launch_recon(const ssa_recon_job* jobs, int njobs, cudaStream_t st) {
+    const int sm = smem_bytes<LOGH>(1);
+    cudaError_t e = set_smem(k_recon<LOGH>, sm);
+    if (e != cudaSuccess) return (int)e;
+    k_recon<LOGH><<<dim3(1, njobs), FftShape<LOGH>::BLOCK, sm, st>>>(jobs);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_spectrum(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
+    if (njobs <= 0 || maxcols <= 0) return 0;
+#define CALL(L) return launch_spectrum<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
+    SSA_LOGH_DISPATCH(logh, CALL)
+#undef CALL
+    return 0;
+}
+extern "C" int ssad_corr(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
+    if (njobs <= 0 || maxcols <= 0) return 0;
+#define CALL(L) return launch_corr<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
+    SSA_LOGH_DISPATCH(logh, CALL)
+#undef CALL
+    return 0;
+}
+extern "C" int ssad_elem_recon(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
+    if (njobs <= 0 || maxcols <= 0) return 0;
+#define CALL(L) return launch_elem<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
+    SSA_LOGH_DISPATCH(logh, CALL)
+#undef CALL
+    return 0;
+}
+extern "C" int ssad_recon(const ssa_recon_job* d_jobs, int njobs, int logh, void* stream) {
+    if (njobs <= 0) return 0;
+#define CALL(L) return launch_recon<L>(d_jobs, njobs, (cudaStream_t)stream)
+    SSA_LOGH_DISPATCH(logh, CALL)
+#undef CALL
+    return 0;
+}
+
+extern "C" int ssad_gram(const ssa_gram_job* d_jobs, int njobs, int maxchunks, int weighted, void* stream) {
+    if (njobs <= 0 || maxchunks <= 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (weighted)
+        k_gram<true><<<dim3(maxchunks, njobs), GRAM_THREADS, 0, st>>>(d_jobs);
+    else
+        k_gram<false><<<dim3(maxchunks, njobs), GRAM_THREADS, 0, st>>>(d_jobs);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_chol(const ssa_chol_job* d_jobs, int njobs, void* stream) {
+    if (njobs <= 0) return 0;
+    cudaError_t e = set_smem(k_chol, SMALL_SMEM);
+    if (e != cudaSuccess) return (int)e;
+    k_chol<<<njobs, SMALL_THREADS, SMALL_SMEM, (cudaStream_t)stream>>>(d_jobs);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_rowmul(const ssa_rowmul_job* d_jobs, int njobs, int maxrows, int maxn, void* stream) {
+    if (njobs <= 0 || maxrows <= 0) return 0;
+    if (maxn > SSA_MAX_KP) return (int)cudaErrorInvalidValue;
+    k_rowmul<<<dim3((maxrows + ROWMUL_THREADS - 1) / ROWMUL_THREADS, njobs), ROWMUL_THREADS, 0,
+               (cudaStream_t)stream>>>(d_jobs);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_rr(const ssa_rr_job* d_jobs, int njobs, void* stream) {
+    if (njobs <= 0) return 0;
+    cudaError_t e = set_smem(k_rr, SMALL_SMEM);
+    if (e != cudaSuccess) return (int)e;
+    k_rr<<<njobs, SMALL_THREADS, SMALL_SMEM, (cudaStream_t)stream>>>(d_jobs);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_wfin(const ssa_wfin_job* d_jobs, int njobs, void* stream) {
+    if (njobs <= 0) return 0;
+    k_wfin<<<njobs, SMALL_THREADS, 0, (cudaStream_t)stream>>>(d_jobs);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_lrf(const ssa_lrf_job* d_jobs, int njobs, void* stream) {
+    if (njobs <= 0) return 0;
+    k_lrf<<<njobs, SMALL_THREADS, 0, (cudaStream_t)stream>>>(d_jobs);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_group_sum(ssa_gsum_job job, void* stream) {
+    if (job.B <= 0 || job.n_groups <= 0) return 0;
+    k_group_sum<<<dim3((job.N + 255) / 256, job.n_groups, job.B), 256, 0, (cudaStream_t)stream>>>(job);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_gaussian(float* out, long long ld, int rows, int ncols, int col0, unsigned long long seed,
+                             void* stream) {
+    if (rows <= 0 || ncols <= 0) return 0;
+    const int npairs = (rows + 1) / 2;
+    const int bx = (npairs + 255) / 256;
+    k_gaussian<<<dim3(bx < 64 ? bx : 64, ncols), 256, 0, (cudaStream_t)stream>>>(out, ld, rows, ncols, col0, seed);
+    return launched(cudaGetLastError());
+}

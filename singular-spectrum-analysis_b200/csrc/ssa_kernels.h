@@ -1,0 +1,171 @@
+/*
+ * C-ABI between the C host layer (ssa_host.c) and the sm_100a kernels (ssa_kernels.cu).
+ * Plain pointers and sizes only; every pointer is device memory unless its name says host.
+ * Each launcher enqueues work on `stream` and returns a cudaError_t value (0 = success)
+ * without synchronising.
+ *
+ * Job tables (arrays of the structs below) live in device memory; one launch processes every
+ * job of a table, blockIdx.y selecting the job. Column-major matrices: column c of an m x n
+ * matrix with leading dimension ld starts at c * ld. Leading dimensions of float matrices are
+ * even, so columns are 8-byte aligned. Spectra are interleaved complex floats (re, im), H + 1
+ * values for a real sequence of length M = 2H (bins 0..H).
+ */
+#ifndef SSA_KERNELS_H
+#define SSA_KERNELS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Largest (k + p) the Gram / Cholesky / Rayleigh-Ritz kernels hold on chip. */
+#define SSA_MAX_KP 64
+/* Rows staged in shared memory per step of the Gram kernel. */
+#define SSA_GRAM_CHUNK 128
+
+/* FFT-length bucket: real length M = 2^(logh + 1). */
+int ssad_logh_for(int N);
+
+/* Column job for the FFT kernels (signal spectrum, correlation matvec, reconstruction). */
+typedef struct
+{
+    const float *in;      /* column c at in + c * ld_in; NULL => generated N(0,1) (seed) */
+    const double *in64;   /* double input (signal spectrum only), used when in == NULL and in64 != NULL */
+    const float *in2;     /* second operand column c at in2 + c * ld_in2 (reconstruction: V) */
+    float *out;           /* column c at out + c * ld_out */
+    const float *X;       /* spectrum of the series (correlation) */
+    float *spec;          /* spectrum output (spectrum kernel): column c at spec + c * ld_spec floats */
+    const double *scale;  /* optional per-column scale (sigma), NULL = 1 */
+    double *norm2;        /* optional per-column weighted norm^2 output (reconstruction) */
+    unsigned long long seed;
+    long long ld_in, ld_out, ld_spec, ld_in2;
+    int n_in, n_out, ncols, n_in2;
+    int col0;             /* first generated column index (RNG counter offset) */
+    int N, L, K;          /* series dims, used for the diagonal-averaging weights */
+} ssa_col_job;
+
+/* Gram job: part[chunk] = A_chunk^T W A_chunk (n x n, FP64) over rows of A (m x n, ld). */
+typedef struct
+{
+    const float *A;
+    double *part;         /* nchunks * n(n+1)/2 doubles: packed upper triangle, row-major */
+    double *colsum;       /* optional: nchunks * n partial column sums of A, NULL = skip */
+    long long ld;
+    int m, n;
+    int rows_per_cta;     /* rows folded into one partial (multiple of SSA_GRAM_CHUNK) */
+    int weighted;         /* 1: row t weighted by min(t+1, L, K, N-t) */
+    int N, L, K;
+} ssa_gram_job;
+
+/* Cholesky job: G = sum of the partials; G = R^T R; Rinv = R^{-1} (fp32, n x n col-major). */
+typedef struct
+{
+    const double *part;
+    float *Rinv;
+    int *status;          /* set to a nonzero code on failure (non-finite Gram) */
+    int nchunks, n;
+    int pad_[2];
+} ssa_chol_job;
+
+/* C[:, 0:p] = A[:, 0:n] * Bm[0:n, 0:p] row by row (in place allowed when C == A, p <= n and
+ * Bm is upper triangular or row i of C depends only on row i of A). */
+typedef struct
+{
+    const float *A;
+    const float *Bm;      /* n x p col-major, ld = ldb */
+    float *C;
+    double *colsum;       /* optional: per-CTA partial column sums of C, [blockIdx.x][p] */
+    long long lda, ldc;
+    int m, n, p, ldb;
+} ssa_rowmul_job;
+
+/* Rows of C per k_rowmul CTA (granularity of the colsum partials). */
+#define SSA_ROWMUL_ROWS 128
+
+/* Rayleigh-Ritz job: G_B = sum of partials (kp x kp), eigen-decomposition in FP64,
+ * sigma (k), Zu = Z[:, :k] and Zv = Z[:, :k] diag(1/sigma), both sign-fixed with the column
+ * sums of Q (sum_i U[i, j] >= 0). */
+typedef struct
+{
+    const double *part;
+    const double *qsum;   /* nchunks_q * kp partial column sums of Q */
+    double *sigma;        /* k */
+    float *Zu, *Zv;       /* kp x k, ld = kp */
+    int *status;
+    int nchunks, nchunks_q, kp, k;
+} ssa_rr_job;
+
+/* Reconstruction from cached spectra: out = inv_w * IFFT(sum_{g} Us[g] * Vs[g]). */
+typedef struct
+{
+    const float *Us, *Vs;     /* spectra: component i at Us + i * ld_spec */
+    const int *group;         /* n_group component indices (out of range skipped) */
+    double *out64;            /* optional double output (N) */
+    float *out;               /* optional float output (N) */
+    long long ld_spec;
+    int n_group, k;
+    int N, L, K;
+    int pad_;
+} ssa_recon_job;
+
+/* W-correlation finish: W[i][j] = G_ij / sqrt(G_ii G_jj) (0 when a norm <= 1e-12). */
+typedef struct
+{
+    const double *part;
+    double *W;                /* k x k row-major */
+    int nchunks, k;
+} ssa_wfin_job;
+
+/* R-forecast: LRF from U rows (FP64) and the recurrence over the reconstruction. */
+typedef struct
+{
+    const float *U;           /* L x k, ld */
+    const int *group;
+    const double *recon;      /* N reconstructed values of the group */
+    double *R;                /* L - 1 LRF coefficients (output) */
+    double *buf;              /* scratch: L - 1 + h */
+    double *out;              /* h forecasts */
+    double *verticality;
+    int *status;
+    long long ld;
+    int L, N, n_group, h, k;
+    int pad_;
+} ssa_lrf_job;
+
+/* Group sums of elementary reconstructions: out[s][g][t] = sum_{i in group g} recon[s][i][t]. */
+typedef struct
+{
+    const float *recon;       /* series s, component i at recon + s * recon_series + i * ld_recon */
+    long long ld_recon, recon_series;
+    const int *group_idx;     /* concatenated component indices */
+    const int *group_off;     /* n_groups + 1 offsets into group_idx */
+    double *out;              /* series s, group g at out + s * out_series + g * N */
+    long long out_series;
+    int n_groups, N, k, B;
+} ssa_gsum_job;
+
+int ssad_init_device(void);
+int ssad_group_sum(ssa_gsum_job job, void *stream);
+int ssad_spectrum(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);
+int ssad_corr(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);
+int ssad_elem_recon(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);
+/* All jobs of one launch share `weighted`. */
+int ssad_gram(const ssa_gram_job *d_jobs, int njobs, int maxchunks, int weighted, void *stream);
+int ssad_chol(const ssa_chol_job *d_jobs, int njobs, void *stream);
+int ssad_rowmul(const ssa_rowmul_job *d_jobs, int njobs, int maxrows, int maxn, void *stream);
+int ssad_rr(const ssa_rr_job *d_jobs, int njobs, void *stream);
+int ssad_recon(const ssa_recon_job *d_jobs, int njobs, int logh, void *stream);
+int ssad_wfin(const ssa_wfin_job *d_jobs, int njobs, void *stream);
+int ssad_lrf(const ssa_lrf_job *d_jobs, int njobs, void *stream);
+/* Column-major K x ncols N(0,1) matrix from the device generator (the same values the
+ * correlation kernel generates when its input is NULL). */
+int ssad_gaussian(float *out, long long ld, int rows, int ncols, int col0, unsigned long long seed,
+                  void *stream);
+/* Count of kernel launches issued by this library since load (all devices). */
+unsigned long long ssad_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

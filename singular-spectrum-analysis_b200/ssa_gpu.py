@@ -1,0 +1,501 @@
+"""Python interface of the B200 SSA library (libssa.so in this directory).
+
+Mirrors the classes and functions of SSA-Opt's ctypes wrapper (MKL/py/ssa_wrapper.py: ``SSA``
+:600-1202, ``MSSA`` :1208-1371, ``cadzow`` :415-489) with the same method names, argument
+meaning and error behaviour (``ValueError`` on a failed init, ``RuntimeError`` on a failed
+call), and adds what the reference wrapper cannot express: power iterations and a caller-supplied
+Gaussian test matrix for the randomized decomposition, and the batched pipeline (``SSABatch``).
+
+Every numerical call runs on the GPU through the C ABI of libssa.so; there is no CPU path.
+Importing this module raises ``ImportError`` when libssa.so has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libssa.so"
+if not LIB_PATH.exists():
+    raise ImportError(f"{LIB_PATH} is missing: run build.py (nvcc, sm_100a) first")
+
+_lib = ctypes.CDLL(str(LIB_PATH))
+
+c_double_p = ctypes.POINTER(ctypes.c_double)
+c_int_p = ctypes.POINTER(ctypes.c_int)
+
+
+class _Opaque1024(ctypes.Structure):
+    _fields_ = [("_opaque", ctypes.c_char * 1024)]
+
+
+class _SSA_LRF(ctypes.Structure):
+    _fields_ = [("R", c_double_p), ("L", ctypes.c_int), ("verticality", ctypes.c_double), ("valid", ctypes.c_bool)]
+
+
+class _SSA_CadzowResult(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("final_diff", ctypes.c_double), ("converged", ctypes.c_double)]
+
+
+class _BatchResults(ctypes.Structure):
+    _fields_ = [("sigma", ctypes.c_void_p), ("W", ctypes.c_void_p), ("groups", ctypes.c_void_p),
+                ("recon", ctypes.c_void_p), ("ld_recon", ctypes.c_longlong), ("status", ctypes.c_void_p),
+                ("stream", ctypes.c_void_p)]
+
+
+_P = ctypes.POINTER(_Opaque1024)
+
+
+def _sig(name, restype, *argtypes):
+    f = getattr(_lib, name)
+    f.restype = restype
+    f.argtypes = list(argtypes)
+    return f
+
+
+_I, _D, _V = ctypes.c_int, ctypes.c_double, None
+_sig("ssa_opt_init", _I, _P, c_double_p, _I, _I)
+_sig("ssa_opt_free", _V, _P)
+_sig("ssa_opt_prepare", _I, _P, _I, _I)
+_sig("ssa_opt_free_prepared", _V, _P)
+_sig("ssa_opt_update_signal", _I, _P, c_double_p)
+_sig("ssa_opt_decompose", _I, _P, _I, _I)
+_sig("ssa_opt_decompose_block", _I, _P, _I, _I, _I)
+_sig("ssa_opt_decompose_randomized", _I, _P, _I, _I)
+_sig("ssa_opt_decompose_randomized_ex", _I, _P, _I, _I, _I, c_double_p)
+_sig("ssa_opt_reconstruct", _I, _P, c_int_p, _I, c_double_p)
+_sig("ssa_opt_cache_ffts", _I, _P)
+_sig("ssa_opt_forecast", _I, _P, c_int_p, _I, _I, c_double_p)
+_sig("ssa_opt_forecast_full", _I, _P, c_int_p, _I, _I, c_double_p)
+_sig("ssa_opt_compute_lrf", _I, _P, c_int_p, _I, ctypes.POINTER(_SSA_LRF))
+_sig("ssa_opt_lrf_free", _V, ctypes.POINTER(_SSA_LRF))
+_sig("ssa_opt_forecast_with_lrf", _I, ctypes.POINTER(_SSA_LRF), c_double_p, _I, _I, c_double_p)
+_sig("ssa_opt_wcorr_matrix", _I, _P, c_double_p)
+_sig("ssa_opt_wcorr_pair", _D, _P, _I, _I)
+_sig("ssa_opt_variance_explained", _D, _P, _I, _I)
+_sig("ssa_opt_find_periodic_pairs", _I, _P, c_int_p, _I, _D, _D)
+_sig("ssa_opt_get_trend", _I, _P, c_double_p)
+_sig("ssa_opt_get_noise", _I, _P, _I, c_double_p)
+_sig("ssa_opt_get_singular_values", _I, _P, c_double_p, _I)
+_sig("ssa_opt_get_eigenvalues", _I, _P, c_double_p, _I)
+_sig("ssa_opt_get_total_variance", _D, _P)
+_sig("ssa_opt_hankel_matvec_dev", _I, _P, c_double_p, c_double_p)
+_sig("ssa_opt_hankel_matvec_T_dev", _I, _P, c_double_p, c_double_p)
+_sig("ssa_opt_cadzow", _I, c_double_p, _I, _I, _I, _I, _D, c_double_p, ctypes.POINTER(_SSA_CadzowResult))
+_sig("ssa_opt_cadzow_weighted", _I, c_double_p, _I, _I, _I, _I, _D, _D, c_double_p,
+     ctypes.POINTER(_SSA_CadzowResult))
+_sig("mssa_opt_init", _I, _P, c_double_p, _I, _I, _I)
+_sig("mssa_opt_decompose", _I, _P, _I, _I)
+_sig("mssa_opt_decompose_ex", _I, _P, _I, _I, _I, c_double_p)
+_sig("mssa_opt_reconstruct", _I, _P, _I, c_int_p, _I, c_double_p)
+_sig("mssa_opt_reconstruct_all", _I, _P, c_int_p, _I, c_double_p)
+_sig("mssa_opt_series_contributions", _I, _P, c_double_p)
+_sig("mssa_opt_variance_explained", _D, _P, _I, _I)
+_sig("mssa_opt_free", _V, _P)
+_sig("ssa_opt_copy_factors", _I, _P, c_double_p, c_double_p)
+_sig("ssa_b200_kernel_launches", ctypes.c_ulonglong)
+_sig("ssa_b200_sizeof_ssa_opt", _I)
+_sig("ssa_batch_create", _I, ctypes.POINTER(ctypes.c_void_p), _I, _I, _I, _I, _I, _I, c_int_p, c_int_p, _I)
+_sig("ssa_batch_destroy", _V, ctypes.c_void_p)
+_sig("ssa_batch_run", _I, ctypes.c_void_p, c_double_p, _I, ctypes.c_uint64, c_double_p, c_double_p, c_double_p)
+_sig("ssa_batch_run_device", _I, ctypes.c_void_p, ctypes.c_void_p, _I, ctypes.c_uint64)
+_sig("ssa_batch_sync", _I, ctypes.c_void_p)
+_sig("ssa_batch_device_results", _I, ctypes.c_void_p, ctypes.POINTER(_BatchResults))
+_sig("ssa_batch_set_profiling", _I, ctypes.c_void_p, _I)
+_sig("ssa_batch_profile", _I, ctypes.c_void_p, c_double_p, ctypes.POINTER(ctypes.c_longlong), _I)
+
+PROFILE_KINDS = ("spectrum", "corr", "gram", "chol", "rowmul", "rr", "elem_recon", "wcorr_finish", "group_sum",
+                 "recon", "lrf")
+
+
+def kernel_launches() -> int:
+    """CUDA kernel launches issued by libssa.so in this process."""
+    return int(_lib.ssa_b200_kernel_launches())
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(c_double_p)
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(c_int_p)
+
+
+class CadzowResult:
+    """Result of Cadzow iterations (MKL/py/ssa_wrapper.py:400-413)."""
+
+    def __init__(self, signal: np.ndarray, iterations: int, final_diff: float, converged: bool):
+        self.signal = signal
+        self.iterations = iterations
+        self.final_diff = final_diff
+        self.converged = converged
+
+    def __repr__(self):
+        return f"CadzowResult(iterations={self.iterations}, final_diff={self.final_diff:.2e}, converged={self.converged})"
+
+
+def cadzow(x: np.ndarray, L: int, rank: int, max_iter: int = 20, tol: float = 1e-9, alpha: float = 1.0) -> CadzowResult:
+    """Cadzow iterations (MKL/py/ssa_wrapper.py:415-489 -> ssa_opt_cadzow)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    N = len(x)
+    out = np.zeros(N)
+    res = _SSA_CadzowResult()
+    if alpha == 1.0:
+        ret = _lib.ssa_opt_cadzow(_dp(x), N, L, rank, max_iter, tol, _dp(out), ctypes.byref(res))
+    else:
+        ret = _lib.ssa_opt_cadzow_weighted(_dp(x), N, L, rank, max_iter, tol, alpha, _dp(out), ctypes.byref(res))
+    if ret < 0:
+        raise RuntimeError("Cadzow iterations failed")
+    return CadzowResult(out, res.iterations, res.final_diff, bool(res.converged))
+
+
+class SSA:
+    """Univariate SSA on the GPU (interface of MKL/py/ssa_wrapper.py:600-1202)."""
+
+    def __init__(self, x: np.ndarray, L: int):
+        self._ctx = _Opaque1024()
+        self._x = np.ascontiguousarray(x, dtype=np.float64)
+        self.N = len(self._x)
+        self.L = L
+        self.K = self.N - L + 1
+        self.n_components = 0
+        self._decomposed = False
+        self._prepared = False
+        self._prepared_k = 0
+        self._prepared_oversampling = 0
+        if _lib.ssa_opt_init(ctypes.byref(self._ctx), _dp(self._x), self.N, L) != 0:
+            raise ValueError(f"SSA initialization failed (N={self.N}, L={L})")
+
+    def __del__(self):
+        if hasattr(self, "_ctx"):
+            _lib.ssa_opt_free(ctypes.byref(self._ctx))
+
+    def prepare(self, max_k: int, oversampling: int = 8) -> "SSA":
+        if _lib.ssa_opt_prepare(ctypes.byref(self._ctx), max_k, oversampling) != 0:
+            raise RuntimeError(f"prepare() failed (max_k={max_k})")
+        self._prepared = True
+        self._prepared_k = max_k
+        self._prepared_oversampling = oversampling
+        return self
+
+    def update_signal(self, new_x: np.ndarray) -> "SSA":
+        new_x = np.ascontiguousarray(new_x, dtype=np.float64)
+        if len(new_x) != self.N:
+            raise ValueError(f"Signal length mismatch: {len(new_x)} vs {self.N}")
+        if _lib.ssa_opt_update_signal(ctypes.byref(self._ctx), _dp(new_x)) != 0:
+            raise RuntimeError("update_signal() failed")
+        self._x = new_x
+        return self
+
+    def decompose(self, k: int, method: str = "randomized", **kwargs) -> "SSA":
+        """``method`` "randomized" (kwargs: oversampling=8, power_iters=0, omega=None),
+        "block" (block_size, max_iter) or "sequential" (max_iter)."""
+        if method == "randomized":
+            oversampling = kwargs.get("oversampling", 8)
+            q = int(kwargs.get("power_iters", 0))
+            omega = kwargs.get("omega", None)
+            kp = k + oversampling
+            if not self._prepared or kp > self._prepared_k + self._prepared_oversampling:
+                self.prepare(k, oversampling)
+            if q == 0 and omega is None:
+                ret = _lib.ssa_opt_decompose_randomized(ctypes.byref(self._ctx), k, oversampling)
+            else:
+                om = None
+                if omega is not None:
+                    om = np.asfortranarray(omega, dtype=np.float64)
+                    if om.shape[0] != self.K:
+                        raise ValueError(f"omega must have K={self.K} rows")
+                    om = np.ascontiguousarray(om.T)  # column-major K x kp as flat memory
+                ret = _lib.ssa_opt_decompose_randomized_ex(ctypes.byref(self._ctx), k, oversampling, q,
+                                                            _dp(om) if om is not None else None)
+        elif method == "block":
+            block_size = kwargs.get("block_size", min(k, 32))
+            max_iter = kwargs.get("max_iter", 100)
+            ret = _lib.ssa_opt_decompose_block(ctypes.byref(self._ctx), k, block_size, max_iter)
+        elif method == "sequential":
+            ret = _lib.ssa_opt_decompose(ctypes.byref(self._ctx), k, kwargs.get("max_iter", 100))
+        else:
+            raise ValueError(f"Unknown method: {method}")
+        if ret != 0:
+            raise RuntimeError(f"Decomposition failed (method={method}, k={k})")
+        self.n_components = min(k, min(self.L, self.K))
+        self._decomposed = True
+        return self
+
+    def _need(self):
+        if not self._decomposed:
+            raise RuntimeError("Call decompose() first")
+
+    @property
+    def singular_values(self) -> np.ndarray:
+        self._need()
+        out = np.zeros(self.n_components)
+        n = _lib.ssa_opt_get_singular_values(ctypes.byref(self._ctx), _dp(out), self.n_components)
+        return out[:n]
+
+    @property
+    def eigenvalues(self) -> np.ndarray:
+        self._need()
+        out = np.zeros(self.n_components)
+        n = _lib.ssa_opt_get_eigenvalues(ctypes.byref(self._ctx), _dp(out), self.n_components)
+        return out[:n]
+
+    @property
+    def total_variance(self) -> float:
+        self._need()
+        return _lib.ssa_opt_get_total_variance(ctypes.byref(self._ctx))
+
+    def reconstruct(self, group: List[int]) -> np.ndarray:
+        self._need()
+        out = np.zeros(self.N)
+        g = np.ascontiguousarray(group, dtype=np.int32)
+        if _lib.ssa_opt_reconstruct(ctypes.byref(self._ctx), _ip(g), len(group), _dp(out)) != 0:
+            raise RuntimeError("Reconstruction failed")
+        return out
+
+    def cache_ffts(self) -> "SSA":
+        if _lib.ssa_opt_cache_ffts(ctypes.byref(self._ctx)) != 0:
+            raise RuntimeError("cache_ffts failed")
+        return self
+
+    def forecast(self, group: List[int], n_forecast: int) -> np.ndarray:
+        self._need()
+        out = np.zeros(n_forecast)
+        g = np.ascontiguousarray(group, dtype=np.int32)
+        if _lib.ssa_opt_forecast(ctypes.byref(self._ctx), _ip(g), len(group), n_forecast, _dp(out)) != 0:
+            raise RuntimeError("Forecast failed (verticality >= 1?)")
+        return out
+
+    def forecast_full(self, group: List[int], n_forecast: int) -> np.ndarray:
+        self._need()
+        out = np.zeros(self.N + n_forecast)
+        g = np.ascontiguousarray(group, dtype=np.int32)
+        if _lib.ssa_opt_forecast_full(ctypes.byref(self._ctx), _ip(g), len(group), n_forecast, _dp(out)) != 0:
+            raise RuntimeError("Forecast failed")
+        return out
+
+    def lrf(self, group: List[int]) -> Tuple[np.ndarray, float]:
+        """LRF coefficients R (L - 1) and verticality nu^2 (ssa_opt_compute_lrf)."""
+        self._need()
+        g = np.ascontiguousarray(group, dtype=np.int32)
+        lrf = _SSA_LRF()
+        if _lib.ssa_opt_compute_lrf(ctypes.byref(self._ctx), _ip(g), len(group), ctypes.byref(lrf)) != 0:
+            raise RuntimeError("compute_lrf failed")
+        R = np.ctypeslib.as_array(lrf.R, shape=(self.L - 1,)).copy()
+        v = lrf.verticality
+        _lib.ssa_opt_lrf_free(ctypes.byref(lrf))
+        return R, v
+
+    def get_trend(self) -> np.ndarray:
+        self._need()
+        out = np.zeros(self.N)
+        if _lib.ssa_opt_get_trend(ctypes.byref(self._ctx), _dp(out)) != 0:
+            raise RuntimeError("get_trend failed")
+        return out
+
+    def get_noise(self, noise_start: int) -> np.ndarray:
+        self._need()
+        out = np.zeros(self.N)
+        if _lib.ssa_opt_get_noise(ctypes.byref(self._ctx), noise_start, _dp(out)) != 0:
+            raise RuntimeError("get_noise failed")
+        return out
+
+    def cadzow(self, rank: int, max_iter: int = 20, tol: float = 1e-9, alpha: float = 1.0) -> CadzowResult:
+        return cadzow(self._x, self.L, rank, max_iter, tol, alpha)
+
+    def wcorr_matrix(self) -> np.ndarray:
+        self._need()
+        k = self.n_components
+        W = np.zeros((k, k))
+        if _lib.ssa_opt_wcorr_matrix(ctypes.byref(self._ctx), _dp(W)) != 0:
+            raise RuntimeError("wcorr_matrix failed")
+        return W
+
+    def wcorr(self, i: int, j: int) -> float:
+        self._need()
+        return _lib.ssa_opt_wcorr_pair(ctypes.byref(self._ctx), i, j)
+
+    def variance_explained(self, start: int = 0, end: int = -1) -> float:
+        self._need()
+        return _lib.ssa_opt_variance_explained(ctypes.byref(self._ctx), start, end)
+
+    def find_periodic_pairs(self, max_pairs: int = 10, sv_tol: float = 0.1,
+                            wcorr_thresh: float = 0.5) -> List[Tuple[int, int]]:
+        self._need()
+        pairs = np.zeros(2 * max_pairs, dtype=np.int32)
+        n = _lib.ssa_opt_find_periodic_pairs(ctypes.byref(self._ctx), _ip(pairs), max_pairs, sv_tol, wcorr_thresh)
+        return [(int(pairs[2 * i]), int(pairs[2 * i + 1])) for i in range(n)]
+
+    def hankel_matvec(self, v: np.ndarray) -> np.ndarray:
+        """y = H v on the device (invalidates a previous decomposition of this object)."""
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        y = np.zeros(self.L)
+        if _lib.ssa_opt_hankel_matvec_dev(ctypes.byref(self._ctx), _dp(v), _dp(y)) != 0:
+            raise RuntimeError("hankel_matvec failed")
+        self._decomposed = False
+        return y
+
+    def hankel_matvec_T(self, u: np.ndarray) -> np.ndarray:
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        z = np.zeros(self.K)
+        if _lib.ssa_opt_hankel_matvec_T_dev(ctypes.byref(self._ctx), _dp(u), _dp(z)) != 0:
+            raise RuntimeError("hankel_matvec_T failed")
+        self._decomposed = False
+        return z
+
+    # factor access (host mirrors of the SSA_Opt fields U, V)
+    def factors(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """(U L x k, V K x k, sigma k) copied from the context's host fields."""
+        self._need()
+        k = self.n_components
+        U = np.zeros((k, self.L))
+        V = np.zeros((k, self.K))
+        if _lib.ssa_opt_copy_factors(ctypes.byref(self._ctx), _dp(U), _dp(V)) != k:
+            raise RuntimeError("copy_factors failed")
+        return U.T.copy(), V.T.copy(), self.singular_values
+
+    def parestimate(self, group: Optional[List[int]] = None):
+        raise RuntimeError("ESPRIT (parestimate) is not part of the accelerated path")
+
+    def vforecast(self, group: List[int], n_forecast: int) -> np.ndarray:
+        raise RuntimeError("V-forecast is not part of the accelerated path")
+
+
+class MSSA:
+    """Multivariate SSA on the GPU (interface of MKL/py/ssa_wrapper.py:1208-1371)."""
+
+    def __init__(self, X: np.ndarray, L: int):
+        self._ctx = _Opaque1024()
+        self._X = np.ascontiguousarray(X, dtype=np.float64)
+        if self._X.ndim != 2:
+            raise ValueError("X must be 2D array of shape (M, N)")
+        self.M, self.N = self._X.shape
+        self.L = L
+        self.K = self.N - L + 1
+        self.n_components = 0
+        self._decomposed = False
+        if _lib.mssa_opt_init(ctypes.byref(self._ctx), _dp(self._X), self.M, self.N, L) != 0:
+            raise ValueError(f"MSSA initialization failed (M={self.M}, N={self.N}, L={L})")
+
+    def __del__(self):
+        if hasattr(self, "_ctx"):
+            _lib.mssa_opt_free(ctypes.byref(self._ctx))
+
+    def decompose(self, k: int, oversampling: int = 8, power_iters: int = 0,
+                  omega: Optional[np.ndarray] = None) -> "MSSA":
+        if power_iters == 0 and omega is None:
+            ret = _lib.mssa_opt_decompose(ctypes.byref(self._ctx), k, oversampling)
+        else:
+            om = None
+            if omega is not None:
+                om = np.ascontiguousarray(np.asarray(omega, dtype=np.float64).T)
+            ret = _lib.mssa_opt_decompose_ex(ctypes.byref(self._ctx), k, oversampling, power_iters,
+                                             _dp(om) if om is not None else None)
+        if ret != 0:
+            raise RuntimeError(f"MSSA decomposition failed (k={k})")
+        self.n_components = k
+        self._decomposed = True
+        return self
+
+    def reconstruct(self, series_idx: int, group: List[int]) -> np.ndarray:
+        if not self._decomposed:
+            raise RuntimeError("Call decompose() first")
+        out = np.zeros(self.N)
+        g = np.ascontiguousarray(group, dtype=np.int32)
+        if _lib.mssa_opt_reconstruct(ctypes.byref(self._ctx), series_idx, _ip(g), len(group), _dp(out)) != 0:
+            raise RuntimeError("Reconstruction failed")
+        return out
+
+    def reconstruct_all(self, group: List[int]) -> np.ndarray:
+        if not self._decomposed:
+            raise RuntimeError("Call decompose() first")
+        out = np.zeros((self.M, self.N))
+        g = np.ascontiguousarray(group, dtype=np.int32)
+        if _lib.mssa_opt_reconstruct_all(ctypes.byref(self._ctx), _ip(g), len(group), _dp(out)) != 0:
+            raise RuntimeError("Reconstruction failed")
+        return out
+
+    def series_contributions(self) -> np.ndarray:
+        if not self._decomposed:
+            raise RuntimeError("Call decompose() first")
+        c = np.zeros((self.M, self.n_components))
+        if _lib.mssa_opt_series_contributions(ctypes.byref(self._ctx), _dp(c)) != 0:
+            raise RuntimeError("series_contributions failed")
+        return c
+
+    def variance_explained(self, start: int = 0, end: int = -1) -> float:
+        if not self._decomposed:
+            raise RuntimeError("Call decompose() first")
+        return _lib.mssa_opt_variance_explained(ctypes.byref(self._ctx), start, end)
+
+
+class SSABatch:
+    """Batched pipeline for up to ``max_series`` series of length N: decomposition, all k
+    elementary reconstructions, W-correlation and the sums of ``groups`` (ssa_batch_* C ABI)."""
+
+    def __init__(self, max_series: int, N: int, L: int, k: int, oversampling: int = 10, power_iters: int = 2,
+                 groups: Sequence[Sequence[int]] = ((0,), (1, 2))):
+        self.max_series, self.N, self.L = max_series, N, L
+        K = N - L + 1
+        kp = min(k + oversampling, L, K)
+        self.k = min(k, kp)
+        self.groups = [list(g) for g in groups]
+        idx = np.ascontiguousarray([i for g in self.groups for i in g] or [0], dtype=np.int32)
+        sizes = np.ascontiguousarray([len(g) for g in self.groups] or [0], dtype=np.int32)
+        self._h = ctypes.c_void_p()
+        if _lib.ssa_batch_create(ctypes.byref(self._h), max_series, N, L, k, oversampling, power_iters,
+                                 _ip(idx), _ip(sizes), len(self.groups)) != 0:
+            raise ValueError("ssa_batch_create failed")
+        self._keep = (idx, sizes)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.ssa_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def run(self, X: np.ndarray, seed: int = 0):
+        """Host-to-host run. Returns (sigma B x k, W B x k x k, groups B x n_groups x N)."""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        B = X.shape[0]
+        sigma = np.zeros((B, self.k))
+        W = np.zeros((B, self.k, self.k))
+        G = np.zeros((B, len(self.groups), self.N))
+        if _lib.ssa_batch_run(self._h, _dp(X), B, seed, _dp(sigma), _dp(W), _dp(G) if self.groups else None) != 0:
+            raise RuntimeError("ssa_batch_run failed")
+        return sigma, W, G
+
+    def run_device(self, d_x_ptr: int, B: int, seed: int = 0) -> None:
+        """Enqueue a run on device-resident input (B x N doubles at device address d_x_ptr)."""
+        if _lib.ssa_batch_run_device(self._h, ctypes.c_void_p(d_x_ptr), B, seed) != 0:
+            raise RuntimeError("ssa_batch_run_device failed")
+
+    def run_host_ptrs(self, x_ptr: int, B: int, seed: int, sigma_ptr: int, W_ptr: int, groups_ptr: int) -> None:
+        """Host-to-host run on caller-owned (ideally pinned) buffers given by address."""
+        vp = lambda a: ctypes.cast(ctypes.c_void_p(a), c_double_p) if a else None  # noqa: E731
+        if _lib.ssa_batch_run(self._h, vp(x_ptr), B, seed, vp(sigma_ptr), vp(W_ptr), vp(groups_ptr)) != 0:
+            raise RuntimeError("ssa_batch_run failed")
+
+    def sync(self) -> None:
+        if _lib.ssa_batch_sync(self._h) != 0:
+            raise RuntimeError("a series of the batch failed")
+
+    def set_profiling(self, on: bool) -> None:
+        if _lib.ssa_batch_set_profiling(self._h, 1 if on else 0) != 0:
+            raise RuntimeError("ssa_batch_set_profiling failed")
+
+    def profile(self) -> dict:
+        """{kind: (milliseconds, launches)} accumulated since profiling was switched on."""
+        ms = (ctypes.c_double * len(PROFILE_KINDS))()
+        n = (ctypes.c_longlong * len(PROFILE_KINDS))()
+        if _lib.ssa_batch_profile(self._h, ms, n, len(PROFILE_KINDS)) < 0:
+            raise RuntimeError("ssa_batch_profile failed")
+        return {k: (ms[i], int(n[i])) for i, k in enumerate(PROFILE_KINDS)}
+
+    def device_results(self) -> dict:
+        r = _BatchResults()
+        if _lib.ssa_batch_device_results(self._h, ctypes.byref(r)) != 0:
+            raise RuntimeError("ssa_batch_device_results failed")
+        return {"sigma": r.sigma, "W": r.W, "groups": r.groups, "recon": r.recon, "ld_recon": r.ld_recon,
+                "status": r.status, "stream": r.stream}

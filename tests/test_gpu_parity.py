@@ -1,0 +1,229 @@
+"""Parity of the CUDA path (through the C ABI of libssa.so) with the FP64 oracle.
+
+Tolerances (FP32 FFT convolutions and block products, FP64 Gram accumulation / Cholesky /
+Rayleigh-Ritz / LRF):
+  * matvec: max |y - y_ref| <= 1e-5 * ||x||_2 ||v||_2 (scale-relative; the reference's own KAT
+    uses 1e-10 absolute in FP64);
+  * singular values: relative error <= SIG_TOL = 1e-5 for every component whose relative gap
+    to its neighbours exceeds 1e-3, <= 1e-4 for the rest;
+  * reconstructions of groups [0] and [1, 2]: relative L2 <= REC_TOL = 1e-5 after sign
+    alignment (signs follow the reference rule sum(U[:, i]) >= 0, so no alignment is needed
+    unless that sum is ~0);
+  * W-correlation: max abs <= 1e-4 on the well-separated block, diagonal 1 within 1e-6.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SIG_TOL = 1e-5
+REC_TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    import ssa_gpu
+
+    return ssa_gpu
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def sigma_errors(s, ref):
+    rel = np.abs(s - ref) / ref
+    gap = np.full(len(ref), np.inf)
+    d = np.abs(np.diff(ref)) / ref[:-1]
+    gap[:-1] = np.minimum(gap[:-1], d)
+    gap[1:] = np.minimum(gap[1:], d)
+    return rel, gap
+
+
+@pytest.mark.parametrize("N,L", [(100, 25), (4, 2), (5, 3), (31, 10), (33, 32), (777, 300), (1000, 250),
+                                 (4096, 1024), (10000, 2500), (20000, 5000), (32768, 8192), (999, 998)])
+def test_matvec_vs_direct(gpu, oracle, N, L):
+    rng = np.random.default_rng(N + L)
+    if N == 100:
+        i = np.arange(N)
+        x = np.sin(0.1 * i) + 0.5 * np.cos(0.25 * i)  # MKL/test/ssa_opt_test.c:1474-1477
+    else:
+        x = rng.standard_normal(N) + 0.001 * np.arange(N)
+    K = N - L + 1
+    v = np.cos(0.05 * np.arange(K)) if N == 100 else rng.standard_normal(K)
+    u = rng.standard_normal(L)
+    s = gpu.SSA(x, L)
+    y = s.hankel_matvec(v)
+    z = s.hankel_matvec_T(u)
+    yr = oracle.hankel_matvec(x, v, L, oracle.next_pow2(max(N, 32)))
+    zr = oracle.hankel_matvec_T(x, u, L, oracle.next_pow2(max(N, 32)))
+    assert np.max(np.abs(y - yr)) <= 1e-5 * np.linalg.norm(x) * np.linalg.norm(v)
+    assert np.max(np.abs(z - zr)) <= 1e-5 * np.linalg.norm(x) * np.linalg.norm(u)
+
+
+@pytest.mark.parametrize("q", [0, 2])
+def test_config1_parity_host_omega(gpu, oracle, q):
+    x, clean, Om = oracle.config1(seed=0)
+    N, L, k, p = 1000, 250, 50, 10
+    d = oracle.decompose_randomized(x, L, k, p, Om, q=q)
+    gs = gpu.SSA(x, L)
+    gs.decompose(k, oversampling=p, power_iters=q, omega=Om)
+    U, V, s = gs.factors()
+    rel, gap = sigma_errors(s, d.sigma)
+    sep = gap > 1e-3
+    print(f"\nq={q}: max sigma rel err {rel.max():.2e} (separated {rel[sep].max():.2e})")
+    assert np.all(rel[sep] <= SIG_TOL)
+    assert np.all(rel <= 1e-4)
+    assert np.max(np.abs(U.T @ U - np.eye(k))) < 1e-4
+    for g in ([0], [1, 2]):
+        e = rel_l2(gs.reconstruct(g), oracle.reconstruct(d, g, N, L))
+        print(f"  group {g}: rel L2 {e:.2e}")
+        assert e <= REC_TOL
+    W = gs.wcorr_matrix()
+    Wr = oracle.wcorr_matrix(d, N, L)
+    print(f"  W max abs err {np.max(np.abs(W - Wr)):.2e}")
+    assert np.max(np.abs(np.diag(W) - 1.0)) < 1e-6
+    assert np.max(np.abs(W[:5, :5] - Wr[:5, :5])) < 1e-4
+
+
+def test_device_generator_matches_replica(gpu, oracle):
+    x, clean, _ = oracle.config1(seed=0)
+    N, L, k, p = 1000, 250, 20, 10
+    K = N - L + 1
+    gs = gpu.SSA(x, L)
+    gs.decompose(k, oversampling=p)  # q = 0, generated Omega, first draw of this context
+    Om = oracle.device_gaussian(oracle.single_series_seed(0), K, k + p)
+    d = oracle.decompose_randomized(x, L, k, p, Om, q=0)
+    rel, gap = sigma_errors(gs.singular_values, d.sigma)
+    assert np.all(rel[gap > 1e-3] <= SIG_TOL)
+    assert rel_l2(gs.reconstruct([0]), oracle.reconstruct(d, [0], N, L)) <= REC_TOL
+
+
+def test_q2_vs_dense_truth(gpu, oracle):
+    x, clean, Om = oracle.config1(seed=0)
+    N, L, k, p = 1000, 250, 50, 10
+    t = oracle.dense_svd(x, L, k)
+    gs = gpu.SSA(x, L)
+    gs.decompose(k, oversampling=p, power_iters=2, omega=Om)
+    s = gs.singular_values
+    # leading components converge to the exact SVD with q = 2 (oracle: <= 1e-9 for 3 components)
+    assert np.max(np.abs(s[:3] - t.sigma[:3]) / t.sigma[:3]) <= SIG_TOL
+    assert rel_l2(gs.reconstruct([0]), oracle.reconstruct(t, [0], N, L)) <= REC_TOL
+
+
+def test_forecast_parity(gpu, oracle):
+    x, clean, Om = oracle.config1(seed=0)
+    N, L, k, p = 1000, 250, 10, 10
+    d = oracle.decompose_randomized(x, L, k, p, Om[:, :k + p], q=2)
+    gs = gpu.SSA(x, L)
+    gs.decompose(k, oversampling=p, power_iters=2, omega=Om[:, :k + p])
+    g = [0, 1, 2]
+    R, nu2 = gs.lrf(g)
+    Rr, nu2r = oracle.compute_lrf(d, g, L)
+    assert abs(nu2 - nu2r) < 1e-5
+    assert rel_l2(R, Rr) < 1e-4
+    f = gs.forecast(g, 50)
+    fr = oracle.forecast(d, g, 50, N, L)
+    assert rel_l2(f, fr) < 1e-4
+    full = gs.forecast_full(g, 20)
+    assert rel_l2(full[:N], oracle.reconstruct(d, g, N, L)) <= REC_TOL
+    assert rel_l2(full[N:], fr[:20]) < 1e-4
+
+
+def test_reconstruct_edge_groups(gpu, oracle):
+    x, _, Om = oracle.config1(seed=0)
+    N, L, k, p = 1000, 250, 8, 4
+    d = oracle.decompose_randomized(x, L, k, p, Om[:, :k + p], q=1)
+    gs = gpu.SSA(x, L)
+    gs.decompose(k, oversampling=p, power_iters=1, omega=Om[:, :k + p])
+    # out-of-range indices are skipped (MKL/ssa_opt.h:2347-2348)
+    assert rel_l2(gs.reconstruct([0, 99, -3]), oracle.reconstruct(d, [0], N, L)) <= REC_TOL
+    assert np.all(gs.reconstruct([50]) == 0.0)
+    # full group = sum of all components
+    assert rel_l2(gs.reconstruct(list(range(k))), oracle.reconstruct(d, list(range(k)), N, L)) <= REC_TOL
+    # get_trend / get_noise
+    assert rel_l2(gs.get_trend(), oracle.reconstruct(d, [0], N, L)) <= REC_TOL
+    assert rel_l2(gs.get_noise(3), oracle.reconstruct(d, list(range(3, k)), N, L)) <= 1e-4
+    assert np.all(gs.get_noise(k) == 0.0)
+    with pytest.raises(RuntimeError):
+        gs.reconstruct([])
+    # cached spectra give the same values
+    a = gs.reconstruct([1, 2])
+    gs.cache_ffts()
+    assert np.array_equal(a, gs.reconstruct([1, 2]))
+
+
+def test_api_errors(gpu, oracle):
+    x = oracle.reference_test_signal(1000)
+    with pytest.raises(ValueError):
+        gpu.SSA(x[:3], 2)
+    with pytest.raises(ValueError):
+        gpu.SSA(x, 1)
+    with pytest.raises(ValueError):
+        gpu.SSA(x, 1000)
+    with pytest.raises(ValueError):
+        gpu.SSA(np.zeros(40000), 100)  # longer than one CTA's FFT (N <= 32768)
+    s = gpu.SSA(x, 250)
+    with pytest.raises(RuntimeError):
+        s.reconstruct([0])
+    with pytest.raises(RuntimeError):
+        s.decompose(60, oversampling=10)  # k + p > SSA_MAX_KP
+    s.decompose(5, oversampling=5)
+    with pytest.raises(RuntimeError):
+        s.forecast([0, 7], 5)  # out-of-range index in the LRF group (MKL/ssa_opt.h:2781-2785)
+    assert s.wcorr(0, 99) == 0.0
+    assert s.variance_explained(0, -1) == pytest.approx(1.0)
+
+
+def test_update_signal_and_repeat(gpu, oracle):
+    x, _, Om = oracle.config1(seed=0)
+    y, _, _ = oracle.config1(seed=5)
+    N, L, k, p = 1000, 250, 10, 6
+    s = gpu.SSA(x, L)
+    s.decompose(k, oversampling=p, power_iters=2, omega=Om[:, :k + p])
+    s.update_signal(y)
+    with pytest.raises(RuntimeError):
+        s.reconstruct([0])
+    s.decompose(k, oversampling=p, power_iters=2, omega=Om[:, :k + p])
+    d = oracle.decompose_randomized(y, L, k, p, Om[:, :k + p], q=2)
+    rel, gap = sigma_errors(s.singular_values, d.sigma)
+    assert np.all(rel[gap > 1e-3] <= SIG_TOL)
+
+
+def test_constant_signal(gpu):
+    # MKL/test/ssa_opt_test.c:1289-1322: rank-1 trajectory matrix.
+    x = np.full(300, 5.0)
+    s = gpu.SSA(x, 75)
+    s.decompose(5, oversampling=5)
+    sv = s.singular_values
+    assert sv[0] == pytest.approx(5.0 * np.sqrt(75 * 226), rel=1e-5)
+    assert np.all(sv[1:] < 1e-4 * sv[0])
+    assert np.max(np.abs(s.reconstruct([0]) - 5.0)) < 1e-4
+
+
+def test_batch_matches_single_and_oracle(gpu, oracle):
+    B, N, L, k, p, q = 6, 2000, 500, 20, 10, 2
+    X = oracle.config2_batch(B, seed=11, N=N)
+    b = gpu.SSABatch(B, N, L, k, oversampling=p, power_iters=q, groups=[[0], [1, 2]])
+    sig, W, G = b.run(X, seed=123)
+    # batch invariance: series 0 alone in the same engine gives the same bits as in the mix
+    sig0, W0, G0 = b.run(X[0:1], seed=123)
+    assert np.array_equal(sig0[0], sig[0])
+    assert np.array_equal(G0[0], G[0])
+    assert np.array_equal(W0[0], W[0])
+    for s_ in range(B):
+        Om = oracle.device_gaussian(oracle.series_seed(123, s_), N - L + 1, k + p)
+        d = oracle.decompose_randomized(X[s_], L, k, p, Om, q=q)
+        rel, gap = sigma_errors(sig[s_], d.sigma)
+        assert np.all(rel[gap > 1e-3] <= SIG_TOL), (s_, rel.max())
+        assert rel_l2(G[s_, 0], oracle.reconstruct(d, [0], N, L)) <= REC_TOL
+        assert rel_l2(G[s_, 1], oracle.reconstruct(d, [1, 2], N, L)) <= REC_TOL
+        assert np.max(np.abs(np.diag(W[s_]) - 1.0)) < 1e-6
+
+
+def test_kernel_launch_counter(gpu, oracle):
+    before = gpu.kernel_launches()
+    s = gpu.SSA(oracle.reference_test_signal(500), 125)
+    s.decompose(10)
+    s.reconstruct([0])
+    assert gpu.kernel_launches() > before
