@@ -560,6 +560,8 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_rr(const ssa_rr_job* __restri
     const int ne = (n + 1) & ~1;  // even count; index n is a dummy when n is odd
     for (int i = threadIdx.x; i < ne; i += blockDim.x) perm[i] = i;
     __syncthreads();
+    double gmax = 0.0;
+    for (int i = 0; i < n; ++i) gmax = fmax(gmax, fabs(G[i * SLD + i]));
     const int npairs = ne / 2;
     for (int sweep = 0; sweep < 40; ++sweep) {
         if (threadIdx.x == 0) notconv = 0;
@@ -577,7 +579,10 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_rr(const ssa_rr_job* __restri
                 if (q < n) {
                     const double apq = G[p * SLD + q];
                     const double app = G[p * SLD + p], aqq = G[q * SLD + q];
-                    if (fabs(apq) > 1e-300 && fabs(apq) > 1e-15 * sqrt(fabs(app * aqq))) {
+                    // Rotate unless the pair is already decoupled: relative to its own diagonal
+                    // (keeps small eigenvalues accurate) or below rounding of the largest one.
+                    if (fabs(apq) > 1e-300 && fabs(apq) > 1e-14 * sqrt(fabs(app * aqq)) &&
+                        fabs(apq) > 1e-16 * gmax) {
                         notconv = 1;
                         const double tau = (aqq - app) / (2.0 * apq);
                         const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));

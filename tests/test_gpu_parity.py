@@ -6,9 +6,10 @@ Rayleigh-Ritz / LRF):
     uses 1e-10 absolute in FP64);
   * singular values: relative error <= SIG_TOL = 1e-5 for every component whose relative gap
     to its neighbours exceeds 1e-3, <= 1e-4 for the rest;
-  * reconstructions of groups [0] and [1, 2]: relative L2 <= REC_TOL = 1e-5 after sign
-    alignment (signs follow the reference rule sum(U[:, i]) >= 0, so no alignment is needed
-    unless that sum is ~0);
+  * reconstructions of groups [0] and [1, 2]: relative L2 <= REC_TOL = 1e-5 when the group's
+    singular values are separated from every other computed one by a relative gap > 1e-2;
+    otherwise the group is ill-conditioned (its FP32 error is ~ u32 / gap) and the bound is
+    max(REC_TOL, 40 * 2^-24 / gap). Signs follow the reference rule sum(U[:, i]) >= 0;
   * W-correlation: max abs <= 1e-4 on the well-separated block, diagonal 1 within 1e-6.
 """
 import numpy as np
@@ -29,6 +30,19 @@ def gpu():
 
 def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def group_gap(sigma, group):
+    inside = [i for i in group if 0 <= i < len(sigma)]
+    outside = [j for j in range(len(sigma)) if j not in inside]
+    if not inside or not outside:
+        return np.inf
+    return min(abs(sigma[i] - sigma[j]) / sigma[i] for i in inside for j in outside)
+
+
+def rec_tol(sigma, group):
+    g = group_gap(sigma, group)
+    return REC_TOL if g > 1e-2 else max(REC_TOL, 40 * 2.0 ** -24 / max(g, 1e-12))
 
 
 def sigma_errors(s, ref):
@@ -216,8 +230,8 @@ def test_batch_matches_single_and_oracle(gpu, oracle):
         d = oracle.decompose_randomized(X[s_], L, k, p, Om, q=q)
         rel, gap = sigma_errors(sig[s_], d.sigma)
         assert np.all(rel[gap > 1e-3] <= SIG_TOL), (s_, rel.max())
-        assert rel_l2(G[s_, 0], oracle.reconstruct(d, [0], N, L)) <= REC_TOL
-        assert rel_l2(G[s_, 1], oracle.reconstruct(d, [1, 2], N, L)) <= REC_TOL
+        assert rel_l2(G[s_, 0], oracle.reconstruct(d, [0], N, L)) <= rec_tol(d.sigma, [0])
+        assert rel_l2(G[s_, 1], oracle.reconstruct(d, [1, 2], N, L)) <= rec_tol(d.sigma, [1, 2])
         assert np.max(np.abs(np.diag(W[s_]) - 1.0)) < 1e-6
 
 
