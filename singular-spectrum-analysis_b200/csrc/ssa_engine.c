@@ -374,7 +374,7 @@ static int chol(ssa_engine *e, int nb, int nch, int n)
     {
         ssa_chol_job *J = &jobs[s];
         J->part = e->part + (size_t)s * nchmax * np;
-        J->Rinv = e->Rinv + (size_t)s * e->kp * e->kp;
+        J->R = e->Rinv + (size_t)s * e->kp * e->kp;
         J->status = e->status + s;
         J->nchunks = nch;
         J->n = n;
@@ -392,7 +392,7 @@ static int chol(ssa_engine *e, int nb, int nch, int n)
 /* C_s = A_s * M_s for all series (M_s small, n x p, ld ldb, per-series stride mstride). */
 static int rowmul(ssa_engine *e, int nb, const float *A, size_t astride, long long lda, int m, int n,
                   const float *Mm, size_t mstride, int ldb, int p, float *C, size_t cstride, long long ldc,
-                  double *colsum)
+                  double *colsum, int trsm)
 {
     ssa_rowmul_job *jobs = (ssa_rowmul_job *)calloc((size_t)nb, sizeof(ssa_rowmul_job));
     if (!jobs)
@@ -411,6 +411,7 @@ static int rowmul(ssa_engine *e, int nb, const float *A, size_t astride, long lo
         J->n = n;
         J->p = p;
         J->ldb = ldb;
+        J->trsm = trsm;
     }
     void *d = ssae_push_jobs(e, jobs, sizeof(ssa_rowmul_job) * nb);
     free(jobs);
@@ -429,7 +430,7 @@ static int cholqr_pass(ssa_engine *e, int nb, float *A, size_t sstride, long lon
     const int nch = (m + rows - 1) / rows;
     CK(gram(e, nb, A, sstride, ld, m, n, rows, 0));
     CK(chol(e, nb, nch, n));
-    return rowmul(e, nb, A, sstride, ld, m, n, e->Rinv, (size_t)e->kp * e->kp, n, n, A, sstride, ld, colsum);
+    return rowmul(e, nb, A, sstride, ld, m, n, e->Rinv, (size_t)e->kp * e->kp, n, n, A, sstride, ld, colsum, 1);
 }
 
 int ssae_decompose(ssa_engine *e, int nb, int kp, int k, int q, const float *d_omega, long long omega_ld,
@@ -489,8 +490,8 @@ int ssae_decompose(ssa_engine *e, int nb, int kp, int k, int q, const float *d_o
         CK(rc_);
     }
     /* U = Q Zu (in place over Y), V = B Zv (in place over Z) */
-    CK(rowmul(e, nb, e->Y, sY, e->ldL, L, kp, e->Zu, (size_t)e->kp * e->k, kp, k, e->Y, sY, e->ldL, NULL));
-    CK(rowmul(e, nb, e->Z, sZ, e->ldK, K, kp, e->Zv, (size_t)e->kp * e->k, kp, k, e->Z, sZ, e->ldK, NULL));
+    CK(rowmul(e, nb, e->Y, sY, e->ldL, L, kp, e->Zu, (size_t)e->kp * e->k, kp, k, e->Y, sY, e->ldL, NULL, 0));
+    CK(rowmul(e, nb, e->Z, sZ, e->ldK, K, kp, e->Zv, (size_t)e->kp * e->k, kp, k, e->Z, sZ, e->ldK, NULL, 0));
     return 0;
 }
 

@@ -46,10 +46,35 @@ __device__ __forceinline__ float2 mul_mi(float2 a) {
     return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
 }
 
-// exp(-+2 pi i t / TW_N) for t in [0, TW_N)
-template <bool INV>
-__device__ __forceinline__ float2 twiddle(int t) {
-    float2 w = g_tw[t];
+// Two-level twiddle table in shared memory for resolution M = 2^LOGM:
+//   W_M^t = hi[t >> LO] * lo[t & (2^LO - 1)],  lo[j] = W_M^j,  hi[i] = W_M^(i 2^LO).
+// Each factor is a correctly rounded FP32 value from the FP64-computed global table, so a
+// twiddle costs two shared loads and one complex multiply (~1 ulp extra error).
+template <int LOGM>
+struct TwSplit {
+    static constexpr int LO = (LOGM + 1) / 2;
+    static constexpr int HI = LOGM - LO;
+    static constexpr int NLO = 1 << LO;
+    static constexpr int NHI = 1 << HI;
+    static constexpr int N = NLO + NHI;  // float2 entries
+};
+
+// Fill the table (lo first, then hi); caller syncs before use.
+template <int LOGM>
+__device__ __forceinline__ void load_twiddles(float2* tab) {
+    using S = TwSplit<LOGM>;
+    static_assert(LOGM <= SSA_TW_LOG, "twiddle resolution exceeds the global table");
+    for (int i = threadIdx.x; i < S::N; i += blockDim.x) {
+        const int t = i < S::NLO ? i : (i - S::NLO) << S::LO;
+        tab[i] = g_tw[t << (SSA_TW_LOG - LOGM)];
+    }
+}
+
+// W_M^t (forward sign) or its conjugate, t in [0, M)
+template <int LOGM, bool INV>
+__device__ __forceinline__ float2 twiddle(const float2* tab, int t) {
+    using S = TwSplit<LOGM>;
+    float2 w = cmul(tab[S::NLO + (t >> S::LO)], tab[t & (S::NLO - 1)]);
     if (INV) w.y = -w.y;
     return w;
 }
@@ -160,7 +185,7 @@ struct FftShape {
 
 // One Stockham pass of radix 2^RLOG after 2^LOGNS points have been combined.
 template <int RLOG, int LOGNS, int LOGH, bool INV>
-__device__ __forceinline__ void fft_pass(float2* s, int tid) {
+__device__ __forceinline__ void fft_pass(float2* s, const float2* tw, int tid) {
     constexpr int R = 1 << RLOG;
     constexpr int H = 1 << LOGH;
     constexpr int T = H / 16;
@@ -184,10 +209,10 @@ __device__ __forceinline__ void fft_pass(float2* s, int tid) {
             const int j = tid + b * T;
             const int k = j & (NS - 1);
             if constexpr (LOGNS > 0) {
-                // W_{NS R}^{r k} = table index (r k) << (TW_LOG - LOGNS - RLOG)
-                constexpr int SH = SSA_TW_LOG - LOGNS - RLOG;
+                // W_{NS R}^{r k} = W_M^{(r k) << (LOGM - LOGNS - RLOG)}, M = 2H
+                constexpr int SH = LOGH + 1 - LOGNS - RLOG;
 #pragma unroll
-                for (int r = 1; r < R; ++r) a[b * R + r] = cmul(a[b * R + r], twiddle<INV>((r * k) << SH));
+                for (int r = 1; r < R; ++r) a[b * R + r] = cmul(a[b * R + r], twiddle<LOGH + 1, INV>(tw, (r * k) << SH));
             }
             dftR<R, INV>(a + b * R);
             const int base = (j - k) * R + k;
@@ -199,20 +224,21 @@ __device__ __forceinline__ void fft_pass(float2* s, int tid) {
 }
 
 template <int LOGH, bool INV, int LOGNS>
-__device__ __forceinline__ void fft_passes(float2* s, int tid) {
+__device__ __forceinline__ void fft_passes(float2* s, const float2* tw, int tid) {
     if constexpr (LOGNS + 4 <= LOGH) {
-        fft_pass<4, LOGNS, LOGH, INV>(s, tid);
-        fft_passes<LOGH, INV, LOGNS + 4>(s, tid);
+        fft_pass<4, LOGNS, LOGH, INV>(s, tw, tid);
+        fft_passes<LOGH, INV, LOGNS + 4>(s, tw, tid);
     } else if constexpr (LOGNS < LOGH) {
-        fft_pass<LOGH - LOGNS, LOGNS, LOGH, INV>(s, tid);
+        fft_pass<LOGH - LOGNS, LOGNS, LOGH, INV>(s, tw, tid);
     }
 }
 
-// In-place H-point complex FFT (unnormalised) of the padded shared buffer s. Must be called
-// by every thread of the CTA; the caller syncs before (data in s) and may read s after.
+// In-place H-point complex FFT (unnormalised) of the padded shared buffer s, with the twiddle
+// table of resolution M = 2H in tw (load_twiddles<LOGH + 1>). Must be called by every thread
+// of the CTA; the caller syncs before (data and table in shared memory) and may read s after.
 template <int LOGH, bool INV>
-__device__ __forceinline__ void fft_block(float2* s) {
-    fft_passes<LOGH, INV, 0>(s, threadIdx.x);
+__device__ __forceinline__ void fft_block(float2* s, const float2* tw) {
+    fft_passes<LOGH, INV, 0>(s, tw, threadIdx.x);
 }
 
 // Load a real sequence a[0..n) (zero beyond n, up to M = 2H) into s as z[n] = a[2n] + i a[2n+1],
@@ -275,8 +301,14 @@ __device__ __forceinline__ void pack_pair(float2 pk, float2 pm, float2 wk, float
 
 // W_M^k for M = 2^(LOGH+1)
 template <int LOGH>
-__device__ __forceinline__ float2 wm(int k) {
-    return g_tw[k << (SSA_TW_LOG - LOGH - 1)];
+__device__ __forceinline__ float2 wm(const float2* tw, int k) {
+    return twiddle<LOGH + 1, false>(tw, k);
+}
+
+// Shared-memory floats2 needed for `bufs` transform buffers plus the twiddle table.
+template <int LOGH>
+__host__ __device__ constexpr int fft_smem_f2(int bufs) {
+    return bufs * spad_size(1 << LOGH) + TwSplit<LOGH + 1>::N;
 }
 
 }  // namespace ssa

@@ -136,9 +136,11 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_spectrum(const ssa_co
     const ssa_col_job J = jobs[blockIdx.y];
     const int c = blockIdx.x;
     if (c >= J.ncols) return;
+    float2* tw = smem + spad_size(H);
+    load_twiddles<LOGH + 1>(tw);
     load_column<LOGH>(smem, J, c);
     __syncthreads();
-    fft_block<LOGH, false>(smem);
+    fft_block<LOGH, false>(smem, tw);
     float2* out = reinterpret_cast<float2*>(J.spec + (long long)c * J.ld_spec);
     for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
         if (k == 0) {
@@ -147,7 +149,7 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_spectrum(const ssa_co
             out[H] = make_float2(z0.x - z0.y, 0.f);
         } else {
             float2 ak, am;
-            unpack_pair<LOGH>(smem[spad(k)], smem[spad(H - k)], wm<LOGH>(k), ak, am);
+            unpack_pair<LOGH>(smem[spad(k)], smem[spad(H - k)], wm<LOGH>(tw, k), ak, am);
             out[k] = ak;
             out[H - k] = am;
         }
@@ -161,9 +163,11 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_corr(const ssa_col_jo
     const ssa_col_job J = jobs[blockIdx.y];
     const int c = blockIdx.x;
     if (c >= J.ncols) return;
+    float2* tw = smem + spad_size(H);
+    load_twiddles<LOGH + 1>(tw);
     load_column<LOGH>(smem, J, c);
     __syncthreads();
-    fft_block<LOGH, false>(smem);
+    fft_block<LOGH, false>(smem, tw);
     const float2* X = reinterpret_cast<const float2*>(J.X);
     for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
         float2 zk, zm;
@@ -174,7 +178,7 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_corr(const ssa_col_jo
             pack_pair(p0, ph, make_float2(1.f, 0.f), zk, zm);
             smem[spad(0)] = zk;
         } else {
-            const float2 w = wm<LOGH>(k);
+            const float2 w = wm<LOGH>(tw, k);
             float2 ak, am;
             unpack_pair<LOGH>(smem[spad(k)], smem[spad(H - k)], w, ak, am);
             const float2 pk = cmulc(X[k], ak);
@@ -185,7 +189,7 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_corr(const ssa_col_jo
         }
     }
     __syncthreads();
-    fft_block<LOGH, true>(smem);
+    fft_block<LOGH, true>(smem, tw);
     store_real<LOGH>(smem, J.out + (long long)c * J.ld_out, J.n_out, 1.0f / (float)H);
 }
 
@@ -198,15 +202,17 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_elem_recon(const ssa_
     __shared__ double red[32];
     float2* s1 = smem;
     float2* s2 = smem + spad_size(H);
+    float2* tw = smem + 2 * spad_size(H);
     const ssa_col_job J = jobs[blockIdx.y];
     const int c = blockIdx.x;
     if (c >= J.ncols) return;
     const float sc = J.scale ? (float)J.scale[c] : 1.0f;
+    load_twiddles<LOGH + 1>(tw);
     load_real<LOGH>(s1, J.in + (long long)c * J.ld_in, J.n_in, sc);
     load_real<LOGH>(s2, J.in2 + (long long)c * J.ld_in2, J.n_in2, 1.0f);
     __syncthreads();
-    fft_block<LOGH, false>(s1);
-    fft_block<LOGH, false>(s2);
+    fft_block<LOGH, false>(s1, tw);
+    fft_block<LOGH, false>(s2, tw);
     for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
         float2 zk, zm;
         if (k == 0) {
@@ -216,7 +222,7 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_elem_recon(const ssa_
             pack_pair(make_float2(p0, 0.f), make_float2(ph, 0.f), make_float2(1.f, 0.f), zk, zm);
             s1[spad(0)] = zk;
         } else {
-            const float2 w = wm<LOGH>(k);
+            const float2 w = wm<LOGH>(tw, k);
             float2 ak, am, bk, bm;
             unpack_pair<LOGH>(s1[spad(k)], s1[spad(H - k)], w, ak, am);
             unpack_pair<LOGH>(s2[spad(k)], s2[spad(H - k)], w, bk, bm);
@@ -226,7 +232,7 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_elem_recon(const ssa_
         }
     }
     __syncthreads();
-    fft_block<LOGH, true>(s1);
+    fft_block<LOGH, true>(s1, tw);
     float* out = J.out + (long long)c * J.ld_out;
     const float inv_h = 1.0f / (float)H;
     double acc = 0.0;
@@ -248,6 +254,9 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_recon(const ssa_recon
     constexpr int H = 1 << LOGH;
     extern __shared__ float2 smem[];
     const ssa_recon_job J = jobs[blockIdx.y];
+    float2* tw = smem + spad_size(H);
+    load_twiddles<LOGH + 1>(tw);
+    __syncthreads();
     for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
         float2 pk = make_float2(0.f, 0.f), pm = make_float2(0.f, 0.f);
         for (int g = 0; g < J.n_group; ++g) {
@@ -265,13 +274,13 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_recon(const ssa_recon
             pack_pair(pk, pm, make_float2(1.f, 0.f), zk, zm);
             smem[spad(0)] = zk;
         } else {
-            pack_pair(pk, pm, wm<LOGH>(k), zk, zm);
+            pack_pair(pk, pm, wm<LOGH>(tw, k), zk, zm);
             smem[spad(k)] = zk;
             smem[spad(H - k)] = zm;
         }
     }
     __syncthreads();
-    fft_block<LOGH, true>(smem);
+    fft_block<LOGH, true>(smem, tw);
     const float inv_h = 1.0f / (float)H;
     for (int t = threadIdx.x; t < J.N; t += blockDim.x) {
         const float2 z = smem[spad(t >> 1)];
@@ -391,36 +400,25 @@ __global__ void __launch_bounds__(GRAM_THREADS) k_gram(const ssa_gram_job* __res
 
 #define SMALL_THREADS 256
 #define SLD (SSA_MAX_KP + 1)
+#define SMALL_SMEM (2 * SSA_MAX_KP * SLD * (int)sizeof(double))
 
+// Sum the packed-upper Gram partials into the symmetric column-major matrix G (ld SLD).
 __device__ void reduce_packed(const double* __restrict__ part, int nchunks, int n, double* G) {
     const int np = n * (n + 1) / 2;
-    for (int e = threadIdx.x; e < np; e += blockDim.x) {
-        // invert pk_index
-        int i = 0, rem = e;
-        while (rem >= n - i) {
-            rem -= n - i;
-            ++i;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int i = warp; i < n; i += nw) {
+        const int base = i * n - (i * (i - 1)) / 2 - i;  // pk_index(i, j, n) = base + j
+        for (int j = i + lane; j < n; j += 32) {
+            double s = 0.0;
+            for (int c = 0; c < nchunks; ++c) s += part[(long long)c * np + base + j];
+            G[j * SLD + i] = s;
+            G[i * SLD + j] = s;
         }
-        const int j = i + rem;
-        double s = 0.0;
-        for (int c = 0; c < nchunks; ++c) s += part[(long long)c * np + e];
-        G[i * SLD + j] = s;
-        G[j * SLD + i] = s;
     }
 }
 
-#define SMALL_SMEM (2 * SSA_MAX_KP * SLD * (int)sizeof(double))
-
-__global__ void __launch_bounds__(SMALL_THREADS) k_chol(const ssa_chol_job* __restrict__ jobs) {
-    extern __shared__ double dsm[];
-    double* G = dsm;
-    double* Rm = dsm + SSA_MAX_KP * SLD;
-    __shared__ double red[32];
-    __shared__ double dmax_s;
-    const ssa_chol_job J = jobs[blockIdx.x];
-    const int n = J.n;
-    reduce_packed(J.part, J.nchunks, n, G);
-    __syncthreads();
+// Largest diagonal entry (>= 0) of G, or -1 when a diagonal entry is not finite.
+__device__ double diag_max(const double* G, int n, double* red) {
     double dm = 0.0;
     int bad = 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -428,58 +426,67 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_chol(const ssa_chol_job* __re
         if (!isfinite(d)) bad = 1;
         dm = fmax(dm, d);
     }
-    // max-reduce via warp shuffles on (dm, bad)
     for (int o = 16; o > 0; o >>= 1) {
         dm = fmax(dm, __shfl_down_sync(0xffffffffu, dm, o));
         bad |= __shfl_down_sync(0xffffffffu, bad, o);
     }
+    __syncthreads();
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = bad ? -1.0 : dm;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double m = 0.0;
-        int b = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-            if (red[w] < 0.0) b = 1;
-            m = fmax(m, red[w]);
-        }
-        dmax_s = b ? -1.0 : m;
-        if (b && J.status) atomicOr(J.status, 1);
+    double m = 0.0;
+    int b = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        if (red[w] < 0.0) b = 1;
+        m = fmax(m, red[w]);
     }
     __syncthreads();
-    const double dmax = dmax_s;
-    // Pivot floor: directions below this are treated as rounding noise (rank-deficient input).
-    const double floor_ = dmax > 0.0 ? dmax * 1e-13 * (double)n : 1.0;
-    for (int e = threadIdx.x; e < n * SLD; e += blockDim.x) Rm[e] = 0.0;
-    __syncthreads();
-    // Right-looking Cholesky: G = R^T R, R upper (row j of R in Rm[j][:]).
+    return b ? -1.0 : m;
+}
+
+// In-place Cholesky G = R^T R of the symmetric column-major G (ld SLD): on return G holds R
+// (upper, R[r][c] at G[c * SLD + r]) with zeros below the diagonal. Pivots below `floor_` are
+// raised to it: directions that small are rounding noise of a rank-deficient input.
+__device__ void chol_upper_inplace(double* G, int n, double floor_) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (int j = 0; j < n; ++j) {
-        if (threadIdx.x == 0) {
-            double d = G[j * SLD + j];
-            if (!(d > floor_)) d = floor_;
-            Rm[j * SLD + j] = sqrt(d);
-        }
+        // every thread reads the pivot before anyone overwrites it
+        double d = G[j * SLD + j];
+        if (!(d > floor_)) d = floor_;
+        d = sqrt(d);
+        const double inv = 1.0 / d;
         __syncthreads();
-        const double djj = Rm[j * SLD + j];
-        for (int c = j + 1 + threadIdx.x; c < n; c += blockDim.x) Rm[j * SLD + c] = G[j * SLD + c] / djj;
+        if (threadIdx.x == 0) G[j * SLD + j] = d;
+        for (int c = j + 1 + threadIdx.x; c < n; c += blockDim.x) G[c * SLD + j] *= inv;
         __syncthreads();
-        const int m = n - j - 1;
-        for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
-            const int r = j + 1 + e / m, c = j + 1 + e % m;
-            if (r <= c) G[r * SLD + c] -= Rm[j * SLD + r] * Rm[j * SLD + c];
+        // trailing update of the upper triangle: rows r > j (one warp per row), columns c >= r
+        for (int r = j + 1 + warp; r < n; r += nw) {
+            const double rjr = G[r * SLD + j];
+            for (int c = r + lane; c < n; c += 32) G[c * SLD + r] -= rjr * G[c * SLD + j];
         }
         __syncthreads();
     }
-    // Inverse of the upper-triangular R, one column per thread (back substitution).
-    float* Ri = J.Rinv;
-    for (int c = threadIdx.x; c < n; c += blockDim.x) {
-        double x[SSA_MAX_KP];
-#pragma unroll 1
-        for (int i = c; i >= 0; --i) {
-            double s = (i == c) ? 1.0 : 0.0;
-            for (int l = i + 1; l <= c; ++l) s -= Rm[i * SLD + l] * x[l];
-            x[i] = s / Rm[i * SLD + i];
-        }
-        for (int i = 0; i < n; ++i) Ri[i + c * n] = i <= c ? (float)x[i] : 0.f;
+    for (int c = warp; c < n; c += nw)
+        for (int r = c + 1 + lane; r < n; r += 32) G[c * SLD + r] = 0.0;
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(SMALL_THREADS) k_chol(const ssa_chol_job* __restrict__ jobs) {
+    extern __shared__ double dsm[];
+    __shared__ double red[32];
+    double* G = dsm;
+    const ssa_chol_job J = jobs[blockIdx.x];
+    const int n = J.n;
+    reduce_packed(J.part, J.nchunks, n, G);
+    __syncthreads();
+    const double dmax = diag_max(G, n, red);
+    if (dmax < 0.0) {
+        if (threadIdx.x == 0 && J.status) atomicOr(J.status, 1);
+    }
+    const double floor_ = dmax > 0.0 ? dmax * 1e-13 * (double)n : 1.0;
+    chol_upper_inplace(G, n, floor_);
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int c = e / n, r = e - c * n;
+        J.R[e] = (float)G[c * SLD + r];
     }
 }
 
@@ -491,14 +498,17 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_chol(const ssa_chol_job* __re
 
 __global__ void __launch_bounds__(ROWMUL_THREADS) k_rowmul(const ssa_rowmul_job* __restrict__ jobs) {
     __shared__ float sB[SSA_MAX_KP * SSA_MAX_KP];
+    __shared__ float sInv[SSA_MAX_KP];
     __shared__ double wsum[ROWMUL_THREADS / 32][SSA_MAX_KP];
     const ssa_rowmul_job J = jobs[blockIdx.y];
     const int n = J.n, p = J.p;
     if (blockIdx.x * ROWMUL_THREADS >= J.m) return;
     for (int e = threadIdx.x; e < SSA_MAX_KP * p; e += blockDim.x) {
-        const int l = e % SSA_MAX_KP, j = e / SSA_MAX_KP;
+        const int j = e / SSA_MAX_KP, l = e - j * SSA_MAX_KP;
         sB[e] = l < n ? J.Bm[l + j * J.ldb] : 0.f;
     }
+    if (J.trsm)
+        for (int j = threadIdx.x; j < SSA_MAX_KP; j += blockDim.x) sInv[j] = j < n ? 1.0f / J.Bm[j + j * J.ldb] : 0.f;
     __syncthreads();
     const int i = blockIdx.x * ROWMUL_THREADS + threadIdx.x;
     const bool live = i < J.m;
@@ -507,21 +517,46 @@ __global__ void __launch_bounds__(ROWMUL_THREADS) k_rowmul(const ssa_rowmul_job*
     for (int l = 0; l < SSA_MAX_KP; ++l)
         a[l] = (live && l < n) ? J.A[(long long)i + (long long)l * J.lda] : 0.f;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int j = 0; j < p; ++j) {
-        const float* b = sB + j * SSA_MAX_KP;
-        float s0 = 0.f, s1 = 0.f;
+    if (J.trsm) {
+        // x R = a, R upper: x_j = (a_j - sum_{l<j} x_l R[l][j]) / R[j][j]; a is overwritten by x
 #pragma unroll
-        for (int l = 0; l < SSA_MAX_KP; l += 2) {
-            s0 = fmaf(a[l], b[l], s0);
-            s1 = fmaf(a[l + 1], b[l + 1], s1);
+        for (int j = 0; j < SSA_MAX_KP; ++j) {
+            if (j < n) {
+                const float* b = sB + j * SSA_MAX_KP;
+                float s0 = a[j], s1 = 0.f;
+#pragma unroll
+                for (int l = 0; l < j; l += 2) {
+                    s0 = fmaf(-a[l], b[l], s0);
+                    if (l + 1 < j) s1 = fmaf(-a[l + 1], b[l + 1], s1);
+                }
+                const float c = (s0 + s1) * sInv[j];
+                a[j] = c;
+                if (live) J.C[(long long)i + (long long)j * J.ldc] = c;
+                if (J.colsum) {
+                    double v = live ? (double)c : 0.0;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                    if (lane == 0) wsum[warp][j] = v;
+                }
+            }
         }
-        const float c = s0 + s1;
-        if (live) J.C[(long long)i + (long long)j * J.ldc] = c;
-        if (J.colsum) {
-            double v = live ? (double)c : 0.0;
+    } else {
+        for (int j = 0; j < p; ++j) {
+            const float* b = sB + j * SSA_MAX_KP;
+            float s0 = 0.f, s1 = 0.f;
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-            if (lane == 0) wsum[warp][j] = v;
+            for (int l = 0; l < SSA_MAX_KP; l += 2) {
+                s0 = fmaf(a[l], b[l], s0);
+                s1 = fmaf(a[l + 1], b[l + 1], s1);
+            }
+            const float c = s0 + s1;
+            if (live) J.C[(long long)i + (long long)j * J.ldc] = c;
+            if (J.colsum) {
+                double v = live ? (double)c : 0.0;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                if (lane == 0) wsum[warp][j] = v;
+            }
         }
     }
     if (J.colsum) {
@@ -538,20 +573,27 @@ __global__ void __launch_bounds__(ROWMUL_THREADS) k_rowmul(const ssa_rowmul_job*
 // Rayleigh-Ritz: FP64 parallel cyclic Jacobi on G_B = B^T B
 // ---------------------------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(SMALL_THREADS) k_rr(const ssa_rr_job* __restrict__ jobs) {
+#define RR_THREADS 512
+
+// Rayleigh-Ritz: B^T B = R^T R (FP64 Cholesky), then one-sided (Hestenes) Jacobi on the
+// columns of R: R Z = W Sigma with orthonormal Z, so B^T B = Z Sigma^2 Z^T. One warp per column
+// pair of a round-robin step; each lane owns rows lane and lane + 32.
+__global__ void __launch_bounds__(RR_THREADS) k_rr(const ssa_rr_job* __restrict__ jobs) {
     extern __shared__ double dsm[];
-    double* G = dsm;
+    double* A = dsm;                    // column c at A + c * SLD
     double* Z = dsm + SSA_MAX_KP * SLD;
-    __shared__ double rc[SSA_MAX_KP / 2], rs[SSA_MAX_KP / 2];
-    __shared__ int pp[SSA_MAX_KP / 2], pq[SSA_MAX_KP / 2];
     __shared__ int perm[SSA_MAX_KP + 1];
     __shared__ double qs[SSA_MAX_KP];
+    __shared__ double nrm[SSA_MAX_KP];
     __shared__ int order[SSA_MAX_KP];
+    __shared__ double red[32];
     __shared__ int notconv;
     const ssa_rr_job J = jobs[blockIdx.x];
     const int n = J.kp;
-    reduce_packed(J.part, J.nchunks, n, G);
-    for (int e = threadIdx.x; e < n * SLD; e += blockDim.x) Z[e] = ((e % SLD) == (e / SLD)) ? 1.0 : 0.0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    reduce_packed(J.part, J.nchunks, n, A);
+    for (int c = warp; c < n; c += nw)
+        for (int r = lane; r < n; r += 32) Z[c * SLD + r] = (r == c) ? 1.0 : 0.0;
     for (int l = threadIdx.x; l < n; l += blockDim.x) {
         double s = 0.0;
         for (int c = 0; c < J.nchunks_q; ++c) s += J.qsum[(long long)c * n + l];
@@ -560,69 +602,55 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_rr(const ssa_rr_job* __restri
     const int ne = (n + 1) & ~1;  // even count; index n is a dummy when n is odd
     for (int i = threadIdx.x; i < ne; i += blockDim.x) perm[i] = i;
     __syncthreads();
-    double gmax = 0.0;
-    for (int i = 0; i < n; ++i) gmax = fmax(gmax, fabs(G[i * SLD + i]));
+    const double dmax = diag_max(A, n, red);
+    if (dmax < 0.0) {
+        if (threadIdx.x == 0 && J.status) atomicOr(J.status, 2);
+    }
+    chol_upper_inplace(A, n, dmax > 0.0 ? dmax * 1e-15 : 1.0);
     const int npairs = ne / 2;
+    const double tiny = 1e-300;
     for (int sweep = 0; sweep < 40; ++sweep) {
         if (threadIdx.x == 0) notconv = 0;
         __syncthreads();
         for (int step = 0; step < ne - 1; ++step) {
-            // rotations for this step
-            for (int t = threadIdx.x; t < npairs; t += blockDim.x) {
+            for (int t = warp; t < npairs; t += nw) {
                 int p = perm[t], q = perm[ne - 1 - t];
-                if (p > q) {
-                    const int tmp = p;
-                    p = q;
-                    q = tmp;
+                if (q >= n || p >= n) continue;
+                double* ap = A + p * SLD;
+                double* aq = A + q * SLD;
+                double al = 0.0, be = 0.0, ga = 0.0;
+                for (int r = lane; r < n; r += 32) {
+                    const double x = ap[r], y = aq[r];
+                    al = fma(x, x, al);
+                    be = fma(y, y, be);
+                    ga = fma(x, y, ga);
                 }
-                double c = 1.0, s = 0.0;
-                if (q < n) {
-                    const double apq = G[p * SLD + q];
-                    const double app = G[p * SLD + p], aqq = G[q * SLD + q];
-                    // Rotate unless the pair is already decoupled: relative to its own diagonal
-                    // (keeps small eigenvalues accurate) or below rounding of the largest one.
-                    if (fabs(apq) > 1e-300 && fabs(apq) > 1e-14 * sqrt(fabs(app * aqq)) &&
-                        fabs(apq) > 1e-16 * gmax) {
-                        notconv = 1;
-                        const double tau = (aqq - app) / (2.0 * apq);
-                        const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                        c = 1.0 / sqrt(1.0 + tt * tt);
-                        s = tt * c;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    al += __shfl_xor_sync(0xffffffffu, al, o);
+                    be += __shfl_xor_sync(0xffffffffu, be, o);
+                    ga += __shfl_xor_sync(0xffffffffu, ga, o);
+                }
+                if (fabs(ga) > tiny && fabs(ga) > 1e-15 * sqrt(al * be)) {
+                    if (lane == 0) notconv = 1;
+                    const double zeta = (be - al) / (2.0 * ga);
+                    const double tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                    const double cs = 1.0 / sqrt(1.0 + tt * tt);
+                    const double sn = cs * tt;
+                    double* zp = Z + p * SLD;
+                    double* zq = Z + q * SLD;
+                    for (int r = lane; r < n; r += 32) {
+                        const double x = ap[r], y = aq[r];
+                        ap[r] = cs * x - sn * y;
+                        aq[r] = sn * x + cs * y;
+                        const double u = zp[r], v = zq[r];
+                        zp[r] = cs * u - sn * v;
+                        zq[r] = sn * u + cs * v;
                     }
                 }
-                pp[t] = p;
-                pq[t] = q;
-                rc[t] = c;
-                rs[t] = s;
             }
             __syncthreads();
-            // G <- G J and Z <- Z J (columns p, q)
-            for (int e = threadIdx.x; e < npairs * n; e += blockDim.x) {
-                const int t = e / n, r = e % n;
-                const int p = pp[t], q = pq[t];
-                if (q >= n || rs[t] == 0.0) continue;
-                const double c = rc[t], s = rs[t];
-                const double gp = G[r * SLD + p], gq = G[r * SLD + q];
-                G[r * SLD + p] = c * gp - s * gq;
-                G[r * SLD + q] = s * gp + c * gq;
-                const double zp = Z[r * SLD + p], zq = Z[r * SLD + q];
-                Z[r * SLD + p] = c * zp - s * zq;
-                Z[r * SLD + q] = s * zp + c * zq;
-            }
-            __syncthreads();
-            // G <- J^T G (rows p, q)
-            for (int e = threadIdx.x; e < npairs * n; e += blockDim.x) {
-                const int t = e / n, r = e % n;
-                const int p = pp[t], q = pq[t];
-                if (q >= n || rs[t] == 0.0) continue;
-                const double c = rc[t], s = rs[t];
-                const double gp = G[p * SLD + r], gq = G[q * SLD + r];
-                G[p * SLD + r] = c * gp - s * gq;
-                G[q * SLD + r] = s * gp + c * gq;
-            }
-            __syncthreads();
-            // round-robin: keep perm[0], rotate perm[1..ne-1]
-            if (threadIdx.x == 0) {
+            if (threadIdx.x == 0) {  // round-robin: keep perm[0], rotate perm[1..ne-1]
                 const int last = perm[ne - 1];
                 for (int i = ne - 1; i > 1; --i) perm[i] = perm[i - 1];
                 perm[1] = last;
@@ -630,14 +658,22 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_rr(const ssa_rr_job* __restri
             __syncthreads();
         }
         if (!notconv) break;
-        __syncthreads();
     }
+    // sigma_c = ||A[:, c]||
+    for (int c = warp; c < n; c += nw) {
+        double s = 0.0;
+        for (int r = lane; r < n; r += 32) s = fma(A[c * SLD + r], A[c * SLD + r], s);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) nrm[c] = sqrt(s);
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
         for (int i = 0; i < n; ++i) order[i] = i;
-        for (int i = 0; i < n; ++i) {  // selection sort, descending eigenvalue
+        for (int i = 0; i < n; ++i) {  // selection sort, descending singular value
             int best = i;
             for (int j = i + 1; j < n; ++j)
-                if (G[order[j] * SLD + order[j]] > G[order[best] * SLD + order[best]]) best = j;
+                if (nrm[order[j]] > nrm[order[best]]) best = j;
             const int tmp = order[i];
             order[i] = order[best];
             order[best] = tmp;
@@ -645,21 +681,24 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_rr(const ssa_rr_job* __restri
     }
     __syncthreads();
     const int k = J.k;
-    for (int j = threadIdx.x; j < k; j += blockDim.x) {
+    for (int j = warp; j < k; j += nw) {
         const int col = order[j];
-        const double lam = G[col * SLD + col];
-        const double sg = sqrt(fmax(lam, 0.0));
+        const double sg = nrm[col];
         double dot = 0.0;
-        for (int l = 0; l < n; ++l) dot += qs[l] * Z[l * SLD + col];
+        for (int l = lane; l < n; l += 32) dot = fma(qs[l], Z[col * SLD + l], dot);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
         const double sgn = dot < 0.0 ? -1.0 : 1.0;
-        const double isg = sg > 1e-300 ? 1.0 / sg : 0.0;
-        for (int l = 0; l < n; ++l) {
-            const double z = sgn * Z[l * SLD + col];
+        const double isg = sg > tiny ? 1.0 / sg : 0.0;
+        for (int l = lane; l < n; l += 32) {
+            const double z = sgn * Z[col * SLD + l];
             J.Zu[l + j * n] = (float)z;
             J.Zv[l + j * n] = (float)(z * isg);
         }
-        J.sigma[j] = sg;
-        if (!isfinite(sg) && J.status) atomicOr(J.status, 2);
+        if (lane == 0) {
+            J.sigma[j] = sg;
+            if (!isfinite(sg) && J.status) atomicOr(J.status, 2);
+        }
     }
 }
 
@@ -776,7 +815,7 @@ extern "C" int ssad_init_device(void) {
 }
 
 template <int LOGH>
-static int smem_bytes(int bufs) { return bufs * spad_size(1 << LOGH) * (int)sizeof(float2); }
+static int smem_bytes(int bufs) { return fft_smem_f2<LOGH>(bufs) * (int)sizeof(float2); }
 
 template <typename KernelT>
 static cudaError_t set_smem(KernelT kern, int bytes) {
@@ -893,7 +932,7 @@ extern "C" int ssad_rr(const ssa_rr_job* d_jobs, int njobs, void* stream) {
     if (njobs <= 0) return 0;
     cudaError_t e = set_smem(k_rr, SMALL_SMEM);
     if (e != cudaSuccess) return (int)e;
-    k_rr<<<njobs, SMALL_THREADS, SMALL_SMEM, (cudaStream_t)stream>>>(d_jobs);
+    k_rr<<<njobs, RR_THREADS, SMALL_SMEM, (cudaStream_t)stream>>>(d_jobs);
     return launched(cudaGetLastError());
 }
 

@@ -58,18 +58,21 @@ typedef struct
     int N, L, K;
 } ssa_gram_job;
 
-/* Cholesky job: G = sum of the partials; G = R^T R; Rinv = R^{-1} (fp32, n x n col-major). */
+/* Cholesky job: G = sum of the partials; G = R^T R with R upper triangular, written as fp32
+ * n x n column-major (R[r][c] at R[r + c n], zeros below the diagonal). */
 typedef struct
 {
     const double *part;
-    float *Rinv;
+    float *R;
     int *status;          /* set to a nonzero code on failure (non-finite Gram) */
     int nchunks, n;
     int pad_[2];
 } ssa_chol_job;
 
-/* C[:, 0:p] = A[:, 0:n] * Bm[0:n, 0:p] row by row (in place allowed when C == A, p <= n and
- * Bm is upper triangular or row i of C depends only on row i of A). */
+/* Row-by-row products with a small matrix (in place allowed: C == A, since every thread reads
+ * its whole row of A before writing its row of C):
+ *   trsm == 0: C[:, 0:p] = A[:, 0:n] * Bm[0:n, 0:p];
+ *   trsm == 1: C = A * Bm^{-1} for upper-triangular Bm (p == n), by forward substitution. */
 typedef struct
 {
     const float *A;
@@ -78,6 +81,8 @@ typedef struct
     double *colsum;       /* optional: per-CTA partial column sums of C, [blockIdx.x][p] */
     long long lda, ldc;
     int m, n, p, ldb;
+    int trsm;
+    int pad_;
 } ssa_rowmul_job;
 
 /* Rows of C per k_rowmul CTA (granularity of the colsum partials). */
