@@ -61,6 +61,10 @@ typedef struct
 } ssa_batch_results;
 
 int ssa_batch_device_results(const ssa_batch *b, ssa_batch_results *out);
+/* Copy the status words of the first n series of the last run (0 = ok; bit 0: non-finite
+ * Gram in an orthonormalisation, bit 1: non-finite Rayleigh-Ritz result). Waits for the batch
+ * stream. Returns 0 or -1. */
+int ssa_batch_status(ssa_batch *b, int *status, int n);
 /* Wait for the batch stream; returns 0 when every series of the last run succeeded. */
 int ssa_batch_sync(ssa_batch *b);
 
@@ -85,6 +89,10 @@ int ssa_batch_profile(ssa_batch *b, double *ms, long long *launches, int nkinds)
 /* ---- library information ------------------------------------------------------------------ */
 /* Number of CUDA kernel launches issued by this library in this process. */
 unsigned long long ssa_b200_kernel_launches(void);
+/* Device self-check record of the current device: {violations, kernel, block, code, value};
+ * kernels that validate their job tables record the first violation there instead of
+ * accessing memory with it. reset != 0 clears the record. Returns 0 or -1. */
+int ssa_b200_device_checks(unsigned int *out5, int reset);
 /* sizeof(SSA_Opt) as compiled into the library. */
 int ssa_b200_sizeof_ssa_opt(void);
 

@@ -929,4 +929,5 @@ int ssa_opt_copy_factors(const SSA_Opt *ssa, double *U, double *V)
 
 /* ---- library information ----------------------------------------------------------------- */
 unsigned long long ssa_b200_kernel_launches(void) { return ssad_launch_count(); }
+int ssa_b200_device_checks(unsigned int *out5, int reset) { return ssad_read_checks(out5, reset) == 0 ? 0 : -1; }
 int ssa_b200_sizeof_ssa_opt(void) { return (int)sizeof(SSA_Opt); }

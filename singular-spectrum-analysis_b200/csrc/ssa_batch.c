@@ -221,3 +221,12 @@ int ssa_batch_profile(ssa_batch *b, double *ms, long long *launches, int nkinds)
     }
     return SSAK_NKINDS;
 }
+
+int ssa_batch_status(ssa_batch *b, int *status, int n)
+{
+    if (!b || !status || n < 1 || n > b->e.B)
+        return -1;
+    if (cudaStreamSynchronize(b->e.st) != cudaSuccess)
+        return -1;
+    return cudaMemcpy(status, b->e.status, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : -1;
+}

@@ -11,6 +11,7 @@
  */
 #include "ssa_engine.h"
 
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -55,6 +56,10 @@ int ssae_create(ssa_engine *e, int B, int N, int L, int kp, int k, cudaStream_t 
         return (int)cudaErrorInvalidValue;
     CK(cudaGetDevice(&e->device));
     CK(ssad_init_device());
+    {
+        const char *sc = getenv("SSA_SYNC_CHECK");
+        e->sync_check = sc && sc[0] == '1';
+    }
     e->B = B;
     e->N = N;
     e->L = L;
@@ -135,8 +140,16 @@ int ssae_set_profiling(ssa_engine *e, int on)
     return 0;
 }
 
+static const char *kind_name(int k)
+{
+    static const char *names[SSAK_NKINDS] = {"spectrum", "corr", "gram", "chol", "rowmul", "rr",
+                                             "elem_recon", "wcorr_finish", "group_sum", "recon", "lrf"};
+    return (k >= 0 && k < SSAK_NKINDS) ? names[k] : "?";
+}
+
 void ssae_prof_begin(ssa_engine *e, int kind)
 {
+    e->cur_kind = kind;
     if (!e->prof || e->nev >= SSA_PROF_MAX)
         return;
     e->ev_kind[e->nev] = kind;
@@ -145,6 +158,12 @@ void ssae_prof_begin(ssa_engine *e, int kind)
 
 void ssae_prof_end(ssa_engine *e)
 {
+    if (e->sync_check)
+    {
+        cudaError_t err = cudaStreamSynchronize(e->st);
+        if (err != cudaSuccess)
+            fprintf(stderr, "ssa: stage %s failed: %s\n", kind_name(e->cur_kind), cudaGetErrorString(err));
+    }
     if (!e->prof || e->nev >= SSA_PROF_MAX)
         return;
     cudaEventRecord(e->ev[2 * e->nev + 1], e->st);

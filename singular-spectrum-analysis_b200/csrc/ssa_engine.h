@@ -75,6 +75,10 @@ typedef struct
     double *W;                   /* B * k * k */
     float *Us, *Vs;              /* cached spectra B * k * ldS (allocated on demand) */
     ssa_job_arena ja;
+    /* SSA_SYNC_CHECK=1 in the environment: wait after every launch and report the first
+     * failing stage on stderr (debugging aid; off by default) */
+    int sync_check;
+    int cur_kind;
     /* stage profiler: event pairs around launches while prof != 0 */
     int prof;
     int nev;

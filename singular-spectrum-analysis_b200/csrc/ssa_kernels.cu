@@ -29,6 +29,29 @@
 using namespace ssa;
 
 static std::atomic<unsigned long long> g_launches{0};
+
+// Device-side self-check record: {violations, kernel id, block, code, value}. Kernels that
+// validate their job write the first violation here and skip the work of that block.
+__device__ unsigned int g_ssa_check[5];
+
+__device__ __forceinline__ void check_fail(unsigned kernel, unsigned code, unsigned value) {
+    if (atomicAdd(&g_ssa_check[0], 1u) == 0) {
+        g_ssa_check[1] = kernel;
+        g_ssa_check[2] = blockIdx.x + 65536u * blockIdx.y;
+        g_ssa_check[3] = code;
+        g_ssa_check[4] = value;
+    }
+}
+
+extern "C" int ssad_read_checks(unsigned int* out5, int reset) {
+    cudaError_t e = cudaMemcpyFromSymbol(out5, g_ssa_check, sizeof(unsigned int) * 5);
+    if (e != cudaSuccess) return (int)e;
+    if (reset) {
+        unsigned int z[5] = {0, 0, 0, 0, 0};
+        e = cudaMemcpyToSymbol(g_ssa_check, z, sizeof(z));
+    }
+    return (int)e;
+}
 static inline int launched(cudaError_t e) {
     g_launches.fetch_add(1, std::memory_order_relaxed);
     return (int)e;
@@ -591,6 +614,18 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr(const ssa_rr_job* __restrict_
     const ssa_rr_job J = jobs[blockIdx.x];
     const int n = J.kp;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    {
+        unsigned code = 0, val = 0;
+        if (n < 1 || n > SSA_MAX_KP) code = 1, val = (unsigned)n;
+        else if (J.k < 1 || J.k > n) code = 2, val = (unsigned)J.k;
+        else if (J.nchunks < 1 || J.nchunks > (1 << 16)) code = 3, val = (unsigned)J.nchunks;
+        else if (J.nchunks_q < 1 || J.nchunks_q > (1 << 16)) code = 4, val = (unsigned)J.nchunks_q;
+        else if (!J.part || !J.qsum || !J.sigma || !J.Zu || !J.Zv || !J.status) code = 5;
+        if (code) {
+            if (threadIdx.x == 0) check_fail(6, code, val);
+            return;
+        }
+    }
     reduce_packed(J.part, J.nchunks, n, A);
     for (int c = warp; c < n; c += nw)
         for (int r = lane; r < n; r += 32) Z[c * SLD + r] = (r == c) ? 1.0 : 0.0;
@@ -616,6 +651,10 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr(const ssa_rr_job* __restrict_
             for (int t = warp; t < npairs; t += nw) {
                 int p = perm[t], q = perm[ne - 1 - t];
                 if (q >= n || p >= n) continue;
+                if (p < 0 || q < 0) {
+                    if (lane == 0) check_fail(6, 6, (unsigned)(p * 1000 + q));
+                    continue;
+                }
                 double* ap = A + p * SLD;
                 double* aq = A + q * SLD;
                 double al = 0.0, be = 0.0, ga = 0.0;
@@ -657,7 +696,11 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr(const ssa_rr_job* __restrict_
             }
             __syncthreads();
         }
-        if (!notconv) break;
+        // Every thread reads the flag before thread 0 may reset it for the next sweep; otherwise
+        // warps could leave the loop at different sweeps and desynchronise the barriers.
+        const bool converged = !notconv;
+        __syncthreads();
+        if (converged) break;
     }
     // sigma_c = ||A[:, c]||
     for (int c = warp; c < n; c += nw) {
@@ -683,6 +726,10 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr(const ssa_rr_job* __restrict_
     const int k = J.k;
     for (int j = warp; j < k; j += nw) {
         const int col = order[j];
+        if (col < 0 || col >= n) {
+            if (lane == 0) check_fail(6, 7, (unsigned)col);
+            continue;
+        }
         const double sg = nrm[col];
         double dot = 0.0;
         for (int l = lane; l < n; l += 32) dot = fma(qs[l], Z[col * SLD + l], dot);

@@ -167,6 +167,9 @@ int ssad_lrf(const ssa_lrf_job *d_jobs, int njobs, void *stream);
  * correlation kernel generates when its input is NULL). */
 int ssad_gaussian(float *out, long long ld, int rows, int ncols, int col0, unsigned long long seed,
                   void *stream);
+/* Read (and optionally reset) the device self-check record {violations, kernel, block, code,
+ * value} of the current device. */
+int ssad_read_checks(unsigned int *out5, int reset);
 /* Count of kernel launches issued by this library since load (all devices). */
 unsigned long long ssad_launch_count(void);
 

@@ -104,6 +104,7 @@ _sig("ssa_batch_run_device", _I, ctypes.c_void_p, ctypes.c_void_p, _I, ctypes.c_
 _sig("ssa_batch_sync", _I, ctypes.c_void_p)
 _sig("ssa_batch_device_results", _I, ctypes.c_void_p, ctypes.POINTER(_BatchResults))
 _sig("ssa_batch_set_profiling", _I, ctypes.c_void_p, _I)
+_sig("ssa_batch_status", _I, ctypes.c_void_p, c_int_p, _I)
 _sig("ssa_batch_profile", _I, ctypes.c_void_p, c_double_p, ctypes.POINTER(ctypes.c_longlong), _I)
 
 PROFILE_KINDS = ("spectrum", "corr", "gram", "chol", "rowmul", "rr", "elem_recon", "wcorr_finish", "group_sum",
@@ -480,6 +481,13 @@ class SSABatch:
     def sync(self) -> None:
         if _lib.ssa_batch_sync(self._h) != 0:
             raise RuntimeError("a series of the batch failed")
+
+    def status(self, n: int) -> np.ndarray:
+        """Status words of the first n series of the last run (0 = ok)."""
+        st = np.zeros(n, dtype=np.int32)
+        if _lib.ssa_batch_status(self._h, _ip(st), n) != 0:
+            raise RuntimeError("ssa_batch_status failed")
+        return st
 
     def set_profiling(self, on: bool) -> None:
         if _lib.ssa_batch_set_profiling(self._h, 1 if on else 0) != 0:

@@ -241,3 +241,34 @@ def test_kernel_launch_counter(gpu, oracle):
     s.decompose(10)
     s.reconstruct([0])
     assert gpu.kernel_launches() > before
+
+
+def _device_checks(gpu):
+    import ctypes
+    chk = (ctypes.c_uint * 5)()
+    assert gpu._lib.ssa_b200_device_checks(chk, 1) == 0
+    return list(chk)
+
+
+def test_full_size_batch_clean(gpu, oracle):
+    """Uniform-batch sizes (N = 10000, L = 2500, k = 50, p = 10, q = 2) over 256 series: every
+    series succeeds, the kernels' self-checks record nothing, and two series match the oracle."""
+    import torch
+
+    B, N, L, k, p, q = 256, 10000, 2500, 50, 10, 2
+    _device_checks(gpu)
+    X = oracle.config2_batch(B, seed=3, N=N)
+    d_x = torch.from_numpy(X).cuda()
+    b = gpu.SSABatch(B, N, L, k, oversampling=p, power_iters=q, groups=[[0], [1, 2]])
+    for seed in (5, 6):
+        b.run_device(d_x.data_ptr(), B, seed=seed)
+        b.sync()
+    assert np.count_nonzero(b.status(B)) == 0
+    assert _device_checks(gpu)[0] == 0
+    sig, W, G = b.run(X, seed=6)
+    for s_ in (0, B - 1):
+        Om = oracle.device_gaussian(oracle.series_seed(6, s_), N - L + 1, k + p)
+        d = oracle.decompose_randomized(X[s_], L, k, p, Om, q=q)
+        rel, gap = sigma_errors(sig[s_], d.sigma)
+        assert np.all(rel[gap > 1e-3] <= SIG_TOL), (s_, rel.max())
+        assert rel_l2(G[s_, 1], oracle.reconstruct(d, [1, 2], N, L)) <= rec_tol(d.sigma, [1, 2])
