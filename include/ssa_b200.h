@@ -86,6 +86,27 @@ int ssa_opt_copy_factors(const SSA_Opt *ssa, double *U, double *V);
 int ssa_batch_set_profiling(ssa_batch *b, int on);
 int ssa_batch_profile(ssa_batch *b, double *ms, long long *launches, int nkinds);
 
+/* ---- W-correlation without device allocation --------------------------------------------
+ * No counterpart in the reference: an addition for callers that must not have device memory
+ * allocated on their behalf, such as a host application whose device memory is owned up
+ * front by another framework's allocator, or a latency-critical loop that cannot take the
+ * implicit device synchronisation of cudaMalloc. It computes the k x k W-correlation matrix
+ * (row-major, FP64) of a decomposition the caller already holds in device memory: U (L x k,
+ * column-major, leading dimension ldU), V (K x k, ldV), sigma (k doubles), K = N - L + 1, and
+ * writes it to the device array d_W. It calls no cudaMalloc, cudaFree or other allocating
+ * routine: its scratch is one fixed array of about 1.1 MB inside the library, which every GPU
+ * that loads the library holds until the process exits. Limits: N <= 8192 and k <= 32
+ * (larger sizes return -2 without touching the GPU); ldU and ldV even and U, V 8-byte aligned.
+ * The work is enqueued on `stream` (a cudaStream_t, NULL for the default stream) and the call
+ * returns without waiting. The first call on a device also performs that device's one-time
+ * set-up (twiddle table upload and the lookup of the scratch array's device address), so make
+ * the first call on each device before any stream capture. All calls on a device share the
+ * scratch array, which keeps the previous call's contents: calls that may overlap on the GPU
+ * (different streams without ordering between them) race and must be serialised by the
+ * caller. Returns 0, -1 (invalid argument or CUDA error) or -2 (size beyond the limits). */
+int ssa_wcorr_noalloc(const float *d_U, long long ldU, const float *d_V, long long ldV, const double *d_sigma,
+                      int N, int L, int k, double *d_W, void *stream);
+
 /* ---- library information ------------------------------------------------------------------ */
 /* Number of CUDA kernel launches issued by this library in this process. */
 unsigned long long ssa_b200_kernel_launches(void);

@@ -1009,3 +1009,128 @@ extern "C" int ssad_gaussian(float* out, long long ld, int rows, int ncols, int 
     k_gaussian<<<dim3(bx < 64 ? bx : 64, ncols), 256, 0, (cudaStream_t)stream>>>(out, ld, rows, ncols, col0, seed);
     return launched(cudaGetLastError());
 }
+
+// ---------------------------------------------------------------------------------------------
+// W-correlation without any device allocation (ssa_wcorr_noalloc, declared in ssa_b200.h)
+//
+// Some callers cannot let a library allocate device memory: a host application whose device
+// memory is owned up front by another framework's allocator (cudaMalloc behind its back would
+// break its accounting), or a latency-critical loop that must not take cudaMalloc's implicit
+// device synchronisation. This entry point serves them: it computes the W-correlation matrix of
+// a decomposition the caller already holds in device memory, and the only device memory it
+// touches besides the caller's inputs and output is the fixed array below, which every GPU that
+// loads the library holds until the process exits.
+// ---------------------------------------------------------------------------------------------
+
+#define SSA_NOALLOC_JOB_BYTES 1024
+#define SSA_NOALLOC_ROWS 1024  // Gram rows per partial
+#define SSA_NOALLOC_NCH ((SSA_NOALLOC_MAX_N + SSA_NOALLOC_ROWS - 1) / SSA_NOALLOC_ROWS)
+#define SSA_NOALLOC_PART_BYTES (SSA_NOALLOC_NCH * (SSA_NOALLOC_MAX_K * (SSA_NOALLOC_MAX_K + 1) / 2) * 8)
+#define SSA_NOALLOC_RECON_BYTES (SSA_NOALLOC_MAX_K * SSA_NOALLOC_MAX_N * 4)
+#define SSA_NOALLOC_BYTES (SSA_NOALLOC_JOB_BYTES + SSA_NOALLOC_PART_BYTES + SSA_NOALLOC_RECON_BYTES)
+
+// Scratch shared by every call on a device: [job tables | Gram partials | reconstructions].
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SSA_NOALLOC_BYTES];
+
+#include <cstring>
+#include <mutex>
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[64];
+static bool g_noalloc_ready[64];
+static float2 g_noalloc_tw_host[SSA_TW_N];  // FP64-computed twiddles, filled once per process
+
+// Per-device set-up, run by the first call on a device with that device current: upload the
+// twiddle table from static host storage and look up the device address of the scratch array
+// (host code must not pass the symbol itself to a kernel: on the host it is only a stand-in).
+static int noalloc_setup(int dev, void** scratch) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (g_noalloc_ready[dev]) {
+        *scratch = g_noalloc_ptr[dev];
+        return 0;
+    }
+    static bool tw_filled = false;
+    if (!tw_filled) {
+        for (int t = 0; t < SSA_TW_N; ++t) {
+            const double a = -2.0 * M_PI * (double)t / (double)SSA_TW_N;
+            g_noalloc_tw_host[t] = make_float2((float)cos(a), (float)sin(a));
+        }
+        tw_filled = true;
+    }
+    cudaError_t e = cudaMemcpyToSymbol(g_tw, g_noalloc_tw_host, sizeof(g_noalloc_tw_host));
+    if (e != cudaSuccess) return -1;
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) return -1;
+    g_noalloc_ptr[dev] = p;
+    g_noalloc_ready[dev] = true;
+    *scratch = p;
+    return 0;
+}
+
+extern "C" __attribute__((visibility("default"))) int ssa_wcorr_noalloc(
+    const float* d_U, long long ldU, const float* d_V, long long ldV, const double* d_sigma, int N, int L, int k,
+    double* d_W, void* stream) {
+    if (!d_U || !d_V || !d_sigma || !d_W || N < 4 || L < 2 || L > N - 1 || k < 1) return -1;
+    const int K = N - L + 1;
+    if (k > L || k > K || ldU < L || ldV < K || (ldU & 1) || (ldV & 1) ||
+        (((uintptr_t)d_U) & 7) || (((uintptr_t)d_V) & 7))
+        return -1;
+    if (N > SSA_NOALLOC_MAX_N || k > SSA_NOALLOC_MAX_K) return -2;  // beyond the fixed scratch
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
+    void* scratch = nullptr;
+    if (noalloc_setup(dev, &scratch) != 0) return -1;
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned char* base = (unsigned char*)scratch;
+    ssa_col_job* d_elem = (ssa_col_job*)base;
+    ssa_gram_job* d_gram = (ssa_gram_job*)(base + 256);
+    ssa_wfin_job* d_wfin = (ssa_wfin_job*)(base + 512);
+    double* d_part = (double*)(base + SSA_NOALLOC_JOB_BYTES);
+    float* d_recon = (float*)(base + SSA_NOALLOC_JOB_BYTES + SSA_NOALLOC_PART_BYTES);
+    const long long ldN = (N + 3) & ~3LL;
+    const int nch = (N + SSA_NOALLOC_ROWS - 1) / SSA_NOALLOC_ROWS;
+    // Every partial and every reconstruction row the later stages read is written first, so the
+    // scratch needs no clearing between calls.
+    ssa_col_job je;
+    memset(&je, 0, sizeof(je));
+    je.in = d_U;
+    je.ld_in = ldU;
+    je.n_in = L;
+    je.in2 = d_V;
+    je.ld_in2 = ldV;
+    je.n_in2 = K;
+    je.scale = d_sigma;
+    je.out = d_recon;
+    je.ld_out = ldN;
+    je.ncols = k;
+    je.N = N;
+    je.L = L;
+    je.K = K;
+    ssa_gram_job jg;
+    memset(&jg, 0, sizeof(jg));
+    jg.A = d_recon;
+    jg.part = d_part;
+    jg.ld = ldN;
+    jg.m = N;
+    jg.n = k;
+    jg.rows_per_cta = SSA_NOALLOC_ROWS;
+    jg.weighted = 1;
+    jg.N = N;
+    jg.L = L;
+    jg.K = K;
+    ssa_wfin_job jw;
+    memset(&jw, 0, sizeof(jw));
+    jw.part = d_part;
+    jw.W = d_W;
+    jw.nchunks = nch;
+    jw.k = k;
+    if (cudaMemcpyAsync(d_elem, &je, sizeof(je), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(d_gram, &jg, sizeof(jg), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(d_wfin, &jw, sizeof(jw), cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return -1;
+    if (ssad_elem_recon(d_elem, 1, k, ssad_logh_for(N), st) != 0) return -1;
+    if (ssad_gram(d_gram, 1, nch, 1, st) != 0) return -1;
+    if (ssad_wfin(d_wfin, 1, st) != 0) return -1;
+    return 0;
+}

@@ -19,6 +19,10 @@
 extern "C" {
 #endif
 
+/* Size limits of the fixed scratch used by ssa_wcorr_noalloc (ssa_b200.h). */
+#define SSA_NOALLOC_MAX_N 8192
+#define SSA_NOALLOC_MAX_K 32
+
 /* Largest (k + p) the Gram / Cholesky / Rayleigh-Ritz kernels hold on chip. */
 #define SSA_MAX_KP 64
 /* Rows staged in shared memory per step of the Gram kernel. */
