@@ -4,8 +4,9 @@
  * one kernel per stage over all series. Nothing here computes numbers on the CPU.
  *
  * Randomized decomposition (reference MKL/ssa_opt.h:1685-1763, plus q power iterations):
- *   Y = H Omega; Q = CholQR2(Y);
- *   repeat q times: Z = H^T Q; Z = CholQR(Z); Y = H Z; Q = CholQR2(Y);
+ *   Y = H Omega;
+ *   repeat q times: Q = CholQR(Y); Z = H^T Q; Z = CholQR(Z); Y = H Z;
+ *   Q = CholQR2(Y);
  *   B = H^T Q; B^T B = Z_r Lambda Z_r^T (FP64 Jacobi); sigma = sqrt(Lambda);
  *   U = Q Z_r[:, :k], V = B Z_r[:, :k] Sigma^{-1}, signs so that sum_i U[i, j] >= 0.
  */
@@ -464,8 +465,9 @@ int ssae_decompose(ssa_engine *e, int nb, int kp, int k, int q, const float *d_o
     CK(sweep(e, nb, kp, 0, d_omega, omega_ld, seed, 1));
     for (int it = 0; it < q; it++)
     {
-        /* Q = orth(Y) (two passes), Z = H^T Q, Z = orth(Z) (one pass), Y = H Z */
-        CK(cholqr_pass(e, nb, e->Y, sY, e->ldL, L, kp, e->rows_L, NULL));
+        /* Intermediate bases need to be well conditioned, not orthonormal to rounding: one
+         * CholQR pass (FP64 Gram, so the loss of orthogonality is ~u32 cond(Y)).
+         * Q = orth(Y), Z = H^T Q, Z = orth(Z), Y = H Z */
         CK(cholqr_pass(e, nb, e->Y, sY, e->ldL, L, kp, e->rows_L, NULL));
         CK(sweep(e, nb, kp, 1, NULL, 0, 0, 0));
         CK(cholqr_pass(e, nb, e->Z, sZ, e->ldK, K, kp, e->rows_K, NULL));

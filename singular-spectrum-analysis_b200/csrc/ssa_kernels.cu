@@ -520,7 +520,7 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_chol(const ssa_chol_job* __re
 #define ROWMUL_THREADS SSA_ROWMUL_ROWS
 
 __global__ void __launch_bounds__(ROWMUL_THREADS) k_rowmul(const ssa_rowmul_job* __restrict__ jobs) {
-    __shared__ float sB[SSA_MAX_KP * SSA_MAX_KP];
+    __shared__ __align__(16) float sB[SSA_MAX_KP * SSA_MAX_KP];
     __shared__ float sInv[SSA_MAX_KP];
     __shared__ double wsum[ROWMUL_THREADS / 32][SSA_MAX_KP];
     const ssa_rowmul_job J = jobs[blockIdx.y];
@@ -547,11 +547,17 @@ __global__ void __launch_bounds__(ROWMUL_THREADS) k_rowmul(const ssa_rowmul_job*
             if (j < n) {
                 const float* b = sB + j * SSA_MAX_KP;
                 float s0 = a[j], s1 = 0.f;
+                // float4 broadcast loads: one shared-memory wavefront feeds four FMAs per lane
 #pragma unroll
-                for (int l = 0; l < j; l += 2) {
-                    s0 = fmaf(-a[l], b[l], s0);
-                    if (l + 1 < j) s1 = fmaf(-a[l + 1], b[l + 1], s1);
+                for (int l = 0; l < (j & ~3); l += 4) {
+                    const float4 bv = *reinterpret_cast<const float4*>(b + l);
+                    s0 = fmaf(-a[l], bv.x, s0);
+                    s1 = fmaf(-a[l + 1], bv.y, s1);
+                    s0 = fmaf(-a[l + 2], bv.z, s0);
+                    s1 = fmaf(-a[l + 3], bv.w, s1);
                 }
+#pragma unroll
+                for (int l = (j & ~3); l < j; ++l) s0 = fmaf(-a[l], b[l], s0);
                 const float c = (s0 + s1) * sInv[j];
                 a[j] = c;
                 if (live) J.C[(long long)i + (long long)j * J.ldc] = c;
@@ -568,9 +574,12 @@ __global__ void __launch_bounds__(ROWMUL_THREADS) k_rowmul(const ssa_rowmul_job*
             const float* b = sB + j * SSA_MAX_KP;
             float s0 = 0.f, s1 = 0.f;
 #pragma unroll
-            for (int l = 0; l < SSA_MAX_KP; l += 2) {
-                s0 = fmaf(a[l], b[l], s0);
-                s1 = fmaf(a[l + 1], b[l + 1], s1);
+            for (int l = 0; l < SSA_MAX_KP; l += 4) {
+                const float4 bv = *reinterpret_cast<const float4*>(b + l);
+                s0 = fmaf(a[l], bv.x, s0);
+                s1 = fmaf(a[l + 1], bv.y, s1);
+                s0 = fmaf(a[l + 2], bv.z, s0);
+                s1 = fmaf(a[l + 3], bv.w, s1);
             }
             const float c = s0 + s1;
             if (live) J.C[(long long)i + (long long)j * J.ldc] = c;
