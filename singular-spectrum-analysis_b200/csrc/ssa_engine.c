@@ -450,7 +450,7 @@ static int cholqr_pass(ssa_engine *e, int nb, float *A, size_t sstride, long lon
     const int nch = (m + rows - 1) / rows;
     CK(gram(e, nb, A, sstride, ld, m, n, rows, 0));
     CK(chol(e, nb, nch, n));
-    return rowmul(e, nb, A, sstride, ld, m, n, e->Rinv, (size_t)e->kp * e->kp, n, n, A, sstride, ld, colsum, 1);
+    return rowmul(e, nb, A, sstride, ld, m, n, e->Rinv, (size_t)e->kp * e->kp, n, n, A, sstride, ld, colsum, 0);
 }
 
 int ssae_decompose(ssa_engine *e, int nb, int kp, int k, int q, const float *d_omega, long long omega_ld,

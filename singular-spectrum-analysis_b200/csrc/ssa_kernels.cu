@@ -153,7 +153,7 @@ __device__ __forceinline__ void load_column(float2* s, const ssa_col_job& J, int
 // ---------------------------------------------------------------------------------------------
 
 template <int LOGH>
-__global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_spectrum(const ssa_col_job* __restrict__ jobs) {
+__global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k_spectrum(const ssa_col_job* __restrict__ jobs) {
     constexpr int H = 1 << LOGH;
     extern __shared__ float2 smem[];
     const ssa_col_job J = jobs[blockIdx.y];
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_spectrum(const ssa_co
 }
 
 template <int LOGH>
-__global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_corr(const ssa_col_job* __restrict__ jobs) {
+__global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k_corr(const ssa_col_job* __restrict__ jobs) {
     constexpr int H = 1 << LOGH;
     extern __shared__ float2 smem[];
     const ssa_col_job J = jobs[blockIdx.y];
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_elem_recon(const ssa_
 
 // Grouped reconstruction from cached spectra.
 template <int LOGH>
-__global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_recon(const ssa_recon_job* __restrict__ jobs) {
+__global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k_recon(const ssa_recon_job* __restrict__ jobs) {
     constexpr int H = 1 << LOGH;
     extern __shared__ float2 smem[];
     const ssa_recon_job J = jobs[blockIdx.y];
@@ -497,6 +497,7 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_chol(const ssa_chol_job* __re
     extern __shared__ double dsm[];
     __shared__ double red[32];
     double* G = dsm;
+    double* X = dsm + SSA_MAX_KP * SLD;
     const ssa_chol_job J = jobs[blockIdx.x];
     const int n = J.n;
     reduce_packed(J.part, J.nchunks, n, G);
@@ -507,9 +508,22 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_chol(const ssa_chol_job* __re
     }
     const double floor_ = dmax > 0.0 ? dmax * 1e-13 * (double)n : 1.0;
     chol_upper_inplace(G, n, floor_);
+    // X = R^{-1} (upper), row by row from the bottom: X[i][c] = (delta_ic - sum_{l=i+1..c}
+    // R[i][l] X[l][c]) / R[i][i]; R[i][l] sits at G[l * SLD + i], X[l][c] at X[c * SLD + l].
+    for (int e = threadIdx.x; e < SSA_MAX_KP * SLD; e += blockDim.x) X[e] = 0.0;
+    __syncthreads();
+    for (int i = n - 1; i >= 0; --i) {
+        const double rii = G[i * SLD + i];
+        for (int c = i + threadIdx.x; c < n; c += blockDim.x) {
+            double sacc = (c == i) ? 1.0 : 0.0;
+            for (int l = i + 1; l <= c; ++l) sacc -= G[l * SLD + i] * X[c * SLD + l];
+            X[c * SLD + i] = sacc / rii;
+        }
+        __syncthreads();
+    }
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int c = e / n, r = e - c * n;
-        J.R[e] = (float)G[c * SLD + r];
+        J.R[e] = (float)X[c * SLD + r];
     }
 }
 
@@ -517,88 +531,74 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_chol(const ssa_chol_job* __re
 // Row-by-row product with a small matrix: C[i, :p] = A[i, :n] Bm
 // ---------------------------------------------------------------------------------------------
 
-#define ROWMUL_THREADS SSA_ROWMUL_ROWS
+// C[r, 0:p] = A[r, 0:n] M for the SSA_ROWMUL_ROWS rows of one tile. Thread (g, j) owns output
+// column j (M[:, j] in registers) for the rows r = g, g + 2, ...; rows are read from a
+// row-major shared copy of the tile as broadcast float4s, four rows at a time so that four
+// independent FMA chains are in flight. Outputs go through shared memory so that the global
+// stores stay coalesced along the columns. In place (C == A) is safe: the tile is in shared
+// memory before any output is written.
+#define ROWMUL_THREADS 128
+#define RM_AST 68  // row stride of the shared A tile (floats, multiple of 4)
+#define RM_SMEM ((SSA_ROWMUL_ROWS * RM_AST + SSA_ROWMUL_ROWS * (SSA_MAX_KP + 1)) * (int)sizeof(float))
 
 __global__ void __launch_bounds__(ROWMUL_THREADS) k_rowmul(const ssa_rowmul_job* __restrict__ jobs) {
-    __shared__ __align__(16) float sB[SSA_MAX_KP * SSA_MAX_KP];
-    __shared__ float sInv[SSA_MAX_KP];
-    __shared__ double wsum[ROWMUL_THREADS / 32][SSA_MAX_KP];
+    extern __shared__ float rsm[];
+    float* As = rsm;                               // [row][l], stride RM_AST
+    float* Cs = rsm + SSA_ROWMUL_ROWS * RM_AST;    // [row][j], stride SSA_MAX_KP + 1
+    __shared__ double csum[2][SSA_MAX_KP];
     const ssa_rowmul_job J = jobs[blockIdx.y];
     const int n = J.n, p = J.p;
-    if (blockIdx.x * ROWMUL_THREADS >= J.m) return;
-    for (int e = threadIdx.x; e < SSA_MAX_KP * p; e += blockDim.x) {
-        const int j = e / SSA_MAX_KP, l = e - j * SSA_MAX_KP;
-        sB[e] = l < n ? J.Bm[l + j * J.ldb] : 0.f;
+    const int r0 = blockIdx.x * SSA_ROWMUL_ROWS;
+    if (r0 >= J.m) return;
+    const int rows = min(SSA_ROWMUL_ROWS, J.m - r0);
+    // stage the tile (coalesced along rows), zero-padded to 64 columns and SSA_ROWMUL_ROWS rows
+    for (int e = threadIdx.x; e < SSA_ROWMUL_ROWS * SSA_MAX_KP; e += blockDim.x) {
+        const int l = e / SSA_ROWMUL_ROWS, r = e - l * SSA_ROWMUL_ROWS;
+        float v = 0.f;
+        if (l < n && r < rows) v = J.A[(long long)(r0 + r) + (long long)l * J.lda];
+        As[r * RM_AST + l] = v;
     }
-    if (J.trsm)
-        for (int j = threadIdx.x; j < SSA_MAX_KP; j += blockDim.x) sInv[j] = j < n ? 1.0f / J.Bm[j + j * J.ldb] : 0.f;
+    const int j = threadIdx.x & 63, g = threadIdx.x >> 6;
+    float mcol[SSA_MAX_KP];
+#pragma unroll
+    for (int l = 0; l < SSA_MAX_KP; ++l) mcol[l] = (j < p && l < n) ? J.Bm[l + j * J.ldb] : 0.f;
     __syncthreads();
-    const int i = blockIdx.x * ROWMUL_THREADS + threadIdx.x;
-    const bool live = i < J.m;
-    float a[SSA_MAX_KP];
+    double cs = 0.0;
+    for (int r = g * 4; r < SSA_ROWMUL_ROWS; r += 8) {
+        const float* a0 = As + r * RM_AST;
+        float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
 #pragma unroll
-    for (int l = 0; l < SSA_MAX_KP; ++l)
-        a[l] = (live && l < n) ? J.A[(long long)i + (long long)l * J.lda] : 0.f;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (J.trsm) {
-        // x R = a, R upper: x_j = (a_j - sum_{l<j} x_l R[l][j]) / R[j][j]; a is overwritten by x
-#pragma unroll
-        for (int j = 0; j < SSA_MAX_KP; ++j) {
-            if (j < n) {
-                const float* b = sB + j * SSA_MAX_KP;
-                float s0 = a[j], s1 = 0.f;
-                // float4 broadcast loads: one shared-memory wavefront feeds four FMAs per lane
-#pragma unroll
-                for (int l = 0; l < (j & ~3); l += 4) {
-                    const float4 bv = *reinterpret_cast<const float4*>(b + l);
-                    s0 = fmaf(-a[l], bv.x, s0);
-                    s1 = fmaf(-a[l + 1], bv.y, s1);
-                    s0 = fmaf(-a[l + 2], bv.z, s0);
-                    s1 = fmaf(-a[l + 3], bv.w, s1);
-                }
-#pragma unroll
-                for (int l = (j & ~3); l < j; ++l) s0 = fmaf(-a[l], b[l], s0);
-                const float c = (s0 + s1) * sInv[j];
-                a[j] = c;
-                if (live) J.C[(long long)i + (long long)j * J.ldc] = c;
-                if (J.colsum) {
-                    double v = live ? (double)c : 0.0;
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-                    if (lane == 0) wsum[warp][j] = v;
-                }
-            }
+        for (int l = 0; l < SSA_MAX_KP; l += 4) {
+            const float4 x0 = *reinterpret_cast<const float4*>(a0 + l);
+            const float4 x1 = *reinterpret_cast<const float4*>(a0 + RM_AST + l);
+            const float4 x2 = *reinterpret_cast<const float4*>(a0 + 2 * RM_AST + l);
+            const float4 x3 = *reinterpret_cast<const float4*>(a0 + 3 * RM_AST + l);
+            c0 = fmaf(x0.x, mcol[l], c0); c0 = fmaf(x0.y, mcol[l + 1], c0);
+            c0 = fmaf(x0.z, mcol[l + 2], c0); c0 = fmaf(x0.w, mcol[l + 3], c0);
+            c1 = fmaf(x1.x, mcol[l], c1); c1 = fmaf(x1.y, mcol[l + 1], c1);
+            c1 = fmaf(x1.z, mcol[l + 2], c1); c1 = fmaf(x1.w, mcol[l + 3], c1);
+            c2 = fmaf(x2.x, mcol[l], c2); c2 = fmaf(x2.y, mcol[l + 1], c2);
+            c2 = fmaf(x2.z, mcol[l + 2], c2); c2 = fmaf(x2.w, mcol[l + 3], c2);
+            c3 = fmaf(x3.x, mcol[l], c3); c3 = fmaf(x3.y, mcol[l + 1], c3);
+            c3 = fmaf(x3.z, mcol[l + 2], c3); c3 = fmaf(x3.w, mcol[l + 3], c3);
         }
-    } else {
-        for (int j = 0; j < p; ++j) {
-            const float* b = sB + j * SSA_MAX_KP;
-            float s0 = 0.f, s1 = 0.f;
-#pragma unroll
-            for (int l = 0; l < SSA_MAX_KP; l += 4) {
-                const float4 bv = *reinterpret_cast<const float4*>(b + l);
-                s0 = fmaf(a[l], bv.x, s0);
-                s1 = fmaf(a[l + 1], bv.y, s1);
-                s0 = fmaf(a[l + 2], bv.z, s0);
-                s1 = fmaf(a[l + 3], bv.w, s1);
-            }
-            const float c = s0 + s1;
-            if (live) J.C[(long long)i + (long long)j * J.ldc] = c;
-            if (J.colsum) {
-                double v = live ? (double)c : 0.0;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-                if (lane == 0) wsum[warp][j] = v;
-            }
-        }
+        float* cr = Cs + r * (SSA_MAX_KP + 1) + j;
+        cr[0] = c0;
+        cr[SSA_MAX_KP + 1] = c1;
+        cr[2 * (SSA_MAX_KP + 1)] = c2;
+        cr[3 * (SSA_MAX_KP + 1)] = c3;
+        if (r < rows) cs += (double)c0;
+        if (r + 1 < rows) cs += (double)c1;
+        if (r + 2 < rows) cs += (double)c2;
+        if (r + 3 < rows) cs += (double)c3;
     }
-    if (J.colsum) {
-        __syncthreads();
-        for (int j = threadIdx.x; j < p; j += blockDim.x) {
-            double t = 0.0;
-            for (int w = 0; w < ROWMUL_THREADS / 32; ++w) t += wsum[w][j];
-            J.colsum[(long long)blockIdx.x * p + j] = t;
-        }
+    if (J.colsum) csum[g][j] = cs;
+    __syncthreads();
+    for (int e = threadIdx.x; e < SSA_ROWMUL_ROWS * p; e += blockDim.x) {
+        const int jj = e / SSA_ROWMUL_ROWS, r = e - jj * SSA_ROWMUL_ROWS;
+        if (r < rows) J.C[(long long)(r0 + r) + (long long)jj * J.ldc] = Cs[r * (SSA_MAX_KP + 1) + jj];
     }
+    if (J.colsum && threadIdx.x < p) J.colsum[(long long)blockIdx.x * p + threadIdx.x] = csum[0][threadIdx.x] + csum[1][threadIdx.x];
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -979,7 +979,9 @@ extern "C" int ssad_chol(const ssa_chol_job* d_jobs, int njobs, void* stream) {
 extern "C" int ssad_rowmul(const ssa_rowmul_job* d_jobs, int njobs, int maxrows, int maxn, void* stream) {
     if (njobs <= 0 || maxrows <= 0) return 0;
     if (maxn > SSA_MAX_KP) return (int)cudaErrorInvalidValue;
-    k_rowmul<<<dim3((maxrows + ROWMUL_THREADS - 1) / ROWMUL_THREADS, njobs), ROWMUL_THREADS, 0,
+    cudaError_t e = set_smem(k_rowmul, RM_SMEM);
+    if (e != cudaSuccess) return (int)e;
+    k_rowmul<<<dim3((maxrows + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS, njobs), ROWMUL_THREADS, RM_SMEM,
                (cudaStream_t)stream>>>(d_jobs);
     return launched(cudaGetLastError());
 }

@@ -62,8 +62,9 @@ typedef struct
     int N, L, K;
 } ssa_gram_job;
 
-/* Cholesky job: G = sum of the partials; G = R^T R with R upper triangular, written as fp32
- * n x n column-major (R[r][c] at R[r + c n], zeros below the diagonal). */
+/* Cholesky job: G = sum of the partials; G = R^T R with R upper triangular; writes R^{-1}
+ * (computed in FP64) as fp32 n x n column-major (X[r][c] at R[r + c n], zeros below the
+ * diagonal). */
 typedef struct
 {
     const double *part;
@@ -73,10 +74,9 @@ typedef struct
     int pad_[2];
 } ssa_chol_job;
 
-/* Row-by-row products with a small matrix (in place allowed: C == A, since every thread reads
- * its whole row of A before writing its row of C):
- *   trsm == 0: C[:, 0:p] = A[:, 0:n] * Bm[0:n, 0:p];
- *   trsm == 1: C = A * Bm^{-1} for upper-triangular Bm (p == n), by forward substitution. */
+/* Row-by-row products with a small matrix: C[:, 0:p] = A[:, 0:n] * Bm[0:n, 0:p] (in place
+ * allowed: C == A; each tile of rows is staged in shared memory before it is overwritten).
+ * `trsm` is reserved (0). */
 typedef struct
 {
     const float *A;
