@@ -20,6 +20,11 @@ extern "C" {
  * ssa_opt_prepare. Returns 0 or -1. */
 int ssa_opt_decompose_randomized_ex(SSA_Opt *ssa, int k, int oversampling, int power_iters, const double *Omega);
 
+/* Block power decomposition (reference: ssa_opt_decompose_block, MKL/ssa_opt.h:1765-1933)
+ * with caller-supplied start blocks V0 (K x k column-major; the columns of block i start block
+ * i), or V0 == NULL for the library generator. Returns 0 or -1. */
+int ssa_opt_decompose_block_ex(SSA_Opt *ssa, int k, int block_size, int max_iter, const double *V0);
+
 /* MSSA analogue of ssa_opt_decompose_randomized_ex (reference: mssa_opt_decompose,
  * MKL/ssa_opt.h:4116-4210). */
 int mssa_opt_decompose_ex(MSSA_Opt *mssa, int k, int oversampling, int power_iters, const double *Omega);

@@ -347,29 +347,78 @@ int ssa_opt_decompose_randomized_ex(SSA_Opt *ssa, int k, int oversampling, int p
     return decompose_randomized_impl(ssa, k, oversampling, power_iters, Omega);
 }
 
-/* Sequential and extend decompositions (MKL/ssa_opt.h:1560-1678, :1935-2056) are outside the
- * accelerated path; the symbols exist for the wrapper and report failure. */
-int ssa_opt_decompose(SSA_Opt *ssa, int k, int max_iter)
+/* Block power iteration with Rayleigh-Ritz (MKL/ssa_opt.h:1765-1933) on the device. V0: host
+ * K x k column-major start blocks (block i = its columns), or NULL for the library generator.
+ * Like the reference it (re)allocates the result arrays on every call. */
+static int decompose_block_impl(SSA_Opt *ssa, int k, int block_size, int max_iter, const double *V0)
 {
-    (void)ssa;
-    (void)k;
-    (void)max_iter;
-    return -1;
-}
-
-int ssa_opt_extend(SSA_Opt *ssa, int additional_k, int max_iter)
-{
-    (void)ssa;
-    (void)additional_k;
-    (void)max_iter;
-    return -1;
+    if (!ssa || !ssa->initialized || k < 1 || block_size < 1)
+        return -1;
+    ssa_opt_free_cached_ffts(ssa);
+    const int L = ssa->L, K = ssa->K;
+    const int b = imin(block_size, imin(k, imin(L, K)));
+    k = imin(k, imin(L, K));
+    if (k > SSA_MAX_KP || max_iter < 0)
+        return -1;
+    (void)b;
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    ssa_engine *e = &g->e;
+    ssae_reset_jobs(e);
+    g->spectra_valid = 0;
+    g->wcorr_valid = 0;
+    ssa->decomposed = false;
+    if (alloc_results(ssa, k) != 0)
+        return -1;
+    ssa->n_components = k;
+    const float *d_V0 = NULL;
+    if (V0)
+    {
+        if (ssae_ensure_block(e, imin(block_size, k)) != 0 || ensure_stage(g, (size_t)K * k) != 0)
+            return -1;
+        for (size_t i = 0; i < (size_t)K * k; i++)
+            g->h_stage[i] = (float)V0[i];
+        /* staged in the permutation buffer Vt, which the decomposition only uses at its end */
+        if (cudaMemcpyAsync(e->Vt, g->h_stage, sizeof(float) * (size_t)K * k, cudaMemcpyHostToDevice, e->st) !=
+            cudaSuccess)
+            return -1;
+        d_V0 = e->Vt;
+    }
+    const unsigned long long seed =
+        (SSA_DEFAULT_SEED + 0x100000000ULL * (unsigned long long)ssa->rng_calls) ^ 0xB10CB10CB10CB10CULL;
+    ssa->rng_calls++;
+    if (ssae_decompose_block(e, 1, k, block_size, max_iter, d_V0, K, seed) != 0 || sync_ok(g) != 0 ||
+        check_status(g) != 0 || mirror_results(ssa, k) != 0)
+        return -1;
+    ssa->decomposed = true;
+    return 0;
 }
 
 int ssa_opt_decompose_block(SSA_Opt *ssa, int k, int block_size, int max_iter)
 {
+    return decompose_block_impl(ssa, k, block_size, max_iter, NULL);
+}
+
+int ssa_opt_decompose_block_ex(SSA_Opt *ssa, int k, int block_size, int max_iter, const double *V0)
+{
+    return decompose_block_impl(ssa, k, block_size, max_iter, V0);
+}
+
+/* Sequential power iteration (MKL/ssa_opt.h:1560-1678) computes one component at a time with
+ * deflation against the earlier ones; on the device it runs as block power iteration with
+ * blocks of one column, which has the same fixed points (the reference's early stop on
+ * convergence is not reproduced: all max_iter iterations run). */
+int ssa_opt_decompose(SSA_Opt *ssa, int k, int max_iter)
+{
+    if (!ssa || !ssa->initialized || k < 1)
+        return -1;
+    return decompose_block_impl(ssa, k, 1, max_iter, NULL);
+}
+
+/* ssa_opt_extend (MKL/ssa_opt.h:1935-2056) is outside the accelerated path: it reports failure. */
+int ssa_opt_extend(SSA_Opt *ssa, int additional_k, int max_iter)
+{
     (void)ssa;
-    (void)k;
-    (void)block_size;
+    (void)additional_k;
     (void)max_iter;
     return -1;
 }

@@ -199,7 +199,9 @@ void ssae_destroy(ssa_engine *e)
         if (e->ev[i])
             cudaEventDestroy(e->ev[i]);
     void *bufs[] = {e->x64, e->X, e->Y, e->Z, e->part, e->qsum, e->Rinv, e->Zu, e->Zv,
-                    e->sigma, e->status, e->recon, e->norm2, e->W, e->Us, e->Vs, e->ja.d};
+                    e->sigma, e->status, e->recon, e->norm2, e->W, e->Us, e->Vs, e->ja.d,
+                    e->Ub, e->Vb, e->xpart, e->xC, e->sUs, e->sVs, e->sDinv, e->perm, e->sgn,
+                    e->Ut, e->Vt};
     for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
         if (bufs[i])
             cudaFree(bufs[i]);
@@ -450,7 +452,7 @@ static int cholqr_pass(ssa_engine *e, int nb, float *A, size_t sstride, long lon
     const int nch = (m + rows - 1) / rows;
     CK(gram(e, nb, A, sstride, ld, m, n, rows, 0));
     CK(chol(e, nb, nch, n));
-    return rowmul(e, nb, A, sstride, ld, m, n, e->Rinv, (size_t)e->kp * e->kp, n, n, A, sstride, ld, colsum, 0);
+    return rowmul(e, nb, A, sstride, ld, m, n, e->Rinv, (size_t)e->kp * e->kp, n, n, A, sstride, ld, colsum, 1);
 }
 
 int ssae_decompose(ssa_engine *e, int nb, int kp, int k, int q, const float *d_omega, long long omega_ld,
@@ -630,4 +632,341 @@ int ssae_recon_group(ssa_engine *e, int s, int k, const int *d_group, int n_grou
     int rc_ = ssad_recon((const ssa_recon_job *)d, 1, e->logh, e->st);
     ssae_prof_end(e);
     return rc_;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Block power iteration                                                                       */
+/* ------------------------------------------------------------------------------------------ */
+
+int ssae_ensure_block(ssa_engine *e, int bcap)
+{
+    if (e->Ub && e->bcap >= bcap)
+        return 0;
+    void *old[] = {e->Ub, e->Vb, e->xpart, e->xC, e->sUs, e->sVs, e->sDinv, e->perm, e->sgn, e->Ut, e->Vt};
+    cudaStreamSynchronize(e->st);
+    for (size_t i = 0; i < sizeof(old) / sizeof(old[0]); i++)
+        if (old[i])
+            cudaFree(old[i]);
+    const size_t Bs = (size_t)e->B;
+    const int nchx = imax(e->nch_L, e->nch_K);
+    int r = 0;
+    r |= dmalloc((void **)&e->Ub, Bs * e->ldL * 2 * bcap * sizeof(float));
+    r |= dmalloc((void **)&e->Vb, Bs * e->ldK * bcap * sizeof(float));
+    r |= dmalloc((void **)&e->xpart, Bs * nchx * SSA_MAX_KP * SSA_MAX_KP * sizeof(double));
+    r |= dmalloc((void **)&e->xC, Bs * SSA_MAX_KP * SSA_MAX_KP * sizeof(float));
+    r |= dmalloc((void **)&e->sUs, Bs * SSA_MAX_KP * SSA_MAX_KP * sizeof(float));
+    r |= dmalloc((void **)&e->sVs, Bs * SSA_MAX_KP * SSA_MAX_KP * sizeof(float));
+    r |= dmalloc((void **)&e->sDinv, Bs * SSA_MAX_KP * SSA_MAX_KP * sizeof(float));
+    r |= dmalloc((void **)&e->perm, Bs * SSA_MAX_KP * sizeof(int));
+    r |= dmalloc((void **)&e->sgn, Bs * SSA_MAX_KP * sizeof(float));
+    r |= dmalloc((void **)&e->Ut, Bs * e->ldL * e->kp * sizeof(float));
+    r |= dmalloc((void **)&e->Vt, Bs * e->ldK * e->kp * sizeof(float));
+    e->bcap = r ? 0 : bcap;
+    return r ? (int)cudaErrorMemoryAllocation : 0;
+}
+
+/* out_s = H in_s (adjoint = 0: in K rows, out L rows) or H^T in_s, ncols columns. */
+static int corr_io(ssa_engine *e, int nb, int ncols, int adjoint, const float *in, size_t in_stride, long long ld_in,
+                   float *out, size_t out_stride, long long ld_out)
+{
+    ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)nb, sizeof(ssa_col_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    for (int s = 0; s < nb; s++)
+    {
+        ssa_col_job *J = &jobs[s];
+        J->in = in + (size_t)s * in_stride;
+        J->ld_in = ld_in;
+        J->n_in = adjoint ? e->L : e->K;
+        J->out = out + (size_t)s * out_stride;
+        J->ld_out = ld_out;
+        J->n_out = adjoint ? e->K : e->L;
+        J->X = e->X + (size_t)s * e->ldS;
+        J->ncols = ncols;
+        J->N = e->N;
+        J->L = e->L;
+        J->K = e->K;
+    }
+    void *d = ssae_push_jobs(e, jobs, sizeof(ssa_col_job) * nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_CORR);
+    int rc_ = ssad_corr((const ssa_col_job *)d, nb, ncols, e->logh, e->st);
+    ssae_prof_end(e);
+    return rc_;
+}
+
+/* X_s -= Q_s (Q_s^T X_s): Q_s m x nq (ldq), X_s m x nx (ldx); FP64-accumulated cross products. */
+static int deflate(ssa_engine *e, int nb, float *Xm, size_t xs, long long ldx, int nx, const float *Q, size_t qs,
+                   long long ldq, int nq, int m, int rows)
+{
+    const int nch = (m + rows - 1) / rows;
+    const int nchx = imax(e->nch_L, e->nch_K);
+    ssa_xgram_job *xg = (ssa_xgram_job *)calloc((size_t)nb, sizeof(ssa_xgram_job));
+    ssa_xreduce_job *xr = (ssa_xreduce_job *)calloc((size_t)nb, sizeof(ssa_xreduce_job));
+    if (!xg || !xr)
+    {
+        free(xg);
+        free(xr);
+        return (int)cudaErrorMemoryAllocation;
+    }
+    for (int s = 0; s < nb; s++)
+    {
+        xg[s].A = Q + (size_t)s * qs;
+        xg[s].B = Xm + (size_t)s * xs;
+        xg[s].part = e->xpart + (size_t)s * nchx * SSA_MAX_KP * SSA_MAX_KP;
+        xg[s].lda = ldq;
+        xg[s].ldb = ldx;
+        xg[s].m = m;
+        xg[s].na = nq;
+        xg[s].nb = nx;
+        xg[s].rows_per_cta = rows;
+        xr[s].part = xg[s].part;
+        xr[s].out = e->xC + (size_t)s * SSA_MAX_KP * SSA_MAX_KP;
+        xr[s].nchunks = nch;
+        xr[s].na = nq;
+        xr[s].nb = nx;
+    }
+    void *dg = ssae_push_jobs(e, xg, sizeof(ssa_xgram_job) * nb);
+    void *dr = ssae_push_jobs(e, xr, sizeof(ssa_xreduce_job) * nb);
+    free(xg);
+    free(xr);
+    if (!dg || !dr)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_GRAM);
+    int rc = ssad_xgram((const ssa_xgram_job *)dg, nb, nch, e->st);
+    ssae_prof_end(e);
+    CK(rc);
+    ssae_prof_begin(e, SSAK_GRAM);
+    rc = ssad_xreduce((const ssa_xreduce_job *)dr, nb, e->st);
+    ssae_prof_end(e);
+    CK(rc);
+    /* X = X - Q C */
+    ssa_rowmul_job *rj = (ssa_rowmul_job *)calloc((size_t)nb, sizeof(ssa_rowmul_job));
+    if (!rj)
+        return (int)cudaErrorMemoryAllocation;
+    for (int s = 0; s < nb; s++)
+    {
+        ssa_rowmul_job *J = &rj[s];
+        J->A = Q + (size_t)s * qs;
+        J->Bm = e->xC + (size_t)s * SSA_MAX_KP * SSA_MAX_KP;
+        J->C = Xm + (size_t)s * xs;
+        J->sub = Xm + (size_t)s * xs;
+        J->lda = ldq;
+        J->ldc = ldx;
+        J->ldsub = ldx;
+        J->m = m;
+        J->n = nq;
+        J->p = nx;
+        J->ldb = nq;
+    }
+    void *d = ssae_push_jobs(e, rj, sizeof(ssa_rowmul_job) * nb);
+    free(rj);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_ROWMUL);
+    rc = ssad_rowmul((const ssa_rowmul_job *)d, nb, m, nq, e->st);
+    ssae_prof_end(e);
+    return rc;
+}
+
+int ssae_decompose_block(ssa_engine *e, int nb, int k, int bsize, int max_iter, const float *d_V0, long long v0_ld,
+                         unsigned long long seed)
+{
+    const int L = e->L, K = e->K;
+    if (nb < 1 || nb > e->B || k < 1 || bsize < 1 || max_iter < 0)
+        return (int)cudaErrorInvalidValue;
+    k = imin(k, imin(L, K));
+    const int b = imin(bsize, k);
+    if (k > e->kp || k > e->k || b > SSA_MAX_KP)
+        return (int)cudaErrorInvalidValue;
+    CK(ssae_ensure_block(e, b));
+    CK(cudaMemsetAsync(e->status, 0, sizeof(int) * nb, e->st));
+    const size_t sY = (size_t)e->ldL * e->kp, sZ = (size_t)e->ldK * e->kp;
+    const size_t sUb = (size_t)e->ldL * 2 * e->bcap, sVb = (size_t)e->ldK * e->bcap;
+    float *Ub = e->Ub, *Ub2 = e->Ub + (size_t)e->ldL * e->bcap, *Vb = e->Vb;
+    const size_t s64 = (size_t)SSA_MAX_KP * SSA_MAX_KP;
+    int comp = 0;
+    while (comp < k)
+    {
+        const int cb = imin(b, k - comp);
+        /* start block */
+        for (int s = 0; s < nb; s++)
+        {
+            if (d_V0)
+                CK(cudaMemcpy2DAsync(Vb + (size_t)s * sVb, sizeof(float) * e->ldK,
+                                     d_V0 + (size_t)s * v0_ld * k + (size_t)comp * v0_ld, sizeof(float) * v0_ld,
+                                     sizeof(float) * K, cb, cudaMemcpyDeviceToDevice, e->st));
+            else
+                CK(ssad_gaussian(Vb + (size_t)s * sVb, e->ldK, K, cb, comp,
+                                 seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(s + 1)), e->st));
+        }
+        if (comp > 0)
+            CK(deflate(e, nb, Vb, sVb, e->ldK, cb, e->Z, sZ, e->ldK, comp, K, e->rows_K));
+        CK(cholqr_pass(e, nb, Vb, sVb, e->ldK, K, cb, e->rows_K, NULL));
+        CK(cholqr_pass(e, nb, Vb, sVb, e->ldK, K, cb, e->rows_K, NULL));
+        for (int it = 0; it < max_iter; it++)
+        {
+            const int last = it == max_iter - 1;
+            /* FP32 iterates are re-orthonormalised every half-step (the reference: every fifth),
+             * which keeps the subspaces identical and avoids FP32 overflow. */
+            CK(corr_io(e, nb, cb, 0, Vb, sVb, e->ldK, Ub, sUb, e->ldL));
+            if (comp > 0)
+                CK(deflate(e, nb, Ub, sUb, e->ldL, cb, e->Y, sY, e->ldL, comp, L, e->rows_L));
+            CK(cholqr_pass(e, nb, Ub, sUb, e->ldL, L, cb, e->rows_L, NULL));
+            if (last)
+                CK(cholqr_pass(e, nb, Ub, sUb, e->ldL, L, cb, e->rows_L, NULL));
+            CK(corr_io(e, nb, cb, 1, Ub, sUb, e->ldL, Vb, sVb, e->ldK));
+            if (comp > 0)
+                CK(deflate(e, nb, Vb, sVb, e->ldK, cb, e->Z, sZ, e->ldK, comp, K, e->rows_K));
+            CK(cholqr_pass(e, nb, Vb, sVb, e->ldK, K, cb, e->rows_K, NULL));
+            if (last)
+                CK(cholqr_pass(e, nb, Vb, sVb, e->ldK, K, cb, e->rows_K, NULL));
+        }
+        /* U_block2 = H V_block (deflated); M = U_block^T U_block2 = Us S Vs^T */
+        CK(corr_io(e, nb, cb, 0, Vb, sVb, e->ldK, Ub2, sUb, e->ldL));
+        if (comp > 0)
+            CK(deflate(e, nb, Ub2, sUb, e->ldL, cb, e->Y, sY, e->ldL, comp, L, e->rows_L));
+        {
+            const int nch = (L + e->rows_L - 1) / e->rows_L;
+            const int nchx = imax(e->nch_L, e->nch_K);
+            ssa_xgram_job *xg = (ssa_xgram_job *)calloc((size_t)nb, sizeof(ssa_xgram_job));
+            ssa_svd_job *sv = (ssa_svd_job *)calloc((size_t)nb, sizeof(ssa_svd_job));
+            if (!xg || !sv)
+            {
+                free(xg);
+                free(sv);
+                return (int)cudaErrorMemoryAllocation;
+            }
+            for (int s = 0; s < nb; s++)
+            {
+                xg[s].A = Ub + (size_t)s * sUb;
+                xg[s].B = Ub2 + (size_t)s * sUb;
+                xg[s].part = e->xpart + (size_t)s * nchx * s64;
+                xg[s].lda = e->ldL;
+                xg[s].ldb = e->ldL;
+                xg[s].m = L;
+                xg[s].na = cb;
+                xg[s].nb = cb;
+                xg[s].rows_per_cta = e->rows_L;
+                sv[s].part = xg[s].part;
+                sv[s].sigma = e->sigma + (size_t)s * e->k + comp;
+                sv[s].Us = e->sUs + (size_t)s * s64;
+                sv[s].Vs = e->sVs + (size_t)s * s64;
+                sv[s].Dinv = e->sDinv + (size_t)s * s64;
+                sv[s].status = e->status + s;
+                sv[s].nchunks = nch;
+                sv[s].n = cb;
+            }
+            void *dg = ssae_push_jobs(e, xg, sizeof(ssa_xgram_job) * nb);
+            void *ds = ssae_push_jobs(e, sv, sizeof(ssa_svd_job) * nb);
+            free(xg);
+            free(sv);
+            if (!dg || !ds)
+                return (int)cudaErrorMemoryAllocation;
+            ssae_prof_begin(e, SSAK_GRAM);
+            int rc = ssad_xgram((const ssa_xgram_job *)dg, nb, nch, e->st);
+            ssae_prof_end(e);
+            CK(rc);
+            ssae_prof_begin(e, SSAK_RR);
+            rc = ssad_svdsmall((const ssa_svd_job *)ds, nb, e->st);
+            ssae_prof_end(e);
+            CK(rc);
+        }
+        /* U[:, comp:comp+cb] = U_block Us */
+        CK(rowmul(e, nb, Ub, sUb, e->ldL, L, cb, e->sUs, s64, cb, cb, e->Y + (size_t)comp * e->ldL, sY, e->ldL,
+                  NULL, 0));
+        /* V_block = H^T U[:, comp:comp+cb] (deflated); V[:, comp:comp+cb] = V_block Sigma^{-1} */
+        CK(corr_io(e, nb, cb, 1, e->Y + (size_t)comp * e->ldL, sY, e->ldL, Vb, sVb, e->ldK));
+        if (comp > 0)
+            CK(deflate(e, nb, Vb, sVb, e->ldK, cb, e->Z, sZ, e->ldK, comp, K, e->rows_K));
+        CK(rowmul(e, nb, Vb, sVb, e->ldK, K, cb, e->sDinv, s64, cb, cb, e->Z + (size_t)comp * e->ldK, sZ, e->ldK,
+                  NULL, 0));
+        comp += cb;
+    }
+    /* exchange sort by sigma and sign rule (MKL/ssa_opt.h:1896-1919) */
+    {
+        ssa_sortsign_job *ss = (ssa_sortsign_job *)calloc((size_t)nb, sizeof(ssa_sortsign_job));
+        ssa_permcols_job *pc = (ssa_permcols_job *)calloc((size_t)nb * 4, sizeof(ssa_permcols_job));
+        if (!ss || !pc)
+        {
+            free(ss);
+            free(pc);
+            return (int)cudaErrorMemoryAllocation;
+        }
+        for (int s = 0; s < nb; s++)
+        {
+            ss[s].U = e->Y + (size_t)s * sY;
+            ss[s].sigma = e->sigma + (size_t)s * e->k;
+            ss[s].perm = e->perm + (size_t)s * SSA_MAX_KP;
+            ss[s].sign = e->sgn + (size_t)s * SSA_MAX_KP;
+            ss[s].ldU = e->ldL;
+            ss[s].L = L;
+            ss[s].k = k;
+            /* Y -> Ut and Z -> Vt permuted, then copied back unpermuted-identity */
+            ssa_permcols_job *a = &pc[4 * s];
+            a[0].src = e->Y + (size_t)s * sY;
+            a[0].dst = e->Ut + (size_t)s * sY;
+            a[0].lds = a[0].ldd = e->ldL;
+            a[0].m = L;
+            a[1].src = e->Z + (size_t)s * sZ;
+            a[1].dst = e->Vt + (size_t)s * sZ;
+            a[1].lds = a[1].ldd = e->ldK;
+            a[1].m = K;
+            for (int t = 0; t < 2; t++)
+            {
+                a[t].perm = ss[s].perm;
+                a[t].sign = ss[s].sign;
+                a[t].k = k;
+            }
+        }
+        void *dss = ssae_push_jobs(e, ss, sizeof(ssa_sortsign_job) * nb);
+        free(ss);
+        if (!dss)
+        {
+            free(pc);
+            return (int)cudaErrorMemoryAllocation;
+        }
+        ssae_prof_begin(e, SSAK_RR);
+        int rc = ssad_sortsign((const ssa_sortsign_job *)dss, nb, e->st);
+        ssae_prof_end(e);
+        if (rc)
+        {
+            free(pc);
+            return rc;
+        }
+        /* permute U and V into the staging buffers, then copy them back */
+        ssa_permcols_job *pu = (ssa_permcols_job *)calloc((size_t)nb, sizeof(ssa_permcols_job));
+        ssa_permcols_job *pv = (ssa_permcols_job *)calloc((size_t)nb, sizeof(ssa_permcols_job));
+        if (!pu || !pv)
+        {
+            free(pc);
+            free(pu);
+            free(pv);
+            return (int)cudaErrorMemoryAllocation;
+        }
+        for (int s = 0; s < nb; s++)
+        {
+            pu[s] = pc[4 * s];
+            pv[s] = pc[4 * s + 1];
+        }
+        free(pc);
+        void *dpu = ssae_push_jobs(e, pu, sizeof(ssa_permcols_job) * nb);
+        void *dpv = ssae_push_jobs(e, pv, sizeof(ssa_permcols_job) * nb);
+        free(pu);
+        free(pv);
+        if (!dpu || !dpv)
+            return (int)cudaErrorMemoryAllocation;
+        CK(ssad_permcols((const ssa_permcols_job *)dpu, nb, L, e->st));
+        CK(ssad_permcols((const ssa_permcols_job *)dpv, nb, K, e->st));
+        for (int s = 0; s < nb; s++)
+        {
+            CK(cudaMemcpy2DAsync(e->Y + (size_t)s * sY, sizeof(float) * e->ldL, e->Ut + (size_t)s * sY,
+                                 sizeof(float) * e->ldL, sizeof(float) * L, k, cudaMemcpyDeviceToDevice, e->st));
+            CK(cudaMemcpy2DAsync(e->Z + (size_t)s * sZ, sizeof(float) * e->ldK, e->Vt + (size_t)s * sZ,
+                                 sizeof(float) * e->ldK, sizeof(float) * K, k, cudaMemcpyDeviceToDevice, e->st));
+        }
+    }
+    return 0;
 }

@@ -74,6 +74,15 @@ typedef struct
     double *norm2;               /* B * k */
     double *W;                   /* B * k * k */
     float *Us, *Vs;              /* cached spectra B * k * ldS (allocated on demand) */
+    /* block power scratch (allocated on demand by ssae_decompose_block) */
+    int bcap;                    /* block columns the scratch holds */
+    float *Ub, *Vb;              /* B * ldL * 2 bcap, B * ldK * bcap */
+    double *xpart;               /* B * max(nch_L, nch_K) * 64 * 64 cross Gram partials */
+    float *xC;                   /* B * 64 * 64 deflation coefficients */
+    float *sUs, *sVs, *sDinv;    /* B * 64 * 64 small SVD factors */
+    int *perm;                   /* B * 64 */
+    float *sgn;                  /* B * 64 */
+    float *Ut, *Vt;              /* B * ldL * k, B * ldK * k permutation staging */
     ssa_job_arena ja;
     /* SSA_SYNC_CHECK=1 in the environment: wait after every launch and report the first
      * failing stage on stderr (debugging aid; off by default) */
@@ -114,6 +123,14 @@ int ssae_spectra(ssa_engine *e, int nb, int k);
 /* One correlation sweep on series 0 over `ncols` columns already in Z (forward: Y = H Z) or
  * Y (adjoint: Z = H^T Y). */
 int ssae_matvec(ssa_engine *e, int ncols, int adjoint);
+/* Block power iteration with Rayleigh-Ritz (reference MKL/ssa_opt.h:1765-1933) for nb
+ * series: k components in blocks of bsize, max_iter iterations per block, deflation against the
+ * finished components. d_V0: device K x k start blocks per series (stride v0_ld * k, leading
+ * dimension v0_ld; block i = columns of that block), or NULL for the device generator. Results
+ * in Y (U), Z (V), sigma; sorted by sigma with the reference's sign rule. */
+int ssae_decompose_block(ssa_engine *e, int nb, int k, int bsize, int max_iter, const float *d_V0,
+                         long long v0_ld, unsigned long long seed);
+int ssae_ensure_block(ssa_engine *e, int bcap);
 /* Grouped reconstruction of series s from cached spectra into d_out (double, N). */
 int ssae_recon_group(ssa_engine *e, int s, int k, const int *d_group, int n_group, double *d_out);
 

@@ -497,7 +497,6 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_chol(const ssa_chol_job* __re
     extern __shared__ double dsm[];
     __shared__ double red[32];
     double* G = dsm;
-    double* X = dsm + SSA_MAX_KP * SLD;
     const ssa_chol_job J = jobs[blockIdx.x];
     const int n = J.n;
     reduce_packed(J.part, J.nchunks, n, G);
@@ -508,22 +507,9 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_chol(const ssa_chol_job* __re
     }
     const double floor_ = dmax > 0.0 ? dmax * 1e-13 * (double)n : 1.0;
     chol_upper_inplace(G, n, floor_);
-    // X = R^{-1} (upper), row by row from the bottom: X[i][c] = (delta_ic - sum_{l=i+1..c}
-    // R[i][l] X[l][c]) / R[i][i]; R[i][l] sits at G[l * SLD + i], X[l][c] at X[c * SLD + l].
-    for (int e = threadIdx.x; e < SSA_MAX_KP * SLD; e += blockDim.x) X[e] = 0.0;
-    __syncthreads();
-    for (int i = n - 1; i >= 0; --i) {
-        const double rii = G[i * SLD + i];
-        for (int c = i + threadIdx.x; c < n; c += blockDim.x) {
-            double sacc = (c == i) ? 1.0 : 0.0;
-            for (int l = i + 1; l <= c; ++l) sacc -= G[l * SLD + i] * X[c * SLD + l];
-            X[c * SLD + i] = sacc / rii;
-        }
-        __syncthreads();
-    }
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int c = e / n, r = e - c * n;
-        J.R[e] = (float)X[c * SLD + r];
+        J.R[e] = (float)G[c * SLD + r];
     }
 }
 
@@ -531,74 +517,89 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_chol(const ssa_chol_job* __re
 // Row-by-row product with a small matrix: C[i, :p] = A[i, :n] Bm
 // ---------------------------------------------------------------------------------------------
 
-// C[r, 0:p] = A[r, 0:n] M for the SSA_ROWMUL_ROWS rows of one tile. Thread (g, j) owns output
-// column j (M[:, j] in registers) for the rows r = g, g + 2, ...; rows are read from a
-// row-major shared copy of the tile as broadcast float4s, four rows at a time so that four
-// independent FMA chains are in flight. Outputs go through shared memory so that the global
-// stores stay coalesced along the columns. In place (C == A) is safe: the tile is in shared
-// memory before any output is written.
-#define ROWMUL_THREADS 128
-#define RM_AST 68  // row stride of the shared A tile (floats, multiple of 4)
-#define RM_SMEM ((SSA_ROWMUL_ROWS * RM_AST + SSA_ROWMUL_ROWS * (SSA_MAX_KP + 1)) * (int)sizeof(float))
+#define ROWMUL_THREADS SSA_ROWMUL_ROWS
 
 __global__ void __launch_bounds__(ROWMUL_THREADS) k_rowmul(const ssa_rowmul_job* __restrict__ jobs) {
-    extern __shared__ float rsm[];
-    float* As = rsm;                               // [row][l], stride RM_AST
-    float* Cs = rsm + SSA_ROWMUL_ROWS * RM_AST;    // [row][j], stride SSA_MAX_KP + 1
-    __shared__ double csum[2][SSA_MAX_KP];
+    __shared__ __align__(16) float sB[SSA_MAX_KP * SSA_MAX_KP];
+    __shared__ float sInv[SSA_MAX_KP];
+    __shared__ double wsum[ROWMUL_THREADS / 32][SSA_MAX_KP];
     const ssa_rowmul_job J = jobs[blockIdx.y];
     const int n = J.n, p = J.p;
-    const int r0 = blockIdx.x * SSA_ROWMUL_ROWS;
-    if (r0 >= J.m) return;
-    const int rows = min(SSA_ROWMUL_ROWS, J.m - r0);
-    // stage the tile (coalesced along rows), zero-padded to 64 columns and SSA_ROWMUL_ROWS rows
-    for (int e = threadIdx.x; e < SSA_ROWMUL_ROWS * SSA_MAX_KP; e += blockDim.x) {
-        const int l = e / SSA_ROWMUL_ROWS, r = e - l * SSA_ROWMUL_ROWS;
-        float v = 0.f;
-        if (l < n && r < rows) v = J.A[(long long)(r0 + r) + (long long)l * J.lda];
-        As[r * RM_AST + l] = v;
+    if (blockIdx.x * ROWMUL_THREADS >= J.m) return;
+    for (int e = threadIdx.x; e < SSA_MAX_KP * p; e += blockDim.x) {
+        const int j = e / SSA_MAX_KP, l = e - j * SSA_MAX_KP;
+        sB[e] = l < n ? J.Bm[l + j * J.ldb] : 0.f;
     }
-    const int j = threadIdx.x & 63, g = threadIdx.x >> 6;
-    float mcol[SSA_MAX_KP];
-#pragma unroll
-    for (int l = 0; l < SSA_MAX_KP; ++l) mcol[l] = (j < p && l < n) ? J.Bm[l + j * J.ldb] : 0.f;
+    if (J.trsm)
+        for (int j = threadIdx.x; j < SSA_MAX_KP; j += blockDim.x) sInv[j] = j < n ? 1.0f / J.Bm[j + j * J.ldb] : 0.f;
     __syncthreads();
-    double cs = 0.0;
-    for (int r = g * 4; r < SSA_ROWMUL_ROWS; r += 8) {
-        const float* a0 = As + r * RM_AST;
-        float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
+    const int i = blockIdx.x * ROWMUL_THREADS + threadIdx.x;
+    const bool live = i < J.m;
+    float a[SSA_MAX_KP];
 #pragma unroll
-        for (int l = 0; l < SSA_MAX_KP; l += 4) {
-            const float4 x0 = *reinterpret_cast<const float4*>(a0 + l);
-            const float4 x1 = *reinterpret_cast<const float4*>(a0 + RM_AST + l);
-            const float4 x2 = *reinterpret_cast<const float4*>(a0 + 2 * RM_AST + l);
-            const float4 x3 = *reinterpret_cast<const float4*>(a0 + 3 * RM_AST + l);
-            c0 = fmaf(x0.x, mcol[l], c0); c0 = fmaf(x0.y, mcol[l + 1], c0);
-            c0 = fmaf(x0.z, mcol[l + 2], c0); c0 = fmaf(x0.w, mcol[l + 3], c0);
-            c1 = fmaf(x1.x, mcol[l], c1); c1 = fmaf(x1.y, mcol[l + 1], c1);
-            c1 = fmaf(x1.z, mcol[l + 2], c1); c1 = fmaf(x1.w, mcol[l + 3], c1);
-            c2 = fmaf(x2.x, mcol[l], c2); c2 = fmaf(x2.y, mcol[l + 1], c2);
-            c2 = fmaf(x2.z, mcol[l + 2], c2); c2 = fmaf(x2.w, mcol[l + 3], c2);
-            c3 = fmaf(x3.x, mcol[l], c3); c3 = fmaf(x3.y, mcol[l + 1], c3);
-            c3 = fmaf(x3.z, mcol[l + 2], c3); c3 = fmaf(x3.w, mcol[l + 3], c3);
+    for (int l = 0; l < SSA_MAX_KP; ++l)
+        a[l] = (live && l < n) ? J.A[(long long)i + (long long)l * J.lda] : 0.f;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (J.trsm) {
+        // x R = a, R upper: x_j = (a_j - sum_{l<j} x_l R[l][j]) / R[j][j]; a is overwritten by x
+#pragma unroll
+        for (int j = 0; j < SSA_MAX_KP; ++j) {
+            if (j < n) {
+                const float* b = sB + j * SSA_MAX_KP;
+                float s0 = a[j], s1 = 0.f;
+                // float4 broadcast loads: one shared-memory wavefront feeds four FMAs per lane
+#pragma unroll
+                for (int l = 0; l < (j & ~3); l += 4) {
+                    const float4 bv = *reinterpret_cast<const float4*>(b + l);
+                    s0 = fmaf(-a[l], bv.x, s0);
+                    s1 = fmaf(-a[l + 1], bv.y, s1);
+                    s0 = fmaf(-a[l + 2], bv.z, s0);
+                    s1 = fmaf(-a[l + 3], bv.w, s1);
+                }
+#pragma unroll
+                for (int l = (j & ~3); l < j; ++l) s0 = fmaf(-a[l], b[l], s0);
+                const float c = (s0 + s1) * sInv[j];
+                a[j] = c;
+                if (live) J.C[(long long)i + (long long)j * J.ldc] = c;  // subtract mode is GEMM-only
+                if (J.colsum) {
+                    double v = live ? (double)c : 0.0;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                    if (lane == 0) wsum[warp][j] = v;
+                }
+            }
         }
-        float* cr = Cs + r * (SSA_MAX_KP + 1) + j;
-        cr[0] = c0;
-        cr[SSA_MAX_KP + 1] = c1;
-        cr[2 * (SSA_MAX_KP + 1)] = c2;
-        cr[3 * (SSA_MAX_KP + 1)] = c3;
-        if (r < rows) cs += (double)c0;
-        if (r + 1 < rows) cs += (double)c1;
-        if (r + 2 < rows) cs += (double)c2;
-        if (r + 3 < rows) cs += (double)c3;
+    } else {
+        for (int j = 0; j < p; ++j) {
+            const float* b = sB + j * SSA_MAX_KP;
+            float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+            for (int l = 0; l < SSA_MAX_KP; l += 4) {
+                const float4 bv = *reinterpret_cast<const float4*>(b + l);
+                s0 = fmaf(a[l], bv.x, s0);
+                s1 = fmaf(a[l + 1], bv.y, s1);
+                s0 = fmaf(a[l + 2], bv.z, s0);
+                s1 = fmaf(a[l + 3], bv.w, s1);
+            }
+            float c = s0 + s1;
+            if (J.sub && live) c = J.sub[(long long)i + (long long)j * J.ldsub] - c;
+            if (live) J.C[(long long)i + (long long)j * J.ldc] = c;
+            if (J.colsum) {
+                double v = live ? (double)c : 0.0;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                if (lane == 0) wsum[warp][j] = v;
+            }
+        }
     }
-    if (J.colsum) csum[g][j] = cs;
-    __syncthreads();
-    for (int e = threadIdx.x; e < SSA_ROWMUL_ROWS * p; e += blockDim.x) {
-        const int jj = e / SSA_ROWMUL_ROWS, r = e - jj * SSA_ROWMUL_ROWS;
-        if (r < rows) J.C[(long long)(r0 + r) + (long long)jj * J.ldc] = Cs[r * (SSA_MAX_KP + 1) + jj];
+    if (J.colsum) {
+        __syncthreads();
+        for (int j = threadIdx.x; j < p; j += blockDim.x) {
+            double t = 0.0;
+            for (int w = 0; w < ROWMUL_THREADS / 32; ++w) t += wsum[w][j];
+            J.colsum[(long long)blockIdx.x * p + j] = t;
+        }
     }
-    if (J.colsum && threadIdx.x < p) J.colsum[(long long)blockIdx.x * p + threadIdx.x] = csum[0][threadIdx.x] + csum[1][threadIdx.x];
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -606,6 +607,86 @@ __global__ void __launch_bounds__(ROWMUL_THREADS) k_rowmul(const ssa_rowmul_job*
 // ---------------------------------------------------------------------------------------------
 
 #define RR_THREADS 512
+
+// One-sided (Hestenes) Jacobi on the n columns of A (column c at A + c * SLD, FP64, shared
+// memory): A <- A J with J a product of plane rotations accumulated into Z (initialised by the
+// caller), until every column pair is orthogonal to 1e-15 relative. Round-robin pairing, one
+// warp per pair, lanes own rows lane and lane + 32. perm needs n + 1 ints; on return nrm[c] =
+// ||A[:, c]||. Called by every thread of the block.
+__device__ void onesided_jacobi(double* A, double* Z, int n, int* perm, int* notconv, double* nrm) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int ne = (n + 1) & ~1;  // even count; index n is a dummy when n is odd
+    for (int i = threadIdx.x; i < ne; i += blockDim.x) perm[i] = i;
+    __syncthreads();
+    const int npairs = ne / 2;
+    const double tiny = 1e-300;
+    for (int sweep = 0; sweep < 40; ++sweep) {
+        if (threadIdx.x == 0) *notconv = 0;
+        __syncthreads();
+        for (int step = 0; step < ne - 1; ++step) {
+            for (int t = warp; t < npairs; t += nw) {
+                int p = perm[t], q = perm[ne - 1 - t];
+                if (q >= n || p >= n) continue;
+                if (p < 0 || q < 0) {
+                    if (lane == 0) check_fail(6, 6, (unsigned)(p * 1000 + q));
+                    continue;
+                }
+                double* ap = A + p * SLD;
+                double* aq = A + q * SLD;
+                double al = 0.0, be = 0.0, ga = 0.0;
+                for (int r = lane; r < n; r += 32) {
+                    const double x = ap[r], y = aq[r];
+                    al = fma(x, x, al);
+                    be = fma(y, y, be);
+                    ga = fma(x, y, ga);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    al += __shfl_xor_sync(0xffffffffu, al, o);
+                    be += __shfl_xor_sync(0xffffffffu, be, o);
+                    ga += __shfl_xor_sync(0xffffffffu, ga, o);
+                }
+                if (fabs(ga) > tiny && fabs(ga) > 1e-15 * sqrt(al * be)) {
+                    if (lane == 0) *notconv = 1;
+                    const double zeta = (be - al) / (2.0 * ga);
+                    const double tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                    const double cs = 1.0 / sqrt(1.0 + tt * tt);
+                    const double sn = cs * tt;
+                    double* zp = Z + p * SLD;
+                    double* zq = Z + q * SLD;
+                    for (int r = lane; r < n; r += 32) {
+                        const double x = ap[r], y = aq[r];
+                        ap[r] = cs * x - sn * y;
+                        aq[r] = sn * x + cs * y;
+                        const double u = zp[r], v = zq[r];
+                        zp[r] = cs * u - sn * v;
+                        zq[r] = sn * u + cs * v;
+                    }
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {  // round-robin: keep perm[0], rotate perm[1..ne-1]
+                const int last = perm[ne - 1];
+                for (int i = ne - 1; i > 1; --i) perm[i] = perm[i - 1];
+                perm[1] = last;
+            }
+            __syncthreads();
+        }
+        // Every thread reads the flag before thread 0 may reset it for the next sweep; otherwise
+        // warps could leave the loop at different sweeps and desynchronise the barriers.
+        const bool converged = !*notconv;
+        __syncthreads();
+        if (converged) break;
+    }
+    for (int c = warp; c < n; c += nw) {
+        double s = 0.0;
+        for (int r = lane; r < n; r += 32) s = fma(A[c * SLD + r], A[c * SLD + r], s);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) nrm[c] = sqrt(s);
+    }
+    __syncthreads();
+}
 
 // Rayleigh-Ritz: B^T B = R^T R (FP64 Cholesky), then one-sided (Hestenes) Jacobi on the
 // columns of R: R Z = W Sigma with orthonormal Z, so B^T B = Z Sigma^2 Z^T. One warp per column
@@ -643,82 +724,13 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr(const ssa_rr_job* __restrict_
         for (int c = 0; c < J.nchunks_q; ++c) s += J.qsum[(long long)c * n + l];
         qs[l] = s;
     }
-    const int ne = (n + 1) & ~1;  // even count; index n is a dummy when n is odd
-    for (int i = threadIdx.x; i < ne; i += blockDim.x) perm[i] = i;
     __syncthreads();
     const double dmax = diag_max(A, n, red);
     if (dmax < 0.0) {
         if (threadIdx.x == 0 && J.status) atomicOr(J.status, 2);
     }
     chol_upper_inplace(A, n, dmax > 0.0 ? dmax * 1e-15 : 1.0);
-    const int npairs = ne / 2;
-    const double tiny = 1e-300;
-    for (int sweep = 0; sweep < 40; ++sweep) {
-        if (threadIdx.x == 0) notconv = 0;
-        __syncthreads();
-        for (int step = 0; step < ne - 1; ++step) {
-            for (int t = warp; t < npairs; t += nw) {
-                int p = perm[t], q = perm[ne - 1 - t];
-                if (q >= n || p >= n) continue;
-                if (p < 0 || q < 0) {
-                    if (lane == 0) check_fail(6, 6, (unsigned)(p * 1000 + q));
-                    continue;
-                }
-                double* ap = A + p * SLD;
-                double* aq = A + q * SLD;
-                double al = 0.0, be = 0.0, ga = 0.0;
-                for (int r = lane; r < n; r += 32) {
-                    const double x = ap[r], y = aq[r];
-                    al = fma(x, x, al);
-                    be = fma(y, y, be);
-                    ga = fma(x, y, ga);
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    al += __shfl_xor_sync(0xffffffffu, al, o);
-                    be += __shfl_xor_sync(0xffffffffu, be, o);
-                    ga += __shfl_xor_sync(0xffffffffu, ga, o);
-                }
-                if (fabs(ga) > tiny && fabs(ga) > 1e-15 * sqrt(al * be)) {
-                    if (lane == 0) notconv = 1;
-                    const double zeta = (be - al) / (2.0 * ga);
-                    const double tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-                    const double cs = 1.0 / sqrt(1.0 + tt * tt);
-                    const double sn = cs * tt;
-                    double* zp = Z + p * SLD;
-                    double* zq = Z + q * SLD;
-                    for (int r = lane; r < n; r += 32) {
-                        const double x = ap[r], y = aq[r];
-                        ap[r] = cs * x - sn * y;
-                        aq[r] = sn * x + cs * y;
-                        const double u = zp[r], v = zq[r];
-                        zp[r] = cs * u - sn * v;
-                        zq[r] = sn * u + cs * v;
-                    }
-                }
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) {  // round-robin: keep perm[0], rotate perm[1..ne-1]
-                const int last = perm[ne - 1];
-                for (int i = ne - 1; i > 1; --i) perm[i] = perm[i - 1];
-                perm[1] = last;
-            }
-            __syncthreads();
-        }
-        // Every thread reads the flag before thread 0 may reset it for the next sweep; otherwise
-        // warps could leave the loop at different sweeps and desynchronise the barriers.
-        const bool converged = !notconv;
-        __syncthreads();
-        if (converged) break;
-    }
-    // sigma_c = ||A[:, c]||
-    for (int c = warp; c < n; c += nw) {
-        double s = 0.0;
-        for (int r = lane; r < n; r += 32) s = fma(A[c * SLD + r], A[c * SLD + r], s);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) nrm[c] = sqrt(s);
-    }
+    onesided_jacobi(A, Z, n, perm, &notconv, nrm);
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int i = 0; i < n; ++i) order[i] = i;
@@ -745,7 +757,7 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr(const ssa_rr_job* __restrict_
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
         const double sgn = dot < 0.0 ? -1.0 : 1.0;
-        const double isg = sg > tiny ? 1.0 / sg : 0.0;
+        const double isg = sg > 1e-300 ? 1.0 / sg : 0.0;
         for (int l = lane; l < n; l += 32) {
             const double z = sgn * Z[col * SLD + l];
             J.Zu[l + j * n] = (float)z;
@@ -756,6 +768,206 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr(const ssa_rr_job* __restrict_
             if (!isfinite(sg) && J.status) atomicOr(J.status, 2);
         }
     }
+}
+
+
+// ---------------------------------------------------------------------------------------------
+// Block power iteration support (reference MKL/ssa_opt.h:1765-1933): cross Grams for deflation
+// and the block Rayleigh quotient, small SVD, final ordering
+// ---------------------------------------------------------------------------------------------
+
+#define XG_SMEM (2 * SSA_MAX_KP * GSTR * (int)sizeof(float))
+
+__global__ void __launch_bounds__(GRAM_THREADS) k_xgram(const ssa_xgram_job* __restrict__ jobs) {
+    extern __shared__ float xsm[];
+    float* sA = xsm;
+    float* sB = xsm + SSA_MAX_KP * GSTR;
+    const ssa_xgram_job J = jobs[blockIdx.y];
+    const int chunk = blockIdx.x;
+    const int r_begin = chunk * J.rows_per_cta;
+    if (r_begin >= J.m) return;
+    const int r_end = min(J.m, r_begin + J.rows_per_cta);
+    const int na = J.na, nb = J.nb;
+    const int tba = (na + 3) >> 2, tbb = (nb + 3) >> 2;
+    const int ntiles = tba * tbb;
+    double acc[2][4][4];
+    int ti[2], tj[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int t = threadIdx.x + q * GRAM_THREADS;
+        ti[q] = t < ntiles ? t / tbb : -1;
+        tj[q] = t < ntiles ? t - (t / tbb) * tbb : -1;
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[q][a][b] = 0.0;
+    }
+    for (int r0 = r_begin; r0 < r_end; r0 += SSA_GRAM_CHUNK) {
+        const int rows = min(SSA_GRAM_CHUNK, r_end - r0);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < SSA_MAX_KP * SSA_GRAM_CHUNK; idx += GRAM_THREADS) {
+            const int col = idx / SSA_GRAM_CHUNK, r = idx - col * SSA_GRAM_CHUNK;
+            float va = 0.f, vb = 0.f;
+            if (r < rows) {
+                if (col < na) va = J.A[(long long)(r0 + r) + (long long)col * J.lda];
+                if (col < nb) vb = J.B[(long long)(r0 + r) + (long long)col * J.ldb];
+            }
+            sA[col * GSTR + r] = va;
+            sB[col * GSTR + r] = vb;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            if (ti[q] < 0) continue;
+            const float* pa = sA + (ti[q] * 4) * GSTR;
+            const float* pb = sB + (tj[q] * 4) * GSTR;
+            for (int r = 0; r < rows; ++r) {
+                double x[4], y[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    x[u] = (double)pa[u * GSTR + r];
+                    y[u] = (double)pb[u * GSTR + r];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) acc[q][u][v] = fma(x[u], y[v], acc[q][u][v]);
+            }
+        }
+    }
+    double* part = J.part + (long long)chunk * na * nb;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        if (ti[q] < 0) continue;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int i = ti[q] * 4 + u, j = tj[q] * 4 + v;
+                if (i < na && j < nb) part[i * nb + j] = acc[q][u][v];
+            }
+    }
+}
+
+__global__ void k_xreduce(const ssa_xreduce_job* __restrict__ jobs) {
+    const ssa_xreduce_job J = jobs[blockIdx.x];
+    const int tot = J.na * J.nb;
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+        double s = 0.0;
+        for (int c = 0; c < J.nchunks; ++c) s += J.part[(long long)c * tot + e];
+        const int i = e / J.nb, j = e - i * J.nb;
+        J.out[i + j * J.na] = (float)s;
+    }
+}
+
+__global__ void __launch_bounds__(RR_THREADS) k_svdsmall(const ssa_svd_job* __restrict__ jobs) {
+    extern __shared__ double dsm[];
+    double* A = dsm;                    // column j of M at A + j * SLD
+    double* Z = dsm + SSA_MAX_KP * SLD;
+    __shared__ int perm[SSA_MAX_KP + 1];
+    __shared__ double nrm[SSA_MAX_KP];
+    __shared__ int order[SSA_MAX_KP];
+    __shared__ int notconv;
+    const ssa_svd_job J = jobs[blockIdx.x];
+    const int n = J.n;
+    if (n < 1 || n > SSA_MAX_KP || J.nchunks < 1) {
+        if (threadIdx.x == 0) check_fail(7, 1, (unsigned)n);
+        return;
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        double s = 0.0;
+        for (int c = 0; c < J.nchunks; ++c) s += J.part[(long long)c * n * n + e];
+        const int i = e / n, j = e - i * n;
+        A[j * SLD + i] = s;
+    }
+    for (int c = warp; c < n; c += nw)
+        for (int r = lane; r < n; r += 32) Z[c * SLD + r] = (r == c) ? 1.0 : 0.0;
+    __syncthreads();
+    onesided_jacobi(A, Z, n, perm, &notconv, nrm);
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < n; ++i) order[i] = i;
+        for (int i = 0; i < n; ++i) {  // descending singular value
+            int best = i;
+            for (int j = i + 1; j < n; ++j)
+                if (nrm[order[j]] > nrm[order[best]]) best = j;
+            const int tmp = order[i];
+            order[i] = order[best];
+            order[best] = tmp;
+        }
+    }
+    __syncthreads();
+    for (int j = warp; j < n; j += nw) {
+        const int col = order[j];
+        if (col < 0 || col >= n) {
+            if (lane == 0) check_fail(7, 2, (unsigned)col);
+            continue;
+        }
+        const double sg = nrm[col];
+        const double isg = sg > 1e-300 ? 1.0 / sg : 0.0;
+        for (int i = lane; i < n; i += 32) {
+            J.Us[i + j * n] = (float)(A[col * SLD + i] * isg);
+            J.Vs[i + j * n] = (float)Z[col * SLD + i];
+            J.Dinv[i + j * n] = (i == j) ? (float)(sg > 1e-12 ? 1.0 / sg : 1.0) : 0.f;
+        }
+        if (lane == 0) {
+            J.sigma[j] = sg;
+            if (!isfinite(sg) && J.status) atomicOr(J.status, 2);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_sortsign(const ssa_sortsign_job* __restrict__ jobs) {
+    __shared__ double colsum[SSA_MAX_KP];
+    __shared__ double sv[SSA_MAX_KP];
+    __shared__ int pm[SSA_MAX_KP];
+    const ssa_sortsign_job J = jobs[blockIdx.x];
+    const int k = J.k;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (k < 1 || k > SSA_MAX_KP) {
+        if (threadIdx.x == 0) check_fail(8, 1, (unsigned)k);
+        return;
+    }
+    for (int c = warp; c < k; c += nw) {
+        double s = 0.0;
+        for (int r = lane; r < J.L; r += 32) s += (double)J.U[(long long)r + (long long)c * J.ldU];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) colsum[c] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < k; ++i) {
+            sv[i] = J.sigma[i];
+            pm[i] = i;
+        }
+        // the reference's exchange sort (MKL/ssa_opt.h:1896-1908)
+        for (int i = 0; i < k - 1; ++i)
+            for (int j = i + 1; j < k; ++j)
+                if (sv[j] > sv[i]) {
+                    const double t = sv[i];
+                    sv[i] = sv[j];
+                    sv[j] = t;
+                    const int u = pm[i];
+                    pm[i] = pm[j];
+                    pm[j] = u;
+                }
+        for (int i = 0; i < k; ++i) {
+            J.sigma[i] = sv[i];
+            J.perm[i] = pm[i];
+            J.sign[i] = colsum[pm[i]] < 0.0 ? -1.f : 1.f;
+        }
+    }
+}
+
+__global__ void k_permcols(const ssa_permcols_job* __restrict__ jobs) {
+    const ssa_permcols_job J = jobs[blockIdx.z];
+    const int j = blockIdx.y;
+    if (j >= J.k) return;
+    const int src = J.perm[j];
+    const float sg = J.sign[j];
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < J.m; r += gridDim.x * blockDim.x)
+        J.dst[(long long)r + (long long)j * J.ldd] = sg * J.src[(long long)r + (long long)src * J.lds];
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -979,9 +1191,7 @@ extern "C" int ssad_chol(const ssa_chol_job* d_jobs, int njobs, void* stream) {
 extern "C" int ssad_rowmul(const ssa_rowmul_job* d_jobs, int njobs, int maxrows, int maxn, void* stream) {
     if (njobs <= 0 || maxrows <= 0) return 0;
     if (maxn > SSA_MAX_KP) return (int)cudaErrorInvalidValue;
-    cudaError_t e = set_smem(k_rowmul, RM_SMEM);
-    if (e != cudaSuccess) return (int)e;
-    k_rowmul<<<dim3((maxrows + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS, njobs), ROWMUL_THREADS, RM_SMEM,
+    k_rowmul<<<dim3((maxrows + ROWMUL_THREADS - 1) / ROWMUL_THREADS, njobs), ROWMUL_THREADS, 0,
                (cudaStream_t)stream>>>(d_jobs);
     return launched(cudaGetLastError());
 }
@@ -1009,6 +1219,41 @@ extern "C" int ssad_lrf(const ssa_lrf_job* d_jobs, int njobs, void* stream) {
 extern "C" int ssad_group_sum(ssa_gsum_job job, void* stream) {
     if (job.B <= 0 || job.n_groups <= 0) return 0;
     k_group_sum<<<dim3((job.N + 255) / 256, job.n_groups, job.B), 256, 0, (cudaStream_t)stream>>>(job);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_xgram(const ssa_xgram_job* d_jobs, int njobs, int maxchunks, void* stream) {
+    if (njobs <= 0 || maxchunks <= 0) return 0;
+    cudaError_t e = set_smem(k_xgram, XG_SMEM);
+    if (e != cudaSuccess) return (int)e;
+    k_xgram<<<dim3(maxchunks, njobs), GRAM_THREADS, XG_SMEM, (cudaStream_t)stream>>>(d_jobs);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_xreduce(const ssa_xreduce_job* d_jobs, int njobs, void* stream) {
+    if (njobs <= 0) return 0;
+    k_xreduce<<<njobs, 256, 0, (cudaStream_t)stream>>>(d_jobs);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_svdsmall(const ssa_svd_job* d_jobs, int njobs, void* stream) {
+    if (njobs <= 0) return 0;
+    cudaError_t e = set_smem(k_svdsmall, SMALL_SMEM);
+    if (e != cudaSuccess) return (int)e;
+    k_svdsmall<<<njobs, RR_THREADS, SMALL_SMEM, (cudaStream_t)stream>>>(d_jobs);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_sortsign(const ssa_sortsign_job* d_jobs, int njobs, void* stream) {
+    if (njobs <= 0) return 0;
+    k_sortsign<<<njobs, 256, 0, (cudaStream_t)stream>>>(d_jobs);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_permcols(const ssa_permcols_job* d_jobs, int njobs, int maxrows, void* stream) {
+    if (njobs <= 0 || maxrows <= 0) return 0;
+    const int bx = min((maxrows + 255) / 256, 64);
+    k_permcols<<<dim3(bx, SSA_MAX_KP, njobs), 256, 0, (cudaStream_t)stream>>>(d_jobs);
     return launched(cudaGetLastError());
 }
 

@@ -62,9 +62,8 @@ typedef struct
     int N, L, K;
 } ssa_gram_job;
 
-/* Cholesky job: G = sum of the partials; G = R^T R with R upper triangular; writes R^{-1}
- * (computed in FP64) as fp32 n x n column-major (X[r][c] at R[r + c n], zeros below the
- * diagonal). */
+/* Cholesky job: G = sum of the partials; G = R^T R with R upper triangular, written as fp32
+ * n x n column-major (R[r][c] at R[r + c n], zeros below the diagonal). */
 typedef struct
 {
     const double *part;
@@ -74,20 +73,76 @@ typedef struct
     int pad_[2];
 } ssa_chol_job;
 
-/* Row-by-row products with a small matrix: C[:, 0:p] = A[:, 0:n] * Bm[0:n, 0:p] (in place
- * allowed: C == A; each tile of rows is staged in shared memory before it is overwritten).
- * `trsm` is reserved (0). */
+/* Row-by-row products with a small matrix (in place allowed: C == A, since every thread reads
+ * its whole row of A before writing its row of C):
+ *   trsm == 0: C[:, 0:p] = A[:, 0:n] * Bm[0:n, 0:p], or sub - A * Bm when sub != NULL;
+ *   trsm == 1: C = A * Bm^{-1} for upper-triangular Bm (p == n), by forward substitution. */
 typedef struct
 {
     const float *A;
     const float *Bm;      /* n x p col-major, ld = ldb */
     float *C;
     double *colsum;       /* optional: per-CTA partial column sums of C, [blockIdx.x][p] */
-    long long lda, ldc;
+    const float *sub;     /* optional: C = sub - A * Bm (sub may alias C), ld = ldsub */
+    long long lda, ldc, ldsub;
     int m, n, p, ldb;
     int trsm;
     int pad_;
 } ssa_rowmul_job;
+
+/* Cross Gram partials: part[chunk][i * nb + j] = sum over the chunk's rows r of A[r][i] B[r][j]
+ * (FP64 accumulation), A m x na (lda), B m x nb (ldb), na, nb <= SSA_MAX_KP. */
+typedef struct
+{
+    const float *A, *B;
+    double *part;
+    long long lda, ldb;
+    int m, na, nb, rows_per_cta;
+} ssa_xgram_job;
+
+/* Sum of cross Gram partials into a fp32 na x nb column-major matrix (ld na). */
+typedef struct
+{
+    const double *part;
+    float *out;
+    int nchunks, na, nb, pad_;
+} ssa_xreduce_job;
+
+/* SVD of a small square matrix M = sum of cross Gram partials (n x n, M[i][j] at i * n + j):
+ * M = Us diag(sigma) Vs^T by one-sided Jacobi in FP64, sigma descending. Outputs fp32 n x n
+ * column-major (ld n): Us, Vs, and Dinv = diag(1 / sigma) (1 where sigma <= 1e-12). */
+typedef struct
+{
+    const double *part;
+    double *sigma;
+    float *Us, *Vs, *Dinv;
+    int *status;
+    int nchunks, n;
+} ssa_svd_job;
+
+/* Final ordering of a block decomposition: permutation of the k components by sigma (the
+ * reference's exchange sort) and signs (sum_i U[i, j] >= 0 after the sort), applied to sigma
+ * in place; perm/sign are written for ssa_permcols. */
+typedef struct
+{
+    const float *U;
+    double *sigma;
+    int *perm;
+    float *sign;
+    long long ldU;
+    int L, k;
+} ssa_sortsign_job;
+
+/* dst[:, j] = sign[j] * src[:, perm[j]] for j < k, rows < m. */
+typedef struct
+{
+    const float *src;
+    float *dst;
+    const int *perm;
+    const float *sign;
+    long long lds, ldd;
+    int m, k;
+} ssa_permcols_job;
 
 /* Rows of C per k_rowmul CTA (granularity of the colsum partials). */
 #define SSA_ROWMUL_ROWS 128
@@ -154,6 +209,11 @@ typedef struct
     int n_groups, N, k, B;
 } ssa_gsum_job;
 
+int ssad_xgram(const ssa_xgram_job *d_jobs, int njobs, int maxchunks, void *stream);
+int ssad_xreduce(const ssa_xreduce_job *d_jobs, int njobs, void *stream);
+int ssad_svdsmall(const ssa_svd_job *d_jobs, int njobs, void *stream);
+int ssad_sortsign(const ssa_sortsign_job *d_jobs, int njobs, void *stream);
+int ssad_permcols(const ssa_permcols_job *d_jobs, int njobs, int maxrows, void *stream);
 int ssad_init_device(void);
 int ssad_group_sum(ssa_gsum_job job, void *stream);
 int ssad_spectrum(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);

@@ -65,6 +65,7 @@ _sig("ssa_opt_decompose", _I, _P, _I, _I)
 _sig("ssa_opt_decompose_block", _I, _P, _I, _I, _I)
 _sig("ssa_opt_decompose_randomized", _I, _P, _I, _I)
 _sig("ssa_opt_decompose_randomized_ex", _I, _P, _I, _I, _I, c_double_p)
+_sig("ssa_opt_decompose_block_ex", _I, _P, _I, _I, _I, c_double_p)
 _sig("ssa_opt_reconstruct", _I, _P, c_int_p, _I, c_double_p)
 _sig("ssa_opt_cache_ffts", _I, _P)
 _sig("ssa_opt_forecast", _I, _P, c_int_p, _I, _I, c_double_p)
@@ -214,7 +215,12 @@ class SSA:
         elif method == "block":
             block_size = kwargs.get("block_size", min(k, 32))
             max_iter = kwargs.get("max_iter", 100)
-            ret = _lib.ssa_opt_decompose_block(ctypes.byref(self._ctx), k, block_size, max_iter)
+            v0 = kwargs.get("v0", None)
+            if v0 is None:
+                ret = _lib.ssa_opt_decompose_block(ctypes.byref(self._ctx), k, block_size, max_iter)
+            else:
+                v = np.ascontiguousarray(np.asarray(v0, dtype=np.float64).T)  # K x k column-major
+                ret = _lib.ssa_opt_decompose_block_ex(ctypes.byref(self._ctx), k, block_size, max_iter, _dp(v))
         elif method == "sequential":
             ret = _lib.ssa_opt_decompose(ctypes.byref(self._ctx), k, kwargs.get("max_iter", 100))
         else:

@@ -272,3 +272,47 @@ def test_full_size_batch_clean(gpu, oracle):
         rel, gap = sigma_errors(sig[s_], d.sigma)
         assert np.all(rel[gap > 1e-3] <= SIG_TOL), (s_, rel.max())
         assert rel_l2(G[s_, 1], oracle.reconstruct(d, [1, 2], N, L)) <= rec_tol(d.sigma, [1, 2])
+
+
+@pytest.mark.parametrize("k,bsize,max_iter", [(10, 4, 20), (6, 6, 30), (8, 3, 7)])
+def test_block_power_parity(gpu, oracle, k, bsize, max_iter):
+    """Block power iteration (MKL/ssa_opt.h:1765-1933) with the same start blocks as the oracle.
+    The device re-orthonormalises every half-step (the reference every fifth); the subspaces,
+    hence the Rayleigh-Ritz results, are the same."""
+    x, _, _ = oracle.config1(seed=0)
+    N, L = 1000, 250
+    K = N - L + 1
+    rng = np.random.default_rng(k * 100 + bsize)
+    V0 = rng.uniform(-0.5, 0.5, (K, k))
+    blocks, c = [], 0
+    while c < k:
+        cb = min(bsize, k - c)
+        blocks.append(V0[:, c:c + cb])
+        c += cb
+    d = oracle.decompose_block(x, L, k, bsize, max_iter, blocks)
+    gs = gpu.SSA(x, L)
+    gs.decompose(k, method="block", block_size=bsize, max_iter=max_iter, v0=V0)
+    U, V, s = gs.factors()
+    rel, gap = sigma_errors(s, d.sigma)
+    assert np.all(rel[gap > 1e-3] <= SIG_TOL), rel.max()
+    assert np.all(rel <= 1e-4)
+    for g in ([0], [1, 2]):
+        assert rel_l2(gs.reconstruct(g), oracle.reconstruct(d, g, N, L)) <= rec_tol(d.sigma, g)
+
+
+def test_sequential_and_block_agree_with_exact(gpu, oracle):
+    # MKL/test/ssa_opt_test.c:1690-1733: methods agree within 1%; here also vs the exact SVD.
+    x = oracle.reference_test_signal(500)
+    N, L, k = 500, 125, 6
+    t = oracle.dense_svd(x, L, k)
+    a = gpu.SSA(x, L)
+    a.decompose(k, method="sequential", max_iter=100)
+    b = gpu.SSA(x, L)
+    b.decompose(k, method="block", block_size=3, max_iter=100)
+    sa, sb = a.singular_values, b.singular_values
+    assert np.max(np.abs(sa - sb) / sb) < 1e-2
+    assert np.max(np.abs(sb - t.sigma) / t.sigma) < 1e-2
+    assert np.abs(sb[0] - t.sigma[0]) / t.sigma[0] < 1e-5
+    assert np.all(np.diff(sb) <= 0)
+    U, V, _ = b.factors()
+    assert np.all(U.sum(axis=0) >= 0)
