@@ -83,6 +83,10 @@ int ssa_opt_hankel_matvec_T_dev(SSA_Opt *ssa, const double *u, double *z);
  * k = n_components. Either pointer may be NULL. Returns k or -1. */
 int ssa_opt_copy_factors(const SSA_Opt *ssa, double *U, double *V);
 
+/* The same for a decomposed MSSA context: U ((M L) x k, channel m in rows m L .. m L + L - 1),
+ * V (K x k) and sigma (k). Any pointer may be NULL. Returns k or -1. */
+int mssa_opt_copy_factors(const MSSA_Opt *mssa, double *U, double *V, double *sigma);
+
 /* Stage profiler of a batch: with profiling on, every kernel launch of ssa_batch_run* is
  * bracketed by CUDA events on the batch stream. ssa_batch_profile waits for the stream and
  * returns the accumulated milliseconds and launch counts per kernel kind in the order

@@ -500,6 +500,7 @@ def cadzow(x: np.ndarray, L: int, rank: int, max_iter: int, tol: float, Omega: n
     (signal, iterations, final_diff, converged)."""
     y = np.asarray(x, dtype=np.float64).copy()
     N = len(y)
+    K = N - L + 1
     ynorm = float(np.linalg.norm(y))
     if ynorm < 1e-15:
         ynorm = 1.0
@@ -507,8 +508,12 @@ def cadzow(x: np.ndarray, L: int, rank: int, max_iter: int, tol: float, Omega: n
     converged = False
     it = 0
     group = list(range(rank))
+    randomized = rank + 8 < min(L, K) // 2  # :3212
     while it < max_iter:
-        dec = decompose_randomized(y, L, rank, 8, Omega, q=q)
+        if randomized:
+            dec = decompose_randomized(y, L, rank, 8, Omega, q=q)
+        else:  # :3227-3231, block size min(rank, 16), 3 iterations; Omega holds the start blocks
+            dec = decompose_block(y, L, rank, min(rank, 16), 3, _split_blocks(Omega, rank, min(rank, 16)))
         y_new = reconstruct(dec, group, N, L)
         diff = float(np.linalg.norm(y_new - y)) / ynorm
         y = y_new
@@ -517,6 +522,58 @@ def cadzow(x: np.ndarray, L: int, rank: int, max_iter: int, tol: float, Omega: n
             converged = True
             break
     return y, it, diff, converged
+
+
+def _split_blocks(V0: np.ndarray, k: int, b: int) -> list:
+    blocks, c = [], 0
+    while c < k:
+        cb = min(b, k - c)
+        blocks.append(np.asarray(V0)[:, c:c + cb])
+        c += cb
+    return blocks
+
+
+def cadzow_weighted(x: np.ndarray, L: int, rank: int, max_iter: int, tol: float, alpha: float,
+                    Omega: np.ndarray, q: int = 0):
+    """ssa_opt_cadzow_weighted (ssa_opt.h:3294-3315): alpha * cadzow(x) + (1 - alpha) * x."""
+    y, it, diff, conv = cadzow(x, L, rank, max_iter, tol, Omega, q)
+    if alpha < 1.0:
+        y = alpha * y + (1.0 - alpha) * np.asarray(x, dtype=np.float64)
+    return y, it, diff, conv
+
+
+def cadzow_inplace(x: np.ndarray, L: int, rank: int, max_iter: int, tol: float,
+                   omegas: Sequence[np.ndarray]):
+    """ssa_opt_cadzow_inplace (ssa_opt.h:3319-3442) on a prepared context, randomized branch:
+    iteration i draws the test matrix omegas[i]. The first reconstruction sets the norm; later
+    ones are compared with the previous reconstruction; the signal is replaced by the
+    reconstruction except after the last iteration. Returns (last reconstruction, iterations,
+    final_diff, converged, signal held by the context)."""
+    y = np.asarray(x, dtype=np.float64).copy()
+    N = len(y)
+    group = list(range(rank))
+    y_norm, diff, converged = 1.0, 0.0, False
+    y_prev = None
+    y_new = None
+    it = 0
+    while it < max_iter:
+        dec = decompose_randomized(y, L, rank, 8, omegas[it], q=0)
+        y_new = reconstruct(dec, group, N, L)
+        if it == 0:
+            y_norm = float(np.linalg.norm(y_new))
+            if y_norm < 1e-15:
+                y_norm = 1.0
+        else:
+            diff = float(np.linalg.norm(y_new - y_prev)) / y_norm
+            if diff < tol:
+                converged = True
+                it += 1
+                break
+        y_prev = y_new
+        if it < max_iter - 1:
+            y = y_new.copy()
+        it += 1
+    return y_new, it, diff, converged, y
 
 
 # ---------------------------------------------------------------------------------------------
@@ -671,6 +728,19 @@ def series_seed(seed: int, s: int) -> int:
 def single_series_seed(calls: int = 0) -> int:
     """Seed the single-series API uses for its `calls`-th generated test matrix (42 + 2^32 calls)."""
     return series_seed((42 + (calls << 32)) & _M64, 0)
+
+
+def block_seed(calls: int = 0) -> int:
+    """Seed of the single-series block method's `calls`-th start blocks; series 0's columns
+    come from series_seed(block_seed(calls), 0), column c of the K x k start matrix being the
+    generator's column c."""
+    return ((42 + (calls << 32)) ^ 0xB10CB10CB10CB10C) & _M64
+
+
+def mssa_seed(calls: int = 0) -> int:
+    """Seed of an MSSA context's `calls`-th generated K x kp test matrix (used as is, with no
+    per-series mixing: the channels share one matrix)."""
+    return ((42 + (calls << 32)) ^ 0x4D55535341) & _M64
 
 
 def device_gaussian(seed_s: int, K: int, kp: int) -> np.ndarray:

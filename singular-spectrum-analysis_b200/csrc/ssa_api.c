@@ -976,6 +976,276 @@ int ssa_opt_copy_factors(const SSA_Opt *ssa, double *U, double *V)
     return k;
 }
 
+/* ---- Cadzow iterations (MKL/ssa_opt.h:3165-3442) --------------------------------------------
+ * The signal stays on the device for the whole loop: each iteration decomposes the context's
+ * current signal, reconstructs the leading `rank` components into g->d_out and reduces
+ * ||y_new - y|| on the device; the host reads back two doubles per iteration for the stopping
+ * test. The reference picks the randomized branch when rank + 8 < min(L, K) / 2 (:3212) and the
+ * block method (block size min(rank, 16), 3 iterations) otherwise or when the randomized one
+ * fails (:3213-3232). */
+
+static int cadzow_use_randomized(int rank, int L, int K) { return rank + 8 < imin(L, K) / 2; }
+
+/* Decompose the current device signal (spectrum already in e->X) to `rank` components and
+ * reconstruct them into g->d_out; waits for the device. 0 on success, -1 on a launch error, 1
+ * when the decomposition reported a failure status. */
+static int cadzow_project(SSA_Opt *ssa, int rank, int randomized, unsigned long long seed, int *k_out)
+{
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    ssa_engine *e = &g->e;
+    const int L = ssa->L, K = ssa->K;
+    int k;
+    g->spectra_valid = 0;
+    g->wcorr_valid = 0;
+    if (randomized)
+    {
+        const int kp = imin(rank + 8, imin(L, K));
+        k = imin(rank, kp);
+        if (kp > e->kp || ssae_decompose(e, 1, kp, k, 0, NULL, 0, seed) != 0)
+            return -1;
+    }
+    else
+    {
+        k = imin(rank, imin(L, K));
+        if (k > e->k || ssae_decompose_block(e, 1, k, imin(rank, 16), 3, NULL, K, seed) != 0)
+            return -1;
+    }
+    if (sync_ok(g) != 0)
+        return -1;
+    if (check_status(g) != 0)
+        return 1;
+    if (ssae_spectra(e, 1, k) != 0 || ssae_recon_group(e, 0, k, g->d_group, rank, g->d_out) != 0)
+        return -1;
+    g->spectra_valid = 1;
+    ssa->n_components = k;
+    *k_out = k;
+    return 0;
+}
+
+static int cadzow_setup(struct ssa_gpu_ctx *g, int rank, double **d_aux, size_t aux_doubles)
+{
+    int *grp = (int *)malloc(sizeof(int) * rank);
+    if (!grp)
+        return -1;
+    for (int i = 0; i < rank; i++)
+        grp[i] = i;
+    int rc = ensure_group(g, grp, rank);
+    rc |= sync_ok(g);
+    free(grp);
+    if (rc || cudaMalloc((void **)d_aux, sizeof(double) * aux_doubles) != cudaSuccess)
+        return -1;
+    return cudaMemsetAsync(*d_aux, 0, sizeof(double) * aux_doubles, g->e.st) == cudaSuccess ? 0 : -1;
+}
+
+static int cadzow_run(const double *x, int N, int L, int rank, int max_iter, double tol, double alpha,
+                      double *output, SSA_CadzowResult *result)
+{
+    if (!x || !output || N < 4 || L < 2 || L > N - 1 || rank < 1 || max_iter < 1)
+        return -1;
+    const int K = N - L + 1;
+    if (imin(rank, imin(L, K)) > SSA_MAX_KP)
+        return -1;
+    SSA_Opt ssa;
+    if (ssa_opt_init(&ssa, x, N, L) != 0)
+        return -1;
+    struct ssa_gpu_ctx *g = ssa.gpu;
+    ssa_engine *e = &g->e;
+    double *d_aux = NULL; /* diff^2, |y|^2, then the input signal when blending */
+    const int blend = alpha < 1.0;
+    if (cadzow_setup(g, rank, &d_aux, 2 + (blend ? (size_t)N : 0)) != 0)
+    {
+        ssa_opt_free(&ssa);
+        return -1;
+    }
+    double ynorm = 0.0;
+    for (int i = 0; i < N; i++)
+        ynorm += x[i] * x[i];
+    ynorm = sqrt(ynorm);
+    if (ynorm < 1e-15)
+        ynorm = 1.0;
+    int rc = 0, iter, k = 0;
+    double diff = 0.0;
+    int converged = 0;
+    if (blend)
+        rc |= cudaMemcpyAsync(d_aux + 2, e->x64, sizeof(double) * N, cudaMemcpyDeviceToDevice, e->st) != cudaSuccess;
+    const int randomized = cadzow_use_randomized(rank, L, K);
+    for (iter = 0; iter < max_iter && !rc; iter++)
+    {
+        ssae_reset_jobs(e);
+        if (iter > 0 && ssae_signal_spectrum(e, e->x64, 1) != 0)
+        {
+            rc = -1;
+            break;
+        }
+        /* every iteration runs in a freshly initialised context in the reference, whose
+         * generator restarts: the same seed each time */
+        int pr = 1;
+        if (randomized)
+            pr = cadzow_project(&ssa, rank, 1, SSA_DEFAULT_SEED, &k);
+        if (pr == 1)
+            pr = cadzow_project(&ssa, rank, 0, SSA_DEFAULT_SEED ^ 0xB10CB10CB10CB10CULL, &k);
+        if (pr != 0)
+        {
+            rc = -1;
+            break;
+        }
+        double h[2];
+        if (ssad_diffnorm(g->d_out, e->x64, N, d_aux, e->st) != 0 ||
+            cudaMemcpyAsync(e->x64, g->d_out, sizeof(double) * N, cudaMemcpyDeviceToDevice, e->st) != cudaSuccess ||
+            cudaMemcpyAsync(h, d_aux, sizeof(double) * 2, cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
+            sync_ok(g) != 0)
+        {
+            rc = -1;
+            break;
+        }
+        diff = sqrt(h[0]) / ynorm;
+        if (diff < tol)
+        {
+            converged = 1;
+            iter++;
+            break;
+        }
+    }
+    if (!rc && blend &&
+        ssad_axpby(e->x64, d_aux + 2, e->x64, alpha, 1.0 - alpha, N, e->st) != 0)
+        rc = -1;
+    if (!rc && (cudaMemcpyAsync(output, e->x64, sizeof(double) * N, cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
+                sync_ok(g) != 0))
+        rc = -1;
+    cudaFree(d_aux);
+    ssa_opt_free(&ssa);
+    if (rc)
+        return -1;
+    if (result)
+    {
+        result->iterations = iter;
+        result->final_diff = diff;
+        result->converged = converged ? 1.0 : 0.0;
+    }
+    return iter;
+}
+
+int ssa_opt_cadzow(const ssa_real *x, int N, int L, int rank, int max_iter, ssa_real tol, ssa_real *output,
+                   SSA_CadzowResult *result)
+{
+    return cadzow_run(x, N, L, rank, max_iter, tol, 1.0, output, result);
+}
+
+/* output = alpha * cadzow(x) + (1 - alpha) * x (MKL/ssa_opt.h:3294-3315), blended on the device. */
+int ssa_opt_cadzow_weighted(const ssa_real *x, int N, int L, int rank, int max_iter, ssa_real tol, ssa_real alpha,
+                            ssa_real *output, SSA_CadzowResult *result)
+{
+    if (alpha <= 0.0 || alpha > 1.0)
+        return -1;
+    return cadzow_run(x, N, L, rank, max_iter, tol, alpha, output, result);
+}
+
+/* In-place variant (MKL/ssa_opt.h:3319-3442): iterates on the context's own signal. The first
+ * reconstruction sets the norm for the relative difference; later ones are compared with the
+ * previous reconstruction; the signal is replaced by the reconstruction except after the last
+ * iteration. The randomized branch needs a prepared context with room for rank + 8 columns and
+ * draws a new test matrix per call, like the reference's generator stream. On return the context
+ * holds the last decomposition (host fields mirrored). */
+int ssa_opt_cadzow_inplace(SSA_Opt *ssa, int rank, int max_iter, ssa_real tol, SSA_CadzowResult *result)
+{
+    if (!ssa || !ssa->initialized || rank < 1 || max_iter < 1)
+        return -1;
+    const int N = ssa->N, L = ssa->L, K = ssa->K;
+    if (imin(rank, imin(L, K)) > SSA_MAX_KP)
+        return -1;
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    ssa_engine *e = &g->e;
+    double *d_aux = NULL; /* diff^2, |y|^2, previous reconstruction (N) */
+    ssae_reset_jobs(e);
+    if (cadzow_setup(g, rank, &d_aux, 2 + (size_t)N) != 0)
+        return -1;
+    double *d_prev = d_aux + 2;
+    double y_norm = 1.0, diff = 0.0;
+    int converged = 0, iter, rc = 0, k = 0;
+    for (iter = 0; iter < max_iter; iter++)
+    {
+        ssae_reset_jobs(e);
+        const int randomized = cadzow_use_randomized(rank, L, K);
+        ssa_opt_free_cached_ffts(ssa);
+        ssa->decomposed = false;
+        ssa->n_components = 0;
+        ssa->total_variance = 0.0;
+        int pr = 1;
+        if (randomized && ssa->prepared && rank + 8 <= ssa->prepared_kp)
+        {
+            const unsigned long long seed = SSA_DEFAULT_SEED + 0x100000000ULL * (unsigned long long)ssa->rng_calls;
+            ssa->rng_calls++;
+            pr = cadzow_project(ssa, rank, 1, seed, &k);
+        }
+        if (pr == 1)
+        {
+            const unsigned long long seed =
+                (SSA_DEFAULT_SEED + 0x100000000ULL * (unsigned long long)ssa->rng_calls) ^ 0xB10CB10CB10CB10CULL;
+            ssa->rng_calls++;
+            pr = cadzow_project(ssa, rank, 0, seed, &k);
+        }
+        if (pr != 0)
+        {
+            rc = -1;
+            break;
+        }
+        double h[2];
+        if (ssad_diffnorm(g->d_out, d_prev, N, d_aux, e->st) != 0 ||
+            cudaMemcpyAsync(d_prev, g->d_out, sizeof(double) * N, cudaMemcpyDeviceToDevice, e->st) != cudaSuccess ||
+            cudaMemcpyAsync(h, d_aux, sizeof(double) * 2, cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
+            sync_ok(g) != 0)
+        {
+            rc = -1;
+            break;
+        }
+        if (iter == 0)
+        {
+            y_norm = sqrt(h[1]);
+            if (y_norm < 1e-15)
+                y_norm = 1.0;
+        }
+        else
+        {
+            diff = sqrt(h[0]) / y_norm;
+            if (diff < tol)
+            {
+                converged = 1;
+                iter++;
+                break;
+            }
+        }
+        if (iter < max_iter - 1)
+        {
+            /* the decomposition's factors stay in the engine; only the signal and its spectrum
+             * change (the engine keeps them apart) */
+            if (cudaMemcpyAsync(e->x64, g->d_out, sizeof(double) * N, cudaMemcpyDeviceToDevice, e->st) !=
+                    cudaSuccess ||
+                ssae_signal_spectrum(e, e->x64, 1) != 0)
+            {
+                rc = -1;
+                break;
+            }
+        }
+    }
+    cudaFree(d_aux);
+    if (rc)
+        return -1;
+    /* mirror the last decomposition and the current signal's spectrum */
+    if (alloc_results(ssa, k) != 0)
+        return -1;
+    ssa->n_components = k;
+    if (mirror_results(ssa, k) != 0 || mirror_spectrum(ssa) != 0)
+        return -1;
+    ssa->decomposed = true;
+    if (result)
+    {
+        result->iterations = iter;
+        result->final_diff = diff;
+        result->converged = converged ? 1.0 : 0.0;
+    }
+    return iter;
+}
+
 /* ---- library information ----------------------------------------------------------------- */
 unsigned long long ssa_b200_kernel_launches(void) { return ssad_launch_count(); }
 int ssa_b200_device_checks(unsigned int *out5, int reset) { return ssad_read_checks(out5, reset) == 0 ? 0 : -1; }

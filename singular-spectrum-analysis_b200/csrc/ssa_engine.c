@@ -352,20 +352,29 @@ int ssae_matvec(ssa_engine *e, int ncols, int adjoint)
 }
 
 /* Gram partials of the m x n blocks A_s (stride per series `sstride`, leading dim ld). */
+static int gram_ps(ssa_engine *e, int nb, const float *A, size_t sstride, long long ld, int m, int n, int rows,
+                   int weighted, size_t pstride);
+
 static int gram(ssa_engine *e, int nb, const float *A, size_t sstride, long long ld, int m, int n, int rows,
                 int weighted)
+{
+    const int nchmax = imax(e->nch_L, imax(e->nch_K, e->nch_N));
+    return gram_ps(e, nb, A, sstride, ld, m, n, rows, weighted, (size_t)nchmax * e->kp * (e->kp + 1) / 2);
+}
+
+/* Gram partials with series s's partials at e->part + s * pstride. */
+static int gram_ps(ssa_engine *e, int nb, const float *A, size_t sstride, long long ld, int m, int n, int rows,
+                   int weighted, size_t pstride)
 {
     ssa_gram_job *jobs = (ssa_gram_job *)calloc((size_t)nb, sizeof(ssa_gram_job));
     if (!jobs)
         return (int)cudaErrorMemoryAllocation;
     const int nch = (m + rows - 1) / rows;
-    const int nchmax = imax(e->nch_L, imax(e->nch_K, e->nch_N));
-    const size_t np = (size_t)e->kp * (e->kp + 1) / 2;
     for (int s = 0; s < nb; s++)
     {
         ssa_gram_job *J = &jobs[s];
         J->A = A + (size_t)s * sstride;
-        J->part = e->part + (size_t)s * nchmax * np;
+        J->part = e->part + (size_t)s * pstride;
         J->ld = ld;
         J->m = m;
         J->n = n;
@@ -967,6 +976,106 @@ int ssae_decompose_block(ssa_engine *e, int nb, int k, int bsize, int max_iter, 
             CK(cudaMemcpy2DAsync(e->Z + (size_t)s * sZ, sizeof(float) * e->ldK, e->Vt + (size_t)s * sZ,
                                  sizeof(float) * e->ldK, sizeof(float) * K, k, cudaMemcpyDeviceToDevice, e->st));
         }
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* MSSA: M channels of one instance are the engine's series; the stacked (M L) x K operator    */
+/* (reference MKL/ssa_opt.h:4069-4114) is applied channel by channel.                          */
+/* ------------------------------------------------------------------------------------------ */
+
+/* One CholQR pass on the stacked block [Y_0; ...; Y_{M-1}] (each L x n): Gram = sum of the
+ * channel Grams, one Cholesky, the same R applied to every channel. */
+static int mssa_cholqr(ssa_engine *e, int M, int n, double *colsum)
+{
+    const size_t sY = (size_t)e->ldL * e->kp;
+    const int nch = (e->L + e->rows_L - 1) / e->rows_L;
+    const size_t np = (size_t)n * (n + 1) / 2;
+    CK(gram_ps(e, M, e->Y, sY, e->ldL, e->L, n, e->rows_L, 0, (size_t)nch * np));
+    ssa_chol_job J;
+    memset(&J, 0, sizeof(J));
+    J.part = e->part;
+    J.R = e->Rinv;
+    J.status = e->status;
+    J.nchunks = M * nch;
+    J.n = n;
+    void *d = ssae_push_jobs(e, &J, sizeof(J));
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_CHOL);
+    int rc = ssad_chol((const ssa_chol_job *)d, 1, e->st);
+    ssae_prof_end(e);
+    CK(rc);
+    return rowmul(e, M, e->Y, sY, e->ldL, e->L, n, e->Rinv, 0, n, n, e->Y, sY, e->ldL, colsum, 1);
+}
+
+/* Z_0 = sum_m H_m^T Y_m (per-channel adjoints into Z_m, then a fixed-order channel sum). */
+static int mssa_adjoint(ssa_engine *e, int M, int n)
+{
+    const size_t sY = (size_t)e->ldL * e->kp, sZ = (size_t)e->ldK * e->kp;
+    CK(corr_io(e, M, n, 1, e->Y, sY, e->ldL, e->Z, sZ, e->ldK));
+    return ssad_slabsum(e->Z, e->Z, (long long)sZ, M, (long long)e->ldK * n, e->st);
+}
+
+int ssae_mssa_decompose(ssa_engine *e, int M, int kp, int k, int q, const float *d_omega, unsigned long long seed)
+{
+    if (M < 1 || M > e->B || kp < 1 || kp > e->kp || k < 1 || k > imin(kp, e->k))
+        return (int)cudaErrorInvalidValue;
+    const size_t sY = (size_t)e->ldL * e->kp, sZ = (size_t)e->ldK * e->kp;
+    const int K = e->K;
+    CK(cudaMemsetAsync(e->status, 0, sizeof(int) * M, e->st));
+    /* Omega (shared by every channel) in Z_0 */
+    if (d_omega && d_omega != e->Z)
+        CK(cudaMemcpy2DAsync(e->Z, sizeof(float) * e->ldK, d_omega, sizeof(float) * e->ldK, sizeof(float) * K, kp,
+                             cudaMemcpyDeviceToDevice, e->st));
+    else if (!d_omega)
+        CK(ssad_gaussian(e->Z, e->ldK, K, kp, 0, seed, e->st));
+    /* Y_m = H_m Omega */
+    CK(corr_io(e, M, kp, 0, e->Z, 0, e->ldK, e->Y, sY, e->ldL));
+    for (int it = 0; it < q; it++)
+    {
+        CK(mssa_cholqr(e, M, kp, NULL));
+        CK(mssa_adjoint(e, M, kp));
+        CK(cholqr_pass(e, 1, e->Z, sZ, e->ldK, K, kp, e->rows_K, NULL));
+        CK(corr_io(e, M, kp, 0, e->Z, 0, e->ldK, e->Y, sY, e->ldL));
+    }
+    CK(mssa_cholqr(e, M, kp, NULL));
+    CK(mssa_cholqr(e, M, kp, e->qsum));
+    /* B = sum_m H_m^T Q_m, Rayleigh-Ritz on B^T B */
+    CK(mssa_adjoint(e, M, kp));
+    CK(gram(e, 1, e->Z, sZ, e->ldK, K, kp, e->rows_K, 0));
+    {
+        ssa_rr_job J;
+        memset(&J, 0, sizeof(J));
+        J.part = e->part;
+        J.qsum = e->qsum;
+        J.sigma = e->sigma;
+        J.Zu = e->Zu;
+        J.Zv = e->Zv;
+        J.status = e->status;
+        J.nchunks = (K + e->rows_K - 1) / e->rows_K;
+        J.nchunks_q = M * ((e->L + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS);
+        J.kp = kp;
+        J.k = k;
+        void *d = ssae_push_jobs(e, &J, sizeof(J));
+        if (!d)
+            return (int)cudaErrorMemoryAllocation;
+        ssae_prof_begin(e, SSAK_RR);
+        int rc = ssad_rr((const ssa_rr_job *)d, 1, e->st);
+        ssae_prof_end(e);
+        CK(rc);
+    }
+    /* U_m = Q_m Zu for every channel; V = B Zv into Z_0 */
+    CK(rowmul(e, M, e->Y, sY, e->ldL, e->L, kp, e->Zu, 0, kp, k, e->Y, sY, e->ldL, NULL, 0));
+    CK(rowmul(e, 1, e->Z, sZ, e->ldK, K, kp, e->Zv, 0, kp, k, e->Z, sZ, e->ldK, NULL, 0));
+    /* every channel's V slot gets V (the per-channel spectra of the reconstruction use them) */
+    for (int m = 1; m < M; m++)
+    {
+        CK(cudaMemcpy2DAsync(e->Z + (size_t)m * sZ, sizeof(float) * e->ldK, e->Z, sizeof(float) * e->ldK,
+                             sizeof(float) * K, k, cudaMemcpyDeviceToDevice, e->st));
+        CK(cudaMemcpyAsync(e->sigma + (size_t)m * e->k, e->sigma, sizeof(double) * k, cudaMemcpyDeviceToDevice,
+                           e->st));
     }
     return 0;
 }

@@ -131,6 +131,11 @@ int ssae_matvec(ssa_engine *e, int ncols, int adjoint);
 int ssae_decompose_block(ssa_engine *e, int nb, int k, int bsize, int max_iter, const float *d_V0,
                          long long v0_ld, unsigned long long seed);
 int ssae_ensure_block(ssa_engine *e, int bcap);
+/* MSSA randomized decomposition of one instance whose M channels are the engine's first M
+ * series (reference MKL/ssa_opt.h:4116-4210, plus q power iterations). d_omega: device K x kp
+ * test matrix (ld ldK) or NULL for the generator with `seed`. Results: U_m in Y_m (L x k per
+ * channel), V in every Z_m, sigma in series 0's slot. */
+int ssae_mssa_decompose(ssa_engine *e, int M, int kp, int k, int q, const float *d_omega, unsigned long long seed);
 /* Grouped reconstruction of series s from cached spectra into d_out (double, N). */
 int ssae_recon_group(ssa_engine *e, int s, int k, const int *d_group, int n_group, double *d_out);
 

@@ -971,6 +971,49 @@ __global__ void k_permcols(const ssa_permcols_job* __restrict__ jobs) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// Small elementwise / reduction kernels (MSSA channel sums, contributions, Cadzow)
+// ---------------------------------------------------------------------------------------------
+
+__global__ void k_slabsum(float* out, const float* in, long long stride, int nslab, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        float acc = 0.f;
+        for (int sl = 0; sl < nslab; ++sl) acc += in[(long long)sl * stride + i];
+        out[i] = acc;
+    }
+}
+
+__global__ void k_colnorm2(const float* A, long long sstride, long long ld, int m, int k, double* out) {
+    __shared__ double red[32];
+    const int s = blockIdx.y, j = blockIdx.x;
+    const float* a = A + (long long)s * sstride + (long long)j * ld;
+    double acc = 0.0;
+    for (int r = threadIdx.x; r < m; r += blockDim.x) acc += (double)a[r] * (double)a[r];
+    acc = block_sum<double>(acc, red);
+    if (threadIdx.x == 0) out[(long long)s * k + j] = acc;
+}
+
+__global__ void k_diffnorm(const double* a, const double* b, long long n, double* out2) {
+    __shared__ double red[32];
+    double d2 = 0.0, a2 = 0.0;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+        const double d = a[i] - b[i];
+        d2 += d * d;
+        a2 += a[i] * a[i];
+    }
+    d2 = block_sum<double>(d2, red);
+    a2 = block_sum<double>(a2, red);
+    if (threadIdx.x == 0) {
+        out2[0] = d2;
+        out2[1] = a2;
+    }
+}
+
+__global__ void k_axpby(const double* a, const double* b, double* out, double alpha, double beta, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = alpha * a[i] + beta * b[i];
+}
+
+// ---------------------------------------------------------------------------------------------
 // W-correlation finish and LRF forecast
 // ---------------------------------------------------------------------------------------------
 
@@ -1254,6 +1297,33 @@ extern "C" int ssad_permcols(const ssa_permcols_job* d_jobs, int njobs, int maxr
     if (njobs <= 0 || maxrows <= 0) return 0;
     const int bx = min((maxrows + 255) / 256, 64);
     k_permcols<<<dim3(bx, SSA_MAX_KP, njobs), 256, 0, (cudaStream_t)stream>>>(d_jobs);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_slabsum(float* out, const float* in, long long stride, int nslab, long long n, void* stream) {
+    if (n <= 0 || nslab <= 0) return 0;
+    const long long blocks = (n + 255) / 256;
+    k_slabsum<<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0, (cudaStream_t)stream>>>(out, in, stride, nslab, n);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_colnorm2(const float* A, long long sstride, long long ld, int m, int k, int nb, double* out,
+                             void* stream) {
+    if (nb <= 0 || k <= 0) return 0;
+    k_colnorm2<<<dim3(k, nb), 256, 0, (cudaStream_t)stream>>>(A, sstride, ld, m, k, out);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_diffnorm(const double* a, const double* b, long long n, double* out2, void* stream) {
+    k_diffnorm<<<1, 1024, 0, (cudaStream_t)stream>>>(a, b, n, out2);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_axpby(const double* a, const double* b, double* out, double alpha, double beta, long long n,
+                          void* stream) {
+    if (n <= 0) return 0;
+    const long long blocks = (n + 255) / 256;
+    k_axpby<<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0, (cudaStream_t)stream>>>(a, b, out, alpha, beta, n);
     return launched(cudaGetLastError());
 }
 

@@ -214,6 +214,14 @@ int ssad_xreduce(const ssa_xreduce_job *d_jobs, int njobs, void *stream);
 int ssad_svdsmall(const ssa_svd_job *d_jobs, int njobs, void *stream);
 int ssad_sortsign(const ssa_sortsign_job *d_jobs, int njobs, void *stream);
 int ssad_permcols(const ssa_permcols_job *d_jobs, int njobs, int maxrows, void *stream);
+/* out[i] = sum_{s < nslab} in[s * stride + i] for i < n (fixed order; out may alias slab 0). */
+int ssad_slabsum(float *out, const float *in, long long stride, int nslab, long long n, void *stream);
+/* out[s * k + j] = sum_r A[s][r][j]^2 (FP64) for nb column blocks A_s = A + s * sstride (m x k, ld). */
+int ssad_colnorm2(const float *A, long long sstride, long long ld, int m, int k, int nb, double *out, void *stream);
+/* out2[0] = sum (a - b)^2, out2[1] = sum a^2 over n doubles (FP64, one CTA, fixed order). */
+int ssad_diffnorm(const double *a, const double *b, long long n, double *out2, void *stream);
+/* out[i] = alpha a[i] + beta b[i] (doubles). */
+int ssad_axpby(const double *a, const double *b, double *out, double alpha, double beta, long long n, void *stream);
 int ssad_init_device(void);
 int ssad_group_sum(ssa_gsum_job job, void *stream);
 int ssad_spectrum(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);

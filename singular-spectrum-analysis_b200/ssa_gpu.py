@@ -96,6 +96,8 @@ _sig("mssa_opt_series_contributions", _I, _P, c_double_p)
 _sig("mssa_opt_variance_explained", _D, _P, _I, _I)
 _sig("mssa_opt_free", _V, _P)
 _sig("ssa_opt_copy_factors", _I, _P, c_double_p, c_double_p)
+_sig("mssa_opt_copy_factors", _I, _P, c_double_p, c_double_p, c_double_p)
+_sig("ssa_opt_cadzow_inplace", _I, _P, _I, _I, _D, ctypes.POINTER(_SSA_CadzowResult))
 _sig("ssa_b200_kernel_launches", ctypes.c_ulonglong)
 _sig("ssa_b200_sizeof_ssa_opt", _I)
 _sig("ssa_batch_create", _I, ctypes.POINTER(ctypes.c_void_p), _I, _I, _I, _I, _I, _I, c_int_p, c_int_p, _I)
@@ -312,6 +314,19 @@ class SSA:
     def cadzow(self, rank: int, max_iter: int = 20, tol: float = 1e-9, alpha: float = 1.0) -> CadzowResult:
         return cadzow(self._x, self.L, rank, max_iter, tol, alpha)
 
+    def cadzow_inplace(self, rank: int, max_iter: int = 20, tol: float = 1e-9) -> CadzowResult:
+        """In-place Cadzow on this context (ssa_opt_cadzow_inplace): the context's signal becomes
+        the iterate and its decomposition the last one; ``signal`` is its rank-``rank``
+        reconstruction."""
+        res = _SSA_CadzowResult()
+        ret = _lib.ssa_opt_cadzow_inplace(ctypes.byref(self._ctx), rank, max_iter, tol, ctypes.byref(res))
+        if ret < 0:
+            raise RuntimeError("in-place Cadzow iterations failed")
+        self._decomposed = True
+        self.n_components = int(_lib.ssa_opt_copy_factors(ctypes.byref(self._ctx), None, None))
+        return CadzowResult(self.reconstruct(list(range(rank))), res.iterations, res.final_diff,
+                            bool(res.converged))
+
     def wcorr_matrix(self) -> np.ndarray:
         self._need()
         k = self.n_components
@@ -402,9 +417,25 @@ class MSSA:
                                              _dp(om) if om is not None else None)
         if ret != 0:
             raise RuntimeError(f"MSSA decomposition failed (k={k})")
-        self.n_components = k
+        self.n_components = int(_lib.mssa_opt_copy_factors(ctypes.byref(self._ctx), None, None, None))
         self._decomposed = True
         return self
+
+    def factors(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """(U (M L x k), V (K x k), sigma (k)) of the last decomposition."""
+        if not self._decomposed:
+            raise RuntimeError("Call decompose() first")
+        k = self.n_components
+        U = np.zeros((k, self.M * self.L))
+        V = np.zeros((k, self.K))
+        s = np.zeros(k)
+        if _lib.mssa_opt_copy_factors(ctypes.byref(self._ctx), _dp(U), _dp(V), _dp(s)) != k:
+            raise RuntimeError("copy_factors failed")
+        return U.T.copy(), V.T.copy(), s
+
+    @property
+    def singular_values(self) -> np.ndarray:
+        return self.factors()[2]
 
     def reconstruct(self, series_idx: int, group: List[int]) -> np.ndarray:
         if not self._decomposed:
