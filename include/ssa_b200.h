@@ -6,6 +6,7 @@
 #ifndef SSA_B200_H
 #define SSA_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -86,6 +87,38 @@ int ssa_opt_copy_factors(const SSA_Opt *ssa, double *U, double *V);
 /* The same for a decomposed MSSA context: U ((M L) x k, channel m in rows m L .. m L + L - 1),
  * V (K x k) and sigma (k). Any pointer may be NULL. Returns k or -1. */
 int mssa_opt_copy_factors(const MSSA_Opt *mssa, double *U, double *V, double *sigma);
+
+/* ---- Uneven batches ------------------------------------------------------------------------
+ * B series of different lengths N[s], windows L[s] and ranks k[s] (common oversampling p and
+ * power iterations q) through the same pipeline as ssa_batch_*: randomized decomposition with
+ * the device generator (series s seeded seed ^ 0x9E3779B97F4A7C15 (s + 1), as in ssa_batch_*),
+ * all k[s] elementary reconstructions, W-correlation and group sums. Series are bucketed by FFT
+ * length (M = next power of two >= max(N, 32), N <= 32768); each bucket runs one launch per
+ * stage on its own stream and the buckets overlap on the device. No counterpart in the
+ * reference, whose API takes one series per context.
+ *
+ * Inputs and outputs are packed in series order: x holds N[s] doubles at sum_{t<s} N[t];
+ * sigma k'[s] at sum_{t<s} k'[t]; W k'[s]^2 (row-major) at sum_{t<s} k'[t]^2; groups
+ * n_groups x N[s] at n_groups sum_{t<s} N[t], where k'[s] = min(k[s], L[s], N[s] - L[s] + 1).
+ * ssa_rbatch_layout returns these offsets (4 per series: x, sigma, W, groups) and the four
+ * totals of the last run. Device buffers grow as needed and are reused across runs.
+ * Returns 0 / -1 (invalid shape, N > 32768, k + p > 64, or a series whose decomposition
+ * failed). */
+typedef struct ssa_rbatch ssa_rbatch;
+int ssa_rbatch_create(ssa_rbatch **out, int oversampling, int power_iters, const int *group_idx,
+                      const int *group_sizes, int n_groups);
+void ssa_rbatch_destroy(ssa_rbatch *b);
+int ssa_rbatch_run(ssa_rbatch *b, int B, const int *N, const int *L, const int *k, const double *x,
+                   uint64_t seed, double *sigma, double *W, double *groups);
+/* d_x in device memory; enqueues only (ssa_rbatch_sync waits and checks every series). */
+int ssa_rbatch_run_device(ssa_rbatch *b, int B, const int *N, const int *L, const int *k, const double *d_x,
+                          uint64_t seed);
+int ssa_rbatch_sync(ssa_rbatch *b);
+int ssa_rbatch_layout(const ssa_rbatch *b, size_t *offsets, size_t *totals);
+/* Device pointers of the packed outputs and the stream every run ends on (recon is NULL). */
+int ssa_rbatch_device_results(const ssa_rbatch *b, ssa_batch_results *out);
+int ssa_rbatch_set_profiling(ssa_rbatch *b, int on);
+int ssa_rbatch_profile(ssa_rbatch *b, double *ms, long long *launches, int nkinds);
 
 /* Stage profiler of a batch: with profiling on, every kernel launch of ssa_batch_run* is
  * bracketed by CUDA events on the batch stream. ssa_batch_profile waits for the stream and

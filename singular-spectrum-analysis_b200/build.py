@@ -18,7 +18,7 @@ INCLUDE = HERE.parent / "include"
 OUT = HERE / "libssa.so"
 BUILD = HERE / "_build"
 
-C_SOURCES = ["ssa_engine.c", "ssa_api.c", "ssa_batch.c", "ssa_mssa.c"]
+C_SOURCES = ["ssa_engine.c", "ssa_api.c", "ssa_batch.c", "ssa_mssa.c", "ssa_ragged.c"]
 CU_SOURCES = ["ssa_kernels.cu"]
 
 NVCC_FLAGS = [

@@ -123,6 +123,47 @@ int ssae_create(ssa_engine *e, int B, int N, int L, int kp, int k, cudaStream_t 
     return 0;
 }
 
+int ssae_create_light(ssa_engine *e, size_t arena_bytes, cudaStream_t stream)
+{
+    memset(e, 0, sizeof(*e));
+    CK(cudaGetDevice(&e->device));
+    CK(ssad_init_device());
+    {
+        const char *sc = getenv("SSA_SYNC_CHECK");
+        e->sync_check = sc && sc[0] == '1';
+    }
+    if (stream)
+    {
+        e->st = stream;
+    }
+    else
+    {
+        CK(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+        e->own_stream = 1;
+    }
+    return ssae_grow_arena(e, arena_bytes);
+}
+
+int ssae_grow_arena(ssa_engine *e, size_t bytes)
+{
+    if (bytes <= e->ja.cap)
+        return 0;
+    if (e->st)
+        CK(cudaStreamSynchronize(e->st));
+    if (e->ja.h)
+        cudaFreeHost(e->ja.h);
+    if (e->ja.d)
+        cudaFree(e->ja.d);
+    e->ja.h = NULL;
+    e->ja.d = NULL;
+    e->ja.cap = 0;
+    e->ja.used = 0;
+    CK(cudaMallocHost((void **)&e->ja.h, bytes));
+    CK(cudaMalloc((void **)&e->ja.d, bytes));
+    e->ja.cap = bytes;
+    return 0;
+}
+
 int ssae_set_profiling(ssa_engine *e, int on)
 {
     if (on && !e->ev[0])
@@ -221,11 +262,41 @@ int ssae_ensure_recon(ssa_engine *e)
 
 int ssae_ensure_spectra(ssa_engine *e)
 {
-    if (e->Us && e->Vs)
-        return 0;
     size_t bytes = (size_t)e->B * e->k * e->ldS * sizeof(float);
-    CK(dmalloc((void **)&e->Us, bytes));
-    return dmalloc((void **)&e->Vs, bytes);
+    if (!e->Us)
+        CK(dmalloc((void **)&e->Us, bytes));
+    if (!e->Vs)
+        CK(dmalloc((void **)&e->Vs, bytes));
+    return 0;
+}
+
+/* Spectra of sigma_i u_i only (into Us), for the one-buffer elementary reconstruction. */
+static int u_spectra(ssa_engine *e, int nb, int k)
+{
+    if (!e->Us)
+        CK(dmalloc((void **)&e->Us, (size_t)e->B * e->k * e->ldS * sizeof(float)));
+    ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)nb, sizeof(ssa_col_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    for (int s = 0; s < nb; s++)
+    {
+        ssa_col_job *Ju = &jobs[s];
+        Ju->in = e->Y + (size_t)s * e->ldL * e->kp;
+        Ju->ld_in = e->ldL;
+        Ju->n_in = e->L;
+        Ju->scale = e->sigma + (size_t)s * e->k;
+        Ju->spec = e->Us + (size_t)s * e->k * e->ldS;
+        Ju->ld_spec = e->ldS;
+        Ju->ncols = k;
+    }
+    void *d = ssae_push_jobs(e, jobs, sizeof(ssa_col_job) * nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_SPECTRUM);
+    int rc_ = ssad_spectrum((const ssa_col_job *)d, nb, k, e->logh, e->st);
+    ssae_prof_end(e);
+    return rc_;
 }
 
 void ssae_reset_jobs(ssa_engine *e)
@@ -530,6 +601,9 @@ int ssae_decompose(ssa_engine *e, int nb, int kp, int k, int q, const float *d_o
 int ssae_elem_recon(ssa_engine *e, int nb, int k)
 {
     CK(ssae_ensure_recon(e));
+    const int one_buffer = e->logh > SSA_ELEM2_MAX_LOGH;
+    if (one_buffer)
+        CK(u_spectra(e, nb, k));
     ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)nb, sizeof(ssa_col_job));
     if (!jobs)
         return (int)cudaErrorMemoryAllocation;
@@ -550,13 +624,19 @@ int ssae_elem_recon(ssa_engine *e, int nb, int k)
         J->N = e->N;
         J->L = e->L;
         J->K = e->K;
+        if (one_buffer)
+        {
+            J->spec = e->Us + (size_t)s * e->k * e->ldS;
+            J->ld_spec = e->ldS;
+        }
     }
     void *d = ssae_push_jobs(e, jobs, sizeof(ssa_col_job) * nb);
     free(jobs);
     if (!d)
         return (int)cudaErrorMemoryAllocation;
     ssae_prof_begin(e, SSAK_ELEM);
-    int rc_ = ssad_elem_recon((const ssa_col_job *)d, nb, k, e->logh, e->st);
+    int rc_ = one_buffer ? ssad_elem_recon1((const ssa_col_job *)d, nb, k, e->logh, e->st)
+                         : ssad_elem_recon((const ssa_col_job *)d, nb, k, e->logh, e->st);
     ssae_prof_end(e);
     return rc_;
 }

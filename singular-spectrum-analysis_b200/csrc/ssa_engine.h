@@ -107,6 +107,11 @@ int ssae_prof_collect(ssa_engine *e);
 
 /* Allocate buffers for up to B series. Returns 0 or a cudaError_t value. */
 int ssae_create(ssa_engine *e, int B, int N, int L, int kp, int k, cudaStream_t stream);
+/* Stream, job arena (arena_bytes) and profiler only, no series buffers: the uneven-batch
+ * pipeline (ssa_ragged.c) keeps its own buffers and drives the kernels through this. */
+int ssae_create_light(ssa_engine *e, size_t arena_bytes, cudaStream_t stream);
+/* Enlarge the job arena to at least `bytes` (waits for the stream first). */
+int ssae_grow_arena(ssa_engine *e, size_t bytes);
 void ssae_destroy(ssa_engine *e);
 int ssae_ensure_recon(ssa_engine *e);
 int ssae_ensure_spectra(ssa_engine *e);

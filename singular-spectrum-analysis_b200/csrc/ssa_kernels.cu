@@ -271,6 +271,74 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_elem_recon(const ssa_
     if (threadIdx.x == 0 && J.norm2) J.norm2[c] = acc;
 }
 
+// Elementary reconstruction with one FFT buffer: the spectrum of sigma_c u_c (bins 0..H of the
+// real length-2H transform, as k_spectrum writes it) comes from global memory; v_c is transformed
+// in shared memory. Same outputs as k_elem_recon.
+template <int LOGH>
+__global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_elem_recon1(const ssa_col_job* __restrict__ jobs) {
+    constexpr int H = 1 << LOGH;
+    extern __shared__ float2 smem[];
+    __shared__ double red[32];
+    float2* s2 = smem;
+    float2* tw = smem + spad_size(H);
+    const ssa_col_job J = jobs[blockIdx.y];
+    const int c = blockIdx.x;
+    if (c >= J.ncols) return;
+    load_twiddles<LOGH + 1>(tw);
+    load_real<LOGH>(s2, J.in2 + (long long)c * J.ld_in2, J.n_in2, 1.0f);
+    __syncthreads();
+    fft_block<LOGH, false>(s2, tw);
+    const float2* us = reinterpret_cast<const float2*>(J.spec + (long long)c * J.ld_spec);
+    for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
+        float2 zk, zm;
+        if (k == 0) {
+            const float2 b0 = s2[spad(0)];
+            const float p0 = us[0].x * (b0.x + b0.y);
+            const float ph = us[H].x * (b0.x - b0.y);
+            pack_pair(make_float2(p0, 0.f), make_float2(ph, 0.f), make_float2(1.f, 0.f), zk, zm);
+            s2[spad(0)] = zk;
+        } else {
+            const float2 w = wm<LOGH>(tw, k);
+            float2 bk, bm;
+            unpack_pair<LOGH>(s2[spad(k)], s2[spad(H - k)], w, bk, bm);
+            pack_pair(cmul(us[k], bk), cmul(us[H - k], bm), w, zk, zm);
+            s2[spad(k)] = zk;
+            s2[spad(H - k)] = zm;
+        }
+    }
+    __syncthreads();
+    fft_block<LOGH, true>(s2, tw);
+    float* out = J.out + (long long)c * J.ld_out;
+    const float inv_h = 1.0f / (float)H;
+    double acc = 0.0;
+    for (int t = threadIdx.x; t < J.N; t += blockDim.x) {
+        const float2 z = s2[spad(t >> 1)];
+        const float p = ((t & 1) ? z.y : z.x) * inv_h;
+        const int cnt = diag_count(t, J.N, J.L, J.K);
+        const float v = p / (float)cnt;
+        out[t] = v;
+        acc += (double)p * (double)p / (double)cnt;
+    }
+    acc = block_sum<double>(acc, red);
+    if (threadIdx.x == 0 && J.norm2) J.norm2[c] = acc;
+}
+
+// Group sums of an uneven batch: one job per series.
+__global__ void k_group_sum_ragged(const ssa_rgsum_job* __restrict__ jobs, const int* __restrict__ group_idx,
+                                   const int* __restrict__ group_off) {
+    const ssa_rgsum_job J = jobs[blockIdx.z];
+    const int g = blockIdx.y;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= J.N) return;
+    double acc = 0.0;
+    for (int e = group_off[g]; e < group_off[g + 1]; ++e) {
+        const int i = group_idx[e];
+        if (i < 0 || i >= J.k) continue;
+        acc += (double)J.recon[(long long)i * J.ld_recon + t];
+    }
+    J.out[(long long)g * J.N + t] = acc;
+}
+
 // Grouped reconstruction from cached spectra.
 template <int LOGH>
 __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k_recon(const ssa_recon_job* __restrict__ jobs) {
@@ -1176,6 +1244,14 @@ static int launch_elem(const ssa_col_job* jobs, int njobs, int maxcols, cudaStre
     return launched(cudaGetLastError());
 }
 template <int LOGH>
+static int launch_elem1(const ssa_col_job* jobs, int njobs, int maxcols, cudaStream_t st) {
+    const int sm = smem_bytes<LOGH>(1);
+    cudaError_t e = set_smem(k_elem_recon1<LOGH>, sm);
+    if (e != cudaSuccess) return (int)e;
+    k_elem_recon1<LOGH><<<dim3(maxcols, njobs), FftShape<LOGH>::BLOCK, sm, st>>>(jobs);
+    return launched(cudaGetLastError());
+}
+template <int LOGH>
 static int launch_recon(const ssa_recon_job* jobs, int njobs, cudaStream_t st) {
     const int sm = smem_bytes<LOGH>(1);
     cudaError_t e = set_smem(k_recon<LOGH>, sm);
@@ -1204,6 +1280,21 @@ extern "C" int ssad_elem_recon(const ssa_col_job* d_jobs, int njobs, int maxcols
     SSA_LOGH_DISPATCH(logh, CALL)
 #undef CALL
     return 0;
+}
+extern "C" int ssad_elem_recon1(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
+    if (njobs <= 0 || maxcols <= 0) return 0;
+#define CALL(L) return launch_elem1<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
+    SSA_LOGH_DISPATCH(logh, CALL)
+#undef CALL
+    return 0;
+}
+extern "C" int ssad_group_sum_ragged(const ssa_rgsum_job* d_jobs, int njobs, int maxN, const int* group_idx,
+                                     const int* group_off, int n_groups, void* stream) {
+    if (njobs <= 0 || n_groups <= 0 || maxN <= 0) return 0;
+    if (njobs > 65535 || n_groups > 65535) return (int)cudaErrorInvalidValue;
+    k_group_sum_ragged<<<dim3((maxN + 255) / 256, n_groups, njobs), 256, 0, (cudaStream_t)stream>>>(d_jobs, group_idx,
+                                                                                                    group_off);
+    return launched(cudaGetLastError());
 }
 extern "C" int ssad_recon(const ssa_recon_job* d_jobs, int njobs, int logh, void* stream) {
     if (njobs <= 0) return 0;

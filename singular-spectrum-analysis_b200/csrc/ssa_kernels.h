@@ -224,6 +224,23 @@ int ssad_diffnorm(const double *a, const double *b, long long n, double *out2, v
 int ssad_axpby(const double *a, const double *b, double *out, double alpha, double beta, long long n, void *stream);
 int ssad_init_device(void);
 int ssad_group_sum(ssa_gsum_job job, void *stream);
+/* Per-series group sums for uneven batches: out[g * N + t] = sum_{i in group g, i < k} recon[i * ld + t]
+ * for the series of each job (group index lists shared by all jobs). */
+typedef struct
+{
+    const float *recon;
+    double *out;          /* n_groups x N doubles */
+    long long ld_recon;
+    int N, k;
+} ssa_rgsum_job;
+int ssad_group_sum_ragged(const ssa_rgsum_job *d_jobs, int njobs, int maxN, const int *group_idx,
+                          const int *group_off, int n_groups, void *stream);
+/* Elementary reconstructions with one FFT buffer: the spectrum of sigma_c u_c is read from
+ * spec + c * ld_spec (written by ssad_spectrum), v_c from in2; outputs as ssad_elem_recon. For
+ * FFT lengths where two buffers exceed shared memory (logh >= 14). */
+int ssad_elem_recon1(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);
+/* Largest logh for which ssad_elem_recon (two shared-memory buffers) can run. */
+#define SSA_ELEM2_MAX_LOGH 13
 int ssad_spectrum(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);
 int ssad_corr(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);
 int ssad_elem_recon(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);

@@ -1,0 +1,945 @@
+/*
+ * Uneven batches: B series of different lengths N[s], windows L[s] and ranks k[s] through the
+ * randomized pipeline (decomposition with q power iterations, all k[s] elementary
+ * reconstructions, W-correlation, group sums) in one launch per stage per FFT-length bucket.
+ *
+ * The kernels are job-driven (every job carries its own dims, pointers and leading dims, and
+ * CTAs beyond a job's columns or rows return at once), so a bucket's launch covers series of any
+ * shape whose FFT length M = 2^(logh+1) is the bucket's. Each bucket owns a CUDA stream; the
+ * buckets of one run overlap on the device and join the batch's main stream at the end.
+ *
+ * Per-series layout inside a bucket (element offsets computed on the host per run):
+ *   X     [i * ldS]            signal spectrum (bucket-uniform ldS)
+ *   Y     [oY]  ldL x kp       range finder block, then U
+ *   Z     [oZ]  ldK x kp       Z block, then B, then V
+ *   part  [opart]              FP64 Gram partials, max(nch) * kp (kp + 1) / 2
+ *   qsum  [oqsum] nq x kp      column-sum partials of the final Q (sign rule)
+ *   R     [oR]  kp x kp        Cholesky factor of the last CholQR pass
+ *   Zu/Zv [oZu] kp x k         Ritz rotations
+ *   recon [orecon] k x ldN     elementary reconstructions
+ *   norm2 [onorm] k
+ *   Us    [ospec] k x ldS      spectra of sigma_i u_i (one-buffer reconstruction only)
+ * Batch-level packed arrays (series order): x (sum N), sigma (sum k), W (sum k^2),
+ * groups (n_groups * sum N), status (B).
+ */
+#include <stdlib.h>
+#include <string.h>
+
+#include <cuda_runtime_api.h>
+
+#include "ssa_engine.h"
+#include "../../include/ssa_opt.h"
+
+#define CK(x)                  \
+    do                         \
+    {                          \
+        int _e = (int)(x);     \
+        if (_e != 0)           \
+            return _e;         \
+    } while (0)
+
+#define RB_MIN_LOGH 4
+#define RB_MAX_LOGH 14
+#define RB_NB (RB_MAX_LOGH + 1)
+
+typedef struct
+{
+    int src; /* index in the batch */
+    int N, L, K, kp, k;
+    long long ldL, ldK, ldN;
+    int rows_L, rows_K, rows_N, nch_L, nch_K, nch_N, nq;
+    size_t oY, oZ, opart, oqsum, oR, oZu, orecon, onorm, ospec;
+    size_t ox, osig, oW, ogrp;
+} rser;
+
+typedef struct
+{
+    ssa_engine e; /* stream, job arena, profiler */
+    int live;
+    int logh;
+    long long ldS;
+    int nb, cap_nb;
+    rser *sd;
+    float *X, *Y, *Z, *R, *Zu, *Zv, *recon, *Us;
+    double *part, *qsum, *norm2;
+    size_t cX, cY, cZ, cR, cZu, cZv, crecon, cUs, cpart, cqsum, cnorm;
+    cudaEvent_t done;
+} rbucket;
+
+struct ssa_rbatch
+{
+    int p, q, n_groups, total_idx;
+    int *d_gidx, *d_goff;
+    rbucket bk[RB_NB];
+    cudaStream_t main;
+    cudaEvent_t ev_in;
+    int prof;
+    double *d_xs;
+    size_t c_xs;
+    double *sigma, *W, *groups;
+    size_t c_sig, c_W, c_grp;
+    int *status;
+    int c_status;
+    int B;
+    size_t n_x, n_sig, n_W, n_grp;
+    size_t *h_off; /* 4 B offsets of the last run: x, sigma, W, groups */
+};
+
+static int imin(int a, int b) { return a < b ? a : b; }
+static int imax(int a, int b) { return a > b ? a : b; }
+static long long round4(long long v) { return (v + 3) & ~3LL; }
+
+static int gram_rows(int m, int nb)
+{
+    /* about two CTAs per SM over the bucket's series; at least one staging chunk per CTA */
+    int target = 296 / (nb > 0 ? nb : 1);
+    if (target < 1)
+        target = 1;
+    int rows = (m + target - 1) / target;
+    rows = ((rows + SSA_GRAM_CHUNK - 1) / SSA_GRAM_CHUNK) * SSA_GRAM_CHUNK;
+    return imax(rows, SSA_GRAM_CHUNK);
+}
+
+/* Grow a device buffer to at least `need` elements of `elem` bytes (contents not kept). */
+static int grow(void **p, size_t *cap, size_t need, size_t elem)
+{
+    if (need <= *cap && *p)
+        return 0;
+    if (*p)
+        cudaFree(*p);
+    *p = NULL;
+    *cap = 0;
+    if (need == 0)
+        return 0;
+    size_t n = need + need / 8;
+    CK(cudaMalloc(p, n * elem));
+    *cap = n;
+    return 0;
+}
+
+static void bucket_free(rbucket *b)
+{
+    if (!b->live)
+        return;
+    ssae_destroy(&b->e); /* stream, arena, profiler events */
+    void *bufs[] = {b->X, b->Y, b->Z, b->R, b->Zu, b->Zv, b->recon, b->Us, b->part, b->qsum, b->norm2};
+    for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
+        if (bufs[i])
+            cudaFree(bufs[i]);
+    if (b->done)
+        cudaEventDestroy(b->done);
+    free(b->sd);
+    memset(b, 0, sizeof(*b));
+}
+
+void ssa_rbatch_destroy(ssa_rbatch *rb)
+{
+    if (!rb)
+        return;
+    if (rb->main)
+        cudaStreamSynchronize(rb->main);
+    for (int i = 0; i < RB_NB; i++)
+        bucket_free(&rb->bk[i]);
+    void *bufs[] = {rb->d_gidx, rb->d_goff, rb->d_xs, rb->sigma, rb->W, rb->groups, rb->status};
+    for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
+        if (bufs[i])
+            cudaFree(bufs[i]);
+    if (rb->ev_in)
+        cudaEventDestroy(rb->ev_in);
+    if (rb->main)
+        cudaStreamDestroy(rb->main);
+    free(rb->h_off);
+    free(rb);
+}
+
+int ssa_rbatch_create(ssa_rbatch **out, int oversampling, int power_iters, const int *group_idx,
+                      const int *group_sizes, int n_groups)
+{
+    if (!out || power_iters < 0 || n_groups < 0 || (n_groups > 0 && (!group_idx || !group_sizes)))
+        return -1;
+    *out = NULL;
+    ssa_rbatch *rb = (ssa_rbatch *)calloc(1, sizeof(*rb));
+    if (!rb)
+        return -1;
+    rb->p = oversampling <= 0 ? 8 : oversampling;
+    rb->q = power_iters;
+    rb->n_groups = n_groups;
+    if (ssad_init_device() != 0 || cudaStreamCreateWithFlags(&rb->main, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&rb->ev_in, cudaEventDisableTiming) != cudaSuccess)
+    {
+        ssa_rbatch_destroy(rb);
+        return -1;
+    }
+    if (n_groups > 0)
+    {
+        int *off = (int *)malloc(sizeof(int) * (n_groups + 1));
+        if (!off)
+        {
+            ssa_rbatch_destroy(rb);
+            return -1;
+        }
+        off[0] = 0;
+        for (int g = 0; g < n_groups; g++)
+            off[g + 1] = off[g] + (group_sizes[g] > 0 ? group_sizes[g] : 0);
+        rb->total_idx = off[n_groups];
+        int rc = cudaMalloc((void **)&rb->d_goff, sizeof(int) * (n_groups + 1)) != cudaSuccess;
+        rc |= cudaMalloc((void **)&rb->d_gidx, sizeof(int) * (rb->total_idx > 0 ? rb->total_idx : 1)) != cudaSuccess;
+        if (!rc)
+            rc |= cudaMemcpy(rb->d_goff, off, sizeof(int) * (n_groups + 1), cudaMemcpyHostToDevice) != cudaSuccess;
+        if (!rc && rb->total_idx > 0)
+            rc |= cudaMemcpy(rb->d_gidx, group_idx, sizeof(int) * rb->total_idx, cudaMemcpyHostToDevice) !=
+                  cudaSuccess;
+        free(off);
+        if (rc)
+        {
+            ssa_rbatch_destroy(rb);
+            return -1;
+        }
+    }
+    *out = rb;
+    return 0;
+}
+
+static int bucket_setup(rbucket *b, int logh, int prof)
+{
+    if (!b->live)
+    {
+        CK(ssae_create_light(&b->e, 1 << 20, NULL));
+        CK(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
+        b->live = 1;
+    }
+    if (prof && !b->e.prof)
+        CK(ssae_set_profiling(&b->e, 1));
+    b->logh = logh;
+    b->ldS = round4(2LL * ((1 << logh) + 1) + 2);
+    return 0;
+}
+
+/* ---- stages ------------------------------------------------------------------------------ */
+
+static int r_spectrum(rbucket *b, const double *d_x)
+{
+    ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)b->nb, sizeof(ssa_col_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    for (int i = 0; i < b->nb; i++)
+    {
+        const rser *S = &b->sd[i];
+        ssa_col_job *J = &jobs[i];
+        J->in64 = d_x + S->ox;
+        J->ld_in = S->N;
+        J->n_in = S->N;
+        J->spec = b->X + (size_t)i * b->ldS;
+        J->ld_spec = b->ldS;
+        J->ncols = 1;
+        J->N = S->N;
+        J->L = S->L;
+        J->K = S->K;
+    }
+    void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_col_job) * b->nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(&b->e, SSAK_SPECTRUM);
+    int rc = ssad_spectrum((const ssa_col_job *)d, b->nb, 1, b->logh, b->e.st);
+    ssae_prof_end(&b->e);
+    return rc;
+}
+
+/* adjoint 0: Y = H (Omega | Z); adjoint 1: Z = H^T Y. generate: Omega from the device generator. */
+static int r_sweep(rbucket *b, int adjoint, int generate, unsigned long long seed)
+{
+    ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)b->nb, sizeof(ssa_col_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    int maxc = 0;
+    for (int i = 0; i < b->nb; i++)
+    {
+        const rser *S = &b->sd[i];
+        ssa_col_job *J = &jobs[i];
+        float *Ys = b->Y + S->oY, *Zs = b->Z + S->oZ;
+        if (!adjoint)
+        {
+            if (generate)
+            {
+                J->in = NULL;
+                J->seed = seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(S->src + 1));
+            }
+            else
+            {
+                J->in = Zs;
+                J->ld_in = S->ldK;
+            }
+            J->n_in = S->K;
+            J->out = Ys;
+            J->ld_out = S->ldL;
+            J->n_out = S->L;
+        }
+        else
+        {
+            J->in = Ys;
+            J->ld_in = S->ldL;
+            J->n_in = S->L;
+            J->out = Zs;
+            J->ld_out = S->ldK;
+            J->n_out = S->K;
+        }
+        J->X = b->X + (size_t)i * b->ldS;
+        J->ncols = S->kp;
+        J->N = S->N;
+        J->L = S->L;
+        J->K = S->K;
+        maxc = imax(maxc, S->kp);
+    }
+    void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_col_job) * b->nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(&b->e, SSAK_CORR);
+    int rc = ssad_corr((const ssa_col_job *)d, b->nb, maxc, b->logh, b->e.st);
+    ssae_prof_end(&b->e);
+    return rc;
+}
+
+enum
+{
+    SIDE_L = 0, /* Y blocks, L x kp */
+    SIDE_K = 1, /* Z blocks, K x kp */
+    SIDE_N = 2  /* elementary reconstructions, N x k, weighted */
+};
+
+static int r_gram(rbucket *b, int side)
+{
+    ssa_gram_job *jobs = (ssa_gram_job *)calloc((size_t)b->nb, sizeof(ssa_gram_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    int maxch = 0;
+    for (int i = 0; i < b->nb; i++)
+    {
+        const rser *S = &b->sd[i];
+        ssa_gram_job *J = &jobs[i];
+        if (side == SIDE_L)
+        {
+            J->A = b->Y + S->oY;
+            J->ld = S->ldL;
+            J->m = S->L;
+            J->n = S->kp;
+            J->rows_per_cta = S->rows_L;
+            maxch = imax(maxch, S->nch_L);
+        }
+        else if (side == SIDE_K)
+        {
+            J->A = b->Z + S->oZ;
+            J->ld = S->ldK;
+            J->m = S->K;
+            J->n = S->kp;
+            J->rows_per_cta = S->rows_K;
+            maxch = imax(maxch, S->nch_K);
+        }
+        else
+        {
+            J->A = b->recon + S->orecon;
+            J->ld = S->ldN;
+            J->m = S->N;
+            J->n = S->k;
+            J->rows_per_cta = S->rows_N;
+            J->weighted = 1;
+            maxch = imax(maxch, S->nch_N);
+        }
+        J->part = b->part + S->opart;
+        J->N = S->N;
+        J->L = S->L;
+        J->K = S->K;
+    }
+    void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_gram_job) * b->nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(&b->e, SSAK_GRAM);
+    int rc = ssad_gram((const ssa_gram_job *)d, b->nb, maxch, side == SIDE_N, b->e.st);
+    ssae_prof_end(&b->e);
+    return rc;
+}
+
+static int r_chol(rbucket *b, int side, int *status)
+{
+    ssa_chol_job *jobs = (ssa_chol_job *)calloc((size_t)b->nb, sizeof(ssa_chol_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    for (int i = 0; i < b->nb; i++)
+    {
+        const rser *S = &b->sd[i];
+        ssa_chol_job *J = &jobs[i];
+        J->part = b->part + S->opart;
+        J->R = b->R + S->oR;
+        J->status = status + S->src;
+        J->nchunks = side == SIDE_L ? S->nch_L : S->nch_K;
+        J->n = S->kp;
+    }
+    void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_chol_job) * b->nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(&b->e, SSAK_CHOL);
+    int rc = ssad_chol((const ssa_chol_job *)d, b->nb, b->e.st);
+    ssae_prof_end(&b->e);
+    return rc;
+}
+
+/* trsm: A = A R^{-1} in place (column-sum partials into qsum when `colsum`);
+ * else A[:, :k] = A Zrot (U = Q Zu on the L side, V = B Zv on the K side). */
+static int r_rowmul(rbucket *b, int side, int trsm, int colsum)
+{
+    ssa_rowmul_job *jobs = (ssa_rowmul_job *)calloc((size_t)b->nb, sizeof(ssa_rowmul_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    int maxm = 0, maxn = 0;
+    for (int i = 0; i < b->nb; i++)
+    {
+        const rser *S = &b->sd[i];
+        ssa_rowmul_job *J = &jobs[i];
+        float *A = side == SIDE_L ? b->Y + S->oY : b->Z + S->oZ;
+        const long long ld = side == SIDE_L ? S->ldL : S->ldK;
+        const int m = side == SIDE_L ? S->L : S->K;
+        J->A = A;
+        J->C = A;
+        J->lda = ld;
+        J->ldc = ld;
+        J->m = m;
+        J->n = S->kp;
+        J->ldb = S->kp;
+        if (trsm)
+        {
+            J->Bm = b->R + S->oR;
+            J->p = S->kp;
+            J->trsm = 1;
+            J->colsum = colsum ? b->qsum + S->oqsum : NULL;
+        }
+        else
+        {
+            J->Bm = (side == SIDE_L ? b->Zu : b->Zv) + S->oZu;
+            J->p = S->k;
+        }
+        maxm = imax(maxm, m);
+        maxn = imax(maxn, S->kp);
+    }
+    void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_rowmul_job) * b->nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(&b->e, SSAK_ROWMUL);
+    int rc = ssad_rowmul((const ssa_rowmul_job *)d, b->nb, maxm, maxn, b->e.st);
+    ssae_prof_end(&b->e);
+    return rc;
+}
+
+static int r_cholqr(rbucket *b, int side, int colsum, int *status)
+{
+    CK(r_gram(b, side));
+    CK(r_chol(b, side, status));
+    return r_rowmul(b, side, 1, colsum);
+}
+
+static int r_rr(rbucket *b, double *sigma, int *status)
+{
+    ssa_rr_job *jobs = (ssa_rr_job *)calloc((size_t)b->nb, sizeof(ssa_rr_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    for (int i = 0; i < b->nb; i++)
+    {
+        const rser *S = &b->sd[i];
+        ssa_rr_job *J = &jobs[i];
+        J->part = b->part + S->opart;
+        J->qsum = b->qsum + S->oqsum;
+        J->sigma = sigma + S->osig;
+        J->Zu = b->Zu + S->oZu;
+        J->Zv = b->Zv + S->oZu;
+        J->status = status + S->src;
+        J->nchunks = S->nch_K;
+        J->nchunks_q = S->nq;
+        J->kp = S->kp;
+        J->k = S->k;
+    }
+    void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_rr_job) * b->nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(&b->e, SSAK_RR);
+    int rc = ssad_rr((const ssa_rr_job *)d, b->nb, b->e.st);
+    ssae_prof_end(&b->e);
+    return rc;
+}
+
+static int r_elem(rbucket *b, const double *sigma)
+{
+    const int one = b->logh > SSA_ELEM2_MAX_LOGH;
+    ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)b->nb, sizeof(ssa_col_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    int maxk = 0;
+    if (one)
+    {
+        /* spectra of sigma_i u_i first; the reconstruction kernel then holds one FFT buffer */
+        for (int i = 0; i < b->nb; i++)
+        {
+            const rser *S = &b->sd[i];
+            ssa_col_job *J = &jobs[i];
+            J->in = b->Y + S->oY;
+            J->ld_in = S->ldL;
+            J->n_in = S->L;
+            J->scale = sigma + S->osig;
+            J->spec = b->Us + S->ospec;
+            J->ld_spec = b->ldS;
+            J->ncols = S->k;
+            maxk = imax(maxk, S->k);
+        }
+        void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_col_job) * b->nb);
+        if (!d)
+        {
+            free(jobs);
+            return (int)cudaErrorMemoryAllocation;
+        }
+        ssae_prof_begin(&b->e, SSAK_SPECTRUM);
+        int rc = ssad_spectrum((const ssa_col_job *)d, b->nb, maxk, b->logh, b->e.st);
+        ssae_prof_end(&b->e);
+        if (rc)
+        {
+            free(jobs);
+            return rc;
+        }
+        memset(jobs, 0, sizeof(ssa_col_job) * b->nb);
+    }
+    for (int i = 0; i < b->nb; i++)
+    {
+        const rser *S = &b->sd[i];
+        ssa_col_job *J = &jobs[i];
+        J->in = b->Y + S->oY;
+        J->ld_in = S->ldL;
+        J->n_in = S->L;
+        J->in2 = b->Z + S->oZ;
+        J->ld_in2 = S->ldK;
+        J->n_in2 = S->K;
+        J->scale = sigma + S->osig;
+        J->out = b->recon + S->orecon;
+        J->ld_out = S->ldN;
+        J->norm2 = b->norm2 + S->onorm;
+        J->ncols = S->k;
+        J->N = S->N;
+        J->L = S->L;
+        J->K = S->K;
+        if (one)
+        {
+            J->spec = b->Us + S->ospec;
+            J->ld_spec = b->ldS;
+        }
+        maxk = imax(maxk, S->k);
+    }
+    void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_col_job) * b->nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(&b->e, SSAK_ELEM);
+    int rc = one ? ssad_elem_recon1((const ssa_col_job *)d, b->nb, maxk, b->logh, b->e.st)
+                 : ssad_elem_recon((const ssa_col_job *)d, b->nb, maxk, b->logh, b->e.st);
+    ssae_prof_end(&b->e);
+    return rc;
+}
+
+static int r_wcorr(rbucket *b, double *W)
+{
+    CK(r_gram(b, SIDE_N));
+    ssa_wfin_job *jobs = (ssa_wfin_job *)calloc((size_t)b->nb, sizeof(ssa_wfin_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    for (int i = 0; i < b->nb; i++)
+    {
+        const rser *S = &b->sd[i];
+        jobs[i].part = b->part + S->opart;
+        jobs[i].W = W + S->oW;
+        jobs[i].nchunks = S->nch_N;
+        jobs[i].k = S->k;
+    }
+    void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_wfin_job) * b->nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(&b->e, SSAK_WFIN);
+    int rc = ssad_wfin((const ssa_wfin_job *)d, b->nb, b->e.st);
+    ssae_prof_end(&b->e);
+    return rc;
+}
+
+static int r_gsum(rbucket *b, ssa_rbatch *rb)
+{
+    ssa_rgsum_job *jobs = (ssa_rgsum_job *)calloc((size_t)b->nb, sizeof(ssa_rgsum_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    int maxN = 0;
+    for (int i = 0; i < b->nb; i++)
+    {
+        const rser *S = &b->sd[i];
+        jobs[i].recon = b->recon + S->orecon;
+        jobs[i].ld_recon = S->ldN;
+        jobs[i].out = rb->groups + S->ogrp;
+        jobs[i].N = S->N;
+        jobs[i].k = S->k;
+        maxN = imax(maxN, S->N);
+    }
+    void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_rgsum_job) * b->nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(&b->e, SSAK_GSUM);
+    int rc = ssad_group_sum_ragged((const ssa_rgsum_job *)d, b->nb, maxN, rb->d_gidx, rb->d_goff, rb->n_groups,
+                                   b->e.st);
+    ssae_prof_end(&b->e);
+    return rc;
+}
+
+/* Whole pipeline of one bucket on its stream (the stage order of ssae_decompose,
+ * ssae_elem_recon, ssae_wcorr and the batch group sums). */
+static int bucket_run(rbucket *b, ssa_rbatch *rb, const double *d_x, unsigned long long seed)
+{
+    CK(r_spectrum(b, d_x));
+    CK(r_sweep(b, 0, 1, seed));
+    for (int it = 0; it < rb->q; it++)
+    {
+        CK(r_cholqr(b, SIDE_L, 0, rb->status));
+        CK(r_sweep(b, 1, 0, 0));
+        CK(r_cholqr(b, SIDE_K, 0, rb->status));
+        CK(r_sweep(b, 0, 0, 0));
+    }
+    CK(r_cholqr(b, SIDE_L, 0, rb->status));
+    CK(r_cholqr(b, SIDE_L, 1, rb->status));
+    CK(r_sweep(b, 1, 0, 0));
+    CK(r_gram(b, SIDE_K));
+    CK(r_rr(b, rb->sigma, rb->status));
+    CK(r_rowmul(b, SIDE_L, 0, 0));
+    CK(r_rowmul(b, SIDE_K, 0, 0));
+    CK(r_elem(b, rb->sigma));
+    CK(r_wcorr(b, rb->W));
+    if (rb->n_groups > 0)
+        CK(r_gsum(b, rb));
+    return 0;
+}
+
+/* Validate, assign series to buckets, compute every offset and size the buffers. */
+static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
+{
+    for (int s = 0; s < B; s++)
+    {
+        if (N[s] < 4 || L[s] < 2 || L[s] > N[s] - 1 || k[s] < 1)
+            return -1;
+        const int K = N[s] - L[s] + 1;
+        const int kp = imin(k[s] + rb->p, imin(L[s], K));
+        if (kp > SSA_MAX_KP)
+            return -1;
+        const int logh = ssad_logh_for(N[s]);
+        if (logh > RB_MAX_LOGH || logh < RB_MIN_LOGH)
+            return -1;
+    }
+    int count[RB_NB] = {0};
+    for (int s = 0; s < B; s++)
+        count[ssad_logh_for(N[s])]++;
+    for (int g = 0; g < RB_NB; g++)
+        if (count[g] > 65535) /* the job index is blockIdx.y in the column kernels */
+            return -1;
+    for (int g = 0; g < RB_NB; g++)
+    {
+        rbucket *b = &rb->bk[g];
+        b->nb = 0;
+        if (!count[g])
+            continue;
+        if (bucket_setup(b, g, rb->prof) != 0)
+            return -1;
+        if (count[g] > b->cap_nb)
+        {
+            rser *sd = (rser *)realloc(b->sd, sizeof(rser) * count[g]);
+            if (!sd)
+                return -1;
+            b->sd = sd;
+            b->cap_nb = count[g];
+        }
+    }
+    /* packed batch offsets */
+    size_t ox = 0, osig = 0, oW = 0, ogrp = 0;
+    for (int s = 0; s < B; s++)
+    {
+        rbucket *b = &rb->bk[ssad_logh_for(N[s])];
+        rser *S = &b->sd[b->nb++];
+        memset(S, 0, sizeof(*S));
+        S->src = s;
+        S->N = N[s];
+        S->L = L[s];
+        S->K = N[s] - L[s] + 1;
+        S->kp = imin(k[s] + rb->p, imin(S->L, S->K));
+        S->k = imin(k[s], S->kp);
+        S->ox = ox;
+        S->osig = osig;
+        S->oW = oW;
+        S->ogrp = ogrp;
+        ox += (size_t)S->N;
+        osig += (size_t)S->k;
+        oW += (size_t)S->k * S->k;
+        ogrp += (size_t)rb->n_groups * S->N;
+        rb->h_off[4 * s + 0] = S->ox;
+        rb->h_off[4 * s + 1] = S->osig;
+        rb->h_off[4 * s + 2] = S->oW;
+        rb->h_off[4 * s + 3] = S->ogrp;
+    }
+    rb->n_x = ox;
+    rb->n_sig = osig;
+    rb->n_W = oW;
+    rb->n_grp = ogrp;
+    /* per-bucket offsets and buffers */
+    for (int g = 0; g < RB_NB; g++)
+    {
+        rbucket *b = &rb->bk[g];
+        if (!b->nb)
+            continue;
+        size_t oY = 0, oZ = 0, opart = 0, oqsum = 0, oR = 0, oZu = 0, orecon = 0, onorm = 0, ospec = 0;
+        for (int i = 0; i < b->nb; i++)
+        {
+            rser *S = &b->sd[i];
+            S->ldL = round4(S->L);
+            S->ldK = round4(S->K);
+            S->ldN = round4(S->N);
+            S->rows_L = gram_rows(S->L, b->nb);
+            S->rows_K = gram_rows(S->K, b->nb);
+            S->rows_N = gram_rows(S->N, b->nb);
+            S->nch_L = (S->L + S->rows_L - 1) / S->rows_L;
+            S->nch_K = (S->K + S->rows_K - 1) / S->rows_K;
+            S->nch_N = (S->N + S->rows_N - 1) / S->rows_N;
+            S->nq = (S->L + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS;
+            S->oY = oY;
+            S->oZ = oZ;
+            S->opart = opart;
+            S->oqsum = oqsum;
+            S->oR = oR;
+            S->oZu = oZu;
+            S->orecon = orecon;
+            S->onorm = onorm;
+            S->ospec = ospec;
+            oY += (size_t)S->ldL * S->kp;
+            oZ += (size_t)S->ldK * S->kp;
+            opart += (size_t)imax(S->nch_L, imax(S->nch_K, S->nch_N)) * S->kp * (S->kp + 1) / 2;
+            oqsum += (size_t)S->nq * S->kp;
+            oR += (size_t)S->kp * S->kp;
+            oZu += (size_t)S->kp * S->k;
+            orecon += (size_t)S->k * S->ldN;
+            onorm += (size_t)S->k;
+            ospec += (size_t)S->k * b->ldS;
+        }
+        /* one run pushes 13 + 6 q job tables of at most sizeof(ssa_col_job) bytes per series,
+         * each 16-byte aligned */
+        const size_t arena = ((size_t)b->nb * sizeof(ssa_col_job) + 16) * (size_t)(16 + 6 * rb->q) + (1 << 16);
+        int rc = ssae_grow_arena(&b->e, arena);
+        rc |= grow((void **)&b->X, &b->cX, (size_t)b->nb * b->ldS, sizeof(float));
+        rc |= grow((void **)&b->Y, &b->cY, oY, sizeof(float));
+        rc |= grow((void **)&b->Z, &b->cZ, oZ, sizeof(float));
+        rc |= grow((void **)&b->part, &b->cpart, opart, sizeof(double));
+        rc |= grow((void **)&b->qsum, &b->cqsum, oqsum, sizeof(double));
+        rc |= grow((void **)&b->R, &b->cR, oR, sizeof(float));
+        rc |= grow((void **)&b->Zu, &b->cZu, oZu, sizeof(float));
+        rc |= grow((void **)&b->Zv, &b->cZv, oZu, sizeof(float));
+        rc |= grow((void **)&b->recon, &b->crecon, orecon, sizeof(float));
+        rc |= grow((void **)&b->norm2, &b->cnorm, onorm, sizeof(double));
+        if (b->logh > SSA_ELEM2_MAX_LOGH)
+            rc |= grow((void **)&b->Us, &b->cUs, ospec, sizeof(float));
+        if (rc)
+            return -1;
+    }
+    int rc = 0;
+    rc |= grow((void **)&rb->sigma, &rb->c_sig, rb->n_sig, sizeof(double));
+    rc |= grow((void **)&rb->W, &rb->c_W, rb->n_W, sizeof(double));
+    if (rb->n_groups > 0)
+        rc |= grow((void **)&rb->groups, &rb->c_grp, rb->n_grp, sizeof(double));
+    if (B > rb->c_status)
+    {
+        if (rb->status)
+            cudaFree(rb->status);
+        rb->status = NULL;
+        rb->c_status = 0;
+        if (cudaMalloc((void **)&rb->status, sizeof(int) * B) != cudaSuccess)
+            return -1;
+        rb->c_status = B;
+    }
+    return rc ? -1 : 0;
+}
+
+/* ---- entry points ------------------------------------------------------------------------ */
+
+/* Wait for the previous run on every stream and reset the job arenas. */
+static int quiesce(ssa_rbatch *rb)
+{
+    int rc = cudaStreamSynchronize(rb->main) != cudaSuccess;
+    for (int g = 0; g < RB_NB; g++)
+        if (rb->bk[g].live)
+            ssae_reset_jobs(&rb->bk[g].e);
+    return rc ? -1 : 0;
+}
+
+static int ensure_hoff(ssa_rbatch *rb, int B)
+{
+    size_t *h = (size_t *)realloc(rb->h_off, sizeof(size_t) * 4 * (size_t)B);
+    if (!h)
+        return -1;
+    rb->h_off = h;
+    return 0;
+}
+
+/* Enqueue a run whose packed input d_x is ready at the main stream's current position. */
+static int run_enqueue(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k, const double *d_x,
+                       unsigned long long seed)
+{
+    if (ensure_hoff(rb, B) != 0 || plan(rb, B, N, L, k) != 0)
+        return -1;
+    rb->B = B;
+    if (cudaMemsetAsync(rb->status, 0, sizeof(int) * B, rb->main) != cudaSuccess ||
+        cudaEventRecord(rb->ev_in, rb->main) != cudaSuccess)
+        return -1;
+    /* largest FFT lengths first: they take longest */
+    for (int g = RB_NB - 1; g >= 0; g--)
+    {
+        rbucket *b = &rb->bk[g];
+        if (!b->nb)
+            continue;
+        if (cudaStreamWaitEvent(b->e.st, rb->ev_in, 0) != cudaSuccess || bucket_run(b, rb, d_x, seed) != 0 ||
+            cudaEventRecord(b->done, b->e.st) != cudaSuccess ||
+            cudaStreamWaitEvent(rb->main, b->done, 0) != cudaSuccess)
+            return -1;
+    }
+    return 0;
+}
+
+int ssa_rbatch_run_device(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k, const double *d_x,
+                          uint64_t seed)
+{
+    if (!rb || B < 1 || !N || !L || !k || !d_x)
+        return -1;
+    if (quiesce(rb) != 0)
+        return -1;
+    return run_enqueue(rb, B, N, L, k, d_x, (unsigned long long)seed);
+}
+
+int ssa_rbatch_sync(ssa_rbatch *rb)
+{
+    if (!rb)
+        return -1;
+    if (cudaStreamSynchronize(rb->main) != cudaSuccess)
+        return -1;
+    if (rb->B <= 0)
+        return 0;
+    int *st = (int *)malloc(sizeof(int) * rb->B);
+    if (!st)
+        return -1;
+    int rc = cudaMemcpy(st, rb->status, sizeof(int) * rb->B, cudaMemcpyDeviceToHost) != cudaSuccess;
+    for (int s = 0; s < rb->B && !rc; s++)
+        if (st[s] != 0)
+            rc = 1;
+    free(st);
+    return rc ? -1 : 0;
+}
+
+int ssa_rbatch_run(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k, const double *x, uint64_t seed,
+                   double *sigma, double *W, double *groups)
+{
+    if (!rb || B < 1 || !N || !L || !k || !x)
+        return -1;
+    size_t nx = 0;
+    for (int s = 0; s < B; s++)
+    {
+        if (N[s] < 1)
+            return -1;
+        nx += (size_t)N[s];
+    }
+    if (quiesce(rb) != 0 || grow((void **)&rb->d_xs, &rb->c_xs, nx, sizeof(double)) != 0)
+        return -1;
+    if (cudaMemcpyAsync(rb->d_xs, x, sizeof(double) * nx, cudaMemcpyHostToDevice, rb->main) != cudaSuccess)
+        return -1;
+    if (run_enqueue(rb, B, N, L, k, rb->d_xs, (unsigned long long)seed) != 0)
+        return -1;
+    if (sigma && cudaMemcpyAsync(sigma, rb->sigma, sizeof(double) * rb->n_sig, cudaMemcpyDeviceToHost, rb->main) !=
+                     cudaSuccess)
+        return -1;
+    if (W && cudaMemcpyAsync(W, rb->W, sizeof(double) * rb->n_W, cudaMemcpyDeviceToHost, rb->main) != cudaSuccess)
+        return -1;
+    if (groups && rb->n_groups > 0 &&
+        cudaMemcpyAsync(groups, rb->groups, sizeof(double) * rb->n_grp, cudaMemcpyDeviceToHost, rb->main) !=
+            cudaSuccess)
+        return -1;
+    return ssa_rbatch_sync(rb);
+}
+
+int ssa_rbatch_layout(const ssa_rbatch *rb, size_t *offsets, size_t *totals)
+{
+    if (!rb || rb->B <= 0)
+        return -1;
+    if (offsets)
+        memcpy(offsets, rb->h_off, sizeof(size_t) * 4 * (size_t)rb->B);
+    if (totals)
+    {
+        totals[0] = rb->n_x;
+        totals[1] = rb->n_sig;
+        totals[2] = rb->n_W;
+        totals[3] = rb->n_grp;
+    }
+    return rb->B;
+}
+
+int ssa_rbatch_device_results(const ssa_rbatch *rb, ssa_batch_results *out)
+{
+    if (!rb || !out)
+        return -1;
+    memset(out, 0, sizeof(*out));
+    out->sigma = rb->sigma;
+    out->W = rb->W;
+    out->groups = rb->groups;
+    out->status = rb->status;
+    out->stream = (void *)rb->main;
+    return 0;
+}
+
+int ssa_rbatch_set_profiling(ssa_rbatch *rb, int on)
+{
+    if (!rb)
+        return -1;
+    rb->prof = on;
+    for (int g = 0; g < RB_NB; g++)
+        if (rb->bk[g].live && ssae_set_profiling(&rb->bk[g].e, on) != 0)
+            return -1;
+    return 0;
+}
+
+/* Stage times summed over the buckets (buckets overlap on the device, so the sum can exceed the
+ * wall time of a run). */
+int ssa_rbatch_profile(ssa_rbatch *rb, double *ms, long long *launches, int nkinds)
+{
+    if (!rb || !ms || !launches)
+        return -1;
+    const int n = nkinds < SSAK_NKINDS ? nkinds : SSAK_NKINDS;
+    for (int k = 0; k < n; k++)
+    {
+        ms[k] = 0.0;
+        launches[k] = 0;
+    }
+    for (int g = 0; g < RB_NB; g++)
+    {
+        rbucket *b = &rb->bk[g];
+        if (!b->live)
+            continue;
+        if (ssae_prof_collect(&b->e) != 0)
+            return -1;
+        for (int k = 0; k < n; k++)
+        {
+            ms[k] += b->e.prof_ms[k];
+            launches[k] += b->e.prof_n[k];
+        }
+        for (int k = 0; k < SSAK_NKINDS; k++)
+        {
+            b->e.prof_ms[k] = 0.0;
+            b->e.prof_n[k] = 0;
+        }
+    }
+    return SSAK_NKINDS;
+}

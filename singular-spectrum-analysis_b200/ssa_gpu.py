@@ -544,3 +544,116 @@ class SSABatch:
             raise RuntimeError("ssa_batch_device_results failed")
         return {"sigma": r.sigma, "W": r.W, "groups": r.groups, "recon": r.recon, "ld_recon": r.ld_recon,
                 "status": r.status, "stream": r.stream}
+
+
+_sig("ssa_rbatch_create", _I, ctypes.POINTER(ctypes.c_void_p), _I, _I, c_int_p, c_int_p, _I)
+_sig("ssa_rbatch_destroy", _V, ctypes.c_void_p)
+_sig("ssa_rbatch_run", _I, ctypes.c_void_p, _I, c_int_p, c_int_p, c_int_p, c_double_p, ctypes.c_uint64,
+     c_double_p, c_double_p, c_double_p)
+_sig("ssa_rbatch_run_device", _I, ctypes.c_void_p, _I, c_int_p, c_int_p, c_int_p, ctypes.c_void_p, ctypes.c_uint64)
+_sig("ssa_rbatch_sync", _I, ctypes.c_void_p)
+_sig("ssa_rbatch_layout", _I, ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t))
+_sig("ssa_rbatch_device_results", _I, ctypes.c_void_p, ctypes.POINTER(_BatchResults))
+_sig("ssa_rbatch_set_profiling", _I, ctypes.c_void_p, _I)
+_sig("ssa_rbatch_profile", _I, ctypes.c_void_p, c_double_p, ctypes.POINTER(ctypes.c_longlong), _I)
+
+
+class SSARaggedBatch:
+    """Uneven batch (ssa_rbatch_* C ABI): series of different N, L and k through decomposition,
+    all elementary reconstructions, W-correlation and the sums of ``groups`` in one pass, one
+    launch per stage per FFT-length bucket."""
+
+    def __init__(self, oversampling: int = 10, power_iters: int = 2,
+                 groups: Sequence[Sequence[int]] = ((0,), (1, 2))):
+        self.p, self.q = oversampling, power_iters
+        self.groups = [list(g) for g in groups]
+        idx = np.ascontiguousarray([i for g in self.groups for i in g] or [0], dtype=np.int32)
+        sizes = np.ascontiguousarray([len(g) for g in self.groups] or [0], dtype=np.int32)
+        self._h = ctypes.c_void_p()
+        if _lib.ssa_rbatch_create(ctypes.byref(self._h), oversampling, power_iters, _ip(idx), _ip(sizes),
+                                  len(self.groups)) != 0:
+            raise ValueError("ssa_rbatch_create failed")
+        self._keep = (idx, sizes)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.ssa_rbatch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    @staticmethod
+    def _dims(N, L, k):
+        N = np.ascontiguousarray(N, dtype=np.int32)
+        L = np.ascontiguousarray(L, dtype=np.int32)
+        k = np.ascontiguousarray(k, dtype=np.int32)
+        if not (len(N) == len(L) == len(k)):
+            raise ValueError("N, L and k must have one entry per series")
+        return N, L, k
+
+    @staticmethod
+    def effective_k(N, L, k) -> np.ndarray:
+        """Components per series: min(k, L, N - L + 1) (at least 1 for the output layout)."""
+        N, L, k = (np.asarray(a, dtype=np.int64) for a in (N, L, k))
+        return np.maximum(np.minimum(k, np.minimum(L, N - L + 1)), 1)
+
+    def run(self, series: Sequence[np.ndarray], L: Sequence[int], k: Sequence[int], seed: int = 0):
+        """Host-to-host run. Returns per-series lists (sigma, W, groups)."""
+        Na, La, ka = self._dims([len(x) for x in series], L, k)
+        x = np.ascontiguousarray(np.concatenate([np.asarray(s, dtype=np.float64) for s in series]))
+        ke = self.effective_k(Na, La, ka)
+        sig = np.zeros(int(ke.sum()))
+        W = np.zeros(int((ke * ke).sum()))
+        G = np.zeros(max(1, len(self.groups) * int(Na.sum())))
+        if _lib.ssa_rbatch_run(self._h, len(Na), _ip(Na), _ip(La), _ip(ka), _dp(x), seed, _dp(sig), _dp(W),
+                               _dp(G) if self.groups else None) != 0:
+            raise RuntimeError("ssa_rbatch_run failed")
+        return self._unpack(Na, ke, sig, W, G)
+
+    def _unpack(self, Na, ke, sig, W, G):
+        out_s, out_w, out_g = [], [], []
+        o_s = o_w = o_g = 0
+        ng = len(self.groups)
+        for n, kk in zip(Na.tolist(), ke.tolist()):
+            out_s.append(sig[o_s:o_s + kk])
+            out_w.append(W[o_w:o_w + kk * kk].reshape(kk, kk))
+            out_g.append(G[o_g:o_g + ng * n].reshape(ng, n))
+            o_s += kk
+            o_w += kk * kk
+            o_g += ng * n
+        return out_s, out_w, out_g
+
+    def run_device(self, d_x_ptr: int, N, L, k, seed: int = 0) -> None:
+        """Enqueue a run on device-resident packed input (sum N doubles at d_x_ptr)."""
+        Na, La, ka = self._dims(N, L, k)
+        if _lib.ssa_rbatch_run_device(self._h, len(Na), _ip(Na), _ip(La), _ip(ka), ctypes.c_void_p(d_x_ptr),
+                                      seed) != 0:
+            raise RuntimeError("ssa_rbatch_run_device failed")
+
+    def run_host_ptrs(self, N, L, k, x_ptr: int, seed: int, sigma_ptr: int, W_ptr: int, groups_ptr: int) -> None:
+        """Host-to-host run on caller-owned (ideally pinned) packed buffers given by address."""
+        Na, La, ka = self._dims(N, L, k)
+        vp = lambda a: ctypes.cast(ctypes.c_void_p(a), c_double_p) if a else None  # noqa: E731
+        if _lib.ssa_rbatch_run(self._h, len(Na), _ip(Na), _ip(La), _ip(ka), vp(x_ptr), seed, vp(sigma_ptr),
+                               vp(W_ptr), vp(groups_ptr)) != 0:
+            raise RuntimeError("ssa_rbatch_run failed")
+
+    def sync(self) -> None:
+        if _lib.ssa_rbatch_sync(self._h) != 0:
+            raise RuntimeError("a series of the uneven batch failed")
+
+    def set_profiling(self, on: bool) -> None:
+        if _lib.ssa_rbatch_set_profiling(self._h, 1 if on else 0) != 0:
+            raise RuntimeError("ssa_rbatch_set_profiling failed")
+
+    def profile(self) -> dict:
+        """{kind: (milliseconds summed over buckets, launches)} since profiling was switched on."""
+        ms = (ctypes.c_double * len(PROFILE_KINDS))()
+        n = (ctypes.c_longlong * len(PROFILE_KINDS))()
+        if _lib.ssa_rbatch_profile(self._h, ms, n, len(PROFILE_KINDS)) < 0:
+            raise RuntimeError("ssa_rbatch_profile failed")
+        return {kk: (ms[i], int(n[i])) for i, kk in enumerate(PROFILE_KINDS)}
+
+    def device_results(self) -> dict:
+        r = _BatchResults()
+        if _lib.ssa_rbatch_device_results(self._h, ctypes.byref(r)) != 0:
+            raise RuntimeError("ssa_rbatch_device_results failed")
+        return {"sigma": r.sigma, "W": r.W, "groups": r.groups, "status": r.status, "stream": r.stream}

@@ -1,0 +1,146 @@
+"""Uneven batches (ssa_rbatch_*) against the FP64 oracle, against the uniform batch, and alone
+versus in a mix.
+
+Tolerances as in the single-series parity tests: singular values relative <= 1e-5 where the
+relative gap to the neighbours exceeds 1e-3 (1e-4 otherwise); group reconstructions relative L2
+<= 1e-5 for groups separated by a relative gap > 1e-2, else max(1e-5, 40 * 2^-24 / gap);
+W-correlation diagonal 1 within 1e-6 and max abs <= 1e-4 on the leading well-separated block.
+A series run alone and in a mix differs only in how its FP64 Gram partials are chunked, so the
+two agree to the same tolerances.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SIG_TOL = 1e-5
+REC_TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    import ssa_gpu
+
+    return ssa_gpu
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def group_gap(sigma, group):
+    inside = [i for i in group if 0 <= i < len(sigma)]
+    outside = [j for j in range(len(sigma)) if j not in inside]
+    if not inside or not outside:
+        return np.inf
+    return min(abs(sigma[i] - sigma[j]) / sigma[i] for i in inside for j in outside)
+
+
+def rec_tol(sigma, group):
+    g = group_gap(sigma, group)
+    return REC_TOL if g > 1e-2 else max(REC_TOL, 40 * 2.0 ** -24 / max(g, 1e-12))
+
+
+def check_sigma(s, ref):
+    rel = np.abs(s - ref) / ref
+    gap = np.full(len(ref), np.inf)
+    d = np.abs(np.diff(ref)) / ref[:-1]
+    gap[:-1] = np.minimum(gap[:-1], d)
+    gap[1:] = np.minimum(gap[1:], d)
+    assert np.all(rel[gap > 1e-3] <= SIG_TOL), rel.max()
+    assert np.all(rel <= 1e-4), rel.max()
+
+
+def leading_block(sigma, kmax=6):
+    """Leading components whose relative gap to every other computed one exceeds 1e-2."""
+    return [i for i in range(min(kmax, len(sigma))) if group_gap(sigma, [i]) > 1e-2]
+
+
+def test_uneven_batch_vs_oracle(gpu, oracle):
+    mix = oracle.config3_batch(10, seed=2, nmin=500, nmax=20000)
+    # both reconstruction paths: a series above 16384 (one FFT buffer) and small ones
+    rng = np.random.default_rng(77)
+    mix.append((oracle.walk_sines(rng, 18000), 4500, 12))
+    mix.append((oracle.walk_sines(rng, 700), 175, 40))
+    p, q, seed = 10, 2, 31
+    rb = gpu.SSARaggedBatch(oversampling=p, power_iters=q, groups=[[0], [1, 2]])
+    xs = [m[0] for m in mix]
+    Ls = [m[1] for m in mix]
+    ks = [m[2] for m in mix]
+    sig, W, G = rb.run(xs, Ls, ks, seed=seed)
+    for s, (x, L, k) in enumerate(mix):
+        N = len(x)
+        K = N - L + 1
+        kp = min(k + p, L, K)
+        Om = oracle.device_gaussian(oracle.series_seed(seed, s), K, kp)
+        d = oracle.decompose_randomized(x, L, k, p, Om, q=q)
+        check_sigma(sig[s], d.sigma)
+        for gi, g in enumerate(([0], [1, 2])):
+            e = rel_l2(G[s][gi], oracle.reconstruct(d, g, N, L))
+            assert e <= rec_tol(d.sigma, g), (s, N, g, e)
+        Wr = oracle.wcorr_matrix(d, N, L)
+        assert np.max(np.abs(np.diag(W[s]) - 1.0)) < 1e-6
+        blk = leading_block(d.sigma)
+        if blk:
+            assert np.max(np.abs(W[s][np.ix_(blk, blk)] - Wr[np.ix_(blk, blk)])) < 1e-4, (s, N)
+
+
+def test_uneven_equals_uniform_for_equal_shapes(gpu, oracle):
+    B, N, L, k = 6, 3000, 750, 20
+    X = oracle.config2_batch(B, seed=5, N=N)
+    ub = gpu.SSABatch(B, N, L, k, oversampling=10, power_iters=2)
+    s_u, W_u, G_u = ub.run(X, seed=9)
+    rb = gpu.SSARaggedBatch(oversampling=10, power_iters=2)
+    s_r, W_r, G_r = rb.run(list(X), [L] * B, [k] * B, seed=9)
+    for s in range(B):
+        np.testing.assert_allclose(s_r[s], s_u[s], rtol=1e-12, atol=0)
+        np.testing.assert_allclose(G_r[s], G_u[s], rtol=0, atol=1e-9 * np.abs(G_u[s]).max())
+        np.testing.assert_allclose(W_r[s], W_u[s], rtol=0, atol=1e-9)
+
+
+def test_alone_equals_in_mix(gpu, oracle):
+    mix = oracle.config3_batch(8, seed=12, nmin=500, nmax=9000)
+    xs = [m[0] for m in mix]
+    Ls = [m[1] for m in mix]
+    ks = [m[2] for m in mix]
+    rb = gpu.SSARaggedBatch(oversampling=10, power_iters=2)
+    sig, W, G = rb.run(xs, Ls, ks, seed=4)
+    for s in (0, 3, 7):
+        # the same series at the same batch position (its generator seed depends on it), the
+        # positions before it taken by short noise series in another FFT-length bucket
+        pad_x = [np.random.default_rng(i).standard_normal(64) for i in range(s)] + [xs[s]]
+        pad_L = [16] * s + [Ls[s]]
+        pad_k = [2] * s + [ks[s]]
+        s1, W1, G1 = rb.run(pad_x, pad_L, pad_k, seed=4)
+        check_sigma(s1[s], sig[s])
+        for gi, g in enumerate(([0], [1, 2])):
+            assert rel_l2(G1[s][gi], G[s][gi]) <= rec_tol(sig[s], g)
+
+
+def test_uneven_batch_rejects_bad_series(gpu, oracle):
+    rb = gpu.SSARaggedBatch()
+    x = np.sin(np.arange(100.0)) + 0.1 * np.random.default_rng(1).standard_normal(100)
+    with pytest.raises(RuntimeError):
+        rb.run([x], [100], [5])  # L > N - 1
+    with pytest.raises(RuntimeError):
+        rb.run([np.zeros(40000)], [100], [5])  # beyond the largest FFT length
+    s, W, G = rb.run([x, x[:50]], [25, 10], [4, 3])  # still usable afterwards
+    assert len(s[0]) == 4 and len(s[1]) == 3
+
+
+def test_single_series_wcorr_one_buffer_path(gpu, oracle):
+    """N = 20000 needs the one-buffer elementary reconstruction (FFT length 32768)."""
+    rng = np.random.default_rng(8)
+    x = oracle.walk_sines(rng, 20000)
+    N, L, k, p = 20000, 5000, 10, 10
+    K = N - L + 1
+    Om = rng.standard_normal((K, k + p))
+    d = oracle.decompose_randomized(x, L, k, p, Om, q=2)
+    s = gpu.SSA(x, L)
+    s.decompose(k, oversampling=p, power_iters=2, omega=Om)
+    check_sigma(s.singular_values, d.sigma)
+    W = s.wcorr_matrix()
+    Wr = oracle.wcorr_matrix(d, N, L)
+    assert np.max(np.abs(np.diag(W) - 1.0)) < 1e-6
+    blk = leading_block(d.sigma)
+    assert blk and np.max(np.abs(W[np.ix_(blk, blk)] - Wr[np.ix_(blk, blk)])) < 1e-4
