@@ -93,7 +93,7 @@ int mssa_opt_copy_factors(const MSSA_Opt *mssa, double *U, double *V, double *si
  * power iterations q) through the same pipeline as ssa_batch_*: randomized decomposition with
  * the device generator (series s seeded seed ^ 0x9E3779B97F4A7C15 (s + 1), as in ssa_batch_*),
  * all k[s] elementary reconstructions, W-correlation and group sums. Series are bucketed by FFT
- * length (M = next power of two >= max(N, 32), N <= 32768); each bucket runs one launch per
+ * length (M = next power of two >= max(N, 32), N <= 131072); each bucket runs one launch per
  * stage on its own stream and the buckets overlap on the device. No counterpart in the
  * reference, whose API takes one series per context.
  *
@@ -102,7 +102,7 @@ int mssa_opt_copy_factors(const MSSA_Opt *mssa, double *U, double *V, double *si
  * n_groups x N[s] at n_groups sum_{t<s} N[t], where k'[s] = min(k[s], L[s], N[s] - L[s] + 1).
  * ssa_rbatch_layout returns these offsets (4 per series: x, sigma, W, groups) and the four
  * totals of the last run. Device buffers grow as needed and are reused across runs.
- * Returns 0 / -1 (invalid shape, N > 32768, k + p > 64, or a series whose decomposition
+ * Returns 0 / -1 (invalid shape, N > 131072, k + p > 64, or a series whose decomposition
  * failed). */
 typedef struct ssa_rbatch ssa_rbatch;
 int ssa_rbatch_create(ssa_rbatch **out, int oversampling, int power_iters, const int *group_idx,
@@ -119,6 +119,74 @@ int ssa_rbatch_layout(const ssa_rbatch *b, size_t *offsets, size_t *totals);
 int ssa_rbatch_device_results(const ssa_rbatch *b, ssa_batch_results *out);
 int ssa_rbatch_set_profiling(ssa_rbatch *b, int on);
 int ssa_rbatch_profile(ssa_rbatch *b, double *ms, long long *launches, int nkinds);
+
+/* ---- Request server ------------------------------------------------------------------------
+ * Continuous batching of mixed-size requests on one GPU (no counterpart in the reference, whose
+ * API is one synchronous call per series). A worker thread takes submitted requests in arrival
+ * order and gathers decompositions into uneven batches (ssa_rbatch_*), each within a share of
+ * the device-memory budget; up to max_inflight batches run at once on their own streams, so
+ * requests that arrive while others are on the GPU start as soon as a batch slot and memory are
+ * free. Decompositions use the randomized pipeline with oversampling p and q power iterations,
+ * the device generator seeded with the request's `seed`, and compute the reconstructions of
+ * groups [0] and [1, 2] and the W-correlation matrix.
+ *
+ * A SSA_REQ_DECOMPOSE_RECON request leaves its series resident under series_id: the LRF
+ * coefficients of the group [0, 1, 2] (MKL/ssa_opt.h:2766-2816) and the last L - 1 values of
+ * that group's reconstruction stay in device memory, a quarter of the budget at most (least
+ * recently used series evicted first). A SSA_REQ_FORECAST request on a resident series runs the
+ * R-forecast recurrence (:2818-2841) for h steps without decomposing again; one that arrives
+ * while its series' decomposition is still queued or running waits for it. Requests fail
+ * (status -1) on invalid shapes, N > 131072, k + p > 64, a series larger than a batch's share
+ * of the budget, a forecast on a series that is not resident, or an LRF whose verticality
+ * coefficient is >= 1 (fewer than 3 components also leave nothing to forecast from).
+ * Output pointers may be NULL; they must stay valid until the request completes. */
+enum
+{
+    SSA_REQ_DECOMPOSE_RECON = 0, /* outputs: sigma, groups (2 x N: [0] then [1, 2]) */
+    SSA_REQ_DECOMPOSE_WCORR = 1, /* outputs: sigma, W (k' x k', row-major) */
+    SSA_REQ_FORECAST = 2         /* outputs: forecast (h values after the series' end) */
+};
+typedef struct
+{
+    int type;
+    int series_id;      /* resident key (DECOMPOSE_RECON) or target (FORECAST) */
+    int N, L, k;        /* decompositions */
+    int h;              /* forecast steps (1 .. 4096) */
+    const double *x;    /* decompositions: N input values (host) */
+    uint64_t seed;      /* generator seed of the decomposition */
+    double *sigma;      /* k' = min(k, L, N - L + 1) values */
+    double *groups;     /* 2 x N */
+    double *W;          /* k' x k' */
+    double *forecast;   /* h */
+    /* set by the server */
+    int status;         /* 1 while in progress, then 0 (done) or -1 (failed) */
+    int k_out;          /* k' */
+    double t_arrival;   /* seconds on ssa_server_now's clock */
+    double t_done;
+    void *priv;         /* reserved for the server */
+} ssa_request;
+typedef struct
+{
+    long long submitted, completed, failed;
+    long long batches, decompositions, max_batch;
+    long long forecast_batches, forecasts;
+    long long evictions, not_resident;
+    size_t resident_bytes, resident_budget, batch_budget;
+} ssa_server_stats;
+typedef struct ssa_server ssa_server;
+/* hbm_budget_bytes 0: 80 % of the free device memory at creation. */
+int ssa_server_create(ssa_server **out, size_t hbm_budget_bytes, int max_inflight, int max_batch, int oversampling,
+                      int power_iters);
+/* Waits for every submitted request, then stops the worker and frees everything. */
+void ssa_server_destroy(ssa_server *s);
+/* Thread-safe; stamps t_arrival. The request must stay valid until it completes. */
+int ssa_server_submit(ssa_server *s, ssa_request *r);
+/* Wait until every submitted request has completed. */
+int ssa_server_drain(ssa_server *s);
+/* Submit reqs[i] at arrival_s[i] seconds after the call (ascending), then drain. */
+int ssa_server_replay(ssa_server *s, ssa_request *reqs, const double *arrival_s, int n);
+int ssa_server_stats_get(ssa_server *s, ssa_server_stats *st);
+double ssa_server_now(void);
 
 /* Stage profiler of a batch: with profiling on, every kernel launch of ssa_batch_run* is
  * bracketed by CUDA events on the batch stream. ssa_batch_profile waits for the stream and

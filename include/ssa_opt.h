@@ -12,7 +12,7 @@
  * Differences a caller can observe (all documented, none changes a signature):
  *   - fft_len is next_pow2(N) (at least 32) instead of next_pow2(N + K - 1); circular
  *     correlation and convolution of length >= N never wrap for these lengths.
- *   - N is limited to 32768 per series; (k + oversampling) is limited to SSA_MAX_KP = 64.
+ *   - N is limited to 131072 per series; (k + oversampling) is limited to SSA_MAX_KP = 64.
  *     Larger requests return -1.
  *   - The Gaussian test matrix of ssa_opt_decompose_randomized comes from the library's own
  *     counter-based generator (seed 42, advancing per call) instead of MKL's MT2203 stream.

@@ -18,7 +18,7 @@ INCLUDE = HERE.parent / "include"
 OUT = HERE / "libssa.so"
 BUILD = HERE / "_build"
 
-C_SOURCES = ["ssa_engine.c", "ssa_api.c", "ssa_batch.c", "ssa_mssa.c", "ssa_ragged.c"]
+C_SOURCES = ["ssa_engine.c", "ssa_api.c", "ssa_batch.c", "ssa_mssa.c", "ssa_ragged.c", "ssa_server.c"]
 CU_SOURCES = ["ssa_kernels.cu"]
 
 NVCC_FLAGS = [
@@ -78,7 +78,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         objs.append(o)
     if force or _stale(OUT, objs):
         cmd = [nvcc, "-shared", "-cudart", "static", "-gencode", "arch=compute_100a,code=sm_100a",
-               "-o", str(OUT), *map(str, objs), "-lm"]
+               "-o", str(OUT), *map(str, objs), "-lm", "-lpthread"]
         if verbose:
             print(" ".join(cmd))
         _run(cmd)

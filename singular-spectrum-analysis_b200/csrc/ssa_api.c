@@ -120,7 +120,7 @@ int ssa_opt_init(SSA_Opt *ssa, const ssa_real *x, int N, int L)
         return -1;
     memset(ssa, 0, sizeof(SSA_Opt));
     const int logh = ssad_logh_for(N);
-    if (logh > 14)
+    if (logh > SSA_MAX_LOGH_ALL)
         return -1;
     ssa->N = N;
     ssa->L = L;

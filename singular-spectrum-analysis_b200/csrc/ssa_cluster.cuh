@@ -1,0 +1,410 @@
+// FFT lengths beyond one CTA's shared memory (real length M = 2^16 and 2^17, i.e. series up to
+// N = 131072): each transform runs on a thread-block cluster of C = H / 8192 CTAs.
+//
+// Packed sequence z[n] = a[2n] + i a[2n+1], n < H = C H1 (H1 = 8192). CTA r of the cluster holds
+// the decimated sequence z_r[m] = z[C m + r] and transforms it locally (fft_block, H1 points):
+// Z_r = DFT_H1(z_r). The H-point spectrum is then
+//     Z[k1 + H1 k2] = sum_r W_H^{r k1} W_C^{r k2} Z_r[k1],   k1 < H1, k2 < C,
+// a C-point DFT per k1 of the twiddled partial spectra. Each k1 and its mirror H1 - k1 belong to
+// one CTA (the real-FFT unpacking pairs bin k with H - k, and H - (k1 + H1 k2) =
+// (H1 - k1) + H1 (C - 1 - k2)), which reads the C partial values at both through distributed
+// shared memory, forms the 2C bins, applies the per-kernel spectral operation and, where an
+// inverse transform follows, writes the inverse combination
+//     T_r[k1] = W_H^{-r k1} sum_k2 Z'[k1 + H1 k2] W_C^{-r k2}
+// back into CTA r's buffer at the same slot k1 (only the owner of k1 touches slot k1 in any
+// CTA, so reading and writing in place needs no barrier in between). After a cluster barrier
+// each CTA inverts its T_r locally: z'[C m + r] = IDFT_H1(T_r)[m].
+//
+// Cluster barriers: one after the local forward transforms (every partial spectrum complete and
+// every CTA resident), one after the exchange; a kernel whose last remote access is a read
+// (spectrum) or a write into rank 0 (norm reduction) ends with one more, so that no CTA leaves
+// while another still addresses its shared memory.
+
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
+
+#define SSA_CL_LOGH1 13
+#define SSA_CL_MAX_LOGH 16
+
+template <int LOGH>
+struct ClShape {
+    static constexpr int LOGH1 = SSA_CL_LOGH1;
+    static constexpr int H1 = 1 << LOGH1;
+    static constexpr int C = 1 << (LOGH - LOGH1);
+    static constexpr int H = 1 << LOGH;
+    static constexpr int BLOCK = FftShape<LOGH1>::BLOCK;
+    static constexpr int NITEM = H1 / 2 + 1;  // k1 = 0 .. H1/2, each with its mirror
+};
+
+template <int LOGH>
+__host__ __device__ constexpr int cl_smem_f2() {
+    return spad_size(ClShape<LOGH>::H1) + TwSplit<SSA_CL_LOGH1 + 1>::N + TwSplit<LOGH + 1>::N;
+}
+
+enum { CL_SPEC = 0, CL_CORR = 1, CL_ELEM = 2, CL_RECON = 3 };
+
+// Operands of the per-bin spectral operation.
+struct ClOp {
+    const float2* X;     // CL_CORR: signal spectrum (H + 1 bins)
+    float2* spec;        // CL_SPEC: output spectrum
+    const float2* us;    // CL_ELEM: spectrum of sigma u
+    const ssa_recon_job* R;  // CL_RECON
+};
+
+// Sum over the group of Us_i[k] Vs_i[k] (CL_RECON).
+__device__ __forceinline__ float2 cl_group_product(const ssa_recon_job& J, int k) {
+    float2 p = make_float2(0.f, 0.f);
+    for (int g = 0; g < J.n_group; ++g) {
+        const int i = J.group[g];
+        if (i < 0 || i >= J.k) continue;
+        const float2* us = reinterpret_cast<const float2*>(J.Us + (long long)i * J.ld_spec);
+        const float2* vs = reinterpret_cast<const float2*>(J.Vs + (long long)i * J.ld_spec);
+        p = cadd(p, cmul(us[k], vs[k]));
+    }
+    return p;
+}
+
+// Bins k and H - k (1 <= k <= H/2) of the packed transform in zk, zm are replaced by the packed
+// output spectrum (or, for CL_SPEC, the real spectrum is written out).
+template <int LOGH, int KIND>
+__device__ __forceinline__ void cl_pair(const ClOp& op, int k, float2& zk, float2& zm, const float2* twM) {
+    constexpr int H = 1 << LOGH;
+    const float2 w = twiddle<LOGH + 1, false>(twM, k);
+    float2 pk, pm;
+    if constexpr (KIND == CL_RECON) {
+        pk = cl_group_product(*op.R, k);
+        pm = cl_group_product(*op.R, H - k);
+    } else {
+        float2 ak, am;
+        unpack_pair<LOGH>(zk, zm, w, ak, am);
+        if constexpr (KIND == CL_SPEC) {
+            op.spec[k] = ak;
+            op.spec[H - k] = am;
+            return;
+        } else if constexpr (KIND == CL_CORR) {
+            pk = cmulc(op.X[k], ak);
+            pm = cmulc(op.X[H - k], am);
+        } else {
+            pk = cmul(op.us[k], ak);
+            pm = cmul(op.us[H - k], am);
+        }
+    }
+    pack_pair(pk, pm, w, zk, zm);
+}
+
+// Bin 0 with the Nyquist bin H, both real, packed together in z0.
+template <int LOGH, int KIND>
+__device__ __forceinline__ void cl_dc(const ClOp& op, float2& z0) {
+    constexpr int H = 1 << LOGH;
+    float2 zk, zm;
+    if constexpr (KIND == CL_SPEC) {
+        op.spec[0] = make_float2(z0.x + z0.y, 0.f);
+        op.spec[H] = make_float2(z0.x - z0.y, 0.f);
+        return;
+    } else if constexpr (KIND == CL_CORR) {
+        pack_pair(cscale(op.X[0], z0.x + z0.y), cscale(op.X[H], z0.x - z0.y), make_float2(1.f, 0.f), zk, zm);
+    } else if constexpr (KIND == CL_ELEM) {
+        const float p0 = op.us[0].x * (z0.x + z0.y);
+        const float ph = op.us[H].x * (z0.x - z0.y);
+        pack_pair(make_float2(p0, 0.f), make_float2(ph, 0.f), make_float2(1.f, 0.f), zk, zm);
+    } else {
+        pack_pair(cl_group_product(*op.R, 0), cl_group_product(*op.R, H), make_float2(1.f, 0.f), zk, zm);
+    }
+    z0 = zk;
+}
+
+// Owner phase over this CTA's items: gather (unless CL_RECON), spectral operation, scatter
+// (unless CL_SPEC). rs[q] is CTA q's transform buffer.
+template <int LOGH, int KIND>
+__device__ __forceinline__ void cl_exchange(float2* const* rs, const float2* twM, int rank, const ClOp& op) {
+    using S = ClShape<LOGH>;
+    constexpr int C = S::C, H1 = S::H1, H = S::H;
+    for (int g = rank * S::BLOCK + (int)threadIdx.x; g < S::NITEM; g += C * S::BLOCK) {
+        const int ka = g, kb = (H1 - g) & (H1 - 1);
+        const bool self = ka == kb;  // k1 = 0 or H1/2
+        float2 za[C], zb[C];
+        if constexpr (KIND != CL_RECON) {
+#pragma unroll
+            for (int q = 0; q < C; ++q) {
+                float2 v = rs[q][spad(ka)];
+                if (q > 0) v = cmul(v, twiddle<LOGH + 1, false>(twM, 2 * q * ka));
+                za[q] = v;
+            }
+            dftR<C, false>(za);
+            if (!self) {
+#pragma unroll
+                for (int q = 0; q < C; ++q) {
+                    float2 v = rs[q][spad(kb)];
+                    if (q > 0) v = cmul(v, twiddle<LOGH + 1, false>(twM, 2 * q * kb));
+                    zb[q] = v;
+                }
+                dftR<C, false>(zb);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < C; ++q) za[q] = zb[q] = make_float2(0.f, 0.f);
+        }
+        if (!self) {
+            // bin ka + H1 q pairs with kb + H1 (C - 1 - q)
+#pragma unroll
+            for (int q = 0; q < C; ++q) {
+                const int k = ka + H1 * q;
+                if (k <= H / 2) cl_pair<LOGH, KIND>(op, k, za[q], zb[C - 1 - q], twM);
+                else cl_pair<LOGH, KIND>(op, H - k, zb[C - 1 - q], za[q], twM);
+            }
+        } else if (ka == 0) {
+            // bin H1 q pairs with H1 (C - q); q = 0 is DC with Nyquist, q = C/2 is bin H/2
+            cl_dc<LOGH, KIND>(op, za[0]);
+#pragma unroll
+            for (int q = 1; q < C / 2; ++q) cl_pair<LOGH, KIND>(op, H1 * q, za[q], za[C - q], twM);
+            {
+                float2 z1 = za[C / 2], z2 = za[C / 2];
+                cl_pair<LOGH, KIND>(op, H / 2, z1, z2, twM);
+                za[C / 2] = z2;
+            }
+        } else {
+            // ka = H1/2: bin H1/2 + H1 q pairs with H1/2 + H1 (C - 1 - q)
+#pragma unroll
+            for (int q = 0; q < C / 2; ++q) cl_pair<LOGH, KIND>(op, ka + H1 * q, za[q], za[C - 1 - q], twM);
+        }
+        if constexpr (KIND != CL_SPEC) {
+            dftR<C, true>(za);
+#pragma unroll
+            for (int q = 0; q < C; ++q) {
+                float2 v = za[q];
+                if (q > 0) v = cmul(v, twiddle<LOGH + 1, true>(twM, 2 * q * ka));
+                rs[q][spad(ka)] = v;
+            }
+            if (!self) {
+                dftR<C, true>(zb);
+#pragma unroll
+                for (int q = 0; q < C; ++q) {
+                    float2 v = zb[q];
+                    if (q > 0) v = cmul(v, twiddle<LOGH + 1, true>(twM, 2 * q * kb));
+                    rs[q][spad(kb)] = v;
+                }
+            }
+        }
+    }
+}
+
+// Decimated load of column c: z_r[m] = (a[2i], a[2i+1]) with i = C m + r.
+template <int LOGH>
+__device__ __forceinline__ void cl_load(float2* s, const float* f32, const double* f64, float sc, int n,
+                                        unsigned long long seed, int col, int rank) {
+    using S = ClShape<LOGH>;
+    for (int m = threadIdx.x; m < S::H1; m += blockDim.x) {
+        const int i = m * S::C + rank;
+        const int t = 2 * i;
+        float2 v = make_float2(0.f, 0.f);
+        if (t < n) {
+            if (f32) {
+                v.x = f32[t] * sc;
+                v.y = t + 1 < n ? f32[t + 1] * sc : 0.f;
+            } else if (f64) {
+                v.x = (float)f64[t];
+                v.y = t + 1 < n ? (float)f64[t + 1] : 0.f;
+            } else {
+                v = gauss_pair(seed, col, i);
+                if (t + 1 >= n) v.y = 0.f;
+            }
+        }
+        s[spad(m)] = v;
+    }
+}
+
+// Spectrum (CL_SPEC), correlation sweep (CL_CORR) and one-buffer elementary reconstruction
+// (CL_ELEM) on clusters; grid (C x columns, jobs), one cluster per column.
+template <int LOGH, int KIND>
+__global__ void __launch_bounds__(ClShape<LOGH>::BLOCK) k_cl_col(const ssa_col_job* __restrict__ jobs) {
+    using S = ClShape<LOGH>;
+    extern __shared__ float2 smem[];
+    __shared__ double red[32];
+    __shared__ double cl_part[S::C];
+    float2* s = smem;
+    float2* tw1 = s + spad_size(S::H1);
+    float2* twM = tw1 + TwSplit<S::LOGH1 + 1>::N;
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const ssa_col_job J = jobs[blockIdx.y];
+    const int c = blockIdx.x / S::C;
+    if (c >= J.ncols) return;  // the whole cluster shares c
+    load_twiddles<S::LOGH1 + 1>(tw1);
+    load_twiddles<LOGH + 1>(twM);
+    if constexpr (KIND == CL_ELEM) {
+        cl_load<LOGH>(s, J.in2 + (long long)c * J.ld_in2, nullptr, 1.0f, J.n_in2, 0, 0, rank);
+    } else {
+        const float sc = J.scale ? (float)J.scale[c] : 1.0f;
+        cl_load<LOGH>(s, J.in ? J.in + (long long)c * J.ld_in : nullptr,
+                      (!J.in && J.in64) ? J.in64 + (long long)c * J.ld_in : nullptr, sc, J.n_in, J.seed,
+                      J.col0 + c, rank);
+    }
+    __syncthreads();
+    fft_block<S::LOGH1, false>(s, tw1);
+    cl.sync();
+    float2* rs[S::C];
+#pragma unroll
+    for (int q = 0; q < S::C; ++q) rs[q] = cl.map_shared_rank(s, q);
+    ClOp op;
+    op.X = reinterpret_cast<const float2*>(J.X);
+    op.spec = KIND == CL_SPEC ? reinterpret_cast<float2*>(J.spec + (long long)c * J.ld_spec) : nullptr;
+    op.us = KIND == CL_ELEM ? reinterpret_cast<const float2*>(J.spec + (long long)c * J.ld_spec) : nullptr;
+    op.R = nullptr;
+    cl_exchange<LOGH, KIND>(rs, twM, rank, op);
+    cl.sync();
+    if constexpr (KIND == CL_SPEC) return;
+    fft_block<S::LOGH1, true>(s, tw1);
+    const float inv_h = 1.0f / (float)S::H;
+    if constexpr (KIND == CL_CORR) {
+        float* out = J.out + (long long)c * J.ld_out;
+        for (int m = threadIdx.x; m < S::H1; m += blockDim.x) {
+            const int t = 2 * (m * S::C + rank);
+            if (t >= J.n_out) continue;
+            const float2 z = s[spad(m)];
+            out[t] = z.x * inv_h;
+            if (t + 1 < J.n_out) out[t + 1] = z.y * inv_h;
+        }
+    } else {
+        const float sc = J.scale ? (float)J.scale[c] : 1.0f;
+        const float* u = J.in + (long long)c * J.ld_in;
+        const float* vv = J.in2 + (long long)c * J.ld_in2;
+        float* out = J.out + (long long)c * J.ld_out;
+        double acc = 0.0;
+        for (int m = threadIdx.x; m < S::H1; m += blockDim.x) {
+            const float2 z = s[spad(m)];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int t = 2 * (m * S::C + rank) + h;
+                if (t >= J.N) continue;
+                double p = (double)((h ? z.y : z.x) * inv_h);
+                if (edge_diag(t, J.N)) p = (double)sc * diag_sum(u, vv, t, J.n_in, J.n_in2);
+                const int cnt = diag_count(t, J.N, J.L, J.K);
+                out[t] = (float)(p / (double)cnt);
+                acc += p * p / (double)cnt;
+            }
+        }
+        acc = block_sum<double>(acc, red);
+        if (threadIdx.x == 0) cl.map_shared_rank(cl_part, 0)[rank] = acc;
+        cl.sync();
+        if (rank == 0 && threadIdx.x == 0 && J.norm2) {
+            double t = 0.0;
+            for (int q = 0; q < S::C; ++q) t += cl_part[q];
+            J.norm2[c] = t;
+        }
+    }
+}
+
+// Grouped reconstruction from cached spectra on clusters; grid (C, jobs).
+template <int LOGH>
+__global__ void __launch_bounds__(ClShape<LOGH>::BLOCK) k_cl_recon(const ssa_recon_job* __restrict__ jobs) {
+    using S = ClShape<LOGH>;
+    extern __shared__ float2 smem[];
+    float2* s = smem;
+    float2* tw1 = s + spad_size(S::H1);
+    float2* twM = tw1 + TwSplit<S::LOGH1 + 1>::N;
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const ssa_recon_job J = jobs[blockIdx.y];
+    load_twiddles<S::LOGH1 + 1>(tw1);
+    load_twiddles<LOGH + 1>(twM);
+    __syncthreads();
+    cl.sync();  // every CTA of the cluster is resident before the remote stores
+    float2* rs[S::C];
+#pragma unroll
+    for (int q = 0; q < S::C; ++q) rs[q] = cl.map_shared_rank(s, q);
+    ClOp op;
+    op.X = nullptr;
+    op.spec = nullptr;
+    op.us = nullptr;
+    op.R = &J;
+    cl_exchange<LOGH, CL_RECON>(rs, twM, rank, op);
+    cl.sync();
+    fft_block<S::LOGH1, true>(s, tw1);
+    const float inv_h = 1.0f / (float)S::H;
+    for (int m = threadIdx.x; m < S::H1; m += blockDim.x) {
+        const float2 z = s[spad(m)];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int t = 2 * (m * S::C + rank) + h;
+            if (t >= J.N) continue;
+            double p = (double)((h ? z.y : z.x) * inv_h);
+            if (J.U && edge_diag(t, J.N)) {
+                p = 0.0;
+                for (int g = 0; g < J.n_group; ++g) {
+                    const int i = J.group[g];
+                    if (i < 0 || i >= J.k) continue;
+                    p += (double)(float)J.sigma[i] *
+                         diag_sum(J.U + (long long)i * J.ldU, J.V + (long long)i * J.ldV, t, J.L, J.K);
+                }
+            }
+            const double v = p / (double)diag_count(t, J.N, J.L, J.K);
+            if (J.out64) J.out64[t] = v;
+            if (J.out) J.out[t] = (float)v;
+        }
+    }
+}
+
+template <int LOGH, int KIND>
+static int launch_cl_col(const ssa_col_job* jobs, int njobs, int maxcols, cudaStream_t st) {
+    using S = ClShape<LOGH>;
+    const int sm = cl_smem_f2<LOGH>() * (int)sizeof(float2);
+    cudaError_t e = cudaFuncSetAttribute(k_cl_col<LOGH, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return (int)e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(S::C * maxcols, njobs, 1);
+    cfg.blockDim = dim3(S::BLOCK, 1, 1);
+    cfg.dynamicSmemBytes = sm;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = S::C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, k_cl_col<LOGH, KIND>, jobs);
+    return launched(e != cudaSuccess ? e : cudaGetLastError());
+}
+
+template <int LOGH>
+static int launch_cl_recon(const ssa_recon_job* jobs, int njobs, cudaStream_t st) {
+    using S = ClShape<LOGH>;
+    const int sm = cl_smem_f2<LOGH>() * (int)sizeof(float2);
+    cudaError_t e = cudaFuncSetAttribute(k_cl_recon<LOGH>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return (int)e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(S::C, njobs, 1);
+    cfg.blockDim = dim3(S::BLOCK, 1, 1);
+    cfg.dynamicSmemBytes = sm;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = S::C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, k_cl_recon<LOGH>, jobs);
+    return launched(e != cudaSuccess ? e : cudaGetLastError());
+}
+
+// logh 15 or 16 (callers check)
+static int cl_col_dispatch(int kind, const ssa_col_job* jobs, int njobs, int maxcols, int logh, cudaStream_t st) {
+#define SSA_CL_CASE(L)                                                                        \
+    if (logh == L) {                                                                          \
+        if (kind == CL_SPEC) return launch_cl_col<L, CL_SPEC>(jobs, njobs, maxcols, st);     \
+        if (kind == CL_CORR) return launch_cl_col<L, CL_CORR>(jobs, njobs, maxcols, st);     \
+        return launch_cl_col<L, CL_ELEM>(jobs, njobs, maxcols, st);                           \
+    }
+    SSA_CL_CASE(15)
+    SSA_CL_CASE(16)
+#undef SSA_CL_CASE
+    return (int)cudaErrorInvalidValue;
+}
+
+static int cl_recon_dispatch(const ssa_recon_job* jobs, int njobs, int logh, cudaStream_t st) {
+    if (logh == 15) return launch_cl_recon<15>(jobs, njobs, st);
+    if (logh == 16) return launch_cl_recon<16>(jobs, njobs, st);
+    return (int)cudaErrorInvalidValue;
+}

@@ -53,7 +53,7 @@ int ssae_create(ssa_engine *e, int B, int N, int L, int kp, int k, cudaStream_t 
     if (B < 1 || N < 4 || L < 2 || L > N - 1 || kp < 1 || kp > SSA_MAX_KP || k < 1 || k > kp)
         return (int)cudaErrorInvalidValue;
     int logh = ssad_logh_for(N);
-    if (logh > 14)
+    if (logh > SSA_MAX_LOGH_ALL)
         return (int)cudaErrorInvalidValue;
     CK(cudaGetDevice(&e->device));
     CK(ssad_init_device());
@@ -706,6 +706,11 @@ int ssae_recon_group(ssa_engine *e, int s, int k, const int *d_group, int n_grou
     memset(&J, 0, sizeof(J));
     J.Us = e->Us + (size_t)s * e->k * e->ldS;
     J.Vs = e->Vs + (size_t)s * e->k * e->ldS;
+    J.U = e->Y + (size_t)s * e->ldL * e->kp;
+    J.V = e->Z + (size_t)s * e->ldK * e->kp;
+    J.ldU = e->ldL;
+    J.ldV = e->ldK;
+    J.sigma = e->sigma + (size_t)s * e->k;
     J.group = d_group;
     J.out64 = d_out;
     J.ld_spec = e->ldS;

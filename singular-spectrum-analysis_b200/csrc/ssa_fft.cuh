@@ -15,7 +15,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#define SSA_TW_LOG 15
+#define SSA_TW_LOG 17
 #define SSA_TW_N (1 << SSA_TW_LOG)
 // Largest complex FFT a single CTA holds: H = 2^14 points (real length M = 32768).
 #define SSA_MAX_LOGH 14

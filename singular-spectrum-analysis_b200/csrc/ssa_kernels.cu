@@ -90,6 +90,18 @@ __device__ __forceinline__ int diag_count(int t, int N, int L, int K) {
     return c > 0 ? c : 1;
 }
 
+__device__ __forceinline__ bool edge_diag(int t, int N) { return t < SSA_EDGE || t >= N - SSA_EDGE; }
+
+// sum_{i + j = t} u[i] v[j] over 0 <= i < L, 0 <= j < K, in FP64 (at most SSA_EDGE terms on an
+// edge anti-diagonal).
+__device__ __forceinline__ double diag_sum(const float* __restrict__ u, const float* __restrict__ v, int t, int L,
+                                           int K) {
+    const int i0 = max(0, t - K + 1), i1 = min(t, L - 1);
+    double s = 0.0;
+    for (int i = i0; i <= i1; ++i) s = fma((double)u[i], (double)v[t - i], s);
+    return s;
+}
+
 template <typename T>
 __device__ __forceinline__ T block_sum(T v, T* red) {
     // red: >= 32 entries of shared scratch; returns the total to every thread. Fixed order.
@@ -258,14 +270,16 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_elem_recon(const ssa_
     fft_block<LOGH, true>(s1, tw);
     float* out = J.out + (long long)c * J.ld_out;
     const float inv_h = 1.0f / (float)H;
+    const float* u = J.in + (long long)c * J.ld_in;
+    const float* vv = J.in2 + (long long)c * J.ld_in2;
     double acc = 0.0;
     for (int t = threadIdx.x; t < J.N; t += blockDim.x) {
         const float2 z = s1[spad(t >> 1)];
-        const float p = ((t & 1) ? z.y : z.x) * inv_h;
+        double p = (double)(((t & 1) ? z.y : z.x) * inv_h);
+        if (edge_diag(t, J.N)) p = (double)sc * diag_sum(u, vv, t, J.n_in, J.n_in2);
         const int cnt = diag_count(t, J.N, J.L, J.K);
-        const float v = p / (float)cnt;
-        out[t] = v;
-        acc += (double)p * (double)p / (double)cnt;
+        out[t] = (float)(p / (double)cnt);
+        acc += p * p / (double)cnt;
     }
     acc = block_sum<double>(acc, red);
     if (threadIdx.x == 0 && J.norm2) J.norm2[c] = acc;
@@ -310,14 +324,17 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_elem_recon1(const ssa
     fft_block<LOGH, true>(s2, tw);
     float* out = J.out + (long long)c * J.ld_out;
     const float inv_h = 1.0f / (float)H;
+    const float sc = J.scale ? (float)J.scale[c] : 1.0f;
+    const float* u = J.in + (long long)c * J.ld_in;
+    const float* vv = J.in2 + (long long)c * J.ld_in2;
     double acc = 0.0;
     for (int t = threadIdx.x; t < J.N; t += blockDim.x) {
         const float2 z = s2[spad(t >> 1)];
-        const float p = ((t & 1) ? z.y : z.x) * inv_h;
+        double p = (double)(((t & 1) ? z.y : z.x) * inv_h);
+        if (edge_diag(t, J.N)) p = (double)sc * diag_sum(u, vv, t, J.n_in, J.n_in2);
         const int cnt = diag_count(t, J.N, J.L, J.K);
-        const float v = p / (float)cnt;
-        out[t] = v;
-        acc += (double)p * (double)p / (double)cnt;
+        out[t] = (float)(p / (double)cnt);
+        acc += p * p / (double)cnt;
     }
     acc = block_sum<double>(acc, red);
     if (threadIdx.x == 0 && J.norm2) J.norm2[c] = acc;
@@ -375,8 +392,17 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k
     const float inv_h = 1.0f / (float)H;
     for (int t = threadIdx.x; t < J.N; t += blockDim.x) {
         const float2 z = smem[spad(t >> 1)];
-        const float p = ((t & 1) ? z.y : z.x) * inv_h;
-        const double v = (double)p / (double)diag_count(t, J.N, J.L, J.K);
+        double p = (double)(((t & 1) ? z.y : z.x) * inv_h);
+        if (J.U && edge_diag(t, J.N)) {
+            p = 0.0;
+            for (int g = 0; g < J.n_group; ++g) {
+                const int i = J.group[g];
+                if (i < 0 || i >= J.k) continue;
+                p += (double)(float)J.sigma[i] *
+                     diag_sum(J.U + (long long)i * J.ldU, J.V + (long long)i * J.ldV, t, J.L, J.K);
+            }
+        }
+        const double v = p / (double)diag_count(t, J.N, J.L, J.K);
         if (J.out64) J.out64[t] = v;
         if (J.out) J.out[t] = (float)v;
     }
@@ -1142,6 +1168,25 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_lrf(const ssa_lrf_job* __rest
     }
 }
 
+// Recurrence of the R-forecast from stored coefficients; forecasts so far stay in shared memory.
+__global__ void __launch_bounds__(SMALL_THREADS) k_forecast_apply(const ssa_fc_job* __restrict__ jobs) {
+    __shared__ double red[32];
+    __shared__ double fo[SSA_FC_MAX_H];
+    const ssa_fc_job J = jobs[blockIdx.x];
+    const int w = J.w;
+    for (int t = 0; t < J.h; ++t) {
+        double s = 0.0;
+        for (int j = threadIdx.x; j < w; j += blockDim.x) {
+            const int i = t + j;
+            s += J.R[j] * (i < w ? J.tail[i] : fo[i - w]);
+        }
+        s = block_sum<double>(s, red);
+        if (threadIdx.x == 0) fo[t] = s;
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < J.h; t += blockDim.x) J.out[t] = fo[t];
+}
+
 __global__ void k_group_sum(ssa_gsum_job J) {
     const int s = blockIdx.z, g = blockIdx.y;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1260,8 +1305,11 @@ static int launch_recon(const ssa_recon_job* jobs, int njobs, cudaStream_t st) {
     return launched(cudaGetLastError());
 }
 
+#include "ssa_cluster.cuh"
+
 extern "C" int ssad_spectrum(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
     if (njobs <= 0 || maxcols <= 0) return 0;
+    if (logh > SSA_MAX_LOGH) return cl_col_dispatch(CL_SPEC, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);
 #define CALL(L) return launch_spectrum<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
     SSA_LOGH_DISPATCH(logh, CALL)
 #undef CALL
@@ -1269,6 +1317,7 @@ extern "C" int ssad_spectrum(const ssa_col_job* d_jobs, int njobs, int maxcols, 
 }
 extern "C" int ssad_corr(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
     if (njobs <= 0 || maxcols <= 0) return 0;
+    if (logh > SSA_MAX_LOGH) return cl_col_dispatch(CL_CORR, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);
 #define CALL(L) return launch_corr<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
     SSA_LOGH_DISPATCH(logh, CALL)
 #undef CALL
@@ -1283,6 +1332,7 @@ extern "C" int ssad_elem_recon(const ssa_col_job* d_jobs, int njobs, int maxcols
 }
 extern "C" int ssad_elem_recon1(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
     if (njobs <= 0 || maxcols <= 0) return 0;
+    if (logh > SSA_MAX_LOGH) return cl_col_dispatch(CL_ELEM, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);
 #define CALL(L) return launch_elem1<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
     SSA_LOGH_DISPATCH(logh, CALL)
 #undef CALL
@@ -1298,6 +1348,7 @@ extern "C" int ssad_group_sum_ragged(const ssa_rgsum_job* d_jobs, int njobs, int
 }
 extern "C" int ssad_recon(const ssa_recon_job* d_jobs, int njobs, int logh, void* stream) {
     if (njobs <= 0) return 0;
+    if (logh > SSA_MAX_LOGH) return cl_recon_dispatch(d_jobs, njobs, logh, (cudaStream_t)stream);
 #define CALL(L) return launch_recon<L>(d_jobs, njobs, (cudaStream_t)stream)
     SSA_LOGH_DISPATCH(logh, CALL)
 #undef CALL
@@ -1347,6 +1398,12 @@ extern "C" int ssad_wfin(const ssa_wfin_job* d_jobs, int njobs, void* stream) {
 extern "C" int ssad_lrf(const ssa_lrf_job* d_jobs, int njobs, void* stream) {
     if (njobs <= 0) return 0;
     k_lrf<<<njobs, SMALL_THREADS, 0, (cudaStream_t)stream>>>(d_jobs);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_forecast_apply(const ssa_fc_job* d_jobs, int njobs, void* stream) {
+    if (njobs <= 0) return 0;
+    k_forecast_apply<<<njobs, SMALL_THREADS, 0, (cudaStream_t)stream>>>(d_jobs);
     return launched(cudaGetLastError());
 }
 

@@ -30,6 +30,9 @@ extern "C" {
 
 /* FFT-length bucket: real length M = 2^(logh + 1). */
 int ssad_logh_for(int N);
+/* Largest bucket: logh 16 (M = 131072, series up to N = 131072). Buckets up to 14 run one CTA
+ * per transform, 15 and 16 a thread-block cluster of 4 or 8 CTAs. */
+#define SSA_MAX_LOGH_ALL 16
 
 /* Column job for the FFT kernels (signal spectrum, correlation matvec, reconstruction). */
 typedef struct
@@ -160,18 +163,28 @@ typedef struct
     int nchunks, nchunks_q, kp, k;
 } ssa_rr_job;
 
-/* Reconstruction from cached spectra: out = inv_w * IFFT(sum_{g} Us[g] * Vs[g]). */
+/* Reconstruction from cached spectra: out = inv_w * IFFT(sum_{g} Us[g] * Vs[g]). When U is set,
+ * the first and last SSA_EDGE anti-diagonals are summed directly from sigma_i U_i and V_i instead
+ * (see SSA_EDGE). */
 typedef struct
 {
     const float *Us, *Vs;     /* spectra: component i at Us + i * ld_spec */
     const int *group;         /* n_group component indices (out of range skipped) */
     double *out64;            /* optional double output (N) */
     float *out;               /* optional float output (N) */
-    long long ld_spec;
+    const float *U, *V;       /* optional factors: column i at U + i * ldU (L rows), V + i * ldV (K rows) */
+    const double *sigma;
+    long long ld_spec, ldU, ldV;
     int n_group, k;
     int N, L, K;
     int pad_;
 } ssa_recon_job;
+
+/* Anti-diagonals at each end of the series that the reconstruction kernels sum directly (FP64)
+ * instead of taking from the FP32 FFT convolution: diagonal averaging divides the convolution's
+ * roughly uniform absolute rounding error by the anti-diagonal's length, so the short ones at the
+ * ends would otherwise dominate the reconstruction error. */
+#define SSA_EDGE 128
 
 /* W-correlation finish: W[i][j] = G_ij / sqrt(G_ii G_jj) (0 when a norm <= 1e-12). */
 typedef struct
@@ -252,6 +265,17 @@ int ssad_rr(const ssa_rr_job *d_jobs, int njobs, void *stream);
 int ssad_recon(const ssa_recon_job *d_jobs, int njobs, int logh, void *stream);
 int ssad_wfin(const ssa_wfin_job *d_jobs, int njobs, void *stream);
 int ssad_lrf(const ssa_lrf_job *d_jobs, int njobs, void *stream);
+/* R-forecast from stored LRF coefficients: out[t] = sum_{j < w} R[j] v[t + j] for t < h, where
+ * v = (tail[0..w), out[0..t)) (the recurrence of MKL/ssa_opt.h:2818-2841). One CTA per job. */
+typedef struct
+{
+    const double *R;      /* w = L - 1 coefficients */
+    const double *tail;   /* last w reconstructed values */
+    double *out;          /* h forecasts */
+    int w, h;
+} ssa_fc_job;
+#define SSA_FC_MAX_H 4096
+int ssad_forecast_apply(const ssa_fc_job *d_jobs, int njobs, void *stream);
 /* Column-major K x ncols N(0,1) matrix from the device generator (the same values the
  * correlation kernel generates when its input is NULL). */
 int ssad_gaussian(float *out, long long ld, int rows, int ncols, int col0, unsigned long long seed,

@@ -79,7 +79,7 @@ int mssa_opt_init(MSSA_Opt *mssa, const ssa_real *X, int M, int N, int L)
         return -1;
     memset(mssa, 0, sizeof(*mssa));
     const int logh = ssad_logh_for(N);
-    if (logh > 14)
+    if (logh > SSA_MAX_LOGH_ALL)
         return -1;
     mssa->M = M;
     mssa->N = N;

@@ -39,7 +39,7 @@
     } while (0)
 
 #define RB_MIN_LOGH 4
-#define RB_MAX_LOGH 14
+#define RB_MAX_LOGH SSA_MAX_LOGH_ALL
 #define RB_NB (RB_MAX_LOGH + 1)
 
 typedef struct
@@ -83,6 +83,13 @@ struct ssa_rbatch
     int B;
     size_t n_x, n_sig, n_W, n_grp;
     size_t *h_off; /* 4 B offsets of the last run: x, sigma, W, groups */
+    /* optional per-run extensions (ssar_run_enqueue_ex) */
+    const unsigned long long *cur_seeds; /* per-series generator seeds, or NULL */
+    double *const *cur_lrf;              /* per-series LRF destinations, or NULL */
+    int lrf_slot, n_lrf_group, lrf_gmax;
+    int *d_lrf_group;
+    int *lrf_status;
+    int c_lrf_status;
 };
 
 static int imin(int a, int b) { return a < b ? a : b; }
@@ -140,7 +147,8 @@ void ssa_rbatch_destroy(ssa_rbatch *rb)
         cudaStreamSynchronize(rb->main);
     for (int i = 0; i < RB_NB; i++)
         bucket_free(&rb->bk[i]);
-    void *bufs[] = {rb->d_gidx, rb->d_goff, rb->d_xs, rb->sigma, rb->W, rb->groups, rb->status};
+    void *bufs[] = {rb->d_gidx, rb->d_goff, rb->d_xs, rb->sigma, rb->W, rb->groups, rb->status, rb->lrf_status,
+                    rb->d_lrf_group};
     for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
         if (bufs[i])
             cudaFree(bufs[i]);
@@ -246,8 +254,9 @@ static int r_spectrum(rbucket *b, const double *d_x)
     return rc;
 }
 
-/* adjoint 0: Y = H (Omega | Z); adjoint 1: Z = H^T Y. generate: Omega from the device generator. */
-static int r_sweep(rbucket *b, int adjoint, int generate, unsigned long long seed)
+/* adjoint 0: Y = H (Omega | Z); adjoint 1: Z = H^T Y. generate: Omega from the device generator,
+ * series seed seeds[src] when given, else seed mixed with the batch position. */
+static int r_sweep(rbucket *b, int adjoint, int generate, unsigned long long seed, const unsigned long long *seeds)
 {
     ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)b->nb, sizeof(ssa_col_job));
     if (!jobs)
@@ -263,7 +272,7 @@ static int r_sweep(rbucket *b, int adjoint, int generate, unsigned long long see
             if (generate)
             {
                 J->in = NULL;
-                J->seed = seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(S->src + 1));
+                J->seed = seeds ? seeds[S->src] : seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(S->src + 1));
             }
             else
             {
@@ -596,22 +605,67 @@ static int r_gsum(rbucket *b, ssa_rbatch *rb)
     return rc;
 }
 
+/* LRF coefficients and reconstruction tail of the forecast group (group slot rb->lrf_slot) into
+ * the per-series destinations: R (L-1), tail (L-1), verticality (1) doubles. */
+static int r_lrf(rbucket *b, ssa_rbatch *rb)
+{
+    ssa_lrf_job *jobs = (ssa_lrf_job *)calloc((size_t)b->nb, sizeof(ssa_lrf_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    int n = 0;
+    for (int i = 0; i < b->nb; i++)
+    {
+        const rser *S = &b->sd[i];
+        double *dst = rb->cur_lrf[S->src];
+        if (!dst || rb->lrf_gmax >= S->k)
+            continue;
+        ssa_lrf_job *J = &jobs[n++];
+        J->U = b->Y + S->oY;
+        J->ld = S->ldL;
+        J->group = rb->d_lrf_group;
+        J->n_group = rb->n_lrf_group;
+        J->recon = rb->groups + S->ogrp + (size_t)rb->lrf_slot * S->N;
+        J->R = dst;
+        J->buf = dst + (S->L - 1);
+        J->out = NULL;
+        J->verticality = dst + 2 * (size_t)(S->L - 1);
+        J->status = rb->lrf_status + S->src;
+        J->L = S->L;
+        J->N = S->N;
+        J->h = 0;
+        J->k = S->k;
+    }
+    if (!n)
+    {
+        free(jobs);
+        return 0;
+    }
+    void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_lrf_job) * n);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(&b->e, SSAK_LRF);
+    int rc = ssad_lrf((const ssa_lrf_job *)d, n, b->e.st);
+    ssae_prof_end(&b->e);
+    return rc;
+}
+
 /* Whole pipeline of one bucket on its stream (the stage order of ssae_decompose,
  * ssae_elem_recon, ssae_wcorr and the batch group sums). */
 static int bucket_run(rbucket *b, ssa_rbatch *rb, const double *d_x, unsigned long long seed)
 {
     CK(r_spectrum(b, d_x));
-    CK(r_sweep(b, 0, 1, seed));
+    CK(r_sweep(b, 0, 1, seed, rb->cur_seeds));
     for (int it = 0; it < rb->q; it++)
     {
         CK(r_cholqr(b, SIDE_L, 0, rb->status));
-        CK(r_sweep(b, 1, 0, 0));
+        CK(r_sweep(b, 1, 0, 0, NULL));
         CK(r_cholqr(b, SIDE_K, 0, rb->status));
-        CK(r_sweep(b, 0, 0, 0));
+        CK(r_sweep(b, 0, 0, 0, NULL));
     }
     CK(r_cholqr(b, SIDE_L, 0, rb->status));
     CK(r_cholqr(b, SIDE_L, 1, rb->status));
-    CK(r_sweep(b, 1, 0, 0));
+    CK(r_sweep(b, 1, 0, 0, NULL));
     CK(r_gram(b, SIDE_K));
     CK(r_rr(b, rb->sigma, rb->status));
     CK(r_rowmul(b, SIDE_L, 0, 0));
@@ -620,6 +674,8 @@ static int bucket_run(rbucket *b, ssa_rbatch *rb, const double *d_x, unsigned lo
     CK(r_wcorr(b, rb->W));
     if (rb->n_groups > 0)
         CK(r_gsum(b, rb));
+    if (rb->cur_lrf && rb->n_lrf_group > 0 && rb->n_groups > 0)
+        CK(r_lrf(b, rb));
     return 0;
 }
 
@@ -764,6 +820,16 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
             return -1;
         rb->c_status = B;
     }
+    if (B > rb->c_lrf_status)
+    {
+        if (rb->lrf_status)
+            cudaFree(rb->lrf_status);
+        rb->lrf_status = NULL;
+        rb->c_lrf_status = 0;
+        if (cudaMalloc((void **)&rb->lrf_status, sizeof(int) * B) != cudaSuccess)
+            return -1;
+        rb->c_lrf_status = B;
+    }
     return rc ? -1 : 0;
 }
 
@@ -796,6 +862,7 @@ static int run_enqueue(ssa_rbatch *rb, int B, const int *N, const int *L, const 
         return -1;
     rb->B = B;
     if (cudaMemsetAsync(rb->status, 0, sizeof(int) * B, rb->main) != cudaSuccess ||
+        cudaMemsetAsync(rb->lrf_status, 0, sizeof(int) * B, rb->main) != cudaSuccess ||
         cudaEventRecord(rb->ev_in, rb->main) != cudaSuccess)
         return -1;
     /* largest FFT lengths first: they take longest */
@@ -942,4 +1009,82 @@ int ssa_rbatch_profile(ssa_rbatch *rb, double *ms, long long *launches, int nkin
         }
     }
     return SSAK_NKINDS;
+}
+
+/* ---- extensions for the request server (ssa_ragged_int.h) ------------------------------- */
+
+int ssar_set_lrf_group(ssa_rbatch *rb, int slot, const int *group, int n_group)
+{
+    if (!rb || slot < 0 || slot >= rb->n_groups || n_group < 1 || n_group > SSA_MAX_KP)
+        return -1;
+    int gmax = 0;
+    for (int i = 0; i < n_group; i++)
+    {
+        if (group[i] < 0 || group[i] >= SSA_MAX_KP)
+            return -1;
+        gmax = imax(gmax, group[i]);
+    }
+    if (!rb->d_lrf_group && cudaMalloc((void **)&rb->d_lrf_group, sizeof(int) * SSA_MAX_KP) != cudaSuccess)
+        return -1;
+    if (cudaMemcpy(rb->d_lrf_group, group, sizeof(int) * n_group, cudaMemcpyHostToDevice) != cudaSuccess)
+        return -1;
+    rb->lrf_slot = slot;
+    rb->n_lrf_group = n_group;
+    rb->lrf_gmax = gmax;
+    return 0;
+}
+
+int ssar_run_enqueue_ex(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k, const double *d_x,
+                        const unsigned long long *seeds, double *const *lrf_dst)
+{
+    if (!rb || B < 1 || !N || !L || !k || !d_x)
+        return -1;
+    if (quiesce(rb) != 0)
+        return -1;
+    rb->cur_seeds = seeds;
+    rb->cur_lrf = lrf_dst;
+    int rc = run_enqueue(rb, B, N, L, k, d_x, 0);
+    rb->cur_seeds = NULL;
+    rb->cur_lrf = NULL;
+    return rc;
+}
+
+cudaStream_t ssar_main_stream(const ssa_rbatch *rb) { return rb->main; }
+const int *ssar_status(const ssa_rbatch *rb) { return rb->status; }
+const int *ssar_lrf_status(const ssa_rbatch *rb) { return rb->lrf_status; }
+const double *ssar_sigma(const ssa_rbatch *rb) { return rb->sigma; }
+const double *ssar_W(const ssa_rbatch *rb) { return rb->W; }
+const double *ssar_groups(const ssa_rbatch *rb) { return rb->groups; }
+const size_t *ssar_offsets(const ssa_rbatch *rb) { return rb->h_off; }
+void ssar_totals(const ssa_rbatch *rb, size_t *t4)
+{
+    t4[0] = rb->n_x;
+    t4[1] = rb->n_sig;
+    t4[2] = rb->n_W;
+    t4[3] = rb->n_grp;
+}
+
+/* Device bytes one series of this shape occupies in a bucket and in the packed outputs. */
+size_t ssar_series_bytes(int N, int L, int k, int p, int n_groups)
+{
+    const int K = N - L + 1;
+    const int kp = imin(k + p, imin(L, K));
+    k = imin(k, kp);
+    const int logh = ssad_logh_for(N);
+    const size_t ldS = (size_t)round4(2LL * ((1 << logh) + 1) + 2);
+    const int nb_est = 64; /* Gram chunking at moderate bucket sizes */
+    const int nch = imax(imax((L + gram_rows(L, nb_est) - 1) / gram_rows(L, nb_est),
+                              (K + gram_rows(K, nb_est) - 1) / gram_rows(K, nb_est)),
+                         (N + gram_rows(N, nb_est) - 1) / gram_rows(N, nb_est));
+    size_t b = 0;
+    b += 4 * ldS;                                               /* X */
+    b += 4 * (size_t)(round4(L) + round4(K)) * kp;               /* Y, Z */
+    b += 8 * (size_t)nch * kp * (kp + 1) / 2;                    /* part */
+    b += 8 * (size_t)((L + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS) * kp; /* qsum */
+    b += 4 * (size_t)kp * kp + 8 * (size_t)kp * k;               /* R, Zu, Zv */
+    b += 4 * (size_t)k * round4(N) + 8 * (size_t)k;              /* recon, norm2 */
+    if (logh > SSA_ELEM2_MAX_LOGH)
+        b += 4 * (size_t)k * ldS;                                /* Us */
+    b += 8 * ((size_t)N + k + (size_t)k * k + (size_t)n_groups * N); /* x, sigma, W, groups */
+    return b + b / 8;                                           /* growth slack */
 }

@@ -1,0 +1,937 @@
+/*
+ * Request server: continuous batching of decompose / reconstruct / W-correlation / forecast
+ * requests of mixed size on one GPU.
+ *
+ * One worker thread owns the device work. Requests are queued by ssa_server_submit (any thread)
+ * and taken in arrival order. Decompositions are gathered into uneven batches (ssa_ragged.c),
+ * each batch bounded by a device-memory share of the HBM budget; up to `max_inflight` batches
+ * run at once on their own streams, so requests that arrive while others are on the GPU start
+ * as soon as a batch slot is free and overlap with the running ones. A decompose+reconstruct
+ * request leaves its series resident: the LRF coefficients of the forecast group [0, 1, 2] and
+ * the last L - 1 values of that group's reconstruction stay in device memory (stream-ordered
+ * pool, least recently used entries evicted beyond the resident share of the budget), so a later
+ * forecast request on that series runs the recurrence only (batched, one CTA per request)
+ * without decomposing again. Every request is stamped with its arrival and completion times on
+ * the host's monotonic clock; completion means its outputs are in host memory.
+ */
+#include <errno.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include <cuda_runtime_api.h>
+
+#include "ssa_engine.h"
+#include "ssa_ragged_int.h"
+#include "../../include/ssa_opt.h"
+
+#define SRV_GROUPS 3 /* [0], [1, 2], [0, 1, 2] (forecast group) */
+
+static const int g_group_idx[] = {0, 1, 2, 0, 1, 2};
+static const int g_group_sizes[] = {1, 2, 3};
+static const int g_fc_group[] = {0, 1, 2};
+static int g_not_resident; /* marker: the request was seen and gets no resident entry */
+
+enum
+{
+    RES_PENDING = 0,
+    RES_READY = 1,
+    RES_FAILED = 2
+};
+
+typedef struct res_entry
+{
+    int id;
+    int state;
+    int L;
+    int refs;          /* in-flight forecasts using it */
+    double *d;         /* R (L-1), tail (L-1), verticality */
+    size_t bytes;
+    struct res_entry *prev, *next; /* LRU list, most recent first */
+    struct res_entry *hnext;
+} res_entry;
+
+typedef struct
+{
+    ssa_rbatch *rb;
+    int busy;
+    int n, cap;
+    ssa_request **req;
+    int *N, *L, *k;
+    unsigned long long *seeds;
+    double **lrf_dst;
+    res_entry **res;
+    double *h_x, *h_sig, *h_W, *h_grp;
+    size_t c_x, c_sig, c_W, c_grp;
+    int *h_st, *h_lst;
+    size_t c_st, c_lst;
+    double *d_x;
+    size_t c_dx;
+    size_t bytes;
+    cudaEvent_t done;
+} slot_t;
+
+typedef struct
+{
+    cudaStream_t st;
+    cudaEvent_t done;
+    int busy;
+    int n, cap;
+    ssa_request **req;
+    res_entry **res;
+    ssa_fc_job *h_jobs, *d_jobs;
+    double *h_out, *d_out;
+    size_t c_hout, c_dout;
+} fslot_t;
+
+struct ssa_server
+{
+    pthread_t th;
+    int th_live;
+    pthread_mutex_t mu;
+    pthread_cond_t cv;      /* worker wake-up */
+    pthread_cond_t cv_done; /* drain */
+    int stop;
+    /* submitted, not yet taken by the worker (ring) */
+    ssa_request **q;
+    int qhead, qcount, qcap;
+    long long outstanding; /* submitted and not completed */
+    /* worker-private */
+    ssa_request **pend; /* taken, waiting for a slot (decompositions) or a target (forecasts) */
+    int npend, cpend;
+    slot_t *slots;
+    int nslots;
+    fslot_t fs;
+    int p, q_iters, max_batch;
+    size_t budget, batch_budget, res_budget, res_bytes;
+    res_entry **htab;
+    int hcap;
+    res_entry *lru_head, *lru_tail;
+    cudaStream_t pool_st;
+    cudaEvent_t ev_pool;
+    int device;
+    ssa_server_stats stats;
+};
+
+double ssa_server_now(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+static int imin(int a, int b) { return a < b ? a : b; }
+
+/* ---- resident store ------------------------------------------------------------------------ */
+
+static res_entry *res_find(ssa_server *s, int id)
+{
+    res_entry *e = s->htab[(unsigned)id % (unsigned)s->hcap];
+    while (e && e->id != id)
+        e = e->hnext;
+    return e;
+}
+
+static void lru_unlink(ssa_server *s, res_entry *e)
+{
+    if (e->prev)
+        e->prev->next = e->next;
+    else
+        s->lru_head = e->next;
+    if (e->next)
+        e->next->prev = e->prev;
+    else
+        s->lru_tail = e->prev;
+    e->prev = e->next = NULL;
+}
+
+static void lru_front(ssa_server *s, res_entry *e)
+{
+    e->next = s->lru_head;
+    e->prev = NULL;
+    if (s->lru_head)
+        s->lru_head->prev = e;
+    s->lru_head = e;
+    if (!s->lru_tail)
+        s->lru_tail = e;
+}
+
+static void res_remove(ssa_server *s, res_entry *e)
+{
+    res_entry **pp = &s->htab[(unsigned)e->id % (unsigned)s->hcap];
+    while (*pp && *pp != e)
+        pp = &(*pp)->hnext;
+    if (*pp)
+        *pp = e->hnext;
+    lru_unlink(s, e);
+    if (e->d)
+        cudaFreeAsync(e->d, s->pool_st);
+    s->res_bytes -= e->bytes;
+    free(e);
+}
+
+/* Evict least recently used entries that nothing uses until `need` more bytes fit. */
+static int res_make_room(ssa_server *s, size_t need)
+{
+    res_entry *e = s->lru_tail;
+    while (s->res_bytes + need > s->res_budget && e)
+    {
+        res_entry *prev = e->prev;
+        if (e->refs == 0 && e->state != RES_PENDING)
+        {
+            res_remove(s, e);
+            s->stats.evictions++;
+        }
+        e = prev;
+    }
+    return s->res_bytes + need <= s->res_budget ? 0 : -1;
+}
+
+/* New pending entry for series `id` with window L, without device memory yet (replaces an idle
+ * older one); forecasts on the series wait while it is pending. */
+static res_entry *res_create(ssa_server *s, int id, int L)
+{
+    res_entry *old = res_find(s, id);
+    if (old)
+    {
+        if (old->refs > 0 || old->state == RES_PENDING)
+            return NULL;
+        res_remove(s, old);
+    }
+    res_entry *e = (res_entry *)calloc(1, sizeof(res_entry));
+    if (!e)
+        return NULL;
+    e->id = id;
+    e->L = L;
+    e->state = RES_PENDING;
+    unsigned h = (unsigned)id % (unsigned)s->hcap;
+    e->hnext = s->htab[h];
+    s->htab[h] = e;
+    lru_front(s, e);
+    return e;
+}
+
+/* Device memory for a pending entry when its decomposition is launched: R (L-1), tail (L-1) and
+ * verticality doubles, evicting least recently used idle series beyond the resident budget. */
+static int res_alloc(ssa_server *s, res_entry *e)
+{
+    const size_t bytes = sizeof(double) * (2 * (size_t)(e->L - 1) + 1);
+    if (res_make_room(s, bytes) != 0)
+        return -1;
+    if (cudaMallocAsync((void **)&e->d, bytes, s->pool_st) != cudaSuccess)
+    {
+        e->d = NULL;
+        return -1;
+    }
+    e->bytes = bytes;
+    s->res_bytes += bytes;
+    return 0;
+}
+
+/* ---- helpers ------------------------------------------------------------------------------ */
+
+static int grow_host(void **p, size_t *cap, size_t need, size_t elem)
+{
+    if (need <= *cap && *p)
+        return 0;
+    if (*p)
+        cudaFreeHost(*p);
+    *p = NULL;
+    *cap = 0;
+    size_t n = need + need / 4 + 16;
+    if (cudaMallocHost(p, n * elem) != cudaSuccess)
+        return -1;
+    *cap = n;
+    return 0;
+}
+
+static int grow_dev(void **p, size_t *cap, size_t need, size_t elem)
+{
+    if (need <= *cap && *p)
+        return 0;
+    if (*p)
+        cudaFree(*p);
+    *p = NULL;
+    *cap = 0;
+    size_t n = need + need / 4 + 16;
+    if (cudaMalloc(p, n * elem) != cudaSuccess)
+        return -1;
+    *cap = n;
+    return 0;
+}
+
+static int ensure_cap(void ***arr, int *cap, int need, size_t elem)
+{
+    if (need <= *cap)
+        return 0;
+    int n = need + need / 2 + 8;
+    void **a = (void **)realloc(*arr, elem * (size_t)n);
+    if (!a)
+        return -1;
+    *arr = a;
+    *cap = n;
+    return 0;
+}
+
+static void finish_request(ssa_server *s, ssa_request *r, int status)
+{
+    r->status = status;
+    r->t_done = ssa_server_now();
+    pthread_mutex_lock(&s->mu);
+    s->outstanding--;
+    if (status == 0)
+        s->stats.completed++;
+    else
+        s->stats.failed++;
+    pthread_cond_broadcast(&s->cv_done);
+    pthread_mutex_unlock(&s->mu);
+}
+
+static int is_decomp(const ssa_request *r) { return r->type == SSA_REQ_DECOMPOSE_RECON || r->type == SSA_REQ_DECOMPOSE_WCORR; }
+
+static int valid_decomp(const ssa_server *s, const ssa_request *r)
+{
+    if (!r->x || r->N < 4 || r->L < 2 || r->L > r->N - 1 || r->k < 1 || ssad_logh_for(r->N) > SSA_MAX_LOGH_ALL)
+        return 0;
+    const int K = r->N - r->L + 1;
+    return imin(r->k + s->p, imin(r->L, K)) <= SSA_MAX_KP;
+}
+
+/* ---- decomposition batches ------------------------------------------------------------------ */
+
+static int slot_reserve(slot_t *sl, int n)
+{
+    if (n <= sl->cap)
+        return 0;
+    int c = n + n / 2 + 16;
+    void *a[8];
+    a[0] = realloc(sl->req, sizeof(ssa_request *) * c);
+    if (a[0])
+        sl->req = (ssa_request **)a[0];
+    a[1] = realloc(sl->N, sizeof(int) * c);
+    if (a[1])
+        sl->N = (int *)a[1];
+    a[2] = realloc(sl->L, sizeof(int) * c);
+    if (a[2])
+        sl->L = (int *)a[2];
+    a[3] = realloc(sl->k, sizeof(int) * c);
+    if (a[3])
+        sl->k = (int *)a[3];
+    a[4] = realloc(sl->seeds, sizeof(unsigned long long) * c);
+    if (a[4])
+        sl->seeds = (unsigned long long *)a[4];
+    a[5] = realloc(sl->lrf_dst, sizeof(double *) * c);
+    if (a[5])
+        sl->lrf_dst = (double **)a[5];
+    a[6] = realloc(sl->res, sizeof(res_entry *) * c);
+    if (a[6])
+        sl->res = (res_entry **)a[6];
+    for (int i = 0; i < 7; i++)
+        if (!a[i])
+            return -1;
+    sl->cap = c;
+    return 0;
+}
+
+/* Launch the batch gathered in sl (sl->n requests, dims filled). */
+static int slot_launch(ssa_server *s, slot_t *sl)
+{
+    size_t nx = 0;
+    for (int i = 0; i < sl->n; i++)
+        nx += (size_t)sl->N[i];
+    if (grow_host((void **)&sl->h_x, &sl->c_x, nx, sizeof(double)) != 0 ||
+        grow_dev((void **)&sl->d_x, &sl->c_dx, nx, sizeof(double)) != 0)
+        return -1;
+    size_t o = 0;
+    for (int i = 0; i < sl->n; i++)
+    {
+        memcpy(sl->h_x + o, sl->req[i]->x, sizeof(double) * sl->N[i]);
+        o += (size_t)sl->N[i];
+    }
+    cudaStream_t ms = ssar_main_stream(sl->rb);
+    /* resident blocks were allocated on the pool stream: order the batch after them */
+    if (cudaEventRecord(s->ev_pool, s->pool_st) != cudaSuccess || cudaStreamWaitEvent(ms, s->ev_pool, 0) != cudaSuccess)
+        return -1;
+    if (cudaMemcpyAsync(sl->d_x, sl->h_x, sizeof(double) * nx, cudaMemcpyHostToDevice, ms) != cudaSuccess)
+        return -1;
+    if (ssar_run_enqueue_ex(sl->rb, sl->n, sl->N, sl->L, sl->k, sl->d_x, sl->seeds, sl->lrf_dst) != 0)
+        return -1;
+    size_t t4[4];
+    ssar_totals(sl->rb, t4);
+    if (grow_host((void **)&sl->h_sig, &sl->c_sig, t4[1], sizeof(double)) != 0 ||
+        grow_host((void **)&sl->h_W, &sl->c_W, t4[2], sizeof(double)) != 0 ||
+        grow_host((void **)&sl->h_grp, &sl->c_grp, t4[3], sizeof(double)) != 0 ||
+        grow_host((void **)&sl->h_st, &sl->c_st, (size_t)sl->n, sizeof(int)) != 0 ||
+        grow_host((void **)&sl->h_lst, &sl->c_lst, (size_t)sl->n, sizeof(int)) != 0)
+        return -1;
+    if (cudaMemcpyAsync(sl->h_sig, ssar_sigma(sl->rb), sizeof(double) * t4[1], cudaMemcpyDeviceToHost, ms) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(sl->h_W, ssar_W(sl->rb), sizeof(double) * t4[2], cudaMemcpyDeviceToHost, ms) != cudaSuccess ||
+        cudaMemcpyAsync(sl->h_grp, ssar_groups(sl->rb), sizeof(double) * t4[3], cudaMemcpyDeviceToHost, ms) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(sl->h_st, ssar_status(sl->rb), sizeof(int) * sl->n, cudaMemcpyDeviceToHost, ms) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(sl->h_lst, ssar_lrf_status(sl->rb), sizeof(int) * sl->n, cudaMemcpyDeviceToHost, ms) !=
+            cudaSuccess ||
+        cudaEventRecord(sl->done, ms) != cudaSuccess)
+        return -1;
+    sl->busy = 1;
+    s->stats.batches++;
+    s->stats.decompositions += sl->n;
+    if (sl->n > s->stats.max_batch)
+        s->stats.max_batch = sl->n;
+    return 0;
+}
+
+static void slot_finish(ssa_server *s, slot_t *sl, int launch_ok)
+{
+    const size_t *off = launch_ok ? ssar_offsets(sl->rb) : NULL;
+    for (int i = 0; i < sl->n; i++)
+    {
+        ssa_request *r = sl->req[i];
+        int ok = launch_ok && sl->h_st[i] == 0;
+        if (ok)
+        {
+            const int K = r->N - r->L + 1;
+            const int kp = imin(r->k + s->p, imin(r->L, K));
+            const int ke = imin(r->k, kp);
+            r->k_out = ke;
+            if (r->sigma)
+                memcpy(r->sigma, sl->h_sig + off[4 * i + 1], sizeof(double) * ke);
+            if (r->W)
+                memcpy(r->W, sl->h_W + off[4 * i + 2], sizeof(double) * ke * ke);
+            if (r->groups)
+                memcpy(r->groups, sl->h_grp + off[4 * i + 3], sizeof(double) * 2 * r->N);
+        }
+        res_entry *e = sl->res[i];
+        if (e) /* the forecast group [0, 1, 2] needs at least 3 components */
+            e->state = (ok && e->d && sl->h_lst[i] == 0 && r->k_out > 2) ? RES_READY : RES_FAILED;
+        finish_request(s, r, ok ? 0 : -1);
+    }
+    sl->n = 0;
+    sl->busy = 0;
+}
+
+/* ---- forecast batches ------------------------------------------------------------------- */
+
+static int fs_launch(ssa_server *s)
+{
+    fslot_t *f = &s->fs;
+    size_t nout = 0;
+    for (int i = 0; i < f->n; i++)
+        nout += (size_t)f->req[i]->h;
+    if (grow_dev((void **)&f->d_out, &f->c_dout, nout, sizeof(double)) != 0)
+        return -1;
+    if (grow_host((void **)&f->h_out, &f->c_hout, nout, sizeof(double)) != 0)
+        return -1;
+    size_t o = 0;
+    for (int i = 0; i < f->n; i++)
+    {
+        ssa_fc_job *J = &f->h_jobs[i];
+        res_entry *e = f->res[i];
+        J->R = e->d;
+        J->tail = e->d + (e->L - 1);
+        J->out = f->d_out + o;
+        J->w = e->L - 1;
+        J->h = f->req[i]->h;
+        o += (size_t)J->h;
+    }
+    if (cudaMemcpyAsync(f->d_jobs, f->h_jobs, sizeof(ssa_fc_job) * f->n, cudaMemcpyHostToDevice, f->st) !=
+            cudaSuccess ||
+        ssad_forecast_apply(f->d_jobs, f->n, f->st) != 0 ||
+        cudaMemcpyAsync(f->h_out, f->d_out, sizeof(double) * nout, cudaMemcpyDeviceToHost, f->st) != cudaSuccess ||
+        cudaEventRecord(f->done, f->st) != cudaSuccess)
+        return -1;
+    f->busy = 1;
+    s->stats.forecast_batches++;
+    s->stats.forecasts += f->n;
+    return 0;
+}
+
+static void fs_finish(ssa_server *s, int ok)
+{
+    fslot_t *f = &s->fs;
+    size_t o = 0;
+    for (int i = 0; i < f->n; i++)
+    {
+        ssa_request *r = f->req[i];
+        if (ok && r->forecast)
+            memcpy(r->forecast, f->h_out + o, sizeof(double) * r->h);
+        o += (size_t)r->h;
+        f->res[i]->refs--;
+        finish_request(s, r, ok ? 0 : -1);
+    }
+    f->n = 0;
+    f->busy = 0;
+}
+
+/* ---- worker ---------------------------------------------------------------------------------- */
+
+static int poll_done(ssa_server *s)
+{
+    int progressed = 0;
+    for (int i = 0; i < s->nslots; i++)
+    {
+        slot_t *sl = &s->slots[i];
+        if (!sl->busy)
+            continue;
+        cudaError_t q = cudaEventQuery(sl->done);
+        if (q == cudaErrorNotReady)
+            continue;
+        slot_finish(s, sl, q == cudaSuccess);
+        progressed = 1;
+    }
+    if (s->fs.busy)
+    {
+        cudaError_t q = cudaEventQuery(s->fs.done);
+        if (q != cudaErrorNotReady)
+        {
+            fs_finish(s, q == cudaSuccess);
+            progressed = 1;
+        }
+    }
+    return progressed;
+}
+
+/* Move submitted requests to the worker's pending list (arrival order kept). */
+static void take_queue(ssa_server *s)
+{
+    pthread_mutex_lock(&s->mu);
+    if (s->qcount > 0 && ensure_cap((void ***)&s->pend, &s->cpend, s->npend + s->qcount, sizeof(ssa_request *)) == 0)
+    {
+        while (s->qcount > 0)
+        {
+            s->pend[s->npend++] = s->q[s->qhead];
+            s->qhead = (s->qhead + 1) % s->qcap;
+            s->qcount--;
+        }
+    }
+    pthread_mutex_unlock(&s->mu);
+}
+
+/* Form and launch at most one forecast batch and one decomposition batch per free slot. */
+static int dispatch(ssa_server *s)
+{
+    int progressed = 0;
+    slot_t *free_slot = NULL;
+    for (int i = 0; i < s->nslots && !free_slot; i++)
+        if (!s->slots[i].busy)
+            free_slot = &s->slots[i];
+    fslot_t *f = s->fs.busy ? NULL : &s->fs;
+    size_t bytes = 0;
+    int kept = 0;
+    for (int i = 0; i < s->npend; i++)
+    {
+        ssa_request *r = s->pend[i];
+        int keep = 1;
+        if (r->type == SSA_REQ_FORECAST)
+        {
+            res_entry *e = res_find(s, r->series_id);
+            if (!e || e->state == RES_FAILED || r->h < 1 || r->h > SSA_FC_MAX_H)
+            {
+                finish_request(s, r, -1);
+                keep = 0;
+                progressed = 1;
+            }
+            else if (e->state == RES_READY && f && f->n < s->max_batch)
+            {
+                if (f->n >= f->cap)
+                {
+                    int c = f->cap ? 2 * f->cap : 256;
+                    void *a = realloc(f->req, sizeof(ssa_request *) * c);
+                    void *b = a ? realloc(f->res, sizeof(res_entry *) * c) : NULL;
+                    if (a)
+                        f->req = (ssa_request **)a;
+                    if (b)
+                        f->res = (res_entry **)b;
+                    ssa_fc_job *hj = NULL, *dj = NULL;
+                    if (a && b && cudaMallocHost((void **)&hj, sizeof(ssa_fc_job) * c) == cudaSuccess &&
+                        cudaMalloc((void **)&dj, sizeof(ssa_fc_job) * c) == cudaSuccess)
+                    {
+                        if (f->h_jobs)
+                            cudaFreeHost(f->h_jobs);
+                        if (f->d_jobs)
+                            cudaFree(f->d_jobs);
+                        f->h_jobs = hj;
+                        f->d_jobs = dj;
+                        f->cap = c;
+                    }
+                    else
+                    {
+                        if (hj)
+                            cudaFreeHost(hj);
+                        f = NULL; /* try again next round */
+                    }
+                }
+                if (f && f->n < f->cap)
+                {
+                    e->refs++;
+                    lru_unlink(s, e);
+                    lru_front(s, e);
+                    f->req[f->n] = r;
+                    f->res[f->n] = e;
+                    f->n++;
+                    keep = 0;
+                }
+            }
+        }
+        else if (is_decomp(r))
+        {
+            if (r->type == SSA_REQ_DECOMPOSE_RECON && !r->priv && valid_decomp(s, r))
+            {
+                /* pending resident entry from the moment the request is seen, so forecasts on
+                 * the series that arrive later wait for it */
+                r->priv = res_create(s, r->series_id, r->L);
+                if (!r->priv)
+                {
+                    s->stats.not_resident++;
+                    r->priv = (void *)&g_not_resident;
+                }
+            }
+            if (!valid_decomp(s, r))
+            {
+                finish_request(s, r, -1);
+                keep = 0;
+                progressed = 1;
+            }
+            else if (free_slot && free_slot->n < s->max_batch)
+            {
+                const size_t b = ssar_series_bytes(r->N, r->L, r->k, s->p, SRV_GROUPS);
+                if (b > s->batch_budget)
+                {
+                    if (r->priv && r->priv != (void *)&g_not_resident)
+                        ((res_entry *)r->priv)->state = RES_FAILED;
+                    finish_request(s, r, -1); /* larger than a batch's share of the budget */
+                    keep = 0;
+                    progressed = 1;
+                }
+                else if (bytes + b <= s->batch_budget && slot_reserve(free_slot, free_slot->n + 1) == 0)
+                {
+                    slot_t *sl = free_slot;
+                    const int j = sl->n;
+                    res_entry *e = r->priv == (void *)&g_not_resident ? NULL : (res_entry *)r->priv;
+                    if (e && !e->d && res_alloc(s, e) != 0)
+                        s->stats.not_resident++; /* runs, but its series will not be resident */
+                    sl->req[j] = r;
+                    sl->N[j] = r->N;
+                    sl->L[j] = r->L;
+                    sl->k[j] = r->k;
+                    sl->seeds[j] = r->seed;
+                    sl->lrf_dst[j] = e ? e->d : NULL;
+                    sl->res[j] = e;
+                    sl->n++;
+                    bytes += b;
+                    keep = 0;
+                }
+            }
+        }
+        else
+        {
+            finish_request(s, r, -1);
+            keep = 0;
+            progressed = 1;
+        }
+        if (keep)
+            s->pend[kept++] = r;
+    }
+    s->npend = kept;
+    if (f && f->n > 0)
+    {
+        if (fs_launch(s) != 0)
+            fs_finish(s, 0);
+        progressed = 1;
+    }
+    if (free_slot && free_slot->n > 0)
+    {
+        free_slot->bytes = bytes;
+        if (slot_launch(s, free_slot) != 0)
+            slot_finish(s, free_slot, 0);
+        progressed = 1;
+    }
+    return progressed;
+}
+
+static int any_busy(const ssa_server *s)
+{
+    if (s->fs.busy)
+        return 1;
+    for (int i = 0; i < s->nslots; i++)
+        if (s->slots[i].busy)
+            return 1;
+    return 0;
+}
+
+static void *worker(void *arg)
+{
+    ssa_server *s = (ssa_server *)arg;
+    cudaSetDevice(s->device);
+    for (;;)
+    {
+        int progressed = poll_done(s);
+        take_queue(s);
+        progressed |= dispatch(s);
+        if (progressed)
+            continue;
+        pthread_mutex_lock(&s->mu);
+        if (s->stop && s->qcount == 0 && s->npend == 0 && !any_busy(s))
+        {
+            pthread_mutex_unlock(&s->mu);
+            break;
+        }
+        if (s->qcount == 0)
+        {
+            if (any_busy(s) || s->npend > 0)
+            {
+                /* device work in flight (or requests waiting on it): poll again shortly */
+                struct timespec ts;
+                clock_gettime(CLOCK_REALTIME, &ts);
+                ts.tv_nsec += 20000;
+                if (ts.tv_nsec >= 1000000000L)
+                {
+                    ts.tv_sec++;
+                    ts.tv_nsec -= 1000000000L;
+                }
+                pthread_cond_timedwait(&s->cv, &s->mu, &ts);
+            }
+            else if (!s->stop)
+            {
+                pthread_cond_wait(&s->cv, &s->mu);
+            }
+        }
+        pthread_mutex_unlock(&s->mu);
+    }
+    return NULL;
+}
+
+/* ---- public API ---------------------------------------------------------------------------- */
+
+int ssa_server_create(ssa_server **out, size_t hbm_budget_bytes, int max_inflight, int max_batch, int oversampling,
+                      int power_iters)
+{
+    if (!out || max_inflight < 1 || max_inflight > 16 || max_batch < 1 || power_iters < 0)
+        return -1;
+    *out = NULL;
+    ssa_server *s = (ssa_server *)calloc(1, sizeof(*s));
+    if (!s)
+        return -1;
+    s->p = oversampling <= 0 ? 8 : oversampling;
+    s->q_iters = power_iters;
+    s->max_batch = max_batch;
+    if (cudaGetDevice(&s->device) != cudaSuccess || ssad_init_device() != 0)
+    {
+        free(s);
+        return -1;
+    }
+    if (hbm_budget_bytes == 0)
+    {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess)
+        {
+            free(s);
+            return -1;
+        }
+        hbm_budget_bytes = fr / 10 * 8;
+    }
+    s->budget = hbm_budget_bytes;
+    s->res_budget = hbm_budget_bytes / 4;
+    s->batch_budget = (hbm_budget_bytes - s->res_budget) / (size_t)max_inflight;
+    s->hcap = 65521;
+    s->htab = (res_entry **)calloc((size_t)s->hcap, sizeof(res_entry *));
+    s->qcap = 1 << 16;
+    s->q = (ssa_request **)malloc(sizeof(ssa_request *) * s->qcap);
+    s->nslots = max_inflight;
+    s->slots = (slot_t *)calloc((size_t)max_inflight, sizeof(slot_t));
+    if (!s->htab || !s->q || !s->slots)
+    {
+        ssa_server_destroy(s);
+        return -1;
+    }
+    pthread_mutex_init(&s->mu, NULL);
+    pthread_cond_init(&s->cv, NULL);
+    pthread_cond_init(&s->cv_done, NULL);
+    for (int i = 0; i < max_inflight; i++)
+    {
+        slot_t *sl = &s->slots[i];
+        if (ssa_rbatch_create(&sl->rb, s->p, power_iters, g_group_idx, g_group_sizes, SRV_GROUPS) != 0 ||
+            ssar_set_lrf_group(sl->rb, 2, g_fc_group, 3) != 0 ||
+            cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming) != cudaSuccess)
+        {
+            ssa_server_destroy(s);
+            return -1;
+        }
+    }
+    if (cudaStreamCreateWithFlags(&s->fs.st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->fs.done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->pool_st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_pool, cudaEventDisableTiming) != cudaSuccess)
+    {
+        ssa_server_destroy(s);
+        return -1;
+    }
+    {
+        /* keep freed resident blocks cached in the pool instead of returning them to the driver */
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess)
+        {
+            unsigned long long thr = (unsigned long long)s->res_budget;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+    }
+    if (pthread_create(&s->th, NULL, worker, s) != 0)
+    {
+        ssa_server_destroy(s);
+        return -1;
+    }
+    s->th_live = 1;
+    *out = s;
+    return 0;
+}
+
+int ssa_server_submit(ssa_server *s, ssa_request *r)
+{
+    if (!s || !r)
+        return -1;
+    r->status = 1; /* in progress */
+    r->k_out = 0;
+    r->priv = NULL;
+    r->t_done = 0.0;
+    r->t_arrival = ssa_server_now();
+    pthread_mutex_lock(&s->mu);
+    if (s->qcount == s->qcap || s->stop)
+    {
+        pthread_mutex_unlock(&s->mu);
+        r->status = -1;
+        return -1;
+    }
+    s->q[(s->qhead + s->qcount) % s->qcap] = r;
+    s->qcount++;
+    s->outstanding++;
+    s->stats.submitted++;
+    pthread_cond_signal(&s->cv);
+    pthread_mutex_unlock(&s->mu);
+    return 0;
+}
+
+int ssa_server_drain(ssa_server *s)
+{
+    if (!s)
+        return -1;
+    pthread_mutex_lock(&s->mu);
+    while (s->outstanding > 0)
+        pthread_cond_wait(&s->cv_done, &s->mu);
+    pthread_mutex_unlock(&s->mu);
+    return 0;
+}
+
+int ssa_server_replay(ssa_server *s, ssa_request *reqs, const double *arrival_s, int n)
+{
+    if (!s || !reqs || !arrival_s || n < 0)
+        return -1;
+    const double t0 = ssa_server_now();
+    int rc = 0;
+    for (int i = 0; i < n; i++)
+    {
+        const double due = t0 + arrival_s[i];
+        for (;;)
+        {
+            const double now = ssa_server_now();
+            if (now >= due)
+                break;
+            const double d = due - now;
+            if (d > 200e-6)
+            {
+                struct timespec ts = {0, (long)((d - 100e-6) * 1e9)};
+                nanosleep(&ts, NULL);
+            }
+        }
+        if (ssa_server_submit(s, &reqs[i]) != 0)
+            rc = -1;
+    }
+    ssa_server_drain(s);
+    return rc;
+}
+
+int ssa_server_stats_get(ssa_server *s, ssa_server_stats *st)
+{
+    if (!s || !st)
+        return -1;
+    pthread_mutex_lock(&s->mu);
+    *st = s->stats;
+    st->resident_bytes = s->res_bytes;
+    st->resident_budget = s->res_budget;
+    st->batch_budget = s->batch_budget;
+    pthread_mutex_unlock(&s->mu);
+    return 0;
+}
+
+void ssa_server_destroy(ssa_server *s)
+{
+    if (!s)
+        return;
+    if (s->th_live)
+    {
+        ssa_server_drain(s);
+        pthread_mutex_lock(&s->mu);
+        s->stop = 1;
+        pthread_cond_broadcast(&s->cv);
+        pthread_mutex_unlock(&s->mu);
+        pthread_join(s->th, NULL);
+        pthread_mutex_destroy(&s->mu);
+        pthread_cond_destroy(&s->cv);
+        pthread_cond_destroy(&s->cv_done);
+    }
+    cudaDeviceSynchronize();
+    for (int i = 0; s->slots && i < s->nslots; i++)
+    {
+        slot_t *sl = &s->slots[i];
+        if (sl->rb)
+            ssa_rbatch_destroy(sl->rb);
+        if (sl->done)
+            cudaEventDestroy(sl->done);
+        void *hp[] = {sl->h_x, sl->h_sig, sl->h_W, sl->h_grp, sl->h_st, sl->h_lst};
+        for (size_t j = 0; j < sizeof(hp) / sizeof(hp[0]); j++)
+            if (hp[j])
+                cudaFreeHost(hp[j]);
+        if (sl->d_x)
+            cudaFree(sl->d_x);
+        free(sl->req);
+        free(sl->N);
+        free(sl->L);
+        free(sl->k);
+        free(sl->seeds);
+        free(sl->lrf_dst);
+        free(sl->res);
+    }
+    free(s->slots);
+    if (s->htab)
+    {
+        while (s->lru_head)
+            res_remove(s, s->lru_head);
+        free(s->htab);
+    }
+    if (s->pool_st)
+    {
+        cudaStreamSynchronize(s->pool_st);
+        cudaStreamDestroy(s->pool_st);
+    }
+    if (s->ev_pool)
+        cudaEventDestroy(s->ev_pool);
+    if (s->fs.st)
+        cudaStreamDestroy(s->fs.st);
+    if (s->fs.done)
+        cudaEventDestroy(s->fs.done);
+    if (s->fs.h_jobs)
+        cudaFreeHost(s->fs.h_jobs);
+    if (s->fs.d_jobs)
+        cudaFree(s->fs.d_jobs);
+    if (s->fs.h_out)
+        cudaFreeHost(s->fs.h_out);
+    if (s->fs.d_out)
+        cudaFree(s->fs.d_out);
+    free(s->fs.req);
+    free(s->fs.res);
+    free(s->pend);
+    free(s->q);
+    free(s);
+}

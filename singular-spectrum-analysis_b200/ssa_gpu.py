@@ -657,3 +657,146 @@ class SSARaggedBatch:
         if _lib.ssa_rbatch_device_results(self._h, ctypes.byref(r)) != 0:
             raise RuntimeError("ssa_rbatch_device_results failed")
         return {"sigma": r.sigma, "W": r.W, "groups": r.groups, "status": r.status, "stream": r.stream}
+
+
+class _Request(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("series_id", ctypes.c_int), ("N", ctypes.c_int), ("L", ctypes.c_int),
+                ("k", ctypes.c_int), ("h", ctypes.c_int), ("x", c_double_p), ("seed", ctypes.c_uint64),
+                ("sigma", c_double_p), ("groups", c_double_p), ("W", c_double_p), ("forecast", c_double_p),
+                ("status", ctypes.c_int), ("k_out", ctypes.c_int), ("t_arrival", ctypes.c_double),
+                ("t_done", ctypes.c_double), ("priv", ctypes.c_void_p)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_longlong) for n in ("submitted", "completed", "failed", "batches", "decompositions",
+                                                  "max_batch", "forecast_batches", "forecasts", "evictions",
+                                                  "not_resident")] + \
+               [(n, ctypes.c_size_t) for n in ("resident_bytes", "resident_budget", "batch_budget")]
+
+
+_sig("ssa_server_create", _I, ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t, _I, _I, _I, _I)
+_sig("ssa_server_destroy", _V, ctypes.c_void_p)
+_sig("ssa_server_submit", _I, ctypes.c_void_p, ctypes.POINTER(_Request))
+_sig("ssa_server_drain", _I, ctypes.c_void_p)
+_sig("ssa_server_replay", _I, ctypes.c_void_p, ctypes.POINTER(_Request), c_double_p, _I)
+_sig("ssa_server_stats_get", _I, ctypes.c_void_p, ctypes.POINTER(_ServerStats))
+_sig("ssa_server_now", _D)
+
+REQ_DECOMPOSE_RECON, REQ_DECOMPOSE_WCORR, REQ_FORECAST = 0, 1, 2
+
+
+class Requests:
+    """A block of requests for SSAServer (ssa_request array) with their host buffers.
+
+    ``add_decompose(x, L, k, series_id, seed, wcorr=False)`` and ``add_forecast(series_id, h)``
+    append requests; after the server has completed them, ``result(i)`` returns a dict of the
+    outputs, ``status`` and the latency in seconds."""
+
+    def __init__(self, capacity: int, keep_outputs: bool = True):
+        self.arr = (_Request * max(1, capacity))()
+        self.n = 0
+        self.keep_outputs = keep_outputs
+        self._bufs = []
+
+    def _next(self):
+        if self.n >= len(self.arr):
+            raise IndexError("request block is full")
+        r = self.arr[self.n]
+        self.n += 1
+        return r
+
+    def add_decompose(self, x: np.ndarray, L: int, k: int, series_id: int = 0, seed: int = 0,
+                      wcorr: bool = False) -> int:
+        r = self._next()
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        N = len(x)
+        r.type = REQ_DECOMPOSE_WCORR if wcorr else REQ_DECOMPOSE_RECON
+        r.series_id, r.N, r.L, r.k, r.seed = series_id, N, L, k, seed
+        r.x = _dp(x)
+        bufs = {"x": x}
+        if self.keep_outputs:
+            ke = max(1, min(k, L, N - L + 1))
+            bufs["sigma"] = np.zeros(ke)
+            r.sigma = _dp(bufs["sigma"])
+            if wcorr:
+                bufs["W"] = np.zeros((ke, ke))
+                r.W = _dp(bufs["W"])
+            else:
+                bufs["groups"] = np.zeros((2, N))
+                r.groups = _dp(bufs["groups"])
+        self._bufs.append(bufs)
+        return self.n - 1
+
+    def add_forecast(self, series_id: int, h: int) -> int:
+        r = self._next()
+        r.type = REQ_FORECAST
+        r.series_id, r.h = series_id, h
+        bufs = {}
+        if self.keep_outputs:
+            bufs["forecast"] = np.zeros(h)
+            r.forecast = _dp(bufs["forecast"])
+        self._bufs.append(bufs)
+        return self.n - 1
+
+    def result(self, i: int) -> dict:
+        r = self.arr[i]
+        out = {k: v for k, v in self._bufs[i].items() if k != "x"}
+        if "sigma" in out:
+            out["sigma"] = out["sigma"][:r.k_out] if r.k_out else out["sigma"][:0]
+        out["status"] = r.status
+        out["latency"] = r.t_done - r.t_arrival
+        return out
+
+    def latencies(self) -> np.ndarray:
+        return np.array([self.arr[i].t_done - self.arr[i].t_arrival for i in range(self.n)])
+
+    def statuses(self) -> np.ndarray:
+        return np.array([self.arr[i].status for i in range(self.n)])
+
+    def times(self) -> tuple[np.ndarray, np.ndarray]:
+        return (np.array([self.arr[i].t_arrival for i in range(self.n)]),
+                np.array([self.arr[i].t_done for i in range(self.n)]))
+
+
+class SSAServer:
+    """Continuous-batching request server (ssa_server_* C ABI)."""
+
+    def __init__(self, hbm_budget_bytes: int = 0, max_inflight: int = 3, max_batch: int = 4096,
+                 oversampling: int = 10, power_iters: int = 2):
+        self._h = ctypes.c_void_p()
+        if _lib.ssa_server_create(ctypes.byref(self._h), hbm_budget_bytes, max_inflight, max_batch, oversampling,
+                                  power_iters) != 0:
+            raise ValueError("ssa_server_create failed")
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.ssa_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, reqs: Requests, i: int) -> None:
+        if _lib.ssa_server_submit(self._h, ctypes.byref(reqs.arr[i])) != 0:
+            raise RuntimeError("ssa_server_submit failed")
+
+    def drain(self) -> None:
+        _lib.ssa_server_drain(self._h)
+
+    def run(self, reqs: Requests, arrivals: Optional[np.ndarray] = None) -> None:
+        """Submit every request of the block at its arrival offset (seconds; all at once when
+        None) and wait until all have completed."""
+        arr = np.zeros(reqs.n) if arrivals is None else np.ascontiguousarray(arrivals, dtype=np.float64)
+        if len(arr) != reqs.n:
+            raise ValueError("one arrival time per request")
+        if _lib.ssa_server_replay(self._h, reqs.arr, _dp(arr), reqs.n) != 0:
+            raise RuntimeError("ssa_server_replay failed")
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        _lib.ssa_server_stats_get(self._h, ctypes.byref(st))
+        return {n: getattr(st, n) for n, _ in _ServerStats._fields_}
+
+
+def server_now() -> float:
+    return float(_lib.ssa_server_now())

@@ -176,7 +176,7 @@ def test_api_errors(gpu, oracle):
     with pytest.raises(ValueError):
         gpu.SSA(x, 1000)
     with pytest.raises(ValueError):
-        gpu.SSA(np.zeros(40000), 100)  # longer than one CTA's FFT (N <= 32768)
+        gpu.SSA(np.zeros(140000), 100)  # beyond the largest FFT length (N <= 131072)
     s = gpu.SSA(x, 250)
     with pytest.raises(RuntimeError):
         s.reconstruct([0])

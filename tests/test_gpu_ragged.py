@@ -123,7 +123,7 @@ def test_uneven_batch_rejects_bad_series(gpu, oracle):
     with pytest.raises(RuntimeError):
         rb.run([x], [100], [5])  # L > N - 1
     with pytest.raises(RuntimeError):
-        rb.run([np.zeros(40000)], [100], [5])  # beyond the largest FFT length
+        rb.run([np.zeros(140000)], [100], [5])  # beyond the largest FFT length
     s, W, G = rb.run([x, x[:50]], [25, 10], [4, 3])  # still usable afterwards
     assert len(s[0]) == 4 and len(s[1]) == 3
 
