@@ -1,16 +1,20 @@
-"""Throughput benchmark of the B200 SSA hot path.
+"""Throughput and latency benchmark of the B200 SSA hot path on the mixed-N serving stream.
 
-Workload (default): the uniform batch — B = 4096 independent series, N = 10000, L = 2500,
-k = 50, oversampling p = 10, q = 2 power iterations; per series: randomized decomposition
-(device-generated Gaussian test matrix), all k elementary reconstructions, the k x k
-W-correlation matrix and the reconstructions of groups [0] and [1, 2]. One step = one pass of
-that pipeline over the whole batch. Signals: seeded synthetic trend + two sinusoids (periods
-U[6, 200], amplitudes U(0.5, 3)) + Gaussian noise at SNR U(0, 15) dB.
+Workload (default): requests with N log-uniform in [500, 100000], L = round(N/4), k uniform in
+{10..50}, oversampling p = 10, q = 2 power iterations; 50 % decompose + reconstruct groups [0] and
+[1, 2] (the series then stays resident), 30 % R-forecast of 50 steps on an already-resident series,
+20 % decompose + W-correlation. Signals: seeded random-walk trend + 1-3 sinusoids + Gaussian noise
+at SNR U(0, 15) dB (the uneven-batch generator). One SSA = one served request.
 
-Output: one JSON line (rank 0). `value` = series per second over all ranks with inputs
-resident in HBM (inputs of 328 MB per GPU are larger than L2, so no flush is needed);
-`e2e` = the same through the host-buffer C ABI (ssa_batch_run: pinned host input -> device ->
-pinned host outputs). `--impl reference` times the reference's CPU implementation instead.
+Output: one JSON line (rank 0).
+  value  series/s of the uneven-batch pipeline over the stream's decompositions with inputs
+         resident in HBM (CUDA events on the batch's stream; inputs larger than L2);
+  e2e    requests/s of the request server (ssa_server_*, host buffers, H2D and D2H inside) with the
+         whole stream offered at once;
+  latency_ms  p50 / p99 arrival-to-result latency at Poisson arrival rates 1k-50k requests/s;
+  plain_gpu_path  the same stream one request per call through the reference-compatible API;
+  cpu_baseline    the reference's CPU implementation on a bounded sample of the stream.
+`--impl reference` times the reference's CPU implementation instead.
 """
 from __future__ import annotations
 
@@ -45,30 +49,93 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--batch", type=int, default=4096)
-    ap.add_argument("--N", type=int, default=10000)
-    ap.add_argument("--L", type=int, default=2500)
-    ap.add_argument("--k", type=int, default=50)
+    ap.add_argument("--batch", type=int, default=2048, help="series per device step")
+    ap.add_argument("--requests", type=int, default=4096, help="stream length for the saturated server run")
+    ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")
+    ap.add_argument("--nmin", type=int, default=500)
+    ap.add_argument("--nmax", type=int, default=100000)
     ap.add_argument("--p", type=int, default=10)
     ap.add_argument("--q", type=int, default=2)
-    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-uniform", action="store_true")
+    ap.add_argument("--no-rates", action="store_true")
     return ap.parse_args()
 
 
 def workload_config(a) -> dict:
-    return {"workload": f"uniform batch: {a.batch} series x N={a.N}, L={a.L}, k={a.k}, p={a.p}, q={a.q}; "
-                        "decompose + all k elementary reconstructions + W-correlation + groups [0],[1,2]",
-            "series_per_gpu": a.batch, "N": a.N, "L": a.L, "k": a.k, "oversampling": a.p, "power_iters": a.q,
-            "l2": "inputs larger than L2 (B x N doubles per GPU)", "parallelism": "series sharded per GPU, no collective"}
+    return {"workload": f"mixed-N serving stream: N log-uniform [{a.nmin}, {a.nmax}], L = N/4, k ~ U{{10..50}}, "
+                        f"p = {a.p}, q = {a.q}; 50% decompose + reconstruct [0],[1,2] (series stays resident), "
+                        "30% R-forecast 50 steps on a resident series, 20% decompose + W-correlation",
+            "series_per_step": a.batch, "stream_requests": a.requests, "oversampling": a.p, "power_iters": a.q,
+            "rates_per_s": [int(r) for r in a.rates.split(",")], "seed": a.seed,
+            "l2": "inputs larger than L2 (packed signals of a step: ~300 MB)",
+            "parallelism": "series sharded per GPU, no collective"}
 
 
-def make_signals(B: int, N: int, seed: int) -> np.ndarray:
+# ------------------------------------------------------------------------------------------
+# the stream
+# ------------------------------------------------------------------------------------------
+
+RECON, WCORR, FORECAST = 0, 1, 2
+
+
+def make_series(rng: np.random.Generator, nmin: int, nmax: int):
     import ssa_oracle
 
-    return ssa_oracle.config2_batch(B, seed=seed, N=N)
+    N = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
+    L = max(2, int(round(N / 4)))
+    k = int(rng.integers(10, 51))
+    return ssa_oracle.walk_sines(rng, N), L, k
+
+
+def make_stream(n: int, seed: int, nmin: int, nmax: int) -> list:
+    """Request specs: (type, x, L, k, target) in arrival order; a forecast names the index of an
+    earlier decompose + reconstruct request."""
+    rng = np.random.default_rng(seed)
+    out, recon_idx = [], []
+    for i in range(n):
+        u = rng.random()
+        t = RECON if u < 0.5 else (FORECAST if u < 0.8 else WCORR)
+        if t == FORECAST and not recon_idx:
+            t = RECON
+        if t == FORECAST:
+            out.append((FORECAST, None, 0, 0, recon_idx[int(rng.integers(0, len(recon_idx)))]))
+        else:
+            x, L, k = make_series(rng, nmin, nmax)
+            out.append((t, x, L, k, -1))
+            if t == RECON:
+                recon_idx.append(i)
+    return out
+
+
+def stream_requests(gpu, specs, id_base: int, keep_outputs: bool = True, pinned: bool = True):
+    """Request block for the server; inputs and outputs in page-locked host memory. Returns the
+    block and the bytes it moves host -> device and device -> host."""
+    R = gpu.Requests(len(specs), keep_outputs=keep_outputs, pinned=pinned)
+    h2d = d2h = 0
+    for i, (t, x, L, k, tgt) in enumerate(specs):
+        if t == FORECAST:
+            R.add_forecast(id_base + tgt, 50)
+            d2h += 8 * 50 if keep_outputs else 0
+        else:
+            R.add_decompose(x, L, k, series_id=id_base + i, seed=id_base + i, wcorr=(t == WCORR))
+            N = len(x)
+            ke = min(k, L, N - L + 1)
+            h2d += 8 * N
+            if keep_outputs:
+                d2h += 8 * (ke + (ke * ke if t == WCORR else 2 * N))
+    return R, h2d, d2h
+
+
+def corr_bytes(N: int, L: int, k: int, p: int, q: int) -> int:
+    """Algorithmic FP32 bytes of the correlation sweeps of one series: the generated first sweep
+    writes Y (L x kp); every other sweep reads one block and writes the other."""
+    K = N - L + 1
+    kp = min(k + p, L, K)
+    return 4 * kp * (L + (2 * q + 1) * (L + K))
 
 
 # ------------------------------------------------------------------------------------------
@@ -114,33 +181,36 @@ def _port_worker(args):
     return time.perf_counter() - t0
 
 
-def cpu_reference(a, budget_s: float = 20.0, series: int | None = None) -> dict:
-    """Time the reference CPU path on a bounded sample: one series per process on every host
-    core. Returns {"value" (series/s), "cores", "kind", "sample"}."""
+def cpu_reference(a, budget_s: float = 20.0) -> dict:
+    """Time the reference CPU path on a bounded sample of the stream's decompositions: one series
+    per process on every host core, as many series as fit the budget. Forecast requests are
+    counted at no cost, so requests/s = decompositions/s / 0.7 (the stream's decomposition
+    share). Returns {"value", "unit", "cores", "kind", "sample"}."""
     cores = len(os.sched_getaffinity(0))
     use_ref = (ORACLE / "_ref" / "libssa_ref.so").exists()
-    X = make_signals(max(cores, 1) * 64, a.N, a.seed + 1000)
+    rng = np.random.default_rng(a.seed + 1000)
     ctx = mp.get_context("spawn")
+    done = 0
+    nsum = 0
     with ctx.Pool(cores, initializer=_pin_blas) as pool:
-        # one calibration series per core, then as many rounds as fit the budget
-        if use_ref:
-            t = pool.map(_ref_worker, [(X[i], a.L, a.k, a.p) for i in range(cores)])
-        else:
-            t = pool.map(_port_worker, [(X[i], a.L, a.k, a.p, a.q) for i in range(cores)])
-        per = max(statistics.median(t), 1e-6)
-        rounds = max(1, int(budget_s / per)) if series is None else max(1, math.ceil(series / cores))
-        n = min(rounds * cores, len(X))
         t0 = time.perf_counter()
-        if use_ref:
-            pool.map(_ref_worker, [(X[i], a.L, a.k, a.p) for i in range(n)])
-        else:
-            pool.map(_port_worker, [(X[i], a.L, a.k, a.p, a.q) for i in range(n)])
+        while True:
+            batch = [make_series(rng, a.nmin, a.nmax) for _ in range(cores)]
+            if use_ref:
+                pool.map(_ref_worker, [(x, L, k, a.p) for x, L, k in batch])
+            else:
+                pool.map(_port_worker, [(x, L, k, a.p, a.q) for x, L, k in batch])
+            done += len(batch)
+            nsum += sum(len(b[0]) for b in batch)
+            if time.perf_counter() - t0 >= budget_s:
+                break
         el = time.perf_counter() - t0
     kind = "reference" if use_ref else "port"
-    what = ("MKL/ssa_opt_ref.h (reference pure-C path: randomized SVD q=0, reconstruct, W-corr)" if use_ref
-            else "NumPy FP64 port of MKL/ssa_opt.h randomized SVD (q as configured), reconstruct, W-corr")
-    return {"value": n / el, "unit": "SSA/s", "cores": cores, "kind": kind,
-            "sample": f"{n} series of N={a.N}, L={a.L}, k={a.k}, p={a.p}, one per process on {cores} cores; {what}"}
+    what = ("MKL/ssa_opt_ref.h (reference pure-C path: randomized SVD q=0, reconstruct [0],[1,2], W-corr)"
+            if use_ref else "NumPy FP64 port of MKL/ssa_opt.h randomized SVD, reconstruct, W-corr")
+    return {"value": done / el / 0.7, "unit": "SSA/s", "cores": cores, "kind": kind,
+            "sample": f"{done} stream decompositions (mean N {nsum / max(done, 1):.0f}) in {el:.1f} s, one per "
+                      f"process on {cores} cores, forecasts counted at no cost; {what}"}
 
 
 def _pin_blas():
@@ -210,12 +280,178 @@ def measured_peak_hbm() -> tuple[float, str]:
 # main
 # ------------------------------------------------------------------------------------------
 
+def device_steps(gpu, torch, a, rank: int, world: int) -> dict:
+    """Uneven-batch pipeline over `a.batch` stream decompositions with inputs resident in HBM."""
+    rng = np.random.default_rng(a.seed + 7919 * (rank + 1))
+    series = [make_series(rng, a.nmin, a.nmax) for _ in range(a.batch)]
+    Ns = [len(x) for x, _, _ in series]
+    Ls = [L for _, L, _ in series]
+    ks = [k for _, _, k in series]
+    d_x = torch.from_numpy(np.concatenate([x for x, _, _ in series])).to("cuda")
+    rb = gpu.SSARaggedBatch(oversampling=a.p, power_iters=a.q, groups=[[0], [1, 2]])
+    stream = torch.cuda.ExternalStream(rb.device_results()["stream"])
+    for w in range(a.warmup):
+        rb.run_device(d_x.data_ptr(), Ns, Ls, ks, seed=1000 + w)
+        rb.sync()
+    rb.set_profiling(True)
+    rb.profile()  # discard the warm-up stages
+    launches0 = gpu.kernel_launches()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ev[0].record(stream)
+        for i in range(a.steps):
+            rb.run_device(d_x.data_ptr(), Ns, Ls, ks, seed=i)
+            ev[i + 1].record(stream)
+        torch.cuda.synchronize()
+        rb.sync()
+    launches = gpu.kernel_launches() - launches0
+    prof = rb.profile()
+    rb.set_profiling(False)
+    step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(a.steps)]
+    total_ms = ev[0].elapsed_time(ev[a.steps])
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    cb = sum(corr_bytes(N, L, k, a.p, a.q) for N, L, k in zip(Ns, Ls, ks))
+    corr_ms, corr_n = prof["corr"]
+    peak, peak_kind = measured_peak_hbm()
+    per_launch = cb * a.steps / max(corr_n, 1)
+    avg_ms = corr_ms / max(corr_n, 1)
+    achieved = per_launch / (avg_ms / 1e3) / 1e9
+    tot = max(sum(v[0] for v in prof.values()), 1e-9)
+    out = {"value": a.batch * a.steps * world / (total_ms / 1e3), "ms_per_step": total_ms / a.steps,
+           "step_ms": step_ms, "launches": launches,
+           "share": {kk: round(v[0] / tot, 4) for kk, v in prof.items() if v[1]},
+           "mean_N": float(np.mean(Ns)), "clocks": clk.summary(),
+           "roofline": {"bound": "hbm", "kernel": "k_corr / k_cl_col<CL_CORR> (FFT correlation matvec sweeps)",
+                        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_source": peak_kind, "traffic": None,
+                        "avg_launch_ms": avg_ms, "algorithmic_bytes_per_launch": per_launch,
+                        "note": "launch times summed over FFT-length buckets that overlap on separate streams "
+                                "(conservative); traffic of the uniform batch's k_corr capture equals its "
+                                "algorithmic bytes within 2%"}}
+    del rb, d_x
+    torch.cuda.empty_cache()
+    return out
+
+
+def server_runs(gpu, torch, a, rank: int, world: int) -> dict:
+    """Saturated server run over the whole stream (e2e) and the latency sweep (rank 0)."""
+    specs = make_stream(a.requests, a.seed + 31 * rank, a.nmin, a.nmax)
+    srv = gpu.SSAServer(hbm_budget_bytes=150 * 10**9, max_inflight=3, max_batch=4096, oversampling=a.p,
+                        power_iters=a.q)
+    # warm-up: the whole stream once (every batch slot grows its device buffers to full size)
+    W, _, _ = stream_requests(gpu, specs, id_base=10**7)
+    for _ in range(2):
+        srv.run(W)
+    R, h2d, d2h = stream_requests(gpu, specs, id_base=2 * 10**7)
+    st0 = srv.stats()
+    srv.run(R)
+    st1 = srv.stats()
+    timed = {kk: st1[kk] - st0[kk] for kk in ("batches", "decompositions", "forecast_batches", "forecasts",
+                                                "host_launch_s", "host_finish_s")}
+    ta, td = R.times()
+    st = R.statuses()
+    el = float(td.max() - ta.min())
+    if world > 1:
+        t = torch.tensor([el], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        el = float(t.item())
+    out = {"e2e": {"value": len(specs) * world / el, "unit": "SSA/s", "h2d_bytes_per_step": h2d,
+                   "d2h_bytes_per_step": d2h, "requests": len(specs), "failed": int((st != 0).sum()),
+                   "seconds": el, "server_timed_run": timed,
+                   "what": "ssa_server_* C API, page-locked host buffers, the whole stream offered at t=0 (one "
+                           "step = the stream): H2D of every signal and D2H of every requested result (sigma, "
+                           "groups [0],[1,2] / W, forecasts) inside the timed region"}}
+    if rank == 0 and world == 1 and not a.no_rates:
+        sweep = {}
+        rng = np.random.default_rng(a.seed + 99)
+        for ri, rate in enumerate(int(r) for r in a.rates.split(",")):
+            n = min(len(specs), max(400, int(rate * 0.8)))
+            Rr, _, _ = stream_requests(gpu, specs[:n], id_base=(3 + ri) * 10**7)
+            arr = np.cumsum(rng.exponential(1.0 / rate, n))
+            srv.run(Rr, arr)
+            ta, td = Rr.times()
+            lat = (td - ta) * 1e3
+            ok = Rr.statuses() == 0
+            sweep[str(rate)] = {"requests": n, "achieved_per_s": n / float(td.max() - ta.min()),
+                                "p50_ms": float(np.percentile(lat[ok], 50)), "p99_ms": float(np.percentile(lat[ok], 99)),
+                                "failed": int((~ok).sum())}
+        sustained = [r for r, v in sweep.items() if v["achieved_per_s"] >= 0.9 * int(r)]
+        best = max(sustained, key=int) if sustained else min(sweep, key=int)
+        out["latency_ms"] = {"p50": sweep[best]["p50_ms"], "p99": sweep[best]["p99_ms"], "at_rate_per_s": int(best),
+                             "what": "arrival-to-result latency (host clock) at the highest swept Poisson rate the "
+                                     "server sustains (achieved >= 90% of offered)", "sweep": sweep}
+    srv.close()
+    return out
+
+
+def plain_path(gpu, a, n: int = 120) -> dict:
+    """The stream's first n requests one per call through the reference-compatible API."""
+    specs = make_stream(n, a.seed, a.nmin, a.nmax)
+    objs, lat, failed = {}, [], 0
+    t0 = time.perf_counter()
+    for i, (t, x, L, k, tgt) in enumerate(specs):
+        ts = time.perf_counter()
+        try:
+            if t == FORECAST:
+                objs[tgt].forecast([0, 1, 2], 50)
+            else:
+                s = gpu.SSA(x, L)
+                s.decompose(k, oversampling=a.p, power_iters=a.q)
+                if t == RECON:
+                    s.reconstruct([0])
+                    s.reconstruct([1, 2])
+                    objs[i] = s
+                else:
+                    s.wcorr_matrix()
+        except (RuntimeError, KeyError):
+            failed += 1
+        lat.append((time.perf_counter() - ts) * 1e3)
+    el = time.perf_counter() - t0
+    return {"value": n / el, "unit": "SSA/s", "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "failed": failed,
+            "what": f"first {n} requests of the stream, one per call (SSA() + decompose(q={a.q}) + reconstruct x2 "
+                    "/ wcorr_matrix / forecast on the kept context) through libssa.so's reference API, host wall clock"}
+
+
+def uniform_batch(gpu, torch, a, B: int = 4096, N: int = 10000, L: int = 2500, k: int = 50, steps: int = 3) -> dict:
+    """The uniform batch of identical series (4096 x N=10000), for comparison with earlier lines."""
+    import ssa_oracle
+
+    X = ssa_oracle.config2_batch(B, seed=1, N=N)
+    d_x = torch.from_numpy(X).to("cuda")
+    batch = gpu.SSABatch(B, N, L, k, oversampling=a.p, power_iters=a.q, groups=[[0], [1, 2]])
+    stream = torch.cuda.ExternalStream(batch.device_results()["stream"])
+    for w in range(3):
+        batch.run_device(d_x.data_ptr(), B, seed=1000 + w)
+        batch.sync()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(steps):
+        batch.run_device(d_x.data_ptr(), B, seed=i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    batch.sync()
+    ms = e0.elapsed_time(e1)
+    del batch, d_x
+    torch.cuda.empty_cache()
+    return {"value": B * steps / (ms / 1e3), "unit": "SSA/s", "ms_per_step": ms / steps,
+            "workload": f"{B} series x N={N}, L={L}, k={k}, p={a.p}, q={a.q}; decompose + all elementary "
+                        "reconstructions + W-correlation + groups [0],[1,2]; inputs resident in HBM"}
+
+
 def main():
     a = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    metric = "SSA/sec"
+    metric = "SSA/sec (mixed-N serving stream)"
     cfg = workload_config(a)
 
     if a.impl == "reference":
@@ -252,117 +488,25 @@ def main():
         ssa_build.build()
         import ssa_gpu
 
-    B, N = a.batch, a.N
-    X = make_signals(B, N, a.seed + 7919 * rank)
-    d_x = torch.from_numpy(X).to("cuda")
-    batch = ssa_gpu.SSABatch(B, N, a.L, a.k, oversampling=a.p, power_iters=a.q, groups=[[0], [1, 2]])
-    res = batch.device_results()
-    stream = torch.cuda.ExternalStream(res["stream"])
-
-    for w in range(a.warmup):
-        batch.run_device(d_x.data_ptr(), B, seed=1000 + w)
-        batch.sync()
-
-    batch.set_profiling(True)
-    launches0 = ssa_gpu.kernel_launches()
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
-    with ClockSampler(torch.cuda.current_device()) as clk:
-        ev[0].record(stream)
-        for i in range(a.steps):
-            batch.run_device(d_x.data_ptr(), B, seed=i)
-            ev[i + 1].record(stream)
-        torch.cuda.synchronize()
-        batch.sync()
-    launches = ssa_gpu.kernel_launches() - launches0
-    prof = batch.profile()
-    batch.set_profiling(False)
-    step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(a.steps)]
-    total_ms = ev[0].elapsed_time(ev[a.steps])
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = B * a.steps * world / (total_ms / 1e3)
-
-    # roofline of the dominant kernel (the correlation matvec sweeps)
-    K = N - a.L + 1
-    kp = min(a.k + a.p, a.L, K)
-    corr_ms, corr_n = prof["corr"]
-    sweeps = 2 * a.q + 2  # Y = H Omega, q x (H^T Q, H Z), B = H^T Q
-    # algorithmic bytes of one sweep: every probe column read once (not for the generated
-    # Omega) and written once, FP32; H has N values per series.
-    fwd = kp * a.L * 4
-    adj = kp * K * 4
-    bytes_total = B * ((0 + fwd) + a.q * ((fwd + adj) + (adj + fwd)) + (fwd + adj))
-    per_launch_bytes = bytes_total / sweeps
-    avg_ms = corr_ms / max(corr_n, 1)
-    peak, peak_kind = measured_peak_hbm()
-    achieved = per_launch_bytes / (avg_ms / 1e3) / 1e9
-    dominant = max(prof.items(), key=lambda kv: kv[1][0])
-    # DRAM bytes per k_corr launch from the ncu capture of the 512-series case of this shape
-    # (mean over one pipeline pass: 1057.2 MB per 512 series), scaled by the series count.
-    traffic = None
-    if (N, a.L, a.k, a.p, a.q) == (10000, 2500, 50, 10, 2):
-        traffic = 1057.2e6 / 512 * B
-    roofline = {"bound": "hbm", "kernel": "k_corr (FFT correlation matvec sweep)", "achieved": achieved,
-                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": traffic, "traffic_source": "ncu dram__bytes_read+write of a 512-series capture, scaled", "avg_launch_ms": avg_ms, "algorithmic_bytes_per_launch": per_launch_bytes,
-                "dominant_kernel_by_time": dominant[0]}
-    share = {k: round(v[0] / max(sum(x[0] for x in prof.values()), 1e-9), 4) for k, v in prof.items() if v[1]}
-
-    line = {"metric": metric, "value": value, "unit": "SSA/s", "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "fp32 (FP64 Gram/Cholesky/Rayleigh-Ritz)", "data": "synthetic",
-            "config": cfg, "latency_ms": {"p50": statistics.median(step_ms),
-                                          "p99": float(np.percentile(step_ms, 99)),
-                                          "what": "per-step (whole batch) device time"},
-            "gpu_launches": launches, "kernel_share": share, "roofline": roofline, "clocks": clk.summary()}
-
+    dev = device_steps(ssa_gpu, torch, a, rank, world)
+    line = {"metric": metric, "value": dev["value"], "unit": "SSA/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": dev["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32 (FP64 Gram/Cholesky/Rayleigh-Ritz/LRF)", "data": "synthetic",
+            "config": cfg, "gpu_launches": dev["launches"], "kernel_share": dev["share"],
+            "roofline": dev["roofline"], "clocks": dev["clocks"],
+            "value_what": f"series/s of the uneven-batch pipeline (ssa_rbatch_run_device) over {a.batch} stream "
+                          f"decompositions per step (mean N {dev['mean_N']:.0f}): decomposition, all elementary "
+                          "reconstructions, W-correlation, groups [0],[1,2]; inputs resident in HBM"}
     if not a.no_e2e:
-        xs = torch.from_numpy(X).pin_memory()
-        k = batch.k
-        sig = torch.empty((B, k), dtype=torch.float64).pin_memory()
-        W = torch.empty((B, k, k), dtype=torch.float64).pin_memory()
-        G = torch.empty((B, 2, N), dtype=torch.float64).pin_memory()
-        batch.run_host_ptrs(xs.data_ptr(), B, 77, sig.data_ptr(), W.data_ptr(), G.data_ptr())
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e2e_steps = max(1, min(a.steps, 3))
-        e0.record(stream)
-        for i in range(e2e_steps):
-            batch.run_host_ptrs(xs.data_ptr(), B, 77 + i, sig.data_ptr(), W.data_ptr(), G.data_ptr())
-        e1.record(stream)
-        torch.cuda.synchronize()
-        e_ms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([e_ms], device="cuda", dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e_ms = float(t.item())
-        line["e2e"] = {"value": B * e2e_steps * world / (e_ms / 1e3), "unit": "SSA/s",
-                       "h2d_bytes_per_step": B * N * 8, "d2h_bytes_per_step": B * (k + k * k + 2 * N) * 8,
-                       "what": "ssa_batch_run on pinned host buffers (H2D signals, D2H sigma, W, groups)"}
-
+        line.update(server_runs(ssa_gpu, torch, a, rank, world))
     if rank == 0 and world == 1 and not a.no_plain:
-        # plain drop-in path: one series per call through the reference-compatible C API
-        n = 16
-        Xp = X[:n]
-        t0 = time.perf_counter()
-        for i in range(n):
-            s = ssa_gpu.SSA(Xp[i], a.L)
-            s.decompose(a.k, oversampling=a.p, power_iters=a.q)
-            s.reconstruct([0])
-            s.reconstruct([1, 2])
-            s.wcorr_matrix()
-            del s
-        el = time.perf_counter() - t0
-        line["plain_gpu_path"] = {"value": n / el, "unit": "SSA/s",
-                                  "what": f"{n} series, one per call: SSA() + decompose(q={a.q}) + 2 reconstructs + "
-                                          "wcorr_matrix through libssa.so (host wall clock)"}
+        line["plain_gpu_path"] = plain_path(ssa_gpu, a)
+        if "e2e" in line:
+            line["e2e_over_plain"] = line["e2e"]["value"] / line["plain_gpu_path"]["value"]
+    if rank == 0 and world == 1 and not a.no_uniform:
+        line["uniform_batch"] = uniform_batch(ssa_gpu, torch, a)
     if rank == 0 and world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_reference(a, budget_s=20.0)
-
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

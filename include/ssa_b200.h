@@ -114,6 +114,9 @@ int ssa_rbatch_run(ssa_rbatch *b, int B, const int *N, const int *L, const int *
 int ssa_rbatch_run_device(ssa_rbatch *b, int B, const int *N, const int *L, const int *k, const double *d_x,
                           uint64_t seed);
 int ssa_rbatch_sync(ssa_rbatch *b);
+/* Every buffer of a run lives in one device arena, grown in stream order when a run needs more;
+ * reserving it up front keeps growth (and the driver allocation behind it) out of later runs. */
+int ssa_rbatch_reserve(ssa_rbatch *b, size_t bytes);
 int ssa_rbatch_layout(const ssa_rbatch *b, size_t *offsets, size_t *totals);
 /* Device pointers of the packed outputs and the stream every run ends on (recon is NULL). */
 int ssa_rbatch_device_results(const ssa_rbatch *b, ssa_batch_results *out);
@@ -172,9 +175,11 @@ typedef struct
     long long forecast_batches, forecasts;
     long long evictions, not_resident;
     size_t resident_bytes, resident_budget, batch_budget;
+    double host_launch_s, host_finish_s; /* worker time spent forming / completing batches */
 } ssa_server_stats;
 typedef struct ssa_server ssa_server;
-/* hbm_budget_bytes 0: 80 % of the free device memory at creation. */
+/* hbm_budget_bytes 0: 80 % of the free device memory at creation, device memory taken as batches
+ * need it; an explicit budget reserves every batch slot's device arena at creation. */
 int ssa_server_create(ssa_server **out, size_t hbm_budget_bytes, int max_inflight, int max_batch, int oversampling,
                       int power_iters);
 /* Waits for every submitted request, then stops the worker and frees everything. */
@@ -187,6 +192,12 @@ int ssa_server_drain(ssa_server *s);
 int ssa_server_replay(ssa_server *s, ssa_request *reqs, const double *arrival_s, int n);
 int ssa_server_stats_get(ssa_server *s, ssa_server_stats *st);
 double ssa_server_now(void);
+/* Page-locked host memory. Request inputs and outputs in page-locked memory are copied straight
+ * to and from the device; pageable ones go through a fixed staging area per batch slot (256 MB in,
+ * 512 MB out), which bounds how many of them one batch takes (a request whose pageable buffers
+ * alone exceed it fails). All output buffers of one request should be of the same kind. */
+void *ssa_host_alloc(size_t bytes);
+void ssa_host_free(void *p);
 
 /* Stage profiler of a batch: with profiling on, every kernel launch of ssa_batch_run* is
  * bracketed by CUDA events on the batch stream. ssa_batch_profile waits for the stream and

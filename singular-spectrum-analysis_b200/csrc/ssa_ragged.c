@@ -60,9 +60,10 @@ typedef struct
     long long ldS;
     int nb, cap_nb;
     rser *sd;
+    /* views into the batch's device arena for the current run */
     float *X, *Y, *Z, *R, *Zu, *Zv, *recon, *Us;
     double *part, *qsum, *norm2;
-    size_t cX, cY, cZ, cR, cZu, cZv, crecon, cUs, cpart, cqsum, cnorm;
+    size_t sz[11]; /* bytes of X, Y, Z, part, qsum, R, Zu, Zv, recon, norm2, Us for the run */
     cudaEvent_t done;
 } rbucket;
 
@@ -76,10 +77,11 @@ struct ssa_rbatch
     int prof;
     double *d_xs;
     size_t c_xs;
+    /* one device arena holds every bucket buffer and the packed outputs of a run */
+    char *arena;
+    size_t arena_cap;
     double *sigma, *W, *groups;
-    size_t c_sig, c_W, c_grp;
     int *status;
-    int c_status;
     int B;
     size_t n_x, n_sig, n_W, n_grp;
     size_t *h_off; /* 4 B offsets of the last run: x, sigma, W, groups */
@@ -89,7 +91,6 @@ struct ssa_rbatch
     int lrf_slot, n_lrf_group, lrf_gmax;
     int *d_lrf_group;
     int *lrf_status;
-    int c_lrf_status;
 };
 
 static int imin(int a, int b) { return a < b ? a : b; }
@@ -107,19 +108,49 @@ static int gram_rows(int m, int nb)
     return imax(rows, SSA_GRAM_CHUNK);
 }
 
-/* Grow a device buffer to at least `need` elements of `elem` bytes (contents not kept). */
-static int grow(void **p, size_t *cap, size_t need, size_t elem)
+/* The library's stream-ordered memory pool on the current device: freed blocks stay cached in
+ * it (release threshold at its maximum), so re-growing buffers costs no driver allocation. */
+cudaMemPool_t ssar_pool(void)
+{
+    static cudaMemPool_t pools[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return NULL;
+    if (!pools[dev])
+    {
+        struct cudaMemPoolProps props;
+        memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess)
+            return NULL;
+        unsigned long long thr = ~0ULL;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        pools[dev] = pool;
+    }
+    return pools[dev];
+}
+
+/* Grow a device buffer to at least `need` elements of `elem` bytes (contents not kept), in
+ * stream order on `st` (the stream that uses it), so that growing never waits for the device:
+ * cudaFree would synchronise every stream, including other batches in flight. */
+static int grow(void **p, size_t *cap, size_t need, size_t elem, cudaStream_t st)
 {
     if (need <= *cap && *p)
         return 0;
     if (*p)
-        cudaFree(*p);
+        cudaFreeAsync(*p, st);
     *p = NULL;
     *cap = 0;
     if (need == 0)
         return 0;
     size_t n = need + need / 8;
-    CK(cudaMalloc(p, n * elem));
+    cudaMemPool_t pool = ssar_pool();
+    if (!pool)
+        return (int)cudaErrorMemoryAllocation;
+    CK(cudaMallocFromPoolAsync(p, n * elem, pool, st));
     *cap = n;
     return 0;
 }
@@ -128,11 +159,7 @@ static void bucket_free(rbucket *b)
 {
     if (!b->live)
         return;
-    ssae_destroy(&b->e); /* stream, arena, profiler events */
-    void *bufs[] = {b->X, b->Y, b->Z, b->R, b->Zu, b->Zv, b->recon, b->Us, b->part, b->qsum, b->norm2};
-    for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
-        if (bufs[i])
-            cudaFree(bufs[i]);
+    ssae_destroy(&b->e); /* stream, job arena, profiler events */
     if (b->done)
         cudaEventDestroy(b->done);
     free(b->sd);
@@ -147,8 +174,7 @@ void ssa_rbatch_destroy(ssa_rbatch *rb)
         cudaStreamSynchronize(rb->main);
     for (int i = 0; i < RB_NB; i++)
         bucket_free(&rb->bk[i]);
-    void *bufs[] = {rb->d_gidx, rb->d_goff, rb->d_xs, rb->sigma, rb->W, rb->groups, rb->status, rb->lrf_status,
-                    rb->d_lrf_group};
+    void *bufs[] = {rb->d_gidx, rb->d_goff, rb->d_xs, rb->arena, rb->d_lrf_group};
     for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
         if (bufs[i])
             cudaFree(bufs[i]);
@@ -158,6 +184,10 @@ void ssa_rbatch_destroy(ssa_rbatch *rb)
         cudaStreamDestroy(rb->main);
     free(rb->h_off);
     free(rb);
+    /* hand the pool's cached blocks back to the driver (blocks in use elsewhere stay) */
+    cudaMemPool_t pool = ssar_pool();
+    if (pool)
+        cudaMemPoolTrimTo(pool, 0);
 }
 
 int ssa_rbatch_create(ssa_rbatch **out, int oversampling, int power_iters, const int *group_idx,
@@ -679,7 +709,27 @@ static int bucket_run(rbucket *b, ssa_rbatch *rb, const double *d_x, unsigned lo
     return 0;
 }
 
-/* Validate, assign series to buckets, compute every offset and size the buffers. */
+/* Device arena of at least `bytes` (stream-ordered on the main stream after the previous run). */
+int ssa_rbatch_reserve(ssa_rbatch *rb, size_t bytes)
+{
+    if (!rb)
+        return -1;
+    if (bytes <= rb->arena_cap)
+        return 0;
+    cudaMemPool_t pool = ssar_pool();
+    if (!pool)
+        return -1;
+    if (rb->arena)
+        cudaFreeAsync(rb->arena, rb->main);
+    rb->arena = NULL;
+    rb->arena_cap = 0;
+    if (cudaMallocFromPoolAsync((void **)&rb->arena, bytes, pool, rb->main) != cudaSuccess)
+        return -1;
+    rb->arena_cap = bytes;
+    return 0;
+}
+
+/* Validate, assign series to buckets, compute every offset and carve the buffers. */
 static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
 {
     for (int s = 0; s < B; s++)
@@ -789,48 +839,84 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
         /* one run pushes 13 + 6 q job tables of at most sizeof(ssa_col_job) bytes per series,
          * each 16-byte aligned */
         const size_t arena = ((size_t)b->nb * sizeof(ssa_col_job) + 16) * (size_t)(16 + 6 * rb->q) + (1 << 16);
-        int rc = ssae_grow_arena(&b->e, arena);
-        rc |= grow((void **)&b->X, &b->cX, (size_t)b->nb * b->ldS, sizeof(float));
-        rc |= grow((void **)&b->Y, &b->cY, oY, sizeof(float));
-        rc |= grow((void **)&b->Z, &b->cZ, oZ, sizeof(float));
-        rc |= grow((void **)&b->part, &b->cpart, opart, sizeof(double));
-        rc |= grow((void **)&b->qsum, &b->cqsum, oqsum, sizeof(double));
-        rc |= grow((void **)&b->R, &b->cR, oR, sizeof(float));
-        rc |= grow((void **)&b->Zu, &b->cZu, oZu, sizeof(float));
-        rc |= grow((void **)&b->Zv, &b->cZv, oZu, sizeof(float));
-        rc |= grow((void **)&b->recon, &b->crecon, orecon, sizeof(float));
-        rc |= grow((void **)&b->norm2, &b->cnorm, onorm, sizeof(double));
-        if (b->logh > SSA_ELEM2_MAX_LOGH)
-            rc |= grow((void **)&b->Us, &b->cUs, ospec, sizeof(float));
-        if (rc)
+        if (ssae_grow_arena(&b->e, arena) != 0)
             return -1;
+        b->sz[0] = (size_t)b->nb * b->ldS * sizeof(float); /* X */
+        b->sz[1] = oY * sizeof(float);
+        b->sz[2] = oZ * sizeof(float);
+        b->sz[3] = opart * sizeof(double);
+        b->sz[4] = oqsum * sizeof(double);
+        b->sz[5] = oR * sizeof(float);
+        b->sz[6] = oZu * sizeof(float);
+        b->sz[7] = oZu * sizeof(float);
+        b->sz[8] = orecon * sizeof(float);
+        b->sz[9] = onorm * sizeof(double);
+        b->sz[10] = b->logh > SSA_ELEM2_MAX_LOGH ? ospec * sizeof(float) : 0;
     }
-    int rc = 0;
-    rc |= grow((void **)&rb->sigma, &rb->c_sig, rb->n_sig, sizeof(double));
-    rc |= grow((void **)&rb->W, &rb->c_W, rb->n_W, sizeof(double));
-    if (rb->n_groups > 0)
-        rc |= grow((void **)&rb->groups, &rb->c_grp, rb->n_grp, sizeof(double));
-    if (B > rb->c_status)
+    /* carve the arena: every bucket's buffers, then the packed outputs and status words */
+    size_t need = 0;
+    for (int g = 0; g < RB_NB; g++)
+        if (rb->bk[g].nb)
+            for (int i = 0; i < 11; i++)
+                need += (rb->bk[g].sz[i] + 255) & ~(size_t)255;
+    const size_t tail[5] = {rb->n_sig * sizeof(double), rb->n_W * sizeof(double),
+                            rb->n_groups > 0 ? rb->n_grp * sizeof(double) : 0, (size_t)B * sizeof(int),
+                            (size_t)B * sizeof(int)};
+    for (int i = 0; i < 5; i++)
+        need += (tail[i] + 255) & ~(size_t)255;
+    if (need > rb->arena_cap && ssa_rbatch_reserve(rb, need + need / 8) != 0)
+        return -1;
+    size_t off = 0;
+#define RB_CARVE(ptr, bytes)                                  \
+    do                                                        \
+    {                                                         \
+        (ptr) = (void *)(rb->arena + off);                    \
+        off += ((size_t)(bytes) + 255) & ~(size_t)255;        \
+    } while (0)
+    for (int g = 0; g < RB_NB; g++)
     {
-        if (rb->status)
-            cudaFree(rb->status);
-        rb->status = NULL;
-        rb->c_status = 0;
-        if (cudaMalloc((void **)&rb->status, sizeof(int) * B) != cudaSuccess)
-            return -1;
-        rb->c_status = B;
+        rbucket *b = &rb->bk[g];
+        if (!b->nb)
+            continue;
+        void *v;
+        RB_CARVE(v, b->sz[0]);
+        b->X = (float *)v;
+        RB_CARVE(v, b->sz[1]);
+        b->Y = (float *)v;
+        RB_CARVE(v, b->sz[2]);
+        b->Z = (float *)v;
+        RB_CARVE(v, b->sz[3]);
+        b->part = (double *)v;
+        RB_CARVE(v, b->sz[4]);
+        b->qsum = (double *)v;
+        RB_CARVE(v, b->sz[5]);
+        b->R = (float *)v;
+        RB_CARVE(v, b->sz[6]);
+        b->Zu = (float *)v;
+        RB_CARVE(v, b->sz[7]);
+        b->Zv = (float *)v;
+        RB_CARVE(v, b->sz[8]);
+        b->recon = (float *)v;
+        RB_CARVE(v, b->sz[9]);
+        b->norm2 = (double *)v;
+        RB_CARVE(v, b->sz[10]);
+        b->Us = b->sz[10] ? (float *)v : NULL;
     }
-    if (B > rb->c_lrf_status)
     {
-        if (rb->lrf_status)
-            cudaFree(rb->lrf_status);
-        rb->lrf_status = NULL;
-        rb->c_lrf_status = 0;
-        if (cudaMalloc((void **)&rb->lrf_status, sizeof(int) * B) != cudaSuccess)
-            return -1;
-        rb->c_lrf_status = B;
+        void *v;
+        RB_CARVE(v, tail[0]);
+        rb->sigma = (double *)v;
+        RB_CARVE(v, tail[1]);
+        rb->W = (double *)v;
+        RB_CARVE(v, tail[2]);
+        rb->groups = rb->n_groups > 0 ? (double *)v : NULL;
+        RB_CARVE(v, tail[3]);
+        rb->status = (int *)v;
+        RB_CARVE(v, tail[4]);
+        rb->lrf_status = (int *)v;
     }
-    return rc ? -1 : 0;
+#undef RB_CARVE
+    return 0;
 }
 
 /* ---- entry points ------------------------------------------------------------------------ */
@@ -920,7 +1006,7 @@ int ssa_rbatch_run(ssa_rbatch *rb, int B, const int *N, const int *L, const int 
             return -1;
         nx += (size_t)N[s];
     }
-    if (quiesce(rb) != 0 || grow((void **)&rb->d_xs, &rb->c_xs, nx, sizeof(double)) != 0)
+    if (quiesce(rb) != 0 || grow((void **)&rb->d_xs, &rb->c_xs, nx, sizeof(double), rb->main) != 0)
         return -1;
     if (cudaMemcpyAsync(rb->d_xs, x, sizeof(double) * nx, cudaMemcpyHostToDevice, rb->main) != cudaSuccess)
         return -1;

@@ -32,6 +32,8 @@ const double *ssar_groups(const ssa_rbatch *rb);
 const size_t *ssar_offsets(const ssa_rbatch *rb);
 void ssar_totals(const ssa_rbatch *rb, size_t *t4);
 size_t ssar_series_bytes(int N, int L, int k, int p, int n_groups);
+/* The library's stream-ordered device memory pool (current device), blocks cached on free. */
+cudaMemPool_t ssar_pool(void);
 
 #ifdef __cplusplus
 }

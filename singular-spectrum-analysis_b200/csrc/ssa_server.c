@@ -62,13 +62,14 @@ typedef struct
     unsigned long long *seeds;
     double **lrf_dst;
     res_entry **res;
-    double *h_x, *h_sig, *h_W, *h_grp;
-    size_t c_x, c_sig, c_W, c_grp;
-    int *h_st, *h_lst;
-    size_t c_st, c_lst;
+    /* per request: offsets (doubles) of its input in d_x and, for pageable buffers, in the
+     * pinned staging areas (SIZE_MAX = copied directly from / to the caller's pinned memory) */
+    size_t *xoff, *sin, *sout;
+    double *h_in, *h_out; /* pinned staging, fixed at creation */
+    int *h_st, *h_lst;    /* max_batch status words */
     double *d_x;
     size_t c_dx;
-    size_t bytes;
+    size_t bytes, in_used, out_used;
     cudaEvent_t done;
 } slot_t;
 
@@ -122,6 +123,54 @@ double ssa_server_now(void)
 }
 
 static int imin(int a, int b) { return a < b ? a : b; }
+
+/* Pinned staging per batch slot for callers' pageable buffers (allocated once at creation; a
+ * batch admits pageable requests while their bytes fit). Page-locked caller buffers
+ * (ssa_host_alloc or any cudaHostAlloc / cudaHostRegister memory) are copied directly. */
+#define SRV_STAGE_IN (256u << 20)
+#define SRV_STAGE_OUT (512u << 20)
+#define SRV_DIRECT ((size_t)-1)
+
+static int is_pinned(const void *p)
+{
+    if (!p)
+        return 0;
+    struct cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return 0;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+static int req_kout(const ssa_server *s, const ssa_request *r)
+{
+    const int K = r->N - r->L + 1;
+    const int kp = imin(r->k + s->p, imin(r->L, K));
+    return imin(r->k, kp);
+}
+
+/* Output bytes a decomposition request asks for (sigma, groups or W). */
+static size_t req_out_doubles(const ssa_server *s, const ssa_request *r)
+{
+    const size_t ke = (size_t)req_kout(s, r);
+    size_t n = r->sigma ? ke : 0;
+    if (r->type == SSA_REQ_DECOMPOSE_RECON && r->groups)
+        n += 2 * (size_t)r->N;
+    if (r->type == SSA_REQ_DECOMPOSE_WCORR && r->W)
+        n += ke * ke;
+    return n;
+}
+
+static const void *first_output(const ssa_request *r)
+{
+    if (r->sigma)
+        return r->sigma;
+    if (r->type == SSA_REQ_DECOMPOSE_RECON)
+        return r->groups;
+    return r->W;
+}
 
 /* ---- resident store ------------------------------------------------------------------------ */
 
@@ -219,7 +268,8 @@ static int res_alloc(ssa_server *s, res_entry *e)
     const size_t bytes = sizeof(double) * (2 * (size_t)(e->L - 1) + 1);
     if (res_make_room(s, bytes) != 0)
         return -1;
-    if (cudaMallocAsync((void **)&e->d, bytes, s->pool_st) != cudaSuccess)
+    cudaMemPool_t pool = ssar_pool();
+    if (!pool || cudaMallocFromPoolAsync((void **)&e->d, bytes, pool, s->pool_st) != cudaSuccess)
     {
         e->d = NULL;
         return -1;
@@ -330,47 +380,109 @@ static int slot_reserve(slot_t *sl, int n)
     for (int i = 0; i < 7; i++)
         if (!a[i])
             return -1;
+    size_t *z[3] = {NULL, NULL, NULL};
+    z[0] = (size_t *)realloc(sl->xoff, sizeof(size_t) * c);
+    if (z[0])
+        sl->xoff = z[0];
+    z[1] = (size_t *)realloc(sl->sin, sizeof(size_t) * c);
+    if (z[1])
+        sl->sin = z[1];
+    z[2] = (size_t *)realloc(sl->sout, sizeof(size_t) * c);
+    if (z[2])
+        sl->sout = z[2];
+    if (!z[0] || !z[1] || !z[2])
+        return -1;
     sl->cap = c;
     return 0;
 }
 
-/* Launch the batch gathered in sl (sl->n requests, dims filled). */
+/* Launch the batch gathered in sl (sl->n requests, dims and staging offsets filled). */
 static int slot_launch(ssa_server *s, slot_t *sl)
 {
+    const double t0 = ssa_server_now();
     size_t nx = 0;
     for (int i = 0; i < sl->n; i++)
-        nx += (size_t)sl->N[i];
-    if (grow_host((void **)&sl->h_x, &sl->c_x, nx, sizeof(double)) != 0 ||
-        grow_dev((void **)&sl->d_x, &sl->c_dx, nx, sizeof(double)) != 0)
-        return -1;
-    size_t o = 0;
-    for (int i = 0; i < sl->n; i++)
     {
-        memcpy(sl->h_x + o, sl->req[i]->x, sizeof(double) * sl->N[i]);
-        o += (size_t)sl->N[i];
+        sl->xoff[i] = nx;
+        nx += (size_t)sl->N[i];
     }
     cudaStream_t ms = ssar_main_stream(sl->rb);
+    if (sl->c_dx < nx)
+    {
+        /* stream-ordered, so that growing does not wait for the other slots' work */
+        if (sl->d_x)
+            cudaFreeAsync(sl->d_x, ms);
+        sl->d_x = NULL;
+        sl->c_dx = 0;
+        if (cudaMallocFromPoolAsync((void **)&sl->d_x, sizeof(double) * (nx + nx / 4), ssar_pool(), ms) != cudaSuccess)
+            return -1;
+        sl->c_dx = nx + nx / 4;
+    }
     /* resident blocks were allocated on the pool stream: order the batch after them */
     if (cudaEventRecord(s->ev_pool, s->pool_st) != cudaSuccess || cudaStreamWaitEvent(ms, s->ev_pool, 0) != cudaSuccess)
         return -1;
-    if (cudaMemcpyAsync(sl->d_x, sl->h_x, sizeof(double) * nx, cudaMemcpyHostToDevice, ms) != cudaSuccess)
-        return -1;
+    /* inputs: pinned buffers directly; pageable ones through the staging area, consecutive staged
+     * requests in one copy */
+    int i = 0;
+    while (i < sl->n)
+    {
+        const ssa_request *r = sl->req[i];
+        if (sl->sin[i] == SRV_DIRECT)
+        {
+            if (cudaMemcpyAsync(sl->d_x + sl->xoff[i], r->x, sizeof(double) * r->N, cudaMemcpyHostToDevice, ms) !=
+                cudaSuccess)
+                return -1;
+            i++;
+            continue;
+        }
+        int j = i;
+        size_t run = 0;
+        while (j < sl->n && sl->sin[j] != SRV_DIRECT && sl->sin[j] == sl->sin[i] + run)
+        {
+            memcpy(sl->h_in + sl->sin[j], sl->req[j]->x, sizeof(double) * sl->req[j]->N);
+            run += (size_t)sl->req[j]->N;
+            j++;
+        }
+        if (cudaMemcpyAsync(sl->d_x + sl->xoff[i], sl->h_in + sl->sin[i], sizeof(double) * run,
+                            cudaMemcpyHostToDevice, ms) != cudaSuccess)
+            return -1;
+        i = j;
+    }
     if (ssar_run_enqueue_ex(sl->rb, sl->n, sl->N, sl->L, sl->k, sl->d_x, sl->seeds, sl->lrf_dst) != 0)
         return -1;
-    size_t t4[4];
-    ssar_totals(sl->rb, t4);
-    if (grow_host((void **)&sl->h_sig, &sl->c_sig, t4[1], sizeof(double)) != 0 ||
-        grow_host((void **)&sl->h_W, &sl->c_W, t4[2], sizeof(double)) != 0 ||
-        grow_host((void **)&sl->h_grp, &sl->c_grp, t4[3], sizeof(double)) != 0 ||
-        grow_host((void **)&sl->h_st, &sl->c_st, (size_t)sl->n, sizeof(int)) != 0 ||
-        grow_host((void **)&sl->h_lst, &sl->c_lst, (size_t)sl->n, sizeof(int)) != 0)
-        return -1;
-    if (cudaMemcpyAsync(sl->h_sig, ssar_sigma(sl->rb), sizeof(double) * t4[1], cudaMemcpyDeviceToHost, ms) !=
-            cudaSuccess ||
-        cudaMemcpyAsync(sl->h_W, ssar_W(sl->rb), sizeof(double) * t4[2], cudaMemcpyDeviceToHost, ms) != cudaSuccess ||
-        cudaMemcpyAsync(sl->h_grp, ssar_groups(sl->rb), sizeof(double) * t4[3], cudaMemcpyDeviceToHost, ms) !=
-            cudaSuccess ||
-        cudaMemcpyAsync(sl->h_st, ssar_status(sl->rb), sizeof(int) * sl->n, cudaMemcpyDeviceToHost, ms) !=
+    /* outputs the requests ask for */
+    const size_t *off = ssar_offsets(sl->rb);
+    const double *dsig = ssar_sigma(sl->rb), *dW = ssar_W(sl->rb), *dg = ssar_groups(sl->rb);
+    for (i = 0; i < sl->n; i++)
+    {
+        ssa_request *r = sl->req[i];
+        const int ke = req_kout(s, r);
+        const int direct = sl->sout[i] == SRV_DIRECT;
+        size_t so = sl->sout[i];
+        if (r->sigma)
+        {
+            double *dst = direct ? r->sigma : sl->h_out + so;
+            if (cudaMemcpyAsync(dst, dsig + off[4 * i + 1], sizeof(double) * ke, cudaMemcpyDeviceToHost, ms) !=
+                cudaSuccess)
+                return -1;
+            so += (size_t)ke;
+        }
+        if (r->type == SSA_REQ_DECOMPOSE_RECON && r->groups)
+        {
+            double *dst = direct ? r->groups : sl->h_out + so;
+            if (cudaMemcpyAsync(dst, dg + off[4 * i + 3], sizeof(double) * 2 * r->N, cudaMemcpyDeviceToHost, ms) !=
+                cudaSuccess)
+                return -1;
+        }
+        if (r->type == SSA_REQ_DECOMPOSE_WCORR && r->W)
+        {
+            double *dst = direct ? r->W : sl->h_out + so;
+            if (cudaMemcpyAsync(dst, dW + off[4 * i + 2], sizeof(double) * ke * ke, cudaMemcpyDeviceToHost, ms) !=
+                cudaSuccess)
+                return -1;
+        }
+    }
+    if (cudaMemcpyAsync(sl->h_st, ssar_status(sl->rb), sizeof(int) * sl->n, cudaMemcpyDeviceToHost, ms) !=
             cudaSuccess ||
         cudaMemcpyAsync(sl->h_lst, ssar_lrf_status(sl->rb), sizeof(int) * sl->n, cudaMemcpyDeviceToHost, ms) !=
             cudaSuccess ||
@@ -381,28 +493,34 @@ static int slot_launch(ssa_server *s, slot_t *sl)
     s->stats.decompositions += sl->n;
     if (sl->n > s->stats.max_batch)
         s->stats.max_batch = sl->n;
+    s->stats.host_launch_s += ssa_server_now() - t0;
     return 0;
 }
 
 static void slot_finish(ssa_server *s, slot_t *sl, int launch_ok)
 {
-    const size_t *off = launch_ok ? ssar_offsets(sl->rb) : NULL;
+    const double t0 = ssa_server_now();
     for (int i = 0; i < sl->n; i++)
     {
         ssa_request *r = sl->req[i];
         int ok = launch_ok && sl->h_st[i] == 0;
         if (ok)
         {
-            const int K = r->N - r->L + 1;
-            const int kp = imin(r->k + s->p, imin(r->L, K));
-            const int ke = imin(r->k, kp);
+            const int ke = req_kout(s, r);
             r->k_out = ke;
-            if (r->sigma)
-                memcpy(r->sigma, sl->h_sig + off[4 * i + 1], sizeof(double) * ke);
-            if (r->W)
-                memcpy(r->W, sl->h_W + off[4 * i + 2], sizeof(double) * ke * ke);
-            if (r->groups)
-                memcpy(r->groups, sl->h_grp + off[4 * i + 3], sizeof(double) * 2 * r->N);
+            if (sl->sout[i] != SRV_DIRECT)
+            {
+                size_t so = sl->sout[i];
+                if (r->sigma)
+                {
+                    memcpy(r->sigma, sl->h_out + so, sizeof(double) * ke);
+                    so += (size_t)ke;
+                }
+                if (r->type == SSA_REQ_DECOMPOSE_RECON && r->groups)
+                    memcpy(r->groups, sl->h_out + so, sizeof(double) * 2 * r->N);
+                if (r->type == SSA_REQ_DECOMPOSE_WCORR && r->W)
+                    memcpy(r->W, sl->h_out + so, sizeof(double) * ke * ke);
+            }
         }
         res_entry *e = sl->res[i];
         if (e) /* the forecast group [0, 1, 2] needs at least 3 components */
@@ -411,6 +529,8 @@ static void slot_finish(ssa_server *s, slot_t *sl, int launch_ok)
     }
     sl->n = 0;
     sl->busy = 0;
+    sl->in_used = sl->out_used = 0;
+    s->stats.host_finish_s += ssa_server_now() - t0;
 }
 
 /* ---- forecast batches ------------------------------------------------------------------- */
@@ -606,10 +726,27 @@ static int dispatch(ssa_server *s)
                     keep = 0;
                     progressed = 1;
                 }
-                else if (bytes + b <= s->batch_budget && slot_reserve(free_slot, free_slot->n + 1) == 0)
+                const size_t in_b = is_pinned(r->x) ? 0 : (size_t)r->N;
+                const size_t nout = req_out_doubles(s, r);
+                const size_t out_b = (nout && !is_pinned(first_output(r))) ? nout : 0;
+                if (in_b > SRV_STAGE_IN / sizeof(double) || out_b > SRV_STAGE_OUT / sizeof(double))
+                {
+                    if (r->priv && r->priv != (void *)&g_not_resident)
+                        ((res_entry *)r->priv)->state = RES_FAILED;
+                    finish_request(s, r, -1); /* pageable buffers larger than the staging area */
+                    keep = 0;
+                    progressed = 1;
+                }
+                else if (bytes + b <= s->batch_budget && free_slot->in_used + in_b <= SRV_STAGE_IN / sizeof(double) &&
+                         free_slot->out_used + out_b <= SRV_STAGE_OUT / sizeof(double) &&
+                         slot_reserve(free_slot, free_slot->n + 1) == 0)
                 {
                     slot_t *sl = free_slot;
                     const int j = sl->n;
+                    sl->sin[j] = in_b ? sl->in_used : SRV_DIRECT;
+                    sl->sout[j] = out_b ? sl->out_used : SRV_DIRECT;
+                    sl->in_used += in_b;
+                    sl->out_used += out_b;
                     res_entry *e = r->priv == (void *)&g_not_resident ? NULL : (res_entry *)r->priv;
                     if (e && !e->d && res_alloc(s, e) != 0)
                         s->stats.not_resident++; /* runs, but its series will not be resident */
@@ -723,6 +860,7 @@ int ssa_server_create(ssa_server **out, size_t hbm_budget_bytes, int max_infligh
         free(s);
         return -1;
     }
+    const int reserve = hbm_budget_bytes != 0;
     if (hbm_budget_bytes == 0)
     {
         size_t fr = 0, tot = 0;
@@ -735,7 +873,8 @@ int ssa_server_create(ssa_server **out, size_t hbm_budget_bytes, int max_infligh
     }
     s->budget = hbm_budget_bytes;
     s->res_budget = hbm_budget_bytes / 4;
-    s->batch_budget = (hbm_budget_bytes - s->res_budget) / (size_t)max_inflight;
+    /* device buffers grow by a quarter beyond a batch's estimate: keep the slots inside the budget */
+    s->batch_budget = (hbm_budget_bytes - s->res_budget) / (size_t)max_inflight / 5 * 4;
     s->hcap = 65521;
     s->htab = (res_entry **)calloc((size_t)s->hcap, sizeof(res_entry *));
     s->qcap = 1 << 16;
@@ -755,11 +894,32 @@ int ssa_server_create(ssa_server **out, size_t hbm_budget_bytes, int max_infligh
         slot_t *sl = &s->slots[i];
         if (ssa_rbatch_create(&sl->rb, s->p, power_iters, g_group_idx, g_group_sizes, SRV_GROUPS) != 0 ||
             ssar_set_lrf_group(sl->rb, 2, g_fc_group, 3) != 0 ||
-            cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming) != cudaSuccess)
+            cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaMallocHost((void **)&sl->h_in, SRV_STAGE_IN) != cudaSuccess ||
+            cudaMallocHost((void **)&sl->h_out, SRV_STAGE_OUT) != cudaSuccess ||
+            cudaMallocHost((void **)&sl->h_st, sizeof(int) * (size_t)max_batch) != cudaSuccess ||
+            cudaMallocHost((void **)&sl->h_lst, sizeof(int) * (size_t)max_batch) != cudaSuccess ||
+            (reserve && ssa_rbatch_reserve(sl->rb, s->batch_budget + s->batch_budget / 8) != 0))
         {
             ssa_server_destroy(s);
             return -1;
         }
+    }
+    {
+        /* forecast batches: tables for max_batch jobs and 4 MB of outputs up front (grown if a
+         * batch asks for more) */
+        fslot_t *f = &s->fs;
+        f->req = (ssa_request **)malloc(sizeof(ssa_request *) * (size_t)max_batch);
+        f->res = (res_entry **)malloc(sizeof(res_entry *) * (size_t)max_batch);
+        if (!f->req || !f->res || cudaMallocHost((void **)&f->h_jobs, sizeof(ssa_fc_job) * (size_t)max_batch) != cudaSuccess ||
+            cudaMalloc((void **)&f->d_jobs, sizeof(ssa_fc_job) * (size_t)max_batch) != cudaSuccess ||
+            grow_host((void **)&f->h_out, &f->c_hout, (size_t)1 << 19, sizeof(double)) != 0 ||
+            grow_dev((void **)&f->d_out, &f->c_dout, (size_t)1 << 19, sizeof(double)) != 0)
+        {
+            ssa_server_destroy(s);
+            return -1;
+        }
+        f->cap = max_batch;
     }
     if (cudaStreamCreateWithFlags(&s->fs.st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->fs.done, cudaEventDisableTiming) != cudaSuccess ||
@@ -768,15 +928,6 @@ int ssa_server_create(ssa_server **out, size_t hbm_budget_bytes, int max_infligh
     {
         ssa_server_destroy(s);
         return -1;
-    }
-    {
-        /* keep freed resident blocks cached in the pool instead of returning them to the driver */
-        cudaMemPool_t pool;
-        if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess)
-        {
-            unsigned long long thr = (unsigned long long)s->res_budget;
-            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-        }
     }
     if (pthread_create(&s->th, NULL, worker, s) != 0)
     {
@@ -889,7 +1040,7 @@ void ssa_server_destroy(ssa_server *s)
             ssa_rbatch_destroy(sl->rb);
         if (sl->done)
             cudaEventDestroy(sl->done);
-        void *hp[] = {sl->h_x, sl->h_sig, sl->h_W, sl->h_grp, sl->h_st, sl->h_lst};
+        void *hp[] = {sl->h_in, sl->h_out, sl->h_st, sl->h_lst};
         for (size_t j = 0; j < sizeof(hp) / sizeof(hp[0]); j++)
             if (hp[j])
                 cudaFreeHost(hp[j]);
@@ -902,6 +1053,9 @@ void ssa_server_destroy(ssa_server *s)
         free(sl->seeds);
         free(sl->lrf_dst);
         free(sl->res);
+        free(sl->xoff);
+        free(sl->sin);
+        free(sl->sout);
     }
     free(s->slots);
     if (s->htab)
@@ -934,4 +1088,21 @@ void ssa_server_destroy(ssa_server *s)
     free(s->pend);
     free(s->q);
     free(s);
+    cudaMemPool_t pool = ssar_pool();
+    if (pool)
+        cudaMemPoolTrimTo(pool, 0);
+}
+
+void *ssa_host_alloc(size_t bytes)
+{
+    void *p = NULL;
+    if (bytes == 0 || cudaMallocHost(&p, bytes) != cudaSuccess)
+        return NULL;
+    return p;
+}
+
+void ssa_host_free(void *p)
+{
+    if (p)
+        cudaFreeHost(p);
 }

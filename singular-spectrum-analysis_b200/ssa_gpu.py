@@ -671,7 +671,8 @@ class _ServerStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_longlong) for n in ("submitted", "completed", "failed", "batches", "decompositions",
                                                   "max_batch", "forecast_batches", "forecasts", "evictions",
                                                   "not_resident")] + \
-               [(n, ctypes.c_size_t) for n in ("resident_bytes", "resident_budget", "batch_budget")]
+               [(n, ctypes.c_size_t) for n in ("resident_bytes", "resident_budget", "batch_budget")] + \
+               [(n, ctypes.c_double) for n in ("host_launch_s", "host_finish_s")]
 
 
 _sig("ssa_server_create", _I, ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t, _I, _I, _I, _I)
@@ -681,6 +682,33 @@ _sig("ssa_server_drain", _I, ctypes.c_void_p)
 _sig("ssa_server_replay", _I, ctypes.c_void_p, ctypes.POINTER(_Request), c_double_p, _I)
 _sig("ssa_server_stats_get", _I, ctypes.c_void_p, ctypes.POINTER(_ServerStats))
 _sig("ssa_server_now", _D)
+_sig("ssa_host_alloc", ctypes.c_void_p, ctypes.c_size_t)
+_sig("ssa_host_free", _V, ctypes.c_void_p)
+
+
+class _PinnedPool:
+    """Page-locked host arrays (ssa_host_alloc), freed with the pool."""
+
+    def __init__(self):
+        self._ptrs = []
+
+    def array(self, shape, src: Optional[np.ndarray] = None) -> np.ndarray:
+        n = int(np.prod(shape))
+        p = _lib.ssa_host_alloc(max(1, n) * 8)
+        if not p:
+            raise MemoryError("ssa_host_alloc failed")
+        self._ptrs.append(p)
+        a = np.ctypeslib.as_array(ctypes.cast(p, c_double_p), shape=(max(1, n),))[:n].reshape(shape)
+        if src is not None:
+            a[...] = src
+        else:
+            a[...] = 0.0
+        return a
+
+    def __del__(self):
+        for p in self._ptrs:
+            _lib.ssa_host_free(p)
+        self._ptrs = []
 
 REQ_DECOMPOSE_RECON, REQ_DECOMPOSE_WCORR, REQ_FORECAST = 0, 1, 2
 
@@ -692,11 +720,19 @@ class Requests:
     append requests; after the server has completed them, ``result(i)`` returns a dict of the
     outputs, ``status`` and the latency in seconds."""
 
-    def __init__(self, capacity: int, keep_outputs: bool = True):
+    def __init__(self, capacity: int, keep_outputs: bool = True, pinned: bool = False):
         self.arr = (_Request * max(1, capacity))()
         self.n = 0
         self.keep_outputs = keep_outputs
         self._bufs = []
+        self._pool = _PinnedPool() if pinned else None
+
+    def _buf(self, shape, src=None):
+        if self._pool is not None:
+            return self._pool.array(shape, src)
+        if src is not None:
+            return np.ascontiguousarray(src, dtype=np.float64)
+        return np.zeros(shape)
 
     def _next(self):
         if self.n >= len(self.arr):
@@ -708,7 +744,7 @@ class Requests:
     def add_decompose(self, x: np.ndarray, L: int, k: int, series_id: int = 0, seed: int = 0,
                       wcorr: bool = False) -> int:
         r = self._next()
-        x = np.ascontiguousarray(x, dtype=np.float64)
+        x = self._buf((len(x),), np.asarray(x, dtype=np.float64))
         N = len(x)
         r.type = REQ_DECOMPOSE_WCORR if wcorr else REQ_DECOMPOSE_RECON
         r.series_id, r.N, r.L, r.k, r.seed = series_id, N, L, k, seed
@@ -716,13 +752,13 @@ class Requests:
         bufs = {"x": x}
         if self.keep_outputs:
             ke = max(1, min(k, L, N - L + 1))
-            bufs["sigma"] = np.zeros(ke)
+            bufs["sigma"] = self._buf((ke,))
             r.sigma = _dp(bufs["sigma"])
             if wcorr:
-                bufs["W"] = np.zeros((ke, ke))
+                bufs["W"] = self._buf((ke, ke))
                 r.W = _dp(bufs["W"])
             else:
-                bufs["groups"] = np.zeros((2, N))
+                bufs["groups"] = self._buf((2, N))
                 r.groups = _dp(bufs["groups"])
         self._bufs.append(bufs)
         return self.n - 1
@@ -733,7 +769,7 @@ class Requests:
         r.series_id, r.h = series_id, h
         bufs = {}
         if self.keep_outputs:
-            bufs["forecast"] = np.zeros(h)
+            bufs["forecast"] = self._buf((h,))
             r.forecast = _dp(bufs["forecast"])
         self._bufs.append(bufs)
         return self.n - 1

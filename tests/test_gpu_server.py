@@ -61,12 +61,15 @@ def oracle_dec(oracle, x, L, k, seed):
     return oracle.decompose_randomized(x, L, k, P, Om, q=Q)
 
 
-def test_server_mixed_requests_vs_oracle(gpu, oracle):
+@pytest.mark.parametrize("pinned", [False, True])
+def test_server_mixed_requests_vs_oracle(gpu, oracle, pinned):
+    """Pageable buffers go through the staging areas, page-locked ones are copied directly."""
     rng = np.random.default_rng(21)
-    shapes = [(800, 200, 12), (5000, 1250, 30), (12000, 3000, 20), (18000, 4500, 15), (2500, 625, 45)]
+    shapes = [(800, 200, 12), (5000, 1250, 30), (12000, 3000, 20), (18000, 4500, 15), (2500, 625, 45),
+              (70000, 17500, 14)]
     xs = [oracle.walk_sines(rng, N) for N, _, _ in shapes]
     srv = gpu.SSAServer(max_inflight=2, oversampling=P, power_iters=Q)
-    R = gpu.Requests(3 * len(shapes))
+    R = gpu.Requests(3 * len(shapes), pinned=pinned)
     for i, ((N, L, k), x) in enumerate(zip(shapes, xs)):
         R.add_decompose(x, L, k, series_id=100 + i, seed=1000 + i)
     for i, ((N, L, k), x) in enumerate(zip(shapes, xs)):
