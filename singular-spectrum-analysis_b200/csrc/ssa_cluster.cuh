@@ -200,8 +200,14 @@ __device__ __forceinline__ void cl_load(float2* s, const float* f32, const doubl
         float2 v = make_float2(0.f, 0.f);
         if (t < n) {
             if (f32) {
-                v.x = f32[t] * sc;
-                v.y = t + 1 < n ? f32[t + 1] * sc : 0.f;
+                // t is even and columns start 16-byte aligned: one 8-byte load for the pair
+                if (t + 1 < n) {
+                    v = *reinterpret_cast<const float2*>(f32 + t);
+                    v.x *= sc;
+                    v.y *= sc;
+                } else {
+                    v.x = f32[t] * sc;
+                }
             } else if (f64) {
                 v.x = (float)f64[t];
                 v.y = t + 1 < n ? (float)f64[t + 1] : 0.f;
@@ -217,7 +223,7 @@ __device__ __forceinline__ void cl_load(float2* s, const float* f32, const doubl
 // Spectrum (CL_SPEC), correlation sweep (CL_CORR) and one-buffer elementary reconstruction
 // (CL_ELEM) on clusters; grid (C x columns, jobs), one cluster per column.
 template <int LOGH, int KIND>
-__global__ void __launch_bounds__(ClShape<LOGH>::BLOCK) k_cl_col(const ssa_col_job* __restrict__ jobs) {
+__global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, 2) k_cl_col(const ssa_col_job* __restrict__ jobs) {
     using S = ClShape<LOGH>;
     extern __shared__ float2 smem[];
     __shared__ double red[32];
@@ -262,8 +268,10 @@ __global__ void __launch_bounds__(ClShape<LOGH>::BLOCK) k_cl_col(const ssa_col_j
             const int t = 2 * (m * S::C + rank);
             if (t >= J.n_out) continue;
             const float2 z = s[spad(m)];
-            out[t] = z.x * inv_h;
-            if (t + 1 < J.n_out) out[t + 1] = z.y * inv_h;
+            if (t + 1 < J.n_out)
+                *reinterpret_cast<float2*>(out + t) = make_float2(z.x * inv_h, z.y * inv_h);
+            else
+                out[t] = z.x * inv_h;
         }
     } else {
         const float sc = J.scale ? (float)J.scale[c] : 1.0f;
@@ -297,7 +305,7 @@ __global__ void __launch_bounds__(ClShape<LOGH>::BLOCK) k_cl_col(const ssa_col_j
 
 // Grouped reconstruction from cached spectra on clusters; grid (C, jobs).
 template <int LOGH>
-__global__ void __launch_bounds__(ClShape<LOGH>::BLOCK) k_cl_recon(const ssa_recon_job* __restrict__ jobs) {
+__global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, 2) k_cl_recon(const ssa_recon_job* __restrict__ jobs) {
     using S = ClShape<LOGH>;
     extern __shared__ float2 smem[];
     float2* s = smem;

@@ -30,8 +30,9 @@ static int imax(int a, int b) { return a > b ? a : b; }
 
 static int gram_rows(int m, int B)
 {
-    /* Aim for about two CTAs per SM over all series; at least one staging chunk per CTA. */
-    int target = 296 / (B > 0 ? B : 1);
+    /* Aim for about eight 4-warp CTAs per SM over all series (latency hiding when a launch holds
+     * few series); at least one staging chunk per CTA. */
+    int target = 1184 / (B > 0 ? B : 1);
     if (target < 1)
         target = 1;
     int rows = (m + target - 1) / target;

@@ -702,24 +702,36 @@ __global__ void __launch_bounds__(ROWMUL_THREADS) k_rowmul(const ssa_rowmul_job*
 
 #define RR_THREADS 512
 
+// Round-robin (circle method) position i after `step` rotations of positions 1 .. ne-1 (each
+// rotation moves the last position's index to position 1): pairs (pos(t), pos(ne-1-t)) of one
+// step are disjoint and every pair meets once per ne-1 steps.
+__device__ __forceinline__ int rr_pos(int i, int step, int ne) {
+    if (i == 0) return 0;
+    const int m = ne - 1;
+    int v = (i - 1 - step) % m;
+    if (v < 0) v += m;
+    return 1 + v;
+}
+
 // One-sided (Hestenes) Jacobi on the n columns of A (column c at A + c * SLD, FP64, shared
 // memory): A <- A J with J a product of plane rotations accumulated into Z (initialised by the
-// caller), until every column pair is orthogonal to 1e-15 relative. Round-robin pairing, one
-// warp per pair, lanes own rows lane and lane + 32. perm needs n + 1 ints; on return nrm[c] =
-// ||A[:, c]||. Called by every thread of the block.
-__device__ void onesided_jacobi(double* A, double* Z, int n, int* perm, int* notconv, double* nrm) {
+// caller), until every column pair is orthogonal to 4 sqrt(n) eps relative (rotations below the
+// rounding level of the dot products would otherwise never stop; LAPACK's one-sided Jacobi uses
+// sqrt(m) eps). Round-robin pairing
+// computed from the step number, one warp per pair, lanes own rows lane and lane + 32; one
+// barrier per step. On return nrm[c] = ||A[:, c]||. Called by every thread of the block.
+__device__ void onesided_jacobi(double* A, double* Z, int n, int* notconv, double* nrm) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int ne = (n + 1) & ~1;  // even count; index n is a dummy when n is odd
-    for (int i = threadIdx.x; i < ne; i += blockDim.x) perm[i] = i;
-    __syncthreads();
     const int npairs = ne / 2;
     const double tiny = 1e-300;
+    const double tol = 4.0 * sqrt((double)n) * 2.220446049250313e-16;
     for (int sweep = 0; sweep < 40; ++sweep) {
         if (threadIdx.x == 0) *notconv = 0;
         __syncthreads();
         for (int step = 0; step < ne - 1; ++step) {
             for (int t = warp; t < npairs; t += nw) {
-                int p = perm[t], q = perm[ne - 1 - t];
+                int p = rr_pos(t, step, ne), q = rr_pos(ne - 1 - t, step, ne);
                 if (q >= n || p >= n) continue;
                 if (p < 0 || q < 0) {
                     if (lane == 0) check_fail(6, 6, (unsigned)(p * 1000 + q));
@@ -740,7 +752,7 @@ __device__ void onesided_jacobi(double* A, double* Z, int n, int* perm, int* not
                     be += __shfl_xor_sync(0xffffffffu, be, o);
                     ga += __shfl_xor_sync(0xffffffffu, ga, o);
                 }
-                if (fabs(ga) > tiny && fabs(ga) > 1e-15 * sqrt(al * be)) {
+                if (fabs(ga) > tiny && fabs(ga) > tol * sqrt(al * be)) {
                     if (lane == 0) *notconv = 1;
                     const double zeta = (be - al) / (2.0 * ga);
                     const double tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
@@ -757,12 +769,6 @@ __device__ void onesided_jacobi(double* A, double* Z, int n, int* perm, int* not
                         zq[r] = sn * u + cs * v;
                     }
                 }
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) {  // round-robin: keep perm[0], rotate perm[1..ne-1]
-                const int last = perm[ne - 1];
-                for (int i = ne - 1; i > 1; --i) perm[i] = perm[i - 1];
-                perm[1] = last;
             }
             __syncthreads();
         }
@@ -789,7 +795,6 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr(const ssa_rr_job* __restrict_
     extern __shared__ double dsm[];
     double* A = dsm;                    // column c at A + c * SLD
     double* Z = dsm + SSA_MAX_KP * SLD;
-    __shared__ int perm[SSA_MAX_KP + 1];
     __shared__ double qs[SSA_MAX_KP];
     __shared__ double nrm[SSA_MAX_KP];
     __shared__ int order[SSA_MAX_KP];
@@ -824,18 +829,17 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr(const ssa_rr_job* __restrict_
         if (threadIdx.x == 0 && J.status) atomicOr(J.status, 2);
     }
     chol_upper_inplace(A, n, dmax > 0.0 ? dmax * 1e-15 : 1.0);
-    onesided_jacobi(A, Z, n, perm, &notconv, nrm);
+    onesided_jacobi(A, Z, n, &notconv, nrm);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int i = 0; i < n; ++i) order[i] = i;
-        for (int i = 0; i < n; ++i) {  // selection sort, descending singular value
-            int best = i;
-            for (int j = i + 1; j < n; ++j)
-                if (nrm[order[j]] > nrm[order[best]]) best = j;
-            const int tmp = order[i];
-            order[i] = order[best];
-            order[best] = tmp;
+    // descending singular values: each column's rank is the number of columns before it
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double v = nrm[i];
+        int rank = 0;
+        for (int j = 0; j < n; ++j) {
+            const double w = nrm[j];
+            rank += (w > v) || (w == v && j < i);
         }
+        order[rank] = i;
     }
     __syncthreads();
     const int k = J.k;
@@ -958,7 +962,6 @@ __global__ void __launch_bounds__(RR_THREADS) k_svdsmall(const ssa_svd_job* __re
     extern __shared__ double dsm[];
     double* A = dsm;                    // column j of M at A + j * SLD
     double* Z = dsm + SSA_MAX_KP * SLD;
-    __shared__ int perm[SSA_MAX_KP + 1];
     __shared__ double nrm[SSA_MAX_KP];
     __shared__ int order[SSA_MAX_KP];
     __shared__ int notconv;
@@ -978,17 +981,15 @@ __global__ void __launch_bounds__(RR_THREADS) k_svdsmall(const ssa_svd_job* __re
     for (int c = warp; c < n; c += nw)
         for (int r = lane; r < n; r += 32) Z[c * SLD + r] = (r == c) ? 1.0 : 0.0;
     __syncthreads();
-    onesided_jacobi(A, Z, n, perm, &notconv, nrm);
-    if (threadIdx.x == 0) {
-        for (int i = 0; i < n; ++i) order[i] = i;
-        for (int i = 0; i < n; ++i) {  // descending singular value
-            int best = i;
-            for (int j = i + 1; j < n; ++j)
-                if (nrm[order[j]] > nrm[order[best]]) best = j;
-            const int tmp = order[i];
-            order[i] = order[best];
-            order[best] = tmp;
+    onesided_jacobi(A, Z, n, &notconv, nrm);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {  // descending singular value
+        const double v = nrm[i];
+        int rank = 0;
+        for (int j = 0; j < n; ++j) {
+            const double w = nrm[j];
+            rank += (w > v) || (w == v && j < i);
         }
+        order[rank] = i;
     }
     __syncthreads();
     for (int j = warp; j < n; j += nw) {

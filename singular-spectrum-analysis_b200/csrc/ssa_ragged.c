@@ -99,8 +99,8 @@ static long long round4(long long v) { return (v + 3) & ~3LL; }
 
 static int gram_rows(int m, int nb)
 {
-    /* about two CTAs per SM over the bucket's series; at least one staging chunk per CTA */
-    int target = 296 / (nb > 0 ? nb : 1);
+    /* about eight 4-warp CTAs per SM over the bucket's series; at least one staging chunk per CTA */
+    int target = 1184 / (nb > 0 ? nb : 1);
     if (target < 1)
         target = 1;
     int rows = (m + target - 1) / target;
