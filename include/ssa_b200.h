@@ -88,6 +88,14 @@ int ssa_opt_copy_factors(const SSA_Opt *ssa, double *U, double *V);
  * V (K x k) and sigma (k). Any pointer may be NULL. Returns k or -1. */
 int mssa_opt_copy_factors(const MSSA_Opt *mssa, double *U, double *V, double *sigma);
 
+/* Arithmetic of the W-correlation Gram in every pipeline (single series, batches, server):
+ * 1 (default) = 5th-generation tensor cores, split-TF32 products (hi hi^T + lo hi^T + hi lo^T)
+ * with FP32 accumulation in TMEM per chunk of >= 1024 time steps and FP64 across chunks;
+ * 0 = FP64 accumulation of FP32 products on the CUDA cores. SSA_WCORR_FP64=1 in the environment
+ * selects 0 at start-up. No counterpart in the reference (its W-correlation is FP64 dsyrk). */
+void ssa_b200_set_wcorr_tensor_cores(int on);
+int ssa_b200_wcorr_tensor_cores(void);
+
 /* ---- Uneven batches ------------------------------------------------------------------------
  * B series of different lengths N[s], windows L[s] and ranks k[s] (common oversampling p and
  * power iterations q) through the same pipeline as ssa_batch_*: randomized decomposition with

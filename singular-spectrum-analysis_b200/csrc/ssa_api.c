@@ -1246,6 +1246,9 @@ int ssa_opt_cadzow_inplace(SSA_Opt *ssa, int rank, int max_iter, ssa_real tol, S
     return iter;
 }
 
+void ssa_b200_set_wcorr_tensor_cores(int on) { ssad_set_wcorr_tc(on); }
+int ssa_b200_wcorr_tensor_cores(void) { return ssad_wcorr_tc(); }
+
 /* ---- library information ----------------------------------------------------------------- */
 unsigned long long ssa_b200_kernel_launches(void) { return ssad_launch_count(); }
 int ssa_b200_device_checks(unsigned int *out5, int reset) { return ssad_read_checks(out5, reset) == 0 ? 0 : -1; }

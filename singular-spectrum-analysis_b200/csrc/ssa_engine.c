@@ -642,10 +642,50 @@ int ssae_elem_recon(ssa_engine *e, int nb, int k)
     return rc_;
 }
 
+/* W-correlation Gram on the tensor cores: chunks of at least SSA_TC_MIN_ROWS time steps. */
+static int wgram_tc(ssa_engine *e, int nb, int k, int rows)
+{
+    const int nchmax = imax(e->nch_L, imax(e->nch_K, e->nch_N));
+    const size_t np = (size_t)e->kp * (e->kp + 1) / 2;
+    ssa_gram_job *jobs = (ssa_gram_job *)calloc((size_t)nb, sizeof(ssa_gram_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    for (int s = 0; s < nb; s++)
+    {
+        ssa_gram_job *J = &jobs[s];
+        J->A = e->recon + (size_t)s * e->k * e->ldN;
+        J->part = e->part + (size_t)s * nchmax * np;
+        J->ld = e->ldN;
+        J->m = e->N;
+        J->n = k;
+        J->rows_per_cta = rows;
+        J->weighted = 1;
+        J->N = e->N;
+        J->L = e->L;
+        J->K = e->K;
+        J->status = e->status + s;
+    }
+    void *d = ssae_push_jobs(e, jobs, sizeof(ssa_gram_job) * nb);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_GRAM);
+    int rc_ = ssad_gram_tc((const ssa_gram_job *)d, nb, (e->N + rows - 1) / rows, e->st);
+    ssae_prof_end(e);
+    return rc_;
+}
+
 int ssae_wcorr(ssa_engine *e, int nb, int k)
 {
-    /* weighted Gram of the elementary reconstructions: G_ij = sum_t w_t x~_i[t] x~_j[t] */
-    CK(gram(e, nb, e->recon, (size_t)e->k * e->ldN, e->ldN, e->N, k, e->rows_N, 1));
+    /* weighted Gram of the elementary reconstructions: G_ij = sum_t w_t x~_i[t] x~_j[t], on the
+     * tensor cores (split TF32) or with FP64 accumulation on the CUDA cores */
+    const int tc = ssad_wcorr_tc();
+    const int rows_tc = imax(e->rows_N, SSA_TC_MIN_ROWS);
+    const int nch_w = tc ? (e->N + rows_tc - 1) / rows_tc : e->nch_N;
+    if (tc)
+        CK(wgram_tc(e, nb, k, rows_tc));
+    else
+        CK(gram(e, nb, e->recon, (size_t)e->k * e->ldN, e->ldN, e->N, k, e->rows_N, 1));
     ssa_wfin_job *jobs = (ssa_wfin_job *)calloc((size_t)nb, sizeof(ssa_wfin_job));
     if (!jobs)
         return (int)cudaErrorMemoryAllocation;
@@ -655,7 +695,7 @@ int ssae_wcorr(ssa_engine *e, int nb, int k)
     {
         jobs[s].part = e->part + (size_t)s * nchmax * np;
         jobs[s].W = e->W + (size_t)s * e->k * e->k;
-        jobs[s].nchunks = e->nch_N;
+        jobs[s].nchunks = nch_w;
         jobs[s].k = k;
     }
     void *d = ssae_push_jobs(e, jobs, sizeof(ssa_wfin_job) * nb);

@@ -1307,6 +1307,24 @@ static int launch_recon(const ssa_recon_job* jobs, int njobs, cudaStream_t st) {
 }
 
 #include "ssa_cluster.cuh"
+#include "ssa_tc.cuh"
+
+static int g_wcorr_tc = -1;  // -1: not yet read from the environment
+
+extern "C" void ssad_set_wcorr_tc(int on) { g_wcorr_tc = on ? 1 : 0; }
+
+extern "C" int ssad_wcorr_tc(void) {
+    if (g_wcorr_tc < 0) {
+        const char* v = getenv("SSA_WCORR_FP64");
+        g_wcorr_tc = (v && v[0] == '1') ? 0 : 1;
+    }
+    return g_wcorr_tc;
+}
+
+extern "C" int ssad_gram_tc(const ssa_gram_job* d_jobs, int njobs, int maxchunks, void* stream) {
+    if (njobs <= 0 || maxchunks <= 0) return 0;
+    return launch_gram_tc(d_jobs, njobs, maxchunks, (cudaStream_t)stream);
+}
 
 extern "C" int ssad_spectrum(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
     if (njobs <= 0 || maxcols <= 0) return 0;

@@ -63,7 +63,20 @@ typedef struct
     int rows_per_cta;     /* rows folded into one partial (multiple of SSA_GRAM_CHUNK) */
     int weighted;         /* 1: row t weighted by min(t+1, L, K, N-t) */
     int N, L, K;
+    int *status;          /* optional series status word (tensor-core Gram: 8 = a wait ran out) */
 } ssa_gram_job;
+
+/* Weighted Gram of elementary reconstructions (n <= 64 rows of length m, time-contiguous, the
+ * W-correlation input) on the tensor cores: split-TF32 products with FP32 accumulation in TMEM
+ * per chunk of rows_per_cta time steps (a multiple of 32), FP64 partials in the same packed
+ * layout as ssad_gram. */
+int ssad_gram_tc(const ssa_gram_job *d_jobs, int njobs, int maxchunks, void *stream);
+/* Which W-correlation Gram the pipelines use: 1 = tensor cores (split TF32, default), 0 = FP64
+ * accumulation on the CUDA cores. The environment variable SSA_WCORR_FP64=1 sets 0 at load. */
+void ssad_set_wcorr_tc(int on);
+int ssad_wcorr_tc(void);
+/* Time steps per tensor-core W-Gram partial: chunks long enough to amortise a CTA's set-up. */
+#define SSA_TC_MIN_ROWS 1024
 
 /* Cholesky job: G = sum of the partials; G = R^T R with R upper triangular, written as fp32
  * n x n column-major (R[r][c] at R[r + c n], zeros below the diagonal). */

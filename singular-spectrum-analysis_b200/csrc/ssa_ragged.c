@@ -48,6 +48,7 @@ typedef struct
     int N, L, K, kp, k;
     long long ldL, ldK, ldN;
     int rows_L, rows_K, rows_N, nch_L, nch_K, nch_N, nq;
+    int rows_W, nch_W; /* W-correlation Gram chunks (tensor-core path: longer chunks) */
     size_t oY, oZ, opart, oqsum, oR, oZu, orecon, onorm, ospec;
     size_t ox, osig, oW, ogrp;
 } rser;
@@ -64,6 +65,7 @@ typedef struct
     float *X, *Y, *Z, *R, *Zu, *Zv, *recon, *Us;
     double *part, *qsum, *norm2;
     size_t sz[11]; /* bytes of X, Y, Z, part, qsum, R, Zu, Zv, recon, norm2, Us for the run */
+    int *status_base; /* the batch's status words (indexed by series) */
     cudaEvent_t done;
 } rbucket;
 
@@ -381,9 +383,10 @@ static int r_gram(rbucket *b, int side)
             J->ld = S->ldN;
             J->m = S->N;
             J->n = S->k;
-            J->rows_per_cta = S->rows_N;
+            J->rows_per_cta = S->rows_W;
             J->weighted = 1;
-            maxch = imax(maxch, S->nch_N);
+            J->status = b->status_base + S->src;
+            maxch = imax(maxch, S->nch_W);
         }
         J->part = b->part + S->opart;
         J->N = S->N;
@@ -395,7 +398,8 @@ static int r_gram(rbucket *b, int side)
     if (!d)
         return (int)cudaErrorMemoryAllocation;
     ssae_prof_begin(&b->e, SSAK_GRAM);
-    int rc = ssad_gram((const ssa_gram_job *)d, b->nb, maxch, side == SIDE_N, b->e.st);
+    int rc = (side == SIDE_N && ssad_wcorr_tc()) ? ssad_gram_tc((const ssa_gram_job *)d, b->nb, maxch, b->e.st)
+                                                 : ssad_gram((const ssa_gram_job *)d, b->nb, maxch, side == SIDE_N, b->e.st);
     ssae_prof_end(&b->e);
     return rc;
 }
@@ -595,7 +599,7 @@ static int r_wcorr(rbucket *b, double *W)
         const rser *S = &b->sd[i];
         jobs[i].part = b->part + S->opart;
         jobs[i].W = W + S->oW;
-        jobs[i].nchunks = S->nch_N;
+        jobs[i].nchunks = S->nch_W;
         jobs[i].k = S->k;
     }
     void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_wfin_job) * b->nb);
@@ -816,6 +820,8 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
             S->nch_L = (S->L + S->rows_L - 1) / S->rows_L;
             S->nch_K = (S->K + S->rows_K - 1) / S->rows_K;
             S->nch_N = (S->N + S->rows_N - 1) / S->rows_N;
+            S->rows_W = ssad_wcorr_tc() ? imax(S->rows_N, SSA_TC_MIN_ROWS) : S->rows_N;
+            S->nch_W = (S->N + S->rows_W - 1) / S->rows_W;
             S->nq = (S->L + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS;
             S->oY = oY;
             S->oZ = oZ;
@@ -957,6 +963,7 @@ static int run_enqueue(ssa_rbatch *rb, int B, const int *N, const int *L, const 
         rbucket *b = &rb->bk[g];
         if (!b->nb)
             continue;
+        b->status_base = rb->status;
         if (cudaStreamWaitEvent(b->e.st, rb->ev_in, 0) != cudaSuccess || bucket_run(b, rb, d_x, seed) != 0 ||
             cudaEventRecord(b->done, b->e.st) != cudaSuccess ||
             cudaStreamWaitEvent(rb->main, b->done, 0) != cudaSuccess)

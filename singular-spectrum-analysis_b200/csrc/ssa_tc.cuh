@@ -1,0 +1,243 @@
+// W-correlation Gram on the 5th-generation tensor cores (tcgen05, accumulators in TMEM).
+//
+// G = X diag(w) X^T for the k <= 64 elementary reconstructions X (k x N, component rows
+// contiguous in time) of one series, w_t = diagonal count. Each CTA (128 threads) owns one
+// (series, time chunk) and forms its chunk's partial Gram:
+//   - time tiles of 32 steps: X scaled by sqrt(w_t) is split in registers into TF32 parts
+//     hi = rna_tf32(x), lo = x - hi, written to shared memory in the canonical K-major layout
+//     without swizzle (8-row x 16-byte core matrices; LBO = next 16 bytes of K, SBO = next 8 rows);
+//   - A = [hi; lo] (M = 128 rows) and B = hi (N = 64 rows): one tcgen05.mma.kind::tf32 per 8 time
+//     steps accumulates both hi hi^T and lo hi^T in FP32 in TMEM (128 lanes x 64 columns);
+//   - two operand stages; one elected thread issues the MMAs and commits them to the stage's
+//     mbarrier, which the writers wait on before refilling the stage;
+//   - epilogue: tcgen05.ld of the accumulator, G_ij = HH_ij + LH_ij + LH_ji in FP64 (lo lo^T, of
+//     relative size 2^-22, is dropped), packed upper triangle into the chunk's partial slot (the
+//     layout k_gram writes, so k_wfin reduces either).
+// Every wait on an mbarrier is bounded; a wait that runs out records an error in the job's
+// status word and the kernel leaves after waiting (bounded) for its own MMAs, freeing TMEM.
+
+#define TC_THREADS 128
+#define TC_KT 32                                   // time steps per tile (K)
+#define TC_M 128                                   // A rows: 64 hi + 64 lo
+#define TC_N 64                                    // B rows (components)
+#define TC_A_LBO (TC_M / 8 * 128)                  // bytes between 16-byte K slices of A
+#define TC_B_LBO (TC_N / 8 * 128)
+#define TC_A_BYTES (TC_KT / 4 * TC_A_LBO)          // 16 KB
+#define TC_B_BYTES (TC_KT / 4 * TC_B_LBO)          // 8 KB
+#define TC_STAGE_BYTES (TC_A_BYTES + TC_B_BYTES)
+#define TC_SMEM (2 * TC_STAGE_BYTES)               // 48 KB; the epilogue reuses it
+#define TC_EPI_LD (TC_N + 1)
+#define TC_WAIT_LIMIT (1 << 22)
+
+__device__ __forceinline__ uint32_t tc_smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// UMMA shared-memory descriptor: K-major, no swizzle (layout type 0), version 1.
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// Instruction descriptor: D f32, A and B tf32, both K-major, N = 64, M = 128.
+__device__ __forceinline__ uint32_t tc_idesc() {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_N >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
+}
+
+__device__ __forceinline__ float tc_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void tc_mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc_smem_u32(bar)), "r"(count) : "memory");
+}
+
+// Bounded wait for completion of the phase with the given parity; false when the limit ran out.
+__device__ __forceinline__ bool tc_mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = tc_smem_u32(bar);
+    for (int it = 0; it < TC_WAIT_LIMIT; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (it > 64) __nanosleep(64);
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accum) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+        :
+        : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accum)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(tc_smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_ld8(uint32_t taddr, float* v) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Byte offset of element (row r, time j) of a K-major tile whose K slices are lbo bytes apart.
+__device__ __forceinline__ uint32_t tc_off(int r, int j, uint32_t lbo) {
+    return (uint32_t)(j >> 2) * lbo + (uint32_t)(r >> 3) * 128u + (uint32_t)(r & 7) * 16u + (uint32_t)(j & 3) * 4u;
+}
+
+__global__ void __launch_bounds__(TC_THREADS) k_gram_tc(const ssa_gram_job* __restrict__ jobs) {
+    extern __shared__ __align__(1024) unsigned char tsm[];
+    __shared__ __align__(8) uint64_t bar[3];
+    __shared__ uint32_t tmem_base;
+    __shared__ int failed;
+    const ssa_gram_job J = jobs[blockIdx.y];
+    const int chunk = blockIdx.x;
+    const int t_begin = chunk * J.rows_per_cta;
+    if (t_begin >= J.m) return;
+    const int t_end = min(J.m, t_begin + J.rows_per_cta);
+    const int n = J.n;
+    const int tid = threadIdx.x, warp = tid >> 5;
+
+    if (tid == 0) {
+        tc_mbar_init(&bar[0], 1);
+        tc_mbar_init(&bar[1], 1);
+        tc_mbar_init(&bar[2], 1);
+        failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem_u32(&tmem_base)),
+                     "r"(64)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base;
+    const uint32_t idesc = tc_idesc();
+
+    // each thread fills 16 consecutive time steps of one component row per tile
+    const int c = tid >> 1;
+    const int j0 = (tid & 1) * 16;
+    const float* xrow = J.A + (long long)c * J.ld;
+    const int ntiles = (t_end - t_begin + TC_KT - 1) / TC_KT;
+    bool ok = true;
+    for (int it = 0; it < ntiles; ++it) {
+        const int stage = it & 1;
+        unsigned char* sA = tsm + stage * TC_STAGE_BYTES;
+        unsigned char* sB = sA + TC_A_BYTES;
+        if (it >= 2 && !tc_mbar_wait(&bar[stage], ((it >> 1) - 1) & 1)) ok = false;
+        const int t0 = t_begin + it * TC_KT + j0;
+        float v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int t = t0 + q;
+            float x = 0.f;
+            if (c < n && t < t_end) x = xrow[t] * sqrtf((float)diag_count(t, J.N, J.L, J.K));
+            v[q] = x;
+        }
+#pragma unroll
+        for (int q4 = 0; q4 < 4; ++q4) {
+            float4 h, l;
+            h.x = tc_tf32(v[4 * q4 + 0]);
+            h.y = tc_tf32(v[4 * q4 + 1]);
+            h.z = tc_tf32(v[4 * q4 + 2]);
+            h.w = tc_tf32(v[4 * q4 + 3]);
+            l.x = v[4 * q4 + 0] - h.x;
+            l.y = v[4 * q4 + 1] - h.y;
+            l.z = v[4 * q4 + 2] - h.z;
+            l.w = v[4 * q4 + 3] - h.w;
+            const int j = j0 + 4 * q4;
+            *reinterpret_cast<float4*>(sA + tc_off(c, j, TC_A_LBO)) = h;
+            *reinterpret_cast<float4*>(sA + tc_off(c + 64, j, TC_A_LBO)) = l;
+            *reinterpret_cast<float4*>(sB + tc_off(c, j, TC_B_LBO)) = h;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a0 = tc_smem_u32(sA), b0 = tc_smem_u32(sB);
+#pragma unroll
+            for (int ks = 0; ks < TC_KT / 8; ++ks) {
+                const uint64_t da = tc_desc(a0 + ks * 2 * TC_A_LBO, TC_A_LBO, 128);
+                const uint64_t db = tc_desc(b0 + ks * 2 * TC_B_LBO, TC_B_LBO, 128);
+                tc_mma(tmem, da, db, idesc, (it > 0 || ks > 0) ? 1u : 0u);
+            }
+            tc_commit(&bar[stage]);
+        }
+    }
+    // the last tile's commit completes after every earlier MMA
+    if (ntiles > 0 && !tc_mbar_wait(&bar[(ntiles - 1) & 1], ((ntiles - 1) >> 1) & 1)) ok = false;
+    if (!ok) failed = 1;
+    __syncthreads();
+    if (failed && ntiles > 0) tc_mbar_wait(&bar[(ntiles - 1) & 1], ((ntiles - 1) >> 1) & 1);  // bounded
+    __syncthreads();
+    tc_fence_after();
+    float* epi = reinterpret_cast<float*>(tsm);  // 128 x TC_EPI_LD floats, over the idle stages
+    if (!failed && ntiles > 0) {
+        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+#pragma unroll
+        for (int cb = 0; cb < TC_N; cb += 8) {
+            float v[8];
+            tc_ld8(tmem + lane_base + (uint32_t)cb, v);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 8; ++q) epi[tid * TC_EPI_LD + cb + q] = v[q];
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64) : "memory");
+    if (failed) {
+        if (tid == 0 && J.status) atomicOr(J.status, 8);
+        if (tid == 0) check_fail(9, 1, (unsigned)chunk);
+        return;
+    }
+    double* part = J.part + (long long)chunk * (n * (n + 1) / 2);
+    const int np = n * (n + 1) / 2;
+    for (int e = tid; e < np; e += TC_THREADS) {
+        // e -> (i, j), i <= j, row-major packed upper triangle
+        int i = 0, rem = e;
+        while (rem >= n - i) {
+            rem -= n - i;
+            ++i;
+        }
+        const int j = i + rem;
+        double g = 0.0;
+        if (ntiles > 0)
+            g = (double)epi[i * TC_EPI_LD + j] + (double)epi[(64 + i) * TC_EPI_LD + j] +
+                (double)epi[(64 + j) * TC_EPI_LD + i];
+        part[pk_index(i, j, n)] = g;
+    }
+}
+
+// Launcher: one CTA per (chunk, job); chunks of rows_per_cta time steps (multiple of 32).
+static int launch_gram_tc(const ssa_gram_job* jobs, int njobs, int maxchunks, cudaStream_t st) {
+    cudaError_t e = cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+    if (e != cudaSuccess) return (int)e;
+    k_gram_tc<<<dim3(maxchunks, njobs), TC_THREADS, TC_SMEM, st>>>(jobs);
+    return launched(cudaGetLastError());
+}

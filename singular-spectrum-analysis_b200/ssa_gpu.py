@@ -110,6 +110,27 @@ _sig("ssa_batch_set_profiling", _I, ctypes.c_void_p, _I)
 _sig("ssa_batch_status", _I, ctypes.c_void_p, c_int_p, _I)
 _sig("ssa_batch_profile", _I, ctypes.c_void_p, c_double_p, ctypes.POINTER(ctypes.c_longlong), _I)
 
+_sig("ssa_b200_set_wcorr_tensor_cores", _V, _I)
+_sig("ssa_b200_wcorr_tensor_cores", _I)
+_sig("ssa_b200_device_checks", _I, ctypes.POINTER(ctypes.c_uint), _I)
+
+
+def set_wcorr_tensor_cores(on: bool) -> None:
+    """W-correlation Gram on the tensor cores (split TF32, default) or in FP64 on the CUDA cores."""
+    _lib.ssa_b200_set_wcorr_tensor_cores(1 if on else 0)
+
+
+def wcorr_tensor_cores() -> bool:
+    return bool(_lib.ssa_b200_wcorr_tensor_cores())
+
+
+def device_checks(reset: bool = True) -> List[int]:
+    """The kernels' self-check record: [count, kernel, block, code, value] (count 0 = clean)."""
+    out = (ctypes.c_uint * 5)()
+    _lib.ssa_b200_device_checks(out, 1 if reset else 0)
+    return list(out)
+
+
 PROFILE_KINDS = ("spectrum", "corr", "gram", "chol", "rowmul", "rr", "elem_recon", "wcorr_finish", "group_sum",
                  "recon", "lrf")
 

@@ -1,0 +1,74 @@
+"""W-correlation Gram on the tensor cores (tcgen05, split TF32, FP32 accumulation in TMEM)
+against the FP64 CUDA-core path and the FP64 oracle, in the single-series API, the uniform batch
+and the uneven batch.
+
+Tolerances: tensor-core vs FP64 path, max |W_tc - W_fp64| <= 5e-6 (the split keeps ~21 bits
+per product; partial sums run in FP32 over chunks of 1024+ time steps, ~sqrt(1024) 2^-24 = 2e-6
+relative, measured 2.1e-6 at most); against the
+oracle, the same bounds as the other parity tests (diagonal 1 within 1e-6, 1e-4 on the leading
+well-separated block); the kernels' self-check record stays clean.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    import ssa_gpu
+
+    yield ssa_gpu
+    ssa_gpu.set_wcorr_tensor_cores(True)
+
+
+def group_gap(sigma, i):
+    others = [abs(sigma[i] - sigma[j]) / sigma[i] for j in range(len(sigma)) if j != i]
+    return min(others) if others else np.inf
+
+
+def w_single(gpu, x, L, k, Om, tc):
+    gpu.set_wcorr_tensor_cores(tc)
+    s = gpu.SSA(x, L)
+    s.decompose(k, oversampling=10, power_iters=2, omega=Om)
+    return s.wcorr_matrix()
+
+
+@pytest.mark.parametrize("N,L,k", [(1000, 250, 50), (5000, 1250, 20), (20000, 5000, 64 - 10), (70000, 17500, 12)])
+def test_tc_wcorr_matches_fp64_and_oracle(gpu, oracle, N, L, k):
+    rng = np.random.default_rng(N)
+    x = oracle.walk_sines(rng, N)
+    K = N - L + 1
+    Om = rng.standard_normal((K, min(k + 10, L, K)))
+    gpu.device_checks(reset=True)
+    Wt = w_single(gpu, x, L, k, Om, True)
+    Wf = w_single(gpu, x, L, k, Om, False)
+    assert gpu.device_checks(reset=True)[0] == 0
+    assert np.max(np.abs(Wt - Wf)) <= 5e-6, np.max(np.abs(Wt - Wf))
+    d = oracle.decompose_randomized(x, L, k, 10, Om, q=2)
+    Wr = oracle.wcorr_matrix(d, N, L)
+    assert np.max(np.abs(np.diag(Wt) - 1.0)) < 1e-6
+    blk = [i for i in range(min(6, k)) if group_gap(d.sigma, i) > 1e-2]
+    if blk:
+        assert np.max(np.abs(Wt[np.ix_(blk, blk)] - Wr[np.ix_(blk, blk)])) < 1e-4
+
+
+def test_tc_wcorr_in_batches(gpu, oracle):
+    B, N, L, k = 8, 4000, 1000, 30
+    X = oracle.config2_batch(B, seed=11, N=N)
+    out = {}
+    for tc in (True, False):
+        gpu.set_wcorr_tensor_cores(tc)
+        ub = gpu.SSABatch(B, N, L, k, oversampling=10, power_iters=2)
+        s_u, W_u, G_u = ub.run(X, seed=5)
+        rb = gpu.SSARaggedBatch(oversampling=10, power_iters=2)
+        mix = oracle.config3_batch(6, seed=13, nmin=500, nmax=90000)
+        s_r, W_r, G_r = rb.run([m[0] for m in mix], [m[1] for m in mix], [m[2] for m in mix], seed=3)
+        out[tc] = (s_u, W_u, G_u, s_r, W_r, G_r)
+    a, b = out[True], out[False]
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[2], b[2])  # only W depends on the mode
+    assert np.max(np.abs(a[1] - b[1])) <= 5e-6
+    for s in range(len(a[4])):
+        assert np.array_equal(a[3][s], b[3][s])
+        assert np.max(np.abs(a[4][s] - b[4][s])) <= 5e-6, s
+    assert gpu.device_checks(reset=True)[0] == 0
