@@ -647,12 +647,13 @@ static int wgram_tc(ssa_engine *e, int nb, int k, int rows)
 {
     const int nchmax = imax(e->nch_L, imax(e->nch_K, e->nch_N));
     const size_t np = (size_t)e->kp * (e->kp + 1) / 2;
-    ssa_gram_job *jobs = (ssa_gram_job *)calloc((size_t)nb, sizeof(ssa_gram_job));
+    ssa_wgram_job *jobs = (ssa_wgram_job *)calloc((size_t)nb, sizeof(ssa_wgram_job));
     if (!jobs)
         return (int)cudaErrorMemoryAllocation;
     for (int s = 0; s < nb; s++)
     {
-        ssa_gram_job *J = &jobs[s];
+        ssa_gram_job *J = &jobs[s].g;
+        jobs[s].status = e->status + s;
         J->A = e->recon + (size_t)s * e->k * e->ldN;
         J->part = e->part + (size_t)s * nchmax * np;
         J->ld = e->ldN;
@@ -663,14 +664,13 @@ static int wgram_tc(ssa_engine *e, int nb, int k, int rows)
         J->N = e->N;
         J->L = e->L;
         J->K = e->K;
-        J->status = e->status + s;
     }
-    void *d = ssae_push_jobs(e, jobs, sizeof(ssa_gram_job) * nb);
+    void *d = ssae_push_jobs(e, jobs, sizeof(ssa_wgram_job) * nb);
     free(jobs);
     if (!d)
         return (int)cudaErrorMemoryAllocation;
     ssae_prof_begin(e, SSAK_GRAM);
-    int rc_ = ssad_gram_tc((const ssa_gram_job *)d, nb, (e->N + rows - 1) / rows, e->st);
+    int rc_ = ssad_gram_tc((const ssa_wgram_job *)d, nb, (e->N + rows - 1) / rows, e->st);
     ssae_prof_end(e);
     return rc_;
 }

@@ -1321,7 +1321,7 @@ extern "C" int ssad_wcorr_tc(void) {
     return g_wcorr_tc;
 }
 
-extern "C" int ssad_gram_tc(const ssa_gram_job* d_jobs, int njobs, int maxchunks, void* stream) {
+extern "C" int ssad_gram_tc(const ssa_wgram_job* d_jobs, int njobs, int maxchunks, void* stream) {
     if (njobs <= 0 || maxchunks <= 0) return 0;
     return launch_gram_tc(d_jobs, njobs, maxchunks, (cudaStream_t)stream);
 }

@@ -63,14 +63,21 @@ typedef struct
     int rows_per_cta;     /* rows folded into one partial (multiple of SSA_GRAM_CHUNK) */
     int weighted;         /* 1: row t weighted by min(t+1, L, K, N-t) */
     int N, L, K;
-    int *status;          /* optional series status word (tensor-core Gram: 8 = a wait ran out) */
 } ssa_gram_job;
+
+/* Tensor-core W-correlation Gram job: the Gram job plus the series status word (8 = a wait on
+ * the tensor cores ran out). */
+typedef struct
+{
+    ssa_gram_job g;
+    int *status;
+} ssa_wgram_job;
 
 /* Weighted Gram of elementary reconstructions (n <= 64 rows of length m, time-contiguous, the
  * W-correlation input) on the tensor cores: split-TF32 products with FP32 accumulation in TMEM
  * per chunk of rows_per_cta time steps (a multiple of 32), FP64 partials in the same packed
  * layout as ssad_gram. */
-int ssad_gram_tc(const ssa_gram_job *d_jobs, int njobs, int maxchunks, void *stream);
+int ssad_gram_tc(const ssa_wgram_job *d_jobs, int njobs, int maxchunks, void *stream);
 /* Which W-correlation Gram the pipelines use: 1 = tensor cores (split TF32, default), 0 = FP64
  * accumulation on the CUDA cores. The environment variable SSA_WCORR_FP64=1 sets 0 at load. */
 void ssad_set_wcorr_tc(int on);

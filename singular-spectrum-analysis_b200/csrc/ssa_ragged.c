@@ -351,9 +351,15 @@ enum
 
 static int r_gram(rbucket *b, int side)
 {
+    const int tc = side == SIDE_N && ssad_wcorr_tc();
     ssa_gram_job *jobs = (ssa_gram_job *)calloc((size_t)b->nb, sizeof(ssa_gram_job));
-    if (!jobs)
+    ssa_wgram_job *wjobs = tc ? (ssa_wgram_job *)calloc((size_t)b->nb, sizeof(ssa_wgram_job)) : NULL;
+    if (!jobs || (tc && !wjobs))
+    {
+        free(jobs);
+        free(wjobs);
         return (int)cudaErrorMemoryAllocation;
+    }
     int maxch = 0;
     for (int i = 0; i < b->nb; i++)
     {
@@ -385,21 +391,27 @@ static int r_gram(rbucket *b, int side)
             J->n = S->k;
             J->rows_per_cta = S->rows_W;
             J->weighted = 1;
-            J->status = b->status_base + S->src;
             maxch = imax(maxch, S->nch_W);
         }
         J->part = b->part + S->opart;
         J->N = S->N;
         J->L = S->L;
         J->K = S->K;
+        if (tc)
+        {
+            wjobs[i].g = *J;
+            wjobs[i].status = b->status_base + S->src;
+        }
     }
-    void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_gram_job) * b->nb);
+    void *d = tc ? ssae_push_jobs(&b->e, wjobs, sizeof(ssa_wgram_job) * b->nb)
+                 : ssae_push_jobs(&b->e, jobs, sizeof(ssa_gram_job) * b->nb);
     free(jobs);
+    free(wjobs);
     if (!d)
         return (int)cudaErrorMemoryAllocation;
     ssae_prof_begin(&b->e, SSAK_GRAM);
-    int rc = (side == SIDE_N && ssad_wcorr_tc()) ? ssad_gram_tc((const ssa_gram_job *)d, b->nb, maxch, b->e.st)
-                                                 : ssad_gram((const ssa_gram_job *)d, b->nb, maxch, side == SIDE_N, b->e.st);
+    int rc = tc ? ssad_gram_tc((const ssa_wgram_job *)d, b->nb, maxch, b->e.st)
+                : ssad_gram((const ssa_gram_job *)d, b->nb, maxch, side == SIDE_N, b->e.st);
     ssae_prof_end(&b->e);
     return rc;
 }

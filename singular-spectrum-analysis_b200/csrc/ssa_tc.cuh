@@ -106,12 +106,13 @@ __device__ __forceinline__ uint32_t tc_off(int r, int j, uint32_t lbo) {
     return (uint32_t)(j >> 2) * lbo + (uint32_t)(r >> 3) * 128u + (uint32_t)(r & 7) * 16u + (uint32_t)(j & 3) * 4u;
 }
 
-__global__ void __launch_bounds__(TC_THREADS) k_gram_tc(const ssa_gram_job* __restrict__ jobs) {
+__global__ void __launch_bounds__(TC_THREADS) k_gram_tc(const ssa_wgram_job* __restrict__ jobs) {
     extern __shared__ __align__(1024) unsigned char tsm[];
     __shared__ __align__(8) uint64_t bar[3];
     __shared__ uint32_t tmem_base;
     __shared__ int failed;
-    const ssa_gram_job J = jobs[blockIdx.y];
+    const ssa_gram_job J = jobs[blockIdx.y].g;
+    int* const status = jobs[blockIdx.y].status;
     const int chunk = blockIdx.x;
     const int t_begin = chunk * J.rows_per_cta;
     if (t_begin >= J.m) return;
@@ -138,26 +139,42 @@ __global__ void __launch_bounds__(TC_THREADS) k_gram_tc(const ssa_gram_job* __re
     const uint32_t tmem = tmem_base;
     const uint32_t idesc = tc_idesc();
 
-    // each thread fills 16 consecutive time steps of one component row per tile
+    // each thread fills 16 consecutive time steps of one component row per tile; the next tile's
+    // values are loaded while the tensor cores work on the current one
     const int c = tid >> 1;
     const int j0 = (tid & 1) * 16;
     const float* xrow = J.A + (long long)c * J.ld;
     const int ntiles = (t_end - t_begin + TC_KT - 1) / TC_KT;
+    float v[16];
+    auto load_tile = [&](int it) {
+        const int t0 = t_begin + it * TC_KT + j0;
+        if (c < n && t0 + 16 <= t_end) {
+            const float4* p4 = reinterpret_cast<const float4*>(xrow + t0);  // 16-byte aligned
+#pragma unroll
+            for (int q4 = 0; q4 < 4; ++q4) {
+                const float4 a = p4[q4];
+                v[4 * q4 + 0] = a.x;
+                v[4 * q4 + 1] = a.y;
+                v[4 * q4 + 2] = a.z;
+                v[4 * q4 + 3] = a.w;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 16; ++q) v[q] = (c < n && t0 + q < t_end) ? xrow[t0 + q] : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int t = min(t0 + q, J.N - 1);
+            v[q] *= sqrtf((float)diag_count(t, J.N, J.L, J.K));
+        }
+    };
     bool ok = true;
+    if (ntiles > 0) load_tile(0);
     for (int it = 0; it < ntiles; ++it) {
         const int stage = it & 1;
         unsigned char* sA = tsm + stage * TC_STAGE_BYTES;
         unsigned char* sB = sA + TC_A_BYTES;
         if (it >= 2 && !tc_mbar_wait(&bar[stage], ((it >> 1) - 1) & 1)) ok = false;
-        const int t0 = t_begin + it * TC_KT + j0;
-        float v[16];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const int t = t0 + q;
-            float x = 0.f;
-            if (c < n && t < t_end) x = xrow[t] * sqrtf((float)diag_count(t, J.N, J.L, J.K));
-            v[q] = x;
-        }
 #pragma unroll
         for (int q4 = 0; q4 < 4; ++q4) {
             float4 h, l;
@@ -188,6 +205,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_gram_tc(const ssa_gram_job* __re
             }
             tc_commit(&bar[stage]);
         }
+        if (it + 1 < ntiles) load_tile(it + 1);
     }
     // the last tile's commit completes after every earlier MMA
     if (ntiles > 0 && !tc_mbar_wait(&bar[(ntiles - 1) & 1], ((ntiles - 1) >> 1) & 1)) ok = false;
@@ -212,7 +230,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_gram_tc(const ssa_gram_job* __re
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64) : "memory");
     if (failed) {
-        if (tid == 0 && J.status) atomicOr(J.status, 8);
+        if (tid == 0 && status) atomicOr(status, 8);
         if (tid == 0) check_fail(9, 1, (unsigned)chunk);
         return;
     }
@@ -235,7 +253,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_gram_tc(const ssa_gram_job* __re
 }
 
 // Launcher: one CTA per (chunk, job); chunks of rows_per_cta time steps (multiple of 32).
-static int launch_gram_tc(const ssa_gram_job* jobs, int njobs, int maxchunks, cudaStream_t st) {
+static int launch_gram_tc(const ssa_wgram_job* jobs, int njobs, int maxchunks, cudaStream_t st) {
     cudaError_t e = cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
     if (e != cudaSuccess) return (int)e;
     k_gram_tc<<<dim3(maxchunks, njobs), TC_THREADS, TC_SMEM, st>>>(jobs);
