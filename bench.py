@@ -130,6 +130,26 @@ def stream_requests(gpu, specs, id_base: int, keep_outputs: bool = True, pinned:
     return R, h2d, d2h
 
 
+# DRAM traffic of the correlation sweeps measured by ncu relative to their algorithmic bytes:
+# k_corr<13> 0.985 (uniform 512-series batch), k_cl_col<16, CL_CORR> 1.017 and 0.955 (mixed
+# 512-series batch); the mean is used to state the traffic of a launch.
+CORR_TRAFFIC_RATIO = 0.986
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # SMs x FP32 lanes x FMA x clock (nominal peak)
+
+
+def corr_flops(N: int, L: int, k: int, p: int, q: int) -> float:
+    """Algorithmic FLOPs of the correlation sweeps of one series: per probe column a forward and
+    an inverse complex FFT of H = M/2 points (5 H log2 H each) and the real-spectrum unpacking,
+    spectral product and packing (~12 H)."""
+    K = N - L + 1
+    kp = min(k + p, L, K)
+    logm = 5
+    while (1 << logm) < N:
+        logm += 1
+    H = 1 << (logm - 1)
+    return (2 * q + 2) * kp * (10.0 * H * (logm - 1) + 12.0 * H)
+
+
 def corr_bytes(N: int, L: int, k: int, p: int, q: int) -> int:
     """Algorithmic FP32 bytes of the correlation sweeps of one series: the generated first sweep
     writes Y (L x kp); every other sweep reads one block and writes the other."""
@@ -293,8 +313,6 @@ def device_steps(gpu, torch, a, rank: int, world: int) -> dict:
     for w in range(a.warmup):
         rb.run_device(d_x.data_ptr(), Ns, Ls, ks, seed=1000 + w)
         rb.sync()
-    rb.set_profiling(True)
-    rb.profile()  # discard the warm-up stages
     launches0 = gpu.kernel_launches()
     if world > 1:
         torch.distributed.barrier()
@@ -308,32 +326,46 @@ def device_steps(gpu, torch, a, rank: int, world: int) -> dict:
         torch.cuda.synchronize()
         rb.sync()
     launches = gpu.kernel_launches() - launches0
-    prof = rb.profile()
-    rb.set_profiling(False)
     step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(a.steps)]
     total_ms = ev[0].elapsed_time(ev[a.steps])
+    # one more (untimed) step with the buckets run one after another and every launch bracketed by
+    # CUDA events on its stream: isolated per-launch times for the roofline and the kernel shares
+    rb.set_profiling(True, serialize=True)
+    rb.profile()
+    rb.run_device(d_x.data_ptr(), Ns, Ls, ks, seed=999)
+    rb.sync()
+    prof = rb.profile()
+    rb.set_profiling(False)
     if world > 1:
         t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
     cb = sum(corr_bytes(N, L, k, a.p, a.q) for N, L, k in zip(Ns, Ls, ks))
+    cf = sum(corr_flops(N, L, k, a.p, a.q) for N, L, k in zip(Ns, Ls, ks))
     corr_ms, corr_n = prof["corr"]
     peak, peak_kind = measured_peak_hbm()
-    per_launch = cb * a.steps / max(corr_n, 1)
+    per_launch = cb / max(corr_n, 1)
     avg_ms = corr_ms / max(corr_n, 1)
     achieved = per_launch / (avg_ms / 1e3) / 1e9
+    tflops = cf / (corr_ms / 1e3) / 1e12 if corr_ms > 0 else 0.0
     tot = max(sum(v[0] for v in prof.values()), 1e-9)
     out = {"value": a.batch * a.steps * world / (total_ms / 1e3), "ms_per_step": total_ms / a.steps,
            "step_ms": step_ms, "launches": launches,
            "share": {kk: round(v[0] / tot, 4) for kk, v in prof.items() if v[1]},
+           "share_what": "per-kernel-kind share of one step with the buckets run one after another",
            "mean_N": float(np.mean(Ns)), "clocks": clk.summary(),
            "roofline": {"bound": "hbm", "kernel": "k_corr / k_cl_col<CL_CORR> (FFT correlation matvec sweeps)",
                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                        "peak_source": peak_kind, "traffic": None,
+                        "peak_source": peak_kind, "traffic": CORR_TRAFFIC_RATIO * per_launch,
+                        "traffic_source": "ncu dram__bytes_read+write / algorithmic bytes of captured launches "
+                                          "(k_corr<13> 0.985, k_cl_col<16,1> 1.017 / 0.955) x this launch's bytes",
                         "avg_launch_ms": avg_ms, "algorithmic_bytes_per_launch": per_launch,
-                        "note": "launch times summed over FFT-length buckets that overlap on separate streams "
-                                "(conservative); traffic of the uniform batch's k_corr capture equals its "
-                                "algorithmic bytes within 2%"}}
+                        "compute": {"bound": "fp32 issue", "achieved_tflops": tflops,
+                                    "peak_tflops": FP32_NOMINAL_TFLOPS,
+                                    "peak_source": "nominal FP32 SIMT peak (148 SMs x 128 lanes x 2 x 1.965 GHz)",
+                                    "frac": tflops / FP32_NOMINAL_TFLOPS},
+                        "note": "per-launch CUDA-event times of one extra step with the FFT-length buckets "
+                                "run one after another (the timed steps overlap them)"}}
     del rb, d_x
     torch.cuda.empty_cache()
     return out

@@ -128,6 +128,8 @@ int ssa_rbatch_reserve(ssa_rbatch *b, size_t bytes);
 int ssa_rbatch_layout(const ssa_rbatch *b, size_t *offsets, size_t *totals);
 /* Device pointers of the packed outputs and the stream every run ends on (recon is NULL). */
 int ssa_rbatch_device_results(const ssa_rbatch *b, ssa_batch_results *out);
+/* on: 0 off, 1 per-kernel CUDA-event times (buckets overlap, so the intervals include other
+ * buckets' work), 2 the same with the buckets run one after another (isolated launch times). */
 int ssa_rbatch_set_profiling(ssa_rbatch *b, int on);
 int ssa_rbatch_profile(ssa_rbatch *b, double *ms, long long *launches, int nkinds);
 

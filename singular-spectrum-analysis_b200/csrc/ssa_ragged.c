@@ -969,17 +969,21 @@ static int run_enqueue(ssa_rbatch *rb, int B, const int *N, const int *L, const 
         cudaMemsetAsync(rb->lrf_status, 0, sizeof(int) * B, rb->main) != cudaSuccess ||
         cudaEventRecord(rb->ev_in, rb->main) != cudaSuccess)
         return -1;
-    /* largest FFT lengths first: they take longest */
+    /* largest FFT lengths first: they take longest. Profiling mode 2 chains the buckets (each
+     * waits for the previous one) so that every launch's event interval is its own. */
+    cudaEvent_t prev = rb->ev_in;
     for (int g = RB_NB - 1; g >= 0; g--)
     {
         rbucket *b = &rb->bk[g];
         if (!b->nb)
             continue;
         b->status_base = rb->status;
-        if (cudaStreamWaitEvent(b->e.st, rb->ev_in, 0) != cudaSuccess || bucket_run(b, rb, d_x, seed) != 0 ||
+        if (cudaStreamWaitEvent(b->e.st, rb->prof == 2 ? prev : rb->ev_in, 0) != cudaSuccess ||
+            bucket_run(b, rb, d_x, seed) != 0 ||
             cudaEventRecord(b->done, b->e.st) != cudaSuccess ||
             cudaStreamWaitEvent(rb->main, b->done, 0) != cudaSuccess)
             return -1;
+        prev = b->done;
     }
     return 0;
 }
@@ -1074,7 +1078,7 @@ int ssa_rbatch_device_results(const ssa_rbatch *rb, ssa_batch_results *out)
 
 int ssa_rbatch_set_profiling(ssa_rbatch *rb, int on)
 {
-    if (!rb)
+    if (!rb || on < 0 || on > 2)
         return -1;
     rb->prof = on;
     for (int g = 0; g < RB_NB; g++)

@@ -661,8 +661,11 @@ class SSARaggedBatch:
         if _lib.ssa_rbatch_sync(self._h) != 0:
             raise RuntimeError("a series of the uneven batch failed")
 
-    def set_profiling(self, on: bool) -> None:
-        if _lib.ssa_rbatch_set_profiling(self._h, 1 if on else 0) != 0:
+    def set_profiling(self, on, serialize: bool = False) -> None:
+        """Per-kernel CUDA-event times; with serialize=True the FFT-length buckets run one after
+        another so that each launch's interval is its own."""
+        mode = (2 if serialize else 1) if on else 0
+        if _lib.ssa_rbatch_set_profiling(self._h, mode) != 0:
             raise RuntimeError("ssa_rbatch_set_profiling failed")
 
     def profile(self) -> dict:

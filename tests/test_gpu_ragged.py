@@ -117,6 +117,26 @@ def test_alone_equals_in_mix(gpu, oracle):
             assert rel_l2(G1[s][gi], G[s][gi]) <= rec_tol(sig[s], g)
 
 
+def test_serialized_profiling_is_bit_identical(gpu, oracle):
+    """Profiling mode 2 only chains the FFT-length buckets on the streams: the same kernels on the
+    same data, so the outputs are bit-identical and every kernel kind reports launches."""
+    mix = oracle.config3_batch(12, seed=21, nmin=500, nmax=70000)
+    xs, Ls, ks = [m[0] for m in mix], [m[1] for m in mix], [m[2] for m in mix]
+    rb = gpu.SSARaggedBatch(oversampling=10, power_iters=2)
+    ref = rb.run(xs, Ls, ks, seed=8)
+    for serialize in (False, True):
+        rb.set_profiling(True, serialize=serialize)
+        rb.profile()
+        out = rb.run(xs, Ls, ks, seed=8)
+        prof = rb.profile()
+        rb.set_profiling(False)
+        for a, b in zip(out, ref):
+            for s in range(len(xs)):
+                assert np.array_equal(a[s], b[s]), s
+        assert prof["corr"][1] > 0 and prof["corr"][0] > 0
+    assert gpu._lib.ssa_rbatch_set_profiling(rb._h, 3) == -1  # unknown mode
+
+
 def test_uneven_batch_rejects_bad_series(gpu, oracle):
     rb = gpu.SSARaggedBatch()
     x = np.sin(np.arange(100.0)) + 0.1 * np.random.default_rng(1).standard_normal(100)
