@@ -114,28 +114,44 @@ __device__ __forceinline__ void cl_dc(const ClOp& op, float2& z0) {
     z0 = zk;
 }
 
+// Distributed shared memory through 32-bit shared::cluster addresses: the address of a slot in
+// CTA q's buffer is mapped on the fly, so no per-rank 64-bit pointers stay live in registers.
+__device__ __forceinline__ uint32_t cl_map(uint32_t local, int q) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(q));
+    return r;
+}
+__device__ __forceinline__ float2 cl_ld(uint32_t a) {
+    float2 v;
+    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a) : "memory");
+    return v;
+}
+__device__ __forceinline__ void cl_st(uint32_t a, float2 v) {
+    asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v.x), "f"(v.y) : "memory");
+}
+
 // Owner phase over this CTA's items: gather (unless CL_RECON), spectral operation, scatter
-// (unless CL_SPEC). rs[q] is CTA q's transform buffer.
+// (unless CL_SPEC). sbase is the shared-window address of this CTA's transform buffer; the
+// same offset in CTA q's window is CTA q's slot.
 template <int LOGH, int KIND>
-__device__ __forceinline__ void cl_exchange(float2* const* rs, const float2* twM, int rank, const ClOp& op) {
+__device__ __forceinline__ void cl_exchange(uint32_t sbase, const float2* twM, int rank, const ClOp& op) {
     using S = ClShape<LOGH>;
     constexpr int C = S::C, H1 = S::H1, H = S::H;
     for (int g = rank * S::BLOCK + (int)threadIdx.x; g < S::NITEM; g += C * S::BLOCK) {
         const int ka = g, kb = (H1 - g) & (H1 - 1);
         const bool self = ka == kb;  // k1 = 0 or H1/2
+        const uint32_t aa = sbase + 8u * (uint32_t)spad(ka), ab = sbase + 8u * (uint32_t)spad(kb);
         float2 za[C], zb[C];
         if constexpr (KIND != CL_RECON) {
 #pragma unroll
-            for (int q = 0; q < C; ++q) {
-                float2 v = rs[q][spad(ka)];
-                if (q > 0) v = cmul(v, twiddle<LOGH + 1, false>(twM, 2 * q * ka));
-                za[q] = v;
-            }
+            for (int q = 0; q < C; ++q) za[q] = cl_ld(cl_map(aa, q));
+#pragma unroll
+            for (int q = 1; q < C; ++q) za[q] = cmul(za[q], twiddle<LOGH + 1, false>(twM, 2 * q * ka));
             dftR<C, false>(za);
             if (!self) {
 #pragma unroll
                 for (int q = 0; q < C; ++q) {
-                    float2 v = rs[q][spad(kb)];
+                    float2 v = cl_ld(cl_map(ab, q));
                     if (q > 0) v = cmul(v, twiddle<LOGH + 1, false>(twM, 2 * q * kb));
                     zb[q] = v;
                 }
@@ -174,7 +190,7 @@ __device__ __forceinline__ void cl_exchange(float2* const* rs, const float2* twM
             for (int q = 0; q < C; ++q) {
                 float2 v = za[q];
                 if (q > 0) v = cmul(v, twiddle<LOGH + 1, true>(twM, 2 * q * ka));
-                rs[q][spad(ka)] = v;
+                cl_st(cl_map(aa, q), v);
             }
             if (!self) {
                 dftR<C, true>(zb);
@@ -182,43 +198,22 @@ __device__ __forceinline__ void cl_exchange(float2* const* rs, const float2* twM
                 for (int q = 0; q < C; ++q) {
                     float2 v = zb[q];
                     if (q > 0) v = cmul(v, twiddle<LOGH + 1, true>(twM, 2 * q * kb));
-                    rs[q][spad(kb)] = v;
+                    cl_st(cl_map(ab, q), v);
                 }
             }
         }
     }
 }
 
-// Decimated load of column c: z_r[m] = (a[2i], a[2i+1]) with i = C m + r.
-template <int LOGH>
-__device__ __forceinline__ void cl_load(float2* s, const float* f32, const double* f64, float sc, int n,
-                                        unsigned long long seed, int col, int rank) {
-    using S = ClShape<LOGH>;
-    for (int m = threadIdx.x; m < S::H1; m += blockDim.x) {
-        const int i = m * S::C + rank;
-        const int t = 2 * i;
-        float2 v = make_float2(0.f, 0.f);
-        if (t < n) {
-            if (f32) {
-                // t is even and columns start 16-byte aligned: one 8-byte load for the pair
-                if (t + 1 < n) {
-                    v = *reinterpret_cast<const float2*>(f32 + t);
-                    v.x *= sc;
-                    v.y *= sc;
-                } else {
-                    v.x = f32[t] * sc;
-                }
-            } else if (f64) {
-                v.x = (float)f64[t];
-                v.y = t + 1 < n ? (float)f64[t + 1] : 0.f;
-            } else {
-                v = gauss_pair(seed, col, i);
-                if (t + 1 >= n) v.y = 0.f;
-            }
-        }
-        s[spad(m)] = v;
-    }
-}
+// Decimated point access of CTA r: its local point m is the global packed point C m + r.
+template <int C, class P>
+struct ClDecim {
+    P p;
+    int rank;
+    static constexpr bool kSmem = false;
+    __device__ __forceinline__ float2 operator()(int m) const { return p(m * C + rank); }
+    __device__ __forceinline__ void operator()(int m, float2 v) const { p(m * C + rank, v); }
+};
 
 // Spectrum (CL_SPEC), correlation sweep (CL_CORR) and one-buffer elementary reconstruction
 // (CL_ELEM) on clusters; grid (C x columns, jobs), one cluster per column.
@@ -238,42 +233,26 @@ __global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, 2) k_cl_col(const ssa_co
     if (c >= J.ncols) return;  // the whole cluster shares c
     load_twiddles<S::LOGH1 + 1>(tw1);
     load_twiddles<LOGH + 1>(twM);
-    if constexpr (KIND == CL_ELEM) {
-        cl_load<LOGH>(s, J.in2 + (long long)c * J.ld_in2, nullptr, 1.0f, J.n_in2, 0, 0, rank);
-    } else {
-        const float sc = J.scale ? (float)J.scale[c] : 1.0f;
-        cl_load<LOGH>(s, J.in ? J.in + (long long)c * J.ld_in : nullptr,
-                      (!J.in && J.in64) ? J.in64 + (long long)c * J.ld_in : nullptr, sc, J.n_in, J.seed,
-                      J.col0 + c, rank);
-    }
-    __syncthreads();
-    fft_block<S::LOGH1, false>(s, tw1);
+    // the first pass of the local transform reads the decimated column from global memory
+    const ColPts in = KIND == CL_ELEM ? ColPts{J.in2 + (long long)c * J.ld_in2, nullptr, 1.0f, J.n_in2, 0, 0}
+                                      : col_pts(J, c);
+    fft_block_io<S::LOGH1, false>(s, ClDecim<S::C, ColPts>{in, rank}, SmemPts{s}, tw1);
     cl.sync();
-    float2* rs[S::C];
-#pragma unroll
-    for (int q = 0; q < S::C; ++q) rs[q] = cl.map_shared_rank(s, q);
     ClOp op;
     op.X = reinterpret_cast<const float2*>(J.X);
     op.spec = KIND == CL_SPEC ? reinterpret_cast<float2*>(J.spec + (long long)c * J.ld_spec) : nullptr;
     op.us = KIND == CL_ELEM ? reinterpret_cast<const float2*>(J.spec + (long long)c * J.ld_spec) : nullptr;
     op.R = nullptr;
-    cl_exchange<LOGH, KIND>(rs, twM, rank, op);
+    cl_exchange<LOGH, KIND>((uint32_t)__cvta_generic_to_shared(s), twM, rank, op);
     cl.sync();
     if constexpr (KIND == CL_SPEC) return;
-    fft_block<S::LOGH1, true>(s, tw1);
     const float inv_h = 1.0f / (float)S::H;
     if constexpr (KIND == CL_CORR) {
-        float* out = J.out + (long long)c * J.ld_out;
-        for (int m = threadIdx.x; m < S::H1; m += blockDim.x) {
-            const int t = 2 * (m * S::C + rank);
-            if (t >= J.n_out) continue;
-            const float2 z = s[spad(m)];
-            if (t + 1 < J.n_out)
-                *reinterpret_cast<float2*>(out + t) = make_float2(z.x * inv_h, z.y * inv_h);
-            else
-                out[t] = z.x * inv_h;
-        }
+        // the last pass of the local inverse transform writes the decimated output column
+        const RealOut out{J.out + (long long)c * J.ld_out, J.n_out, inv_h};
+        fft_block_io<S::LOGH1, true>(s, SmemPts{s}, ClDecim<S::C, RealOut>{out, rank}, tw1);
     } else {
+        fft_block<S::LOGH1, true>(s, tw1);
         const float sc = J.scale ? (float)J.scale[c] : 1.0f;
         const float* u = J.in + (long long)c * J.ld_in;
         const float* vv = J.in2 + (long long)c * J.ld_in2;
@@ -318,15 +297,12 @@ __global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, 2) k_cl_recon(const ssa_
     load_twiddles<LOGH + 1>(twM);
     __syncthreads();
     cl.sync();  // every CTA of the cluster is resident before the remote stores
-    float2* rs[S::C];
-#pragma unroll
-    for (int q = 0; q < S::C; ++q) rs[q] = cl.map_shared_rank(s, q);
     ClOp op;
     op.X = nullptr;
     op.spec = nullptr;
     op.us = nullptr;
     op.R = &J;
-    cl_exchange<LOGH, CL_RECON>(rs, twM, rank, op);
+    cl_exchange<LOGH, CL_RECON>((uint32_t)__cvta_generic_to_shared(s), twM, rank, op);
     cl.sync();
     fft_block<S::LOGH1, true>(s, tw1);
     const float inv_h = 1.0f / (float)S::H;

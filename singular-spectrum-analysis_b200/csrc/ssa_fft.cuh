@@ -185,9 +185,21 @@ struct FftShape {
     static constexpr int MINB = 1024 / BLOCK;
 };
 
+// Point access of a pass: the padded shared buffer, or (first / last pass only) a functor that
+// reads the input point z[i] from global memory / writes the output point z[i] there. A pass
+// that reads global memory needs no barrier before its shared stores, and one that writes
+// global memory needs none after them; a caller that reuses the buffer after a transform whose
+// last pass wrote global memory syncs first.
+struct SmemPts {
+    float2* s;
+    static constexpr bool kSmem = true;
+    __device__ __forceinline__ float2 operator()(int i) const { return s[spad(i)]; }
+    __device__ __forceinline__ void operator()(int i, float2 v) const { s[spad(i)] = v; }
+};
+
 // One Stockham pass of radix 2^RLOG after 2^LOGNS points have been combined.
-template <int RLOG, int LOGNS, int LOGH, bool INV>
-__device__ __forceinline__ void fft_pass(float2* s, const float2* tw, int tid) {
+template <int RLOG, int LOGNS, int LOGH, bool INV, class In, class Out>
+__device__ __forceinline__ void fft_pass(const In& in, const Out& out, const float2* tw, int tid) {
     constexpr int R = 1 << RLOG;
     constexpr int H = 1 << LOGH;
     constexpr int T = H / 16;
@@ -201,10 +213,10 @@ __device__ __forceinline__ void fft_pass(float2* s, const float2* tw, int tid) {
         for (int b = 0; b < NB; ++b) {
             const int j = tid + b * T;
 #pragma unroll
-            for (int r = 0; r < R; ++r) a[b * R + r] = s[spad(j + r * STR)];
+            for (int r = 0; r < R; ++r) a[b * R + r] = in(j + r * STR);
         }
     }
-    __syncthreads();
+    if constexpr (In::kSmem && Out::kSmem) __syncthreads();
     if (active) {
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
@@ -247,19 +259,22 @@ __device__ __forceinline__ void fft_pass(float2* s, const float2* tw, int tid) {
             dftR<R, INV>(a + b * R);
             const int base = (j - k) * R + k;
 #pragma unroll
-            for (int r = 0; r < R; ++r) s[spad(base + r * NS)] = a[b * R + r];
+            for (int r = 0; r < R; ++r) out(base + r * NS, a[b * R + r]);
         }
     }
-    __syncthreads();
+    if constexpr (Out::kSmem) __syncthreads();
 }
 
-template <int LOGH, bool INV, int LOGNS>
-__device__ __forceinline__ void fft_passes(float2* s, const float2* tw, int tid) {
-    if constexpr (LOGNS + 4 <= LOGH) {
-        fft_pass<4, LOGNS, LOGH, INV>(s, tw, tid);
-        fft_passes<LOGH, INV, LOGNS + 4>(s, tw, tid);
-    } else if constexpr (LOGNS < LOGH) {
-        fft_pass<LOGH - LOGNS, LOGNS, LOGH, INV>(s, tw, tid);
+// Passes from LOGNS on; the first one reads through `in`, the last one writes through `out`.
+template <int LOGH, bool INV, int LOGNS, class In, class Out>
+__device__ __forceinline__ void fft_passes(float2* s, const In& in, const Out& out, const float2* tw, int tid) {
+    const SmemPts sp{s};
+    constexpr int RLOG = (LOGNS + 4 <= LOGH) ? 4 : LOGH - LOGNS;
+    if constexpr (LOGNS + RLOG == LOGH) {
+        fft_pass<RLOG, LOGNS, LOGH, INV>(in, out, tw, tid);
+    } else {
+        fft_pass<RLOG, LOGNS, LOGH, INV>(in, sp, tw, tid);
+        fft_passes<LOGH, INV, LOGNS + RLOG>(s, sp, out, tw, tid);
     }
 }
 
@@ -268,7 +283,18 @@ __device__ __forceinline__ void fft_passes(float2* s, const float2* tw, int tid)
 // of the CTA; the caller syncs before (data and table in shared memory) and may read s after.
 template <int LOGH, bool INV>
 __device__ __forceinline__ void fft_block(float2* s, const float2* tw) {
-    fft_passes<LOGH, INV, 0>(s, tw, threadIdx.x);
+    const SmemPts sp{s};
+    fft_passes<LOGH, INV, 0>(s, sp, sp, tw, threadIdx.x);
+}
+
+// The same transform with the input points read by `in` (z[i], i < H) in the first pass and/or
+// the output points handed to `out` (i, Z[i]) by the last pass, so that a global load or store
+// is fused into the transform instead of a separate pass over the shared buffer. With a global
+// `in` the caller needs no barrier before the call for a twiddle table it filled: the first
+// pass uses no twiddles, and its closing barrier publishes the table to the later passes.
+template <int LOGH, bool INV, class In, class Out>
+__device__ __forceinline__ void fft_block_io(float2* s, const In& in, const Out& out, const float2* tw) {
+    fft_passes<LOGH, INV, 0>(s, in, out, tw, threadIdx.x);
 }
 
 // Load a real sequence a[0..n) (zero beyond n, up to M = 2H) into s as z[n] = a[2n] + i a[2n+1],

@@ -129,6 +129,70 @@ __host__ __device__ __forceinline__ int pk_index(int i, int j, int n) {  // i <=
 }
 
 // Load column `c` of job J into the packed buffer s (input, generated, or double signal).
+// Packed input point z[i] = (a[2i], a[2i+1]) of one column (zero from n on), read from global
+// memory by the first FFT pass: FP32 (times sc), FP64, or generated N(0,1) pairs.
+struct ColPts {
+    const float* f32;
+    const double* f64;
+    float sc;
+    int n;
+    unsigned long long seed;
+    int col;
+    static constexpr bool kSmem = false;
+    __device__ __forceinline__ float2 operator()(int i) const {
+        const int t = 2 * i;
+        float2 v = make_float2(0.f, 0.f);
+        if (t < n) {
+            if (f32) {
+                // columns start 8-byte aligned and t is even: one 8-byte load for the pair
+                if (t + 1 < n) {
+                    v = *reinterpret_cast<const float2*>(f32 + t);
+                    v.x *= sc;
+                    v.y *= sc;
+                } else {
+                    v.x = f32[t] * sc;
+                }
+            } else if (f64) {
+                v.x = (float)f64[t];
+                v.y = t + 1 < n ? (float)f64[t + 1] : 0.f;
+            } else {
+                v = gauss_pair(seed, col, i);
+                if (t + 1 >= n) v.y = 0.f;
+            }
+        }
+        return v;
+    }
+};
+
+// Input column c of a job: its FP32 column (scaled by scale[c]), else its FP64 column, else the
+// generated Gaussian test column col0 + c.
+__device__ __forceinline__ ColPts col_pts(const ssa_col_job& J, int c) {
+    ColPts p;
+    p.f32 = J.in ? J.in + (long long)c * J.ld_in : nullptr;
+    p.f64 = (!J.in && J.in64) ? J.in64 + (long long)c * J.ld_in : nullptr;
+    p.sc = (J.in && J.scale) ? (float)J.scale[c] : 1.0f;
+    p.n = J.n_in;
+    p.seed = J.seed;
+    p.col = J.col0 + c;
+    return p;
+}
+
+// Output point Z[i] written by the last FFT pass as the reals out[2i], out[2i+1] (times sc),
+// the first n reals only.
+struct RealOut {
+    float* out;
+    int n;
+    float sc;
+    static constexpr bool kSmem = false;
+    __device__ __forceinline__ void operator()(int i, float2 v) const {
+        const int t = 2 * i;
+        if (t + 1 < n)
+            *reinterpret_cast<float2*>(out + t) = make_float2(v.x * sc, v.y * sc);
+        else if (t < n)
+            out[t] = v.x * sc;
+    }
+};
+
 template <int LOGH>
 __device__ __forceinline__ void load_column(float2* s, const ssa_col_job& J, int c) {
     constexpr int H = 1 << LOGH;
@@ -173,9 +237,7 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k
     if (c >= J.ncols) return;
     float2* tw = smem + spad_size(H);
     load_twiddles<LOGH + 1>(tw);
-    load_column<LOGH>(smem, J, c);
-    __syncthreads();
-    fft_block<LOGH, false>(smem, tw);
+    fft_block_io<LOGH, false>(smem, col_pts(J, c), SmemPts{smem}, tw);
     float2* out = reinterpret_cast<float2*>(J.spec + (long long)c * J.ld_spec);
     for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
         if (k == 0) {
@@ -200,9 +262,7 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k
     if (c >= J.ncols) return;
     float2* tw = smem + spad_size(H);
     load_twiddles<LOGH + 1>(tw);
-    load_column<LOGH>(smem, J, c);
-    __syncthreads();
-    fft_block<LOGH, false>(smem, tw);
+    fft_block_io<LOGH, false>(smem, col_pts(J, c), SmemPts{smem}, tw);
     const float2* X = reinterpret_cast<const float2*>(J.X);
     for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
         float2 zk, zm;
@@ -224,8 +284,8 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k
         }
     }
     __syncthreads();
-    fft_block<LOGH, true>(smem, tw);
-    store_real<LOGH>(smem, J.out + (long long)c * J.ld_out, J.n_out, 1.0f / (float)H);
+    fft_block_io<LOGH, true>(smem, SmemPts{smem}, RealOut{J.out + (long long)c * J.ld_out, J.n_out, 1.0f / (float)H},
+                             tw);
 }
 
 // Elementary reconstruction of component c: x~[t] = inv_w[t] * (sigma_c u_c conv v_c)[t], and
@@ -243,11 +303,9 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_elem_recon(const ssa_
     if (c >= J.ncols) return;
     const float sc = J.scale ? (float)J.scale[c] : 1.0f;
     load_twiddles<LOGH + 1>(tw);
-    load_real<LOGH>(s1, J.in + (long long)c * J.ld_in, J.n_in, sc);
-    load_real<LOGH>(s2, J.in2 + (long long)c * J.ld_in2, J.n_in2, 1.0f);
-    __syncthreads();
-    fft_block<LOGH, false>(s1, tw);
-    fft_block<LOGH, false>(s2, tw);
+    fft_block_io<LOGH, false>(s1, ColPts{J.in + (long long)c * J.ld_in, nullptr, sc, J.n_in, 0, 0}, SmemPts{s1}, tw);
+    fft_block_io<LOGH, false>(s2, ColPts{J.in2 + (long long)c * J.ld_in2, nullptr, 1.0f, J.n_in2, 0, 0}, SmemPts{s2},
+                              tw);
     for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
         float2 zk, zm;
         if (k == 0) {
@@ -299,9 +357,8 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK) k_elem_recon1(const ssa
     const int c = blockIdx.x;
     if (c >= J.ncols) return;
     load_twiddles<LOGH + 1>(tw);
-    load_real<LOGH>(s2, J.in2 + (long long)c * J.ld_in2, J.n_in2, 1.0f);
-    __syncthreads();
-    fft_block<LOGH, false>(s2, tw);
+    fft_block_io<LOGH, false>(s2, ColPts{J.in2 + (long long)c * J.ld_in2, nullptr, 1.0f, J.n_in2, 0, 0}, SmemPts{s2},
+                              tw);
     const float2* us = reinterpret_cast<const float2*>(J.spec + (long long)c * J.ld_spec);
     for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
         float2 zk, zm;
