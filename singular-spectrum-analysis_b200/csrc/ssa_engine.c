@@ -101,7 +101,7 @@ int ssae_create(ssa_engine *e, int B, int N, int L, int kp, int k, cudaStream_t 
     r |= dmalloc((void **)&e->Z, Bs * e->ldK * kp * sizeof(float));
     r |= dmalloc((void **)&e->part, Bs * nchmax * np * sizeof(double));
     r |= dmalloc((void **)&e->qsum, Bs * e->nq * kp * sizeof(double));
-    r |= dmalloc((void **)&e->Rinv, Bs * kp * kp * sizeof(float));
+    r |= dmalloc((void **)&e->Rinv, Bs * kp * kp * sizeof(double));
     r |= dmalloc((void **)&e->Zu, Bs * kp * k * sizeof(float));
     r |= dmalloc((void **)&e->Zv, Bs * kp * k * sizeof(float));
     r |= dmalloc((void **)&e->sigma, Bs * k * sizeof(double));
@@ -477,7 +477,7 @@ static int chol(ssa_engine *e, int nb, int nch, int n)
     {
         ssa_chol_job *J = &jobs[s];
         J->part = e->part + (size_t)s * nchmax * np;
-        J->R = e->Rinv + (size_t)s * e->kp * e->kp;
+        J->Rinv = e->Rinv + (size_t)s * e->kp * e->kp;
         J->status = e->status + s;
         J->nchunks = nch;
         J->n = n;
@@ -492,10 +492,11 @@ static int chol(ssa_engine *e, int nb, int nch, int n)
     return rc_;
 }
 
-/* C_s = A_s * M_s for all series (M_s small, n x p, ld ldb, per-series stride mstride). */
+/* C_s = A_s * M_s for all series (M_s small, n x p, ld ldb, per-series stride mstride; FP32 Mm,
+ * or FP64 Mm64 when that is given). */
 static int rowmul(ssa_engine *e, int nb, const float *A, size_t astride, long long lda, int m, int n,
                   const float *Mm, size_t mstride, int ldb, int p, float *C, size_t cstride, long long ldc,
-                  double *colsum, int trsm)
+                  double *colsum, const double *Mm64)
 {
     ssa_rowmul_job *jobs = (ssa_rowmul_job *)calloc((size_t)nb, sizeof(ssa_rowmul_job));
     if (!jobs)
@@ -505,7 +506,8 @@ static int rowmul(ssa_engine *e, int nb, const float *A, size_t astride, long lo
     {
         ssa_rowmul_job *J = &jobs[s];
         J->A = A + (size_t)s * astride;
-        J->Bm = Mm + (size_t)s * mstride;
+        J->Bm = Mm64 ? NULL : Mm + (size_t)s * mstride;
+        J->Bm64 = Mm64 ? Mm64 + (size_t)s * mstride : NULL;
         J->C = C + (size_t)s * cstride;
         J->colsum = colsum ? colsum + (size_t)s * nqb * p : NULL;
         J->lda = lda;
@@ -514,7 +516,6 @@ static int rowmul(ssa_engine *e, int nb, const float *A, size_t astride, long lo
         J->n = n;
         J->p = p;
         J->ldb = ldb;
-        J->trsm = trsm;
     }
     void *d = ssae_push_jobs(e, jobs, sizeof(ssa_rowmul_job) * nb);
     free(jobs);
@@ -533,7 +534,7 @@ static int cholqr_pass(ssa_engine *e, int nb, float *A, size_t sstride, long lon
     const int nch = (m + rows - 1) / rows;
     CK(gram(e, nb, A, sstride, ld, m, n, rows, 0));
     CK(chol(e, nb, nch, n));
-    return rowmul(e, nb, A, sstride, ld, m, n, e->Rinv, (size_t)e->kp * e->kp, n, n, A, sstride, ld, colsum, 1);
+    return rowmul(e, nb, A, sstride, ld, m, n, NULL, (size_t)e->kp * e->kp, n, n, A, sstride, ld, colsum, e->Rinv);
 }
 
 int ssae_decompose(ssa_engine *e, int nb, int kp, int k, int q, const float *d_omega, long long omega_ld,
@@ -594,8 +595,8 @@ int ssae_decompose(ssa_engine *e, int nb, int kp, int k, int q, const float *d_o
         CK(rc_);
     }
     /* U = Q Zu (in place over Y), V = B Zv (in place over Z) */
-    CK(rowmul(e, nb, e->Y, sY, e->ldL, L, kp, e->Zu, (size_t)e->kp * e->k, kp, k, e->Y, sY, e->ldL, NULL, 0));
-    CK(rowmul(e, nb, e->Z, sZ, e->ldK, K, kp, e->Zv, (size_t)e->kp * e->k, kp, k, e->Z, sZ, e->ldK, NULL, 0));
+    CK(rowmul(e, nb, e->Y, sY, e->ldL, L, kp, e->Zu, (size_t)e->kp * e->k, kp, k, e->Y, sY, e->ldL, NULL, NULL));
+    CK(rowmul(e, nb, e->Z, sZ, e->ldK, K, kp, e->Zv, (size_t)e->kp * e->k, kp, k, e->Z, sZ, e->ldK, NULL, NULL));
     return 0;
 }
 
@@ -1011,13 +1012,13 @@ int ssae_decompose_block(ssa_engine *e, int nb, int k, int bsize, int max_iter, 
         }
         /* U[:, comp:comp+cb] = U_block Us */
         CK(rowmul(e, nb, Ub, sUb, e->ldL, L, cb, e->sUs, s64, cb, cb, e->Y + (size_t)comp * e->ldL, sY, e->ldL,
-                  NULL, 0));
+                  NULL, NULL));
         /* V_block = H^T U[:, comp:comp+cb] (deflated); V[:, comp:comp+cb] = V_block Sigma^{-1} */
         CK(corr_io(e, nb, cb, 1, e->Y + (size_t)comp * e->ldL, sY, e->ldL, Vb, sVb, e->ldK));
         if (comp > 0)
             CK(deflate(e, nb, Vb, sVb, e->ldK, cb, e->Z, sZ, e->ldK, comp, K, e->rows_K));
         CK(rowmul(e, nb, Vb, sVb, e->ldK, K, cb, e->sDinv, s64, cb, cb, e->Z + (size_t)comp * e->ldK, sZ, e->ldK,
-                  NULL, 0));
+                  NULL, NULL));
         comp += cb;
     }
     /* exchange sort by sigma and sign rule (MKL/ssa_opt.h:1896-1919) */
@@ -1122,7 +1123,7 @@ static int mssa_cholqr(ssa_engine *e, int M, int n, double *colsum)
     ssa_chol_job J;
     memset(&J, 0, sizeof(J));
     J.part = e->part;
-    J.R = e->Rinv;
+    J.Rinv = e->Rinv;
     J.status = e->status;
     J.nchunks = M * nch;
     J.n = n;
@@ -1133,7 +1134,7 @@ static int mssa_cholqr(ssa_engine *e, int M, int n, double *colsum)
     int rc = ssad_chol((const ssa_chol_job *)d, 1, e->st);
     ssae_prof_end(e);
     CK(rc);
-    return rowmul(e, M, e->Y, sY, e->ldL, e->L, n, e->Rinv, 0, n, n, e->Y, sY, e->ldL, colsum, 1);
+    return rowmul(e, M, e->Y, sY, e->ldL, e->L, n, NULL, 0, n, n, e->Y, sY, e->ldL, colsum, e->Rinv);
 }
 
 /* Z_0 = sum_m H_m^T Y_m (per-channel adjoints into Z_m, then a fixed-order channel sum). */
@@ -1193,8 +1194,8 @@ int ssae_mssa_decompose(ssa_engine *e, int M, int kp, int k, int q, const float 
         CK(rc);
     }
     /* U_m = Q_m Zu for every channel; V = B Zv into Z_0 */
-    CK(rowmul(e, M, e->Y, sY, e->ldL, e->L, kp, e->Zu, 0, kp, k, e->Y, sY, e->ldL, NULL, 0));
-    CK(rowmul(e, 1, e->Z, sZ, e->ldK, K, kp, e->Zv, 0, kp, k, e->Z, sZ, e->ldK, NULL, 0));
+    CK(rowmul(e, M, e->Y, sY, e->ldL, e->L, kp, e->Zu, 0, kp, k, e->Y, sY, e->ldL, NULL, NULL));
+    CK(rowmul(e, 1, e->Z, sZ, e->ldK, K, kp, e->Zv, 0, kp, k, e->Z, sZ, e->ldK, NULL, NULL));
     /* every channel's V slot gets V (the per-channel spectra of the reconstruction use them) */
     for (int m = 1; m < M; m++)
     {

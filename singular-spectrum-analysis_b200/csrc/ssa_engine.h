@@ -66,7 +66,7 @@ typedef struct
     float *Y, *Z;
     double *part;                /* B * max(nch) * kp(kp+1)/2 */
     double *qsum;                /* B * nq * kp */
-    float *Rinv;                 /* B * kp * kp */
+    double *Rinv;                /* B * kp * kp: R^{-1} of the last CholQR pass */
     float *Zu, *Zv;              /* B * kp * k */
     double *sigma;               /* B * k */
     int *status;                 /* B */

@@ -471,99 +471,143 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k
 
 #define GRAM_THREADS 128
 #define GSTR (SSA_GRAM_CHUNK + 1)
+// Column stride of the staged chunk ([col][row] floats): 132 = 4 (mod 32), so the fragment
+// loads of a warp (row 4s + t, column 8b + g for lane 4g + t) hit 32 distinct banks, and a
+// column starts 16-byte aligned for the 16-byte asynchronous copies.
+#define GRAM_S (SSA_GRAM_CHUNK + 4)
+#define GRAM_STAGE (SSA_MAX_KP * GRAM_S)
+#define GRAM_SMEM (2 * GRAM_STAGE * (int)sizeof(float))
 
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, int bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// D = A B + D for one 8x8 FP64 tile (FP64 tensor cores; lane 4g + t holds A[g][t], B[t][g],
+// D[g][2t], D[g][2t + 1]).
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// Stage rows [r0, r0 + SSA_GRAM_CHUNK) of columns [0, n) into buf ([col][row], stride GRAM_S);
+// rows at or beyond r_end are zero-filled (they belong to another CTA's partial or lie past m).
+__device__ __forceinline__ void gram_stage(uint32_t buf, const ssa_gram_job& J, int r0, int r_end, bool vec) {
+    if (vec) {
+        constexpr int Q = SSA_GRAM_CHUNK / 4;
+        for (int idx = threadIdx.x; idx < J.n * Q; idx += GRAM_THREADS) {
+            const int col = idx / Q, q = idx - col * Q;
+            const int r = r0 + 4 * q;
+            const int valid = min(4, max(0, r_end - r));
+            const float* src = valid > 0 ? J.A + (long long)r + (long long)col * J.ld : J.A;
+            cp_async16(buf + 4u * (uint32_t)(col * GRAM_S + 4 * q), src, 4 * valid);
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < J.n * SSA_GRAM_CHUNK; idx += GRAM_THREADS) {
+            const int col = idx / SSA_GRAM_CHUNK, q = idx - col * SSA_GRAM_CHUNK;
+            const int r = r0 + q;
+            const bool ok = r < r_end;
+            const float* src = ok ? J.A + (long long)r + (long long)col * J.ld : J.A;
+            cp_async4(buf + 4u * (uint32_t)(col * GRAM_S + q), src, ok ? 4 : 0);
+        }
+    }
+}
+
+// Gram partials on the FP64 tensor cores: part[chunk] = A_c^T W A_c over this CTA's rows, FP32
+// data, exact FP64 products (FP32 x FP32 x integer weight), FP64 accumulation. G is cut into
+// 8x8 tiles (nt = ceil(n/8) <= 8 per side); warp w owns the upper-triangle tiles of tile
+// columns w and nt - 1 - w (at most nt + 1 <= 9 tiles), so that the four warps share the work
+// evenly for nt = 7, 8. Chunks of SSA_GRAM_CHUNK rows are staged by asynchronous copies into
+// two buffers, the next one landing while the current one is multiplied.
 template <bool WEIGHTED>
 __global__ void __launch_bounds__(GRAM_THREADS) k_gram(const ssa_gram_job* __restrict__ jobs) {
-    // [col][row] with a padded column stride so that threads reading different columns at
-    // the same row hit different banks.
-    __shared__ float sA[SSA_MAX_KP * GSTR];
-    __shared__ float sw[SSA_GRAM_CHUNK];
+    extern __shared__ __align__(16) float gsm[];
     const ssa_gram_job J = jobs[blockIdx.y];
     const int chunk = blockIdx.x;
     const int r_begin = chunk * J.rows_per_cta;
     if (r_begin >= J.m) return;
     const int r_end = min(J.m, r_begin + J.rows_per_cta);
     const int n = J.n;
-    const int nb = (n + 3) >> 2;
-    const int ntiles = nb * (nb + 1) / 2;
-    // Tile assignment: this thread owns tiles t = tid, tid + 128, ...; at most 2 (n <= 64).
-    double acc[2][4][4];
-    int ti[2], tj[2];
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-        const int t = threadIdx.x + q * GRAM_THREADS;
-        ti[q] = -1;
-        tj[q] = -1;
-        if (t < ntiles) {
-            // upper-triangular tile index -> (bi, bj), bi <= bj
-            int bi = 0, rem = t;
-            while (rem >= nb - bi) {
-                rem -= nb - bi;
-                ++bi;
-            }
-            ti[q] = bi;
-            tj[q] = bi + rem;
-        }
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) acc[q][a][b] = 0.0;
+    const int nt = (n + 7) >> 3;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    // this warp's two tile columns (c2 = -1: none)
+    const int c1 = 2 * warp <= nt - 1 ? warp : -1;
+    const int c2 = (c1 >= 0 && nt - 1 - warp > warp) ? nt - 1 - warp : -1;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(gsm);
+    const bool vec = ((reinterpret_cast<uintptr_t>(J.A) & 15) == 0) && ((J.ld & 3) == 0);
+    // padding columns n .. 8 nt - 1 of both stages read as zeros
+    for (int idx = threadIdx.x; idx < (8 * nt - n) * SSA_GRAM_CHUNK; idx += GRAM_THREADS) {
+        const int col = n + idx / SSA_GRAM_CHUNK, q = idx % SSA_GRAM_CHUNK;
+        gsm[col * GRAM_S + q] = 0.f;
+        gsm[GRAM_STAGE + col * GRAM_S + q] = 0.f;
     }
+    double acc[9][2];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) acc[i][0] = acc[i][1] = 0.0;
     double csum = 0.0;
-    for (int r0 = r_begin; r0 < r_end; r0 += SSA_GRAM_CHUNK) {
-        const int rows = min(SSA_GRAM_CHUNK, r_end - r0);
+    const int nchunk = (r_end - r_begin + SSA_GRAM_CHUNK - 1) / SSA_GRAM_CHUNK;
+    gram_stage(sbase, J, r_begin, r_end, vec);
+    cp_async_commit();
+    for (int ic = 0; ic < nchunk; ++ic) {
+        const int r0 = r_begin + ic * SSA_GRAM_CHUNK;
+        if (ic + 1 < nchunk)
+            gram_stage(sbase + 4u * (uint32_t)(((ic + 1) & 1) * GRAM_STAGE), J, r0 + SSA_GRAM_CHUNK, r_end, vec);
+        cp_async_commit();
+        cp_async_wait<1>();
         __syncthreads();
-        for (int idx = threadIdx.x; idx < nb * 4 * SSA_GRAM_CHUNK; idx += GRAM_THREADS) {
-            const int col = idx / SSA_GRAM_CHUNK, r = idx % SSA_GRAM_CHUNK;
-            float v = 0.f;
-            if (col < n && r < rows) v = J.A[(long long)(r0 + r) + (long long)col * J.ld];
-            sA[col * GSTR + r] = v;
-        }
-        if (WEIGHTED) {
-            for (int r = threadIdx.x; r < SSA_GRAM_CHUNK; r += GRAM_THREADS)
-                sw[r] = r < rows ? (float)diag_count(r0 + r, J.N, J.L, J.K) : 0.f;
-        }
-        __syncthreads();
+        const float* sA = gsm + (ic & 1) * GRAM_STAGE;
         if (J.colsum && threadIdx.x < n) {
             double cs = 0.0;
-            for (int r = 0; r < rows; ++r) cs += (double)sA[threadIdx.x * GSTR + r];
+            for (int r = 0; r < SSA_GRAM_CHUNK; ++r) cs += (double)sA[threadIdx.x * GRAM_S + r];
             csum += cs;
         }
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            if (ti[q] < 0) continue;
-            const float* pa = sA + (ti[q] * 4) * GSTR;
-            const float* pb = sA + (tj[q] * 4) * GSTR;
-            for (int r = 0; r < rows; ++r) {
-                double a[4], b[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    a[u] = (double)pa[u * GSTR + r];
-                    b[u] = (double)pb[u * GSTR + r];
-                }
+        if (c1 >= 0) {
+            const float* pa = sA + g * GRAM_S + t;  // lane's element of tile column 0, k-step 0
+#pragma unroll 2
+            for (int s4 = 0; s4 < SSA_GRAM_CHUNK; s4 += 4) {
+                const float* row = pa + s4;
+                double b1 = (double)row[8 * c1 * GRAM_S];
+                double b2 = c2 >= 0 ? (double)row[8 * c2 * GRAM_S] : 0.0;
                 if (WEIGHTED) {
-                    const double w = (double)sw[r];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) b[u] *= w;
+                    const double w = (double)diag_count(r0 + s4 + t, J.N, J.L, J.K);
+                    b1 *= w;
+                    b2 *= w;
                 }
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) acc[q][u][v] = fma(a[u], b[v], acc[q][u][v]);
+                for (int i = 0; i < 9; ++i) {
+                    // tile i: (i, c1) for i <= c1, else (i - c1 - 1, c2)
+                    const bool first = i <= c1;
+                    const int bi = first ? i : i - c1 - 1;
+                    if (!first && (c2 < 0 || bi > c2)) continue;
+                    const double a = (double)row[8 * bi * GRAM_S];
+                    dmma_8x8x4(acc[i][0], acc[i][1], a, first ? b1 : b2);
+                }
             }
         }
+        __syncthreads();  // this stage is refilled two chunks later
     }
     double* part = J.part + (long long)chunk * (n * (n + 1) / 2);
+    if (c1 >= 0) {
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-        if (ti[q] < 0) continue;
+        for (int i = 0; i < 9; ++i) {
+            const bool first = i <= c1;
+            const int bi = first ? i : i - c1 - 1;
+            if (!first && (c2 < 0 || bi > c2)) continue;
+            const int row = 8 * bi + g;
+            const int cb = 8 * (first ? c1 : c2) + 2 * t;
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const int i = ti[q] * 4 + u, j = tj[q] * 4 + v;
-                if (i < n && j < n && i <= j) part[pk_index(i, j, n)] = acc[q][u][v];
+            for (int h = 0; h < 2; ++h) {
+                const int col = cb + h;
+                if (row < n && col < n && row <= col) part[pk_index(row, col, n)] = acc[i][h];
             }
+        }
     }
     if (J.colsum && threadIdx.x < n) J.colsum[(long long)chunk * n + threadIdx.x] = csum;
 }
@@ -644,6 +688,22 @@ __device__ void chol_upper_inplace(double* G, int n, double floor_) {
     __syncthreads();
 }
 
+// X = R^{-1} for the upper-triangular R in G (both column-major, ld SLD), by row sweeps from the
+// bottom: X[i][j] = (delta_ij - sum_{l=i+1..j} R[i][l] X[l][j]) / R[i][i]. Four threads per
+// column split each sum (blockDim.x = SMALL_THREADS = 256 covers n <= 64 columns).
+__device__ void tri_inv_upper(const double* G, double* X, int n) {
+    const int j = threadIdx.x >> 2, q = threadIdx.x & 3;
+    for (int i = n - 1; i >= 0; --i) {
+        double s = 0.0;
+        if (j < n && j > i)
+            for (int l = i + 1 + q; l <= j; l += 4) s = fma(G[l * SLD + i], X[j * SLD + l], s);
+        s += __shfl_xor_sync(0xffffffffu, s, 1);
+        s += __shfl_xor_sync(0xffffffffu, s, 2);
+        if (j < n && q == 0) X[j * SLD + i] = j >= i ? ((j == i ? 1.0 : 0.0) - s) / G[i * SLD + i] : 0.0;
+        __syncthreads();
+    }
+}
+
 __global__ void __launch_bounds__(SMALL_THREADS) k_chol(const ssa_chol_job* __restrict__ jobs) {
     extern __shared__ double dsm[];
     __shared__ double red[32];
@@ -658,98 +718,116 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_chol(const ssa_chol_job* __re
     }
     const double floor_ = dmax > 0.0 ? dmax * 1e-13 * (double)n : 1.0;
     chol_upper_inplace(G, n, floor_);
+    double* X = dsm + SSA_MAX_KP * SLD;
+    tri_inv_upper(G, X, n);
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int c = e / n, r = e - c * n;
-        J.R[e] = (float)G[c * SLD + r];
+        J.Rinv[e] = X[c * SLD + r];
     }
 }
 
 // ---------------------------------------------------------------------------------------------
-// Row-by-row product with a small matrix: C[i, :p] = A[i, :n] Bm
+// Row products with a small matrix: C = A Bm (or sub - A Bm), FP32 register tiles
 // ---------------------------------------------------------------------------------------------
 
-#define ROWMUL_THREADS SSA_ROWMUL_ROWS
+#define RM_THREADS 256
+#define RM_ROWS SSA_ROWMUL_ROWS
+// A block [col][row] (column stride 132: 16-byte aligned columns), Bm [k][j] (row stride 64).
+#define RM_SA (RM_ROWS + 4)
+#define RM_SMEM (SSA_MAX_KP * RM_SA * (int)sizeof(float) + SSA_MAX_KP * SSA_MAX_KP * (int)sizeof(float) + \
+                 (RM_THREADS / 32) * SSA_MAX_KP * (int)sizeof(double))
 
-__global__ void __launch_bounds__(ROWMUL_THREADS) k_rowmul(const ssa_rowmul_job* __restrict__ jobs) {
-    __shared__ __align__(16) float sB[SSA_MAX_KP * SSA_MAX_KP];
-    __shared__ float sInv[SSA_MAX_KP];
-    __shared__ double wsum[ROWMUL_THREADS / 32][SSA_MAX_KP];
+// One CTA per SSA_ROWMUL_ROWS rows: the rows of A (all n columns) land in shared memory by
+// asynchronous copies while Bm (FP32, or FP64 rounded to FP32) is staged beside them. Warp w
+// owns output columns [8 w, 8 w + 8) and lane l rows [4 l, 4 l + 4): per k one 16-byte load of
+// A (4 rows), two broadcast 16-byte loads of Bm (8 columns) and 32 FMAs. For an upper-triangular
+// Bm (R^{-1} of a CholQR pass) warp w stops at k = 8 w + 7, past which its columns are zero.
+__global__ void __launch_bounds__(RM_THREADS) k_rowmul(const ssa_rowmul_job* __restrict__ jobs) {
+    extern __shared__ __align__(16) unsigned char rsm[];
+    float* sA = reinterpret_cast<float*>(rsm);
+    float* sB = sA + SSA_MAX_KP * RM_SA;
+    double* wsum = reinterpret_cast<double*>(sB + SSA_MAX_KP * SSA_MAX_KP);
     const ssa_rowmul_job J = jobs[blockIdx.y];
     const int n = J.n, p = J.p;
-    if (blockIdx.x * ROWMUL_THREADS >= J.m) return;
-    for (int e = threadIdx.x; e < SSA_MAX_KP * p; e += blockDim.x) {
-        const int j = e / SSA_MAX_KP, l = e - j * SSA_MAX_KP;
-        sB[e] = l < n ? J.Bm[l + j * J.ldb] : 0.f;
+    const int r0 = blockIdx.x * RM_ROWS;
+    if (r0 >= J.m) return;
+    const int rows = min(RM_ROWS, J.m - r0);
+    const uint32_t abase = (uint32_t)__cvta_generic_to_shared(sA);
+    const bool vec = ((reinterpret_cast<uintptr_t>(J.A) & 15) == 0) && ((J.lda & 3) == 0);
+    if (vec) {
+        constexpr int Q = RM_ROWS / 4;
+        for (int idx = threadIdx.x; idx < n * Q; idx += RM_THREADS) {
+            const int col = idx / Q, r = 4 * (idx - col * Q);
+            const int valid = min(4, max(0, rows - r));
+            const float* src = valid > 0 ? J.A + (long long)(r0 + r) + (long long)col * J.lda : J.A;
+            cp_async16(abase + 4u * (uint32_t)(col * RM_SA + r), src, 4 * valid);
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < n * RM_ROWS; idx += RM_THREADS) {
+            const int col = idx / RM_ROWS, r = idx - col * RM_ROWS;
+            const bool ok = r < rows;
+            const float* src = ok ? J.A + (long long)(r0 + r) + (long long)col * J.lda : J.A;
+            cp_async4(abase + 4u * (uint32_t)(col * RM_SA + r), src, ok ? 4 : 0);
+        }
     }
-    if (J.trsm)
-        for (int j = threadIdx.x; j < SSA_MAX_KP; j += blockDim.x) sInv[j] = j < n ? 1.0f / J.Bm[j + j * J.ldb] : 0.f;
+    cp_async_commit();
+    for (int idx = threadIdx.x; idx < n * SSA_MAX_KP; idx += RM_THREADS) {
+        const int k = idx / SSA_MAX_KP, j = idx - k * SSA_MAX_KP;
+        float v = 0.f;
+        if (j < p) v = J.Bm64 ? (float)J.Bm64[k + (long long)j * J.ldb] : J.Bm[k + (long long)j * J.ldb];
+        sB[k * SSA_MAX_KP + j] = v;
+    }
+    cp_async_wait<0>();
     __syncthreads();
-    const int i = blockIdx.x * ROWMUL_THREADS + threadIdx.x;
-    const bool live = i < J.m;
-    float a[SSA_MAX_KP];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c0 = 8 * warp;  // this warp's columns
+    const int rl = 4 * lane;  // this lane's rows
+    float acc[4][8];
 #pragma unroll
-    for (int l = 0; l < SSA_MAX_KP; ++l)
-        a[l] = (live && l < n) ? J.A[(long long)i + (long long)l * J.lda] : 0.f;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (J.trsm) {
-        // x R = a, R upper: x_j = (a_j - sum_{l<j} x_l R[l][j]) / R[j][j]; a is overwritten by x
+    for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int j = 0; j < SSA_MAX_KP; ++j) {
-            if (j < n) {
-                const float* b = sB + j * SSA_MAX_KP;
-                float s0 = a[j], s1 = 0.f;
-                // float4 broadcast loads: one shared-memory wavefront feeds four FMAs per lane
+        for (int v = 0; v < 8; ++v) acc[u][v] = 0.f;
+    if (c0 < p) {
+        const int kend = J.Bm64 ? min(n, c0 + 8) : n;  // R^{-1} is upper triangular
+#pragma unroll 4
+        for (int k = 0; k < kend; ++k) {
+            const float4 a = *reinterpret_cast<const float4*>(sA + k * RM_SA + rl);
+            const float4 b0 = *reinterpret_cast<const float4*>(sB + k * SSA_MAX_KP + c0);
+            const float4 b1 = *reinterpret_cast<const float4*>(sB + k * SSA_MAX_KP + c0 + 4);
+            const float av[4] = {a.x, a.y, a.z, a.w};
+            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
-                for (int l = 0; l < (j & ~3); l += 4) {
-                    const float4 bv = *reinterpret_cast<const float4*>(b + l);
-                    s0 = fmaf(-a[l], bv.x, s0);
-                    s1 = fmaf(-a[l + 1], bv.y, s1);
-                    s0 = fmaf(-a[l + 2], bv.z, s0);
-                    s1 = fmaf(-a[l + 3], bv.w, s1);
-                }
+            for (int u = 0; u < 4; ++u)
 #pragma unroll
-                for (int l = (j & ~3); l < j; ++l) s0 = fmaf(-a[l], b[l], s0);
-                const float c = (s0 + s1) * sInv[j];
-                a[j] = c;
-                if (live) J.C[(long long)i + (long long)j * J.ldc] = c;  // subtract mode is GEMM-only
-                if (J.colsum) {
-                    double v = live ? (double)c : 0.0;
+                for (int v = 0; v < 8; ++v) acc[u][v] = fmaf(av[u], bv[v], acc[u][v]);
+        }
+    }
 #pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-                    if (lane == 0) wsum[warp][j] = v;
+    for (int v = 0; v < 8; ++v) {
+        const int col = c0 + v;
+        double cs = 0.0;
+        if (col < p) {
+            const long long cb = (long long)col * J.ldc;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int row = rl + u;
+                if (row < rows) {
+                    float x = acc[u][v];
+                    if (J.sub) x = J.sub[(long long)(r0 + row) + (long long)col * J.ldsub] - x;
+                    J.C[(long long)(r0 + row) + cb] = x;
+                    cs += (double)x;
                 }
             }
         }
-    } else {
-        for (int j = 0; j < p; ++j) {
-            const float* b = sB + j * SSA_MAX_KP;
-            float s0 = 0.f, s1 = 0.f;
+        if (J.colsum) {
 #pragma unroll
-            for (int l = 0; l < SSA_MAX_KP; l += 4) {
-                const float4 bv = *reinterpret_cast<const float4*>(b + l);
-                s0 = fmaf(a[l], bv.x, s0);
-                s1 = fmaf(a[l + 1], bv.y, s1);
-                s0 = fmaf(a[l + 2], bv.z, s0);
-                s1 = fmaf(a[l + 3], bv.w, s1);
-            }
-            float c = s0 + s1;
-            if (J.sub && live) c = J.sub[(long long)i + (long long)j * J.ldsub] - c;
-            if (live) J.C[(long long)i + (long long)j * J.ldc] = c;
-            if (J.colsum) {
-                double v = live ? (double)c : 0.0;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-                if (lane == 0) wsum[warp][j] = v;
-            }
+            for (int o = 16; o > 0; o >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, o);
+            if (lane == 0 && col < p) wsum[warp * SSA_MAX_KP + col] = cs;
         }
     }
     if (J.colsum) {
         __syncthreads();
-        for (int j = threadIdx.x; j < p; j += blockDim.x) {
-            double t = 0.0;
-            for (int w = 0; w < ROWMUL_THREADS / 32; ++w) t += wsum[w][j];
-            J.colsum[(long long)blockIdx.x * p + j] = t;
-        }
+        for (int j = threadIdx.x; j < p; j += RM_THREADS) J.colsum[(long long)blockIdx.x * p + j] = wsum[(j >> 3) * SSA_MAX_KP + j];
     }
 }
 
@@ -1434,10 +1512,12 @@ extern "C" int ssad_recon(const ssa_recon_job* d_jobs, int njobs, int logh, void
 extern "C" int ssad_gram(const ssa_gram_job* d_jobs, int njobs, int maxchunks, int weighted, void* stream) {
     if (njobs <= 0 || maxchunks <= 0) return 0;
     cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = weighted ? set_smem(k_gram<true>, GRAM_SMEM) : set_smem(k_gram<false>, GRAM_SMEM);
+    if (e != cudaSuccess) return (int)e;
     if (weighted)
-        k_gram<true><<<dim3(maxchunks, njobs), GRAM_THREADS, 0, st>>>(d_jobs);
+        k_gram<true><<<dim3(maxchunks, njobs), GRAM_THREADS, GRAM_SMEM, st>>>(d_jobs);
     else
-        k_gram<false><<<dim3(maxchunks, njobs), GRAM_THREADS, 0, st>>>(d_jobs);
+        k_gram<false><<<dim3(maxchunks, njobs), GRAM_THREADS, GRAM_SMEM, st>>>(d_jobs);
     return launched(cudaGetLastError());
 }
 
@@ -1452,8 +1532,9 @@ extern "C" int ssad_chol(const ssa_chol_job* d_jobs, int njobs, void* stream) {
 extern "C" int ssad_rowmul(const ssa_rowmul_job* d_jobs, int njobs, int maxrows, int maxn, void* stream) {
     if (njobs <= 0 || maxrows <= 0) return 0;
     if (maxn > SSA_MAX_KP) return (int)cudaErrorInvalidValue;
-    k_rowmul<<<dim3((maxrows + ROWMUL_THREADS - 1) / ROWMUL_THREADS, njobs), ROWMUL_THREADS, 0,
-               (cudaStream_t)stream>>>(d_jobs);
+    cudaError_t e = set_smem(k_rowmul, RM_SMEM);
+    if (e != cudaSuccess) return (int)e;
+    k_rowmul<<<dim3((maxrows + RM_ROWS - 1) / RM_ROWS, njobs), RM_THREADS, RM_SMEM, (cudaStream_t)stream>>>(d_jobs);
     return launched(cudaGetLastError());
 }
 

@@ -85,32 +85,32 @@ int ssad_wcorr_tc(void);
 /* Time steps per tensor-core W-Gram partial: chunks long enough to amortise a CTA's set-up. */
 #define SSA_TC_MIN_ROWS 1024
 
-/* Cholesky job: G = sum of the partials; G = R^T R with R upper triangular, written as fp32
- * n x n column-major (R[r][c] at R[r + c n], zeros below the diagonal). */
+/* Cholesky job: G = sum of the partials; G = R^T R with R upper triangular; writes R^{-1}
+ * (upper triangular, FP64) n x n column-major (X[r][c] at Rinv[r + c n], zeros below the
+ * diagonal). */
 typedef struct
 {
     const double *part;
-    float *R;
+    double *Rinv;
     int *status;          /* set to a nonzero code on failure (non-finite Gram) */
     int nchunks, n;
     int pad_[2];
 } ssa_chol_job;
 
-/* Row-by-row products with a small matrix (in place allowed: C == A, since every thread reads
- * its whole row of A before writing its row of C):
- *   trsm == 0: C[:, 0:p] = A[:, 0:n] * Bm[0:n, 0:p], or sub - A * Bm when sub != NULL;
- *   trsm == 1: C = A * Bm^{-1} for upper-triangular Bm (p == n), by forward substitution. */
+/* Row products with a small matrix, FP64 accumulation: C[:, 0:p] = A[:, 0:n] * Bm[0:n, 0:p], or
+ * sub - A * Bm when sub != NULL. In place allowed (C == A): a CTA reads all columns of its
+ * SSA_ROWMUL_ROWS rows before writing them. Bm is FP32 (Bm) or FP64 (Bm64, e.g. R^{-1} of a
+ * CholQR pass: Q = Y R^{-1}). */
 typedef struct
 {
     const float *A;
-    const float *Bm;      /* n x p col-major, ld = ldb */
+    const float *Bm;      /* n x p col-major, ld = ldb; NULL when Bm64 is given */
+    const double *Bm64;   /* n x p col-major, ld = ldb */
     float *C;
     double *colsum;       /* optional: per-CTA partial column sums of C, [blockIdx.x][p] */
     const float *sub;     /* optional: C = sub - A * Bm (sub may alias C), ld = ldsub */
     long long lda, ldc, ldsub;
     int m, n, p, ldb;
-    int trsm;
-    int pad_;
 } ssa_rowmul_job;
 
 /* Cross Gram partials: part[chunk][i * nb + j] = sum over the chunk's rows r of A[r][i] B[r][j]

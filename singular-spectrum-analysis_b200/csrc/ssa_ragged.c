@@ -14,7 +14,7 @@
  *   Z     [oZ]  ldK x kp       Z block, then B, then V
  *   part  [opart]              FP64 Gram partials, max(nch) * kp (kp + 1) / 2
  *   qsum  [oqsum] nq x kp      column-sum partials of the final Q (sign rule)
- *   R     [oR]  kp x kp        Cholesky factor of the last CholQR pass
+ *   R     [oR]  kp x kp        inverse Cholesky factor R^{-1} (FP64) of the last CholQR pass
  *   Zu/Zv [oZu] kp x k         Ritz rotations
  *   recon [orecon] k x ldN     elementary reconstructions
  *   norm2 [onorm] k
@@ -62,7 +62,8 @@ typedef struct
     int nb, cap_nb;
     rser *sd;
     /* views into the batch's device arena for the current run */
-    float *X, *Y, *Z, *R, *Zu, *Zv, *recon, *Us;
+    float *X, *Y, *Z, *Zu, *Zv, *recon, *Us;
+    double *R; /* R^{-1} of the last CholQR pass, FP64 */
     double *part, *qsum, *norm2;
     size_t sz[11]; /* bytes of X, Y, Z, part, qsum, R, Zu, Zv, recon, norm2, Us for the run */
     int *status_base; /* the batch's status words (indexed by series) */
@@ -426,7 +427,7 @@ static int r_chol(rbucket *b, int side, int *status)
         const rser *S = &b->sd[i];
         ssa_chol_job *J = &jobs[i];
         J->part = b->part + S->opart;
-        J->R = b->R + S->oR;
+        J->Rinv = b->R + S->oR;
         J->status = status + S->src;
         J->nchunks = side == SIDE_L ? S->nch_L : S->nch_K;
         J->n = S->kp;
@@ -465,9 +466,8 @@ static int r_rowmul(rbucket *b, int side, int trsm, int colsum)
         J->ldb = S->kp;
         if (trsm)
         {
-            J->Bm = b->R + S->oR;
+            J->Bm64 = b->R + S->oR;
             J->p = S->kp;
-            J->trsm = 1;
             J->colsum = colsum ? b->qsum + S->oqsum : NULL;
         }
         else
@@ -864,7 +864,7 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
         b->sz[2] = oZ * sizeof(float);
         b->sz[3] = opart * sizeof(double);
         b->sz[4] = oqsum * sizeof(double);
-        b->sz[5] = oR * sizeof(float);
+        b->sz[5] = oR * sizeof(double);
         b->sz[6] = oZu * sizeof(float);
         b->sz[7] = oZu * sizeof(float);
         b->sz[8] = orecon * sizeof(float);
@@ -908,7 +908,7 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
         RB_CARVE(v, b->sz[4]);
         b->qsum = (double *)v;
         RB_CARVE(v, b->sz[5]);
-        b->R = (float *)v;
+        b->R = (double *)v;
         RB_CARVE(v, b->sz[6]);
         b->Zu = (float *)v;
         RB_CARVE(v, b->sz[7]);
@@ -1190,7 +1190,7 @@ size_t ssar_series_bytes(int N, int L, int k, int p, int n_groups)
     b += 4 * (size_t)(round4(L) + round4(K)) * kp;               /* Y, Z */
     b += 8 * (size_t)nch * kp * (kp + 1) / 2;                    /* part */
     b += 8 * (size_t)((L + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS) * kp; /* qsum */
-    b += 4 * (size_t)kp * kp + 8 * (size_t)kp * k;               /* R, Zu, Zv */
+    b += 8 * (size_t)kp * kp + 8 * (size_t)kp * k;               /* R^{-1} (FP64), Zu, Zv */
     b += 4 * (size_t)k * round4(N) + 8 * (size_t)k;              /* recon, norm2 */
     if (logh > SSA_ELEM2_MAX_LOGH)
         b += 4 * (size_t)k * ldS;                                /* Us */
