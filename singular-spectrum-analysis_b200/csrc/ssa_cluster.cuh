@@ -130,6 +130,19 @@ __device__ __forceinline__ void cl_st(uint32_t a, float2 v) {
     asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v.x), "f"(v.y) : "memory");
 }
 
+// z[q] *= w^q (q = 1 .. C-1), or times conj(w)^q for the inverse; w^q by repeated products
+// (about q ulp each, as the powers inside the radix-16 passes).
+template <int C, bool INV>
+__device__ __forceinline__ void cl_twiddle(float2* z, float2 w) {
+    if (INV) w.y = -w.y;
+    float2 wq = w;
+#pragma unroll
+    for (int q = 1; q < C; ++q) {
+        z[q] = cmul(z[q], wq);
+        if (q + 1 < C) wq = cmul(wq, w);
+    }
+}
+
 // Owner phase over this CTA's items: gather (unless CL_RECON), spectral operation, scatter
 // (unless CL_SPEC). sbase is the shared-window address of this CTA's transform buffer; the
 // same offset in CTA q's window is CTA q's slot.
@@ -142,19 +155,19 @@ __device__ __forceinline__ void cl_exchange(uint32_t sbase, const float2* twM, i
         const bool self = ka == kb;  // k1 = 0 or H1/2
         const uint32_t aa = sbase + 8u * (uint32_t)spad(ka), ab = sbase + 8u * (uint32_t)spad(kb);
         float2 za[C], zb[C];
+        // W_H^{q k1} for q = 1 .. C-1 as powers of one table value (lanes read consecutive
+        // table entries; a lookup per power would stride the table by 2q entries)
+        const float2 wa = twiddle<LOGH + 1, false>(twM, 2 * ka);
+        const float2 wb = twiddle<LOGH + 1, false>(twM, 2 * kb);
         if constexpr (KIND != CL_RECON) {
 #pragma unroll
             for (int q = 0; q < C; ++q) za[q] = cl_ld(cl_map(aa, q));
-#pragma unroll
-            for (int q = 1; q < C; ++q) za[q] = cmul(za[q], twiddle<LOGH + 1, false>(twM, 2 * q * ka));
+            cl_twiddle<C, false>(za, wa);
             dftR<C, false>(za);
             if (!self) {
 #pragma unroll
-                for (int q = 0; q < C; ++q) {
-                    float2 v = cl_ld(cl_map(ab, q));
-                    if (q > 0) v = cmul(v, twiddle<LOGH + 1, false>(twM, 2 * q * kb));
-                    zb[q] = v;
-                }
+                for (int q = 0; q < C; ++q) zb[q] = cl_ld(cl_map(ab, q));
+                cl_twiddle<C, false>(zb, wb);
                 dftR<C, false>(zb);
             }
         } else {
@@ -186,20 +199,14 @@ __device__ __forceinline__ void cl_exchange(uint32_t sbase, const float2* twM, i
         }
         if constexpr (KIND != CL_SPEC) {
             dftR<C, true>(za);
+            cl_twiddle<C, true>(za, wa);
 #pragma unroll
-            for (int q = 0; q < C; ++q) {
-                float2 v = za[q];
-                if (q > 0) v = cmul(v, twiddle<LOGH + 1, true>(twM, 2 * q * ka));
-                cl_st(cl_map(aa, q), v);
-            }
+            for (int q = 0; q < C; ++q) cl_st(cl_map(aa, q), za[q]);
             if (!self) {
                 dftR<C, true>(zb);
+                cl_twiddle<C, true>(zb, wb);
 #pragma unroll
-                for (int q = 0; q < C; ++q) {
-                    float2 v = zb[q];
-                    if (q > 0) v = cmul(v, twiddle<LOGH + 1, true>(twM, 2 * q * kb));
-                    cl_st(cl_map(ab, q), v);
-                }
+                for (int q = 0; q < C; ++q) cl_st(cl_map(ab, q), zb[q]);
             }
         }
     }

@@ -852,56 +852,76 @@ __device__ __forceinline__ int rr_pos(int i, int step, int ne) {
 // memory): A <- A J with J a product of plane rotations accumulated into Z (initialised by the
 // caller), until every column pair is orthogonal to 4 sqrt(n) eps relative (rotations below the
 // rounding level of the dot products would otherwise never stop; LAPACK's one-sided Jacobi uses
-// sqrt(m) eps). Round-robin pairing
-// computed from the step number, one warp per pair, lanes own rows lane and lane + 32; one
-// barrier per step. On return nrm[c] = ||A[:, c]||. Called by every thread of the block.
+// sqrt(m) eps). Round-robin pairing computed from the step number; one half-warp per pair (so
+// the up to 32 pairs of a step run side by side in 16 warps), lanes own rows l, l + 16, l + 32,
+// l + 48; one barrier per step. The rotation angle follows Rutishauser's formula written as
+//   t = sign(zeta) |2 gamma| / (|beta - alpha| + sqrt((beta - alpha)^2 + 4 gamma^2)),
+//   zeta = (beta - alpha) / (2 gamma),   c = 1 / sqrt(1 + t^2),   s = c t,
+// which is the same t without the intermediate quotient. On return nrm[c] = ||A[:, c]||.
+// Called by every thread of the block.
 __device__ void onesided_jacobi(double* A, double* Z, int n, int* notconv, double* nrm) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int half = lane >> 4, l16 = lane & 15;
     const int ne = (n + 1) & ~1;  // even count; index n is a dummy when n is odd
     const int npairs = ne / 2;
     const double tiny = 1e-300;
     const double tol = 4.0 * sqrt((double)n) * 2.220446049250313e-16;
+    const double tol2 = tol * tol;
     for (int sweep = 0; sweep < 40; ++sweep) {
         if (threadIdx.x == 0) *notconv = 0;
         __syncthreads();
         for (int step = 0; step < ne - 1; ++step) {
-            for (int t = warp; t < npairs; t += nw) {
-                int p = rr_pos(t, step, ne), q = rr_pos(ne - 1 - t, step, ne);
-                if (q >= n || p >= n) continue;
+            // warp-uniform trip count: both halves of a warp run the same iterations
+            for (int t0 = 2 * warp; t0 < npairs; t0 += 2 * nw) {
+                const int t = t0 + half;
+                int p = t < npairs ? rr_pos(t, step, ne) : n;
+                int q = t < npairs ? rr_pos(ne - 1 - t, step, ne) : n;
                 if (p < 0 || q < 0) {
-                    if (lane == 0) check_fail(6, 6, (unsigned)(p * 1000 + q));
-                    continue;
+                    if (l16 == 0) check_fail(6, 6, (unsigned)(p * 1000 + q));
+                    p = q = n;
                 }
-                double* ap = A + p * SLD;
-                double* aq = A + q * SLD;
+                const bool live = p < n && q < n;
+                double* ap = A + (live ? p : 0) * SLD;
+                double* aq = A + (live ? q : 0) * SLD;
                 double al = 0.0, be = 0.0, ga = 0.0;
-                for (int r = lane; r < n; r += 32) {
-                    const double x = ap[r], y = aq[r];
-                    al = fma(x, x, al);
-                    be = fma(y, y, be);
-                    ga = fma(x, y, ga);
+                if (live) {
+#pragma unroll
+                    for (int i = 0; i < SSA_MAX_KP / 16; ++i) {
+                        const int r = l16 + 16 * i;
+                        if (r < n) {
+                            const double x = ap[r], y = aq[r];
+                            al = fma(x, x, al);
+                            be = fma(y, y, be);
+                            ga = fma(x, y, ga);
+                        }
+                    }
                 }
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
+                for (int o = 8; o > 0; o >>= 1) {
                     al += __shfl_xor_sync(0xffffffffu, al, o);
                     be += __shfl_xor_sync(0xffffffffu, be, o);
                     ga += __shfl_xor_sync(0xffffffffu, ga, o);
                 }
-                if (fabs(ga) > tiny && fabs(ga) > tol * sqrt(al * be)) {
-                    if (lane == 0) *notconv = 1;
-                    const double zeta = (be - al) / (2.0 * ga);
-                    const double tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-                    const double cs = 1.0 / sqrt(1.0 + tt * tt);
+                if (live && fabs(ga) > tiny && ga * ga > tol2 * (al * be)) {
+                    if (l16 == 0) *notconv = 1;
+                    const double d = be - al, g2 = 2.0 * ga;
+                    const double mag = fabs(g2) / (fabs(d) + sqrt(fma(d, d, g2 * g2)));
+                    const double tt = ((d >= 0.0) == (g2 >= 0.0) || d == 0.0) ? mag : -mag;
+                    const double cs = rsqrt(fma(tt, tt, 1.0));
                     const double sn = cs * tt;
                     double* zp = Z + p * SLD;
                     double* zq = Z + q * SLD;
-                    for (int r = lane; r < n; r += 32) {
-                        const double x = ap[r], y = aq[r];
-                        ap[r] = cs * x - sn * y;
-                        aq[r] = sn * x + cs * y;
-                        const double u = zp[r], v = zq[r];
-                        zp[r] = cs * u - sn * v;
-                        zq[r] = sn * u + cs * v;
+#pragma unroll
+                    for (int i = 0; i < SSA_MAX_KP / 16; ++i) {
+                        const int r = l16 + 16 * i;
+                        if (r < n) {
+                            const double x = ap[r], y = aq[r];
+                            ap[r] = cs * x - sn * y;
+                            aq[r] = sn * x + cs * y;
+                            const double u = zp[r], v = zq[r];
+                            zp[r] = cs * u - sn * v;
+                            zq[r] = sn * u + cs * v;
+                        }
                     }
                 }
             }
