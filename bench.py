@@ -304,6 +304,10 @@ def device_steps(gpu, torch, a, rank: int, world: int) -> dict:
     """Uneven-batch pipeline over `a.batch` stream decompositions with inputs resident in HBM."""
     rng = np.random.default_rng(a.seed + 7919 * (rank + 1))
     series = [make_series(rng, a.nmin, a.nmax) for _ in range(a.batch)]
+    # request type of each decomposition as in the stream (50 % reconstruct : 20 % W-correlation):
+    # W-correlation requests get W (all elementary reconstructions), reconstruct requests their
+    # groups [0], [1, 2]
+    want_w = rng.random(a.batch) < 2.0 / 7.0
     Ns = [len(x) for x, _, _ in series]
     Ls = [L for _, L, _ in series]
     ks = [k for _, _, k in series]
@@ -311,7 +315,7 @@ def device_steps(gpu, torch, a, rank: int, world: int) -> dict:
     rb = gpu.SSARaggedBatch(oversampling=a.p, power_iters=a.q, groups=[[0], [1, 2]])
     stream = torch.cuda.ExternalStream(rb.device_results()["stream"])
     for w in range(a.warmup):
-        rb.run_device(d_x.data_ptr(), Ns, Ls, ks, seed=1000 + w)
+        rb.run_device(d_x.data_ptr(), Ns, Ls, ks, seed=1000 + w, want_w=want_w)
         rb.sync()
     launches0 = gpu.kernel_launches()
     if world > 1:
@@ -321,7 +325,7 @@ def device_steps(gpu, torch, a, rank: int, world: int) -> dict:
     with ClockSampler(torch.cuda.current_device()) as clk:
         ev[0].record(stream)
         for i in range(a.steps):
-            rb.run_device(d_x.data_ptr(), Ns, Ls, ks, seed=i)
+            rb.run_device(d_x.data_ptr(), Ns, Ls, ks, seed=i, want_w=want_w)
             ev[i + 1].record(stream)
         torch.cuda.synchronize()
         rb.sync()
@@ -332,7 +336,7 @@ def device_steps(gpu, torch, a, rank: int, world: int) -> dict:
     # CUDA events on its stream: isolated per-launch times for the roofline and the kernel shares
     rb.set_profiling(True, serialize=True)
     rb.profile()
-    rb.run_device(d_x.data_ptr(), Ns, Ls, ks, seed=999)
+    rb.run_device(d_x.data_ptr(), Ns, Ls, ks, seed=999, want_w=want_w)
     rb.sync()
     prof = rb.profile()
     rb.set_profiling(False)
@@ -527,8 +531,10 @@ def main():
             "config": cfg, "gpu_launches": dev["launches"], "kernel_share": dev["share"],
             "roofline": dev["roofline"], "clocks": dev["clocks"],
             "value_what": f"series/s of the uneven-batch pipeline (ssa_rbatch_run_device) over {a.batch} stream "
-                          f"decompositions per step (mean N {dev['mean_N']:.0f}): decomposition, all elementary "
-                          "reconstructions, W-correlation, groups [0],[1,2]; inputs resident in HBM"}
+                          f"decompositions per step (mean N {dev['mean_N']:.0f}), each with the outputs of its "
+                          "request type in the stream's 50:20 ratio: decompose + reconstruct -> sigma and groups "
+                          "[0],[1,2]; decompose + W-correlation -> sigma, all elementary reconstructions and W "
+                          "(and the groups); inputs resident in HBM"}
     if not a.no_e2e:
         line.update(server_runs(ssa_gpu, torch, a, rank, world))
     if rank == 0 and world == 1 and not a.no_plain:

@@ -121,6 +121,15 @@ int ssa_rbatch_run(ssa_rbatch *b, int B, const int *N, const int *L, const int *
 /* d_x in device memory; enqueues only (ssa_rbatch_sync waits and checks every series). */
 int ssa_rbatch_run_device(ssa_rbatch *b, int B, const int *N, const int *L, const int *k, const double *d_x,
                           uint64_t seed);
+/* The same runs with per-series outputs: want_w[i] = 1 computes the W-correlation of series i
+ * (and all k elementary reconstructions it needs); 0 skips it, computes only the elementary
+ * reconstructions of the components the groups name, and leaves that series' W block zero.
+ * want_w == NULL is the plain run (W for every series). A request that only asks for grouped
+ * reconstructions (the reference's decompose + reconstruct) then costs no W-correlation work. */
+int ssa_rbatch_run_ex(ssa_rbatch *b, int B, const int *N, const int *L, const int *k, const double *x,
+                      uint64_t seed, double *sigma, double *W, double *groups, const unsigned char *want_w);
+int ssa_rbatch_run_device_ex(ssa_rbatch *b, int B, const int *N, const int *L, const int *k, const double *d_x,
+                             uint64_t seed, const unsigned char *want_w);
 int ssa_rbatch_sync(ssa_rbatch *b);
 /* Every buffer of a run lives in one device arena, grown in stream order when a run needs more;
  * reserving it up front keeps growth (and the driver allocation behind it) out of later runs. */

@@ -49,6 +49,8 @@ typedef struct
     long long ldL, ldK, ldN;
     int rows_L, rows_K, rows_N, nch_L, nch_K, nch_N, nq;
     int rows_W, nch_W; /* W-correlation Gram chunks (tensor-core path: longer chunks) */
+    int wantW;         /* W-correlation requested for this series */
+    int nelem;         /* elementary reconstructions computed: k with W, else those the groups use */
     size_t oY, oZ, opart, oqsum, oR, oZu, orecon, onorm, ospec;
     size_t ox, osig, oW, ogrp;
 } rser;
@@ -73,6 +75,7 @@ typedef struct
 struct ssa_rbatch
 {
     int p, q, n_groups, total_idx;
+    int grp_need; /* highest component index named by a group, plus one */
     int *d_gidx, *d_goff;
     rbucket bk[RB_NB];
     cudaStream_t main;
@@ -91,6 +94,7 @@ struct ssa_rbatch
     /* optional per-run extensions (ssar_run_enqueue_ex) */
     const unsigned long long *cur_seeds; /* per-series generator seeds, or NULL */
     double *const *cur_lrf;              /* per-series LRF destinations, or NULL */
+    const unsigned char *cur_wmask;      /* per-series "W-correlation wanted", or NULL = all */
     int lrf_slot, n_lrf_group, lrf_gmax;
     int *d_lrf_group;
     int *lrf_status;
@@ -223,6 +227,8 @@ int ssa_rbatch_create(ssa_rbatch **out, int oversampling, int power_iters, const
         for (int g = 0; g < n_groups; g++)
             off[g + 1] = off[g] + (group_sizes[g] > 0 ? group_sizes[g] : 0);
         rb->total_idx = off[n_groups];
+        for (int i = 0; i < rb->total_idx; i++)
+            rb->grp_need = imax(rb->grp_need, group_idx[i] + 1);
         int rc = cudaMalloc((void **)&rb->d_goff, sizeof(int) * (n_groups + 1)) != cudaSuccess;
         rc |= cudaMalloc((void **)&rb->d_gidx, sizeof(int) * (rb->total_idx > 0 ? rb->total_idx : 1)) != cudaSuccess;
         if (!rc)
@@ -361,11 +367,13 @@ static int r_gram(rbucket *b, int side)
         free(wjobs);
         return (int)cudaErrorMemoryAllocation;
     }
-    int maxch = 0;
+    int maxch = 0, nj = 0;
     for (int i = 0; i < b->nb; i++)
     {
         const rser *S = &b->sd[i];
-        ssa_gram_job *J = &jobs[i];
+        if (side == SIDE_N && !S->wantW)
+            continue;
+        ssa_gram_job *J = &jobs[nj];
         if (side == SIDE_L)
         {
             J->A = b->Y + S->oY;
@@ -400,19 +408,26 @@ static int r_gram(rbucket *b, int side)
         J->K = S->K;
         if (tc)
         {
-            wjobs[i].g = *J;
-            wjobs[i].status = b->status_base + S->src;
+            wjobs[nj].g = *J;
+            wjobs[nj].status = b->status_base + S->src;
         }
+        nj++;
     }
-    void *d = tc ? ssae_push_jobs(&b->e, wjobs, sizeof(ssa_wgram_job) * b->nb)
-                 : ssae_push_jobs(&b->e, jobs, sizeof(ssa_gram_job) * b->nb);
+    if (nj == 0)
+    {
+        free(jobs);
+        free(wjobs);
+        return 0;
+    }
+    void *d = tc ? ssae_push_jobs(&b->e, wjobs, sizeof(ssa_wgram_job) * nj)
+                 : ssae_push_jobs(&b->e, jobs, sizeof(ssa_gram_job) * nj);
     free(jobs);
     free(wjobs);
     if (!d)
         return (int)cudaErrorMemoryAllocation;
     ssae_prof_begin(&b->e, SSAK_GRAM);
-    int rc = tc ? ssad_gram_tc((const ssa_wgram_job *)d, b->nb, maxch, b->e.st)
-                : ssad_gram((const ssa_gram_job *)d, b->nb, maxch, side == SIDE_N, b->e.st);
+    int rc = tc ? ssad_gram_tc((const ssa_wgram_job *)d, nj, maxch, b->e.st)
+                : ssad_gram((const ssa_gram_job *)d, nj, maxch, side == SIDE_N, b->e.st);
     ssae_prof_end(&b->e);
     return rc;
 }
@@ -545,8 +560,13 @@ static int r_elem(rbucket *b, const double *sigma)
             J->scale = sigma + S->osig;
             J->spec = b->Us + S->ospec;
             J->ld_spec = b->ldS;
-            J->ncols = S->k;
-            maxk = imax(maxk, S->k);
+            J->ncols = S->nelem;
+            maxk = imax(maxk, S->nelem);
+        }
+        if (maxk == 0)
+        {
+            free(jobs);
+            return 0;
         }
         void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_col_job) * b->nb);
         if (!d)
@@ -578,7 +598,7 @@ static int r_elem(rbucket *b, const double *sigma)
         J->out = b->recon + S->orecon;
         J->ld_out = S->ldN;
         J->norm2 = b->norm2 + S->onorm;
-        J->ncols = S->k;
+        J->ncols = S->nelem;
         J->N = S->N;
         J->L = S->L;
         J->K = S->K;
@@ -587,7 +607,12 @@ static int r_elem(rbucket *b, const double *sigma)
             J->spec = b->Us + S->ospec;
             J->ld_spec = b->ldS;
         }
-        maxk = imax(maxk, S->k);
+        maxk = imax(maxk, S->nelem);
+    }
+    if (maxk == 0)
+    {
+        free(jobs);
+        return 0;
     }
     void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_col_job) * b->nb);
     free(jobs);
@@ -606,20 +631,29 @@ static int r_wcorr(rbucket *b, double *W)
     ssa_wfin_job *jobs = (ssa_wfin_job *)calloc((size_t)b->nb, sizeof(ssa_wfin_job));
     if (!jobs)
         return (int)cudaErrorMemoryAllocation;
+    int nj = 0;
     for (int i = 0; i < b->nb; i++)
     {
         const rser *S = &b->sd[i];
-        jobs[i].part = b->part + S->opart;
-        jobs[i].W = W + S->oW;
-        jobs[i].nchunks = S->nch_W;
-        jobs[i].k = S->k;
+        if (!S->wantW)
+            continue;
+        jobs[nj].part = b->part + S->opart;
+        jobs[nj].W = W + S->oW;
+        jobs[nj].nchunks = S->nch_W;
+        jobs[nj].k = S->k;
+        nj++;
     }
-    void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_wfin_job) * b->nb);
+    if (nj == 0)
+    {
+        free(jobs);
+        return 0;
+    }
+    void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_wfin_job) * nj);
     free(jobs);
     if (!d)
         return (int)cudaErrorMemoryAllocation;
     ssae_prof_begin(&b->e, SSAK_WFIN);
-    int rc = ssad_wfin((const ssa_wfin_job *)d, b->nb, b->e.st);
+    int rc = ssad_wfin((const ssa_wfin_job *)d, nj, b->e.st);
     ssae_prof_end(&b->e);
     return rc;
 }
@@ -637,7 +671,7 @@ static int r_gsum(rbucket *b, ssa_rbatch *rb)
         jobs[i].ld_recon = S->ldN;
         jobs[i].out = rb->groups + S->ogrp;
         jobs[i].N = S->N;
-        jobs[i].k = S->k;
+        jobs[i].k = S->nelem; /* covers every grouped component below k */
         maxN = imax(maxN, S->N);
     }
     void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_rgsum_job) * b->nb);
@@ -835,6 +869,8 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
             S->rows_W = ssad_wcorr_tc() ? imax(S->rows_N, SSA_TC_MIN_ROWS) : S->rows_N;
             S->nch_W = (S->N + S->rows_W - 1) / S->rows_W;
             S->nq = (S->L + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS;
+            S->wantW = !rb->cur_wmask || rb->cur_wmask[S->src];
+            S->nelem = S->wantW ? S->k : imin(S->k, rb->grp_need);
             S->oY = oY;
             S->oZ = oZ;
             S->opart = opart;
@@ -850,9 +886,9 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
             oqsum += (size_t)S->nq * S->kp;
             oR += (size_t)S->kp * S->kp;
             oZu += (size_t)S->kp * S->k;
-            orecon += (size_t)S->k * S->ldN;
+            orecon += (size_t)S->nelem * S->ldN;
             onorm += (size_t)S->k;
-            ospec += (size_t)S->k * b->ldS;
+            ospec += (size_t)S->nelem * b->ldS;
         }
         /* one run pushes 13 + 6 q job tables of at most sizeof(ssa_col_job) bytes per series,
          * each 16-byte aligned */
@@ -965,6 +1001,9 @@ static int run_enqueue(ssa_rbatch *rb, int B, const int *N, const int *L, const 
     if (ensure_hoff(rb, B) != 0 || plan(rb, B, N, L, k) != 0)
         return -1;
     rb->B = B;
+    if (rb->cur_wmask && rb->n_W > 0 &&
+        cudaMemsetAsync(rb->W, 0, sizeof(double) * rb->n_W, rb->main) != cudaSuccess)
+        return -1;
     if (cudaMemsetAsync(rb->status, 0, sizeof(int) * B, rb->main) != cudaSuccess ||
         cudaMemsetAsync(rb->lrf_status, 0, sizeof(int) * B, rb->main) != cudaSuccess ||
         cudaEventRecord(rb->ev_in, rb->main) != cudaSuccess)
@@ -991,11 +1030,20 @@ static int run_enqueue(ssa_rbatch *rb, int B, const int *N, const int *L, const 
 int ssa_rbatch_run_device(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k, const double *d_x,
                           uint64_t seed)
 {
+    return ssa_rbatch_run_device_ex(rb, B, N, L, k, d_x, seed, NULL);
+}
+
+int ssa_rbatch_run_device_ex(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k, const double *d_x,
+                             uint64_t seed, const unsigned char *want_w)
+{
     if (!rb || B < 1 || !N || !L || !k || !d_x)
         return -1;
     if (quiesce(rb) != 0)
         return -1;
-    return run_enqueue(rb, B, N, L, k, d_x, (unsigned long long)seed);
+    rb->cur_wmask = want_w;
+    const int rc = run_enqueue(rb, B, N, L, k, d_x, (unsigned long long)seed);
+    rb->cur_wmask = NULL;
+    return rc;
 }
 
 int ssa_rbatch_sync(ssa_rbatch *rb)
@@ -1020,6 +1068,12 @@ int ssa_rbatch_sync(ssa_rbatch *rb)
 int ssa_rbatch_run(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k, const double *x, uint64_t seed,
                    double *sigma, double *W, double *groups)
 {
+    return ssa_rbatch_run_ex(rb, B, N, L, k, x, seed, sigma, W, groups, NULL);
+}
+
+int ssa_rbatch_run_ex(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k, const double *x, uint64_t seed,
+                      double *sigma, double *W, double *groups, const unsigned char *want_w)
+{
     if (!rb || B < 1 || !N || !L || !k || !x)
         return -1;
     size_t nx = 0;
@@ -1033,7 +1087,10 @@ int ssa_rbatch_run(ssa_rbatch *rb, int B, const int *N, const int *L, const int 
         return -1;
     if (cudaMemcpyAsync(rb->d_xs, x, sizeof(double) * nx, cudaMemcpyHostToDevice, rb->main) != cudaSuccess)
         return -1;
-    if (run_enqueue(rb, B, N, L, k, rb->d_xs, (unsigned long long)seed) != 0)
+    rb->cur_wmask = want_w;
+    const int rq = run_enqueue(rb, B, N, L, k, rb->d_xs, (unsigned long long)seed);
+    rb->cur_wmask = NULL;
+    if (rq != 0)
         return -1;
     if (sigma && cudaMemcpyAsync(sigma, rb->sigma, sizeof(double) * rb->n_sig, cudaMemcpyDeviceToHost, rb->main) !=
                      cudaSuccess)
@@ -1144,7 +1201,7 @@ int ssar_set_lrf_group(ssa_rbatch *rb, int slot, const int *group, int n_group)
 }
 
 int ssar_run_enqueue_ex(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k, const double *d_x,
-                        const unsigned long long *seeds, double *const *lrf_dst)
+                        const unsigned long long *seeds, double *const *lrf_dst, const unsigned char *want_w)
 {
     if (!rb || B < 1 || !N || !L || !k || !d_x)
         return -1;
@@ -1152,9 +1209,11 @@ int ssar_run_enqueue_ex(ssa_rbatch *rb, int B, const int *N, const int *L, const
         return -1;
     rb->cur_seeds = seeds;
     rb->cur_lrf = lrf_dst;
+    rb->cur_wmask = want_w;
     int rc = run_enqueue(rb, B, N, L, k, d_x, 0);
     rb->cur_seeds = NULL;
     rb->cur_lrf = NULL;
+    rb->cur_wmask = NULL;
     return rc;
 }
 

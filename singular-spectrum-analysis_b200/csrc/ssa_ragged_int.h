@@ -22,7 +22,7 @@ int ssar_set_lrf_group(ssa_rbatch *rb, int slot, const int *group, int n_group);
  * s; lrf_dst[s] (or NULL, or a NULL entry) receives R (L-1), tail (L-1) and verticality (1)
  * doubles of the forecast group; series whose k does not cover the group are skipped. */
 int ssar_run_enqueue_ex(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k, const double *d_x,
-                        const unsigned long long *seeds, double *const *lrf_dst);
+                        const unsigned long long *seeds, double *const *lrf_dst, const unsigned char *want_w);
 cudaStream_t ssar_main_stream(const ssa_rbatch *rb);
 const int *ssar_status(const ssa_rbatch *rb);
 const int *ssar_lrf_status(const ssa_rbatch *rb);

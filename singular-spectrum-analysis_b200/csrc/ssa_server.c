@@ -61,6 +61,7 @@ typedef struct
     int *N, *L, *k;
     unsigned long long *seeds;
     double **lrf_dst;
+    unsigned char *wantw; /* 1: the request asked for the W-correlation */
     res_entry **res;
     /* per request: offsets (doubles) of its input in d_x and, for pageable buffers, in the
      * pinned staging areas (SIZE_MAX = copied directly from / to the caller's pinned memory) */
@@ -377,7 +378,10 @@ static int slot_reserve(slot_t *sl, int n)
     a[6] = realloc(sl->res, sizeof(res_entry *) * c);
     if (a[6])
         sl->res = (res_entry **)a[6];
-    for (int i = 0; i < 7; i++)
+    a[7] = realloc(sl->wantw, sizeof(unsigned char) * c);
+    if (a[7])
+        sl->wantw = (unsigned char *)a[7];
+    for (int i = 0; i < 8; i++)
         if (!a[i])
             return -1;
     size_t *z[3] = {NULL, NULL, NULL};
@@ -448,7 +452,7 @@ static int slot_launch(ssa_server *s, slot_t *sl)
             return -1;
         i = j;
     }
-    if (ssar_run_enqueue_ex(sl->rb, sl->n, sl->N, sl->L, sl->k, sl->d_x, sl->seeds, sl->lrf_dst) != 0)
+    if (ssar_run_enqueue_ex(sl->rb, sl->n, sl->N, sl->L, sl->k, sl->d_x, sl->seeds, sl->lrf_dst, sl->wantw) != 0)
         return -1;
     /* outputs the requests ask for */
     const size_t *off = ssar_offsets(sl->rb);
@@ -756,6 +760,7 @@ static int dispatch(ssa_server *s)
                     sl->k[j] = r->k;
                     sl->seeds[j] = r->seed;
                     sl->lrf_dst[j] = e ? e->d : NULL;
+                    sl->wantw[j] = r->type == SSA_REQ_DECOMPOSE_WCORR;
                     sl->res[j] = e;
                     sl->n++;
                     bytes += b;
@@ -1052,6 +1057,7 @@ void ssa_server_destroy(ssa_server *s)
         free(sl->k);
         free(sl->seeds);
         free(sl->lrf_dst);
+        free(sl->wantw);
         free(sl->res);
         free(sl->xoff);
         free(sl->sin);

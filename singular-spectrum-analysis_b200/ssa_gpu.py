@@ -572,6 +572,10 @@ _sig("ssa_rbatch_destroy", _V, ctypes.c_void_p)
 _sig("ssa_rbatch_run", _I, ctypes.c_void_p, _I, c_int_p, c_int_p, c_int_p, c_double_p, ctypes.c_uint64,
      c_double_p, c_double_p, c_double_p)
 _sig("ssa_rbatch_run_device", _I, ctypes.c_void_p, _I, c_int_p, c_int_p, c_int_p, ctypes.c_void_p, ctypes.c_uint64)
+_sig("ssa_rbatch_run_ex", _I, ctypes.c_void_p, _I, c_int_p, c_int_p, c_int_p, c_double_p, ctypes.c_uint64,
+     c_double_p, c_double_p, c_double_p, ctypes.c_void_p)
+_sig("ssa_rbatch_run_device_ex", _I, ctypes.c_void_p, _I, c_int_p, c_int_p, c_int_p, ctypes.c_void_p,
+     ctypes.c_uint64, ctypes.c_void_p)
 _sig("ssa_rbatch_sync", _I, ctypes.c_void_p)
 _sig("ssa_rbatch_layout", _I, ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t))
 _sig("ssa_rbatch_device_results", _I, ctypes.c_void_p, ctypes.POINTER(_BatchResults))
@@ -616,16 +620,29 @@ class SSARaggedBatch:
         N, L, k = (np.asarray(a, dtype=np.int64) for a in (N, L, k))
         return np.maximum(np.minimum(k, np.minimum(L, N - L + 1)), 1)
 
-    def run(self, series: Sequence[np.ndarray], L: Sequence[int], k: Sequence[int], seed: int = 0):
-        """Host-to-host run. Returns per-series lists (sigma, W, groups)."""
+    @staticmethod
+    def _mask(want_w, B):
+        """Per-series W-correlation flags as a uint8 array (None = W for every series)."""
+        if want_w is None:
+            return None, None
+        m = np.ascontiguousarray(np.asarray(want_w, dtype=bool).astype(np.uint8))
+        if m.shape != (B,):
+            raise ValueError("want_w must have one entry per series")
+        return m, ctypes.c_void_p(m.ctypes.data)
+
+    def run(self, series: Sequence[np.ndarray], L: Sequence[int], k: Sequence[int], seed: int = 0, want_w=None):
+        """Host-to-host run. Returns per-series lists (sigma, W, groups). With want_w (one flag per
+        series) only the flagged series get their W-correlation (the others' W is zero) and the
+        others compute only the elementary reconstructions their groups use."""
         Na, La, ka = self._dims([len(x) for x in series], L, k)
+        m, mp = self._mask(want_w, len(Na))
         x = np.ascontiguousarray(np.concatenate([np.asarray(s, dtype=np.float64) for s in series]))
         ke = self.effective_k(Na, La, ka)
         sig = np.zeros(int(ke.sum()))
         W = np.zeros(int((ke * ke).sum()))
         G = np.zeros(max(1, len(self.groups) * int(Na.sum())))
-        if _lib.ssa_rbatch_run(self._h, len(Na), _ip(Na), _ip(La), _ip(ka), _dp(x), seed, _dp(sig), _dp(W),
-                               _dp(G) if self.groups else None) != 0:
+        if _lib.ssa_rbatch_run_ex(self._h, len(Na), _ip(Na), _ip(La), _ip(ka), _dp(x), seed, _dp(sig), _dp(W),
+                                  _dp(G) if self.groups else None, mp) != 0:
             raise RuntimeError("ssa_rbatch_run failed")
         return self._unpack(Na, ke, sig, W, G)
 
@@ -642,11 +659,13 @@ class SSARaggedBatch:
             o_g += ng * n
         return out_s, out_w, out_g
 
-    def run_device(self, d_x_ptr: int, N, L, k, seed: int = 0) -> None:
-        """Enqueue a run on device-resident packed input (sum N doubles at d_x_ptr)."""
+    def run_device(self, d_x_ptr: int, N, L, k, seed: int = 0, want_w=None) -> None:
+        """Enqueue a run on device-resident packed input (sum N doubles at d_x_ptr); want_w as in
+        run()."""
         Na, La, ka = self._dims(N, L, k)
-        if _lib.ssa_rbatch_run_device(self._h, len(Na), _ip(Na), _ip(La), _ip(ka), ctypes.c_void_p(d_x_ptr),
-                                      seed) != 0:
+        m, mp = self._mask(want_w, len(Na))
+        if _lib.ssa_rbatch_run_device_ex(self._h, len(Na), _ip(Na), _ip(La), _ip(ka), ctypes.c_void_p(d_x_ptr),
+                                         seed, mp) != 0:
             raise RuntimeError("ssa_rbatch_run_device failed")
 
     def run_host_ptrs(self, N, L, k, x_ptr: int, seed: int, sigma_ptr: int, W_ptr: int, groups_ptr: int) -> None:

@@ -137,6 +137,29 @@ def test_serialized_profiling_is_bit_identical(gpu, oracle):
     assert gpu._lib.ssa_rbatch_set_profiling(rb._h, 3) == -1  # unknown mode
 
 
+def test_per_series_outputs_mask(gpu, oracle):
+    """want_w: series without W compute only the elementary reconstructions their groups use.
+    The decomposition and the group sums do not depend on the mask (bit-identical); flagged
+    series get the same W as in the plain run, the others a zero W block."""
+    mix = oracle.config3_batch(14, seed=31, nmin=500, nmax=70000)
+    xs, Ls, ks = [m[0] for m in mix], [m[1] for m in mix], [m[2] for m in mix]
+    want = np.arange(len(xs)) % 3 == 0
+    rb = gpu.SSARaggedBatch(oversampling=10, power_iters=2)
+    s0, W0, G0 = rb.run(xs, Ls, ks, seed=6)
+    s1, W1, G1 = rb.run(xs, Ls, ks, seed=6, want_w=want)
+    for i in range(len(xs)):
+        assert np.array_equal(s0[i], s1[i]) and np.array_equal(G0[i], G1[i]), i
+        if want[i]:
+            assert np.array_equal(W0[i], W1[i]), i
+        else:
+            assert not W1[i].any(), i
+    s2, W2, G2 = rb.run(xs, Ls, ks, seed=6)  # a plain run after a masked one is whole again
+    for i in range(len(xs)):
+        assert np.array_equal(W0[i], W2[i]) and np.array_equal(G0[i], G2[i]), i
+    with pytest.raises(ValueError):
+        rb.run(xs, Ls, ks, want_w=want[:-1])
+
+
 def test_uneven_batch_rejects_bad_series(gpu, oracle):
     rb = gpu.SSARaggedBatch()
     x = np.sin(np.arange(100.0)) + 0.1 * np.random.default_rng(1).standard_normal(100)
