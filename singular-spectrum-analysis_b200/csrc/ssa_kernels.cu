@@ -498,10 +498,12 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
 
 // Stage rows [r0, r0 + SSA_GRAM_CHUNK) of columns [0, n) into buf ([col][row], stride GRAM_S);
 // rows at or beyond r_end are zero-filled (they belong to another CTA's partial or lie past m).
+#define GRAM_MMA_THREADS 256
+
 __device__ __forceinline__ void gram_stage(uint32_t buf, const ssa_gram_job& J, int r0, int r_end, bool vec) {
     if (vec) {
         constexpr int Q = SSA_GRAM_CHUNK / 4;
-        for (int idx = threadIdx.x; idx < J.n * Q; idx += GRAM_THREADS) {
+        for (int idx = threadIdx.x; idx < J.n * Q; idx += GRAM_MMA_THREADS) {
             const int col = idx / Q, q = idx - col * Q;
             const int r = r0 + 4 * q;
             const int valid = min(4, max(0, r_end - r));
@@ -509,7 +511,7 @@ __device__ __forceinline__ void gram_stage(uint32_t buf, const ssa_gram_job& J, 
             cp_async16(buf + 4u * (uint32_t)(col * GRAM_S + 4 * q), src, 4 * valid);
         }
     } else {
-        for (int idx = threadIdx.x; idx < J.n * SSA_GRAM_CHUNK; idx += GRAM_THREADS) {
+        for (int idx = threadIdx.x; idx < J.n * SSA_GRAM_CHUNK; idx += GRAM_MMA_THREADS) {
             const int col = idx / SSA_GRAM_CHUNK, q = idx - col * SSA_GRAM_CHUNK;
             const int r = r0 + q;
             const bool ok = r < r_end;
@@ -521,12 +523,14 @@ __device__ __forceinline__ void gram_stage(uint32_t buf, const ssa_gram_job& J, 
 
 // Gram partials on the FP64 tensor cores: part[chunk] = A_c^T W A_c over this CTA's rows, FP32
 // data, exact FP64 products (FP32 x FP32 x integer weight), FP64 accumulation. G is cut into
-// 8x8 tiles (nt = ceil(n/8) <= 8 per side); warp w owns the upper-triangle tiles of tile
-// columns w and nt - 1 - w (at most nt + 1 <= 9 tiles), so that the four warps share the work
-// evenly for nt = 7, 8. Chunks of SSA_GRAM_CHUNK rows are staged by asynchronous copies into
-// two buffers, the next one landing while the current one is multiplied.
+// 8x8 tiles (nt = ceil(n/8) <= 8 per side); warps w and w + 4 own the upper-triangle tiles of
+// tile columns w and nt - 1 - w (at most nt + 1 <= 9 tiles), warp w over the first half of each
+// chunk's rows and warp w + 4 over the second half (their sums are added at the end), so that
+// eight warps keep the FP64 tensor pipe busy through the chunk barriers. Chunks of
+// SSA_GRAM_CHUNK rows are staged by asynchronous copies into two buffers, the next one landing
+// while the current one is multiplied.
 template <bool WEIGHTED>
-__global__ void __launch_bounds__(GRAM_THREADS) k_gram(const ssa_gram_job* __restrict__ jobs) {
+__global__ void __launch_bounds__(GRAM_MMA_THREADS, 3) k_gram(const ssa_gram_job* __restrict__ jobs) {
     extern __shared__ __align__(16) float gsm[];
     const ssa_gram_job J = jobs[blockIdx.y];
     const int chunk = blockIdx.x;
@@ -536,14 +540,15 @@ __global__ void __launch_bounds__(GRAM_THREADS) k_gram(const ssa_gram_job* __res
     const int n = J.n;
     const int nt = (n + 7) >> 3;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wq = warp & 3, half = warp >> 2;
     const int g = lane >> 2, t = lane & 3;
     // this warp's two tile columns (c2 = -1: none)
-    const int c1 = 2 * warp <= nt - 1 ? warp : -1;
-    const int c2 = (c1 >= 0 && nt - 1 - warp > warp) ? nt - 1 - warp : -1;
+    const int c1 = 2 * wq <= nt - 1 ? wq : -1;
+    const int c2 = (c1 >= 0 && nt - 1 - wq > wq) ? nt - 1 - wq : -1;
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(gsm);
     const bool vec = ((reinterpret_cast<uintptr_t>(J.A) & 15) == 0) && ((J.ld & 3) == 0);
     // padding columns n .. 8 nt - 1 of both stages read as zeros
-    for (int idx = threadIdx.x; idx < (8 * nt - n) * SSA_GRAM_CHUNK; idx += GRAM_THREADS) {
+    for (int idx = threadIdx.x; idx < (8 * nt - n) * SSA_GRAM_CHUNK; idx += GRAM_MMA_THREADS) {
         const int col = n + idx / SSA_GRAM_CHUNK, q = idx % SSA_GRAM_CHUNK;
         gsm[col * GRAM_S + q] = 0.f;
         gsm[GRAM_STAGE + col * GRAM_S + q] = 0.f;
@@ -570,8 +575,9 @@ __global__ void __launch_bounds__(GRAM_THREADS) k_gram(const ssa_gram_job* __res
         }
         if (c1 >= 0) {
             const float* pa = sA + g * GRAM_S + t;  // lane's element of tile column 0, k-step 0
+            const int s_end = (half + 1) * (SSA_GRAM_CHUNK / 2);
 #pragma unroll 2
-            for (int s4 = 0; s4 < SSA_GRAM_CHUNK; s4 += 4) {
+            for (int s4 = half * (SSA_GRAM_CHUNK / 2); s4 < s_end; s4 += 4) {
                 const float* row = pa + s4;
                 double b1 = (double)row[8 * c1 * GRAM_S];
                 double b2 = c2 >= 0 ? (double)row[8 * c2 * GRAM_S] : 0.0;
@@ -593,8 +599,24 @@ __global__ void __launch_bounds__(GRAM_THREADS) k_gram(const ssa_gram_job* __res
         }
         __syncthreads();  // this stage is refilled two chunks later
     }
+    // the second row half's sums join the first half's through shared memory (stages are free:
+    // every copy has landed and the loop ended on a barrier)
+    double* red = reinterpret_cast<double*>(gsm);
+    if (half == 1 && c1 >= 0) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            red[((wq * 9 + i) * 2 + 0) * 32 + lane] = acc[i][0];
+            red[((wq * 9 + i) * 2 + 1) * 32 + lane] = acc[i][1];
+        }
+    }
+    __syncthreads();
     double* part = J.part + (long long)chunk * (n * (n + 1) / 2);
-    if (c1 >= 0) {
+    if (half == 0 && c1 >= 0) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            acc[i][0] += red[((wq * 9 + i) * 2 + 0) * 32 + lane];
+            acc[i][1] += red[((wq * 9 + i) * 2 + 1) * 32 + lane];
+        }
 #pragma unroll
         for (int i = 0; i < 9; ++i) {
             const bool first = i <= c1;
@@ -732,9 +754,11 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_chol(const ssa_chol_job* __re
 
 #define RM_THREADS 256
 #define RM_ROWS SSA_ROWMUL_ROWS
-// A block [col][row] (column stride 132: 16-byte aligned columns), Bm [k][j] (row stride 64).
+// A block [col][row] (column stride 132: 16-byte aligned columns), Bm [k][j] (row stride 68:
+// 16-byte aligned rows; the staging stores, k fastest across lanes, meet 8 banks).
 #define RM_SA (RM_ROWS + 4)
-#define RM_SMEM (SSA_MAX_KP * RM_SA * (int)sizeof(float) + SSA_MAX_KP * SSA_MAX_KP * (int)sizeof(float) + \
+#define RM_SB (SSA_MAX_KP + 4)
+#define RM_SMEM (SSA_MAX_KP * RM_SA * (int)sizeof(float) + SSA_MAX_KP * RM_SB * (int)sizeof(float) + \
                  (RM_THREADS / 32) * SSA_MAX_KP * (int)sizeof(double))
 
 // One CTA per SSA_ROWMUL_ROWS rows: the rows of A (all n columns) land in shared memory by
@@ -746,7 +770,7 @@ __global__ void __launch_bounds__(RM_THREADS) k_rowmul(const ssa_rowmul_job* __r
     extern __shared__ __align__(16) unsigned char rsm[];
     float* sA = reinterpret_cast<float*>(rsm);
     float* sB = sA + SSA_MAX_KP * RM_SA;
-    double* wsum = reinterpret_cast<double*>(sB + SSA_MAX_KP * SSA_MAX_KP);
+    double* wsum = reinterpret_cast<double*>(sB + SSA_MAX_KP * RM_SB);
     const ssa_rowmul_job J = jobs[blockIdx.y];
     const int n = J.n, p = J.p;
     const int r0 = blockIdx.x * RM_ROWS;
@@ -771,11 +795,25 @@ __global__ void __launch_bounds__(RM_THREADS) k_rowmul(const ssa_rowmul_job* __r
         }
     }
     cp_async_commit();
-    for (int idx = threadIdx.x; idx < n * SSA_MAX_KP; idx += RM_THREADS) {
-        const int k = idx / SSA_MAX_KP, j = idx - k * SSA_MAX_KP;
-        float v = 0.f;
-        if (j < p) v = J.Bm64 ? (float)J.Bm64[k + (long long)j * J.ldb] : J.Bm[k + (long long)j * J.ldb];
-        sB[k * SSA_MAX_KP + j] = v;
+    {
+        // Bm column-major: k fastest across lanes (coalesced), all loads of a thread in flight
+        // together before the stores
+        constexpr int IT = SSA_MAX_KP * SSA_MAX_KP / RM_THREADS;
+        float bv[IT];
+#pragma unroll
+        for (int u = 0; u < IT; ++u) {
+            const int idx = threadIdx.x + u * RM_THREADS;
+            const int k = idx & (SSA_MAX_KP - 1), j = idx / SSA_MAX_KP;
+            float v = 0.f;
+            if (k < n && j < p)
+                v = J.Bm64 ? (float)J.Bm64[k + (long long)j * J.ldb] : J.Bm[k + (long long)j * J.ldb];
+            bv[u] = v;
+        }
+#pragma unroll
+        for (int u = 0; u < IT; ++u) {
+            const int idx = threadIdx.x + u * RM_THREADS;
+            sB[(idx & (SSA_MAX_KP - 1)) * RM_SB + idx / SSA_MAX_KP] = bv[u];
+        }
     }
     cp_async_wait<0>();
     __syncthreads();
@@ -792,8 +830,8 @@ __global__ void __launch_bounds__(RM_THREADS) k_rowmul(const ssa_rowmul_job* __r
 #pragma unroll 4
         for (int k = 0; k < kend; ++k) {
             const float4 a = *reinterpret_cast<const float4*>(sA + k * RM_SA + rl);
-            const float4 b0 = *reinterpret_cast<const float4*>(sB + k * SSA_MAX_KP + c0);
-            const float4 b1 = *reinterpret_cast<const float4*>(sB + k * SSA_MAX_KP + c0 + 4);
+            const float4 b0 = *reinterpret_cast<const float4*>(sB + k * RM_SB + c0);
+            const float4 b1 = *reinterpret_cast<const float4*>(sB + k * RM_SB + c0 + 4);
             const float av[4] = {a.x, a.y, a.z, a.w};
             const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
@@ -1535,9 +1573,9 @@ extern "C" int ssad_gram(const ssa_gram_job* d_jobs, int njobs, int maxchunks, i
     cudaError_t e = weighted ? set_smem(k_gram<true>, GRAM_SMEM) : set_smem(k_gram<false>, GRAM_SMEM);
     if (e != cudaSuccess) return (int)e;
     if (weighted)
-        k_gram<true><<<dim3(maxchunks, njobs), GRAM_THREADS, GRAM_SMEM, st>>>(d_jobs);
+        k_gram<true><<<dim3(maxchunks, njobs), GRAM_MMA_THREADS, GRAM_SMEM, st>>>(d_jobs);
     else
-        k_gram<false><<<dim3(maxchunks, njobs), GRAM_THREADS, GRAM_SMEM, st>>>(d_jobs);
+        k_gram<false><<<dim3(maxchunks, njobs), GRAM_MMA_THREADS, GRAM_SMEM, st>>>(d_jobs);
     return launched(cudaGetLastError());
 }
 
