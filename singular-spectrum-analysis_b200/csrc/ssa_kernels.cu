@@ -840,20 +840,37 @@ __global__ void __launch_bounds__(RM_THREADS) k_rowmul(const ssa_rowmul_job* __r
                 for (int v = 0; v < 8; ++v) acc[u][v] = fmaf(av[u], bv[v], acc[u][v]);
         }
     }
+    // a lane's four rows of a column are contiguous: one 16-byte store (and load of sub) per
+    // column when C (and sub) allow it, so a warp writes 512 contiguous bytes
+    const bool vecC = rl + 4 <= rows && ((reinterpret_cast<uintptr_t>(J.C) & 15) == 0) && ((J.ldc & 3) == 0) &&
+                      (!J.sub || (((reinterpret_cast<uintptr_t>(J.sub) & 15) == 0) && ((J.ldsub & 3) == 0)));
 #pragma unroll
     for (int v = 0; v < 8; ++v) {
         const int col = c0 + v;
         double cs = 0.0;
         if (col < p) {
-            const long long cb = (long long)col * J.ldc;
+            float x[4] = {acc[0][v], acc[1][v], acc[2][v], acc[3][v]};
+            const long long cb = (long long)(r0 + rl) + (long long)col * J.ldc;
+            if (vecC) {
+                if (J.sub) {
+                    const float4 sv =
+                        *reinterpret_cast<const float4*>(J.sub + (long long)(r0 + rl) + (long long)col * J.ldsub);
+                    x[0] = sv.x - x[0];
+                    x[1] = sv.y - x[1];
+                    x[2] = sv.z - x[2];
+                    x[3] = sv.w - x[3];
+                }
+                *reinterpret_cast<float4*>(J.C + cb) = make_float4(x[0], x[1], x[2], x[3]);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int row = rl + u;
-                if (row < rows) {
-                    float x = acc[u][v];
-                    if (J.sub) x = J.sub[(long long)(r0 + row) + (long long)col * J.ldsub] - x;
-                    J.C[(long long)(r0 + row) + cb] = x;
-                    cs += (double)x;
+                for (int u = 0; u < 4; ++u) cs += (double)x[u];
+            } else {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (rl + u < rows) {
+                        if (J.sub) x[u] = J.sub[(long long)(r0 + rl + u) + (long long)col * J.ldsub] - x[u];
+                        J.C[cb + u] = x[u];
+                        cs += (double)x[u];
+                    }
                 }
             }
         }
