@@ -24,7 +24,9 @@
 
 namespace cg = cooperative_groups;
 
+#ifndef SSA_CL_LOGH1
 #define SSA_CL_LOGH1 13
+#endif
 #define SSA_CL_MAX_LOGH 16
 
 template <int LOGH>
@@ -34,6 +36,7 @@ struct ClShape {
     static constexpr int C = 1 << (LOGH - LOGH1);
     static constexpr int H = 1 << LOGH;
     static constexpr int BLOCK = FftShape<LOGH1>::BLOCK;
+    static constexpr int MINB = BLOCK >= 1024 ? 1 : 2;  // CTAs per SM the kernels are built for
     static constexpr int NITEM = H1 / 2 + 1;  // k1 = 0 .. H1/2, each with its mirror
 };
 
@@ -225,7 +228,7 @@ struct ClDecim {
 // Spectrum (CL_SPEC), correlation sweep (CL_CORR) and one-buffer elementary reconstruction
 // (CL_ELEM) on clusters; grid (C x columns, jobs), one cluster per column.
 template <int LOGH, int KIND>
-__global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, 2) k_cl_col(const ssa_col_job* __restrict__ jobs) {
+__global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, ClShape<LOGH>::MINB) k_cl_col(const ssa_col_job* __restrict__ jobs) {
     using S = ClShape<LOGH>;
     extern __shared__ float2 smem[];
     __shared__ double red[32];
@@ -291,7 +294,7 @@ __global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, 2) k_cl_col(const ssa_co
 
 // Grouped reconstruction from cached spectra on clusters; grid (C, jobs).
 template <int LOGH>
-__global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, 2) k_cl_recon(const ssa_recon_job* __restrict__ jobs) {
+__global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, ClShape<LOGH>::MINB) k_cl_recon(const ssa_recon_job* __restrict__ jobs) {
     using S = ClShape<LOGH>;
     extern __shared__ float2 smem[];
     float2* s = smem;
