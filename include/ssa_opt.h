@@ -182,7 +182,9 @@ int ssa_opt_forecast(const SSA_Opt *ssa, const int *group, int n_group, int n_fo
 int ssa_opt_forecast_full(const SSA_Opt *ssa, const int *group, int n_group, int n_forecast, ssa_real *output);
 int ssa_opt_forecast_with_lrf(const SSA_LRF *lrf, const ssa_real *base_signal, int base_len, int n_forecast, ssa_real *output);
 
-/* ---- V-forecast (reference :352-355; out of scope: return -1) ---------------------------- */
+/* ---- V-forecast (reference :352-355, MKL/ssa_opt.h:2906-3084): the per-step projection on the
+ * group eigenvectors, evaluated as its equal LRF recurrence on the device (FP64); _fast starts
+ * from the last L-1 values of base_signal ------------------------------------------------------ */
 int ssa_opt_vforecast(const SSA_Opt *ssa, const int *group, int n_group, int n_forecast, ssa_real *output);
 int ssa_opt_vforecast_full(const SSA_Opt *ssa, const int *group, int n_group, int n_forecast, ssa_real *output);
 int ssa_opt_vforecast_fast(const SSA_Opt *ssa, const int *group, int n_group,

@@ -417,6 +417,50 @@ def forecast_full(dec: Decomposition, group: Sequence[int], n_forecast: int, N: 
     return np.concatenate([rec, forecast_with_lrf(R, rec, n_forecast)])
 
 
+def _vforecast_steps(dec: Decomposition, group: Sequence[int], L: int, buf: np.ndarray, n_forecast: int) -> np.ndarray:
+    """V-forecast recurrence as the reference writes it (ssa_opt.h:2941-2962): every step projects
+    the last L-1 values z on each group eigenvector and sums pi_g (U_trunc,g . z) / (1 - nu^2).
+    `buf` holds the starting window in its first L-1 entries and receives the forecasts."""
+    _, nu2 = compute_lrf(dec, group, L)  # index and verticality checks of ssa_opt.h:2912-2922
+    scale = 1.0 / (1.0 - nu2)
+    w = L - 1
+    out = np.zeros(n_forecast)
+    for h in range(n_forecast):
+        z = buf[h:h + w]
+        x_new = 0.0
+        for idx in group:
+            u = dec.U[:, idx]
+            x_new += u[L - 1] * float(np.dot(u[:w], z))
+        x_new *= scale
+        buf[w + h] = x_new
+        out[h] = x_new
+    return out
+
+
+def vforecast(dec: Decomposition, group: Sequence[int], n_forecast: int, N: int, L: int) -> np.ndarray:
+    """ssa_opt_vforecast (ssa_opt.h:2906-2966): forecast from the group's reconstruction."""
+    rec = reconstruct(dec, group, N, L)
+    buf = np.zeros(L - 1 + n_forecast)
+    buf[:L - 1] = rec[N - (L - 1):]
+    return _vforecast_steps(dec, group, L, buf, n_forecast)
+
+
+def vforecast_full(dec: Decomposition, group: Sequence[int], n_forecast: int, N: int, L: int) -> np.ndarray:
+    """ssa_opt_vforecast_full (ssa_opt.h:2968-3014): reconstruction followed by the forecast."""
+    rec = reconstruct(dec, group, N, L)
+    return np.concatenate([rec, vforecast(dec, group, n_forecast, N, L)])
+
+
+def vforecast_fast(dec: Decomposition, group: Sequence[int], base: np.ndarray, n_forecast: int, L: int) -> np.ndarray:
+    """ssa_opt_vforecast_fast (ssa_opt.h:3016-3078): the recurrence from the last L-1 values of
+    a given base signal (len(base) >= L - 1)."""
+    if len(base) < L - 1 or n_forecast < 1:
+        raise ValueError("base shorter than L - 1")
+    buf = np.zeros(L - 1 + n_forecast)
+    buf[:L - 1] = np.asarray(base, dtype=np.float64)[len(base) - (L - 1):]
+    return _vforecast_steps(dec, group, L, buf, n_forecast)
+
+
 def variance_explained(dec: Decomposition, start: int, end: int) -> float:
     """ssa_opt_variance_explained (ssa_opt.h:3110-3120)."""
     if start < 0 or dec.total_variance <= 0:

@@ -539,8 +539,11 @@ static int ensure_lrf(struct ssa_gpu_ctx *g, size_t doubles)
 
 /* LRF of `group` and, with h > 0, the forecast over the reconstruction of the group.
  * Host outputs: R (L-1, may be NULL), verticality, fc (h). Returns 0 or -1 (verticality). */
-static int lrf_forecast(const SSA_Opt *ssa, const int *group, int n_group, int h, double *R, double *vert,
-                        double *fc, double *recon_out)
+/* LRF of the group and h steps of the recurrence on the device (k_lrf). The recurrence starts
+ * from the last L-1 values of the group's reconstruction, or of `base_tail` (L-1 host values)
+ * when that is given (no reconstruction then). */
+static int lrf_forecast_from(const SSA_Opt *ssa, const int *group, int n_group, int h, double *R, double *vert,
+                             double *fc, double *recon_out, const double *base_tail)
 {
     struct ssa_gpu_ctx *g = ssa->gpu;
     const int L = ssa->L, N = ssa->N;
@@ -550,7 +553,15 @@ static int lrf_forecast(const SSA_Opt *ssa, const int *group, int n_group, int h
     if (ensure_lrf(g, (size_t)(L - 1) + (size_t)(L - 1 + h) + (size_t)h + 1) != 0)
         return -1;
     double *dR = g->d_lrf, *dbuf = dR + (L - 1), *dout = dbuf + (L - 1 + h), *dvert = dout + h;
-    if (recon_device(ssa, group, n_group) != 0)
+    if (base_tail)
+    {
+        /* the caller's window goes where the reconstruction would be (L - 1 <= N doubles) */
+        if (ensure_group(g, group, n_group) != 0 ||
+            cudaMemcpyAsync(g->d_out, base_tail, sizeof(double) * (size_t)(L - 1), cudaMemcpyHostToDevice,
+                            g->e.st) != cudaSuccess)
+            return -1;
+    }
+    else if (recon_device(ssa, group, n_group) != 0)
         return -1;
     ssa_lrf_job J;
     memset(&J, 0, sizeof(J));
@@ -564,7 +575,7 @@ static int lrf_forecast(const SSA_Opt *ssa, const int *group, int n_group, int h
     J.status = g->d_status;
     J.ld = g->e.ldL;
     J.L = L;
-    J.N = N;
+    J.N = base_tail ? L - 1 : N;
     J.n_group = n_group;
     J.h = h;
     J.k = ssa->n_components;
@@ -586,6 +597,12 @@ static int lrf_forecast(const SSA_Opt *ssa, const int *group, int n_group, int h
     if (recon_out && cudaMemcpy(recon_out, g->d_out, sizeof(double) * N, cudaMemcpyDeviceToHost) != cudaSuccess)
         return -1;
     return 0;
+}
+
+static int lrf_forecast(const SSA_Opt *ssa, const int *group, int n_group, int h, double *R, double *vert,
+                        double *fc, double *recon_out)
+{
+    return lrf_forecast_from(ssa, group, n_group, h, R, vert, fc, recon_out, NULL);
 }
 
 static int group_in_range(const SSA_Opt *ssa, const int *group, int n_group)
@@ -852,24 +869,53 @@ int ssa_opt_find_periodic_pairs(const SSA_Opt *ssa, int *pairs, int max_pairs, s
     return n_pairs;
 }
 
-/* ---- out-of-scope symbols kept for the wrapper's optional bindings ---------------------- */
+/* ---- V-forecast (MKL/ssa_opt.h:2906-3084) ------------------------------------------------
+ * The reference's V-forecast projects the last L-1 values on every group eigenvector per step,
+ *   x_new = sum_g pi_g (U_trunc,g . z) / (1 - nu^2),   pi_g = U[L-1, g],  nu^2 = sum_g pi_g^2,
+ * which is R . z with R = U_trunc pi / (1 - nu^2), the LRF of the same group: the same numbers
+ * as the R-forecast up to rounding. Here the projection is folded into R once on the device
+ * (FP64, k_lrf) and each step is one length-(L-1) dot product instead of n_group of them.
+ * Errors as the reference: -1 for an index outside the decomposition or nu^2 >= 1 - 1e-10. */
 
 int ssa_opt_vforecast(const SSA_Opt *ssa, const int *group, int n_group, int n_forecast, ssa_real *output)
 {
-    (void)ssa, (void)group, (void)n_group, (void)n_forecast, (void)output;
-    return -1;
+    if (!ssa || !ssa->decomposed || !group || !output || n_group < 1 || n_forecast < 1)
+        return -1;
+    if (!group_in_range(ssa, group, n_group))
+        return -1;
+    double vert;
+    return lrf_forecast(ssa, group, n_group, n_forecast, NULL, &vert, output, NULL);
 }
+
+/* Reconstruction of the group in output[0, N), the forecast in output[N, N + n_forecast). */
 int ssa_opt_vforecast_full(const SSA_Opt *ssa, const int *group, int n_group, int n_forecast, ssa_real *output)
 {
-    (void)ssa, (void)group, (void)n_group, (void)n_forecast, (void)output;
-    return -1;
+    if (!ssa || !ssa->decomposed || !group || !output || n_group < 1 || n_forecast < 1)
+        return -1;
+    if (!group_in_range(ssa, group, n_group))
+        return -1;
+    double vert;
+    return lrf_forecast(ssa, group, n_group, n_forecast, NULL, &vert, output + ssa->N, output);
 }
+
+/* The recurrence started from the last L-1 values of a caller-supplied base signal
+ * (base_len >= L - 1) instead of the group's reconstruction. */
 int ssa_opt_vforecast_fast(const SSA_Opt *ssa, const int *group, int n_group, const ssa_real *base_signal,
                            int base_len, int n_forecast, ssa_real *output)
 {
-    (void)ssa, (void)group, (void)n_group, (void)base_signal, (void)base_len, (void)n_forecast, (void)output;
-    return -1;
+    if (!ssa || !ssa->decomposed || !group || !base_signal || !output)
+        return -1;
+    if (n_group < 1 || n_forecast < 1 || base_len < ssa->L - 1)
+        return -1;
+    if (!group_in_range(ssa, group, n_group))
+        return -1;
+    double vert;
+    return lrf_forecast_from(ssa, group, n_group, n_forecast, NULL, &vert, output, NULL,
+                             base_signal + (base_len - (ssa->L - 1)));
 }
+
+/* ---- out-of-scope symbols kept for the wrapper's optional bindings ---------------------- */
+
 int ssa_opt_parestimate(const SSA_Opt *ssa, const int *group, int n_group, SSA_ParEstimate *result)
 {
     (void)ssa, (void)group, (void)n_group;

@@ -70,6 +70,9 @@ _sig("ssa_opt_reconstruct", _I, _P, c_int_p, _I, c_double_p)
 _sig("ssa_opt_cache_ffts", _I, _P)
 _sig("ssa_opt_forecast", _I, _P, c_int_p, _I, _I, c_double_p)
 _sig("ssa_opt_forecast_full", _I, _P, c_int_p, _I, _I, c_double_p)
+_sig("ssa_opt_vforecast", _I, _P, c_int_p, _I, _I, c_double_p)
+_sig("ssa_opt_vforecast_full", _I, _P, c_int_p, _I, _I, c_double_p)
+_sig("ssa_opt_vforecast_fast", _I, _P, c_int_p, _I, c_double_p, _I, _I, c_double_p)
 _sig("ssa_opt_compute_lrf", _I, _P, c_int_p, _I, ctypes.POINTER(_SSA_LRF))
 _sig("ssa_opt_lrf_free", _V, ctypes.POINTER(_SSA_LRF))
 _sig("ssa_opt_forecast_with_lrf", _I, ctypes.POINTER(_SSA_LRF), c_double_p, _I, _I, c_double_p)
@@ -306,6 +309,35 @@ class SSA:
             raise RuntimeError("Forecast failed")
         return out
 
+    def vforecast(self, group: List[int], n_forecast: int) -> np.ndarray:
+        """V-forecast (ssa_opt_vforecast): the projection recurrence, equal to the LRF forecast."""
+        self._need()
+        out = np.zeros(n_forecast)
+        g = np.ascontiguousarray(group, dtype=np.int32)
+        if _lib.ssa_opt_vforecast(ctypes.byref(self._ctx), _ip(g), len(group), n_forecast, _dp(out)) != 0:
+            raise RuntimeError("V-forecast failed (verticality >= 1?)")
+        return out
+
+    def vforecast_full(self, group: List[int], n_forecast: int) -> np.ndarray:
+        """Reconstruction of the group followed by its V-forecast (N + n_forecast values)."""
+        self._need()
+        out = np.zeros(self.N + n_forecast)
+        g = np.ascontiguousarray(group, dtype=np.int32)
+        if _lib.ssa_opt_vforecast_full(ctypes.byref(self._ctx), _ip(g), len(group), n_forecast, _dp(out)) != 0:
+            raise RuntimeError("V-forecast failed")
+        return out
+
+    def vforecast_fast(self, group: List[int], base_signal: np.ndarray, n_forecast: int) -> np.ndarray:
+        """V-forecast continuing from the last L - 1 values of base_signal."""
+        self._need()
+        base = np.ascontiguousarray(base_signal, dtype=np.float64)
+        out = np.zeros(n_forecast)
+        g = np.ascontiguousarray(group, dtype=np.int32)
+        if _lib.ssa_opt_vforecast_fast(ctypes.byref(self._ctx), _ip(g), len(group), _dp(base), len(base),
+                                       n_forecast, _dp(out)) != 0:
+            raise RuntimeError("V-forecast failed")
+        return out
+
     def lrf(self, group: List[int]) -> Tuple[np.ndarray, float]:
         """LRF coefficients R (L - 1) and verticality nu^2 (ssa_opt_compute_lrf)."""
         self._need()
@@ -401,9 +433,6 @@ class SSA:
 
     def parestimate(self, group: Optional[List[int]] = None):
         raise RuntimeError("ESPRIT (parestimate) is not part of the accelerated path")
-
-    def vforecast(self, group: List[int], n_forecast: int) -> np.ndarray:
-        raise RuntimeError("V-forecast is not part of the accelerated path")
 
 
 class MSSA:

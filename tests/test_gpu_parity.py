@@ -144,6 +144,37 @@ def test_forecast_parity(gpu, oracle):
     assert rel_l2(full[N:], fr[:20]) < 1e-4
 
 
+def test_vforecast_parity(gpu, oracle):
+    """V-forecast (ssa_opt_vforecast*, MKL/ssa_opt.h:2906-3084) against the oracle's per-step
+    projection form, same tolerances as the R-forecast; the V and R forms agree to FP64 rounding."""
+    x, clean, Om = oracle.config1(seed=0)
+    N, L, k, p = 1000, 250, 10, 10
+    d = oracle.decompose_randomized(x, L, k, p, Om[:, :k + p], q=2)
+    gs = gpu.SSA(x, L)
+    gs.decompose(k, oversampling=p, power_iters=2, omega=Om[:, :k + p])
+    g = [0, 1, 2]
+    fr = oracle.vforecast(d, g, 50, N, L)
+    np.testing.assert_allclose(fr, oracle.forecast(d, g, 50, N, L), rtol=1e-10, atol=1e-10 * np.abs(fr).max())
+    f = gs.vforecast(g, 50)
+    assert rel_l2(f, fr) < 1e-4
+    np.testing.assert_allclose(f, gs.forecast(g, 50), rtol=1e-12, atol=0)
+    full = gs.vforecast_full(g, 20)
+    assert rel_l2(full[:N], oracle.reconstruct(d, g, N, L)) <= REC_TOL
+    assert rel_l2(full[N:], fr[:20]) < 1e-4
+    # from a caller's base signal: the clean signal (any length >= L - 1), and the raw series
+    for base in (clean, x[:600]):
+        fb = gs.vforecast_fast(g, base, 30)
+        fbr = oracle.vforecast_fast(d, g, base, 30, L)
+        assert rel_l2(fb, fbr) < 1e-4
+    # from the group's own reconstruction it is the V-forecast itself
+    np.testing.assert_allclose(gs.vforecast_fast(g, full[:N], 20), f[:20], rtol=1e-9,
+                               atol=1e-9 * np.abs(f).max())
+    with pytest.raises(RuntimeError):
+        gs.vforecast_fast(g, x[:L - 2], 5)  # base shorter than L - 1
+    with pytest.raises(RuntimeError):
+        gs.vforecast([0, 99], 5)  # index outside the decomposition
+
+
 def test_reconstruct_edge_groups(gpu, oracle):
     x, _, Om = oracle.config1(seed=0)
     N, L, k, p = 1000, 250, 8, 4

@@ -127,6 +127,25 @@ def test_lrf_forecast_vs_ref(oracle, reflib):
     assert np.max(np.abs(out - oracle.forecast_full(d, [0, 1, 2], 30, N, L))) < 1e-9
 
 
+def test_vforecast_vs_ref_forecast(oracle, reflib):
+    """The V-forecast restatement (per-step projections, ssa_opt.h:2906-3084) against the
+    reference build's R-forecast on the same factors: the two forms are algebraically equal
+    (x_new = sum_g pi_g U_g . z / (1 - nu^2) = R . z), so they agree to FP64 rounding. The
+    reference's V-forecast lives in the MKL-only header, so this pins it through that identity."""
+    N, L, k = 500, 125, 12
+    x, d, Uc, Vc = _factors(oracle, N, L, k)
+    g = np.array([0, 1, 2], dtype=np.int32)
+    out = np.zeros(N + 30)
+    assert reflib.lib.refdrv_forecast(reflib.d(x), N, L, k, reflib.d(Uc), reflib.d(Vc), reflib.d(d.sigma),
+                                      reflib.i(g), 3, 30, reflib.d(out)) == 0
+    vf = oracle.vforecast_full(d, [0, 1, 2], 30, N, L)
+    assert np.max(np.abs(out - vf)) < 1e-9
+    # the fast form from the reconstruction is the same forecast
+    assert np.max(np.abs(oracle.vforecast_fast(d, [0, 1, 2], vf[:N], 30, L) - vf[N:])) < 1e-9
+    with pytest.raises(ValueError):
+        oracle.vforecast(d, [0, 99], 5, N, L)
+
+
 def test_sequential_ref_vs_dense(oracle, reflib):
     N, L, k = 500, 125, 6
     x = _sig(oracle, N)
