@@ -461,6 +461,121 @@ def vforecast_fast(dec: Decomposition, group: Sequence[int], base: np.ndarray, n
     return _vforecast_steps(dec, group, L, buf, n_forecast)
 
 
+def gap_linear_start(x: np.ndarray, gap: np.ndarray) -> None:
+    """Initial fill of NaN runs by the line between their valid neighbours (ssa_opt.h:3450-3494):
+    point j of a run of n at fraction (j + 1) / (n + 1) (a single point: 0.5); one neighbour
+    only: its value; none: 0."""
+    N = len(x)
+    i = 0
+    while i < N:
+        if not gap[i]:
+            i += 1
+            continue
+        a = i
+        while i < N and gap[i]:
+            i += 1
+        n = i - a
+        lv = x[a - 1] if a > 0 else (x[i] if i < N else 0.0)
+        rv = x[i] if i < N else lv
+        for j in range(n):
+            t = (j + 1) / (n + 1) if n > 1 else 0.5
+            x[a + j] = lv + t * (rv - lv)
+
+
+def gapfill(x: np.ndarray, L: int, rank: int, max_iter: int, tol: float, omega_fn) -> tuple:
+    """ssa_opt_gapfill (ssa_opt.h:3497-3683): linear start, then per iteration a rank-`rank`
+    reconstruction (randomized, q = 0, oversampling 8, a fresh context: omega_fn(K, kp) gives
+    its test matrix) written into the gaps until the relative change of the gap values < tol.
+    Returns (filled signal, iterations, final_diff, converged, n_gaps); ValueError where the
+    reference returns -1."""
+    y = np.asarray(x, dtype=np.float64).copy()
+    N = len(y)
+    if N < 4 or L < 2 or L > N - 1 or rank < 1:
+        raise ValueError("bad shape")
+    gap = np.isnan(y)
+    n_gaps = int(gap.sum())
+    if n_gaps == 0:
+        return y, 0, 0.0, True, 0
+    if N - n_gaps < L + rank:
+        raise ValueError("not enough data")
+    gap_linear_start(y, gap)
+    K = N - L + 1
+    kp = min(rank + 8, L, K)
+    Om = omega_fn(K, kp)
+    old = y[gap].copy()
+    diff, converged, it = 1e10, False, 0
+    group = list(range(rank))
+    while it < max_iter:
+        dec = decompose_randomized(y, L, rank, 8, Om, q=0)
+        rec = reconstruct(dec, group, N, L)
+        new = rec[gap]
+        y[gap] = new
+        so = float(np.sum(old * old))
+        sd = float(np.sum((new - old) ** 2))
+        diff = math.sqrt(sd / so) if so > 1e-12 else math.sqrt(sd)
+        it += 1
+        if diff < tol:
+            converged = True
+            break
+        old = new.copy()
+    return y, it, diff, converged, n_gaps
+
+
+def gapfill_simple(x: np.ndarray, L: int, rank: int, omega_fn) -> tuple:
+    """ssa_opt_gapfill_simple (ssa_opt.h:3685-3878): each NaN run, left to right, from the
+    forecast of the segment before it and the reversed segment after it (each when at least
+    L + rank long; randomized q = 0, oversampling 8, fresh contexts), weighted linearly towards
+    the nearer side; neither: the mean of the neighbours. A right segment that still holds a
+    later run gives no forecast (the reference would decompose its NaNs). Returns (signal, n_gaps)."""
+    y = np.asarray(x, dtype=np.float64).copy()
+    N = len(y)
+    if N < 4 or L < 2 or L > N - 1 or rank < 1:
+        raise ValueError("bad shape")
+    gap = np.isnan(y)
+    n_gaps = int(gap.sum())
+    group = list(range(rank))
+
+    def seg_forecast(seg, h):
+        n = len(seg)
+        K = n - L + 1
+        kp = min(rank + 8, L, K)
+        dec = decompose_randomized(seg, L, rank, 8, omega_fn(K, kp), q=0)
+        try:
+            return forecast(dec, group[:min(rank, dec.k)], h, n, L)
+        except ValueError:
+            return None
+
+    i = 0
+    while i < N:
+        if not gap[i]:
+            i += 1
+            continue
+        a = i
+        while i < N and gap[i]:
+            i += 1
+        glen = i - a
+        fl = seg_forecast(y[:a].copy(), glen) if a >= L + rank else None
+        right_clean = N - i >= L + rank and not gap[i:].any()  # a later unfilled run: no forecast
+        fr = seg_forecast(y[::-1][:N - i].copy(), glen) if right_clean else None
+        for j in range(glen):
+            v = w = 0.0
+            if fl is not None:
+                wl = (glen - j) / glen
+                v += wl * fl[j]
+                w += wl
+            if fr is not None:
+                wr = (j + 1) / glen
+                v += wr * fr[glen - 1 - j]
+                w += wr
+            if w > 0:
+                y[a + j] = v / w
+            else:
+                lv = y[a - 1] if a > 0 else 0.0
+                rv = y[i] if i < N else lv
+                y[a + j] = 0.5 * (lv + rv)
+    return y, n_gaps
+
+
 def variance_explained(dec: Decomposition, start: int, end: int) -> float:
     """ssa_opt_variance_explained (ssa_opt.h:3110-3120)."""
     if start < 0 or dec.total_variance <= 0:

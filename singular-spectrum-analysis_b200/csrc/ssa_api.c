@@ -933,20 +933,6 @@ void ssa_opt_parestimate_free(SSA_ParEstimate *result)
     free(result->rates);
     memset(result, 0, sizeof(*result));
 }
-int ssa_opt_gapfill(ssa_real *x, int N, int L, int rank, int max_iter, ssa_real tol, SSA_GapFillResult *result)
-{
-    (void)x, (void)N, (void)L, (void)rank, (void)max_iter, (void)tol;
-    if (result)
-        memset(result, 0, sizeof(*result));
-    return -1;
-}
-int ssa_opt_gapfill_simple(ssa_real *x, int N, int L, int rank, SSA_GapFillResult *result)
-{
-    (void)x, (void)N, (void)L, (void)rank;
-    if (result)
-        memset(result, 0, sizeof(*result));
-    return -1;
-}
 
 /* ---- MKL tuning exports of MKL/py/ssa_wrapper.c:47-123 ---------------------------------- */
 int ssa_mkl_init(int verbose)
@@ -1291,6 +1277,264 @@ int ssa_opt_cadzow_inplace(SSA_Opt *ssa, int rank, int max_iter, ssa_real tol, S
     }
     return iter;
 }
+
+/* ---- gap filling (MKL/ssa_opt.h:3440-3878) ------------------------------------------------
+ * Missing values are NaN. Both forms modify x in place at the gap positions only. */
+
+/* Gaps start as the straight line between their valid neighbours (one neighbour: that value;
+ * none: 0), point j of a gap of length n at fraction (j + 1) / (n + 1) (a single point: 1/2). */
+static void gap_linear_start(double *x, const unsigned char *gap, int N)
+{
+    int i = 0;
+    while (i < N)
+    {
+        if (!gap[i])
+        {
+            i++;
+            continue;
+        }
+        const int a = i;
+        while (i < N && gap[i])
+            i++;
+        const int n = i - a;
+        const double lv = a > 0 ? x[a - 1] : (i < N ? x[i] : 0.0);
+        const double rv = i < N ? x[i] : lv;
+        for (int j = 0; j < n; j++)
+        {
+            const double t = n > 1 ? (double)(j + 1) / (double)(n + 1) : 0.5;
+            x[a + j] = lv + t * (rv - lv);
+        }
+    }
+}
+
+static int gap_mask(const double *x, int N, unsigned char **gap)
+{
+    *gap = (unsigned char *)calloc((size_t)N, 1);
+    if (!*gap)
+        return -1;
+    int n = 0;
+    for (int i = 0; i < N; i++)
+        if (isnan(x[i]))
+        {
+            (*gap)[i] = 1;
+            n++;
+        }
+    return n;
+}
+
+/* Iterative form: each iteration reconstructs the current signal from its leading `rank`
+ * components (randomized, q = 0, oversampling 8, as the reference's freshly initialised context
+ * per iteration: the same test matrix every time) and writes the reconstruction into the gaps,
+ * until the relative change of the gap values drops below tol. Device-resident: the signal stays
+ * in HBM, each iteration reads back two sums. Returns 0 (iterations etc. in result) or -1. */
+int ssa_opt_gapfill(ssa_real *x, int N, int L, int rank, int max_iter, ssa_real tol, SSA_GapFillResult *result)
+{
+    if (!x || N < 4 || L < 2 || L > N - 1 || rank < 1)
+        return -1;
+    unsigned char *gap = NULL;
+    const int n_gaps = gap_mask(x, N, &gap);
+    if (n_gaps < 0)
+        return -1;
+    if (n_gaps == 0)
+    {
+        free(gap);
+        if (result)
+        {
+            result->iterations = 0;
+            result->final_diff = 0.0;
+            result->converged = 1;
+            result->n_gaps = 0;
+        }
+        return 0;
+    }
+    const int K = N - L + 1;
+    if (N - n_gaps < L + rank || imin(rank + 8, imin(L, K)) > SSA_MAX_KP)
+    {
+        free(gap);
+        return -1;
+    }
+    int *idx = (int *)malloc(sizeof(int) * (size_t)n_gaps);
+    if (!idx)
+    {
+        free(gap);
+        return -1;
+    }
+    for (int i = 0, j = 0; i < N; i++)
+        if (gap[i])
+            idx[j++] = i;
+    gap_linear_start(x, gap, N);
+    free(gap);
+    SSA_Opt ssa;
+    if (ssa_opt_init(&ssa, x, N, L) != 0)
+    {
+        free(idx);
+        return -1;
+    }
+    struct ssa_gpu_ctx *g = ssa.gpu;
+    ssa_engine *e = &g->e;
+    double *d_aux = NULL; /* two sums, then the gap indices */
+    int rc = cadzow_setup(g, rank, &d_aux, 2 + ((size_t)n_gaps + 1) / 2);
+    int *d_idx = d_aux ? (int *)(d_aux + 2) : NULL;
+    if (!rc && cudaMemcpyAsync(d_idx, idx, sizeof(int) * (size_t)n_gaps, cudaMemcpyHostToDevice, e->st) != cudaSuccess)
+        rc = -1;
+    free(idx);
+    int iter = 0, converged = 0, k = 0;
+    double diff = 1e10;
+    for (iter = 0; iter < max_iter && !rc; iter++)
+    {
+        ssae_reset_jobs(e);
+        if (iter > 0 && ssae_signal_spectrum(e, e->x64, 1) != 0)
+        {
+            rc = -1;
+            break;
+        }
+        if (cadzow_project(&ssa, rank, 1, SSA_DEFAULT_SEED, &k) != 0)
+        {
+            rc = -1;
+            break;
+        }
+        double h[2];
+        if (ssad_gapupdate(e->x64, g->d_out, d_idx, n_gaps, d_aux, e->st) != 0 ||
+            cudaMemcpyAsync(h, d_aux, sizeof(double) * 2, cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
+            sync_ok(g) != 0)
+        {
+            rc = -1;
+            break;
+        }
+        diff = h[1] > 1e-12 ? sqrt(h[0] / h[1]) : sqrt(h[0]);
+        if (diff < tol)
+        {
+            converged = 1;
+            iter++;
+            break;
+        }
+    }
+    if (!rc && (cudaMemcpyAsync(x, e->x64, sizeof(double) * (size_t)N, cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
+                sync_ok(g) != 0))
+        rc = -1;
+    cudaFree(d_aux);
+    ssa_opt_free(&ssa);
+    if (rc)
+        return -1;
+    if (result)
+    {
+        result->iterations = iter;
+        result->final_diff = diff;
+        result->converged = converged;
+        result->n_gaps = n_gaps;
+    }
+    return 0;
+}
+
+/* h-step forecast of the leading `rank` components of data[0, n) (randomized, q = 0,
+ * oversampling 8, a fresh context): a malloc'd array, or NULL when the segment cannot be
+ * decomposed or forecast. */
+static double *segment_forecast(const double *data, int n, int L, int rank, const int *group, int h)
+{
+    SSA_Opt s;
+    if (ssa_opt_init(&s, data, n, L) != 0)
+        return NULL;
+    double *f = NULL;
+    if (ssa_opt_prepare(&s, rank, 8) == 0 && ssa_opt_decompose_randomized(&s, rank, 8) == 0)
+    {
+        f = (double *)malloc(sizeof(double) * (size_t)h);
+        if (f && ssa_opt_forecast(&s, group, imin(rank, s.n_components), h, f) != 0)
+        {
+            free(f);
+            f = NULL;
+        }
+    }
+    ssa_opt_free(&s);
+    return f;
+}
+
+/* Single-pass form: every gap run (left to right, earlier runs already filled) is filled from a
+ * forecast of the valid segment before it and a forecast of the reversed segment after it (each
+ * when at least L + rank long), weighted linearly towards the nearer side; with neither, the mean
+ * of the neighbouring values. A forecast that cannot be computed counts as absent, and so does a
+ * segment that still holds a later, unfilled gap (the reference decomposes the NaNs there). */
+int ssa_opt_gapfill_simple(ssa_real *x, int N, int L, int rank, SSA_GapFillResult *result)
+{
+    if (!x || N < 4 || L < 2 || L > N - 1 || rank < 1)
+        return -1;
+    unsigned char *gap = NULL;
+    const int n_gaps = gap_mask(x, N, &gap);
+    if (n_gaps < 0)
+        return -1;
+    int *group = (int *)malloc(sizeof(int) * (size_t)rank);
+    double *rev = (double *)malloc(sizeof(double) * (size_t)N);
+    if (!group || !rev)
+    {
+        free(gap);
+        free(group);
+        free(rev);
+        return -1;
+    }
+    for (int i = 0; i < rank; i++)
+        group[i] = i;
+    int i = 0;
+    while (i < N)
+    {
+        if (!gap[i])
+        {
+            i++;
+            continue;
+        }
+        const int a = i;
+        while (i < N && gap[i])
+            i++;
+        const int glen = i - a, right_len = N - i;
+        double *fl = a >= L + rank ? segment_forecast(x, a, L, rank, group, glen) : NULL;
+        double *fr = NULL;
+        int right_clean = right_len >= L + rank;
+        for (int j = i; j < N && right_clean; j++)
+            right_clean = !gap[j];
+        if (right_clean)
+        {
+            for (int j = 0; j < right_len; j++)
+                rev[j] = x[N - 1 - j];
+            fr = segment_forecast(rev, right_len, L, rank, group, glen);
+        }
+        for (int j = 0; j < glen; j++)
+        {
+            double v = 0.0, w = 0.0;
+            if (fl)
+            {
+                const double wl = (double)(glen - j) / glen;
+                v += wl * fl[j];
+                w += wl;
+            }
+            if (fr)
+            {
+                const double wr = (double)(j + 1) / glen;
+                v += wr * fr[glen - 1 - j]; /* the backcast runs from the right end */
+                w += wr;
+            }
+            if (w > 0.0)
+                x[a + j] = v / w;
+            else
+            {
+                const double lv = a > 0 ? x[a - 1] : 0.0;
+                const double rv = i < N ? x[i] : lv;
+                x[a + j] = 0.5 * (lv + rv);
+            }
+        }
+        free(fl);
+        free(fr);
+    }
+    free(gap);
+    free(group);
+    free(rev);
+    if (result)
+    {
+        result->iterations = 1;
+        result->final_diff = 0.0;
+        result->converged = 1;
+        result->n_gaps = n_gaps;
+    }
+    return 0;
+}
+
 
 void ssa_b200_set_wcorr_tensor_cores(int on) { ssad_set_wcorr_tc(on); }
 int ssa_b200_wcorr_tensor_cores(void) { return ssad_wcorr_tc(); }

@@ -1313,6 +1313,26 @@ __global__ void k_diffnorm(const double* a, const double* b, long long n, double
     }
 }
 
+// Gap filling step: the reconstruction replaces the signal at the gap positions idx[0, n); out2 =
+// {sum (new - old)^2, sum old^2} over the gaps (one CTA).
+__global__ void k_gapupdate(double* x, const double* recon, const int* idx, int n, double* out2) {
+    __shared__ double red[32];
+    double d2 = 0.0, o2 = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int j = idx[i];
+        const double nv = recon[j], ov = x[j];
+        d2 += (nv - ov) * (nv - ov);
+        o2 += ov * ov;
+        x[j] = nv;
+    }
+    d2 = block_sum<double>(d2, red);
+    o2 = block_sum<double>(o2, red);
+    if (threadIdx.x == 0) {
+        out2[0] = d2;
+        out2[1] = o2;
+    }
+}
+
 __global__ void k_axpby(const double* a, const double* b, double* out, double alpha, double beta, long long n) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         out[i] = alpha * a[i] + beta * b[i];
@@ -1691,6 +1711,12 @@ extern "C" int ssad_colnorm2(const float* A, long long sstride, long long ld, in
                              void* stream) {
     if (nb <= 0 || k <= 0) return 0;
     k_colnorm2<<<dim3(k, nb), 256, 0, (cudaStream_t)stream>>>(A, sstride, ld, m, k, out);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_gapupdate(double* x, const double* recon, const int* idx, int n, double* out2, void* stream) {
+    if (n < 1) return 0;
+    k_gapupdate<<<1, 256, 0, (cudaStream_t)stream>>>(x, recon, idx, n, out2);
     return launched(cudaGetLastError());
 }
 

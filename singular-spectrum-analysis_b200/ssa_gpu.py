@@ -179,6 +179,49 @@ def cadzow(x: np.ndarray, L: int, rank: int, max_iter: int = 20, tol: float = 1e
     return CadzowResult(out, res.iterations, res.final_diff, bool(res.converged))
 
 
+class _SSA_GapFillResult(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("final_diff", ctypes.c_double), ("converged", ctypes.c_int),
+                ("n_gaps", ctypes.c_int)]
+
+
+_sig("ssa_opt_gapfill", _I, c_double_p, _I, _I, _I, _I, _D, ctypes.POINTER(_SSA_GapFillResult))
+_sig("ssa_opt_gapfill_simple", _I, c_double_p, _I, _I, _I, ctypes.POINTER(_SSA_GapFillResult))
+
+
+class GapFillResult:
+    """Result of gap filling (MKL/py/ssa_wrapper.py:496-509)."""
+
+    def __init__(self, signal: np.ndarray, iterations: int, final_diff: float, converged: bool, n_gaps: int):
+        self.signal = signal
+        self.iterations = iterations
+        self.final_diff = final_diff
+        self.converged = converged
+        self.n_gaps = n_gaps
+
+    def __repr__(self):
+        return (f"GapFillResult(n_gaps={self.n_gaps}, iterations={self.iterations}, "
+                f"final_diff={self.final_diff:.2e}, converged={self.converged})")
+
+
+def gapfill(x: np.ndarray, L: int, rank: int, max_iter: int = 20, tol: float = 1e-6,
+            method: str = "iterative") -> GapFillResult:
+    """Fill NaN gaps (MKL/py/ssa_wrapper.py:511-590 -> ssa_opt_gapfill / ssa_opt_gapfill_simple):
+    "iterative" re-reconstructs the gaps until they settle, "simple" blends a forecast from the
+    left and a backcast from the right of every gap."""
+    xf = np.ascontiguousarray(np.array(x, dtype=np.float64, copy=True))
+    N = len(xf)
+    res = _SSA_GapFillResult()
+    if method == "iterative":
+        ret = _lib.ssa_opt_gapfill(_dp(xf), N, L, rank, max_iter, tol, ctypes.byref(res))
+    elif method == "simple":
+        ret = _lib.ssa_opt_gapfill_simple(_dp(xf), N, L, rank, ctypes.byref(res))
+    else:
+        raise ValueError(f"Unknown method: {method}. Use 'iterative' or 'simple'")
+    if ret != 0:
+        raise RuntimeError(f"Gap filling failed (ret={ret})")
+    return GapFillResult(xf, res.iterations, res.final_diff, bool(res.converged), res.n_gaps)
+
+
 class SSA:
     """Univariate SSA on the GPU (interface of MKL/py/ssa_wrapper.py:600-1202)."""
 

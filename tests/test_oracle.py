@@ -231,3 +231,44 @@ def test_mssa_m1_matches_ssa(oracle):
     b = oracle.mssa_decompose(x[None, :], L, k, p, Om)
     assert np.allclose(a.sigma, b.sigma, rtol=1e-12)
     assert np.allclose(oracle.reconstruct(a, [0, 1], 400, L), oracle.mssa_reconstruct(b, 0, [0, 1], 1, 400, L))
+
+
+def _gap_signal(N, two_tones=True):
+    """The signals of the reference's gap-filling tests (MKL/test/ssa_opt_test.c:902-1000)."""
+    i = np.arange(N, dtype=np.float64)
+    s = np.sin(2 * np.pi * i / 50.0) + 0.02 * i
+    if two_tones:
+        s += 0.5 * np.sin(2 * np.pi * i / 20.0)
+    return s
+
+
+def test_gapfill_reference_bars(oracle):
+    """The reference's own acceptance bars: iterative fill of 35 gap values (two runs) leaves no
+    NaN and has RMSE < 0.5 at the gaps; the simple form fills a 20-value run."""
+    N, L, rank = 500, 100, 6
+    true = _gap_signal(N)
+    x = true.copy()
+    x[50:65] = np.nan
+    x[150:170] = np.nan
+    om = lambda K, kp: oracle.device_gaussian(oracle.single_series_seed(0), K, kp)  # noqa: E731
+    y, it, diff, conv, ng = oracle.gapfill(x, L, rank, 30, 1e-8, om)
+    assert ng == 35 and it > 0 and not np.isnan(y).any()
+    gaps = np.isnan(x)
+    assert np.sqrt(np.mean((y[gaps] - true[gaps]) ** 2)) < 0.5
+    assert np.array_equal(y[~gaps], x[~gaps])  # only the gaps change
+    t2 = _gap_signal(N, two_tones=False)
+    x2 = t2.copy()
+    x2[200:220] = np.nan
+    y2, ng2 = oracle.gapfill_simple(x2, L, rank, om)
+    assert ng2 == 20 and not np.isnan(y2).any()
+    assert np.sqrt(np.mean((y2[200:220] - t2[200:220]) ** 2)) < 0.5
+
+
+def test_gap_linear_start(oracle):
+    x = np.array([1.0, np.nan, np.nan, 4.0, np.nan, 6.0, np.nan, np.nan])
+    g = np.isnan(x)
+    oracle.gap_linear_start(x, g)
+    np.testing.assert_allclose(x, [1.0, 2.0, 3.0, 4.0, 5.0, 6.0, 6.0, 6.0])
+    y = np.array([np.nan, 2.0])
+    oracle.gap_linear_start(y, np.isnan(y))
+    assert y[0] == 2.0
