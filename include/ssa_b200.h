@@ -250,6 +250,10 @@ int ssa_wcorr_noalloc(const float *d_U, long long ldU, const float *d_V, long lo
 /* ---- library information ------------------------------------------------------------------ */
 /* Number of CUDA kernel launches issued by this library in this process. */
 unsigned long long ssa_b200_kernel_launches(void);
+/* Eigenvalues (wr + i wi) of a real n x n row-major matrix: the host solver ssa_opt_parestimate
+ * uses (Householder-Hessenberg reduction and Francis double-shift QR, FP64), exported so that it
+ * can be checked on its own. No counterpart in the reference (which calls LAPACK dgeev). 0 / -1. */
+int ssa_b200_eigvals(int n, const double *A, double *wr, double *wi);
 /* Device self-check record of the current device: {violations, kernel, block, code, value};
  * kernels that validate their job tables record the first violation there instead of
  * accessing memory with it. reset != 0 clears the record. Returns 0 or -1. */

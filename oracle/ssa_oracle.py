@@ -576,6 +576,25 @@ def gapfill_simple(x: np.ndarray, L: int, rank: int, omega_fn) -> tuple:
     return y, n_gaps
 
 
+def parestimate(dec: Decomposition, group, L: int) -> dict:
+    """ESPRIT (ssa_opt.h:4304-4558): Z = argmin ||U_up Z - U_down|| over the selected
+    eigenvectors (least squares), eigenvalues of Z -> modulus |lambda|, rate log|lambda| (-30
+    below 1e-12), frequency arg(lambda) / 2 pi, period 1 / |frequency| (inf below 1e-12). The
+    eigenvalues come in numpy's order; compare them as a set."""
+    idx = list(range(dec.k)) if not group else list(group)
+    if not idx or L < 3 or any(i < 0 or i >= dec.k for i in idx):
+        raise ValueError("bad group")
+    U = dec.U[:, idx]
+    Z = np.linalg.lstsq(U[:L - 1], U[1:L], rcond=None)[0]
+    lam = np.linalg.eigvals(Z)
+    mod = np.abs(lam)
+    freq = np.angle(lam) / (2 * np.pi)
+    with np.errstate(divide="ignore"):
+        per = np.where(np.abs(freq) > 1e-12, 1.0 / np.abs(freq), np.inf)
+    rate = np.where(mod > 1e-12, np.log(np.maximum(mod, 1e-300)), -30.0)
+    return {"eig": lam, "moduli": mod, "frequencies": freq, "periods": per, "rates": rate}
+
+
 def variance_explained(dec: Decomposition, start: int, end: int) -> float:
     """ssa_opt_variance_explained (ssa_opt.h:3110-3120)."""
     if start < 0 or dec.total_variance <= 0:

@@ -916,12 +916,362 @@ int ssa_opt_vforecast_fast(const SSA_Opt *ssa, const int *group, int n_group, co
 
 /* ---- out-of-scope symbols kept for the wrapper's optional bindings ---------------------- */
 
+/* ---- ESPRIT (MKL/ssa_opt.h:4304-4558) -----------------------------------------------------
+ * The shift-invariance least squares U_up Z = U_down (U_up / U_down: rows 0..L-2 / 1..L-1 of
+ * the selected eigenvectors) is solved through its normal equations: the two k x k cross Grams
+ * come from the device (FP64 products of the FP32 factors, k_xgram over the factor block and its
+ * one-row-shifted view), and since U has orthonormal columns U_up^T U_up = I - pi pi^T (pi: last
+ * row) is well conditioned unless the group is nearly vertical, where the reference's QR solve
+ * is ill-posed too. The k x k solve and eigenvalues run in FP64 on the host. */
+
+/* Eigenvalues of a real n x n matrix (row-major a, overwritten): Householder reduction to upper
+ * Hessenberg form, then Francis double-shift QR steps on the active window with deflation when a
+ * subdiagonal falls below eps times its diagonal neighbours, 1x1 and 2x2 blocks read off in closed
+ * form (Golub & Van Loan, Matrix Computations, Algorithms 7.4.2, 7.5.1 and 7.5.2; an exceptional
+ * shift every 11th step of a stalled window). Eigenvalues are stored at their diagonal position,
+ * a complex pair with the positive imaginary part first. Returns 0, or -1 without convergence
+ * after 60 n steps. */
+static int eig_nonsym(double *a, int n, double *wr, double *wi)
+{
+#define EA(i, j) a[(size_t)(i) * (size_t)n + (size_t)(j)]
+    const double eps = 2.220446049250313e-16;
+    double *v = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    if (!v)
+        return -1;
+    for (int k = 0; k + 2 < n; k++)
+    {
+        const int m = n - k - 1;
+        double al = 0.0;
+        for (int i = 0; i < m; i++)
+            al += EA(k + 1 + i, k) * EA(k + 1 + i, k);
+        al = sqrt(al);
+        if (al == 0.0)
+            continue;
+        if (EA(k + 1, k) > 0.0)
+            al = -al;
+        for (int i = 0; i < m; i++)
+            v[i] = EA(k + 1 + i, k);
+        v[0] -= al;
+        double vn = 0.0;
+        for (int i = 0; i < m; i++)
+            vn += v[i] * v[i];
+        if (vn == 0.0)
+            continue;
+        for (int j = k; j < n; j++)
+        {
+            double t = 0.0;
+            for (int i = 0; i < m; i++)
+                t += v[i] * EA(k + 1 + i, j);
+            t *= 2.0 / vn;
+            for (int i = 0; i < m; i++)
+                EA(k + 1 + i, j) -= t * v[i];
+        }
+        for (int i = 0; i < n; i++)
+        {
+            double t = 0.0;
+            for (int j = 0; j < m; j++)
+                t += EA(i, k + 1 + j) * v[j];
+            t *= 2.0 / vn;
+            for (int j = 0; j < m; j++)
+                EA(i, k + 1 + j) -= t * v[j];
+        }
+        for (int i = k + 2; i < n; i++)
+            EA(i, k) = 0.0;
+    }
+    free(v);
+    double anorm = 0.0;
+    for (int i = 0; i < n; i++)
+        for (int j = (i > 0 ? i - 1 : 0); j < n; j++)
+            anorm += fabs(EA(i, j));
+    int u = n - 1, iter = 0, total = 0;
+    while (u >= 0)
+    {
+        int l = u;
+        for (; l > 0; l--)
+        {
+            double sc = fabs(EA(l - 1, l - 1)) + fabs(EA(l, l));
+            if (sc == 0.0)
+                sc = anorm;
+            if (fabs(EA(l, l - 1)) <= eps * sc)
+            {
+                EA(l, l - 1) = 0.0;
+                break;
+            }
+        }
+        if (l == u)
+        {
+            wr[u] = EA(u, u);
+            wi[u] = 0.0;
+            u--;
+            iter = 0;
+            continue;
+        }
+        if (l == u - 1)
+        {
+            const double p = EA(u - 1, u - 1), q = EA(u - 1, u), r = EA(u, u - 1), d = EA(u, u);
+            const double mid = 0.5 * (p + d), half = 0.5 * (p - d);
+            const double disc = half * half + q * r;
+            if (disc >= 0.0)
+            {
+                const double sq = sqrt(disc);
+                const double l1 = mid + (mid >= 0.0 ? sq : -sq);
+                const double l2 = l1 != 0.0 ? (p * d - q * r) / l1 : mid - sq;
+                wr[u - 1] = l1;
+                wr[u] = l2;
+                wi[u - 1] = wi[u] = 0.0;
+            }
+            else
+            {
+                wr[u - 1] = wr[u] = mid;
+                wi[u - 1] = sqrt(-disc);
+                wi[u] = -wi[u - 1];
+            }
+            u -= 2;
+            iter = 0;
+            continue;
+        }
+        if (++total > 60 * n)
+            return -1;
+        iter++;
+        double s, t;
+        if (iter % 11 == 10)
+        {
+            const double w = fabs(EA(u, u - 1)) + fabs(EA(u - 1, u - 2));
+            s = 1.5 * w;
+            t = w * w;
+        }
+        else
+        {
+            s = EA(u - 1, u - 1) + EA(u, u);
+            t = EA(u - 1, u - 1) * EA(u, u) - EA(u - 1, u) * EA(u, u - 1);
+        }
+        double x = EA(l, l) * EA(l, l) + EA(l, l + 1) * EA(l + 1, l) - s * EA(l, l) + t;
+        double y = EA(l + 1, l) * (EA(l, l) + EA(l + 1, l + 1) - s);
+        double z = EA(l + 1, l) * EA(l + 2, l + 1);
+        for (int k = l; k <= u - 2; k++)
+        {
+            const double nrm = sqrt(x * x + y * y + z * z);
+            if (nrm != 0.0)
+            {
+                const double beta = x > 0.0 ? -nrm : nrm;
+                const double w0 = x - beta, w1 = y, w2 = z;
+                const double ww = w0 * w0 + w1 * w1 + w2 * w2;
+                if (ww != 0.0)
+                {
+                    for (int j = (k > l ? k - 1 : l); j <= u; j++)
+                    {
+                        const double f = 2.0 * (w0 * EA(k, j) + w1 * EA(k + 1, j) + w2 * EA(k + 2, j)) / ww;
+                        EA(k, j) -= f * w0;
+                        EA(k + 1, j) -= f * w1;
+                        EA(k + 2, j) -= f * w2;
+                    }
+                    const int r1 = k + 3 < u ? k + 3 : u;
+                    for (int i = l; i <= r1; i++)
+                    {
+                        const double f = 2.0 * (EA(i, k) * w0 + EA(i, k + 1) * w1 + EA(i, k + 2) * w2) / ww;
+                        EA(i, k) -= f * w0;
+                        EA(i, k + 1) -= f * w1;
+                        EA(i, k + 2) -= f * w2;
+                    }
+                    if (k > l)
+                    {
+                        EA(k + 1, k - 1) = 0.0;
+                        EA(k + 2, k - 1) = 0.0;
+                    }
+                }
+            }
+            x = EA(k + 1, k);
+            y = EA(k + 2, k);
+            if (k < u - 2)
+                z = EA(k + 3, k);
+        }
+        const double nrm = sqrt(x * x + y * y);
+        if (nrm != 0.0)
+        {
+            const double beta = x > 0.0 ? -nrm : nrm;
+            const double w0 = x - beta, w1 = y;
+            const double ww = w0 * w0 + w1 * w1;
+            if (ww != 0.0)
+            {
+                for (int j = u - 2; j <= u; j++)
+                {
+                    const double f = 2.0 * (w0 * EA(u - 1, j) + w1 * EA(u, j)) / ww;
+                    EA(u - 1, j) -= f * w0;
+                    EA(u, j) -= f * w1;
+                }
+                for (int i = l; i <= u; i++)
+                {
+                    const double f = 2.0 * (EA(i, u - 1) * w0 + EA(i, u) * w1) / ww;
+                    EA(i, u - 1) -= f * w0;
+                    EA(i, u) -= f * w1;
+                }
+                EA(u, u - 2) = 0.0;
+            }
+        }
+    }
+#undef EA
+    return 0;
+}
+
+int ssa_b200_eigvals(int n, const double *A, double *wr, double *wi)
+{
+    if (n < 1 || !A || !wr || !wi)
+        return -1;
+    double *a = (double *)malloc(sizeof(double) * (size_t)n * (size_t)n);
+    if (!a)
+        return -1;
+    memcpy(a, A, sizeof(double) * (size_t)n * (size_t)n);
+    const int rc = eig_nonsym(a, n, wr, wi);
+    free(a);
+    return rc;
+}
+
 int ssa_opt_parestimate(const SSA_Opt *ssa, const int *group, int n_group, SSA_ParEstimate *result)
 {
-    (void)ssa, (void)group, (void)n_group;
-    if (result)
+    if (!ssa || !ssa->decomposed || !result)
+        return -1;
+    const int nc = ssa->n_components;
+    const int k = (n_group > 0 && group) ? n_group : nc;
+    if (k < 1 || k > nc)
+        return -1;
+    const int L = ssa->L;
+    if (L < 3)
+        return -1;
+    int *idx = (int *)malloc(sizeof(int) * (size_t)k);
+    if (!idx)
+        return -1;
+    for (int j = 0; j < k; j++)
+    {
+        idx[j] = (n_group > 0 && group) ? group[j] : j;
+        if (idx[j] < 0 || idx[j] >= nc)
+        {
+            free(idx);
+            return -1;
+        }
+    }
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    ssa_engine *e = &g->e;
+    const int m = L - 1;
+    int rows = (m + 127) / 128;
+    rows = ((rows + SSA_GRAM_CHUNK - 1) / SSA_GRAM_CHUNK) * SSA_GRAM_CHUNK;
+    const int nch = (m + rows - 1) / rows;
+    const size_t np = (size_t)nch * nc * nc;
+    double *d_part = NULL, *h_part = (double *)malloc(sizeof(double) * 2 * np);
+    double *G = (double *)calloc((size_t)nc * nc * 2, sizeof(double));
+    double *Z = (double *)malloc(sizeof(double) * (size_t)k * k * 3);
+    double *wr = (double *)malloc(sizeof(double) * (size_t)k * 2);
+    int rc = !h_part || !G || !Z || !wr || cudaMalloc((void **)&d_part, sizeof(double) * 2 * np) != cudaSuccess;
+    if (!rc)
+    {
+        /* job 0: U_up^T U_up, job 1: U_up^T U_down (the same block one row further down) */
+        ssa_xgram_job J[2];
+        memset(J, 0, sizeof(J));
+        for (int q = 0; q < 2; q++)
+        {
+            J[q].A = e->Y;
+            J[q].B = e->Y + q;
+            J[q].part = d_part + (size_t)q * np;
+            J[q].lda = J[q].ldb = e->ldL;
+            J[q].m = m;
+            J[q].na = J[q].nb = nc;
+            J[q].rows_per_cta = rows;
+        }
+        ssae_reset_jobs(e);
+        void *d = ssae_push_jobs(e, J, sizeof(J));
+        rc = !d || ssad_xgram((const ssa_xgram_job *)d, 2, nch, e->st) != 0 ||
+             cudaMemcpyAsync(h_part, d_part, sizeof(double) * 2 * np, cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
+             sync_ok(g) != 0;
+    }
+    if (d_part)
+        cudaFree(d_part);
+    if (!rc)
+    {
+        for (int q = 0; q < 2; q++)
+            for (int c = 0; c < nch; c++)
+                for (size_t t = 0; t < (size_t)nc * nc; t++)
+                    G[(size_t)q * nc * nc + t] += h_part[(size_t)q * np + (size_t)c * nc * nc + t];
+        /* the group's k x k blocks: Gs = U_up^T U_up, Cs = U_up^T U_down (row-major) */
+        double *Gs = Z + (size_t)k * k, *Cs = Gs + (size_t)k * k;
+        for (int a = 0; a < k; a++)
+            for (int b = 0; b < k; b++)
+            {
+                Gs[a * k + b] = G[(size_t)idx[a] * nc + idx[b]];
+                Cs[a * k + b] = G[(size_t)nc * nc + (size_t)idx[a] * nc + idx[b]];
+            }
+        /* Cholesky Gs = R^T R (upper R in place), then Z = R^-1 R^-T Cs */
+        for (int j = 0; j < k && !rc; j++)
+        {
+            double d = Gs[j * k + j];
+            for (int p = 0; p < j; p++)
+                d -= Gs[p * k + j] * Gs[p * k + j];
+            if (!(d > 0.0))
+            {
+                rc = 1;
+                break;
+            }
+            d = sqrt(d);
+            Gs[j * k + j] = d;
+            for (int c = j + 1; c < k; c++)
+            {
+                double t = Gs[j * k + c];
+                for (int p = 0; p < j; p++)
+                    t -= Gs[p * k + j] * Gs[p * k + c];
+                Gs[j * k + c] = t / d;
+            }
+        }
+        if (!rc)
+        {
+            for (int c = 0; c < k; c++)
+            {
+                /* solve R^T y = Cs[:, c], then R z = y */
+                for (int i = 0; i < k; i++)
+                {
+                    double t = Cs[i * k + c];
+                    for (int p = 0; p < i; p++)
+                        t -= Gs[p * k + i] * Z[p * k + c];
+                    Z[i * k + c] = t / Gs[i * k + i];
+                }
+                for (int i = k - 1; i >= 0; i--)
+                {
+                    double t = Z[i * k + c];
+                    for (int p = i + 1; p < k; p++)
+                        t -= Gs[i * k + p] * Z[p * k + c];
+                    Z[i * k + c] = t / Gs[i * k + i];
+                }
+            }
+            rc = eig_nonsym(Z, k, wr, wr + k) != 0;
+        }
+    }
+    if (!rc)
+    {
         memset(result, 0, sizeof(*result));
-    return -1;
+        result->periods = (double *)malloc(sizeof(double) * (size_t)k);
+        result->frequencies = (double *)malloc(sizeof(double) * (size_t)k);
+        result->moduli = (double *)malloc(sizeof(double) * (size_t)k);
+        result->rates = (double *)malloc(sizeof(double) * (size_t)k);
+        result->n_components = k;
+        if (!result->periods || !result->frequencies || !result->moduli || !result->rates)
+        {
+            ssa_opt_parestimate_free(result);
+            rc = 1;
+        }
+        for (int i = 0; i < k && !rc; i++)
+        {
+            const double re = wr[i], im = wr[k + i];
+            const double mod = sqrt(re * re + im * im);
+            const double freq = atan2(im, re) / (2.0 * M_PI);
+            result->moduli[i] = mod;
+            result->rates[i] = mod > 1e-12 ? log(mod) : -30.0;
+            result->frequencies[i] = freq;
+            result->periods[i] = fabs(freq) > 1e-12 ? 1.0 / fabs(freq) : INFINITY;
+        }
+    }
+    free(idx);
+    free(h_part);
+    free(G);
+    free(Z);
+    free(wr);
+    return rc ? -1 : 0;
 }
 void ssa_opt_parestimate_free(SSA_ParEstimate *result)
 {

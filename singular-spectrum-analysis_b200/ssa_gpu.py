@@ -188,6 +188,60 @@ _sig("ssa_opt_gapfill", _I, c_double_p, _I, _I, _I, _I, _D, ctypes.POINTER(_SSA_
 _sig("ssa_opt_gapfill_simple", _I, c_double_p, _I, _I, _I, ctypes.POINTER(_SSA_GapFillResult))
 
 
+class _SSA_ParEstimate(ctypes.Structure):
+    _fields_ = [("periods", c_double_p), ("frequencies", c_double_p), ("moduli", c_double_p),
+                ("rates", c_double_p), ("n_components", ctypes.c_int)]
+
+
+_sig("ssa_opt_parestimate", _I, _P, c_int_p, _I, ctypes.POINTER(_SSA_ParEstimate))
+_sig("ssa_opt_parestimate_free", _V, ctypes.POINTER(_SSA_ParEstimate))
+_sig("ssa_b200_eigvals", _I, _I, c_double_p, c_double_p, c_double_p)
+
+
+class ParEstimate:
+    """ESPRIT result (MKL/py/ssa_wrapper.py:326-413): periods (inf for a trend), frequencies
+    (cycles per sample), moduli (1 = undamped) and rates (log modulus) per eigenvalue."""
+
+    def __init__(self, periods, frequencies, moduli, rates):
+        self.periods = periods
+        self.frequencies = frequencies
+        self.moduli = moduli
+        self.rates = rates
+        self.n_components = len(periods)
+
+    def __repr__(self):
+        return f"ParEstimate(n_components={self.n_components})"
+
+    def summary(self) -> str:
+        lines = ["ESPRIT Frequency Estimation Results", "=" * 50,
+                 f"{'Comp':<6} {'Period':<12} {'Frequency':<12} {'Modulus':<10} {'Rate':<10}", "-" * 50]
+        for i in np.argsort(-self.periods):
+            p = self.periods[i]
+            ps = "Inf (trend)" if np.isinf(p) else f"{p:.2f}"
+            lines.append(f"{i:<6} {ps:<12} {self.frequencies[i]:<12.6f} {self.moduli[i]:<10.4f} {self.rates[i]:<10.4f}")
+        return "\n".join(lines)
+
+    def get_periodic_components(self, min_period: float = 2.0, max_period: Optional[float] = None,
+                                min_modulus: float = 0.9) -> List[int]:
+        out = []
+        for i in range(self.n_components):
+            p, mod = self.periods[i], self.moduli[i]
+            if np.isinf(p) or p < min_period or (max_period is not None and p > max_period) or mod < min_modulus:
+                continue
+            out.append(i)
+        return out
+
+
+def eigvals(A: np.ndarray) -> np.ndarray:
+    """Eigenvalues of a real square matrix with the library's host solver (ssa_b200_eigvals)."""
+    a = np.ascontiguousarray(A, dtype=np.float64)
+    n = a.shape[0]
+    wr, wi = np.zeros(n), np.zeros(n)
+    if _lib.ssa_b200_eigvals(n, _dp(a), _dp(wr), _dp(wi)) != 0:
+        raise RuntimeError("eigenvalues did not converge")
+    return wr + 1j * wi
+
+
 class GapFillResult:
     """Result of gap filling (MKL/py/ssa_wrapper.py:496-509)."""
 
@@ -474,8 +528,23 @@ class SSA:
             raise RuntimeError("copy_factors failed")
         return U.T.copy(), V.T.copy(), self.singular_values
 
-    def parestimate(self, group: Optional[List[int]] = None):
-        raise RuntimeError("ESPRIT (parestimate) is not part of the accelerated path")
+    def parestimate(self, group: Optional[List[int]] = None) -> "ParEstimate":
+        """ESPRIT periods / frequencies / moduli / rates of the selected components (all when
+        group is None), MKL/py/ssa_wrapper.py:1061-1130 -> ssa_opt_parestimate."""
+        self._need()
+        res = _SSA_ParEstimate()
+        if group is not None and len(group) > 0:
+            g = np.ascontiguousarray(group, dtype=np.int32)
+            ret = _lib.ssa_opt_parestimate(ctypes.byref(self._ctx), _ip(g), len(g), ctypes.byref(res))
+        else:
+            ret = _lib.ssa_opt_parestimate(ctypes.byref(self._ctx), None, 0, ctypes.byref(res))
+        if ret != 0:
+            raise RuntimeError("parestimate failed")
+        n = res.n_components
+        arrs = [np.ctypeslib.as_array(getattr(res, f), shape=(n,)).copy()
+                for f in ("periods", "frequencies", "moduli", "rates")]
+        _lib.ssa_opt_parestimate_free(ctypes.byref(res))
+        return ParEstimate(*arrs)
 
 
 class MSSA:

@@ -1,11 +1,13 @@
 """CPU checks of the drop-in boundary: libssa.so loads without a GPU, exports every function
 declared in include/*.h and the export list of the reference shared library, and the unchanged
-reference ctypes wrapper binds against it. No compute calls are made here."""
+reference ctypes wrapper binds against it. No device calls are made here (the one compute call
+is the host eigen-solver)."""
 import ctypes
 import re
 import subprocess
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
@@ -87,3 +89,29 @@ def test_unchanged_reference_wrapper_binds(lib):
     env = dict(os.environ, LD_LIBRARY_PATH=str(LIB.parent))
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env)
     assert r.returncode == 0 and "ok" in r.stdout, r.stderr
+
+
+def test_host_eigen_solver_vs_numpy():
+    """ssa_b200_eigvals (the ESPRIT eigen-solver: Hessenberg + Francis double-shift QR) against
+    numpy on random, rotation-block, companion and defective matrices; no GPU call."""
+    import ssa_gpu
+
+    rng = np.random.default_rng(3)
+    cases = [rng.standard_normal((n, n)) for n in (1, 2, 3, 5, 8, 17, 40, 64)]
+    th = [0.1, 0.7, 2.0]
+    R = np.zeros((6, 6))
+    for i, t in enumerate(th):
+        c, s = np.cos(t), np.sin(t)
+        R[2 * i:2 * i + 2, 2 * i:2 * i + 2] = [[c, -s], [s, c]]
+    Q = np.linalg.qr(rng.standard_normal((6, 6)))[0]
+    cases.append(Q @ R @ Q.T)  # eigenvalues on the unit circle
+    comp = np.zeros((7, 7))
+    comp[0, :] = -np.poly(np.arange(1, 8))[1:]
+    comp[1:, :-1] = np.eye(6)
+    cases.append(comp)  # companion matrix, roots 1..7
+    cases.append(np.array([[2.0, 1.0], [0.0, 2.0]]))  # defective
+    for A in cases:
+        got = np.sort_complex(ssa_gpu.eigvals(A))
+        ref = np.sort_complex(np.linalg.eigvals(A))
+        scale = max(1.0, np.abs(ref).max())
+        assert np.max(np.abs(got - ref)) <= 1e-8 * scale, (A.shape, np.max(np.abs(got - ref)))

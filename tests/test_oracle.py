@@ -272,3 +272,19 @@ def test_gap_linear_start(oracle):
     y = np.array([np.nan, 2.0])
     oracle.gap_linear_start(y, np.isnan(y))
     assert y[0] == 2.0
+
+
+def test_parestimate_reference_known_answers(oracle):
+    """The oracle's ESPRIT meets the reference's known answers (MKL/test/ssa_opt_test.c:1055-1100,
+    2062-2113) on the exact SVD: periods 50 and 20 within 2 samples with moduli > 0.9; periods
+    60, 30 and 15 within 5 %."""
+    i = np.arange(500, dtype=np.float64)
+    x = 3.0 * np.sin(2 * np.pi * i / 50.0) + 2.0 * np.sin(2 * np.pi * i / 20.0)
+    r = oracle.parestimate(oracle.dense_svd(x, 125, 6), [0, 1, 2, 3], 125)
+    assert any(abs(p - 50.0) < 2.0 for p in r["periods"]) and any(abs(p - 20.0) < 2.0 for p in r["periods"])
+    assert all(m > 0.9 for p, m in zip(r["periods"], r["moduli"]) if 5 < p < 100)
+    i = np.arange(600, dtype=np.float64)
+    x = 4.0 * np.sin(2 * np.pi * i / 60.0) + 2.0 * np.sin(2 * np.pi * i / 30.0) + np.sin(2 * np.pi * i / 15.0)
+    r = oracle.parestimate(oracle.dense_svd(x, 150, 8), [0, 1, 2, 3, 4, 5], 150)
+    for tp in (60.0, 30.0, 15.0):
+        assert min(abs(p - tp) / tp for p, m in zip(r["periods"], r["moduli"]) if m > 0.9) < 0.05
