@@ -417,10 +417,30 @@ int ssa_opt_decompose(SSA_Opt *ssa, int k, int max_iter)
 /* ssa_opt_extend (MKL/ssa_opt.h:1935-2056) is outside the accelerated path: it reports failure. */
 int ssa_opt_extend(SSA_Opt *ssa, int additional_k, int max_iter)
 {
-    (void)ssa;
-    (void)additional_k;
-    (void)max_iter;
-    return -1;
+    if (!ssa || !ssa->decomposed || additional_k < 1 || max_iter < 0)
+        return -1;
+    ssa_opt_free_cached_ffts(ssa);
+    const int L = ssa->L, K = ssa->K, old_k = ssa->n_components;
+    const int new_k = imin(old_k + additional_k, imin(L, K));
+    if (new_k <= old_k)
+        return 0;
+    struct ssa_gpu_ctx *g = ssa->gpu;
+    ssa_engine *e = &g->e;
+    if (new_k > e->k || new_k > SSA_MAX_KP)
+        return -1;
+    ssae_reset_jobs(e);
+    g->spectra_valid = 0;
+    g->wcorr_valid = 0;
+    const unsigned long long seed =
+        (SSA_DEFAULT_SEED + 0x100000000ULL * (unsigned long long)ssa->rng_calls) ^ 0xB10CB10CB10CB10CULL;
+    ssa->rng_calls++;
+    ssa->decomposed = false;
+    if (ssae_extend(e, old_k, new_k, max_iter, seed) != 0 || sync_ok(g) != 0 || check_status(g) != 0 ||
+        alloc_results(ssa, new_k) != 0 || mirror_results(ssa, new_k) != 0)
+        return -1;
+    ssa->n_components = new_k;
+    ssa->decomposed = true;
+    return 0;
 }
 
 /* ---- spectra cache and reconstruction -------------------------------------------------- */

@@ -907,13 +907,17 @@ static int deflate(ssa_engine *e, int nb, float *Xm, size_t xs, long long ldx, i
     return rc;
 }
 
-int ssae_decompose_block(ssa_engine *e, int nb, int k, int bsize, int max_iter, const float *d_V0, long long v0_ld,
-                         unsigned long long seed)
+/* Block power iteration for components [comp0, k); components [0, comp0) are already in Y, Z
+ * and sigma (deflated against, re-sorted with the new ones, their signs kept). */
+static int block_power(ssa_engine *e, int nb, int k, int comp0, int bsize, int max_iter, const float *d_V0,
+                       long long v0_ld, unsigned long long seed)
 {
     const int L = e->L, K = e->K;
-    if (nb < 1 || nb > e->B || k < 1 || bsize < 1 || max_iter < 0)
+    if (nb < 1 || nb > e->B || k < 1 || bsize < 1 || max_iter < 0 || comp0 < 0)
         return (int)cudaErrorInvalidValue;
     k = imin(k, imin(L, K));
+    if (comp0 >= k)
+        return (int)cudaErrorInvalidValue;
     const int b = imin(bsize, k);
     if (k > e->kp || k > e->k || b > SSA_MAX_KP)
         return (int)cudaErrorInvalidValue;
@@ -923,7 +927,7 @@ int ssae_decompose_block(ssa_engine *e, int nb, int k, int bsize, int max_iter, 
     const size_t sUb = (size_t)e->ldL * 2 * e->bcap, sVb = (size_t)e->ldK * e->bcap;
     float *Ub = e->Ub, *Ub2 = e->Ub + (size_t)e->ldL * e->bcap, *Vb = e->Vb;
     const size_t s64 = (size_t)SSA_MAX_KP * SSA_MAX_KP;
-    int comp = 0;
+    int comp = comp0;
     while (comp < k)
     {
         const int cb = imin(b, k - comp);
@@ -1040,6 +1044,7 @@ int ssae_decompose_block(ssa_engine *e, int nb, int k, int bsize, int max_iter, 
             ss[s].ldU = e->ldL;
             ss[s].L = L;
             ss[s].k = k;
+            ss[s].sign_from = comp0;
             /* Y -> Ut and Z -> Vt permuted, then copied back unpermuted-identity */
             ssa_permcols_job *a = &pc[4 * s];
             a[0].src = e->Y + (size_t)s * sY;
@@ -1105,6 +1110,17 @@ int ssae_decompose_block(ssa_engine *e, int nb, int k, int bsize, int max_iter, 
         }
     }
     return 0;
+}
+
+int ssae_decompose_block(ssa_engine *e, int nb, int k, int bsize, int max_iter, const float *d_V0, long long v0_ld,
+                         unsigned long long seed)
+{
+    return block_power(e, nb, k, 0, bsize, max_iter, d_V0, v0_ld, seed);
+}
+
+int ssae_extend(ssa_engine *e, int k_old, int k_new, int max_iter, unsigned long long seed)
+{
+    return block_power(e, 1, k_new, k_old, 1, max_iter, NULL, 0, seed);
 }
 
 /* ------------------------------------------------------------------------------------------ */

@@ -136,6 +136,10 @@ int ssae_matvec(ssa_engine *e, int ncols, int adjoint);
 int ssae_decompose_block(ssa_engine *e, int nb, int k, int bsize, int max_iter, const float *d_V0,
                          long long v0_ld, unsigned long long seed);
 int ssae_ensure_block(ssa_engine *e, int bcap);
+/* Components k_old .. k_new - 1 of series 0 added to the k_old already in Y, Z and sigma by
+ * one-column power iterations deflated against them (reference MKL/ssa_opt.h:1935-2056), then
+ * all k_new re-sorted by sigma; the sign rule applies to sorted positions >= k_old. */
+int ssae_extend(ssa_engine *e, int k_old, int k_new, int max_iter, unsigned long long seed);
 /* MSSA randomized decomposition of one instance whose M channels are the engine's first M
  * series (reference MKL/ssa_opt.h:4116-4210, plus q power iterations). d_omega: device K x kp
  * test matrix (ld ldK) or NULL for the generator with `seed`. Results: U_m in Y_m (L x k per

@@ -1260,7 +1260,7 @@ __global__ void __launch_bounds__(256) k_sortsign(const ssa_sortsign_job* __rest
         for (int i = 0; i < k; ++i) {
             J.sigma[i] = sv[i];
             J.perm[i] = pm[i];
-            J.sign[i] = colsum[pm[i]] < 0.0 ? -1.f : 1.f;
+            J.sign[i] = (i >= J.sign_from && colsum[pm[i]] < 0.0) ? -1.f : 1.f;
         }
     }
 }

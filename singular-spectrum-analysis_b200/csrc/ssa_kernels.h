@@ -154,6 +154,7 @@ typedef struct
     float *sign;
     long long ldU;
     int L, k;
+    int sign_from; /* the sign rule applies to sorted positions >= sign_from (0: all) */
 } ssa_sortsign_job;
 
 /* dst[:, j] = sign[j] * src[:, perm[j]] for j < k, rows < m. */

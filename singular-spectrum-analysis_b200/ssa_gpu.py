@@ -99,6 +99,7 @@ _sig("mssa_opt_series_contributions", _I, _P, c_double_p)
 _sig("mssa_opt_variance_explained", _D, _P, _I, _I)
 _sig("mssa_opt_free", _V, _P)
 _sig("ssa_opt_copy_factors", _I, _P, c_double_p, c_double_p)
+_sig("ssa_opt_extend", _I, _P, _I, _I)
 _sig("mssa_opt_copy_factors", _I, _P, c_double_p, c_double_p, c_double_p)
 _sig("ssa_opt_cadzow_inplace", _I, _P, _I, _I, _D, ctypes.POINTER(_SSA_CadzowResult))
 _sig("ssa_b200_kernel_launches", ctypes.c_ulonglong)
@@ -527,6 +528,15 @@ class SSA:
         if _lib.ssa_opt_copy_factors(ctypes.byref(self._ctx), _dp(U), _dp(V)) != k:
             raise RuntimeError("copy_factors failed")
         return U.T.copy(), V.T.copy(), self.singular_values
+
+    def extend(self, additional_k: int, max_iter: int = 100) -> "SSA":
+        """Add components to the current decomposition by deflated one-column power iterations
+        (ssa_opt_extend, MKL/ssa_opt.h:1935-2056); all are then re-sorted by sigma."""
+        self._need()
+        if _lib.ssa_opt_extend(ctypes.byref(self._ctx), additional_k, max_iter) != 0:
+            raise RuntimeError("extend failed")
+        self.n_components = int(_lib.ssa_opt_copy_factors(ctypes.byref(self._ctx), None, None))
+        return self
 
     def parestimate(self, group: Optional[List[int]] = None) -> "ParEstimate":
         """ESPRIT periods / frequencies / moduli / rates of the selected components (all when

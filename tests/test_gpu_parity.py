@@ -175,6 +175,42 @@ def test_vforecast_parity(gpu, oracle):
         gs.vforecast([0, 99], 5)  # index outside the decomposition
 
 
+def test_extend_matches_exact_svd(gpu, oracle):
+    """ssa_opt_extend (MKL/ssa_opt.h:1935-2056): components added to a randomized decomposition by
+    deflated one-column power iterations reach the exact SVD's (sigma within 1e-5 relative for
+    well-separated values; U columns within 5e-4 up to sign: FP32 iterates, and a singular
+    vector's error grows as 1/gap, 1e-4 measured at gaps of a few percent), all re-sorted by
+    sigma; the new
+    components follow the sign rule, the old ones keep theirs."""
+    x, _, Om = oracle.config1(seed=0)
+    N, L = 1000, 250
+    t = oracle.dense_svd(x, L, 12)
+    gs = gpu.SSA(x, L)
+    gs.decompose(4, oversampling=10, power_iters=2, omega=Om[:, :14])
+    U0, _, _ = gs.factors()
+    gs.extend(3, max_iter=200)
+    assert gs.n_components == 7
+    s = gs.singular_values
+    assert np.all(np.diff(s) <= 0)
+    U, V, _ = gs.factors()
+    for i in range(7):
+        gap = min(abs(t.sigma[i] - t.sigma[j]) / t.sigma[i] for j in range(12) if j != i)
+        if gap > 1e-2:
+            assert abs(s[i] - t.sigma[i]) / t.sigma[i] <= 1e-5, i
+            d = min(np.linalg.norm(U[:, i] - t.U[:, i]), np.linalg.norm(U[:, i] + t.U[:, i]))
+            assert d <= 5e-4, (i, d)
+    assert np.all(U[:, 4:].sum(axis=0) >= 0)
+    np.testing.assert_array_equal(U[:, :4], U0)  # the old factors are kept as they were
+    # the largest leading group that does not split a near-degenerate pair (boundary gap > 1e-2)
+    m = max(j for j in range(1, 8) if abs(t.sigma[j - 1] - t.sigma[j]) / t.sigma[j - 1] > 1e-2)
+    assert m >= 4
+    assert rel_l2(gs.reconstruct(list(range(m))), oracle.reconstruct(t, list(range(m)), N, L)) <= 1e-4
+    with pytest.raises(RuntimeError):
+        gs.extend(100, max_iter=5)  # beyond the 64-column capacity of the context
+    with pytest.raises(RuntimeError):
+        gpu.SSA(x, L).extend(2)  # nothing decomposed yet
+
+
 def test_reconstruct_edge_groups(gpu, oracle):
     x, _, Om = oracle.config1(seed=0)
     N, L, k, p = 1000, 250, 8, 4
