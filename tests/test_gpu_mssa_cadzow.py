@@ -88,6 +88,34 @@ def test_mssa_parity_host_omega(gpu, oracle, q):
     assert abs(ve - d.eigenvalues[:4].sum() / d.total_variance) < 1e-6
 
 
+def test_mssa_config4_full_size(gpu, oracle):
+    """One instance at the full MSSA workload shape (M = 16 channels, N = 20000, L = 5000, k = 50,
+    p = 10, q = 2, host test matrix), then 10 rank-50 Cadzow iterations on a channel, against the
+    oracle; same tolerances as above."""
+    rng = np.random.default_rng(3)
+    X = oracle.config4_instance(rng, Mch=16, N=20000)
+    Mch, N = X.shape
+    L, k, p = 5000, 50, 10
+    K = N - L + 1
+    Om = rng.standard_normal((K, k + p))
+    d = oracle.mssa_decompose(X, L, k, p, Om, q=2)
+    m = gpu.MSSA(X, L)
+    m.decompose(k, oversampling=p, power_iters=2, omega=Om)
+    check_sigma(m.singular_values, d.sigma)
+    for ch in (0, Mch - 1):
+        for g in ([0], [1, 2]):
+            e = rel_l2(m.reconstruct(ch, g), oracle.mssa_reconstruct(d, ch, g, Mch, N, L))
+            assert e <= rec_tol(d.sigma, g), (ch, g, e)
+    x = X[0]
+    rank, iters = 50, 10
+    Omc = oracle.device_gaussian(oracle.single_series_seed(0), K, rank + 8)
+    y_ref, it_ref, diff_ref, _ = oracle.cadzow(x, L, rank, iters, 1e-14, Omc)
+    r = gpu.cadzow(x, L, rank, max_iter=iters, tol=1e-14)
+    assert r.iterations == it_ref == iters
+    assert rel_l2(r.signal, y_ref) <= CADZOW_TOL
+    assert abs(r.final_diff - diff_ref) <= 1e-5
+
+
 def test_mssa_default_generator_matches_replica(gpu, oracle):
     X, _ = mssa_case(oracle, seed=5, Mch=3, N=1200)
     Mch, N = X.shape
