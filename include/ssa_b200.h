@@ -131,6 +131,11 @@ int ssa_rbatch_run_ex(ssa_rbatch *b, int B, const int *N, const int *L, const in
 int ssa_rbatch_run_device_ex(ssa_rbatch *b, int B, const int *N, const int *L, const int *k, const double *d_x,
                              uint64_t seed, const unsigned char *want_w);
 int ssa_rbatch_sync(ssa_rbatch *b);
+/* Real FFT length an uneven batch (and the server) uses for a series of length N: the smallest
+ * of 2^a (a <= 17), 49152 and 98304 that is >= N (at least 32), or -1 beyond N = 131072. The
+ * single-series API and the uniform batch use the power of two. No counterpart in the reference
+ * (whose FFT length is the power of two >= N + K - 1). */
+int ssa_b200_fft_length(int N);
 /* Every buffer of a run lives in one device arena, grown in stream order when a run needs more;
  * reserving it up front keeps growth (and the driver allocation behind it) out of later runs. */
 int ssa_rbatch_reserve(ssa_rbatch *b, size_t bytes);

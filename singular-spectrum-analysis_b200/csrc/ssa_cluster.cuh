@@ -1,5 +1,7 @@
-// FFT lengths beyond one CTA's shared memory (real length M = 2^16 and 2^17, i.e. series up to
-// N = 131072): each transform runs on a thread-block cluster of C = H / 8192 CTAs.
+// FFT lengths beyond one CTA's shared memory: each transform runs on a thread-block cluster of
+// C CTAs of H1 = 8192 points, H = C H1 complex points (real length M = 2H): C = 4 and 8 for
+// M = 2^16 and 2^17, C = 3 and 6 for M = 3 * 2^14 and 3 * 2^15, which cut the padding of the
+// series between the powers of two (series up to N = 131072).
 //
 // Packed sequence z[n] = a[2n] + i a[2n+1], n < H = C H1 (H1 = 8192). CTA r of the cluster holds
 // the decimated sequence z_r[m] = z[C m + r] and transforms it locally (fft_block, H1 points):
@@ -24,25 +26,41 @@
 
 namespace cg = cooperative_groups;
 
-#ifndef SSA_CL_LOGH1
+// 8192-point CTAs, two per SM (16384-point CTAs, one per SM, measured 1.3% slower)
 #define SSA_CL_LOGH1 13
-#endif
 #define SSA_CL_MAX_LOGH 16
 
-template <int LOGH>
+__host__ __device__ constexpr int cl_ilog2(int v) { return v <= 1 ? 0 : 1 + cl_ilog2(v >> 1); }
+
+template <int C_>
 struct ClShape {
     static constexpr int LOGH1 = SSA_CL_LOGH1;
     static constexpr int H1 = 1 << LOGH1;
-    static constexpr int C = 1 << (LOGH - LOGH1);
-    static constexpr int H = 1 << LOGH;
+    static constexpr int C = C_;
+    static constexpr int H = C * H1;
     static constexpr int BLOCK = FftShape<LOGH1>::BLOCK;
     static constexpr int MINB = BLOCK >= 1024 ? 1 : 2;  // CTAs per SM the kernels are built for
     static constexpr int NITEM = H1 / 2 + 1;  // k1 = 0 .. H1/2, each with its mirror
+    static constexpr bool POW2 = (C & (C - 1)) == 0;
+    static_assert(POW2 || C % 3 == 0, "cluster sizes are 2^a or 3 * 2^a");
+    // twiddle table of resolution M = 2H: 2^LOGM, or 3 * 2^A3
+    static constexpr int LOGM = cl_ilog2(2 * H);
+    static constexpr int A3 = cl_ilog2(2 * H / 3);
+    using Tw = typename std::conditional<POW2, TwSplit<(POW2 ? LOGM : 1)>, TwSplit3<(POW2 ? 9 : A3)>>::type;
 };
 
-template <int LOGH>
+template <int C>
+__device__ __forceinline__ void cl_load_twM(float2* tab) {
+    using S = ClShape<C>;
+    if constexpr (S::POW2)
+        load_twiddles<S::LOGM>(tab);
+    else
+        load_twiddles3<S::A3>(tab);
+}
+
+template <int C>
 __host__ __device__ constexpr int cl_smem_f2() {
-    return spad_size(ClShape<LOGH>::H1) + TwSplit<SSA_CL_LOGH1 + 1>::N + TwSplit<LOGH + 1>::N;
+    return spad_size(ClShape<C>::H1) + TwSplit<SSA_CL_LOGH1 + 1>::N + ClShape<C>::Tw::N;
 }
 
 enum { CL_SPEC = 0, CL_CORR = 1, CL_ELEM = 2, CL_RECON = 3 };
@@ -70,17 +88,17 @@ __device__ __forceinline__ float2 cl_group_product(const ssa_recon_job& J, int k
 
 // Bins k and H - k (1 <= k <= H/2) of the packed transform in zk, zm are replaced by the packed
 // output spectrum (or, for CL_SPEC, the real spectrum is written out).
-template <int LOGH, int KIND>
+template <int C, int KIND>
 __device__ __forceinline__ void cl_pair(const ClOp& op, int k, float2& zk, float2& zm, const float2* twM) {
-    constexpr int H = 1 << LOGH;
-    const float2 w = twiddle<LOGH + 1, false>(twM, k);
+    constexpr int H = ClShape<C>::H;
+    const float2 w = twiddle_s<typename ClShape<C>::Tw, false>(twM, k);
     float2 pk, pm;
     if constexpr (KIND == CL_RECON) {
         pk = cl_group_product(*op.R, k);
         pm = cl_group_product(*op.R, H - k);
     } else {
         float2 ak, am;
-        unpack_pair<LOGH>(zk, zm, w, ak, am);
+        unpack_pair<0>(zk, zm, w, ak, am);
         if constexpr (KIND == CL_SPEC) {
             op.spec[k] = ak;
             op.spec[H - k] = am;
@@ -97,9 +115,9 @@ __device__ __forceinline__ void cl_pair(const ClOp& op, int k, float2& zk, float
 }
 
 // Bin 0 with the Nyquist bin H, both real, packed together in z0.
-template <int LOGH, int KIND>
+template <int C, int KIND>
 __device__ __forceinline__ void cl_dc(const ClOp& op, float2& z0) {
-    constexpr int H = 1 << LOGH;
+    constexpr int H = ClShape<C>::H;
     float2 zk, zm;
     if constexpr (KIND == CL_SPEC) {
         op.spec[0] = make_float2(z0.x + z0.y, 0.f);
@@ -149,9 +167,9 @@ __device__ __forceinline__ void cl_twiddle(float2* z, float2 w) {
 // Owner phase over this CTA's items: gather (unless CL_RECON), spectral operation, scatter
 // (unless CL_SPEC). sbase is the shared-window address of this CTA's transform buffer; the
 // same offset in CTA q's window is CTA q's slot.
-template <int LOGH, int KIND>
+template <int C_, int KIND>
 __device__ __forceinline__ void cl_exchange(uint32_t sbase, const float2* twM, int rank, const ClOp& op) {
-    using S = ClShape<LOGH>;
+    using S = ClShape<C_>;
     constexpr int C = S::C, H1 = S::H1, H = S::H;
     for (int g = rank * S::BLOCK + (int)threadIdx.x; g < S::NITEM; g += C * S::BLOCK) {
         const int ka = g, kb = (H1 - g) & (H1 - 1);
@@ -160,8 +178,8 @@ __device__ __forceinline__ void cl_exchange(uint32_t sbase, const float2* twM, i
         float2 za[C], zb[C];
         // W_H^{q k1} for q = 1 .. C-1 as powers of one table value (lanes read consecutive
         // table entries; a lookup per power would stride the table by 2q entries)
-        const float2 wa = twiddle<LOGH + 1, false>(twM, 2 * ka);
-        const float2 wb = twiddle<LOGH + 1, false>(twM, 2 * kb);
+        const float2 wa = twiddle_s<typename S::Tw, false>(twM, 2 * ka);
+        const float2 wb = twiddle_s<typename S::Tw, false>(twM, 2 * kb);
         if constexpr (KIND != CL_RECON) {
 #pragma unroll
             for (int q = 0; q < C; ++q) za[q] = cl_ld(cl_map(aa, q));
@@ -182,23 +200,30 @@ __device__ __forceinline__ void cl_exchange(uint32_t sbase, const float2* twM, i
 #pragma unroll
             for (int q = 0; q < C; ++q) {
                 const int k = ka + H1 * q;
-                if (k <= H / 2) cl_pair<LOGH, KIND>(op, k, za[q], zb[C - 1 - q], twM);
-                else cl_pair<LOGH, KIND>(op, H - k, zb[C - 1 - q], za[q], twM);
+                if (k <= H / 2) cl_pair<C_, KIND>(op, k, za[q], zb[C - 1 - q], twM);
+                else cl_pair<C_, KIND>(op, H - k, zb[C - 1 - q], za[q], twM);
             }
         } else if (ka == 0) {
-            // bin H1 q pairs with H1 (C - q); q = 0 is DC with Nyquist, q = C/2 is bin H/2
-            cl_dc<LOGH, KIND>(op, za[0]);
+            // bin H1 q pairs with H1 (C - q); q = 0 is DC with Nyquist; for even C, q = C/2 is
+            // bin H/2 (its own mirror)
+            cl_dc<C_, KIND>(op, za[0]);
 #pragma unroll
-            for (int q = 1; q < C / 2; ++q) cl_pair<LOGH, KIND>(op, H1 * q, za[q], za[C - q], twM);
-            {
+            for (int q = 1; 2 * q < C; ++q) cl_pair<C_, KIND>(op, H1 * q, za[q], za[C - q], twM);
+            if constexpr (C % 2 == 0) {
                 float2 z1 = za[C / 2], z2 = za[C / 2];
-                cl_pair<LOGH, KIND>(op, H / 2, z1, z2, twM);
+                cl_pair<C_, KIND>(op, H / 2, z1, z2, twM);
                 za[C / 2] = z2;
             }
         } else {
-            // ka = H1/2: bin H1/2 + H1 q pairs with H1/2 + H1 (C - 1 - q)
+            // ka = H1/2: bin H1/2 + H1 q pairs with H1/2 + H1 (C - 1 - q); for odd C,
+            // q = (C - 1)/2 is bin H/2 (its own mirror)
 #pragma unroll
-            for (int q = 0; q < C / 2; ++q) cl_pair<LOGH, KIND>(op, ka + H1 * q, za[q], za[C - 1 - q], twM);
+            for (int q = 0; 2 * q + 1 < C; ++q) cl_pair<C_, KIND>(op, ka + H1 * q, za[q], za[C - 1 - q], twM);
+            if constexpr (C % 2 == 1) {
+                float2 z1 = za[C / 2], z2 = za[C / 2];
+                cl_pair<C_, KIND>(op, H / 2, z1, z2, twM);
+                za[C / 2] = z2;
+            }
         }
         if constexpr (KIND != CL_SPEC) {
             dftR<C, true>(za);
@@ -227,9 +252,9 @@ struct ClDecim {
 
 // Spectrum (CL_SPEC), correlation sweep (CL_CORR) and one-buffer elementary reconstruction
 // (CL_ELEM) on clusters; grid (C x columns, jobs), one cluster per column.
-template <int LOGH, int KIND>
-__global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, ClShape<LOGH>::MINB) k_cl_col(const ssa_col_job* __restrict__ jobs) {
-    using S = ClShape<LOGH>;
+template <int C, int KIND>
+__global__ void __launch_bounds__(ClShape<C>::BLOCK, ClShape<C>::MINB) k_cl_col(const ssa_col_job* __restrict__ jobs) {
+    using S = ClShape<C>;
     extern __shared__ float2 smem[];
     __shared__ double red[32];
     __shared__ double cl_part[S::C];
@@ -242,7 +267,7 @@ __global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, ClShape<LOGH>::MINB) k_c
     const int c = blockIdx.x / S::C;
     if (c >= J.ncols) return;  // the whole cluster shares c
     load_twiddles<S::LOGH1 + 1>(tw1);
-    load_twiddles<LOGH + 1>(twM);
+    cl_load_twM<C>(twM);
     // the first pass of the local transform reads the decimated column from global memory
     const ColPts in = KIND == CL_ELEM ? ColPts{J.in2 + (long long)c * J.ld_in2, nullptr, 1.0f, J.n_in2, 0, 0}
                                       : col_pts(J, c);
@@ -253,7 +278,7 @@ __global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, ClShape<LOGH>::MINB) k_c
     op.spec = KIND == CL_SPEC ? reinterpret_cast<float2*>(J.spec + (long long)c * J.ld_spec) : nullptr;
     op.us = KIND == CL_ELEM ? reinterpret_cast<const float2*>(J.spec + (long long)c * J.ld_spec) : nullptr;
     op.R = nullptr;
-    cl_exchange<LOGH, KIND>((uint32_t)__cvta_generic_to_shared(s), twM, rank, op);
+    cl_exchange<C, KIND>((uint32_t)__cvta_generic_to_shared(s), twM, rank, op);
     cl.sync();
     if constexpr (KIND == CL_SPEC) return;
     const float inv_h = 1.0f / (float)S::H;
@@ -293,9 +318,9 @@ __global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, ClShape<LOGH>::MINB) k_c
 }
 
 // Grouped reconstruction from cached spectra on clusters; grid (C, jobs).
-template <int LOGH>
-__global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, ClShape<LOGH>::MINB) k_cl_recon(const ssa_recon_job* __restrict__ jobs) {
-    using S = ClShape<LOGH>;
+template <int C>
+__global__ void __launch_bounds__(ClShape<C>::BLOCK, ClShape<C>::MINB) k_cl_recon(const ssa_recon_job* __restrict__ jobs) {
+    using S = ClShape<C>;
     extern __shared__ float2 smem[];
     float2* s = smem;
     float2* tw1 = s + spad_size(S::H1);
@@ -304,7 +329,7 @@ __global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, ClShape<LOGH>::MINB) k_c
     const int rank = (int)cl.block_rank();
     const ssa_recon_job J = jobs[blockIdx.y];
     load_twiddles<S::LOGH1 + 1>(tw1);
-    load_twiddles<LOGH + 1>(twM);
+    cl_load_twM<C>(twM);
     __syncthreads();
     cl.sync();  // every CTA of the cluster is resident before the remote stores
     ClOp op;
@@ -312,7 +337,7 @@ __global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, ClShape<LOGH>::MINB) k_c
     op.spec = nullptr;
     op.us = nullptr;
     op.R = &J;
-    cl_exchange<LOGH, CL_RECON>((uint32_t)__cvta_generic_to_shared(s), twM, rank, op);
+    cl_exchange<C, CL_RECON>((uint32_t)__cvta_generic_to_shared(s), twM, rank, op);
     cl.sync();
     fft_block<S::LOGH1, true>(s, tw1);
     const float inv_h = 1.0f / (float)S::H;
@@ -339,11 +364,11 @@ __global__ void __launch_bounds__(ClShape<LOGH>::BLOCK, ClShape<LOGH>::MINB) k_c
     }
 }
 
-template <int LOGH, int KIND>
+template <int C, int KIND>
 static int launch_cl_col(const ssa_col_job* jobs, int njobs, int maxcols, cudaStream_t st) {
-    using S = ClShape<LOGH>;
-    const int sm = cl_smem_f2<LOGH>() * (int)sizeof(float2);
-    cudaError_t e = cudaFuncSetAttribute(k_cl_col<LOGH, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    using S = ClShape<C>;
+    const int sm = cl_smem_f2<C>() * (int)sizeof(float2);
+    cudaError_t e = cudaFuncSetAttribute(k_cl_col<C, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return (int)e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(S::C * maxcols, njobs, 1);
@@ -357,15 +382,15 @@ static int launch_cl_col(const ssa_col_job* jobs, int njobs, int maxcols, cudaSt
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, k_cl_col<LOGH, KIND>, jobs);
+    e = cudaLaunchKernelEx(&cfg, k_cl_col<C, KIND>, jobs);
     return launched(e != cudaSuccess ? e : cudaGetLastError());
 }
 
-template <int LOGH>
+template <int C>
 static int launch_cl_recon(const ssa_recon_job* jobs, int njobs, cudaStream_t st) {
-    using S = ClShape<LOGH>;
-    const int sm = cl_smem_f2<LOGH>() * (int)sizeof(float2);
-    cudaError_t e = cudaFuncSetAttribute(k_cl_recon<LOGH>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    using S = ClShape<C>;
+    const int sm = cl_smem_f2<C>() * (int)sizeof(float2);
+    cudaError_t e = cudaFuncSetAttribute(k_cl_recon<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return (int)e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(S::C, njobs, 1);
@@ -379,26 +404,34 @@ static int launch_cl_recon(const ssa_recon_job* jobs, int njobs, cudaStream_t st
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, k_cl_recon<LOGH>, jobs);
+    e = cudaLaunchKernelEx(&cfg, k_cl_recon<C>, jobs);
     return launched(e != cudaSuccess ? e : cudaGetLastError());
 }
 
 // logh 15 or 16 (callers check)
-static int cl_col_dispatch(int kind, const ssa_col_job* jobs, int njobs, int maxcols, int logh, cudaStream_t st) {
-#define SSA_CL_CASE(L)                                                                        \
-    if (logh == L) {                                                                          \
-        if (kind == CL_SPEC) return launch_cl_col<L, CL_SPEC>(jobs, njobs, maxcols, st);     \
-        if (kind == CL_CORR) return launch_cl_col<L, CL_CORR>(jobs, njobs, maxcols, st);     \
-        return launch_cl_col<L, CL_ELEM>(jobs, njobs, maxcols, st);                           \
+// CTAs per cluster of a size code: 15 -> 4, 16 -> 8, SSA_FFT_3x13 -> 3, SSA_FFT_3x14 -> 6.
+static int cl_ctas(int code) {
+    return code == 15 ? 4 : code == 16 ? 8 : code == SSA_FFT_3x13 ? 3 : code == SSA_FFT_3x14 ? 6 : 0;
+}
+
+static int cl_col_dispatch(int kind, const ssa_col_job* jobs, int njobs, int maxcols, int code, cudaStream_t st) {
+#define SSA_CL_CASE(C)                                                                        \
+    if (cl_ctas(code) == C) {                                                                 \
+        if (kind == CL_SPEC) return launch_cl_col<C, CL_SPEC>(jobs, njobs, maxcols, st);     \
+        if (kind == CL_CORR) return launch_cl_col<C, CL_CORR>(jobs, njobs, maxcols, st);     \
+        return launch_cl_col<C, CL_ELEM>(jobs, njobs, maxcols, st);                           \
     }
-    SSA_CL_CASE(15)
-    SSA_CL_CASE(16)
+    SSA_CL_CASE(3)
+    SSA_CL_CASE(4)
+    SSA_CL_CASE(6)
+    SSA_CL_CASE(8)
 #undef SSA_CL_CASE
     return (int)cudaErrorInvalidValue;
 }
 
+// grouped reconstruction (single-series contexts): power-of-two lengths only
 static int cl_recon_dispatch(const ssa_recon_job* jobs, int njobs, int logh, cudaStream_t st) {
-    if (logh == 15) return launch_cl_recon<15>(jobs, njobs, st);
-    if (logh == 16) return launch_cl_recon<16>(jobs, njobs, st);
+    if (logh == 15) return launch_cl_recon<4>(jobs, njobs, st);
+    if (logh == 16) return launch_cl_recon<8>(jobs, njobs, st);
     return (int)cudaErrorInvalidValue;
 }

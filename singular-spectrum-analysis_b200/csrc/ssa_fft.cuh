@@ -23,6 +23,10 @@
 
 // Defined once in the translation unit that includes this header (ssa_kernels.cu).
 __device__ float2 g_tw[SSA_TW_N];
+// Twiddles of the lengths 3 * 2^A: g_tw3[t] = exp(-2 pi i t / (3 * 2^15)), FP64 on the host.
+#define SSA_TW3_LOG 15
+#define SSA_TW3_N (3 << SSA_TW3_LOG)
+__device__ float2 g_tw3[SSA_TW3_N];
 
 namespace ssa {
 
@@ -70,13 +74,38 @@ __device__ __forceinline__ void load_twiddles(float2* tab) {
     }
 }
 
-// W_M^t (forward sign) or its conjugate, t in [0, M)
-template <int LOGM, bool INV>
-__device__ __forceinline__ float2 twiddle(const float2* tab, int t) {
-    using S = TwSplit<LOGM>;
+// The same two-level table for the resolutions M = 3 * 2^A (9 <= A <= SSA_TW3_LOG): lo holds
+// W_M^j for j < 512, hi W_M^(512 i) for i < M / 512.
+template <int A>
+struct TwSplit3 {
+    static constexpr int LO = 9;
+    static constexpr int NLO = 1 << LO;
+    static constexpr int NHI = 3 << (A - LO);
+    static constexpr int N = NLO + NHI;
+};
+
+template <int A>
+__device__ __forceinline__ void load_twiddles3(float2* tab) {
+    using S = TwSplit3<A>;
+    static_assert(A >= S::LO && A <= SSA_TW3_LOG, "twiddle resolution outside the 3 * 2^A table");
+    for (int i = threadIdx.x; i < S::N; i += blockDim.x) {
+        const int t = i < S::NLO ? i : (i - S::NLO) << S::LO;
+        tab[i] = g_tw3[t << (SSA_TW3_LOG - A)];
+    }
+}
+
+// W_M^t (forward sign) or its conjugate from a two-level table with split S, t in [0, M)
+template <class S, bool INV>
+__device__ __forceinline__ float2 twiddle_s(const float2* tab, int t) {
     float2 w = cmul(tab[S::NLO + (t >> S::LO)], tab[t & (S::NLO - 1)]);
     if (INV) w.y = -w.y;
     return w;
+}
+
+// W_M^t (forward sign) or its conjugate, t in [0, M), M = 2^LOGM
+template <int LOGM, bool INV>
+__device__ __forceinline__ float2 twiddle(const float2* tab, int t) {
+    return twiddle_s<TwSplit<LOGM>, INV>(tab, t);
 }
 
 // Multiply by the constant W_16^e (forward sign) or its conjugate.
@@ -167,10 +196,43 @@ __device__ __forceinline__ void dft16(float2* a) {
 #undef SSA_SWP
 }
 
+// 3 points: X1,2 = a0 - (a1 + a2)/2 -/+ i (sqrt 3 / 2)(a1 - a2) (signs of i flipped for INV).
+template <bool INV>
+__device__ __forceinline__ void dft3(float2* a) {
+    constexpr float H3 = 0.86602540378443865f;  // sqrt(3) / 2
+    const float2 s = cadd(a[1], a[2]);
+    const float2 m = make_float2(a[0].x - 0.5f * s.x, a[0].y - 0.5f * s.y);
+    const float2 d = cscale(mul_mi<INV>(csub(a[1], a[2])), H3);
+    a[0] = cadd(a[0], s);
+    a[1] = cadd(m, d);
+    a[2] = csub(m, d);
+}
+
+// 6 = 3 x 2: B_r = DFT3 of a[r], a[r + 2], a[r + 4]; X[k] = B_0[k] + W6^k B_1[k],
+// X[k + 3] = B_0[k] - W6^k B_1[k], k < 3.
+template <bool INV>
+__device__ __forceinline__ void dft6(float2* a) {
+    constexpr float H3 = 0.86602540378443865f;
+    float2 b0[3] = {a[0], a[2], a[4]};
+    float2 b1[3] = {a[1], a[3], a[5]};
+    dft3<INV>(b0);
+    dft3<INV>(b1);
+    const float sg = INV ? 1.f : -1.f;
+    b1[1] = cmul(b1[1], make_float2(0.5f, sg * H3));
+    b1[2] = cmul(b1[2], make_float2(-0.5f, sg * H3));
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        a[k] = cadd(b0[k], b1[k]);
+        a[k + 3] = csub(b0[k], b1[k]);
+    }
+}
+
 template <int R, bool INV>
 __device__ __forceinline__ void dftR(float2* a) {
     if constexpr (R == 2) dft2<INV>(a);
+    else if constexpr (R == 3) dft3<INV>(a);
     else if constexpr (R == 4) dft4<INV>(a);
+    else if constexpr (R == 6) dft6<INV>(a);
     else if constexpr (R == 8) dft8<INV>(a);
     else dft16<INV>(a);
 }

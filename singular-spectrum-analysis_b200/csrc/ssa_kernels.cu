@@ -1452,6 +1452,22 @@ extern "C" int ssad_logh_for(int N) {
     return logm - 1;
 }
 
+extern "C" int ssad_fft_h(int code) {
+    if (code >= 4 && code <= SSA_MAX_LOGH_ALL) return 1 << code;
+    if (code == SSA_FFT_3x13) return 3 << 13;
+    if (code == SSA_FFT_3x14) return 3 << 14;
+    return 0;
+}
+
+extern "C" int ssad_fft_code_for(int N) {
+    const int logh = ssad_logh_for(N);
+    if (logh > SSA_MAX_LOGH_ALL) return -1;  // beyond the largest length
+    // between the cluster powers of two, the 3 * 2^a length when it suffices
+    if (logh == 15 && N <= 2 * (3 << 13)) return SSA_FFT_3x13;
+    if (logh == 16 && N <= 2 * (3 << 14)) return SSA_FFT_3x14;
+    return logh;
+}
+
 extern "C" int ssad_init_device(void) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -1464,6 +1480,13 @@ extern "C" int ssad_init_device(void) {
         tw[t] = make_float2((float)cos(a), (float)sin(a));
     }
     e = cudaMemcpyToSymbol(g_tw, tw.data(), sizeof(float2) * SSA_TW_N);
+    if (e != cudaSuccess) return (int)e;
+    std::vector<float2> tw3(SSA_TW3_N);
+    for (int t = 0; t < SSA_TW3_N; ++t) {
+        const double a = -2.0 * M_PI * (double)t / (double)SSA_TW3_N;
+        tw3[t] = make_float2((float)cos(a), (float)sin(a));
+    }
+    e = cudaMemcpyToSymbol(g_tw3, tw3.data(), sizeof(float2) * SSA_TW3_N);
     if (e != cudaSuccess) return (int)e;
     if (dev < 64) done[dev] = true;
     return 0;
@@ -1558,7 +1581,7 @@ extern "C" int ssad_gram_tc(const ssa_wgram_job* d_jobs, int njobs, int maxchunk
 
 extern "C" int ssad_spectrum(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
     if (njobs <= 0 || maxcols <= 0) return 0;
-    if (logh > SSA_MAX_LOGH) return cl_col_dispatch(CL_SPEC, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);
+    if (logh > SSA_MAX_LOGH) return cl_col_dispatch(CL_SPEC, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);  // 15-18
 #define CALL(L) return launch_spectrum<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
     SSA_LOGH_DISPATCH(logh, CALL)
 #undef CALL

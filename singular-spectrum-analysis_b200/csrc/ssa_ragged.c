@@ -38,9 +38,10 @@
             return _e;         \
     } while (0)
 
+/* buckets are indexed by FFT size code (ssad_fft_code_for): logh 4..16 and the two lengths
+ * 3 * 2^13, 3 * 2^14 between the cluster powers of two */
 #define RB_MIN_LOGH 4
-#define RB_MAX_LOGH SSA_MAX_LOGH_ALL
-#define RB_NB (RB_MAX_LOGH + 1)
+#define RB_NB SSA_FFT_NCODES
 
 typedef struct
 {
@@ -257,8 +258,8 @@ static int bucket_setup(rbucket *b, int logh, int prof)
     }
     if (prof && !b->e.prof)
         CK(ssae_set_profiling(&b->e, 1));
-    b->logh = logh;
-    b->ldS = round4(2LL * ((1 << logh) + 1) + 2);
+    b->logh = logh; /* size code */
+    b->ldS = round4(2LL * (ssad_fft_h(logh) + 1) + 2);
     return 0;
 }
 
@@ -759,6 +760,12 @@ static int bucket_run(rbucket *b, ssa_rbatch *rb, const double *d_x, unsigned lo
     return 0;
 }
 
+int ssa_b200_fft_length(int N)
+{
+    const int code = N >= 1 ? ssad_fft_code_for(N) : -1;
+    return code < 0 ? -1 : 2 * ssad_fft_h(code);
+}
+
 /* Device arena of at least `bytes` (stream-ordered on the main stream after the previous run). */
 int ssa_rbatch_reserve(ssa_rbatch *rb, size_t bytes)
 {
@@ -790,13 +797,13 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
         const int kp = imin(k[s] + rb->p, imin(L[s], K));
         if (kp > SSA_MAX_KP)
             return -1;
-        const int logh = ssad_logh_for(N[s]);
-        if (logh > RB_MAX_LOGH || logh < RB_MIN_LOGH)
+        const int logh = ssad_fft_code_for(N[s]);
+        if (logh >= RB_NB || logh < RB_MIN_LOGH || ssad_fft_h(logh) == 0)
             return -1;
     }
     int count[RB_NB] = {0};
     for (int s = 0; s < B; s++)
-        count[ssad_logh_for(N[s])]++;
+        count[ssad_fft_code_for(N[s])]++;
     for (int g = 0; g < RB_NB; g++)
         if (count[g] > 65535) /* the job index is blockIdx.y in the column kernels */
             return -1;
@@ -821,7 +828,7 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
     size_t ox = 0, osig = 0, oW = 0, ogrp = 0;
     for (int s = 0; s < B; s++)
     {
-        rbucket *b = &rb->bk[ssad_logh_for(N[s])];
+        rbucket *b = &rb->bk[ssad_fft_code_for(N[s])];
         rser *S = &b->sd[b->nb++];
         memset(S, 0, sizeof(*S));
         S->src = s;
@@ -1238,8 +1245,8 @@ size_t ssar_series_bytes(int N, int L, int k, int p, int n_groups)
     const int K = N - L + 1;
     const int kp = imin(k + p, imin(L, K));
     k = imin(k, kp);
-    const int logh = ssad_logh_for(N);
-    const size_t ldS = (size_t)round4(2LL * ((1 << logh) + 1) + 2);
+    const int logh = ssad_fft_code_for(N);
+    const size_t ldS = (size_t)round4(2LL * (ssad_fft_h(logh) + 1) + 2);
     const int nb_est = 64; /* Gram chunking at moderate bucket sizes */
     const int nch = imax(imax((L + gram_rows(L, nb_est) - 1) / gram_rows(L, nb_est),
                               (K + gram_rows(K, nb_est) - 1) / gram_rows(K, nb_est)),

@@ -107,3 +107,29 @@ def test_uneven_batch_across_cluster_lengths(gpu, oracle):
         for gi, g in enumerate(([0], [1, 2])):
             assert rel_l2(G[s][gi], oracle.reconstruct(d, g, N, L)) <= rec_tol(d.sigma, g), (s, N, g)
         assert np.max(np.abs(np.diag(W[s]) - 1.0)) < 1e-6
+
+
+def test_uneven_batch_mixed_radix_boundaries(gpu, oracle):
+    """Both sides of the two 3 * 2^a FFT lengths (real lengths 49152 and 98304, clusters of 3 and
+    6 CTAs) against the oracle: 32769 and 49152 run at 49152, 49153 at 65536, 98304 at 98304,
+    98305 at 131072."""
+    rng = np.random.default_rng(11)
+    mix = [(oracle.walk_sines(rng, N), N // 4, k) for N, k in
+           ((32769, 14), (49152, 22), (49153, 10), (98304, 18), (98305, 9))]
+    p, q, seed = 10, 2, 23
+    rb = gpu.SSARaggedBatch(oversampling=p, power_iters=q, groups=[[0], [1, 2]])
+    sig, W, G = rb.run([m[0] for m in mix], [m[1] for m in mix], [m[2] for m in mix], seed=seed)
+    for s, (x, L, k) in enumerate(mix):
+        N = len(x)
+        K = N - L + 1
+        Om = oracle.device_gaussian(oracle.series_seed(seed, s), K, min(k + p, L, K))
+        d = oracle.decompose_randomized(x, L, k, p, Om, q=q)
+        check_sigma(sig[s], d.sigma)
+        for gi, g in enumerate(([0], [1, 2])):
+            assert rel_l2(G[s][gi], oracle.reconstruct(d, g, N, L)) <= rec_tol(d.sigma, g), (s, N, g)
+        assert np.max(np.abs(np.diag(W[s]) - 1.0)) < 1e-6
+        Wr = oracle.wcorr_matrix(d, N, L)
+        blk = [i for i in range(min(6, len(d.sigma)))
+               if min(abs(d.sigma[i] - d.sigma[j]) / d.sigma[i] for j in range(len(d.sigma)) if j != i) > 1e-2]
+        if blk:
+            assert np.max(np.abs(W[s][np.ix_(blk, blk)] - Wr[np.ix_(blk, blk)])) < 1e-4, (s, N)
