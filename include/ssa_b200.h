@@ -200,6 +200,7 @@ typedef struct
     long long evictions, not_resident;
     size_t resident_bytes, resident_budget, batch_budget;
     double host_launch_s, host_finish_s; /* worker time spent forming / completing batches */
+    double host_launch_max_s;            /* longest forming of one batch since the previous read */
 } ssa_server_stats;
 typedef struct ssa_server ssa_server;
 /* hbm_budget_bytes 0: 80 % of the free device memory at creation, device memory taken as batches

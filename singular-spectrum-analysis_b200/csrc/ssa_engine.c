@@ -30,14 +30,16 @@ static int imax(int a, int b) { return a > b ? a : b; }
 
 static int gram_rows(int m, int B)
 {
-    /* Aim for about eight 4-warp CTAs per SM over all series (latency hiding when a launch holds
-     * few series); at least one staging chunk per CTA. */
+    /* Aim for about 1184 CTAs (eight per SM) over all series (latency hiding when a launch holds
+     * few series). */
     int target = 1184 / (B > 0 ? B : 1);
     if (target < 1)
         target = 1;
     int rows = (m + target - 1) / target;
     rows = ((rows + SSA_GRAM_CHUNK - 1) / SSA_GRAM_CHUNK) * SSA_GRAM_CHUNK;
-    return imax(rows, SSA_GRAM_CHUNK);
+    /* at least four staging chunks per CTA: fewer partials for the per-series kernels to sum
+     * (their latency) when a launch holds few series */
+    return imax(rows, 4 * SSA_GRAM_CHUNK);
 }
 
 static int dmalloc(void **p, size_t bytes)
@@ -149,6 +151,12 @@ int ssae_grow_arena(ssa_engine *e, size_t bytes)
 {
     if (bytes <= e->ja.cap)
         return 0;
+    {
+        const char *ev = getenv("SSA_SERVER_TRACE");
+        if (ev && ev[0] == '1' && e->ja.cap > 0)
+            fprintf(stderr, "ssa_engine: job arena grows %zu -> %zu bytes (frees synchronise the device)\n",
+                    e->ja.cap, bytes);
+    }
     if (e->st)
         CK(cudaStreamSynchronize(e->st));
     if (e->ja.h)

@@ -642,17 +642,44 @@ __global__ void __launch_bounds__(GRAM_MMA_THREADS, 3) k_gram(const ssa_gram_job
 #define SLD (SSA_MAX_KP + 1)
 #define SMALL_SMEM (2 * SSA_MAX_KP * SLD * (int)sizeof(double))
 
-// Sum the packed-upper Gram partials into the symmetric column-major matrix G (ld SLD).
+// Sum the packed-upper Gram partials into the symmetric column-major matrix G (ld SLD). Each
+// thread owns up to four packed entries and walks the chunks four at a time, so that sixteen
+// independent loads of the (L2-resident) partials are in flight: the sum over chunks is a
+// latency chain otherwise, and it sets the latency of the small per-series kernels.
 __device__ void reduce_packed(const double* __restrict__ part, int nchunks, int n, double* G) {
     const int np = n * (n + 1) / 2;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int i = warp; i < n; i += nw) {
-        const int base = i * n - (i * (i - 1)) / 2 - i;  // pk_index(i, j, n) = base + j
-        for (int j = i + lane; j < n; j += 32) {
-            double s = 0.0;
-            for (int c = 0; c < nchunks; ++c) s += part[(long long)c * np + base + j];
-            G[j * SLD + i] = s;
-            G[i * SLD + j] = s;
+    const int bs = blockDim.x;
+    for (int e0 = threadIdx.x; e0 < np; e0 += 4 * bs) {
+        int e[4];
+        double acc[4][4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            e[u] = e0 + u * bs;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
+        }
+        int c = 0;
+        for (; c + 4 <= nchunks; c += 4) {
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (e[u] < np) acc[u][v] += part[(long long)(c + v) * np + e[u]];
+        }
+        for (; c < nchunks; ++c)
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (e[u] < np) acc[u][0] += part[(long long)c * np + e[u]];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (e[u] >= np) continue;
+            // packed row-major upper triangle: row i starts at i n - i (i - 1) / 2
+            int i = 0;
+            while (i + 1 < n && (i + 1) * n - ((i + 1) * i) / 2 <= e[u]) ++i;
+            const int j = i + (e[u] - (i * n - (i * (i - 1)) / 2));
+            const double sum = (acc[u][0] + acc[u][1]) + (acc[u][2] + acc[u][3]);
+            G[j * SLD + i] = sum;
+            G[i * SLD + j] = sum;
         }
     }
 }
@@ -1333,6 +1360,11 @@ __global__ void k_gapupdate(double* x, const double* recon, const int* idx, int 
     }
 }
 
+__global__ void __launch_bounds__(256) k_copy_segments(const ssa_copy_seg* __restrict__ segs) {
+    const ssa_copy_seg S = segs[blockIdx.x];
+    for (long long i = threadIdx.x; i < S.n; i += blockDim.x) S.dst[i] = S.src[i];
+}
+
 __global__ void k_axpby(const double* a, const double* b, double* out, double alpha, double beta, long long n) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         out[i] = alpha * a[i] + beta * b[i];
@@ -1740,6 +1772,12 @@ extern "C" int ssad_colnorm2(const float* A, long long sstride, long long ld, in
 extern "C" int ssad_gapupdate(double* x, const double* recon, const int* idx, int n, double* out2, void* stream) {
     if (n < 1) return 0;
     k_gapupdate<<<1, 256, 0, (cudaStream_t)stream>>>(x, recon, idx, n, out2);
+    return launched(cudaGetLastError());
+}
+
+extern "C" int ssad_copy_segments(const ssa_copy_seg* d_segs, int nseg, void* stream) {
+    if (nseg <= 0) return 0;
+    k_copy_segments<<<nseg, 256, 0, (cudaStream_t)stream>>>(d_segs);
     return launched(cudaGetLastError());
 }
 

@@ -263,6 +263,16 @@ int ssad_slabsum(float *out, const float *in, long long stride, int nslab, long 
 int ssad_colnorm2(const float *A, long long sstride, long long ld, int m, int k, int nb, double *out, void *stream);
 /* out2[0] = sum (a - b)^2, out2[1] = sum a^2 over n doubles (FP64, one CTA, fixed order). */
 int ssad_diffnorm(const double *a, const double *b, long long n, double *out2, void *stream);
+/* Segment copies dst[i] = src[i], i < n, one CTA per segment: dst may be page-locked host memory
+ * mapped into the device address space, so one launch writes many small outputs straight to the
+ * host instead of one copy call each. */
+typedef struct
+{
+    const double *src;
+    double *dst;
+    long long n;
+} ssa_copy_seg;
+int ssad_copy_segments(const ssa_copy_seg *d_segs, int nseg, void *stream);
 /* x[idx[i]] = recon[idx[i]] for i < n; out2 = {sum (new - old)^2, sum old^2} (gap filling). */
 int ssad_gapupdate(double *x, const double *recon, const int *idx, int n, double *out2, void *stream);
 /* out[i] = alpha a[i] + beta b[i] (doubles). */

@@ -22,8 +22,10 @@
  * Batch-level packed arrays (series order): x (sum N), sigma (sum k), W (sum k^2),
  * groups (n_groups * sum N), status (B).
  */
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #include <cuda_runtime_api.h>
 
@@ -107,13 +109,15 @@ static long long round4(long long v) { return (v + 3) & ~3LL; }
 
 static int gram_rows(int m, int nb)
 {
-    /* about eight 4-warp CTAs per SM over the bucket's series; at least one staging chunk per CTA */
+    /* about 1184 CTAs (eight per SM) over the bucket's series */
     int target = 1184 / (nb > 0 ? nb : 1);
     if (target < 1)
         target = 1;
     int rows = (m + target - 1) / target;
     rows = ((rows + SSA_GRAM_CHUNK - 1) / SSA_GRAM_CHUNK) * SSA_GRAM_CHUNK;
-    return imax(rows, SSA_GRAM_CHUNK);
+    /* at least four staging chunks per CTA: fewer partials for the per-series kernels to sum
+     * (their latency) when a launch holds few series */
+    return imax(rows, 4 * SSA_GRAM_CHUNK);
 }
 
 /* The library's stream-ordered memory pool on the current device: freed blocks stay cached in
@@ -983,12 +987,18 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
 /* ---- entry points ------------------------------------------------------------------------ */
 
 /* Wait for the previous run on every stream and reset the job arenas. */
+/* Before a run reuses the buckets' host job tables: the previous run's bucket streams have
+ * consumed them. The main stream is not waited for: it may already hold this run's inputs, and
+ * the new run's buckets are ordered after it anyway. */
 static int quiesce(ssa_rbatch *rb)
 {
-    int rc = cudaStreamSynchronize(rb->main) != cudaSuccess;
+    int rc = 0;
     for (int g = 0; g < RB_NB; g++)
         if (rb->bk[g].live)
+        {
+            rc |= cudaStreamSynchronize(rb->bk[g].e.st) != cudaSuccess;
             ssae_reset_jobs(&rb->bk[g].e);
+        }
     return rc ? -1 : 0;
 }
 
@@ -1212,8 +1222,20 @@ int ssar_run_enqueue_ex(ssa_rbatch *rb, int B, const int *N, const int *L, const
 {
     if (!rb || B < 1 || !N || !L || !k || !d_x)
         return -1;
+    static int trace = -1;
+    if (trace < 0)
+    {
+        const char *ev = getenv("SSA_SERVER_TRACE");
+        trace = ev && ev[0] == '1';
+    }
+    struct timespec q0, q1;
+    clock_gettime(CLOCK_MONOTONIC, &q0);
     if (quiesce(rb) != 0)
         return -1;
+    clock_gettime(CLOCK_MONOTONIC, &q1);
+    const double qms = 1e3 * (double)(q1.tv_sec - q0.tv_sec) + 1e-6 * (double)(q1.tv_nsec - q0.tv_nsec);
+    if (trace && qms > 2.0)
+        fprintf(stderr, "ssa_rbatch: waited %.1f ms for the previous run before enqueueing\n", qms);
     rb->cur_seeds = seeds;
     rb->cur_lrf = lrf_dst;
     rb->cur_wmask = want_w;

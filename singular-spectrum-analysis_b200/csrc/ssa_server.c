@@ -16,6 +16,7 @@
  */
 #include <errno.h>
 #include <pthread.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
@@ -66,8 +67,16 @@ typedef struct
     /* per request: offsets (doubles) of its input in d_x and, for pageable buffers, in the
      * pinned staging areas (SIZE_MAX = copied directly from / to the caller's pinned memory) */
     size_t *xoff, *sin, *sout;
+    /* per request, device addresses of its page-locked caller buffers: input, sigma, groups, W
+     * (NULL where staged or not asked for) */
+    double **hp;
     double *h_in, *h_out; /* pinned staging, fixed at creation */
-    int *h_st, *h_lst;    /* max_batch status words */
+    double *h_in_d, *h_out_d; /* their device addresses */
+    int *h_st, *h_lst;        /* max_batch status words */
+    /* copy segments of the batch's input gather and output scatter (page-locked, read by the
+     * copy kernel through its device address) */
+    ssa_copy_seg *h_seg, *h_seg_d;
+    size_t c_seg;
     double *d_x;
     size_t c_dx;
     size_t bytes, in_used, out_used;
@@ -132,18 +141,24 @@ static int imin(int a, int b) { return a < b ? a : b; }
 #define SRV_STAGE_OUT (512u << 20)
 #define SRV_DIRECT ((size_t)-1)
 
-static int is_pinned(const void *p)
+/* Segments of at most this many doubles: one CTA of the copy kernel each. */
+#define SRV_SEG_CHUNK ((size_t)16384)
+
+/* Device address of page-locked host memory; NULL for pageable memory (staged instead). */
+static double *mapped(const void *p)
 {
     if (!p)
-        return 0;
+        return NULL;
     struct cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess)
     {
         cudaGetLastError();
-        return 0;
+        return NULL;
     }
-    return a.type == cudaMemoryTypeHost;
+    return a.type == cudaMemoryTypeHost ? (double *)a.devicePointer : NULL;
 }
+
+static size_t seg_count(size_t n) { return (n + SRV_SEG_CHUNK - 1) / SRV_SEG_CHUNK; }
 
 static int req_kout(const ssa_server *s, const ssa_request *r)
 {
@@ -164,13 +179,33 @@ static size_t req_out_doubles(const ssa_server *s, const ssa_request *r)
     return n;
 }
 
-static const void *first_output(const ssa_request *r)
+/* Segments of the copy kernel for the input and the outputs of one request. */
+static size_t req_segs(const ssa_server *s, const ssa_request *r)
 {
+    const size_t ke = (size_t)req_kout(s, r);
+    size_t n = seg_count((size_t)r->N);
     if (r->sigma)
-        return r->sigma;
-    if (r->type == SSA_REQ_DECOMPOSE_RECON)
-        return r->groups;
-    return r->W;
+        n += seg_count(ke);
+    if (r->type == SSA_REQ_DECOMPOSE_RECON && r->groups)
+        n += seg_count(2 * (size_t)r->N);
+    if (r->type == SSA_REQ_DECOMPOSE_WCORR && r->W)
+        n += seg_count(ke * ke);
+    return n;
+}
+
+static void seg_add(ssa_copy_seg *t, size_t *ns, const double *src, double *dst, size_t n)
+{
+    while (n > 0)
+    {
+        const size_t m = n < SRV_SEG_CHUNK ? n : SRV_SEG_CHUNK;
+        t[*ns].src = src;
+        t[*ns].dst = dst;
+        t[*ns].n = (long long)m;
+        (*ns)++;
+        src += m;
+        dst += m;
+        n -= m;
+    }
 }
 
 /* ---- resident store ------------------------------------------------------------------------ */
@@ -281,6 +316,19 @@ static int res_alloc(ssa_server *s, res_entry *e)
 }
 
 /* ---- helpers ------------------------------------------------------------------------------ */
+
+/* SSA_SERVER_TRACE=1 in the environment: batch launches that take the worker over 5 ms are
+ * reported on stderr with their phases (a diagnostic for latency tails). */
+static int srv_trace(void)
+{
+    static int v = -1;
+    if (v < 0)
+    {
+        const char *e = getenv("SSA_SERVER_TRACE");
+        v = e && e[0] == '1';
+    }
+    return v;
+}
 
 static int grow_host(void **p, size_t *cap, size_t need, size_t elem)
 {
@@ -396,6 +444,10 @@ static int slot_reserve(slot_t *sl, int n)
         sl->sout = z[2];
     if (!z[0] || !z[1] || !z[2])
         return -1;
+    double **h = (double **)realloc(sl->hp, sizeof(double *) * 4 * (size_t)c);
+    if (!h)
+        return -1;
+    sl->hp = h;
     sl->cap = c;
     return 0;
 }
@@ -425,67 +477,65 @@ static int slot_launch(ssa_server *s, slot_t *sl)
     /* resident blocks were allocated on the pool stream: order the batch after them */
     if (cudaEventRecord(s->ev_pool, s->pool_st) != cudaSuccess || cudaStreamWaitEvent(ms, s->ev_pool, 0) != cudaSuccess)
         return -1;
-    /* inputs: pinned buffers directly; pageable ones through the staging area, consecutive staged
-     * requests in one copy */
-    int i = 0;
-    while (i < sl->n)
+    /* the copy kernel's segment table; the slot is idle, so its table is free */
+    size_t nseg = 0;
+    for (int i = 0; i < sl->n; i++)
+        nseg += req_segs(s, sl->req[i]);
+    if (nseg > sl->c_seg)
+    {
+        if (sl->h_seg)
+            cudaFreeHost(sl->h_seg);
+        sl->h_seg = sl->h_seg_d = NULL;
+        sl->c_seg = 0;
+        if (cudaMallocHost((void **)&sl->h_seg, sizeof(ssa_copy_seg) * (nseg + nseg / 2)) != cudaSuccess ||
+            !(sl->h_seg_d = (ssa_copy_seg *)mapped(sl->h_seg)))
+            return -1;
+        sl->c_seg = nseg + nseg / 2;
+    }
+    /* inputs: one gather launch reading the callers' page-locked buffers, and the staging area
+     * that the pageable ones are copied into */
+    size_t ns = 0;
+    for (int i = 0; i < sl->n; i++)
     {
         const ssa_request *r = sl->req[i];
-        if (sl->sin[i] == SRV_DIRECT)
+        const double *src = sl->hp[4 * i];
+        if (!src)
         {
-            if (cudaMemcpyAsync(sl->d_x + sl->xoff[i], r->x, sizeof(double) * r->N, cudaMemcpyHostToDevice, ms) !=
-                cudaSuccess)
-                return -1;
-            i++;
-            continue;
+            memcpy(sl->h_in + sl->sin[i], r->x, sizeof(double) * r->N);
+            src = sl->h_in_d + sl->sin[i];
         }
-        int j = i;
-        size_t run = 0;
-        while (j < sl->n && sl->sin[j] != SRV_DIRECT && sl->sin[j] == sl->sin[i] + run)
-        {
-            memcpy(sl->h_in + sl->sin[j], sl->req[j]->x, sizeof(double) * sl->req[j]->N);
-            run += (size_t)sl->req[j]->N;
-            j++;
-        }
-        if (cudaMemcpyAsync(sl->d_x + sl->xoff[i], sl->h_in + sl->sin[i], sizeof(double) * run,
-                            cudaMemcpyHostToDevice, ms) != cudaSuccess)
-            return -1;
-        i = j;
+        seg_add(sl->h_seg, &ns, src, sl->d_x + sl->xoff[i], (size_t)r->N);
     }
+    const size_t nin = ns;
+    if (ssad_copy_segments(sl->h_seg_d, (int)nin, ms) != 0)
+        return -1;
+    const double t1 = ssa_server_now();
     if (ssar_run_enqueue_ex(sl->rb, sl->n, sl->N, sl->L, sl->k, sl->d_x, sl->seeds, sl->lrf_dst, sl->wantw) != 0)
         return -1;
-    /* outputs the requests ask for */
+    const double t2 = ssa_server_now();
+    /* outputs the requests ask for: one scatter launch writing the callers' page-locked buffers,
+     * or the staging area slot_finish copies from */
     const size_t *off = ssar_offsets(sl->rb);
     const double *dsig = ssar_sigma(sl->rb), *dW = ssar_W(sl->rb), *dg = ssar_groups(sl->rb);
-    for (i = 0; i < sl->n; i++)
+    for (int i = 0; i < sl->n; i++)
     {
         ssa_request *r = sl->req[i];
-        const int ke = req_kout(s, r);
+        const size_t ke = (size_t)req_kout(s, r);
         const int direct = sl->sout[i] == SRV_DIRECT;
         size_t so = sl->sout[i];
         if (r->sigma)
         {
-            double *dst = direct ? r->sigma : sl->h_out + so;
-            if (cudaMemcpyAsync(dst, dsig + off[4 * i + 1], sizeof(double) * ke, cudaMemcpyDeviceToHost, ms) !=
-                cudaSuccess)
-                return -1;
-            so += (size_t)ke;
+            seg_add(sl->h_seg, &ns, dsig + off[4 * i + 1], direct ? sl->hp[4 * i + 1] : sl->h_out_d + so, ke);
+            so += ke;
         }
         if (r->type == SSA_REQ_DECOMPOSE_RECON && r->groups)
-        {
-            double *dst = direct ? r->groups : sl->h_out + so;
-            if (cudaMemcpyAsync(dst, dg + off[4 * i + 3], sizeof(double) * 2 * r->N, cudaMemcpyDeviceToHost, ms) !=
-                cudaSuccess)
-                return -1;
-        }
+            seg_add(sl->h_seg, &ns, dg + off[4 * i + 3], direct ? sl->hp[4 * i + 2] : sl->h_out_d + so,
+                    2 * (size_t)r->N);
         if (r->type == SSA_REQ_DECOMPOSE_WCORR && r->W)
-        {
-            double *dst = direct ? r->W : sl->h_out + so;
-            if (cudaMemcpyAsync(dst, dW + off[4 * i + 2], sizeof(double) * ke * ke, cudaMemcpyDeviceToHost, ms) !=
-                cudaSuccess)
-                return -1;
-        }
+            seg_add(sl->h_seg, &ns, dW + off[4 * i + 2], direct ? sl->hp[4 * i + 3] : sl->h_out_d + so, ke * ke);
     }
+    if (ssad_copy_segments(sl->h_seg_d + nin, (int)(ns - nin), ms) != 0)
+        return -1;
     if (cudaMemcpyAsync(sl->h_st, ssar_status(sl->rb), sizeof(int) * sl->n, cudaMemcpyDeviceToHost, ms) !=
             cudaSuccess ||
         cudaMemcpyAsync(sl->h_lst, ssar_lrf_status(sl->rb), sizeof(int) * sl->n, cudaMemcpyDeviceToHost, ms) !=
@@ -497,7 +547,13 @@ static int slot_launch(ssa_server *s, slot_t *sl)
     s->stats.decompositions += sl->n;
     if (sl->n > s->stats.max_batch)
         s->stats.max_batch = sl->n;
-    s->stats.host_launch_s += ssa_server_now() - t0;
+    const double dt = ssa_server_now() - t0;
+    s->stats.host_launch_s += dt;
+    if (dt > s->stats.host_launch_max_s)
+        s->stats.host_launch_max_s = dt;
+    if (srv_trace() && dt > 5e-3)
+        fprintf(stderr, "ssa_server: batch of %d formed in %.1f ms (inputs %.1f, enqueue %.1f, outputs %.1f)\n", sl->n,
+                1e3 * dt, 1e3 * (t1 - t0), 1e3 * (t2 - t1), 1e3 * (dt - (t2 - t0)));
     return 0;
 }
 
@@ -730,10 +786,18 @@ static int dispatch(ssa_server *s)
                     keep = 0;
                     progressed = 1;
                 }
-                const size_t in_b = is_pinned(r->x) ? 0 : (size_t)r->N;
+                double *hp[4] = {mapped(r->x), mapped(r->sigma),
+                                 r->type == SSA_REQ_DECOMPOSE_RECON ? mapped(r->groups) : NULL,
+                                 r->type == SSA_REQ_DECOMPOSE_WCORR ? mapped(r->W) : NULL};
+                const int out_direct = (!r->sigma || hp[1]) &&
+                                       (r->type != SSA_REQ_DECOMPOSE_RECON || !r->groups || hp[2]) &&
+                                       (r->type != SSA_REQ_DECOMPOSE_WCORR || !r->W || hp[3]);
+                const size_t in_b = hp[0] ? 0 : (size_t)r->N;
                 const size_t nout = req_out_doubles(s, r);
-                const size_t out_b = (nout && !is_pinned(first_output(r))) ? nout : 0;
-                if (in_b > SRV_STAGE_IN / sizeof(double) || out_b > SRV_STAGE_OUT / sizeof(double))
+                const size_t out_b = (nout && !out_direct) ? nout : 0;
+                if (!keep)
+                    ;
+                else if (in_b > SRV_STAGE_IN / sizeof(double) || out_b > SRV_STAGE_OUT / sizeof(double))
                 {
                     if (r->priv && r->priv != (void *)&g_not_resident)
                         ((res_entry *)r->priv)->state = RES_FAILED;
@@ -749,6 +813,7 @@ static int dispatch(ssa_server *s)
                     const int j = sl->n;
                     sl->sin[j] = in_b ? sl->in_used : SRV_DIRECT;
                     sl->sout[j] = out_b ? sl->out_used : SRV_DIRECT;
+                    memcpy(sl->hp + 4 * (size_t)j, hp, sizeof(hp));
                     sl->in_used += in_b;
                     sl->out_used += out_b;
                     res_entry *e = r->priv == (void *)&g_not_resident ? NULL : (res_entry *)r->priv;
@@ -904,6 +969,9 @@ int ssa_server_create(ssa_server **out, size_t hbm_budget_bytes, int max_infligh
             cudaMallocHost((void **)&sl->h_out, SRV_STAGE_OUT) != cudaSuccess ||
             cudaMallocHost((void **)&sl->h_st, sizeof(int) * (size_t)max_batch) != cudaSuccess ||
             cudaMallocHost((void **)&sl->h_lst, sizeof(int) * (size_t)max_batch) != cudaSuccess ||
+            !(sl->h_in_d = mapped(sl->h_in)) || !(sl->h_out_d = mapped(sl->h_out)) ||
+            cudaMallocHost((void **)&sl->h_seg, sizeof(ssa_copy_seg) * 8 * (size_t)max_batch) != cudaSuccess ||
+            !(sl->h_seg_d = (ssa_copy_seg *)mapped(sl->h_seg)) || !(sl->c_seg = 8 * (size_t)max_batch) ||
             (reserve && ssa_rbatch_reserve(sl->rb, s->batch_budget + s->batch_budget / 8) != 0))
         {
             ssa_server_destroy(s);
@@ -1014,6 +1082,7 @@ int ssa_server_stats_get(ssa_server *s, ssa_server_stats *st)
         return -1;
     pthread_mutex_lock(&s->mu);
     *st = s->stats;
+    s->stats.host_launch_max_s = 0.0; /* the maximum is per read */
     st->resident_bytes = s->res_bytes;
     st->resident_budget = s->res_budget;
     st->batch_budget = s->batch_budget;
@@ -1045,7 +1114,7 @@ void ssa_server_destroy(ssa_server *s)
             ssa_rbatch_destroy(sl->rb);
         if (sl->done)
             cudaEventDestroy(sl->done);
-        void *hp[] = {sl->h_in, sl->h_out, sl->h_st, sl->h_lst};
+        void *hp[] = {sl->h_in, sl->h_out, sl->h_st, sl->h_lst, sl->h_seg};
         for (size_t j = 0; j < sizeof(hp) / sizeof(hp[0]); j++)
             if (hp[j])
                 cudaFreeHost(hp[j]);
@@ -1062,6 +1131,7 @@ void ssa_server_destroy(ssa_server *s)
         free(sl->xoff);
         free(sl->sin);
         free(sl->sout);
+        free(sl->hp);
     }
     free(s->slots);
     if (s->htab)

@@ -866,7 +866,7 @@ class _ServerStats(ctypes.Structure):
                                                   "max_batch", "forecast_batches", "forecasts", "evictions",
                                                   "not_resident")] + \
                [(n, ctypes.c_size_t) for n in ("resident_bytes", "resident_budget", "batch_budget")] + \
-               [(n, ctypes.c_double) for n in ("host_launch_s", "host_finish_s")]
+               [(n, ctypes.c_double) for n in ("host_launch_s", "host_finish_s", "host_launch_max_s")]
 
 
 _sig("ssa_server_create", _I, ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t, _I, _I, _I, _I)
