@@ -131,23 +131,20 @@ def stream_requests(gpu, specs, id_base: int, keep_outputs: bool = True, pinned:
 
 
 # DRAM traffic of the correlation sweeps measured by ncu relative to their algorithmic bytes:
-# k_corr<13> 0.985 (uniform 512-series batch), k_cl_col<16, CL_CORR> 1.017 and 0.955 (mixed
-# 512-series batch); the mean is used to state the traffic of a launch.
-CORR_TRAFFIC_RATIO = 0.986
+# k_corr<13> 0.985 (uniform 512-series batch), k_cl_col<6, CL_CORR> 1.002 and 0.980 (mixed
+# 512-series batch, real FFT length 98304); the mean is used to state the traffic of a launch.
+CORR_TRAFFIC_RATIO = 0.989
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # SMs x FP32 lanes x FMA x clock (nominal peak)
 
 
-def corr_flops(N: int, L: int, k: int, p: int, q: int) -> float:
-    """Algorithmic FLOPs of the correlation sweeps of one series: per probe column a forward and
-    an inverse complex FFT of H = M/2 points (5 H log2 H each) and the real-spectrum unpacking,
-    spectral product and packing (~12 H)."""
+def corr_flops(N: int, L: int, k: int, p: int, q: int, M: int) -> float:
+    """Algorithmic FLOPs of the correlation sweeps of one series at real FFT length M: per probe
+    column a forward and an inverse complex FFT of H = M/2 points (5 H log2 H each, the usual
+    count for any length) and the real-spectrum unpacking, spectral product and packing (~12 H)."""
     K = N - L + 1
     kp = min(k + p, L, K)
-    logm = 5
-    while (1 << logm) < N:
-        logm += 1
-    H = 1 << (logm - 1)
-    return (2 * q + 2) * kp * (10.0 * H * (logm - 1) + 12.0 * H)
+    H = M // 2
+    return (2 * q + 2) * kp * (10.0 * H * math.log2(H) + 12.0 * H)
 
 
 def corr_bytes(N: int, L: int, k: int, p: int, q: int) -> int:
@@ -345,7 +342,7 @@ def device_steps(gpu, torch, a, rank: int, world: int) -> dict:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
     cb = sum(corr_bytes(N, L, k, a.p, a.q) for N, L, k in zip(Ns, Ls, ks))
-    cf = sum(corr_flops(N, L, k, a.p, a.q) for N, L, k in zip(Ns, Ls, ks))
+    cf = sum(corr_flops(N, L, k, a.p, a.q, gpu.fft_length(N)) for N, L, k in zip(Ns, Ls, ks))
     corr_ms, corr_n = prof["corr"]
     peak, peak_kind = measured_peak_hbm()
     per_launch = cb / max(corr_n, 1)
@@ -362,7 +359,7 @@ def device_steps(gpu, torch, a, rank: int, world: int) -> dict:
                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                         "peak_source": peak_kind, "traffic": CORR_TRAFFIC_RATIO * per_launch,
                         "traffic_source": "ncu dram__bytes_read+write / algorithmic bytes of captured launches "
-                                          "(k_corr<13> 0.985, k_cl_col<16,1> 1.017 / 0.955) x this launch's bytes",
+                                          "(k_corr<13> 0.985, k_cl_col<6,1> 1.002 / 0.980) x this launch's bytes",
                         "avg_launch_ms": avg_ms, "algorithmic_bytes_per_launch": per_launch,
                         "compute": {"bound": "fp32 issue", "achieved_tflops": tflops,
                                     "peak_tflops": FP32_NOMINAL_TFLOPS,

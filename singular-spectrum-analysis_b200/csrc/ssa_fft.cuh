@@ -327,12 +327,100 @@ __device__ __forceinline__ void fft_pass(const In& in, const Out& out, const flo
     if constexpr (Out::kSmem) __syncthreads();
 }
 
+// W_32^i (forward sign) or its conjugate, i < 8.
+template <bool INV, int I>
+__device__ __forceinline__ float2 w32c() {
+    static_assert(I >= 0 && I < 8, "W_32^i for i < 8");
+    // c[i] = cos(2 pi i / 32); sin(2 pi i / 32) = c[8 - i]
+    constexpr float c[9] = {1.f, 0.98078528040323044f, 0.92387953251128674f, 0.83146961230254524f,
+                            0.70710678118654752f, 0.55557023301960218f, 0.38268343236508978f, 0.19509032201612826f,
+                            0.f};
+    return make_float2(c[I], INV ? c[8 - I] : -c[8 - I]);
+}
+
+// The last Stockham pass as one radix-32 step (LOGNS = LOGH - 5) instead of a radix-16 pass
+// followed by a radix-2 pass: one shared-memory round trip and one barrier fewer per transform.
+// The two lanes e = 0, 1 of a pair (group j = tid / 2) hold the even and odd inputs
+// x_{2r+e} (r < 16) of the group's 32 points. With u = W_H^{2k} (k = j, the group's twiddle
+// index) lane e forms D_e = DFT16(x_{2r+e} u^r), and the 32 outputs are
+//     X[q] = D_0[q] + c_q D_1[q],  X[q + 16] = D_0[q] - c_q D_1[q],  c_q = W_H^k W_32^q,  q < 16,
+// the odd half's own twiddle W_H^{k} folded into c_q. Lane e keeps q in [8e, 8e + 8): it trades
+// the eight D values it does not combine for the partner's eight it does (one shuffle each).
+template <int LOGNS, int LOGH, bool INV, class In, class Out>
+__device__ __forceinline__ void fft_pass32(const In& in, const Out& out, const float2* tw, int tid) {
+    constexpr int H = 1 << LOGH;
+    constexpr int T = H / 16;
+    constexpr int NS = 1 << LOGNS;  // = H / 32 = the input stride
+    static_assert(LOGNS + 5 == LOGH && LOGNS >= 4, "radix-32 last pass after at least one radix-16 pass");
+    static_assert(T % 32 == 0, "whole warps of lane pairs");
+    const bool active = tid < T;
+    const int j = tid >> 1, e = tid & 1;
+    float2 a[16];
+    if (active) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) a[r] = in(j + (2 * r + e) * NS);
+    }
+    if constexpr (In::kSmem && Out::kSmem) __syncthreads();
+    if (active) {
+        // u^r by the radix-16 pass's scheme: two table values (u, u^4) and products
+        const float2 u1 = twiddle<LOGH + 1, INV>(tw, 4 * j);
+        const float2 u4 = twiddle<LOGH + 1, INV>(tw, 16 * j);
+        const float2 u2 = cmul(u1, u1);
+        const float2 u3 = cmul(u2, u1);
+        a[1] = cmul(a[1], u1);
+        a[2] = cmul(a[2], u2);
+        a[3] = cmul(a[3], u3);
+        a[4] = cmul(a[4], u4);
+        a[5] = cmul(a[5], cmul(u4, u1));
+        a[6] = cmul(a[6], cmul(u4, u2));
+        a[7] = cmul(a[7], cmul(u4, u3));
+        const float2 u8 = cmul(u4, u4);
+        a[8] = cmul(a[8], u8);
+        a[9] = cmul(a[9], cmul(u8, u1));
+        a[10] = cmul(a[10], cmul(u8, u2));
+        a[11] = cmul(a[11], cmul(u8, u3));
+        const float2 u12 = cmul(u8, u4);
+        a[12] = cmul(a[12], u12);
+        a[13] = cmul(a[13], cmul(u12, u1));
+        a[14] = cmul(a[14], cmul(u12, u2));
+        a[15] = cmul(a[15], cmul(u12, u3));
+        dft16<INV>(a);
+        // lane 0 keeps D_0[0..7] and receives D_1[0..7]; lane 1 keeps D_1[8..15] and receives
+        // D_0[8..15]: afterwards a[i] = D_0[8e + i], a[8 + i] = D_1[8e + i]
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float2 snd = e ? a[i] : a[8 + i];
+            float2 rcv;
+            rcv.x = __shfl_xor_sync(0xffffffffu, snd.x, 1);
+            rcv.y = __shfl_xor_sync(0xffffffffu, snd.y, 1);
+            if (e) a[i] = rcv;
+            else a[8 + i] = rcv;
+        }
+        // c_{8e} = W_M^{2k + 8e (H / 16)} = W_M^{2k + e H / 2}, M = 2H; c_{8e + i} = c_{8e} W_32^i
+        const float2 c0 = twiddle<LOGH + 1, INV>(tw, 2 * j + e * (H / 2));
+        const float2 cs[8] = {c0,
+                              cmul(c0, w32c<INV, 1>()), cmul(c0, w32c<INV, 2>()), cmul(c0, w32c<INV, 3>()),
+                              cmul(c0, w32c<INV, 4>()), cmul(c0, w32c<INV, 5>()), cmul(c0, w32c<INV, 6>()),
+                              cmul(c0, w32c<INV, 7>())};
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int q = 8 * e + i;
+            const float2 t = cmul(a[8 + i], cs[i]);
+            out(j + q * NS, cadd(a[i], t));
+            out(j + (q + 16) * NS, csub(a[i], t));
+        }
+    }
+    if constexpr (Out::kSmem) __syncthreads();
+}
+
 // Passes from LOGNS on; the first one reads through `in`, the last one writes through `out`.
 template <int LOGH, bool INV, int LOGNS, class In, class Out>
 __device__ __forceinline__ void fft_passes(float2* s, const In& in, const Out& out, const float2* tw, int tid) {
     const SmemPts sp{s};
     constexpr int RLOG = (LOGNS + 4 <= LOGH) ? 4 : LOGH - LOGNS;
-    if constexpr (LOGNS + RLOG == LOGH) {
+    if constexpr (LOGNS >= 4 && LOGH - LOGNS == 5) {
+        fft_pass32<LOGNS, LOGH, INV>(in, out, tw, tid);
+    } else if constexpr (LOGNS + RLOG == LOGH) {
         fft_pass<RLOG, LOGNS, LOGH, INV>(in, out, tw, tid);
     } else {
         fft_pass<RLOG, LOGNS, LOGH, INV>(in, sp, tw, tid);

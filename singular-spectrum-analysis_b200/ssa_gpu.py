@@ -117,6 +117,7 @@ _sig("ssa_batch_profile", _I, ctypes.c_void_p, c_double_p, ctypes.POINTER(ctypes
 _sig("ssa_b200_set_wcorr_tensor_cores", _V, _I)
 _sig("ssa_b200_wcorr_tensor_cores", _I)
 _sig("ssa_b200_device_checks", _I, ctypes.POINTER(ctypes.c_uint), _I)
+_sig("ssa_b200_fft_length", _I, _I)
 
 
 def set_wcorr_tensor_cores(on: bool) -> None:
@@ -137,6 +138,12 @@ def device_checks(reset: bool = True) -> List[int]:
 
 PROFILE_KINDS = ("spectrum", "corr", "gram", "chol", "rowmul", "rr", "elem_recon", "wcorr_finish", "group_sum",
                  "recon", "lrf")
+
+
+def fft_length(N: int) -> int:
+    """Real FFT length the uneven batches use for a series of length N (a power of two, or 49152 /
+    98304 between the cluster powers of two); -1 beyond 131072."""
+    return int(_lib.ssa_b200_fft_length(int(N)))
 
 
 def kernel_launches() -> int:
@@ -914,15 +921,29 @@ class Requests:
     append requests; after the server has completed them, ``result(i)`` returns a dict of the
     outputs, ``status`` and the latency in seconds."""
 
-    def __init__(self, capacity: int, keep_outputs: bool = True, pinned: bool = False):
+    def __init__(self, capacity: int, keep_outputs: bool = True, pinned=False):
+        """pinned: False (pageable numpy buffers), True (page-locked) or "mixed": request i of a
+        decomposition has, by i % 4, all buffers page-locked / a pageable input with page-locked
+        outputs / a page-locked input with pageable outputs / page-locked input and sigma with a
+        pageable second output; forecast outputs alternate."""
         self.arr = (_Request * max(1, capacity))()
         self.n = 0
         self.keep_outputs = keep_outputs
         self._bufs = []
         self._pool = _PinnedPool() if pinned else None
+        self._mixed = pinned == "mixed"
 
-    def _buf(self, shape, src=None):
-        if self._pool is not None:
+    def _locked(self, role: int) -> bool:
+        """role 0: input, 1: first output, 2: second output"""
+        if self._pool is None:
+            return False
+        if not self._mixed:
+            return True
+        pat = (self.n - 1) % 4
+        return {0: True, 1: role != 0, 2: role == 0, 3: role != 2}[pat]
+
+    def _buf(self, shape, src=None, role: int = 0):
+        if self._locked(role):
             return self._pool.array(shape, src)
         if src is not None:
             return np.ascontiguousarray(src, dtype=np.float64)
@@ -946,13 +967,13 @@ class Requests:
         bufs = {"x": x}
         if self.keep_outputs:
             ke = max(1, min(k, L, N - L + 1))
-            bufs["sigma"] = self._buf((ke,))
+            bufs["sigma"] = self._buf((ke,), role=1)
             r.sigma = _dp(bufs["sigma"])
             if wcorr:
-                bufs["W"] = self._buf((ke, ke))
+                bufs["W"] = self._buf((ke, ke), role=2)
                 r.W = _dp(bufs["W"])
             else:
-                bufs["groups"] = self._buf((2, N))
+                bufs["groups"] = self._buf((2, N), role=2)
                 r.groups = _dp(bufs["groups"])
         self._bufs.append(bufs)
         return self.n - 1
@@ -963,7 +984,7 @@ class Requests:
         r.series_id, r.h = series_id, h
         bufs = {}
         if self.keep_outputs:
-            bufs["forecast"] = self._buf((h,))
+            bufs["forecast"] = self._buf((h,), role=1 + (self.n - 1) % 2)
             r.forecast = _dp(bufs["forecast"])
         self._bufs.append(bufs)
         return self.n - 1

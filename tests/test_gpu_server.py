@@ -61,9 +61,12 @@ def oracle_dec(oracle, x, L, k, seed):
     return oracle.decompose_randomized(x, L, k, P, Om, q=Q)
 
 
-@pytest.mark.parametrize("pinned", [False, True])
+@pytest.mark.parametrize("pinned", [False, True, "mixed"])
 def test_server_mixed_requests_vs_oracle(gpu, oracle, pinned):
-    """Pageable buffers go through the staging areas, page-locked ones are copied directly."""
+    """Pageable buffers go through the staging areas, page-locked ones are read and written by the
+    batch's gather and scatter kernels directly; "mixed" puts both kinds in one batch and within
+    one request (a page-locked input with pageable outputs and the reverse, and requests whose
+    outputs mix both, which are staged as a whole)."""
     rng = np.random.default_rng(21)
     shapes = [(800, 200, 12), (5000, 1250, 30), (12000, 3000, 20), (18000, 4500, 15), (2500, 625, 45),
               (70000, 17500, 14)]
