@@ -106,10 +106,10 @@ typedef struct
     int pad_[2];
 } ssa_chol_job;
 
-/* Row products with a small matrix, FP64 accumulation: C[:, 0:p] = A[:, 0:n] * Bm[0:n, 0:p], or
+/* Row products with a small matrix, FP32 accumulation: C[:, 0:p] = A[:, 0:n] * Bm[0:n, 0:p], or
  * sub - A * Bm when sub != NULL. In place allowed (C == A): a CTA reads all columns of its
  * SSA_ROWMUL_ROWS rows before writing them. Bm is FP32 (Bm) or FP64 (Bm64, e.g. R^{-1} of a
- * CholQR pass: Q = Y R^{-1}). */
+ * CholQR pass: Q = Y R^{-1}; rounded to FP32). */
 typedef struct
 {
     const float *A;
