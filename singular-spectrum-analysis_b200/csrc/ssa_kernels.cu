@@ -496,28 +496,88 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
                  : "d"(a), "d"(b));
 }
 
-// Stage rows [r0, r0 + SSA_GRAM_CHUNK) of columns [0, n) into buf ([col][row], stride GRAM_S);
-// rows at or beyond r_end are zero-filled (they belong to another CTA's partial or lie past m).
 #define GRAM_MMA_THREADS 256
+#define GRAM_HALF (SSA_GRAM_CHUNK / 2)
 
-__device__ __forceinline__ void gram_stage(uint32_t buf, const ssa_gram_job& J, int r0, int r_end, bool vec) {
+// Stage rows [r0 + 64 h, r0 + 64 h + 64) of columns [0, n) into rows [64 h, 64 h + 64) of buf
+// ([col][row], stride GRAM_S), by the 128 threads of half h; rows at or beyond r_end are
+// zero-filled (they belong to another CTA's partial or lie past m).
+__device__ __forceinline__ void gram_stage_half(uint32_t buf, const ssa_gram_job& J, int r0, int r_end, bool vec,
+                                                int h, int th) {
+    const int rb = r0 + GRAM_HALF * h;
+    const uint32_t hb = buf + 4u * (uint32_t)(GRAM_HALF * h);
     if (vec) {
-        constexpr int Q = SSA_GRAM_CHUNK / 4;
-        for (int idx = threadIdx.x; idx < J.n * Q; idx += GRAM_MMA_THREADS) {
+        constexpr int Q = GRAM_HALF / 4;
+        for (int idx = th; idx < J.n * Q; idx += GRAM_MMA_THREADS / 2) {
             const int col = idx / Q, q = idx - col * Q;
-            const int r = r0 + 4 * q;
+            const int r = rb + 4 * q;
             const int valid = min(4, max(0, r_end - r));
             const float* src = valid > 0 ? J.A + (long long)r + (long long)col * J.ld : J.A;
-            cp_async16(buf + 4u * (uint32_t)(col * GRAM_S + 4 * q), src, 4 * valid);
+            cp_async16(hb + 4u * (uint32_t)(col * GRAM_S + 4 * q), src, 4 * valid);
         }
     } else {
-        for (int idx = threadIdx.x; idx < J.n * SSA_GRAM_CHUNK; idx += GRAM_MMA_THREADS) {
-            const int col = idx / SSA_GRAM_CHUNK, q = idx - col * SSA_GRAM_CHUNK;
-            const int r = r0 + q;
+        for (int idx = th; idx < J.n * GRAM_HALF; idx += GRAM_MMA_THREADS / 2) {
+            const int col = idx / GRAM_HALF, q = idx - col * GRAM_HALF;
+            const int r = rb + q;
             const bool ok = r < r_end;
             const float* src = ok ? J.A + (long long)r + (long long)col * J.ld : J.A;
-            cp_async4(buf + 4u * (uint32_t)(col * GRAM_S + q), src, ok ? 4 : 0);
+            cp_async4(hb + 4u * (uint32_t)(col * GRAM_S + q), src, ok ? 4 : 0);
         }
+    }
+}
+
+// Named barrier of one half of the CTA (ids 1 and 2 as immediates, so that only three of the
+// CTA's barriers are in use).
+__device__ __forceinline__ void bar_half(int h) {
+    if (h) asm volatile("bar.sync 2, %0;" ::"n"(GRAM_MMA_THREADS / 2) : "memory");
+    else asm volatile("bar.sync 1, %0;" ::"n"(GRAM_MMA_THREADS / 2) : "memory");
+}
+
+// The chunk loop of warp pair (WQ, WQ + 4): tile columns c1 = WQ (rows 0 .. WQ, when
+// 2 WQ <= nt - 1) and c2 = nt - 1 - WQ (rows 0 .. c2, when c2 > WQ), accumulator slot i <= WQ
+// for (i, c1) and WQ + 1 + i for (i, c2). With WQ a compile-time constant every slot and every
+// row fragment has a fixed register, so each fragment of A is loaded and converted once per
+// k-step for both tile columns (8 - WQ fragments instead of 9 loads).
+template <bool WEIGHTED, int WQ>
+__device__ __forceinline__ void gram_loop(const ssa_gram_job& J, const float* gsm, uint32_t sbase, int r_begin,
+                                          int r_end, int nchunk, bool vec, int nt, int half, int th, int lane,
+                                          double (&acc)[9][2], double& csum) {
+    const int g = lane >> 2, t = lane & 3;
+    const bool has1 = 2 * WQ <= nt - 1;
+    const int c2 = (has1 && nt - 1 - WQ > WQ) ? nt - 1 - WQ : -1;
+    for (int ic = 0; ic < nchunk; ++ic) {
+        const int r0 = r_begin + ic * SSA_GRAM_CHUNK;
+        if (ic + 1 < nchunk)
+            gram_stage_half(sbase + 4u * (uint32_t)(((ic + 1) & 1) * GRAM_STAGE), J, r0 + SSA_GRAM_CHUNK, r_end, vec,
+                            half, th);
+        cp_async_commit();
+        cp_async_wait<1>();
+        bar_half(half);
+        const float* sA = gsm + (ic & 1) * GRAM_STAGE;
+        if (J.colsum && th < J.n) {
+            double cs = 0.0;
+            for (int r = 0; r < GRAM_HALF; ++r) cs += (double)sA[th * GRAM_S + GRAM_HALF * half + r];
+            csum += cs;
+        }
+        if (has1) {
+            const float* pa = sA + g * GRAM_S + t;  // lane's element of tile row 0, k-step 0
+#pragma unroll 2
+            for (int s4 = half * GRAM_HALF; s4 < (half + 1) * GRAM_HALF; s4 += 4) {
+                const float* row = pa + s4;
+                double w = 1.0;
+                if (WEIGHTED) w = (double)diag_count(r0 + s4 + t, J.N, J.L, J.K);
+                const double b1 = w * (double)row[8 * WQ * GRAM_S];
+                const double b2 = c2 >= 0 ? w * (double)row[8 * c2 * GRAM_S] : 0.0;
+#pragma unroll
+                for (int bi = 0; bi < 8; ++bi) {
+                    if (bi > WQ && bi > c2) break;
+                    const double a = (double)row[8 * bi * GRAM_S];
+                    if (bi <= WQ) dmma_8x8x4(acc[bi][0], acc[bi][1], a, b1);
+                    if (bi <= 7 - WQ && bi <= c2) dmma_8x8x4(acc[WQ + 1 + bi][0], acc[WQ + 1 + bi][1], a, b2);
+                }
+            }
+        }
+        bar_half(half);  // this half of the stage is refilled two chunks later
     }
 }
 
@@ -525,10 +585,10 @@ __device__ __forceinline__ void gram_stage(uint32_t buf, const ssa_gram_job& J, 
 // data, exact FP64 products (FP32 x FP32 x integer weight), FP64 accumulation. G is cut into
 // 8x8 tiles (nt = ceil(n/8) <= 8 per side); warps w and w + 4 own the upper-triangle tiles of
 // tile columns w and nt - 1 - w (at most nt + 1 <= 9 tiles), warp w over the first half of each
-// chunk's rows and warp w + 4 over the second half (their sums are added at the end), so that
-// eight warps keep the FP64 tensor pipe busy through the chunk barriers. Chunks of
-// SSA_GRAM_CHUNK rows are staged by asynchronous copies into two buffers, the next one landing
-// while the current one is multiplied.
+// chunk's rows and warp w + 4 over the second half (their sums are added at the end). Each half
+// of the CTA stages its own half of every chunk (asynchronous copies into two buffers, the next
+// chunk landing while the current one is multiplied) and synchronises on its own named barrier,
+// so the two halves do not wait for each other between chunks.
 template <bool WEIGHTED>
 __global__ void __launch_bounds__(GRAM_MMA_THREADS, 3) k_gram(const ssa_gram_job* __restrict__ jobs) {
     extern __shared__ __align__(16) float gsm[];
@@ -541,8 +601,8 @@ __global__ void __launch_bounds__(GRAM_MMA_THREADS, 3) k_gram(const ssa_gram_job
     const int nt = (n + 7) >> 3;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wq = warp & 3, half = warp >> 2;
+    const int th = threadIdx.x & (GRAM_MMA_THREADS / 2 - 1);
     const int g = lane >> 2, t = lane & 3;
-    // this warp's two tile columns (c2 = -1: none)
     const int c1 = 2 * wq <= nt - 1 ? wq : -1;
     const int c2 = (c1 >= 0 && nt - 1 - wq > wq) ? nt - 1 - wq : -1;
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(gsm);
@@ -553,54 +613,23 @@ __global__ void __launch_bounds__(GRAM_MMA_THREADS, 3) k_gram(const ssa_gram_job
         gsm[col * GRAM_S + q] = 0.f;
         gsm[GRAM_STAGE + col * GRAM_S + q] = 0.f;
     }
+    __syncthreads();
     double acc[9][2];
 #pragma unroll
     for (int i = 0; i < 9; ++i) acc[i][0] = acc[i][1] = 0.0;
     double csum = 0.0;
     const int nchunk = (r_end - r_begin + SSA_GRAM_CHUNK - 1) / SSA_GRAM_CHUNK;
-    gram_stage(sbase, J, r_begin, r_end, vec);
+    gram_stage_half(sbase, J, r_begin, r_end, vec, half, th);
     cp_async_commit();
-    for (int ic = 0; ic < nchunk; ++ic) {
-        const int r0 = r_begin + ic * SSA_GRAM_CHUNK;
-        if (ic + 1 < nchunk)
-            gram_stage(sbase + 4u * (uint32_t)(((ic + 1) & 1) * GRAM_STAGE), J, r0 + SSA_GRAM_CHUNK, r_end, vec);
-        cp_async_commit();
-        cp_async_wait<1>();
-        __syncthreads();
-        const float* sA = gsm + (ic & 1) * GRAM_STAGE;
-        if (J.colsum && threadIdx.x < n) {
-            double cs = 0.0;
-            for (int r = 0; r < SSA_GRAM_CHUNK; ++r) cs += (double)sA[threadIdx.x * GRAM_S + r];
-            csum += cs;
-        }
-        if (c1 >= 0) {
-            const float* pa = sA + g * GRAM_S + t;  // lane's element of tile column 0, k-step 0
-            const int s_end = (half + 1) * (SSA_GRAM_CHUNK / 2);
-#pragma unroll 2
-            for (int s4 = half * (SSA_GRAM_CHUNK / 2); s4 < s_end; s4 += 4) {
-                const float* row = pa + s4;
-                double b1 = (double)row[8 * c1 * GRAM_S];
-                double b2 = c2 >= 0 ? (double)row[8 * c2 * GRAM_S] : 0.0;
-                if (WEIGHTED) {
-                    const double w = (double)diag_count(r0 + s4 + t, J.N, J.L, J.K);
-                    b1 *= w;
-                    b2 *= w;
-                }
-#pragma unroll
-                for (int i = 0; i < 9; ++i) {
-                    // tile i: (i, c1) for i <= c1, else (i - c1 - 1, c2)
-                    const bool first = i <= c1;
-                    const int bi = first ? i : i - c1 - 1;
-                    if (!first && (c2 < 0 || bi > c2)) continue;
-                    const double a = (double)row[8 * bi * GRAM_S];
-                    dmma_8x8x4(acc[i][0], acc[i][1], a, first ? b1 : b2);
-                }
-            }
-        }
-        __syncthreads();  // this stage is refilled two chunks later
+    switch (wq) {
+        case 0: gram_loop<WEIGHTED, 0>(J, gsm, sbase, r_begin, r_end, nchunk, vec, nt, half, th, lane, acc, csum); break;
+        case 1: gram_loop<WEIGHTED, 1>(J, gsm, sbase, r_begin, r_end, nchunk, vec, nt, half, th, lane, acc, csum); break;
+        case 2: gram_loop<WEIGHTED, 2>(J, gsm, sbase, r_begin, r_end, nchunk, vec, nt, half, th, lane, acc, csum); break;
+        default: gram_loop<WEIGHTED, 3>(J, gsm, sbase, r_begin, r_end, nchunk, vec, nt, half, th, lane, acc, csum); break;
     }
-    // the second row half's sums join the first half's through shared memory (stages are free:
-    // every copy has landed and the loop ended on a barrier)
+    // the second row half's sums join the first half's through shared memory, once both halves
+    // are done with the stages
+    __syncthreads();
     double* red = reinterpret_cast<double*>(gsm);
     if (half == 1 && c1 >= 0) {
 #pragma unroll
@@ -609,6 +638,8 @@ __global__ void __launch_bounds__(GRAM_MMA_THREADS, 3) k_gram(const ssa_gram_job
             red[((wq * 9 + i) * 2 + 1) * 32 + lane] = acc[i][1];
         }
     }
+    double* csred = red + 4 * 9 * 2 * 32;
+    if (half == 1 && J.colsum && th < n) csred[th] = csum;
     __syncthreads();
     double* part = J.part + (long long)chunk * (n * (n + 1) / 2);
     if (half == 0 && c1 >= 0) {
@@ -631,7 +662,7 @@ __global__ void __launch_bounds__(GRAM_MMA_THREADS, 3) k_gram(const ssa_gram_job
             }
         }
     }
-    if (J.colsum && threadIdx.x < n) J.colsum[(long long)chunk * n + threadIdx.x] = csum;
+    if (half == 0 && J.colsum && th < n) J.colsum[(long long)chunk * n + th] = csum + csred[th];
 }
 
 // ---------------------------------------------------------------------------------------------
