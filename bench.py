@@ -32,6 +32,11 @@ from pathlib import Path
 
 import numpy as np
 
+# one hardware work queue per stream for the bucket streams of the batches in flight (the
+# runtime's default of 8 serialises streams that share a queue); read when the CUDA context is
+# created, so it is set before anything touches the GPU
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = Path(__file__).resolve().parent
 PKG = ROOT / "singular-spectrum-analysis_b200"
 ORACLE = ROOT / "oracle"

@@ -151,6 +151,10 @@ int ssae_grow_arena(ssa_engine *e, size_t bytes)
 {
     if (bytes <= e->ja.cap)
         return 0;
+    /* freeing page-locked and device memory waits for the whole device: grow by at least half
+     * again, so that a slowly growing workload pays that wait a few times, not once per batch */
+    if (e->ja.cap > 0 && bytes < e->ja.cap + e->ja.cap / 2)
+        bytes = e->ja.cap + e->ja.cap / 2;
     {
         const char *ev = getenv("SSA_SERVER_TRACE");
         if (ev && ev[0] == '1' && e->ja.cap > 0)

@@ -12,6 +12,7 @@ Importing this module raises ``ImportError`` when libssa.so has not been built.
 from __future__ import annotations
 
 import ctypes
+import os
 from pathlib import Path
 from typing import List, Optional, Sequence, Tuple
 
@@ -21,6 +22,9 @@ LIB_PATH = Path(__file__).resolve().parent / "libssa.so"
 if not LIB_PATH.exists():
     raise ImportError(f"{LIB_PATH} is missing: run build.py (nvcc, sm_100a) first")
 
+# 32 hardware work queues for the bucket and batch streams (read at CUDA context creation; the
+# library's load-time default does the same for C callers)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 _lib = ctypes.CDLL(str(LIB_PATH))
 
 c_double_p = ctypes.POINTER(ctypes.c_double)
