@@ -690,6 +690,13 @@ static void take_queue(ssa_server *s)
     pthread_mutex_unlock(&s->mu);
 }
 
+/* Size class of a decomposition: series whose transforms run on thread-block clusters (real FFT
+ * length above 32768) take several times longer than the rest, and a batch completes as a whole,
+ * so they are batched apart: a short series never waits for a long one's batch. Within a class
+ * requests keep their arrival order. */
+#define SRV_LONG_N 32768
+static int srv_class(const ssa_request *r) { return r->N > SRV_LONG_N; }
+
 /* Form and launch at most one forecast batch and one decomposition batch per free slot. */
 static int dispatch(ssa_server *s)
 {
@@ -701,6 +708,7 @@ static int dispatch(ssa_server *s)
     fslot_t *f = s->fs.busy ? NULL : &s->fs;
     size_t bytes = 0;
     int kept = 0;
+    int cls = -1; /* size class of the batch being formed */
     for (int i = 0; i < s->npend; i++)
     {
         ssa_request *r = s->pend[i];
@@ -775,8 +783,9 @@ static int dispatch(ssa_server *s)
                 keep = 0;
                 progressed = 1;
             }
-            else if (free_slot && free_slot->n < s->max_batch)
+            else if (free_slot && free_slot->n < s->max_batch && (cls < 0 || srv_class(r) == cls))
             {
+                cls = srv_class(r);
                 const size_t b = ssar_series_bytes(r->N, r->L, r->k, s->p, SRV_GROUPS);
                 if (b > s->batch_budget)
                 {
