@@ -68,15 +68,99 @@ class RefLib:
         return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
 
 
+def build_checkers() -> bool:
+    """Builds oracle/_ref/ with oracle/Makefile (which locates the reference sources: its
+    SSA_REFERENCE_DIR, overridable from the environment). False when they are absent."""
+    r = subprocess.run(["make", "-C", str(ORACLE)], capture_output=True, text=True)
+    return r.returncode == 0
+
+
+def reference_dir():
+    """The reference tree's MKL/ directory as oracle/Makefile resolves it, or None."""
+    r = subprocess.run(["make", "-s", "-C", str(ORACLE), "print-refdir"], capture_output=True, text=True)
+    d = Path(r.stdout.strip()) if r.returncode == 0 and r.stdout.strip() else None
+    return d if d is not None and d.is_dir() else None
+
+
 @pytest.fixture(scope="session")
 def reflib():
     so = ORACLE / "_ref" / "libssa_ref.so"
-    if not so.exists():
-        ref = Path("/root/reference/MKL/ssa_opt_ref.h")
-        if not ref.exists():
-            pytest.skip("reference checker library not built and reference sources absent")
-        subprocess.run(["make", "-C", str(ORACLE)], check=True, capture_output=True)
+    if not so.exists() and not build_checkers():
+        pytest.skip("reference checker library not built and reference sources absent")
     return RefLib(so)
+
+
+class MklRef:
+    """ctypes view of oracle/_ref/libssa_mklshim.so: the reference's own MKL/ssa_opt.h compiled
+    against the MKL-compatibility shim (oracle/mklshim/), entry points of oracle/mklref_driver.c.
+    Gaussian / uniform draws of the reference's VSL streams come from registered buffers."""
+
+    def __init__(self, path: Path):
+        self.lib = ctypes.CDLL(str(path))
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        c_int, c_double = ctypes.c_int, ctypes.c_double
+        L = self.lib
+        L.mklshim_set_gaussian.argtypes = [dp, ctypes.c_long]
+        L.mklshim_set_uniform.argtypes = [dp, ctypes.c_long]
+        L.mkr_randomized.argtypes = [dp, c_int, c_int, c_int, c_int, dp, dp, dp, dp]
+        L.mkr_block.argtypes = [dp, c_int, c_int, c_int, c_int, c_int, dp, dp, dp]
+        L.mkr_sequential.argtypes = [dp, c_int, c_int, c_int, c_int, dp, dp, dp]
+        L.mkr_matvec.argtypes = [dp, c_int, c_int, dp, dp, c_int]
+        L.mkr_pipeline.argtypes = [dp, c_int, c_int, c_int, c_int, ip, ip, c_int, dp, c_int, dp, ip, c_int,
+                                   c_int, dp, dp, dp, dp]
+        L.mkr_wcorr_consumers.argtypes = [dp, c_int, c_int, c_int, c_int, ip, ip, c_int, dp, dp, dp, dp, ip, ip,
+                                          c_int, c_double, c_double, ip]
+        L.mkr_mssa.argtypes = [dp, c_int, c_int, c_int, c_int, c_int, dp, dp, dp, ip, c_int, dp, dp]
+        L.mkr_cadzow.argtypes = [dp, c_int, c_int, c_int, c_int, c_double, c_int, c_double, dp, ip, dp, dp]
+        L.mkr_gapfill.argtypes = [dp, c_int, c_int, c_int, c_int, c_double, c_int, ip, dp, ip, ip]
+        L.mkr_parestimate.argtypes = [dp, c_int, c_int, c_int, c_int, ip, c_int, dp, dp, dp, dp]
+        L.mkr_dims.argtypes = [dp, c_int, c_int, ip, ip]
+        self._gauss = self._unif = None
+
+    @staticmethod
+    def d(a):
+        return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+    @staticmethod
+    def i(a):
+        return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+    def set_gaussian(self, draws):
+        """Every VSL stream created afterwards reads these N(0,1) draws from their start."""
+        self._gauss = None if draws is None else np.ascontiguousarray(draws, dtype=np.float64).ravel()
+        self.lib.mklshim_set_gaussian(self.d(self._gauss), 0 if self._gauss is None else self._gauss.size)
+
+    def set_uniform(self, draws):
+        """Every VSL stream created afterwards reads these U[0, 1) draws from their start."""
+        self._unif = None if draws is None else np.ascontiguousarray(draws, dtype=np.float64).ravel()
+        self.lib.mklshim_set_uniform(self.d(self._unif), 0 if self._unif is None else self._unif.size)
+
+    def exhausted(self) -> bool:
+        return bool(self.lib.mklshim_draws_exhausted())
+
+    @staticmethod
+    def omega_draws(Om):
+        """A K x kp test matrix in the order the reference draws it (column-major)."""
+        return np.ascontiguousarray(np.asarray(Om, dtype=np.float64).T).ravel()
+
+    def randomized(self, x, L, k, p, Om):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        N = len(x)
+        K = N - L + 1
+        self.set_gaussian(self.omega_draws(Om))
+        sig, U, V, tv = np.zeros(k), np.zeros(L * k), np.zeros(K * k), ctypes.c_double()
+        n = self.lib.mkr_randomized(self.d(x), N, L, k, p, self.d(sig), self.d(U), self.d(V), ctypes.byref(tv))
+        assert n > 0 and not self.exhausted()
+        return sig[:n], U[:L * n].reshape(n, L).T, V[:K * n].reshape(n, K).T, tv.value
+
+
+@pytest.fixture(scope="session")
+def mklref():
+    so = ORACLE / "_ref" / "libssa_mklshim.so"
+    if not so.exists() and not build_checkers():
+        pytest.skip("shimmed reference library not built and reference sources absent")
+    return MklRef(so)
 
 
 def gpu_available() -> bool:

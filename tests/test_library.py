@@ -12,7 +12,6 @@ import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
 LIB = ROOT / "singular-spectrum-analysis_b200" / "libssa.so"
-REF_WRAPPER = Path("/root/reference/MKL/py/ssa_wrapper.py")
 
 # Export list of the reference shared library (MKL/py/ssa.def) and the names its ctypes
 # wrapper binds unconditionally (MKL/py/ssa_wrapper.py:125-204, 272-291).
@@ -75,8 +74,18 @@ def test_built_for_sm100a_only():
     assert "sm_100a" in out.stdout
 
 
-@pytest.mark.skipif(not REF_WRAPPER.exists(), reason="reference wrapper not present on this machine")
+def _reference_wrapper():
+    from conftest import reference_dir
+
+    d = reference_dir()
+    w = d / "py" / "ssa_wrapper.py" if d is not None else None
+    if w is None or not w.exists():
+        pytest.skip("reference wrapper not present on this machine")
+    return w
+
+
 def test_unchanged_reference_wrapper_binds(lib):
+    REF_WRAPPER = _reference_wrapper()
     code = (
         "import importlib.util\n"
         f"spec = importlib.util.spec_from_file_location('ssa_wrapper', r'{REF_WRAPPER}')\n"
@@ -84,7 +93,6 @@ def test_unchanged_reference_wrapper_binds(lib):
         "assert m._HAS_GETTERS and m._HAS_CADZOW and m._HAS_ESPRIT and m._HAS_GAPFILL and m._HAS_VFORECAST\n"
         "print('ok')\n"
     )
-    env = {"LD_LIBRARY_PATH": str(LIB.parent), "PATH": "/usr/bin:/bin"}
     import os, sys
     env = dict(os.environ, LD_LIBRARY_PATH=str(LIB.parent))
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env)
