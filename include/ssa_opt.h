@@ -169,6 +169,15 @@ int ssa_opt_reconstruct(const SSA_Opt *ssa, const int *group, int n_group, ssa_r
 int ssa_opt_cache_ffts(SSA_Opt *ssa);
 void ssa_opt_free_cached_ffts(SSA_Opt *ssa);
 
+/* The Hankel matvec y = H v (v: K values, y: L values) and its adjoint z = H^T u (u: L values,
+ * z: K values) on host arrays, computed on the device (reference MKL/ssa_opt.h:871-903, where
+ * they are static functions that the reference's C tests call directly,
+ * MKL/test/ssa_opt_test.c:1484, 1533). Nothing is written on an invalid context. The device
+ * factor buffers serve as the workspace, so a decomposition the context holds is discarded
+ * (decomposed becomes false). */
+void ssa_opt_hankel_matvec(SSA_Opt *ssa, const ssa_real *v, ssa_real *y);
+void ssa_opt_hankel_matvec_T(SSA_Opt *ssa, const ssa_real *u, ssa_real *z);
+
 /* ---- analysis (reference MKL/ssa_opt.h:338-348) ------------------------------------------ */
 int ssa_opt_wcorr_matrix(const SSA_Opt *ssa, ssa_real *W);
 int ssa_opt_wcorr_matrix_fast(const SSA_Opt *ssa, ssa_real *W);
@@ -214,7 +223,8 @@ int ssa_opt_cadzow_weighted(const ssa_real *x, int N, int L, int rank, int max_i
                             ssa_real tol, ssa_real alpha, ssa_real *output, SSA_CadzowResult *result);
 int ssa_opt_cadzow_inplace(SSA_Opt *ssa, int rank, int max_iter, ssa_real tol, SSA_CadzowResult *result);
 
-/* ---- ESPRIT and gap filling (reference :402-430; out of scope: return -1) ----------------- */
+/* ---- ESPRIT and gap filling (reference :402-430): ESPRIT's cross Grams on the device, its
+ * k x k solve and eigenvalues on the host; gap filling device-resident like Cadzow ----------- */
 int ssa_opt_parestimate(const SSA_Opt *ssa, const int *group, int n_group, SSA_ParEstimate *result);
 void ssa_opt_parestimate_free(SSA_ParEstimate *result);
 int ssa_opt_gapfill(ssa_real *x, int N, int L, int rank, int max_iter, ssa_real tol, SSA_GapFillResult *result);

@@ -6,6 +6,7 @@ alone. Usage: ``python build.py`` (from anywhere) or ``build.build()``.
 """
 from __future__ import annotations
 
+import hashlib
 import os
 import shutil
 import subprocess
@@ -44,11 +45,30 @@ def _run(cmd: list[str]) -> None:
         raise RuntimeError("build failed: " + " ".join(cmd) + "\n" + r.stdout + r.stderr)
 
 
-def _stale(target: Path, deps: list[Path]) -> bool:
-    if not target.exists():
-        return True
-    t = target.stat().st_mtime
-    return any(d.stat().st_mtime > t for d in deps)
+def _stale(target: Path, deps: list[Path], cmd: list[str] | None = None) -> bool:
+    """True when `target` is missing or was built from other contents of `deps` (or another
+    command): a content digest is kept beside each target, so clock skew between file systems
+    cannot leave a stale object in place."""
+    h = hashlib.sha256()
+    for d in sorted(deps):
+        h.update(str(d).encode())
+        h.update(d.read_bytes())
+    h.update(" ".join(cmd or []).encode())
+    digest = h.hexdigest()
+    stamp = target.with_name(target.name + ".sha256")
+    if target.exists() and stamp.exists() and stamp.read_text() == digest:
+        return False
+    _pending[target] = (stamp, digest)
+    return True
+
+
+_pending: dict = {}
+
+
+def _done(target: Path) -> None:
+    if target in _pending:
+        stamp, digest = _pending.pop(target)
+        stamp.write_text(digest)
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
@@ -60,28 +80,31 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     for src in CU_SOURCES:
         s = CSRC / src
         o = BUILD / (s.stem + ".cu.o")
-        if force or _stale(o, [s] + headers):
-            cmd = [nvcc, *NVCC_FLAGS, "-I", str(CSRC), "-I", str(INCLUDE), "-c", str(s), "-o", str(o)]
+        cmd = [nvcc, *NVCC_FLAGS, "-I", str(CSRC), "-I", str(INCLUDE), "-c", str(s), "-o", str(o)]
+        if _stale(o, [s] + headers, cmd) or force:
             if verbose:
                 print(" ".join(cmd))
             _run(cmd)
+            _done(o)
         objs.append(o)
     for src in C_SOURCES:
         s = CSRC / src
         o = BUILD / (s.stem + ".c.o")
-        if force or _stale(o, [s] + headers):
-            cmd = ["gcc", "-std=gnu11", "-O2", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-parameter",
-                   "-I", str(cuda / "include"), "-I", str(CSRC), "-I", str(INCLUDE), "-c", str(s), "-o", str(o)]
+        cmd = ["gcc", "-std=gnu11", "-O2", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-parameter",
+               "-I", str(cuda / "include"), "-I", str(CSRC), "-I", str(INCLUDE), "-c", str(s), "-o", str(o)]
+        if _stale(o, [s] + headers, cmd) or force:
             if verbose:
                 print(" ".join(cmd))
             _run(cmd)
+            _done(o)
         objs.append(o)
-    if force or _stale(OUT, objs):
-        cmd = [nvcc, "-shared", "-cudart", "static", "-gencode", "arch=compute_100a,code=sm_100a",
-               "-o", str(OUT), *map(str, objs), "-lm", "-lpthread"]
+    cmd = [nvcc, "-shared", "-cudart", "static", "-gencode", "arch=compute_100a,code=sm_100a",
+           "-o", str(OUT), *map(str, objs), "-lm", "-lpthread"]
+    if _stale(OUT, objs, cmd) or force:
         if verbose:
             print(" ".join(cmd))
         _run(cmd)
+        _done(OUT)
     return OUT
 
 

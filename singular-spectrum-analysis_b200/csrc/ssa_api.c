@@ -782,54 +782,51 @@ ssa_real ssa_opt_get_total_variance(const SSA_Opt *ssa)
 
 /* ---- component statistics and periodic pairs (MKL/ssa_opt.h:2634-2756) ------------------ */
 
+/* Statistics for choosing the signal rank (outputs as MKL/ssa_opt.h:2634-2695 defines them):
+ *   singular_values: the decomposition's sigma;  log_sv[i] = ln(sigma_i + 1e-300);
+ *   gaps[i] (i < n-1): the drop ratio sigma_i / (sigma_{i+1} + 1e-300) between neighbours;
+ *   cumulative_var[i]: share of total_variance held by components 0..i;
+ *   second_diff[i]: curvature of the log spectrum, log_sv[i-1] - 2 log_sv[i] + log_sv[i+1],
+ *                   0 at both ends;
+ *   suggested_signal: 1 + the first position of the largest drop ratio; gap_threshold: that ratio.
+ * The five arrays share one allocation (released by ssa_opt_component_stats_free). -1 when not
+ * decomposed or fewer than two components. */
 int ssa_opt_component_stats(const SSA_Opt *ssa, SSA_ComponentStats *stats)
 {
-    if (!ssa || !ssa->decomposed || !stats)
+    if (!ssa || !stats || !ssa->decomposed || ssa->n_components < 2)
         return -1;
-    int n = ssa->n_components;
-    if (n < 2)
+    const int n = ssa->n_components;
+    double *arena = (double *)malloc(sizeof(double) * (size_t)(5 * n - 1));
+    if (!arena)
         return -1;
-    memset(stats, 0, sizeof(SSA_ComponentStats));
+    memset(stats, 0, sizeof(*stats));
     stats->n = n;
-    stats->singular_values = (double *)malloc(sizeof(double) * n);
-    stats->log_sv = (double *)malloc(sizeof(double) * n);
-    stats->gaps = (double *)malloc(sizeof(double) * (n - 1));
-    stats->cumulative_var = (double *)malloc(sizeof(double) * n);
-    stats->second_diff = (double *)malloc(sizeof(double) * n);
-    if (!stats->singular_values || !stats->log_sv || !stats->gaps || !stats->cumulative_var || !stats->second_diff)
-    {
-        ssa_opt_component_stats_free(stats);
-        return -1;
-    }
-    for (int i = 0; i < n; i++)
-    {
-        stats->singular_values[i] = ssa->sigma[i];
-        stats->log_sv[i] = log(ssa->sigma[i] + 1e-300);
-    }
-    double max_gap = 0.0;
-    int max_gap_idx = 0;
-    for (int i = 0; i < n - 1; i++)
-    {
-        double gap = ssa->sigma[i] / (ssa->sigma[i + 1] + 1e-300);
-        stats->gaps[i] = gap;
-        if (gap > max_gap)
-        {
-            max_gap = gap;
-            max_gap_idx = i;
+    stats->singular_values = arena;
+    stats->log_sv = arena + n;
+    stats->cumulative_var = arena + 2 * n;
+    stats->second_diff = arena + 3 * n;
+    stats->gaps = arena + 4 * n;
+    const double *sv = ssa->sigma;
+    double held = 0.0;
+    int widest = 0;
+    for (int i = 0; i < n; i++) {
+        stats->singular_values[i] = sv[i];
+        stats->log_sv[i] = log(sv[i] + 1e-300);
+        held += ssa->eigenvalues[i];
+        stats->cumulative_var[i] = held / ssa->total_variance;
+        if (i + 1 < n) {
+            stats->gaps[i] = sv[i] / (sv[i + 1] + 1e-300);
+            if (stats->gaps[i] > stats->gaps[widest])
+                widest = i;
         }
     }
-    double cumsum = 0.0;
-    for (int i = 0; i < n; i++)
-    {
-        cumsum += ssa->eigenvalues[i];
-        stats->cumulative_var[i] = cumsum / ssa->total_variance;
+    for (int i = 0; i < n; i++) {
+        const int interior = i > 0 && i < n - 1;
+        stats->second_diff[i] =
+            interior ? (stats->log_sv[i - 1] + stats->log_sv[i + 1]) - 2.0 * stats->log_sv[i] : 0.0;
     }
-    stats->second_diff[0] = 0.0;
-    stats->second_diff[n - 1] = 0.0;
-    for (int i = 1; i < n - 1; i++)
-        stats->second_diff[i] = stats->log_sv[i - 1] - 2.0 * stats->log_sv[i] + stats->log_sv[i + 1];
-    stats->suggested_signal = max_gap_idx + 1;
-    stats->gap_threshold = max_gap;
+    stats->suggested_signal = widest + 1;
+    stats->gap_threshold = stats->gaps[widest];
     return 0;
 }
 
@@ -837,12 +834,8 @@ void ssa_opt_component_stats_free(SSA_ComponentStats *stats)
 {
     if (!stats)
         return;
-    free(stats->singular_values);
-    free(stats->log_sv);
-    free(stats->gaps);
-    free(stats->cumulative_var);
-    free(stats->second_diff);
-    memset(stats, 0, sizeof(SSA_ComponentStats));
+    free(stats->singular_values); /* the one allocation behind all five arrays */
+    memset(stats, 0, sizeof(*stats));
 }
 
 int ssa_opt_find_periodic_pairs(const SSA_Opt *ssa, int *pairs, int max_pairs, ssa_real sv_tol,
@@ -1365,6 +1358,8 @@ static int matvec_dev(SSA_Opt *ssa, const double *in, double *out, int adjoint)
 
 int ssa_opt_hankel_matvec_dev(SSA_Opt *ssa, const double *v, double *y) { return matvec_dev(ssa, v, y, 0); }
 int ssa_opt_hankel_matvec_T_dev(SSA_Opt *ssa, const double *u, double *z) { return matvec_dev(ssa, u, z, 1); }
+void ssa_opt_hankel_matvec(SSA_Opt *ssa, const double *v, double *y) { (void)matvec_dev(ssa, v, y, 0); }
+void ssa_opt_hankel_matvec_T(SSA_Opt *ssa, const double *u, double *z) { (void)matvec_dev(ssa, u, z, 1); }
 
 int ssa_opt_copy_factors(const SSA_Opt *ssa, double *U, double *V)
 {

@@ -39,6 +39,15 @@ class _SSA_LRF(ctypes.Structure):
     _fields_ = [("R", c_double_p), ("L", ctypes.c_int), ("verticality", ctypes.c_double), ("valid", ctypes.c_bool)]
 
 
+class _ComponentStats(ctypes.Structure):
+    """SSA_ComponentStats (MKL/ssa_opt.h:228-248)."""
+    _fields_ = [("n", ctypes.c_int), ("singular_values", ctypes.POINTER(ctypes.c_double)),
+                ("log_sv", ctypes.POINTER(ctypes.c_double)), ("gaps", ctypes.POINTER(ctypes.c_double)),
+                ("cumulative_var", ctypes.POINTER(ctypes.c_double)),
+                ("second_diff", ctypes.POINTER(ctypes.c_double)), ("suggested_signal", ctypes.c_int),
+                ("gap_threshold", ctypes.c_double)]
+
+
 class _SSA_CadzowResult(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("final_diff", ctypes.c_double), ("converged", ctypes.c_double)]
 
@@ -84,6 +93,8 @@ _sig("ssa_opt_wcorr_matrix", _I, _P, c_double_p)
 _sig("ssa_opt_wcorr_pair", _D, _P, _I, _I)
 _sig("ssa_opt_variance_explained", _D, _P, _I, _I)
 _sig("ssa_opt_find_periodic_pairs", _I, _P, c_int_p, _I, _D, _D)
+_sig("ssa_opt_component_stats", _I, _P, ctypes.POINTER(_ComponentStats))
+_sig("ssa_opt_component_stats_free", _V, ctypes.POINTER(_ComponentStats))
 _sig("ssa_opt_get_trend", _I, _P, c_double_p)
 _sig("ssa_opt_get_noise", _I, _P, _I, c_double_p)
 _sig("ssa_opt_get_singular_values", _I, _P, c_double_p, _I)
@@ -504,6 +515,25 @@ class SSA:
     def variance_explained(self, start: int = 0, end: int = -1) -> float:
         self._need()
         return _lib.ssa_opt_variance_explained(ctypes.byref(self._ctx), start, end)
+
+    def component_stats(self) -> dict:
+        """ssa_opt_component_stats: sigma, log sigma, neighbour drop ratios, cumulative variance,
+        log-spectrum curvature, suggested signal rank and its drop ratio."""
+        self._need()
+        st = _ComponentStats()
+        if _lib.ssa_opt_component_stats(ctypes.byref(self._ctx), ctypes.byref(st)) != 0:
+            raise RuntimeError("component_stats failed")
+        n = st.n
+        try:
+            out = {"singular_values": np.ctypeslib.as_array(st.singular_values, (n,)).copy(),
+                   "log_sv": np.ctypeslib.as_array(st.log_sv, (n,)).copy(),
+                   "gaps": np.ctypeslib.as_array(st.gaps, (n - 1,)).copy(),
+                   "cumulative_var": np.ctypeslib.as_array(st.cumulative_var, (n,)).copy(),
+                   "second_diff": np.ctypeslib.as_array(st.second_diff, (n,)).copy(),
+                   "suggested_signal": int(st.suggested_signal), "gap_threshold": float(st.gap_threshold)}
+        finally:
+            _lib.ssa_opt_component_stats_free(ctypes.byref(st))
+        return out
 
     def find_periodic_pairs(self, max_pairs: int = 10, sv_tol: float = 0.1,
                             wcorr_thresh: float = 0.5) -> List[Tuple[int, int]]:
