@@ -244,9 +244,11 @@ int ssa_batch_profile(ssa_batch *b, double *ms, long long *launches, int nkinds)
  * that loads the library holds until the process exits. Limits: N <= 8192 and k <= 32
  * (larger sizes return -2 without touching the GPU); ldU and ldV even and U, V 8-byte aligned.
  * The work is enqueued on `stream` (a cudaStream_t, NULL for the default stream) and the call
- * returns without waiting. The first call on a device also performs that device's one-time
- * set-up (twiddle table upload and the lookup of the scratch array's device address), so make
- * the first call on each device before any stream capture. All calls on a device share the
+ * returns without waiting (its job tables travel as kernel parameters). The first call on a
+ * device also performs that device's one-time set-up (the library's twiddle table upload, if no
+ * other entry point did it yet, and the lookup of the scratch array's device address), so make
+ * the first call on each device before any stream capture. That set-up is kept for the process:
+ * calls must not span a cudaDeviceReset of the device. All calls on a device share the
  * scratch array, which keeps the previous call's contents: calls that may overlap on the GPU
  * (different streams without ordering between them) race and must be serialised by the
  * caller. Returns 0, -1 (invalid argument or CUDA error) or -2 (size beyond the limits). */

@@ -24,6 +24,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 #include <vector>
 
 using namespace ssa;
@@ -1535,7 +1536,12 @@ extern "C" int ssad_init_device(void) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return (int)e;
+    // one upload per device and process; the lock keeps two threads that make their first call
+    // on the same device at once from uploading twice (the second would rewrite the tables while
+    // the first one's kernels may already read them)
+    static std::mutex mu;
     static bool done[64] = {false};
+    std::lock_guard<std::mutex> lock(mu);
     if (dev < 64 && done[dev]) return 0;
     std::vector<float2> tw(SSA_TW_N);
     for (int t = 0; t < SSA_TW_N; ++t) {
@@ -1857,39 +1863,43 @@ extern "C" int ssad_gaussian(float* out, long long ld, int rows, int ncols, int 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[SSA_NOALLOC_BYTES];
 
 #include <cstring>
-#include <mutex>
+
+// The three job tables sit in 256-byte slots at the start of the scratch array.
+static_assert(sizeof(ssa_col_job) <= 256, "ssa_col_job must fit its 256-byte scratch slot");
+static_assert(sizeof(ssa_gram_job) <= 256, "ssa_gram_job must fit its 256-byte scratch slot");
+static_assert(512 + sizeof(ssa_wfin_job) <= SSA_NOALLOC_JOB_BYTES, "ssa_wfin_job must fit the job area");
 
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_ptr[64];
 static bool g_noalloc_ready[64];
-static float2 g_noalloc_tw_host[SSA_TW_N];  // FP64-computed twiddles, filled once per process
 
-// Per-device set-up, run by the first call on a device with that device current: upload the
-// twiddle table from static host storage and look up the device address of the scratch array
-// (host code must not pass the symbol itself to a kernel: on the host it is only a stand-in).
+// Per-device set-up, run by the first call on a device with that device current: the library's
+// own one-time device initialisation (twiddle tables, shared with every other entry point and
+// done once per device), then the lookup of the scratch array's device address (host code must
+// not pass the symbol itself to a kernel: on the host it is only a stand-in).
 static int noalloc_setup(int dev, void** scratch) {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (g_noalloc_ready[dev]) {
         *scratch = g_noalloc_ptr[dev];
         return 0;
     }
-    static bool tw_filled = false;
-    if (!tw_filled) {
-        for (int t = 0; t < SSA_TW_N; ++t) {
-            const double a = -2.0 * M_PI * (double)t / (double)SSA_TW_N;
-            g_noalloc_tw_host[t] = make_float2((float)cos(a), (float)sin(a));
-        }
-        tw_filled = true;
-    }
-    cudaError_t e = cudaMemcpyToSymbol(g_tw, g_noalloc_tw_host, sizeof(g_noalloc_tw_host));
-    if (e != cudaSuccess) return -1;
+    if (ssad_init_device() != 0) return -1;
     void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || p == nullptr) return -1;
     g_noalloc_ptr[dev] = p;
     g_noalloc_ready[dev] = true;
     *scratch = p;
     return 0;
+}
+
+// Stores the three job tables into their scratch slots. They travel as kernel parameters, which
+// the launch copies, so the call neither stages host memory nor waits on the stream.
+__global__ void k_noalloc_jobs(ssa_col_job je, ssa_gram_job jg, ssa_wfin_job jw, ssa_col_job* de,
+                               ssa_gram_job* dg, ssa_wfin_job* dw) {
+    *de = je;
+    *dg = jg;
+    *dw = jw;
 }
 
 extern "C" __attribute__((visibility("default"))) int ssa_wcorr_noalloc(
@@ -1949,10 +1959,8 @@ extern "C" __attribute__((visibility("default"))) int ssa_wcorr_noalloc(
     jw.W = d_W;
     jw.nchunks = nch;
     jw.k = k;
-    if (cudaMemcpyAsync(d_elem, &je, sizeof(je), cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemcpyAsync(d_gram, &jg, sizeof(jg), cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemcpyAsync(d_wfin, &jw, sizeof(jw), cudaMemcpyHostToDevice, st) != cudaSuccess)
-        return -1;
+    k_noalloc_jobs<<<1, 1, 0, st>>>(je, jg, jw, d_elem, d_gram, d_wfin);
+    if (launched(cudaGetLastError()) != 0) return -1;
     if (ssad_elem_recon(d_elem, 1, k, ssad_logh_for(N), st) != 0) return -1;
     if (ssad_gram(d_gram, 1, nch, 1, st) != 0) return -1;
     if (ssad_wfin(d_wfin, 1, st) != 0) return -1;

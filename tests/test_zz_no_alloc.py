@@ -3,10 +3,12 @@
 It serves callers that cannot have device memory allocated for them (an application whose
 device memory is owned by another framework's allocator, or a loop that cannot afford the
 synchronisation of cudaMalloc). The test calls it through the C ABI with device inputs the test
-owns, twice in a row on two different decompositions, and checks each result against the
-W-correlation of the same decomposition from the existing entry point ssa_opt_wcorr_matrix,
-within the W-correlation tolerance of the parity tests. This file is collected last so that a
-failure here leaves every other test already run.
+owns, twice in a row on two different decompositions, on a stream of the caller's, and checks
+each result against the W-correlation of the same decomposition from the existing entry point
+ssa_opt_wcorr_matrix, within the W-correlation tolerance of the parity tests; after the first
+calls (which do the device's one-time set-up) a second round of calls must leave the device's
+free memory unchanged. This file is collected last so that a failure here leaves every other
+test already run.
 """
 import ctypes
 
@@ -52,24 +54,53 @@ def _colmajor(A):
     return t.cuda()
 
 
-def test_noalloc_matches_existing_entry_point_twice(gpu, oracle):
+def _calls(gpu, cases, prepared, stream):
+    """One call per case, back to back on `stream`; returns [(W_ref, device W)]."""
     import torch
 
-    cases = [(11, 4000, 1000, 20), (12, 6000, 1500, 24)]
-    prepared = [_reference_and_inputs(gpu, oracle, *c) for c in cases]
     outs = []
     for (seed, N, L, k), (W_ref, dU, dV, dS) in zip(cases, prepared):
         dW = torch.full((k, k), float("nan"), dtype=torch.float64, device="cuda")
         rc = gpu._lib.ssa_wcorr_noalloc(dU.data_ptr(), dU.shape[1], dV.data_ptr(), dV.shape[1], dS.data_ptr(),
-                                        N, L, k, dW.data_ptr(), None)
+                                        N, L, k, dW.data_ptr(), ctypes.c_void_p(stream.cuda_stream))
         assert rc == 0
         outs.append((W_ref, dW))
-    torch.cuda.synchronize()
+    return outs
+
+
+def _check(outs):
     for W_ref, dW in outs:
         W = dW.cpu().numpy()
         assert np.all(np.isfinite(W))
         assert np.max(np.abs(W - W_ref)) <= W_TOL
         assert np.max(np.abs(np.diag(W) - 1.0)) < 1e-6
+
+
+def test_noalloc_matches_existing_entry_point_twice(gpu, oracle):
+    import torch
+
+    cases = [(11, 4000, 1000, 20), (12, 6000, 1500, 24)]
+    prepared = [_reference_and_inputs(gpu, oracle, *c) for c in cases]
+    stream = torch.cuda.Stream()
+    # the inputs were written on torch's current stream: order the caller's stream after them
+    stream.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(stream):
+        first = _calls(gpu, cases, prepared, stream)
+    stream.synchronize()
+    _check(first)
+    # the first calls did the device's set-up; further calls allocate nothing: the device's free
+    # memory is unchanged (output buffers are made before the measurement)
+    outs = [torch.full((k, k), float("nan"), dtype=torch.float64, device="cuda") for (_, _, _, k) in cases]
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for (seed, N, L, k), (W_ref, dU, dV, dS), dW in zip(cases, prepared, outs):
+        rc = gpu._lib.ssa_wcorr_noalloc(dU.data_ptr(), dU.shape[1], dV.data_ptr(), dV.shape[1], dS.data_ptr(),
+                                        N, L, k, dW.data_ptr(), ctypes.c_void_p(stream.cuda_stream))
+        assert rc == 0
+    stream.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free1 >= free0, (free0, free1)
+    _check([(p[0], dW) for p, dW in zip(prepared, outs)])
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(gpu):
