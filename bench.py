@@ -161,81 +161,140 @@ def corr_bytes(N: int, L: int, k: int, p: int, q: int) -> int:
 
 
 # ------------------------------------------------------------------------------------------
-# CPU reference leg (rank 0 only): MKL/ssa_opt_ref.h compiled from the reference (oracle/_ref)
-# when present, else the NumPy FP64 port of the reference algorithm.
+# CPU reference leg (rank 0 only): the reference's own MKL/ssa_opt.h, compiled unmodified against
+# the MKL-compatibility shim (oracle/_ref/libssa_mklshim.so: CBLAS/LAPACKE from OpenBLAS, own
+# FFT for DFTI), when present; else the NumPy FP64 port of the same algorithm.
 # ------------------------------------------------------------------------------------------
 
+_MKR = None
+
+
+def _mkr():
+    global _MKR
+    if _MKR is None:
+        import ctypes
+        lib = ctypes.CDLL(str(ORACLE / "_ref" / "libssa_mklshim.so"))
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        c_int = ctypes.c_int
+        lib.mkr_pipeline.argtypes = [dp, c_int, c_int, c_int, c_int, ip, ip, c_int, dp, c_int, dp, ip, c_int,
+                                     c_int, dp, dp, dp, dp]
+        lib.mkr_forecast_resident.argtypes = [dp, c_int, c_int, c_int, c_int, ip, c_int, c_int, dp, dp]
+        _MKR = (lib, dp, ip)
+    return _MKR
+
+
 def _ref_worker(args):
-    x, L, k, p = args
+    """One stream request through the reference's call sequence (the Python wrapper's: init ->
+    prepare(k, p) -> decompose_randomized(k, p) -> reconstruct [0], [1, 2] | wcorr_matrix; a
+    forecast request: ssa_opt_forecast([0, 1, 2], 50) on an already decomposed context, timed
+    alone). Returns the request's seconds."""
     import ctypes
-    so = ORACLE / "_ref" / "libssa_ref.so"
-    lib = ctypes.CDLL(str(so))
-    dp = ctypes.POINTER(ctypes.c_double)
-    ip = ctypes.POINTER(ctypes.c_int)
-    lib.refdrv_default_state.restype = ctypes.c_uint64
-    lib.refdrv_pipeline.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
-                                    ip, ip, ctypes.c_int, dp, dp, dp]
+    t, x, L, k, p = args
+    lib, dp, ip = _mkr()
     N = len(x)
     x = np.ascontiguousarray(x, dtype=np.float64)
-    groups = np.array([0, 1, 2], dtype=np.int32)
+    D = lambda a: a.ctypes.data_as(dp)  # noqa: E731
+    I = lambda a: a.ctypes.data_as(ip)  # noqa: E731
+    g3 = np.array([0, 1, 2], dtype=np.int32)
+    if t == FORECAST:
+        fc = np.zeros(50)
+        sec = ctypes.c_double(0.0)
+        lib.mkr_forecast_resident(D(x), N, L, k, p, I(g3), 3, 50, D(fc), ctypes.byref(sec))
+        return sec.value
     sizes = np.array([1, 2], dtype=np.int32)
     sig = np.zeros(k)
-    rec = np.zeros(2 * N)
-    W = np.zeros(k * k)
     t0 = time.perf_counter()
-    lib.refdrv_pipeline(x.ctypes.data_as(dp), N, L, k, p, lib.refdrv_default_state(), groups.ctypes.data_as(ip),
-                        sizes.ctypes.data_as(ip), 2, sig.ctypes.data_as(dp), rec.ctypes.data_as(dp),
-                        W.ctypes.data_as(dp))
+    if t == RECON:
+        rec = np.zeros(2 * N)
+        lib.mkr_pipeline(D(x), N, L, k, p, I(g3), I(sizes), 2, D(rec), 0, None, None, 0, 0, None, None, None, D(sig))
+    else:
+        W = np.zeros(k * k)
+        lib.mkr_pipeline(D(x), N, L, k, p, None, None, 0, None, 1, D(W), None, 0, 0, None, None, None, D(sig))
     return time.perf_counter() - t0
 
 
 def _port_worker(args):
-    x, L, k, p, q = args
+    t, x, L, k, p = args
     import ssa_oracle as O
     N = len(x)
     rng = np.random.default_rng(0)
-    t0 = time.perf_counter()
     Om = O.gaussian_omega(rng, N - L + 1, min(k + p, L, N - L + 1))
-    d = O.decompose_randomized(x, L, k, p, Om, q=q)
-    O.reconstruct(d, [0], N, L)
-    O.reconstruct(d, [1, 2], N, L)
-    O.wcorr_matrix(d, N, L)
+    d = O.decompose_randomized(x, L, k, p, Om, q=0)
+    t0 = time.perf_counter()
+    if t == FORECAST:
+        O.forecast(d, [0, 1, 2], 50, N, L)
+        return time.perf_counter() - t0
+    if t == RECON:
+        O.reconstruct(d, [0], N, L)
+        O.reconstruct(d, [1, 2], N, L)
+    else:
+        O.wcorr_matrix(d, N, L)
     return time.perf_counter() - t0
 
 
+def _spread_order(n: int) -> list:
+    """0..n-1 in bit-reversed (van der Corput) order: every prefix is spread evenly over the
+    range, so a time-bounded prefix of requests sorted by N samples the stream's N quantiles."""
+    bits = max(1, (n - 1).bit_length())
+    out = []
+    for i in range(1 << bits):
+        r = int(format(i, f"0{bits}b")[::-1], 2)
+        if r < n:
+            out.append(r)
+    return out
+
+
 def cpu_reference(a, budget_s: float = 20.0) -> dict:
-    """Time the reference CPU path on a bounded sample of the stream's decompositions: one series
-    per process on every host core, as many series as fit the budget. Forecast requests are
-    counted at no cost, so requests/s = decompositions/s / 0.7 (the stream's decomposition
-    share). Returns {"value", "unit", "cores", "kind", "sample"}."""
+    """Time the reference CPU path on a bounded sample of the stream's requests: one request per
+    process on every host core (each process single-threaded, OpenBLAS included), requests taken
+    in an order that spreads over the stream's sorted N, as many as fit the budget. Forecast
+    requests are timed as the forecast call on a resident (already decomposed) series.
+    Returns {"value", "unit", "cores", "kind", "sample"}."""
     cores = len(os.sched_getaffinity(0))
-    use_ref = (ORACLE / "_ref" / "libssa_ref.so").exists()
-    rng = np.random.default_rng(a.seed + 1000)
+    use_ref = (ORACLE / "_ref" / "libssa_mklshim.so").exists()
+    specs = make_stream(a.requests, a.seed, a.nmin, a.nmax)
+    reqs = []
+    for t, x, L, k, tgt in specs:
+        if t == FORECAST:
+            _, x, L, k, _ = specs[tgt]
+        reqs.append((t, x, L, k))
+    order = sorted(range(len(reqs)), key=lambda i: len(reqs[i][1]))
+    pick = [order[i] for i in _spread_order(len(order))]
     ctx = mp.get_context("spawn")
-    done = 0
-    nsum = 0
+    done, busy, nsum = 0, 0.0, 0
+    worker = _ref_worker if use_ref else _port_worker
     with ctx.Pool(cores, initializer=_pin_blas) as pool:
+        pool.map(_pin_blas, range(cores))  # workers started before the clock
         t0 = time.perf_counter()
-        while True:
-            batch = [make_series(rng, a.nmin, a.nmax) for _ in range(cores)]
-            if use_ref:
-                pool.map(_ref_worker, [(x, L, k, a.p) for x, L, k in batch])
-            else:
-                pool.map(_port_worker, [(x, L, k, a.p, a.q) for x, L, k in batch])
+        pos = 0
+        while pos < len(pick):
+            batch = [reqs[i] for i in pick[pos:pos + cores]]
+            pos += len(batch)
+            secs = pool.map(worker, [(t, x, L, k, a.p) for t, x, L, k in batch])
+            busy += sum(secs)
             done += len(batch)
-            nsum += sum(len(b[0]) for b in batch)
+            nsum += sum(len(b[1]) for b in batch)
             if time.perf_counter() - t0 >= budget_s:
                 break
-        el = time.perf_counter() - t0
+        wall = time.perf_counter() - t0
+    # requests/s with every core busy: cores / mean seconds per request (the wall-clock rate of the
+    # batches, which wait for their slowest request, is reported beside it)
+    value = cores * done / busy if busy > 0 else 0.0
     kind = "reference" if use_ref else "port"
-    what = ("MKL/ssa_opt_ref.h (reference pure-C path: randomized SVD q=0, reconstruct [0],[1,2], W-corr)"
-            if use_ref else "NumPy FP64 port of MKL/ssa_opt.h randomized SVD, reconstruct, W-corr")
-    return {"value": done / el / 0.7, "unit": "SSA/s", "cores": cores, "kind": kind,
-            "sample": f"{done} stream decompositions (mean N {nsum / max(done, 1):.0f}) in {el:.1f} s, one per "
-                      f"process on {cores} cores, forecasts counted at no cost; {what}"}
+    what = ("the reference's MKL/ssa_opt.h compiled unmodified against an MKL-compatibility shim (OpenBLAS "
+            "CBLAS/LAPACKE, own power-of-two real FFT for DFTI; no MKL on this host): randomized SVD with the "
+            "reference's q = 0, uncached reconstructions [0],[1,2], ssa_opt_wcorr_matrix, ssa_opt_forecast"
+            if use_ref else "NumPy FP64 port of MKL/ssa_opt.h randomized SVD (q = 0), reconstruct, W-corr, forecast")
+    mean_stream = float(np.mean([len(r[1]) for r in reqs]))
+    return {"value": value, "unit": "SSA/s", "cores": cores, "kind": kind,
+            "sample": f"{done} of the stream's {len(reqs)} requests (mean N {nsum / max(done, 1):.0f}, stream mean "
+                      f"{mean_stream:.0f}; taken spread over the stream's N quantiles) in {busy:.1f} core-seconds, one "
+                      f"single-threaded process per core on {cores} cores (wall-clock rate of the batches "
+                      f"{done / wall:.1f}/s); {what}"}
 
 
-def _pin_blas():
+def _pin_blas(*_):
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
     os.environ["OMP_NUM_THREADS"] = "1"
 

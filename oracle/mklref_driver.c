@@ -315,6 +315,30 @@ done:
     return rc;
 }
 
+/* An R-forecast request on a resident series, timed: the decomposition (init, prepare,
+ * decompose_randomized) is made first and not timed, then ssa_opt_forecast(fgroup, h) is timed
+ * with the monotonic clock (MKL/ssa_opt.h:2843-2867: reconstruct the group, LRF, recurrence).
+ * *seconds receives the forecast's time. Returns 0 or -1. */
+#include <time.h>
+MKR_EXPORT int mkr_forecast_resident(const double *x, int N, int L, int k, int p, const int *fgroup,
+                                     int nf, int h, double *fc, double *seconds)
+{
+    SSA_Opt s;
+    if (ssa_opt_init(&s, x, N, L) != 0)
+        return -1;
+    int rc = -1;
+    if (ssa_opt_prepare(&s, k, p) == 0 && ssa_opt_decompose_randomized(&s, k, p) == 0) {
+        struct timespec t0, t1;
+        clock_gettime(CLOCK_MONOTONIC, &t0);
+        rc = ssa_opt_forecast(&s, fgroup, nf, h, fc);
+        clock_gettime(CLOCK_MONOTONIC, &t1);
+        if (seconds)
+            *seconds = (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
+    }
+    ssa_opt_free(&s);
+    return rc;
+}
+
 /* FFT length and batch size the reference picks for (N, L) (MKL/ssa_opt.h:1047-1092). */
 MKR_EXPORT int mkr_dims(const double *x, int N, int L, int *fft_len, int *batch_size)
 {
