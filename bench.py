@@ -30,6 +30,11 @@ import threading
 import time
 from pathlib import Path
 
+if mp.current_process().name != "MainProcess":
+    # pool workers (CPU baseline, accuracy checks): one BLAS thread each, set before numpy loads it
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    os.environ["OMP_NUM_THREADS"] = "1"
+
 import numpy as np
 
 # one hardware work queue per stream for the bucket streams of the batches in flight (the
@@ -67,6 +72,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-uniform", action="store_true")
     ap.add_argument("--no-rates", action="store_true")
+    ap.add_argument("--accuracy", type=int, default=64, help="series of the timed batch checked against the FP64 "
+                                                              "oracle after the run (0: none)")
     return ap.parse_args()
 
 
@@ -300,6 +307,98 @@ def _pin_blas(*_):
 
 
 # ------------------------------------------------------------------------------------------
+# accuracy of the timed outputs against the FP64 oracle (CPU, spawn pool; after the timed region)
+# ------------------------------------------------------------------------------------------
+
+DENSE_MAX_N = 6000  # exact dense SVD of the trajectory matrix below this length (seconds each)
+
+
+def _rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _accuracy_worker(args):
+    """Errors of one series' GPU outputs against the FP64 restatement of the same algorithm with
+    the same device-generated test matrix (and against the exact dense SVD for short series)."""
+    import ssa_oracle as O
+    from scipy.linalg import subspace_angles
+    x, L, k, p, q, seed_s, g = args
+    N = len(x)
+    K = N - L + 1
+    kk, kp = O.clamp_kp(L, K, k, p)
+    d = O.decompose_randomized(x, L, kk, p, O.device_gaussian(seed_s, K, kp), q=q)
+    sg = g["sigma"]
+    rel = np.abs(sg - d.sigma) / d.sigma
+    lead = min(3, kk)
+    out = {"N": N, "k": kk, "sigma_rel_max": float(rel.max()), "sigma_rel_lead": float(rel[:lead].max()),
+           "angle_lead": float(np.max(subspace_angles(g["U"][:, :lead], d.U[:, :lead]))),
+           "angle_k": float(np.max(subspace_angles(g["U"], d.U)))}
+    recs = []
+    for gi, grp in enumerate(([0], [1, 2])):
+        if max(grp) < kk:
+            recs.append(_rel_l2(g["groups"][gi], O.reconstruct(d, grp, N, L)))
+    out["recon_rel"] = max(recs) if recs else 0.0
+    if g.get("W") is not None:
+        out["W_abs"] = float(np.max(np.abs(g["W"] - O.wcorr_matrix(d, N, L))))
+    if N <= DENSE_MAX_N:
+        t = O.dense_svd(x, L, kk)
+        out["dense_sigma_rel_lead"] = float(np.max(np.abs(sg[:lead] - t.sigma[:lead]) / t.sigma[:lead]))
+        out["dense_angle_lead"] = float(np.max(subspace_angles(g["U"][:, :lead], t.U[:, :lead])))
+        if lead == 3:
+            out["dense_recon_rel"] = max(_rel_l2(g["groups"][0], O.reconstruct(t, [0], N, L)),
+                                         _rel_l2(g["groups"][1], O.reconstruct(t, [1, 2], N, L)))
+    return out
+
+
+def _forecast_worker(args):
+    import ssa_oracle as O
+    x, L, k, p, q, seed_s, fc = args
+    N = len(x)
+    K = N - L + 1
+    kk, kp = O.clamp_kp(L, K, k, p)
+    d = O.decompose_randomized(x, L, kk, p, O.device_gaussian(seed_s, K, kp), q=q)
+    ref = O.forecast(d, [0, 1, 2], len(fc), N, L)
+    return {"rmse": float(np.sqrt(np.mean((fc - ref) ** 2))),
+            "rel": float(np.sqrt(np.mean((fc - ref) ** 2)) / max(np.sqrt(np.mean(ref ** 2)), 1e-300))}
+
+
+def stratified_sample(Ns, n: int, fft_length) -> list:
+    """n series indices spread over the FFT-length buckets: every bucket contributes in
+    proportion to its series count, at least two where it has them."""
+    by = {}
+    for i, N in enumerate(Ns):
+        by.setdefault(fft_length(N), []).append(i)
+    keys = sorted(by)
+    take = {b: min(len(by[b]), max(2, round(n * len(by[b]) / len(Ns)))) for b in keys}
+    out = []
+    for b in keys:
+        idx = by[b]
+        step = len(idx) / take[b]
+        out += [idx[int(j * step)] for j in range(take[b])]
+    return sorted(out)
+
+
+def summarize_accuracy(rows: list, fcs: list) -> dict:
+    def agg(key):
+        v = np.array([r[key] for r in rows if key in r])
+        return {"max": float(v.max()), "p99": float(np.percentile(v, 99)), "n": int(v.size)} if v.size else None
+    out = {"series": len(rows), "what": "GPU outputs of the timed batch (and of the server run for forecasts) against "
+                                         "the FP64 restatement of the same algorithm with the same device test matrix "
+                                         "(q as timed); dense_* against the exact dense SVD of the trajectory matrix "
+                                         f"for N <= {DENSE_MAX_N}; angles in radians"}
+    for key in ("sigma_rel_lead", "sigma_rel_max", "recon_rel", "W_abs", "angle_lead", "angle_k",
+                "dense_sigma_rel_lead", "dense_angle_lead", "dense_recon_rel"):
+        a = agg(key)
+        if a:
+            out[key] = a
+    if fcs:
+        out["forecast_rmse_rel"] = {"max": max(f["rel"] for f in fcs), "p99": float(np.percentile([f["rel"] for f in fcs], 99)),
+                                    "n": len(fcs), "what": "RMSE of 50-step R-forecasts of group [0,1,2] / RMS of the oracle's"}
+        out["forecast_rmse"] = {"max": max(f["rmse"] for f in fcs)}
+    return out
+
+
+# ------------------------------------------------------------------------------------------
 # clocks sampling during the timed region
 # ------------------------------------------------------------------------------------------
 
@@ -393,6 +492,15 @@ def device_steps(gpu, torch, a, rank: int, world: int) -> dict:
     launches = gpu.kernel_launches() - launches0
     step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(a.steps)]
     total_ms = ev[0].elapsed_time(ev[a.steps])
+    # outputs of the last timed step for a stratified sample (checked on the CPU at the end)
+    acc_jobs = []
+    if rank == 0 and a.accuracy > 0:
+        import ssa_oracle
+        last_seed = a.steps - 1
+        for i in stratified_sample(Ns, a.accuracy, gpu.fft_length):
+            r = rb.series_result(i, Ns[i], Ls[i], ks[i], factors=True)
+            g = {"sigma": r["sigma"], "groups": r["groups"], "U": r["U"], "W": r["W"] if want_w[i] else None}
+            acc_jobs.append((series[i][0], Ls[i], ks[i], a.p, a.q, ssa_oracle.series_seed(last_seed, i), g))
     # one more (untimed) step with the buckets run one after another and every launch bracketed by
     # CUDA events on its stream: isolated per-launch times for the roofline and the kernel shares
     rb.set_profiling(True, serialize=True)
@@ -415,7 +523,7 @@ def device_steps(gpu, torch, a, rank: int, world: int) -> dict:
     tflops = cf / (corr_ms / 1e3) / 1e12 if corr_ms > 0 else 0.0
     tot = max(sum(v[0] for v in prof.values()), 1e-9)
     out = {"value": a.batch * a.steps * world / (total_ms / 1e3), "ms_per_step": total_ms / a.steps,
-           "step_ms": step_ms, "launches": launches,
+           "step_ms": step_ms, "launches": launches, "acc_jobs": acc_jobs,
            "share": {kk: round(v[0] / tot, 4) for kk, v in prof.items() if v[1]},
            "share_what": "per-kernel-kind share of one step with the buckets run one after another",
            "mean_N": float(np.mean(Ns)), "clocks": clk.summary(),
@@ -454,6 +562,13 @@ def server_runs(gpu, torch, a, rank: int, world: int) -> dict:
     ta, td = R.times()
     st = R.statuses()
     el = float(td.max() - ta.min())
+    fc_jobs = []
+    if rank == 0 and a.accuracy > 0:
+        fidx = [i for i, sp in enumerate(specs) if sp[0] == FORECAST and st[i] == 0]
+        for i in fidx[:: max(1, len(fidx) // 32)][:32]:
+            tgt = specs[i][4]
+            _, x, L, k, _ = specs[tgt]
+            fc_jobs.append((x, L, k, a.p, a.q, 2 * 10**7 + tgt, np.array(R.result(i)["forecast"])))
     if world > 1:
         t = torch.tensor([el], device="cuda", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -463,7 +578,7 @@ def server_runs(gpu, torch, a, rank: int, world: int) -> dict:
                    "seconds": el, "server_timed_run": timed,
                    "what": "ssa_server_* C API, page-locked host buffers, the whole stream offered at t=0 (one "
                            "step = the stream): H2D of every signal and D2H of every requested result (sigma, "
-                           "groups [0],[1,2] / W, forecasts) inside the timed region"}}
+                           "groups [0],[1,2] / W, forecasts) inside the timed region"}, "fc_jobs": fc_jobs}
     if rank == 0 and world == 1 and not a.no_rates:
         sweep = {}
         rng = np.random.default_rng(a.seed + 99)
@@ -606,6 +721,12 @@ def main():
         line["uniform_batch"] = uniform_batch(ssa_gpu, torch, a)
     if rank == 0 and world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_reference(a, budget_s=20.0)
+    acc_jobs, fc_jobs = dev.pop("acc_jobs", []), line.pop("fc_jobs", [])
+    if rank == 0 and (acc_jobs or fc_jobs):
+        with mp.get_context("spawn").Pool(min(len(os.sched_getaffinity(0)), 32), initializer=_pin_blas) as pool:
+            rows = pool.map(_accuracy_worker, acc_jobs, chunksize=1)
+            fcs = pool.map(_forecast_worker, fc_jobs, chunksize=1)
+        line["accuracy"] = summarize_accuracy(rows, fcs)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

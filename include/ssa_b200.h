@@ -101,9 +101,10 @@ int ssa_b200_wcorr_tensor_cores(void);
  * power iterations q) through the same pipeline as ssa_batch_*: randomized decomposition with
  * the device generator (series s seeded seed ^ 0x9E3779B97F4A7C15 (s + 1), as in ssa_batch_*),
  * all k[s] elementary reconstructions, W-correlation and group sums. Series are bucketed by FFT
- * length (M = next power of two >= max(N, 32), N <= 131072); each bucket runs one launch per
- * stage on its own stream and the buckets overlap on the device. No counterpart in the
- * reference, whose API takes one series per context.
+ * length (N <= 131072); each bucket runs one launch per
+ * stage on its own stream and the buckets overlap on the device. (M is the FFT length
+ * ssa_b200_fft_length(N): a power of two or one of the mixed lengths 49152 / 98304.) No
+ * counterpart in the reference, whose API takes one series per context.
  *
  * Inputs and outputs are packed in series order: x holds N[s] doubles at sum_{t<s} N[t];
  * sigma k'[s] at sum_{t<s} k'[t]; W k'[s]^2 (row-major) at sum_{t<s} k'[t]^2; groups
@@ -142,6 +143,12 @@ int ssa_rbatch_reserve(ssa_rbatch *b, size_t bytes);
 int ssa_rbatch_layout(const ssa_rbatch *b, size_t *offsets, size_t *totals);
 /* Device pointers of the packed outputs and the stream every run ends on (recon is NULL). */
 int ssa_rbatch_device_results(const ssa_rbatch *b, ssa_batch_results *out);
+/* Outputs of series s of the last run, copied to host arrays after waiting for the run: sigma
+ * (k'), W (k' x k', zero unless computed), groups (n_groups x N), and the factors U (L x k') and
+ * V (K x k', column-major, FP32 on the device, widened). Any pointer may be NULL. Returns k' or
+ * -1. */
+int ssa_rbatch_series_result(ssa_rbatch *b, int s, double *sigma, double *W, double *groups, double *U,
+                             double *V);
 /* on: 0 off, 1 per-kernel CUDA-event times (buckets overlap, so the intervals include other
  * buckets' work), 2 the same with the buckets run one after another (isolated launch times). */
 int ssa_rbatch_set_profiling(ssa_rbatch *b, int on);

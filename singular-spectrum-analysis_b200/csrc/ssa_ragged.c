@@ -1145,6 +1145,66 @@ int ssa_rbatch_layout(const ssa_rbatch *rb, size_t *offsets, size_t *totals)
     return rb->B;
 }
 
+/* Series s of the last run: its bucket entry, or NULL. */
+static const rser *find_series(const ssa_rbatch *rb, int s, const rbucket **bk)
+{
+    for (int g = 0; g < RB_NB; g++)
+    {
+        const rbucket *b = &rb->bk[g];
+        for (int i = 0; i < b->nb; i++)
+            if (b->sd[i].src == s)
+            {
+                *bk = b;
+                return &b->sd[i];
+            }
+    }
+    return NULL;
+}
+
+static int copy_cols_f32(double *dst, const float *src, long long ld, int m, int n, float *tmp)
+{
+    if (cudaMemcpy2D(tmp, sizeof(float) * (size_t)m, src, sizeof(float) * (size_t)ld, sizeof(float) * (size_t)m,
+                     (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -1;
+    for (size_t i = 0; i < (size_t)m * n; i++)
+        dst[i] = (double)tmp[i];
+    return 0;
+}
+
+int ssa_rbatch_series_result(ssa_rbatch *rb, int s, double *sigma, double *W, double *groups, double *U, double *V)
+{
+    if (!rb || s < 0 || s >= rb->B)
+        return -1;
+    const rbucket *b = NULL;
+    const rser *S = find_series(rb, s, &b);
+    if (!S || cudaStreamSynchronize(rb->main) != cudaSuccess)
+        return -1;
+    const int k = S->k;
+    if (sigma && cudaMemcpy(sigma, rb->sigma + S->osig, sizeof(double) * (size_t)k, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -1;
+    if (W && cudaMemcpy(W, rb->W + S->oW, sizeof(double) * (size_t)k * k, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -1;
+    if (groups && rb->n_groups > 0 &&
+        cudaMemcpy(groups, rb->groups + S->ogrp, sizeof(double) * (size_t)rb->n_groups * S->N,
+                   cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -1;
+    if (U || V)
+    {
+        float *tmp = (float *)malloc(sizeof(float) * (size_t)imax(S->L, S->K) * k);
+        if (!tmp)
+            return -1;
+        int rc = 0;
+        if (U)
+            rc |= copy_cols_f32(U, b->Y + S->oY, S->ldL, S->L, k, tmp);
+        if (V)
+            rc |= copy_cols_f32(V, b->Z + S->oZ, S->ldK, S->K, k, tmp);
+        free(tmp);
+        if (rc)
+            return -1;
+    }
+    return k;
+}
+
 int ssa_rbatch_device_results(const ssa_rbatch *rb, ssa_batch_results *out)
 {
     if (!rb || !out)

@@ -893,6 +893,24 @@ class SSARaggedBatch:
             raise RuntimeError("ssa_rbatch_device_results failed")
         return {"sigma": r.sigma, "W": r.W, "groups": r.groups, "status": r.status, "stream": r.stream}
 
+    def series_result(self, s: int, N: int, L: int, k: int, factors: bool = False) -> dict:
+        """Outputs of series s of the last run (waits for it): sigma, W, groups and, with
+        factors=True, U (L x k') and V (K x k')."""
+        ke = int(self.effective_k([N], [L], [k])[0])
+        K = N - L + 1
+        sig, W = np.zeros(ke), np.zeros((ke, ke))
+        G = np.zeros((max(1, len(self.groups)), N))
+        U = np.zeros((ke, L)) if factors else None
+        V = np.zeros((ke, K)) if factors else None
+        n = _lib.ssa_rbatch_series_result(self._h, s, _dp(sig), _dp(W), _dp(G) if self.groups else None,
+                                          _dp(U) if factors else None, _dp(V) if factors else None)
+        if n != ke:
+            raise RuntimeError("ssa_rbatch_series_result failed")
+        out = {"sigma": sig, "W": W, "groups": G[:len(self.groups)]}
+        if factors:
+            out["U"], out["V"] = U.T, V.T
+        return out
+
 
 class _Request(ctypes.Structure):
     _fields_ = [("type", ctypes.c_int), ("series_id", ctypes.c_int), ("N", ctypes.c_int), ("L", ctypes.c_int),
@@ -910,6 +928,8 @@ class _ServerStats(ctypes.Structure):
                [(n, ctypes.c_double) for n in ("host_launch_s", "host_finish_s", "host_launch_max_s")]
 
 
+_sig("ssa_rbatch_series_result", _I, ctypes.c_void_p, _I, c_double_p, c_double_p, c_double_p, c_double_p,
+     c_double_p)
 _sig("ssa_server_create", _I, ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t, _I, _I, _I, _I)
 _sig("ssa_server_destroy", _V, ctypes.c_void_p)
 _sig("ssa_server_submit", _I, ctypes.c_void_p, ctypes.POINTER(_Request))
