@@ -164,29 +164,42 @@ int ssa_rbatch_profile(ssa_rbatch *b, double *ms, long long *launches, int nkind
  * the device generator seeded with the request's `seed`, and compute the reconstructions of
  * groups [0] and [1, 2] and the W-correlation matrix.
  *
- * A SSA_REQ_DECOMPOSE_RECON request leaves its series resident under series_id: the LRF
- * coefficients of the group [0, 1, 2] (MKL/ssa_opt.h:2766-2816) and the last L - 1 values of
- * that group's reconstruction stay in device memory, a quarter of the budget at most (least
- * recently used series evicted first). A SSA_REQ_FORECAST request on a resident series runs the
- * R-forecast recurrence (:2818-2841) for h steps without decomposing again; one that arrives
- * while its series' decomposition is still queued or running waits for it. Requests fail
- * (status -1) on invalid shapes, N > 131072, k + p > 64, a series larger than a batch's share
- * of the budget, a forecast on a series that is not resident, or an LRF whose verticality
- * coefficient is >= 1 (fewer than 3 components also leave nothing to forecast from).
+ * A decomposition request leaves its series resident under series_id: its factors U, V and sigma
+ * (FP32 / FP64), its signal, and the LRF coefficients of the group [0, 1, 2]
+ * (MKL/ssa_opt.h:2766-2816) with the last L - 1 values of that group's reconstruction stay in
+ * device memory, a quarter of the budget at most (least recently used series evicted first).
+ * Follow-up requests on a resident series do not decompose again:
+ *   SSA_REQ_FORECAST      h-step R-forecast (:2818-2867) of `group` (NULL: [0, 1, 2], whose LRF
+ *                         and tail are already resident, so only the recurrence runs);
+ *   SSA_REQ_RECONSTRUCT   reconstruction of `group` (:2325-2400) into out (N values);
+ *   SSA_REQ_CADZOW        with x == NULL: Cadzow iterations (:3165-3290) of rank `rank` on the
+ *                         resident signal, the first projection taken from the resident factors
+ *                         (rank <= k'), the later ones decomposing as the reference does; with x
+ *                         given (and N, L): the same on a new series. Output in out (N values),
+ *                         iterations and final_diff set.
+ * Reconstructions and group forecasts of resident series run in batches of their own (one
+ * launch per stage per FFT-length bucket, elementary reconstructions of the resident factors);
+ * Cadzow requests run one after another on a worker of their own, overlapping the batches. A
+ * follow-up that arrives while its series' decomposition is still queued or running waits for
+ * it. Requests fail (status -1) on invalid shapes, N > 131072, k + p > 64, a series larger than
+ * a batch's share of the budget, a follow-up on a series that is not resident, an empty group,
+ * an LRF whose verticality coefficient is >= 1, or a forecast group with no component below k'.
  * Output pointers may be NULL; they must stay valid until the request completes. */
 enum
 {
     SSA_REQ_DECOMPOSE_RECON = 0, /* outputs: sigma, groups (2 x N: [0] then [1, 2]) */
     SSA_REQ_DECOMPOSE_WCORR = 1, /* outputs: sigma, W (k' x k', row-major) */
-    SSA_REQ_FORECAST = 2         /* outputs: forecast (h values after the series' end) */
+    SSA_REQ_FORECAST = 2,        /* outputs: forecast (h values after the series' end) */
+    SSA_REQ_RECONSTRUCT = 3,     /* outputs: out (N values) */
+    SSA_REQ_CADZOW = 4           /* outputs: out (N values), iterations, final_diff */
 };
 typedef struct
 {
     int type;
-    int series_id;      /* resident key (DECOMPOSE_RECON) or target (FORECAST) */
-    int N, L, k;        /* decompositions */
+    int series_id;      /* resident key (decompositions) or target (follow-ups) */
+    int N, L, k;        /* decompositions (and Cadzow on a new series: N, L) */
     int h;              /* forecast steps (1 .. 4096) */
-    const double *x;    /* decompositions: N input values (host) */
+    const double *x;    /* decompositions: N input values (host); Cadzow: NULL = resident signal */
     uint64_t seed;      /* generator seed of the decomposition */
     double *sigma;      /* k' = min(k, L, N - L + 1) values */
     double *groups;     /* 2 x N */
@@ -198,6 +211,15 @@ typedef struct
     double t_arrival;   /* seconds on ssa_server_now's clock */
     double t_done;
     void *priv;         /* reserved for the server */
+    /* follow-ups and Cadzow */
+    const int *group;   /* component indices (host), n_group of them; NULL: the type's default */
+    int n_group;
+    int rank;           /* Cadzow rank */
+    int max_iter;       /* Cadzow iterations at most */
+    double tol;         /* Cadzow stopping threshold on the relative change */
+    double *out;        /* RECONSTRUCT / CADZOW: N values */
+    int iterations;     /* set by the server (Cadzow) */
+    double final_diff;  /* set by the server (Cadzow) */
 } ssa_request;
 typedef struct
 {
@@ -208,6 +230,8 @@ typedef struct
     size_t resident_bytes, resident_budget, batch_budget;
     double host_launch_s, host_finish_s; /* worker time spent forming / completing batches */
     double host_launch_max_s;            /* longest forming of one batch since the previous read */
+    long long followup_batches, followups; /* reconstruction / group-forecast batches on resident factors */
+    long long cadzow_requests, cadzow_iterations;
 } ssa_server_stats;
 typedef struct ssa_server ssa_server;
 /* hbm_budget_bytes 0: 80 % of the free device memory at creation, device memory taken as batches

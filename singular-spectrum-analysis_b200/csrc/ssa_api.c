@@ -1434,8 +1434,27 @@ static int cadzow_setup(struct ssa_gpu_ctx *g, int rank, double **d_aux, size_t 
     return cudaMemsetAsync(*d_aux, 0, sizeof(double) * aux_doubles, g->e.st) == cudaSuccess ? 0 : -1;
 }
 
+/* The Cadzow loop on x. With y1 given (the rank-`rank` projection of x, e.g. from factors the
+ * caller keeps), that projection counts as the first iteration: its difference to x is measured
+ * and the loop continues from it, so the result equals the plain loop's whenever y1 equals what
+ * the first decomposition would give. */
+static int cadzow_run_from(const double *x, const double *y1, int N, int L, int rank, int max_iter, double tol,
+                           double alpha, double *output, SSA_CadzowResult *result);
+
 static int cadzow_run(const double *x, int N, int L, int rank, int max_iter, double tol, double alpha,
                       double *output, SSA_CadzowResult *result)
+{
+    return cadzow_run_from(x, NULL, N, L, rank, max_iter, tol, alpha, output, result);
+}
+
+int ssab_cadzow_from(const double *x, const double *y1, int N, int L, int rank, int max_iter, double tol,
+                     double *output, SSA_CadzowResult *result)
+{
+    return cadzow_run_from(x, y1, N, L, rank, max_iter, tol, 1.0, output, result);
+}
+
+static int cadzow_run_from(const double *x, const double *y1, int N, int L, int rank, int max_iter, double tol,
+                           double alpha, double *output, SSA_CadzowResult *result)
 {
     if (!x || !output || N < 4 || L < 2 || L > N - 1 || rank < 1 || max_iter < 1)
         return -1;
@@ -1474,17 +1493,29 @@ static int cadzow_run(const double *x, int N, int L, int rank, int max_iter, dou
             rc = -1;
             break;
         }
-        /* every iteration runs in a freshly initialised context in the reference, whose
-         * generator restarts: the same seed each time */
-        int pr = 1;
-        if (randomized)
-            pr = cadzow_project(&ssa, rank, 1, SSA_DEFAULT_SEED, &k);
-        if (pr == 1)
-            pr = cadzow_project(&ssa, rank, 0, SSA_DEFAULT_SEED ^ 0xB10CB10CB10CB10CULL, &k);
-        if (pr != 0)
+        if (iter == 0 && y1)
         {
-            rc = -1;
-            break;
+            /* the given first projection stands in for the first decomposition */
+            if (cudaMemcpyAsync(g->d_out, y1, sizeof(double) * N, cudaMemcpyHostToDevice, e->st) != cudaSuccess)
+            {
+                rc = -1;
+                break;
+            }
+        }
+        else
+        {
+            /* every iteration runs in a freshly initialised context in the reference, whose
+             * generator restarts: the same seed each time */
+            int pr = 1;
+            if (randomized)
+                pr = cadzow_project(&ssa, rank, 1, SSA_DEFAULT_SEED, &k);
+            if (pr == 1)
+                pr = cadzow_project(&ssa, rank, 0, SSA_DEFAULT_SEED ^ 0xB10CB10CB10CB10CULL, &k);
+            if (pr != 0)
+            {
+                rc = -1;
+                break;
+            }
         }
         double h[2];
         if (ssad_diffnorm(g->d_out, e->x64, N, d_aux, e->st) != 0 ||

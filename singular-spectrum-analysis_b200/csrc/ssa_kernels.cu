@@ -405,9 +405,12 @@ __global__ void k_group_sum_ragged(const ssa_rgsum_job* __restrict__ jobs, const
     const int g = blockIdx.y;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= J.N) return;
+    const int* gi = J.gidx ? J.gidx : group_idx + group_off[g];
+    const int gn = J.gidx ? J.gn : group_off[g + 1] - group_off[g];
+    if (J.gidx && g > 0) return;  // a job's own group is its only one
     double acc = 0.0;
-    for (int e = group_off[g]; e < group_off[g + 1]; ++e) {
-        const int i = group_idx[e];
+    for (int e = 0; e < gn; ++e) {
+        const int i = gi[e];
         if (i < 0 || i >= J.k) continue;
         acc += (double)J.recon[(long long)i * J.ld_recon + t];
     }

@@ -280,13 +280,16 @@ int ssad_axpby(const double *a, const double *b, double *out, double alpha, doub
 int ssad_init_device(void);
 int ssad_group_sum(ssa_gsum_job job, void *stream);
 /* Per-series group sums for uneven batches: out[g * N + t] = sum_{i in group g, i < k} recon[i * ld + t]
- * for the series of each job (group index lists shared by all jobs). */
+ * for the series of each job (group index lists shared by all jobs). A job with its own group
+ * (gidx != NULL: gn indices) writes that single group to out[t] and ignores the shared lists. */
 typedef struct
 {
     const float *recon;
     double *out;          /* n_groups x N doubles */
     long long ld_recon;
     int N, k;
+    const int *gidx;      /* device, or NULL */
+    int gn;
 } ssa_rgsum_job;
 int ssad_group_sum_ragged(const ssa_rgsum_job *d_jobs, int njobs, int maxN, const int *group_idx,
                           const int *group_off, int n_groups, void *stream);

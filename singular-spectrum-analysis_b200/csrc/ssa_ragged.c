@@ -54,6 +54,12 @@ typedef struct
     int rows_W, nch_W; /* W-correlation Gram chunks (tensor-core path: longer chunks) */
     int wantW;         /* W-correlation requested for this series */
     int nelem;         /* elementary reconstructions computed: k with W, else those the groups use */
+    /* follow-up runs: the series' resident factors (U ld ldL, V ld ldK, sigma) and its own group
+     * (device indices gx[0..gn), largest index gmax); NULL outside follow-up runs */
+    const float *Ux, *Vx;
+    const double *sx;
+    const int *gx;
+    int gn, gmax;
     size_t oY, oZ, opart, oqsum, oR, oZu, orecon, onorm, ospec;
     size_t ox, osig, oW, ogrp;
 } rser;
@@ -101,6 +107,13 @@ struct ssa_rbatch
     int lrf_slot, n_lrf_group, lrf_gmax;
     int *d_lrf_group;
     int *lrf_status;
+    /* follow-up runs (ssar_run_followup): given factors, per-series groups, no decomposition */
+    int followup;
+    const float *const *fu_U, *const *fu_V;
+    const double *const *fu_sig;
+    const int *fu_goff;
+    int *h_fu_gidx, *d_fu_gidx;
+    size_t c_fu_gidx;
 };
 
 /* The uneven batches run one stream per FFT-length bucket, and the server several batches at
@@ -188,6 +201,10 @@ static void bucket_free(rbucket *b)
 
 void ssa_rbatch_destroy(ssa_rbatch *rb)
 {
+    if (rb && rb->h_fu_gidx)
+        cudaFreeHost(rb->h_fu_gidx);
+    if (rb && rb->d_fu_gidx)
+        cudaFree(rb->d_fu_gidx);
     if (!rb)
         return;
     if (rb->main)
@@ -567,10 +584,10 @@ static int r_elem(rbucket *b, const double *sigma)
         {
             const rser *S = &b->sd[i];
             ssa_col_job *J = &jobs[i];
-            J->in = b->Y + S->oY;
+            J->in = S->Ux ? S->Ux : b->Y + S->oY;
             J->ld_in = S->ldL;
             J->n_in = S->L;
-            J->scale = sigma + S->osig;
+            J->scale = S->sx ? S->sx : sigma + S->osig;
             J->spec = b->Us + S->ospec;
             J->ld_spec = b->ldS;
             J->ncols = S->nelem;
@@ -601,13 +618,13 @@ static int r_elem(rbucket *b, const double *sigma)
     {
         const rser *S = &b->sd[i];
         ssa_col_job *J = &jobs[i];
-        J->in = b->Y + S->oY;
+        J->in = S->Ux ? S->Ux : b->Y + S->oY;
         J->ld_in = S->ldL;
         J->n_in = S->L;
-        J->in2 = b->Z + S->oZ;
+        J->in2 = S->Vx ? S->Vx : b->Z + S->oZ;
         J->ld_in2 = S->ldK;
         J->n_in2 = S->K;
-        J->scale = sigma + S->osig;
+        J->scale = S->sx ? S->sx : sigma + S->osig;
         J->out = b->recon + S->orecon;
         J->ld_out = S->ldN;
         J->norm2 = b->norm2 + S->onorm;
@@ -685,6 +702,8 @@ static int r_gsum(rbucket *b, ssa_rbatch *rb)
         jobs[i].out = rb->groups + S->ogrp;
         jobs[i].N = S->N;
         jobs[i].k = S->nelem; /* covers every grouped component below k */
+        jobs[i].gidx = S->gx;
+        jobs[i].gn = S->gn;
         maxN = imax(maxN, S->N);
     }
     void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_rgsum_job) * b->nb);
@@ -710,14 +729,15 @@ static int r_lrf(rbucket *b, ssa_rbatch *rb)
     {
         const rser *S = &b->sd[i];
         double *dst = rb->cur_lrf[S->src];
-        if (!dst || rb->lrf_gmax >= S->k)
+        const int gmax = S->gx ? S->gmax : rb->lrf_gmax;
+        if (!dst || gmax >= S->k || gmax < 0)
             continue;
         ssa_lrf_job *J = &jobs[n++];
-        J->U = b->Y + S->oY;
+        J->U = S->Ux ? S->Ux : b->Y + S->oY;
         J->ld = S->ldL;
-        J->group = rb->d_lrf_group;
-        J->n_group = rb->n_lrf_group;
-        J->recon = rb->groups + S->ogrp + (size_t)rb->lrf_slot * S->N;
+        J->group = S->gx ? S->gx : rb->d_lrf_group;
+        J->n_group = S->gx ? S->gn : rb->n_lrf_group;
+        J->recon = rb->groups + S->ogrp + (size_t)(S->gx ? 0 : rb->lrf_slot) * S->N;
         J->R = dst;
         J->buf = dst + (S->L - 1);
         J->out = NULL;
@@ -772,6 +792,17 @@ static int bucket_run(rbucket *b, ssa_rbatch *rb, const double *d_x, unsigned lo
     return 0;
 }
 
+/* Follow-up pipeline of one bucket: elementary reconstructions of the series' resident factors
+ * (components 0 .. gmax), the sum of its own group, and the group's LRF where asked for. */
+static int bucket_followup(rbucket *b, ssa_rbatch *rb)
+{
+    CK(r_elem(b, NULL));
+    CK(r_gsum(b, rb));
+    if (rb->cur_lrf)
+        CK(r_lrf(b, rb));
+    return 0;
+}
+
 int ssa_b200_fft_length(int N)
 {
     const int code = N >= 1 ? ssad_fft_code_for(N) : -1;
@@ -806,7 +837,7 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
         if (N[s] < 4 || L[s] < 2 || L[s] > N[s] - 1 || k[s] < 1)
             return -1;
         const int K = N[s] - L[s] + 1;
-        const int kp = imin(k[s] + rb->p, imin(L[s], K));
+        const int kp = imin(k[s] + (rb->followup ? 0 : rb->p), imin(L[s], K));
         if (kp > SSA_MAX_KP)
             return -1;
         const int logh = ssad_fft_code_for(N[s]);
@@ -847,8 +878,20 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
         S->N = N[s];
         S->L = L[s];
         S->K = N[s] - L[s] + 1;
-        S->kp = imin(k[s] + rb->p, imin(S->L, S->K));
+        S->kp = imin(k[s] + (rb->followup ? 0 : rb->p), imin(S->L, S->K));
         S->k = imin(k[s], S->kp);
+        if (rb->followup)
+        {
+            S->Ux = rb->fu_U[s];
+            S->Vx = rb->fu_V[s];
+            S->sx = rb->fu_sig[s];
+            S->gx = rb->d_fu_gidx + rb->fu_goff[s];
+            S->gn = rb->fu_goff[s + 1] - rb->fu_goff[s];
+            S->gmax = -1;
+            for (int e = rb->fu_goff[s]; e < rb->fu_goff[s + 1]; e++)
+                if (rb->h_fu_gidx[e] < S->k && rb->h_fu_gidx[e] > S->gmax)
+                    S->gmax = rb->h_fu_gidx[e];
+        }
         S->ox = ox;
         S->osig = osig;
         S->oW = oW;
@@ -888,8 +931,8 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
             S->rows_W = ssad_wcorr_tc() ? imax(S->rows_N, SSA_TC_MIN_ROWS) : S->rows_N;
             S->nch_W = (S->N + S->rows_W - 1) / S->rows_W;
             S->nq = (S->L + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS;
-            S->wantW = !rb->cur_wmask || rb->cur_wmask[S->src];
-            S->nelem = S->wantW ? S->k : imin(S->k, rb->grp_need);
+            S->wantW = !rb->followup && (!rb->cur_wmask || rb->cur_wmask[S->src]);
+            S->nelem = rb->followup ? S->gmax + 1 : S->wantW ? S->k : imin(S->k, rb->grp_need);
             S->oY = oY;
             S->oZ = oZ;
             S->opart = opart;
@@ -925,6 +968,9 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
         b->sz[8] = orecon * sizeof(float);
         b->sz[9] = onorm * sizeof(double);
         b->sz[10] = b->logh > SSA_ELEM2_MAX_LOGH ? ospec * sizeof(float) : 0;
+        if (rb->followup) /* no decomposition: no signal spectra, probe blocks, Grams or rotations */
+            for (int i = 0; i < 8; i++)
+                b->sz[i] = 0;
     }
     /* carve the arena: every bucket's buffers, then the packed outputs and status words */
     size_t need = 0;
@@ -932,6 +978,8 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
         if (rb->bk[g].nb)
             for (int i = 0; i < 11; i++)
                 need += (rb->bk[g].sz[i] + 255) & ~(size_t)255;
+    if (rb->followup)
+        rb->n_sig = rb->n_W = 0;
     const size_t tail[5] = {rb->n_sig * sizeof(double), rb->n_W * sizeof(double),
                             rb->n_groups > 0 ? rb->n_grp * sizeof(double) : 0, (size_t)B * sizeof(int),
                             (size_t)B * sizeof(int)};
@@ -1043,7 +1091,7 @@ static int run_enqueue(ssa_rbatch *rb, int B, const int *N, const int *L, const 
             continue;
         b->status_base = rb->status;
         if (cudaStreamWaitEvent(b->e.st, rb->prof == 2 ? prev : rb->ev_in, 0) != cudaSuccess ||
-            bucket_run(b, rb, d_x, seed) != 0 ||
+            (rb->followup ? bucket_followup(b, rb) : bucket_run(b, rb, d_x, seed)) != 0 ||
             cudaEventRecord(b->done, b->e.st) != cudaSuccess ||
             cudaStreamWaitEvent(rb->main, b->done, 0) != cudaSuccess)
             return -1;
@@ -1312,6 +1360,64 @@ int ssar_run_enqueue_ex(ssa_rbatch *rb, int B, const int *N, const int *L, const
     rb->cur_lrf = NULL;
     rb->cur_wmask = NULL;
     return rc;
+}
+
+int ssar_run_followup(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k, const float *const *U,
+                      const float *const *V, const double *const *sig, const int *gidx, const int *goff,
+                      double *const *lrf_dst)
+{
+    if (!rb || B < 1 || !N || !L || !k || !U || !V || !sig || !gidx || !goff || rb->n_groups < 1)
+        return -1;
+    if (quiesce(rb) != 0)
+        return -1;
+    /* every series' group, uploaded on the main stream ahead of the buckets (which wait for it) */
+    const size_t ng = (size_t)goff[B];
+    if (ng + 1 > rb->c_fu_gidx)
+    {
+        if (rb->h_fu_gidx)
+            cudaFreeHost(rb->h_fu_gidx);
+        if (rb->d_fu_gidx)
+            cudaFree(rb->d_fu_gidx);
+        rb->h_fu_gidx = NULL;
+        rb->d_fu_gidx = NULL;
+        rb->c_fu_gidx = 0;
+        const size_t c = ng + ng / 2 + 64;
+        if (cudaMallocHost((void **)&rb->h_fu_gidx, sizeof(int) * c) != cudaSuccess ||
+            cudaMalloc((void **)&rb->d_fu_gidx, sizeof(int) * c) != cudaSuccess)
+            return -1;
+        rb->c_fu_gidx = c;
+    }
+    else if (cudaStreamSynchronize(rb->main) != cudaSuccess) /* the previous run's upload is done */
+        return -1;
+    memcpy(rb->h_fu_gidx, gidx, sizeof(int) * ng);
+    if (cudaMemcpyAsync(rb->d_fu_gidx, rb->h_fu_gidx, sizeof(int) * ng, cudaMemcpyHostToDevice, rb->main) !=
+        cudaSuccess)
+        return -1;
+    rb->followup = 1;
+    rb->fu_U = U;
+    rb->fu_V = V;
+    rb->fu_sig = sig;
+    rb->fu_goff = goff;
+    rb->cur_lrf = lrf_dst;
+    /* d_x is not read by a follow-up run: any valid pointer */
+    int rc = run_enqueue(rb, B, N, L, k, (const double *)rb->d_fu_gidx, 0);
+    rb->followup = 0;
+    rb->fu_U = rb->fu_V = NULL;
+    rb->fu_sig = NULL;
+    rb->fu_goff = NULL;
+    rb->cur_lrf = NULL;
+    return rc;
+}
+
+int ssar_series_factors(const ssa_rbatch *rb, int s, const float **U, const float **V)
+{
+    const rbucket *b = NULL;
+    const rser *S = find_series(rb, s, &b);
+    if (!S)
+        return -1;
+    *U = b->Y + S->oY;
+    *V = b->Z + S->oZ;
+    return S->k;
 }
 
 cudaStream_t ssar_main_stream(const ssa_rbatch *rb) { return rb->main; }

@@ -23,6 +23,24 @@ int ssar_set_lrf_group(ssa_rbatch *rb, int slot, const int *group, int n_group);
  * doubles of the forecast group; series whose k does not cover the group are skipped. */
 int ssar_run_enqueue_ex(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k, const double *d_x,
                         const unsigned long long *seeds, double *const *lrf_dst, const unsigned char *want_w);
+/* Follow-up run on resident factors, no decomposition: series s has k[s] components with
+ * factors U[s] (L x k, leading dimension round4(L)), V[s] (K x k, round4(K)), FP32, and sigma[s]
+ * (k doubles), all in device memory, and its own group gidx[goff[s] .. goff[s+1]) (host). The run
+ * writes the group's reconstruction (N doubles at the series' groups offset, group slot 0) and,
+ * where lrf_dst[s] is non-NULL, the group's R (L-1), reconstruction tail (L-1) and verticality.
+ * Indices >= k[s] are skipped. The batch must have been created with at least one group. */
+int ssar_run_followup(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k, const float *const *U,
+                      const float *const *V, const double *const *sig, const int *gidx, const int *goff,
+                      double *const *lrf_dst);
+/* Device factor blocks of series s of the last decomposition run (U: L x k', leading dimension
+ * round4(L); V: K x k', round4(K)); returns k' or -1. Valid until the next run. */
+int ssar_series_factors(const ssa_rbatch *rb, int s, const float **U, const float **V);
+/* Cadzow iterations (the device-resident loop of ssa_opt_cadzow) on the host signal x. With y1
+ * (host, N values) given, it is taken as the first rank-`rank` projection of x: the first
+ * iteration measures it against x instead of decomposing, and the loop continues from it.
+ * Returns the iteration count or -1 (ssa_api.c). */
+int ssab_cadzow_from(const double *x, const double *y1, int N, int L, int rank, int max_iter, double tol,
+                     double *output, SSA_CadzowResult *result);
 cudaStream_t ssar_main_stream(const ssa_rbatch *rb);
 const int *ssar_status(const ssa_rbatch *rb);
 const int *ssar_lrf_status(const ssa_rbatch *rb);

@@ -6,13 +6,17 @@
  * and taken in arrival order. Decompositions are gathered into uneven batches (ssa_ragged.c),
  * each batch bounded by a device-memory share of the HBM budget; up to `max_inflight` batches
  * run at once on their own streams, so requests that arrive while others are on the GPU start
- * as soon as a batch slot is free and overlap with the running ones. A decompose+reconstruct
- * request leaves its series resident: the LRF coefficients of the forecast group [0, 1, 2] and
- * the last L - 1 values of that group's reconstruction stay in device memory (stream-ordered
- * pool, least recently used entries evicted beyond the resident share of the budget), so a later
- * forecast request on that series runs the recurrence only (batched, one CTA per request)
- * without decomposing again. Every request is stamped with its arrival and completion times on
- * the host's monotonic clock; completion means its outputs are in host memory.
+ * as soon as a batch slot is free and overlap with the running ones. A decomposition request
+ * leaves its series resident: its factors U, V, sigma, its signal, the LRF coefficients of the
+ * forecast group [0, 1, 2] and the last L - 1 values of that group's reconstruction stay in
+ * device memory (stream-ordered pool, least recently used entries evicted beyond the resident
+ * share of the budget). Follow-ups on a resident series do not decompose again: a default
+ * forecast runs the recurrence only (batched, one CTA per request); reconstructions and forecasts
+ * of caller-chosen groups run as follow-up batches (elementary reconstructions of the resident
+ * factors, group sums, LRF, recurrence); Cadzow requests run on a worker of their own, a resident
+ * series' first projection taken from its factors. Every request is stamped with its arrival and
+ * completion times on the host's monotonic clock; completion means its outputs are in host
+ * memory.
  */
 #include <errno.h>
 #include <pthread.h>
@@ -46,8 +50,15 @@ typedef struct res_entry
     int id;
     int state;
     int L;
-    int refs;          /* in-flight forecasts using it */
-    double *d;         /* R (L-1), tail (L-1), verticality */
+    int refs;          /* in-flight follow-ups using it */
+    int N, K, k;       /* shape and resident components */
+    int lrf_ok;        /* the default forecast group's LRF is valid */
+    long long ldL, ldK;
+    /* one device block: doubles R (L-1), tail (L-1), verticality, sigma (k), signal (N), then
+     * floats U (ldL x k) and V (ldK x k), the leading dimensions of the batch's factor blocks */
+    double *d;
+    double *sig, *x;
+    float *U, *V;
     size_t bytes;
     struct res_entry *prev, *next; /* LRU list, most recent first */
     struct res_entry *hnext;
@@ -96,6 +107,41 @@ typedef struct
     size_t c_hout, c_dout;
 } fslot_t;
 
+/* Follow-up batch on resident factors: reconstructions, forecasts of caller-chosen groups and the
+ * first projection of Cadzow requests on resident series. */
+typedef struct
+{
+    ssa_rbatch *rb; /* created with one group slot; every series brings its own group */
+    cudaEvent_t done;
+    int busy, n, cap;
+    ssa_request **req;
+    res_entry **res;
+    int *N, *L, *k, *goff, *gidx;
+    int cgidx;
+    const float **U, **V;
+    const double **sig;
+    double **lrf;
+    size_t *tmpoff, *hoff;
+    double *d_tmp; /* per group forecast: R (L-1), tail (L-1), verticality */
+    size_t c_tmp;
+    ssa_fc_job *h_fc, *d_fc;
+    int c_fc;
+    double *d_fcout;
+    size_t c_fcout;
+    double *h_out; /* pinned: reconstructions, resident signals (Cadzow), forecasts */
+    size_t c_hout;
+    int *h_lst;
+} uslot_t;
+
+/* Cadzow requests waiting for the Cadzow worker, with host copies of a resident series' signal
+ * and first projection (NULL for requests that bring their own signal). */
+typedef struct cz_item
+{
+    ssa_request *r;
+    double *x, *y1;
+    struct cz_item *next;
+} cz_item;
+
 struct ssa_server
 {
     pthread_t th;
@@ -123,6 +169,12 @@ struct ssa_server
     cudaEvent_t ev_pool;
     int device;
     ssa_server_stats stats;
+    uslot_t us;
+    /* Cadzow worker: its own thread, queue and wake-up */
+    pthread_t cz_th;
+    int cz_live, cz_stop;
+    cz_item *cz_head, *cz_tail;
+    pthread_cond_t cz_cv;
 };
 
 double ssa_server_now(void)
@@ -273,9 +325,11 @@ static int res_make_room(ssa_server *s, size_t need)
     return s->res_bytes + need <= s->res_budget ? 0 : -1;
 }
 
-/* New pending entry for series `id` with window L, without device memory yet (replaces an idle
- * older one); forecasts on the series wait while it is pending. */
-static res_entry *res_create(ssa_server *s, int id, int L)
+static long long round4ll(long long v) { return (v + 3) & ~3LL; }
+
+/* New pending entry for series `id` of shape (N, L) with k resident components, without device
+ * memory yet (replaces an idle older one); follow-ups on the series wait while it is pending. */
+static res_entry *res_create(ssa_server *s, int id, int N, int L, int k)
 {
     res_entry *old = res_find(s, id);
     if (old)
@@ -289,6 +343,11 @@ static res_entry *res_create(ssa_server *s, int id, int L)
         return NULL;
     e->id = id;
     e->L = L;
+    e->N = N;
+    e->K = N - L + 1;
+    e->k = k;
+    e->ldL = round4ll(L);
+    e->ldK = round4ll(e->K);
     e->state = RES_PENDING;
     unsigned h = (unsigned)id % (unsigned)s->hcap;
     e->hnext = s->htab[h];
@@ -297,11 +356,20 @@ static res_entry *res_create(ssa_server *s, int id, int L)
     return e;
 }
 
-/* Device memory for a pending entry when its decomposition is launched: R (L-1), tail (L-1) and
- * verticality doubles, evicting least recently used idle series beyond the resident budget. */
+/* Doubles before the factor floats of an entry's block (a multiple of 2, so the floats start
+ * 16-byte aligned). */
+static size_t res_dbl(const res_entry *e)
+{
+    const size_t n = 2 * (size_t)(e->L - 1) + 1 + (size_t)e->k + (size_t)e->N;
+    return (n + 1) & ~(size_t)1;
+}
+
+/* Device memory for a pending entry when its decomposition is launched (layout in res_entry),
+ * evicting least recently used idle series beyond the resident budget. */
 static int res_alloc(ssa_server *s, res_entry *e)
 {
-    const size_t bytes = sizeof(double) * (2 * (size_t)(e->L - 1) + 1);
+    const size_t nd = res_dbl(e);
+    const size_t bytes = sizeof(double) * nd + sizeof(float) * (size_t)(e->ldL + e->ldK) * (size_t)e->k;
     if (res_make_room(s, bytes) != 0)
         return -1;
     cudaMemPool_t pool = ssar_pool();
@@ -310,6 +378,10 @@ static int res_alloc(ssa_server *s, res_entry *e)
         e->d = NULL;
         return -1;
     }
+    e->sig = e->d + 2 * (size_t)(e->L - 1) + 1;
+    e->x = e->sig + e->k;
+    e->U = (float *)(e->d + nd);
+    e->V = e->U + e->ldL * e->k;
     e->bytes = bytes;
     s->res_bytes += bytes;
     return 0;
@@ -480,7 +552,13 @@ static int slot_launch(ssa_server *s, slot_t *sl)
     /* the copy kernel's segment table; the slot is idle, so its table is free */
     size_t nseg = 0;
     for (int i = 0; i < sl->n; i++)
+    {
         nseg += req_segs(s, sl->req[i]);
+        const res_entry *e = sl->res[i];
+        if (e && e->d)
+            nseg += seg_count((size_t)e->k) + seg_count((size_t)e->N) + seg_count((size_t)(e->ldL * e->k / 2)) +
+                    seg_count((size_t)(e->ldK * e->k / 2));
+    }
     if (nseg > sl->c_seg)
     {
         if (sl->h_seg)
@@ -533,6 +611,17 @@ static int slot_launch(ssa_server *s, slot_t *sl)
                     2 * (size_t)r->N);
         if (r->type == SSA_REQ_DECOMPOSE_WCORR && r->W)
             seg_add(sl->h_seg, &ns, dW + off[4 * i + 2], direct ? sl->hp[4 * i + 3] : sl->h_out_d + so, ke * ke);
+        /* the series stays resident: sigma, signal and the factor blocks (floats copied as pairs;
+         * both leading dimensions are multiples of 4) */
+        res_entry *e = sl->res[i];
+        const float *U = NULL, *V = NULL;
+        if (e && e->d && ssar_series_factors(sl->rb, i, &U, &V) == e->k)
+        {
+            seg_add(sl->h_seg, &ns, dsig + off[4 * i + 1], e->sig, (size_t)e->k);
+            seg_add(sl->h_seg, &ns, sl->d_x + sl->xoff[i], e->x, (size_t)e->N);
+            seg_add(sl->h_seg, &ns, (const double *)U, (double *)e->U, (size_t)(e->ldL * e->k / 2));
+            seg_add(sl->h_seg, &ns, (const double *)V, (double *)e->V, (size_t)(e->ldK * e->k / 2));
+        }
     }
     if (ssad_copy_segments(sl->h_seg_d + nin, (int)(ns - nin), ms) != 0)
         return -1;
@@ -583,8 +672,12 @@ static void slot_finish(ssa_server *s, slot_t *sl, int launch_ok)
             }
         }
         res_entry *e = sl->res[i];
-        if (e) /* the forecast group [0, 1, 2] needs at least 3 components */
-            e->state = (ok && e->d && sl->h_lst[i] == 0 && r->k_out > 2) ? RES_READY : RES_FAILED;
+        if (e)
+        {
+            e->state = (ok && e->d && r->k_out == e->k) ? RES_READY : RES_FAILED;
+            /* the default forecast group [0, 1, 2] needs at least 3 components */
+            e->lrf_ok = sl->h_lst[i] == 0 && r->k_out > 2;
+        }
         finish_request(s, r, ok ? 0 : -1);
     }
     sl->n = 0;
@@ -646,6 +739,324 @@ static void fs_finish(ssa_server *s, int ok)
     f->busy = 0;
 }
 
+/* ---- follow-up batches on resident factors ---------------------------------------------------- */
+
+static int is_followup(const ssa_request *r)
+{
+    return r->type == SSA_REQ_RECONSTRUCT || (r->type == SSA_REQ_FORECAST && r->group) ||
+           (r->type == SSA_REQ_CADZOW && !r->x);
+}
+
+static int us_reserve(uslot_t *u, int n)
+{
+    if (n <= u->cap)
+        return 0;
+    const int c = n + n / 2 + 16;
+    void *p[13];
+    p[0] = realloc(u->req, sizeof(ssa_request *) * c);
+    if (p[0])
+        u->req = (ssa_request **)p[0];
+    p[1] = realloc(u->res, sizeof(res_entry *) * c);
+    if (p[1])
+        u->res = (res_entry **)p[1];
+    p[2] = realloc(u->N, sizeof(int) * c);
+    if (p[2])
+        u->N = (int *)p[2];
+    p[3] = realloc(u->L, sizeof(int) * c);
+    if (p[3])
+        u->L = (int *)p[3];
+    p[4] = realloc(u->k, sizeof(int) * c);
+    if (p[4])
+        u->k = (int *)p[4];
+    p[5] = realloc(u->goff, sizeof(int) * (c + 1));
+    if (p[5])
+        u->goff = (int *)p[5];
+    p[6] = realloc((void *)u->U, sizeof(float *) * c);
+    if (p[6])
+        u->U = (const float **)p[6];
+    p[7] = realloc((void *)u->V, sizeof(float *) * c);
+    if (p[7])
+        u->V = (const float **)p[7];
+    p[8] = realloc((void *)u->sig, sizeof(double *) * c);
+    if (p[8])
+        u->sig = (const double **)p[8];
+    p[9] = realloc(u->lrf, sizeof(double *) * c);
+    if (p[9])
+        u->lrf = (double **)p[9];
+    p[10] = realloc(u->tmpoff, sizeof(size_t) * c);
+    if (p[10])
+        u->tmpoff = (size_t *)p[10];
+    p[11] = realloc(u->hoff, sizeof(size_t) * c);
+    if (p[11])
+        u->hoff = (size_t *)p[11];
+    p[12] = NULL;
+    for (int i = 0; i < 12; i++)
+        if (!p[i])
+            return -1;
+    int *h = NULL;
+    if (cudaMallocHost((void **)&h, sizeof(int) * c) != cudaSuccess)
+        return -1;
+    if (u->h_lst)
+        cudaFreeHost(u->h_lst);
+    u->h_lst = h;
+    u->cap = c;
+    return 0;
+}
+
+/* Host doubles of a follow-up's outputs in the pinned area: the group reconstruction (N) for
+ * reconstructions and Cadzow (plus the resident signal, N, for Cadzow), h forecasts. */
+static size_t us_out_doubles(const ssa_request *r, const res_entry *e)
+{
+    if (r->type == SSA_REQ_FORECAST)
+        return (size_t)r->h;
+    return (size_t)e->N * (r->type == SSA_REQ_CADZOW ? 2 : 1);
+}
+
+static int us_launch(ssa_server *s)
+{
+    uslot_t *u = &s->us;
+    cudaStream_t st = ssar_main_stream(u->rb);
+    int ng = 0, nfc = 0;
+    size_t ntmp = 0, nfcout = 0, nout = 0;
+    for (int i = 0; i < u->n; i++)
+    {
+        const ssa_request *r = u->req[i];
+        ng += r->type == SSA_REQ_CADZOW ? r->rank : r->n_group;
+        if (r->type == SSA_REQ_FORECAST)
+        {
+            nfc++;
+            ntmp += 2 * (size_t)(u->res[i]->L - 1) + 1;
+            nfcout += (size_t)r->h;
+        }
+        nout += us_out_doubles(r, u->res[i]);
+    }
+    if (ng > u->cgidx)
+    {
+        int *g = (int *)realloc(u->gidx, sizeof(int) * (size_t)(ng + ng / 2 + 16));
+        if (!g)
+            return -1;
+        u->gidx = g;
+        u->cgidx = ng + ng / 2 + 16;
+    }
+    if (grow_dev((void **)&u->d_tmp, &u->c_tmp, ntmp + 1, sizeof(double)) != 0 ||
+        grow_dev((void **)&u->d_fcout, &u->c_fcout, nfcout + 1, sizeof(double)) != 0 ||
+        grow_host((void **)&u->h_out, &u->c_hout, nout + 1, sizeof(double)) != 0)
+        return -1;
+    if (nfc > u->c_fc)
+    {
+        ssa_fc_job *hj = NULL, *dj = NULL;
+        const int c = nfc + nfc / 2 + 16;
+        if (cudaMallocHost((void **)&hj, sizeof(ssa_fc_job) * c) != cudaSuccess ||
+            cudaMalloc((void **)&dj, sizeof(ssa_fc_job) * c) != cudaSuccess)
+        {
+            if (hj)
+                cudaFreeHost(hj);
+            return -1;
+        }
+        if (u->h_fc)
+            cudaFreeHost(u->h_fc);
+        if (u->d_fc)
+            cudaFree(u->d_fc);
+        u->h_fc = hj;
+        u->d_fc = dj;
+        u->c_fc = c;
+    }
+    size_t otmp = 0, ofc = 0, oh = 0;
+    int og = 0, jf = 0;
+    for (int i = 0; i < u->n; i++)
+    {
+        const ssa_request *r = u->req[i];
+        const res_entry *e = u->res[i];
+        u->N[i] = e->N;
+        u->L[i] = e->L;
+        u->k[i] = e->k;
+        u->U[i] = e->U;
+        u->V[i] = e->V;
+        u->sig[i] = e->sig;
+        u->goff[i] = og;
+        if (r->type == SSA_REQ_CADZOW)
+            for (int j = 0; j < r->rank; j++)
+                u->gidx[og++] = j;
+        else
+            for (int j = 0; j < r->n_group; j++)
+                u->gidx[og++] = r->group[j];
+        u->lrf[i] = NULL;
+        u->hoff[i] = oh;
+        oh += us_out_doubles(r, e);
+        if (r->type == SSA_REQ_FORECAST)
+        {
+            u->tmpoff[i] = otmp;
+            u->lrf[i] = u->d_tmp + otmp;
+            ssa_fc_job *J = &u->h_fc[jf++];
+            J->R = u->d_tmp + otmp;
+            J->tail = u->d_tmp + otmp + (e->L - 1);
+            J->out = u->d_fcout + ofc;
+            J->w = e->L - 1;
+            J->h = r->h;
+            otmp += 2 * (size_t)(e->L - 1) + 1;
+            ofc += (size_t)r->h;
+        }
+    }
+    u->goff[u->n] = og;
+    /* the resident blocks were allocated on the pool stream */
+    if (cudaEventRecord(s->ev_pool, s->pool_st) != cudaSuccess || cudaStreamWaitEvent(st, s->ev_pool, 0) != cudaSuccess)
+        return -1;
+    if (ssar_run_followup(u->rb, u->n, u->N, u->L, u->k, (const float *const *)u->U, (const float *const *)u->V,
+                          (const double *const *)u->sig, u->gidx, u->goff, u->lrf) != 0)
+        return -1;
+    if (nfc > 0 && (cudaMemcpyAsync(u->d_fc, u->h_fc, sizeof(ssa_fc_job) * nfc, cudaMemcpyHostToDevice, st) !=
+                        cudaSuccess ||
+                    ssad_forecast_apply(u->d_fc, nfc, st) != 0))
+        return -1;
+    const size_t *off = ssar_offsets(u->rb);
+    const double *dg = ssar_groups(u->rb);
+    ofc = 0;
+    for (int i = 0; i < u->n; i++)
+    {
+        const ssa_request *r = u->req[i];
+        const res_entry *e = u->res[i];
+        double *h = u->h_out + u->hoff[i];
+        cudaError_t c = cudaSuccess;
+        if (r->type == SSA_REQ_FORECAST)
+        {
+            c = cudaMemcpyAsync(h, u->d_fcout + ofc, sizeof(double) * r->h, cudaMemcpyDeviceToHost, st);
+            ofc += (size_t)r->h;
+        }
+        else
+        {
+            c = cudaMemcpyAsync(h, dg + off[4 * i + 3], sizeof(double) * e->N, cudaMemcpyDeviceToHost, st);
+            if (c == cudaSuccess && r->type == SSA_REQ_CADZOW)
+                c = cudaMemcpyAsync(h + e->N, e->x, sizeof(double) * e->N, cudaMemcpyDeviceToHost, st);
+        }
+        if (c != cudaSuccess)
+            return -1;
+    }
+    if (cudaMemcpyAsync(u->h_lst, ssar_lrf_status(u->rb), sizeof(int) * u->n, cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaEventRecord(u->done, st) != cudaSuccess)
+        return -1;
+    u->busy = 1;
+    s->stats.followup_batches++;
+    s->stats.followups += u->n;
+    return 0;
+}
+
+static void cz_push(ssa_server *s, ssa_request *r, double *x, double *y1);
+
+static void us_finish(ssa_server *s, int ok)
+{
+    uslot_t *u = &s->us;
+    for (int i = 0; i < u->n; i++)
+    {
+        ssa_request *r = u->req[i];
+        res_entry *e = u->res[i];
+        const double *h = u->h_out + u->hoff[i];
+        int st = ok ? 0 : -1;
+        if (ok && r->type == SSA_REQ_RECONSTRUCT)
+        {
+            if (r->out)
+                memcpy(r->out, h, sizeof(double) * e->N);
+        }
+        else if (ok && r->type == SSA_REQ_FORECAST)
+        {
+            if (u->h_lst[i] != 0)
+                st = -1; /* verticality >= 1: no LRF */
+            else if (r->forecast)
+                memcpy(r->forecast, h, sizeof(double) * r->h);
+        }
+        else if (ok && r->type == SSA_REQ_CADZOW)
+        {
+            double *x = (double *)malloc(sizeof(double) * e->N), *y1 = (double *)malloc(sizeof(double) * e->N);
+            if (x && y1)
+            {
+                memcpy(y1, h, sizeof(double) * e->N);
+                memcpy(x, h + e->N, sizeof(double) * e->N);
+                r->N = e->N;
+                r->L = e->L;
+                e->refs--;
+                cz_push(s, r, x, y1); /* finished by the Cadzow worker */
+                continue;
+            }
+            free(x);
+            free(y1);
+            st = -1;
+        }
+        e->refs--;
+        finish_request(s, r, st);
+    }
+    u->n = 0;
+    u->busy = 0;
+}
+
+/* ---- Cadzow worker ------------------------------------------------------------------------------ */
+
+static void cz_push(ssa_server *s, ssa_request *r, double *x, double *y1)
+{
+    cz_item *it = (cz_item *)calloc(1, sizeof(cz_item));
+    if (!it)
+    {
+        free(x);
+        free(y1);
+        finish_request(s, r, -1);
+        return;
+    }
+    it->r = r;
+    it->x = x;
+    it->y1 = y1;
+    pthread_mutex_lock(&s->mu);
+    if (s->cz_tail)
+        s->cz_tail->next = it;
+    else
+        s->cz_head = it;
+    s->cz_tail = it;
+    pthread_cond_signal(&s->cz_cv);
+    pthread_mutex_unlock(&s->mu);
+}
+
+/* Runs Cadzow requests one after another: a request with its own signal from the start, one on a
+ * resident series from the projection its follow-up batch made out of the resident factors. */
+static void *cz_worker(void *arg)
+{
+    ssa_server *s = (ssa_server *)arg;
+    cudaSetDevice(s->device);
+    for (;;)
+    {
+        pthread_mutex_lock(&s->mu);
+        while (!s->cz_head && !s->cz_stop)
+            pthread_cond_wait(&s->cz_cv, &s->mu);
+        cz_item *it = s->cz_head;
+        if (!it)
+        {
+            pthread_mutex_unlock(&s->mu);
+            break;
+        }
+        s->cz_head = it->next;
+        if (!s->cz_head)
+            s->cz_tail = NULL;
+        pthread_mutex_unlock(&s->mu);
+        ssa_request *r = it->r;
+        SSA_CadzowResult res;
+        memset(&res, 0, sizeof(res));
+        const double *x = it->x ? it->x : r->x;
+        double *out = r->out ? r->out : (double *)malloc(sizeof(double) * (size_t)r->N);
+        const int rc = out ? ssab_cadzow_from(x, it->y1, r->N, r->L, r->rank, r->max_iter, r->tol, out, &res) : -1;
+        if (!r->out)
+            free(out);
+        r->iterations = res.iterations;
+        r->final_diff = res.final_diff;
+        pthread_mutex_lock(&s->mu);
+        s->stats.cadzow_requests++;
+        if (rc >= 0)
+            s->stats.cadzow_iterations += res.iterations;
+        pthread_mutex_unlock(&s->mu);
+        free(it->x);
+        free(it->y1);
+        free(it);
+        finish_request(s, r, rc >= 0 ? 0 : -1);
+    }
+    return NULL;
+}
+
 /* ---- worker ---------------------------------------------------------------------------------- */
 
 static int poll_done(ssa_server *s)
@@ -668,6 +1079,15 @@ static int poll_done(ssa_server *s)
         if (q != cudaErrorNotReady)
         {
             fs_finish(s, q == cudaSuccess);
+            progressed = 1;
+        }
+    }
+    if (s->us.busy)
+    {
+        cudaError_t q = cudaEventQuery(s->us.done);
+        if (q != cudaErrorNotReady)
+        {
+            us_finish(s, q == cudaSuccess);
             progressed = 1;
         }
     }
@@ -706,6 +1126,7 @@ static int dispatch(ssa_server *s)
         if (!s->slots[i].busy)
             free_slot = &s->slots[i];
     fslot_t *f = s->fs.busy ? NULL : &s->fs;
+    uslot_t *u = s->us.busy ? NULL : &s->us;
     size_t bytes = 0;
     int kept = 0;
     int cls = -1; /* size class of the batch being formed */
@@ -713,10 +1134,11 @@ static int dispatch(ssa_server *s)
     {
         ssa_request *r = s->pend[i];
         int keep = 1;
-        if (r->type == SSA_REQ_FORECAST)
+        if (r->type == SSA_REQ_FORECAST && !r->group)
         {
             res_entry *e = res_find(s, r->series_id);
-            if (!e || e->state == RES_FAILED || r->h < 1 || r->h > SSA_FC_MAX_H)
+            if (!e || e->state == RES_FAILED || (e->state == RES_READY && !e->lrf_ok) || r->h < 1 ||
+                r->h > SSA_FC_MAX_H)
             {
                 finish_request(s, r, -1);
                 keep = 0;
@@ -764,13 +1186,56 @@ static int dispatch(ssa_server *s)
                 }
             }
         }
+        else if (is_followup(r))
+        {
+            res_entry *e = res_find(s, r->series_id);
+            int bad = !e || e->state == RES_FAILED;
+            if (!bad && r->type == SSA_REQ_CADZOW)
+                bad = r->rank < 1 || r->rank > e->k || r->max_iter < 1;
+            else if (!bad)
+            {
+                int any = 0; /* a group needs at least one component the series has */
+                for (int j = 0; r->group && j < r->n_group; j++)
+                    any |= r->group[j] >= 0 && r->group[j] < e->k;
+                bad = !r->group || r->n_group < 1 || (r->type == SSA_REQ_FORECAST && !any) ||
+                      (r->type == SSA_REQ_FORECAST && (r->h < 1 || r->h > SSA_FC_MAX_H));
+            }
+            if (bad)
+            {
+                finish_request(s, r, -1);
+                keep = 0;
+                progressed = 1;
+            }
+            else if (e->state == RES_READY && u && u->n < s->max_batch && us_reserve(u, u->n + 1) == 0)
+            {
+                e->refs++;
+                lru_unlink(s, e);
+                lru_front(s, e);
+                u->req[u->n] = r;
+                u->res[u->n] = e;
+                u->n++;
+                keep = 0;
+            }
+        }
+        else if (r->type == SSA_REQ_CADZOW)
+        {
+            /* a new series: straight to the Cadzow worker */
+            const int ok = r->N >= 4 && r->L >= 2 && r->L <= r->N - 1 && r->rank >= 1 && r->max_iter >= 1 &&
+                           imin(r->rank, imin(r->L, r->N - r->L + 1)) <= SSA_MAX_KP;
+            if (ok)
+                cz_push(s, r, NULL, NULL);
+            else
+                finish_request(s, r, -1);
+            keep = 0;
+            progressed = 1;
+        }
         else if (is_decomp(r))
         {
-            if (r->type == SSA_REQ_DECOMPOSE_RECON && !r->priv && valid_decomp(s, r))
+            if (!r->priv && valid_decomp(s, r))
             {
-                /* pending resident entry from the moment the request is seen, so forecasts on
+                /* pending resident entry from the moment the request is seen, so follow-ups on
                  * the series that arrive later wait for it */
-                r->priv = res_create(s, r->series_id, r->L);
+                r->priv = res_create(s, r->series_id, r->N, r->L, req_kout(s, r));
                 if (!r->priv)
                 {
                     s->stats.not_resident++;
@@ -858,6 +1323,12 @@ static int dispatch(ssa_server *s)
             fs_finish(s, 0);
         progressed = 1;
     }
+    if (u && u->n > 0)
+    {
+        if (us_launch(s) != 0)
+            us_finish(s, 0);
+        progressed = 1;
+    }
     if (free_slot && free_slot->n > 0)
     {
         free_slot->bytes = bytes;
@@ -870,7 +1341,7 @@ static int dispatch(ssa_server *s)
 
 static int any_busy(const ssa_server *s)
 {
-    if (s->fs.busy)
+    if (s->fs.busy || s->us.busy)
         return 1;
     for (int i = 0; i < s->nslots; i++)
         if (s->slots[i].busy)
@@ -1003,6 +1474,16 @@ int ssa_server_create(ssa_server **out, size_t hbm_budget_bytes, int max_infligh
         }
         f->cap = max_batch;
     }
+    {
+        /* follow-up batches: one group slot (each series brings its own group) */
+        static const int one_idx[1] = {0}, one_size[1] = {1};
+        if (ssa_rbatch_create(&s->us.rb, s->p, power_iters, one_idx, one_size, 1) != 0 ||
+            cudaEventCreateWithFlags(&s->us.done, cudaEventDisableTiming) != cudaSuccess || us_reserve(&s->us, 64) != 0)
+        {
+            ssa_server_destroy(s);
+            return -1;
+        }
+    }
     if (cudaStreamCreateWithFlags(&s->fs.st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->fs.done, cudaEventDisableTiming) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s->pool_st, cudaStreamNonBlocking) != cudaSuccess ||
@@ -1011,12 +1492,20 @@ int ssa_server_create(ssa_server **out, size_t hbm_budget_bytes, int max_infligh
         ssa_server_destroy(s);
         return -1;
     }
+    pthread_cond_init(&s->cz_cv, NULL);
     if (pthread_create(&s->th, NULL, worker, s) != 0)
     {
+        pthread_cond_destroy(&s->cz_cv);
         ssa_server_destroy(s);
         return -1;
     }
     s->th_live = 1;
+    if (pthread_create(&s->cz_th, NULL, cz_worker, s) != 0)
+    {
+        ssa_server_destroy(s);
+        return -1;
+    }
+    s->cz_live = 1;
     *out = s;
     return 0;
 }
@@ -1028,6 +1517,8 @@ int ssa_server_submit(ssa_server *s, ssa_request *r)
     r->status = 1; /* in progress */
     r->k_out = 0;
     r->priv = NULL;
+    r->iterations = 0;
+    r->final_diff = 0.0;
     r->t_done = 0.0;
     r->t_arrival = ssa_server_now();
     pthread_mutex_lock(&s->mu);
@@ -1108,12 +1599,17 @@ void ssa_server_destroy(ssa_server *s)
         ssa_server_drain(s);
         pthread_mutex_lock(&s->mu);
         s->stop = 1;
+        s->cz_stop = 1;
         pthread_cond_broadcast(&s->cv);
+        pthread_cond_broadcast(&s->cz_cv);
         pthread_mutex_unlock(&s->mu);
         pthread_join(s->th, NULL);
+        if (s->cz_live)
+            pthread_join(s->cz_th, NULL);
         pthread_mutex_destroy(&s->mu);
         pthread_cond_destroy(&s->cv);
         pthread_cond_destroy(&s->cv_done);
+        pthread_cond_destroy(&s->cz_cv);
     }
     cudaDeviceSynchronize();
     for (int i = 0; s->slots && i < s->nslots; i++)
@@ -1170,6 +1666,38 @@ void ssa_server_destroy(ssa_server *s)
         cudaFree(s->fs.d_out);
     free(s->fs.req);
     free(s->fs.res);
+    {
+        uslot_t *u = &s->us;
+        if (u->rb)
+            ssa_rbatch_destroy(u->rb);
+        if (u->done)
+            cudaEventDestroy(u->done);
+        if (u->h_fc)
+            cudaFreeHost(u->h_fc);
+        if (u->d_fc)
+            cudaFree(u->d_fc);
+        if (u->h_out)
+            cudaFreeHost(u->h_out);
+        if (u->h_lst)
+            cudaFreeHost(u->h_lst);
+        if (u->d_tmp)
+            cudaFree(u->d_tmp);
+        if (u->d_fcout)
+            cudaFree(u->d_fcout);
+        free(u->req);
+        free(u->res);
+        free(u->N);
+        free(u->L);
+        free(u->k);
+        free(u->goff);
+        free(u->gidx);
+        free((void *)u->U);
+        free((void *)u->V);
+        free((void *)u->sig);
+        free(u->lrf);
+        free(u->tmpoff);
+        free(u->hoff);
+    }
     free(s->pend);
     free(s->q);
     free(s);

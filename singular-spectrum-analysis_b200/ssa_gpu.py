@@ -917,7 +917,10 @@ class _Request(ctypes.Structure):
                 ("k", ctypes.c_int), ("h", ctypes.c_int), ("x", c_double_p), ("seed", ctypes.c_uint64),
                 ("sigma", c_double_p), ("groups", c_double_p), ("W", c_double_p), ("forecast", c_double_p),
                 ("status", ctypes.c_int), ("k_out", ctypes.c_int), ("t_arrival", ctypes.c_double),
-                ("t_done", ctypes.c_double), ("priv", ctypes.c_void_p)]
+                ("t_done", ctypes.c_double), ("priv", ctypes.c_void_p),
+                ("group", c_int_p), ("n_group", ctypes.c_int), ("rank", ctypes.c_int), ("max_iter", ctypes.c_int),
+                ("tol", ctypes.c_double), ("out", c_double_p), ("iterations", ctypes.c_int),
+                ("final_diff", ctypes.c_double)]
 
 
 class _ServerStats(ctypes.Structure):
@@ -925,7 +928,9 @@ class _ServerStats(ctypes.Structure):
                                                   "max_batch", "forecast_batches", "forecasts", "evictions",
                                                   "not_resident")] + \
                [(n, ctypes.c_size_t) for n in ("resident_bytes", "resident_budget", "batch_budget")] + \
-               [(n, ctypes.c_double) for n in ("host_launch_s", "host_finish_s", "host_launch_max_s")]
+               [(n, ctypes.c_double) for n in ("host_launch_s", "host_finish_s", "host_launch_max_s")] + \
+               [(n, ctypes.c_longlong) for n in ("followup_batches", "followups", "cadzow_requests",
+                                                  "cadzow_iterations")]
 
 
 _sig("ssa_rbatch_series_result", _I, ctypes.c_void_p, _I, c_double_p, c_double_p, c_double_p, c_double_p,
@@ -965,7 +970,7 @@ class _PinnedPool:
             _lib.ssa_host_free(p)
         self._ptrs = []
 
-REQ_DECOMPOSE_RECON, REQ_DECOMPOSE_WCORR, REQ_FORECAST = 0, 1, 2
+REQ_DECOMPOSE_RECON, REQ_DECOMPOSE_WCORR, REQ_FORECAST, REQ_RECONSTRUCT, REQ_CADZOW = 0, 1, 2, 3, 4
 
 
 class Requests:
@@ -1032,20 +1037,65 @@ class Requests:
         self._bufs.append(bufs)
         return self.n - 1
 
-    def add_forecast(self, series_id: int, h: int) -> int:
+    def _group(self, r, bufs, group):
+        if group is not None:
+            g = np.ascontiguousarray(group, dtype=np.int32)
+            bufs["_group"] = g
+            r.group = _ip(g)
+            r.n_group = len(g)
+
+    def add_forecast(self, series_id: int, h: int, group: Optional[Sequence[int]] = None) -> int:
+        """R-forecast of h steps on a resident series: of the group [0, 1, 2] (resident LRF) or of
+        `group` (computed from the resident factors)."""
         r = self._next()
         r.type = REQ_FORECAST
         r.series_id, r.h = series_id, h
         bufs = {}
+        self._group(r, bufs, group)
         if self.keep_outputs:
             bufs["forecast"] = self._buf((h,), role=1 + (self.n - 1) % 2)
             r.forecast = _dp(bufs["forecast"])
         self._bufs.append(bufs)
         return self.n - 1
 
+    def add_reconstruct(self, series_id: int, N: int, group: Sequence[int]) -> int:
+        """Reconstruction of `group` of a resident series of length N (no decomposition)."""
+        r = self._next()
+        r.type = REQ_RECONSTRUCT
+        r.series_id = series_id
+        bufs = {}
+        self._group(r, bufs, group)
+        if self.keep_outputs:
+            bufs["out"] = self._buf((N,), role=1)
+            r.out = _dp(bufs["out"])
+        self._bufs.append(bufs)
+        return self.n - 1
+
+    def add_cadzow(self, rank: int, max_iter: int = 10, tol: float = 1e-9, series_id: int = 0,
+                   x: Optional[np.ndarray] = None, L: int = 0, N: Optional[int] = None) -> int:
+        """Cadzow iterations of rank `rank`: on the resident series `series_id` (x None; N its length)
+        or on the new signal x with window L."""
+        r = self._next()
+        r.type = REQ_CADZOW
+        r.series_id, r.rank, r.max_iter, r.tol = series_id, rank, max_iter, tol
+        bufs = {}
+        if x is not None:
+            xb = self._buf((len(x),), np.asarray(x, dtype=np.float64))
+            bufs["x"] = xb
+            r.x = _dp(xb)
+            r.N, r.L = len(xb), L
+            N = len(xb)
+        if self.keep_outputs:
+            bufs["out"] = self._buf((N,), role=1)
+            r.out = _dp(bufs["out"])
+        self._bufs.append(bufs)
+        return self.n - 1
+
     def result(self, i: int) -> dict:
         r = self.arr[i]
-        out = {k: v for k, v in self._bufs[i].items() if k != "x"}
+        out = {k: v for k, v in self._bufs[i].items() if k not in ("x", "_group")}
+        if r.type == REQ_CADZOW:
+            out["iterations"], out["final_diff"] = r.iterations, r.final_diff
         if "sigma" in out:
             out["sigma"] = out["sigma"][:r.k_out] if r.k_out else out["sigma"][:0]
         out["status"] = r.status

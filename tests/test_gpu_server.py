@@ -157,13 +157,23 @@ def test_server_rejections_and_waiting(gpu, oracle):
     srv.close()
 
 
+def resident_bytes(N, L, k):
+    """Device bytes of one resident series: R, tail, verticality, sigma and the signal (doubles,
+    rounded to an even count), then U and V with leading dimensions rounded to 4 (floats)."""
+    K = N - L + 1
+    nd = 2 * (L - 1) + 1 + k + N
+    nd += nd & 1
+    r4 = lambda v: (v + 3) & ~3  # noqa: E731
+    return 8 * nd + 4 * (r4(L) + r4(K)) * k
+
+
 def test_server_evicts_beyond_resident_budget(gpu, oracle):
     rng = np.random.default_rng(7)
     N, L, k = 4000, 1000, 10
-    # resident share = budget / 4; each resident series holds 2 (L - 1) + 1 doubles
+    # resident share = budget / 4
     budget = 4 << 20
     srv = gpu.SSAServer(hbm_budget_bytes=budget, max_inflight=2, oversampling=P, power_iters=Q)
-    per = 8 * (2 * (L - 1) + 1)
+    per = resident_bytes(N, L, k)
     n_fit = (budget // 4) // per
     n = n_fit + 15
     R = gpu.Requests(n, keep_outputs=False)
@@ -179,4 +189,117 @@ def test_server_evicts_beyond_resident_budget(gpu, oracle):
     F.add_forecast(n - 1, 5)   # most recent: resident
     srv.run(F)
     assert list(F.statuses()) == [-1, 0]
+    srv.close()
+
+
+def cadzow_from_factors(oracle, x, d, L, rank, iters, tol):
+    """Cadzow on x whose first projection is the reconstruction of components 0..rank-1 of the
+    decomposition d; later iterations as ssa_opt_cadzow (a fresh context each: the first-call test
+    matrix, q = 0, oversampling 8). Returns (signal, iterations, final_diff)."""
+    N = len(x)
+    K = N - L + 1
+    xn = float(np.linalg.norm(x)) or 1.0
+    y = oracle.reconstruct(d, list(range(rank)), N, L)
+    diff = float(np.linalg.norm(y - x)) / xn
+    it = 1
+    Om = oracle.device_gaussian(oracle.single_series_seed(0), K, min(rank + 8, L, K))
+    while it < iters and diff >= tol:
+        dec = oracle.decompose_randomized(y, L, rank, 8, Om, q=0)
+        yn = oracle.reconstruct(dec, list(range(rank)), N, L)
+        diff = float(np.linalg.norm(yn - y)) / xn
+        y = yn
+        it += 1
+    return y, it, diff
+
+
+def _followups(gpu, R, shapes):
+    """Follow-ups on the resident series 7 (reconstruct decomposition) and 8 (W decomposition)."""
+    (N7, L7, k7), (N8, L8, k8) = shapes
+    i = {}
+    i["rec"] = R.add_reconstruct(7, N7, [0, 3, 4])
+    i["rec_skip"] = R.add_reconstruct(8, N8, [1, 2, 99])  # out-of-range indices are skipped
+    i["fc"] = R.add_forecast(8, 30, group=[0, 1, 2, 3])
+    i["fc_default"] = R.add_forecast(7, 30)
+    i["cz"] = R.add_cadzow(4, max_iter=5, tol=1e-14, series_id=7, N=N7)
+    return i
+
+
+def test_server_followups_vs_oracle_alone_and_in_mix(gpu, oracle):
+    """RECONSTRUCT(group), FORECAST(group, h) and CADZOW on resident series: results against the
+    oracle on the same decompositions, the same alone and inside a 40-request mix, and no
+    decomposition issued for them (ssa_server_stats.decompositions unchanged)."""
+    rng = np.random.default_rng(31)
+    shapes = [(6000, 1500, 20), (9000, 2250, 16)]
+    xs = [oracle.walk_sines(rng, N) for N, _, _ in shapes]
+    srv = gpu.SSAServer(max_inflight=2, oversampling=P, power_iters=Q)
+    D = gpu.Requests(2)
+    D.add_decompose(xs[0], shapes[0][1], shapes[0][2], series_id=7, seed=77)
+    D.add_decompose(xs[1], shapes[1][1], shapes[1][2], series_id=8, seed=88, wcorr=True)
+    srv.run(D)
+    assert np.all(D.statuses() == 0)
+    st0 = srv.stats()
+    A = gpu.Requests(5)
+    ia = _followups(gpu, A, shapes)
+    srv.run(A)
+    st1 = srv.stats()
+    assert np.all(A.statuses() == 0), A.statuses()
+    assert st1["decompositions"] == st0["decompositions"] and st1["batches"] == st0["batches"]
+    assert st1["followups"] - st0["followups"] == 4 and st1["cadzow_requests"] - st0["cadzow_requests"] == 1
+    d7 = oracle_dec(oracle, xs[0], shapes[0][1], shapes[0][2], 77)
+    d8 = oracle_dec(oracle, xs[1], shapes[1][1], shapes[1][2], 88)
+    (N7, L7, _), (N8, L8, _) = shapes
+    rec = A.result(ia["rec"])["out"]
+    assert rel_l2(rec, oracle.reconstruct(d7, [0, 3, 4], N7, L7)) <= rec_tol(d7.sigma, [0, 3, 4])
+    rec2 = A.result(ia["rec_skip"])["out"]
+    assert rel_l2(rec2, oracle.reconstruct(d8, [1, 2], N8, L8)) <= rec_tol(d8.sigma, [1, 2])
+    fc = A.result(ia["fc"])["forecast"]
+    assert rel_l2(fc, oracle.forecast(d8, [0, 1, 2, 3], 30, N8, L8)) <= FC_TOL
+    fc7 = A.result(ia["fc_default"])["forecast"]
+    assert rel_l2(fc7, oracle.forecast(d7, [0, 1, 2], 30, N7, L7)) <= FC_TOL
+    cz = A.result(ia["cz"])
+    y_ref, it_ref, diff_ref = cadzow_from_factors(oracle, xs[0], d7, L7, 4, 5, 1e-14)
+    assert cz["iterations"] == it_ref
+    assert rel_l2(cz["out"], y_ref) <= 1e-4
+    assert abs(cz["final_diff"] - diff_ref) <= 1e-5
+    # the same follow-ups in the middle of a stream of 40 other requests of mixed size
+    mix = oracle.config3_batch(40, seed=9, nmin=500, nmax=20000)
+    M = gpu.Requests(45)
+    for j, (xj, Lj, kj) in enumerate(mix[:20]):
+        M.add_decompose(xj, Lj, kj, series_id=400 + j, seed=700 + j, wcorr=bool(j % 3 == 0))
+    im = _followups(gpu, M, shapes)
+    for j, (xj, Lj, kj) in enumerate(mix[20:]):
+        M.add_decompose(xj, Lj, kj, series_id=500 + j, seed=800 + j)
+    srv.run(M, np.cumsum(np.full(M.n, 2e-4)))
+    assert np.all(M.statuses() == 0), M.statuses()
+    for key in ("rec", "rec_skip"):
+        assert rel_l2(M.result(im[key])["out"], A.result(ia[key])["out"]) <= 1e-6
+    for key in ("fc", "fc_default"):
+        assert rel_l2(M.result(im[key])["forecast"], A.result(ia[key])["forecast"]) <= 1e-6
+    assert rel_l2(M.result(im["cz"])["out"], cz["out"]) <= 1e-6
+    srv.close()
+
+
+def test_server_cadzow_new_series_and_followup_rejections(gpu, oracle):
+    """CADZOW on a new series (its own signal) equals ssa_opt_cadzow; follow-ups fail on series
+    that are not resident, empty groups, forecast groups with no component, and ranks above k'."""
+    rng = np.random.default_rng(32)
+    x = oracle.walk_sines(rng, 3000)
+    L = 750
+    srv = gpu.SSAServer(max_inflight=1, oversampling=P, power_iters=Q)
+    R = gpu.Requests(8)
+    i_new = R.add_cadzow(5, max_iter=4, tol=1e-14, x=x, L=L)
+    i_dec = R.add_decompose(x, L, 6, series_id=11, seed=5)
+    i_unknown = R.add_reconstruct(4242, 3000, [0])
+    i_empty = R.add_reconstruct(11, 3000, [])
+    i_nocomp = R.add_forecast(11, 10, group=[50, 60])
+    i_rank = R.add_cadzow(7, max_iter=3, series_id=11, N=3000)  # k' = 6
+    i_ok = R.add_reconstruct(11, 3000, [0, 1])
+    srv.run(R)
+    st = R.statuses()
+    assert st[i_new] == 0 and st[i_dec] == 0 and st[i_ok] == 0
+    assert st[i_unknown] == -1 and st[i_empty] == -1 and st[i_nocomp] == -1 and st[i_rank] == -1
+    ref = gpu.cadzow(x, L, 5, max_iter=4, tol=1e-14)
+    r = R.result(i_new)
+    assert r["iterations"] == ref.iterations
+    assert rel_l2(r["out"], ref.signal) <= 1e-6
     srv.close()
