@@ -132,6 +132,13 @@ int ssa_rbatch_run_ex(ssa_rbatch *b, int B, const int *N, const int *L, const in
 int ssa_rbatch_run_device_ex(ssa_rbatch *b, int B, const int *N, const int *L, const int *k, const double *d_x,
                              uint64_t seed, const unsigned char *want_w);
 int ssa_rbatch_sync(ssa_rbatch *b);
+/* Series whose transforms fit one CTA of 512 threads (real FFT lengths 512 .. 16384) share one
+ * bucket whose correlation sweeps are one persistent launch: every CTA pops (series, column
+ * group, length) tiles from a work queue in device memory, longest lengths first, and runs the
+ * columns of shorter lengths side by side. Off (0), every FFT length is a bucket of its own with
+ * one launch per stage. On by default. No counterpart in the reference. */
+void ssa_b200_set_multi_length(int on);
+int ssa_b200_multi_length(void);
 /* Real FFT length an uneven batch (and the server) uses for a series of length N: the smallest
  * of 2^a (a <= 17), 49152 and 98304 that is >= N (at least 32), or -1 beyond N = 131072. The
  * single-series API and the uniform batch use the power of two. No counterpart in the reference

@@ -289,6 +289,97 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k
                              tw);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Multi-length persistent correlation sweep
+// ---------------------------------------------------------------------------------------------
+
+// Points a tile's unused column slots read: none (n = 0), so they load nothing from global memory.
+__device__ __forceinline__ ColPts idle_pts() {
+    ColPts p;
+    p.f32 = nullptr;
+    p.f64 = nullptr;
+    p.sc = 0.f;
+    p.n = 0;
+    p.seed = 0;
+    p.col = 0;
+    return p;
+}
+
+// Shared-memory floats2 of the multi-length kernel: the largest data region over the lengths
+// (2^(13 - logh) padded buffers of H points, largest at the smallest length) plus the twiddle
+// table of the largest length.
+__host__ __device__ constexpr int multi_data_f2() {
+    return (1 << (SSA_MULTI_MAX_LOGH - SSA_MULTI_MIN_LOGH)) * spad_size(1 << SSA_MULTI_MIN_LOGH);
+}
+__host__ __device__ constexpr int multi_smem_f2() { return multi_data_f2() + TwSplit<SSA_MULTI_MAX_LOGH + 1>::N; }
+
+// One tile at length H = 2^LOGH: column slot g of the CTA (threads g T .. g T + T - 1, T = H / 16)
+// runs column c0 + g of the job as k_corr does, in its own padded buffer.
+template <int LOGH>
+__device__ __forceinline__ void corr_tile(float2* smem, const ssa_col_job* __restrict__ Jp, int c0) {
+    const ssa_col_job& J = *Jp;  // fields read where used (no copy held across the transform)
+    constexpr int H = 1 << LOGH;
+    constexpr int T = H / 16;
+    static_assert(512 % T == 0, "whole column slots per CTA");
+    const int g = threadIdx.x / T, tid = threadIdx.x - g * T;
+    const int c = c0 + g;
+    const bool valid = c < J.ncols;
+    float2* s = smem + g * spad_size(H);
+    float2* tw = smem + multi_data_f2();
+    load_twiddles<LOGH + 1>(tw);  // published by the first pass's closing barrier
+    const SmemPts sp{s};
+    fft_passes<LOGH, false, 0>(s, valid ? col_pts(J, c) : idle_pts(), sp, tw, tid);
+    const float2* X = reinterpret_cast<const float2*>(J.X);
+    for (int k = tid; k <= H / 2; k += T) {
+        if (!valid) break;
+        float2 zk, zm;
+        if (k == 0) {
+            const float2 z0 = s[spad(0)];
+            const float2 p0 = cscale(X[0], z0.x + z0.y);
+            const float2 ph = cscale(X[H], z0.x - z0.y);
+            pack_pair(p0, ph, make_float2(1.f, 0.f), zk, zm);
+            s[spad(0)] = zk;
+        } else {
+            const float2 w = wm<LOGH>(tw, k);
+            float2 ak, am;
+            unpack_pair<LOGH>(s[spad(k)], s[spad(H - k)], w, ak, am);
+            const float2 pk = cmulc(X[k], ak);
+            const float2 pm = cmulc(X[H - k], am);
+            pack_pair(pk, pm, w, zk, zm);
+            s[spad(k)] = zk;
+            s[spad(H - k)] = zm;
+        }
+    }
+    __syncthreads();
+    const RealOut ro{valid ? J.out + (long long)c * J.ld_out : nullptr, valid ? J.n_out : 0, 1.0f / (float)H};
+    fft_passes<LOGH, true, 0>(s, sp, ro, tw, tid);
+}
+
+__global__ void __launch_bounds__(512, 2) k_corr_multi(const ssa_col_job* __restrict__ jobs,
+                                                        const ssa_tile* __restrict__ tiles, int ntiles,
+                                                        int* __restrict__ head) {
+    extern __shared__ float2 smem[];
+    __shared__ int s_tile;
+    for (;;) {
+        __syncthreads();  // the previous tile is done with the buffers, the table and s_tile
+        if (threadIdx.x == 0) s_tile = atomicAdd(head, 1);
+        __syncthreads();
+        const int t = s_tile;
+        if (t >= ntiles) return;
+        const ssa_tile T = tiles[t];
+        const ssa_col_job* J = jobs + T.job;
+        switch (T.logh) {
+            case 8: corr_tile<8>(smem, J, T.c0); break;
+            case 9: corr_tile<9>(smem, J, T.c0); break;
+            case 10: corr_tile<10>(smem, J, T.c0); break;
+            case 11: corr_tile<11>(smem, J, T.c0); break;
+            case 12: corr_tile<12>(smem, J, T.c0); break;
+            case 13: corr_tile<13>(smem, J, T.c0); break;
+            default: check_fail(20, 1, (unsigned)T.logh); break;
+        }
+    }
+}
+
 // Elementary reconstruction of component c: x~[t] = inv_w[t] * (sigma_c u_c conv v_c)[t], and
 // norm2[c] = sum_t w[t] x~[t]^2 (w = diagonal count).
 template <int LOGH>
@@ -1658,6 +1749,25 @@ extern "C" int ssad_spectrum(const ssa_col_job* d_jobs, int njobs, int maxcols, 
     SSA_LOGH_DISPATCH(logh, CALL)
 #undef CALL
     return 0;
+}
+extern "C" int ssad_multi_tile_cols(int logh) {
+    return (logh >= SSA_MULTI_MIN_LOGH && logh <= SSA_MULTI_MAX_LOGH) ? 1 << (SSA_MULTI_MAX_LOGH - logh) : 0;
+}
+extern "C" int ssad_corr_multi(const ssa_col_job* d_jobs, const ssa_tile* d_tiles, int ntiles, int* d_head, int nctas,
+                               void* stream) {
+    if (ntiles <= 0) return 0;
+    const int sm = multi_smem_f2() * (int)sizeof(float2);
+    cudaError_t e = set_smem(k_corr_multi, sm);
+    if (e != cudaSuccess) return (int)e;
+    if (nctas <= 0) {
+        int dev = 0, nsm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        nctas = 2 * (nsm > 0 ? nsm : 148);
+    }
+    if (nctas > ntiles) nctas = ntiles;
+    k_corr_multi<<<nctas, 512, sm, (cudaStream_t)stream>>>(d_jobs, d_tiles, ntiles, d_head);
+    return launched(cudaGetLastError());
 }
 extern "C" int ssad_corr(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
     if (njobs <= 0 || maxcols <= 0) return 0;

@@ -301,6 +301,21 @@ int ssad_elem_recon1(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh
 #define SSA_ELEM2_MAX_LOGH 13
 int ssad_spectrum(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);
 int ssad_corr(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);
+/* Correlation sweeps of series of different FFT lengths in one persistent launch: every CTA
+ * (512 threads) pops tiles from tiles[0 .. ntiles) through the counter *head (zero before the
+ * launch), largest lengths first. A tile is (job, first column c0, logh): the CTA runs the columns
+ * c0 .. c0 + 2^(13 - logh) - 1 of that job side by side (those below the job's ncols), each as
+ * k_corr does. logh in [SSA_MULTI_MIN_LOGH, SSA_MULTI_MAX_LOGH]. nctas 0: two per SM. */
+#define SSA_MULTI_MIN_LOGH 8
+#define SSA_MULTI_MAX_LOGH 13
+typedef struct
+{
+    int job, c0, logh, pad_;
+} ssa_tile;
+int ssad_corr_multi(const ssa_col_job *d_jobs, const ssa_tile *d_tiles, int ntiles, int *d_head, int nctas,
+                    void *stream);
+/* Columns one tile of the multi-length sweep covers at logh. */
+int ssad_multi_tile_cols(int logh);
 int ssad_elem_recon(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);
 /* All jobs of one launch share `weighted`. */
 int ssad_gram(const ssa_gram_job *d_jobs, int njobs, int maxchunks, int weighted, void *stream);

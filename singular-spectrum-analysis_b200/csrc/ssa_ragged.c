@@ -52,6 +52,9 @@ typedef struct
     long long ldL, ldK, ldN;
     int rows_L, rows_K, rows_N, nch_L, nch_K, nch_N, nq;
     int rows_W, nch_W; /* W-correlation Gram chunks (tensor-core path: longer chunks) */
+    int code;          /* FFT size code (a multi-length bucket holds several) */
+    long long ldS;     /* floats of its signal spectrum (2 (H + 1) rounded) */
+    size_t oX;         /* offset of its signal spectrum in the bucket's X */
     int wantW;         /* W-correlation requested for this series */
     int nelem;         /* elementary reconstructions computed: k with W, else those the groups use */
     /* follow-up runs: the series' resident factors (U ld ldL, V ld ldK, sigma) and its own group
@@ -69,6 +72,8 @@ typedef struct
     ssa_engine e; /* stream, job arena, profiler */
     int live;
     int logh;
+    int multi; /* series of every size code SSA_MULTI_MIN_LOGH .. SSA_MULTI_MAX_LOGH: the sweeps run
+                  as one persistent launch over (series, column group, length) tiles */
     long long ldS;
     int nb, cap_nb;
     rser *sd;
@@ -126,6 +131,18 @@ __attribute__((constructor)) static void ssar_hw_queues(void) { setenv("CUDA_DEV
 
 static int imin(int a, int b) { return a < b ? a : b; }
 static int imax(int a, int b) { return a > b ? a : b; }
+
+/* Series whose transforms fit one CTA of 512 threads (size codes SSA_MULTI_MIN_LOGH ..
+ * SSA_MULTI_MAX_LOGH) share one bucket whose correlation sweeps are one persistent launch
+ * (ssad_corr_multi); off, every size code is a bucket of its own. */
+static int g_multi = 1;
+void ssa_b200_set_multi_length(int on) { g_multi = on != 0; }
+int ssa_b200_multi_length(void) { return g_multi; }
+
+static int bucket_of(int code)
+{
+    return (g_multi && code >= SSA_MULTI_MIN_LOGH && code <= SSA_MULTI_MAX_LOGH) ? SSA_MULTI_MAX_LOGH : code;
+}
 static long long round4(long long v) { return (v + 3) & ~3LL; }
 
 static int gram_rows(int m, int nb)
@@ -294,11 +311,88 @@ static int bucket_setup(rbucket *b, int logh, int prof)
 
 /* ---- stages ------------------------------------------------------------------------------ */
 
+/* Series of the bucket with size code `code`, in bucket order (all of them for a one-code bucket). */
+static int code_members(const rbucket *b, int code, int *idx)
+{
+    int n = 0;
+    for (int i = 0; i < b->nb; i++)
+        if (b->sd[i].code == code)
+            idx[n++] = i;
+    return n;
+}
+
+/* Launch `launch(jobs, n, code)` once per size code present in the bucket, each with the jobs of
+ * that code's series (one launch for a one-code bucket). jobs holds one job per series. */
+typedef int (*code_launch_fn)(rbucket *b, const void *d_jobs, int n, int maxc, int code);
+static int per_code(rbucket *b, const void *jobs, size_t jsz, const int *maxc_of, code_launch_fn launch)
+{
+    if (!b->multi)
+    {
+        int maxc = 0;
+        for (int i = 0; i < b->nb; i++)
+            maxc = imax(maxc, maxc_of[i]);
+        void *d = ssae_push_jobs(&b->e, jobs, jsz * b->nb);
+        return d ? launch(b, d, b->nb, maxc, b->logh) : (int)cudaErrorMemoryAllocation;
+    }
+    int *idx = (int *)malloc(sizeof(int) * (size_t)b->nb);
+    char *sub = (char *)malloc(jsz * (size_t)b->nb);
+    if (!idx || !sub)
+    {
+        free(idx);
+        free(sub);
+        return (int)cudaErrorMemoryAllocation;
+    }
+    int rc = 0;
+    for (int code = SSA_MULTI_MAX_LOGH; code >= SSA_MULTI_MIN_LOGH && !rc; code--)
+    {
+        const int n = code_members(b, code, idx);
+        if (!n)
+            continue;
+        int maxc = 0;
+        for (int j = 0; j < n; j++)
+        {
+            memcpy(sub + jsz * j, (const char *)jobs + jsz * idx[j], jsz);
+            maxc = imax(maxc, maxc_of[idx[j]]);
+        }
+        void *d = ssae_push_jobs(&b->e, sub, jsz * n);
+        rc = d ? launch(b, d, n, maxc, code) : (int)cudaErrorMemoryAllocation;
+    }
+    free(idx);
+    free(sub);
+    return rc;
+}
+
+static int launch_spectrum_code(rbucket *b, const void *d, int n, int maxc, int code)
+{
+    if (maxc <= 0)
+        return 0;
+    ssae_prof_begin(&b->e, SSAK_SPECTRUM);
+    const int rc = ssad_spectrum((const ssa_col_job *)d, n, maxc, code, b->e.st);
+    ssae_prof_end(&b->e);
+    return rc;
+}
+
+static int launch_elem_code(rbucket *b, const void *d, int n, int maxc, int code)
+{
+    if (maxc <= 0)
+        return 0;
+    ssae_prof_begin(&b->e, SSAK_ELEM);
+    const int rc = code > SSA_ELEM2_MAX_LOGH ? ssad_elem_recon1((const ssa_col_job *)d, n, maxc, code, b->e.st)
+                                             : ssad_elem_recon((const ssa_col_job *)d, n, maxc, code, b->e.st);
+    ssae_prof_end(&b->e);
+    return rc;
+}
+
 static int r_spectrum(rbucket *b, const double *d_x)
 {
     ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)b->nb, sizeof(ssa_col_job));
-    if (!jobs)
+    int *ones = (int *)malloc(sizeof(int) * (size_t)b->nb);
+    if (!jobs || !ones)
+    {
+        free(jobs);
+        free(ones);
         return (int)cudaErrorMemoryAllocation;
+    }
     for (int i = 0; i < b->nb; i++)
     {
         const rser *S = &b->sd[i];
@@ -306,20 +400,17 @@ static int r_spectrum(rbucket *b, const double *d_x)
         J->in64 = d_x + S->ox;
         J->ld_in = S->N;
         J->n_in = S->N;
-        J->spec = b->X + (size_t)i * b->ldS;
-        J->ld_spec = b->ldS;
+        J->spec = b->X + S->oX;
+        J->ld_spec = S->ldS;
         J->ncols = 1;
         J->N = S->N;
         J->L = S->L;
         J->K = S->K;
+        ones[i] = 1;
     }
-    void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_col_job) * b->nb);
+    const int rc = per_code(b, jobs, sizeof(ssa_col_job), ones, launch_spectrum_code);
     free(jobs);
-    if (!d)
-        return (int)cudaErrorMemoryAllocation;
-    ssae_prof_begin(&b->e, SSAK_SPECTRUM);
-    int rc = ssad_spectrum((const ssa_col_job *)d, b->nb, 1, b->logh, b->e.st);
-    ssae_prof_end(&b->e);
+    free(ones);
     return rc;
 }
 
@@ -362,7 +453,7 @@ static int r_sweep(rbucket *b, int adjoint, int generate, unsigned long long see
             J->ld_out = S->ldK;
             J->n_out = S->K;
         }
-        J->X = b->X + (size_t)i * b->ldS;
+        J->X = b->X + S->oX;
         J->ncols = S->kp;
         J->N = S->N;
         J->L = S->L;
@@ -373,6 +464,46 @@ static int r_sweep(rbucket *b, int adjoint, int generate, unsigned long long see
     free(jobs);
     if (!d)
         return (int)cudaErrorMemoryAllocation;
+    if (b->multi)
+    {
+        /* the work queue: (series, column group, length) tiles, longest lengths first, and its
+         * head counter (zero, copied with the tiles) */
+        int nt = 0;
+        for (int i = 0; i < b->nb; i++)
+        {
+            const int g = ssad_multi_tile_cols(b->sd[i].code);
+            nt += (b->sd[i].kp + g - 1) / g;
+        }
+        ssa_tile *tiles = (ssa_tile *)calloc((size_t)nt + 1, sizeof(ssa_tile));
+        if (!tiles)
+            return (int)cudaErrorMemoryAllocation;
+        int t = 0;
+        for (int code = SSA_MULTI_MAX_LOGH; code >= SSA_MULTI_MIN_LOGH; code--)
+            for (int i = 0; i < b->nb; i++)
+            {
+                const rser *S = &b->sd[i];
+                if (S->code != code)
+                    continue;
+                const int g = ssad_multi_tile_cols(code);
+                for (int c0 = 0; c0 < S->kp; c0 += g)
+                {
+                    tiles[t].job = i;
+                    tiles[t].c0 = c0;
+                    tiles[t].logh = code;
+                    t++;
+                }
+            }
+        /* tiles[nt] is the zeroed counter slot */
+        void *dt = ssae_push_jobs(&b->e, tiles, sizeof(ssa_tile) * ((size_t)nt + 1));
+        free(tiles);
+        if (!dt)
+            return (int)cudaErrorMemoryAllocation;
+        ssae_prof_begin(&b->e, SSAK_CORR);
+        int rc = ssad_corr_multi((const ssa_col_job *)d, (const ssa_tile *)dt, nt, (int *)((ssa_tile *)dt + nt),
+                                 0, b->e.st);
+        ssae_prof_end(&b->e);
+        return rc;
+    }
     ssae_prof_begin(&b->e, SSAK_CORR);
     int rc = ssad_corr((const ssa_col_job *)d, b->nb, maxc, b->logh, b->e.st);
     ssae_prof_end(&b->e);
@@ -572,11 +703,28 @@ static int r_rr(rbucket *b, double *sigma, int *status)
 
 static int r_elem(rbucket *b, const double *sigma)
 {
-    const int one = b->logh > SSA_ELEM2_MAX_LOGH;
+    const int one = b->logh > SSA_ELEM2_MAX_LOGH; /* one-code buckets only: multi-length codes are <= 13 */
     ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)b->nb, sizeof(ssa_col_job));
-    if (!jobs)
+    int *ncols = (int *)malloc(sizeof(int) * (size_t)b->nb);
+    if (!jobs || !ncols)
+    {
+        free(jobs);
+        free(ncols);
         return (int)cudaErrorMemoryAllocation;
+    }
     int maxk = 0;
+    for (int i = 0; i < b->nb; i++)
+    {
+        ncols[i] = b->sd[i].nelem;
+        maxk = imax(maxk, ncols[i]);
+    }
+    if (maxk == 0)
+    {
+        free(jobs);
+        free(ncols);
+        return 0;
+    }
+    int rc = 0;
     if (one)
     {
         /* spectra of sigma_i u_i first; the reconstruction kernel then holds one FFT buffer */
@@ -589,32 +737,13 @@ static int r_elem(rbucket *b, const double *sigma)
             J->n_in = S->L;
             J->scale = S->sx ? S->sx : sigma + S->osig;
             J->spec = b->Us + S->ospec;
-            J->ld_spec = b->ldS;
+            J->ld_spec = S->ldS;
             J->ncols = S->nelem;
-            maxk = imax(maxk, S->nelem);
         }
-        if (maxk == 0)
-        {
-            free(jobs);
-            return 0;
-        }
-        void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_col_job) * b->nb);
-        if (!d)
-        {
-            free(jobs);
-            return (int)cudaErrorMemoryAllocation;
-        }
-        ssae_prof_begin(&b->e, SSAK_SPECTRUM);
-        int rc = ssad_spectrum((const ssa_col_job *)d, b->nb, maxk, b->logh, b->e.st);
-        ssae_prof_end(&b->e);
-        if (rc)
-        {
-            free(jobs);
-            return rc;
-        }
+        rc = per_code(b, jobs, sizeof(ssa_col_job), ncols, launch_spectrum_code);
         memset(jobs, 0, sizeof(ssa_col_job) * b->nb);
     }
-    for (int i = 0; i < b->nb; i++)
+    for (int i = 0; i < b->nb && !rc; i++)
     {
         const rser *S = &b->sd[i];
         ssa_col_job *J = &jobs[i];
@@ -635,23 +764,13 @@ static int r_elem(rbucket *b, const double *sigma)
         if (one)
         {
             J->spec = b->Us + S->ospec;
-            J->ld_spec = b->ldS;
+            J->ld_spec = S->ldS;
         }
-        maxk = imax(maxk, S->nelem);
     }
-    if (maxk == 0)
-    {
-        free(jobs);
-        return 0;
-    }
-    void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_col_job) * b->nb);
+    if (!rc)
+        rc = per_code(b, jobs, sizeof(ssa_col_job), ncols, launch_elem_code);
     free(jobs);
-    if (!d)
-        return (int)cudaErrorMemoryAllocation;
-    ssae_prof_begin(&b->e, SSAK_ELEM);
-    int rc = one ? ssad_elem_recon1((const ssa_col_job *)d, b->nb, maxk, b->logh, b->e.st)
-                 : ssad_elem_recon((const ssa_col_job *)d, b->nb, maxk, b->logh, b->e.st);
-    ssae_prof_end(&b->e);
+    free(ncols);
     return rc;
 }
 
@@ -846,7 +965,7 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
     }
     int count[RB_NB] = {0};
     for (int s = 0; s < B; s++)
-        count[ssad_fft_code_for(N[s])]++;
+        count[bucket_of(ssad_fft_code_for(N[s]))]++;
     for (int g = 0; g < RB_NB; g++)
         if (count[g] > 65535) /* the job index is blockIdx.y in the column kernels */
             return -1;
@@ -858,6 +977,7 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
             continue;
         if (bucket_setup(b, g, rb->prof) != 0)
             return -1;
+        b->multi = bucket_of(SSA_MULTI_MIN_LOGH) == g && g_multi;
         if (count[g] > b->cap_nb)
         {
             rser *sd = (rser *)realloc(b->sd, sizeof(rser) * count[g]);
@@ -871,10 +991,13 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
     size_t ox = 0, osig = 0, oW = 0, ogrp = 0;
     for (int s = 0; s < B; s++)
     {
-        rbucket *b = &rb->bk[ssad_fft_code_for(N[s])];
+        const int code = ssad_fft_code_for(N[s]);
+        rbucket *b = &rb->bk[bucket_of(code)];
         rser *S = &b->sd[b->nb++];
         memset(S, 0, sizeof(*S));
         S->src = s;
+        S->code = code;
+        S->ldS = round4(2LL * (ssad_fft_h(code) + 1) + 2);
         S->N = N[s];
         S->L = L[s];
         S->K = N[s] - L[s] + 1;
@@ -915,7 +1038,7 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
         rbucket *b = &rb->bk[g];
         if (!b->nb)
             continue;
-        size_t oY = 0, oZ = 0, opart = 0, oqsum = 0, oR = 0, oZu = 0, orecon = 0, onorm = 0, ospec = 0;
+        size_t oY = 0, oZ = 0, opart = 0, oqsum = 0, oR = 0, oZu = 0, orecon = 0, onorm = 0, ospec = 0, oX = 0;
         for (int i = 0; i < b->nb; i++)
         {
             rser *S = &b->sd[i];
@@ -942,6 +1065,8 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
             S->orecon = orecon;
             S->onorm = onorm;
             S->ospec = ospec;
+            S->oX = oX;
+            oX += (size_t)S->ldS;
             oY += (size_t)S->ldL * S->kp;
             oZ += (size_t)S->ldK * S->kp;
             opart += (size_t)imax(S->nch_L, imax(S->nch_K, S->nch_N)) * S->kp * (S->kp + 1) / 2;
@@ -950,14 +1075,17 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
             oZu += (size_t)S->kp * S->k;
             orecon += (size_t)S->nelem * S->ldN;
             onorm += (size_t)S->k;
-            ospec += (size_t)S->nelem * b->ldS;
+            ospec += (size_t)S->nelem * S->ldS;
         }
         /* one run pushes 13 + 6 q job tables of at most sizeof(ssa_col_job) bytes per series,
-         * each 16-byte aligned */
-        const size_t arena = ((size_t)b->nb * sizeof(ssa_col_job) + 16) * (size_t)(16 + 6 * rb->q) + (1 << 16);
+         * each 16-byte aligned (a multi-length bucket pushes the per-code stages in up to six
+         * parts, and a tile table of at most 64 tiles per series per sweep) */
+        size_t arena = ((size_t)b->nb * sizeof(ssa_col_job) + 16 * 6) * (size_t)(16 + 6 * rb->q) + (1 << 16);
+        if (b->multi)
+            arena += (size_t)(2 * rb->q + 2) * ((size_t)SSA_MAX_KP * b->nb + 2) * sizeof(ssa_tile);
         if (ssae_grow_arena(&b->e, arena) != 0)
             return -1;
-        b->sz[0] = (size_t)b->nb * b->ldS * sizeof(float); /* X */
+        b->sz[0] = oX * sizeof(float); /* X */
         b->sz[1] = oY * sizeof(float);
         b->sz[2] = oZ * sizeof(float);
         b->sz[3] = opart * sizeof(double);

@@ -60,6 +60,7 @@ typedef struct res_entry
     double *sig, *x;
     float *U, *V;
     size_t bytes;
+    size_t aoff; /* offset in the resident arena, or SIZE_MAX when from the pool */
     struct res_entry *prev, *next; /* LRU list, most recent first */
     struct res_entry *hnext;
 } res_entry;
@@ -170,6 +171,14 @@ struct ssa_server
     int device;
     ssa_server_stats stats;
     uslot_t us;
+    /* resident arena (explicit budget): one device allocation of res_budget bytes, entries carved
+     * first-fit from a sorted list of free spans (no driver call per entry) */
+    char *res_arena;
+    struct rspan
+    {
+        size_t off, len;
+    } *spans;
+    int nspans, cspans;
     /* Cadzow worker: its own thread, queue and wake-up */
     pthread_t cz_th;
     int cz_live, cz_stop;
@@ -294,6 +303,69 @@ static void lru_front(ssa_server *s, res_entry *e)
         s->lru_tail = e;
 }
 
+#define RA_ALIGN ((size_t)256)
+#define RA_NONE ((size_t)-1)
+
+/* First fit over the free spans (sorted by offset). */
+static size_t ra_alloc(ssa_server *s, size_t bytes)
+{
+    bytes = (bytes + RA_ALIGN - 1) & ~(RA_ALIGN - 1);
+    for (int i = 0; i < s->nspans; i++)
+        if (s->spans[i].len >= bytes)
+        {
+            const size_t off = s->spans[i].off;
+            s->spans[i].off += bytes;
+            s->spans[i].len -= bytes;
+            if (s->spans[i].len == 0)
+            {
+                memmove(&s->spans[i], &s->spans[i + 1], sizeof(s->spans[0]) * (size_t)(s->nspans - i - 1));
+                s->nspans--;
+            }
+            return off;
+        }
+    return RA_NONE;
+}
+
+/* Return a span, merging it with its neighbours. */
+static void ra_free(ssa_server *s, size_t off, size_t bytes)
+{
+    bytes = (bytes + RA_ALIGN - 1) & ~(RA_ALIGN - 1);
+    int i = 0;
+    while (i < s->nspans && s->spans[i].off < off)
+        i++;
+    const int merge_prev = i > 0 && s->spans[i - 1].off + s->spans[i - 1].len == off;
+    const int merge_next = i < s->nspans && off + bytes == s->spans[i].off;
+    if (merge_prev && merge_next)
+    {
+        s->spans[i - 1].len += bytes + s->spans[i].len;
+        memmove(&s->spans[i], &s->spans[i + 1], sizeof(s->spans[0]) * (size_t)(s->nspans - i - 1));
+        s->nspans--;
+    }
+    else if (merge_prev)
+        s->spans[i - 1].len += bytes;
+    else if (merge_next)
+    {
+        s->spans[i].off = off;
+        s->spans[i].len += bytes;
+    }
+    else
+    {
+        if (s->nspans == s->cspans)
+        {
+            const int c = s->cspans ? 2 * s->cspans : 1024;
+            void *a = realloc(s->spans, sizeof(s->spans[0]) * (size_t)c);
+            if (!a)
+                return; /* the span is lost to the arena: a leak of space, never an overlap */
+            s->spans = a;
+            s->cspans = c;
+        }
+        memmove(&s->spans[i + 1], &s->spans[i], sizeof(s->spans[0]) * (size_t)(s->nspans - i));
+        s->spans[i].off = off;
+        s->spans[i].len = bytes;
+        s->nspans++;
+    }
+}
+
 static void res_remove(ssa_server *s, res_entry *e)
 {
     res_entry **pp = &s->htab[(unsigned)e->id % (unsigned)s->hcap];
@@ -302,7 +374,9 @@ static void res_remove(ssa_server *s, res_entry *e)
     if (*pp)
         *pp = e->hnext;
     lru_unlink(s, e);
-    if (e->d)
+    if (e->d && e->aoff != RA_NONE)
+        ra_free(s, e->aoff, e->bytes);
+    else if (e->d)
         cudaFreeAsync(e->d, s->pool_st);
     s->res_bytes -= e->bytes;
     free(e);
@@ -372,11 +446,32 @@ static int res_alloc(ssa_server *s, res_entry *e)
     const size_t bytes = sizeof(double) * nd + sizeof(float) * (size_t)(e->ldL + e->ldK) * (size_t)e->k;
     if (res_make_room(s, bytes) != 0)
         return -1;
-    cudaMemPool_t pool = ssar_pool();
-    if (!pool || cudaMallocFromPoolAsync((void **)&e->d, bytes, pool, s->pool_st) != cudaSuccess)
+    e->aoff = RA_NONE;
+    if (s->res_arena)
     {
-        e->d = NULL;
-        return -1;
+        /* evict further least recently used idle series while fragmentation leaves no span */
+        size_t off;
+        while ((off = ra_alloc(s, bytes)) == RA_NONE)
+        {
+            res_entry *v = s->lru_tail;
+            while (v && (v->refs > 0 || v->state == RES_PENDING || v == e))
+                v = v->prev;
+            if (!v)
+                return -1;
+            res_remove(s, v);
+            s->stats.evictions++;
+        }
+        e->aoff = off;
+        e->d = (double *)(s->res_arena + off);
+    }
+    else
+    {
+        cudaMemPool_t pool = ssar_pool();
+        if (!pool || cudaMallocFromPoolAsync((void **)&e->d, bytes, pool, s->pool_st) != cudaSuccess)
+        {
+            e->d = NULL;
+            return -1;
+        }
     }
     e->sig = e->d + 2 * (size_t)(e->L - 1) + 1;
     e->x = e->sig + e->k;
@@ -1474,6 +1569,26 @@ int ssa_server_create(ssa_server **out, size_t hbm_budget_bytes, int max_infligh
         }
         f->cap = max_batch;
     }
+    if (reserve)
+    {
+        /* the resident share of the budget up front: entries are carved from it */
+        if (cudaMalloc((void **)&s->res_arena, s->res_budget) != cudaSuccess)
+        {
+            s->res_arena = NULL;
+            ssa_server_destroy(s);
+            return -1;
+        }
+        s->cspans = 1024;
+        s->spans = malloc(sizeof(s->spans[0]) * (size_t)s->cspans);
+        if (!s->spans)
+        {
+            ssa_server_destroy(s);
+            return -1;
+        }
+        s->spans[0].off = 0;
+        s->spans[0].len = s->res_budget & ~(RA_ALIGN - 1);
+        s->nspans = 1;
+    }
     {
         /* follow-up batches: one group slot (each series brings its own group) */
         static const int one_idx[1] = {0}, one_size[1] = {1};
@@ -1645,6 +1760,9 @@ void ssa_server_destroy(ssa_server *s)
             res_remove(s, s->lru_head);
         free(s->htab);
     }
+    if (s->res_arena)
+        cudaFree(s->res_arena);
+    free(s->spans);
     if (s->pool_st)
     {
         cudaStreamSynchronize(s->pool_st);

@@ -775,6 +775,16 @@ _sig("ssa_rbatch_set_profiling", _I, ctypes.c_void_p, _I)
 _sig("ssa_rbatch_profile", _I, ctypes.c_void_p, c_double_p, ctypes.POINTER(ctypes.c_longlong), _I)
 
 
+def set_multi_length(on: bool) -> None:
+    """Series of real FFT length 512..16384 in one persistent multi-length sweep launch (default)
+    or one bucket per length."""
+    _lib.ssa_b200_set_multi_length(1 if on else 0)
+
+
+def multi_length() -> bool:
+    return bool(_lib.ssa_b200_multi_length())
+
+
 class SSARaggedBatch:
     """Uneven batch (ssa_rbatch_* C ABI): series of different N, L and k through decomposition,
     all elementary reconstructions, W-correlation and the sums of ``groups`` in one pass, one
@@ -933,6 +943,8 @@ class _ServerStats(ctypes.Structure):
                                                   "cadzow_iterations")]
 
 
+_sig("ssa_b200_set_multi_length", _V, _I)
+_sig("ssa_b200_multi_length", _I)
 _sig("ssa_rbatch_series_result", _I, ctypes.c_void_p, _I, c_double_p, c_double_p, c_double_p, c_double_p,
      c_double_p)
 _sig("ssa_server_create", _I, ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t, _I, _I, _I, _I)
