@@ -71,6 +71,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-uniform", action="store_true")
+    ap.add_argument("--no-config4", action="store_true")
     ap.add_argument("--no-rates", action="store_true")
     ap.add_argument("--accuracy", type=int, default=64, help="series of the timed batch checked against the FP64 "
                                                               "oracle after the run (0: none)")
@@ -658,6 +659,54 @@ def uniform_batch(gpu, torch, a, B: int = 4096, N: int = 10000, L: int = 2500, k
                         "reconstructions + W-correlation + groups [0],[1,2]; inputs resident in HBM"}
 
 
+def config4(gpu, torch, a, I: int = 64, M: int = 16, N: int = 20000, L: int = 5000, k: int = 50,
+            iters: int = 10) -> dict:
+    """The multichannel workload: I instances of M correlated channels (random mixings of 4 shared
+    sinusoids + trend + noise at SNR 5 dB), block power of each stacked (M L) x K operator (one
+    block of kp columns, q subspace iterations) and `iters` multivariate Cadzow iterations of rank
+    k, all instances in one batch; inputs resident in HBM."""
+    import ssa_oracle
+
+    rng = np.random.default_rng(3)
+    X = np.stack([ssa_oracle.config4_instance(rng, Mch=M, N=N) for _ in range(I)])
+    d_x = torch.from_numpy(X).to("cuda")
+    d_out = torch.empty_like(d_x)
+    mb = gpu.SSAMultiBatch(I, M, N, L, k, oversampling=a.p, power_iters=a.q)
+    stream = torch.cuda.ExternalStream(mb.stream)
+    mb.run_device(d_x.data_ptr(), 1, seed=7, d_out_ptr=d_out.data_ptr())  # warm-up: buffers, spectra
+    mb.sync()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = gpu.kernel_launches()
+    e0.record(stream)
+    mb.run_device(d_x.data_ptr(), iters, seed=7, d_out_ptr=d_out.data_ptr())
+    e1.record(stream)
+    mb.sync()
+    ms = e0.elapsed_time(e1)
+    diff = mb.diffs(iters)
+    K = N - L + 1
+    kp, kk = mb.kp, mb.k
+    # algorithmic FP32 bytes of one Cadzow iteration of one instance: the block sweeps
+    # ((2 q + 3) kp columns of the K + M L rows), the factors written and read, the M channels in
+    # and out
+    per_iter = 4 * ((2 * a.q + 3) * kp * (K + M * L) + 2 * kk * (K + M * L) + 2 * M * N)
+    total = per_iter * I * iters
+    peak, peak_kind = measured_peak_hbm()
+    achieved = total / (ms / 1e3) / 1e9
+    out = {"value": I / (ms / 1e3), "unit": "instances/s", "ms_per_instance": ms / I, "ms": ms,
+           "ms_per_cadzow_iteration": ms / iters, "launches": gpu.kernel_launches() - launches0,
+           "final_rel_change": {"median": float(np.median(diff[:, -1])), "max": float(diff[:, -1].max())},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_source": peak_kind, "algorithmic_bytes": total,
+                        "what": "4 [(2q+3) kp (K + M L) + 2 k (K + M L) + 2 M N] bytes per instance per Cadzow "
+                                "iteration / whole-run CUDA-event time"},
+           "workload": f"{I} instances x {M} channels, N={N}, L={L}, rank {kk}, block of kp={kp} columns, q={a.q} "
+                       f"subspace iterations per projection, {iters} Cadzow iterations; inputs resident in HBM"}
+    del mb, d_x, d_out
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     a = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -719,6 +768,8 @@ def main():
             line["e2e_over_plain"] = line["e2e"]["value"] / line["plain_gpu_path"]["value"]
     if rank == 0 and world == 1 and not a.no_uniform:
         line["uniform_batch"] = uniform_batch(ssa_gpu, torch, a)
+    if rank == 0 and world == 1 and not a.no_config4:
+        line["config4"] = config4(ssa_gpu, torch, a)
     if rank == 0 and world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_reference(a, budget_s=20.0)
     acc_jobs, fc_jobs = dev.pop("acc_jobs", []), line.pop("fc_jobs", [])

@@ -139,6 +139,18 @@ int ssa_rbatch_sync(ssa_rbatch *b);
  * one launch per stage. On by default. No counterpart in the reference. */
 void ssa_b200_set_multi_length(int on);
 int ssa_b200_multi_length(void);
+/* Launch parameters of the uneven batches chosen per FFT-length bucket (the autotuner of
+ * ssa_tune.py measures candidates and sets them; 0 keeps the built-in heuristic):
+ * gram_ctas[code] the CTA count the Gram partial launches of the bucket with size code `code`
+ * aim at (n entries, codes as ssa_b200_fft_size_code), multi_ctas_per_sm the CTAs per SM of the
+ * persistent multi-length sweep (1 or 2). Host state of the process; returns 0 / -1. get returns
+ * the number of size codes. No counterpart in the reference. */
+int ssa_b200_tune_set(const int *gram_ctas, int n, int multi_ctas_per_sm);
+int ssa_b200_tune_get(int *gram_ctas, int n, int *multi_ctas_per_sm);
+/* Size code of the FFT length for a series of length N (the bucket index the tuning table uses):
+ * log2 of the complex length for powers of two, other values for the mixed lengths; -1 beyond
+ * N = 131072. */
+int ssa_b200_fft_size_code(int N);
 /* Real FFT length an uneven batch (and the server) uses for a series of length N: the smallest
  * of 2^a (a <= 17), 49152 and 98304 that is >= N (at least 32), or -1 beyond N = 131072. The
  * single-series API and the uniform batch use the power of two. No counterpart in the reference
@@ -160,6 +172,46 @@ int ssa_rbatch_series_result(ssa_rbatch *b, int s, double *sigma, double *W, dou
  * buckets' work), 2 the same with the buckets run one after another (isolated launch times). */
 int ssa_rbatch_set_profiling(ssa_rbatch *b, int on);
 int ssa_rbatch_profile(ssa_rbatch *b, double *ms, long long *launches, int nkinds);
+/* CUDA graphs of whole runs (on by default): when a run has the launch signature of the previous
+ * run (the same shapes, per-series options, input and buffer addresses; the generator seed may
+ * differ, it is read from device memory) the run is captured as one graph of all buckets'
+ * launches and copies, and later runs with that signature replay it after restoring the job
+ * tables into the staging areas: one launch call instead of one per stage per bucket. Up to four
+ * graphs per batch, least recently used replaced. Profiling runs never use graphs. */
+int ssa_rbatch_set_graphs(ssa_rbatch *b, int on);
+int ssa_rbatch_graph_stats(const ssa_rbatch *b, long long *captures, long long *replays);
+
+/* ---- Batched multichannel SSA with Cadzow iterations --------------------------------------------
+ * I independent instances of M channels of length N each (the stacked (M L) x K trajectory
+ * operator of MKL/ssa_opt.h:3880-4283 per instance), all processed together, and `iters`
+ * multivariate Cadzow iterations (the reference's ssa_opt_cadzow loop, MKL/ssa_opt.h:3165-3290,
+ * applied to the stacked operator: rank-k projection, then every channel replaced by its
+ * reconstruction from the k components). Each projection is a block power decomposition of the
+ * instance's stacked operator: one block of kp = min(k + p, M L, K) columns from the device
+ * generator (instance seed: seed ^ 0x9E3779B97F4A7C15 (i + 1), the same every iteration),
+ * power_iters subspace iterations with CholQR of the stacked block after every half step, and a
+ * Rayleigh-Ritz step. Channel data is instance-major: channel m of instance i at (i M + m) N.
+ * No counterpart in the reference (whose MSSA is randomized only and whose Cadzow is one channel).
+ * Returns 0 / -1. */
+typedef struct ssa_mbatch ssa_mbatch;
+int ssa_mbatch_create(ssa_mbatch **out, int I, int M, int N, int L, int k, int oversampling, int power_iters);
+void ssa_mbatch_destroy(ssa_mbatch *b);
+/* Device input d_X (I M N doubles); enqueues only. d_out: the channels after the iterations (I M
+ * N), d_sigma: each instance's k singular values of the last projection (I x k); either may be
+ * NULL. */
+int ssa_mbatch_run_device(ssa_mbatch *b, const double *d_X, int iters, uint64_t seed, double *d_out,
+                          double *d_sigma);
+/* Waits for the run; 0 when every instance's decompositions succeeded. */
+int ssa_mbatch_sync(ssa_mbatch *b);
+/* Relative change of every iteration: diff[i iters + t] = ||y_t - y_{t-1}|| / ||x|| over the M
+ * channels of instance i (y_{-1} = x). Waits for the run. */
+int ssa_mbatch_diffs(ssa_mbatch *b, int iters, double *diff);
+/* Host-to-host run (out, sigma, diff as above, host arrays, any may be NULL). */
+int ssa_mbatch_run(ssa_mbatch *b, const double *X, int iters, uint64_t seed, double *out, double *sigma,
+                   double *diff);
+/* Components k and block columns kp the batch computes; its stream. */
+int ssa_mbatch_dims(const ssa_mbatch *b, int *k, int *kp);
+void *ssa_mbatch_stream(const ssa_mbatch *b);
 
 /* ---- Request server ------------------------------------------------------------------------
  * Continuous batching of mixed-size requests on one GPU (no counterpart in the reference, whose

@@ -754,6 +754,30 @@ def cadzow_inplace(x: np.ndarray, L: int, rank: int, max_iter: int, tol: float,
     return y_new, it, diff, converged, y
 
 
+def mssa_cadzow(X: np.ndarray, L: int, rank: int, iters: int, oversampling: int, omega: np.ndarray,
+                q: int) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Multivariate Cadzow iterations on one instance X (M x N): each iteration projects the stacked
+    (M L) x K trajectory operator of the current channels onto its leading `rank` components (the
+    decomposition of mssa_decompose with the given K x kp start block `omega` and q subspace
+    iterations, the same block every iteration, as the reference's fresh contexts restart their
+    generator) and replaces every channel by its reconstruction (mssa_reconstruct of 0..rank-1),
+    the reference's Cadzow loop (ssa_opt.h:3165-3290) applied to the multichannel operator
+    (ssa_opt.h:3880-4283). Returns (channels, sigma of the last projection, relative change
+    ||y_t - y_{t-1}|| / ||X|| per iteration)."""
+    X = np.asarray(X, dtype=np.float64)
+    Mch, N = X.shape
+    xn = float(np.linalg.norm(X)) or 1.0
+    y = X.copy()
+    diffs = []
+    d = None
+    for _ in range(iters):
+        d = mssa_decompose(y, L, rank, oversampling, omega, q=q)
+        yn = np.stack([mssa_reconstruct(d, m, list(range(d.k)), Mch, N, L) for m in range(Mch)])
+        diffs.append(float(np.linalg.norm(yn - y)) / xn)
+        y = yn
+    return y, d.sigma.copy(), np.array(diffs)
+
+
 # ---------------------------------------------------------------------------------------------
 # Synthetic workloads (seeded). Signals first, then Omega, from one numpy Generator (PCG64).
 # ---------------------------------------------------------------------------------------------

@@ -19,7 +19,8 @@ INCLUDE = HERE.parent / "include"
 OUT = HERE / "libssa.so"
 BUILD = HERE / "_build"
 
-C_SOURCES = ["ssa_engine.c", "ssa_api.c", "ssa_batch.c", "ssa_mssa.c", "ssa_ragged.c", "ssa_server.c"]
+C_SOURCES = ["ssa_engine.c", "ssa_api.c", "ssa_batch.c", "ssa_mssa.c", "ssa_ragged.c", "ssa_server.c",
+             "ssa_mbatch.c"]
 CU_SOURCES = ["ssa_kernels.cu"]
 
 NVCC_FLAGS = [

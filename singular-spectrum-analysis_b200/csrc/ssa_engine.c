@@ -1173,6 +1173,211 @@ static int mssa_adjoint(ssa_engine *e, int M, int n)
     return ssad_slabsum(e->Z, e->Z, (long long)sZ, M, (long long)e->ldK * n, e->st);
 }
 
+/* ---- I instances of M channels (series i M .. i M + M - 1 of the engine are instance i) ---- */
+
+/* Stacked CholQR of every instance: the Gram partials of its M channels are contiguous, so one
+ * Cholesky job per instance sums all of them; every channel then takes its instance's R^{-1}. */
+static int mssab_cholqr(ssa_engine *e, int I, int M, int n, double *colsum)
+{
+    const int B = I * M;
+    const size_t sY = (size_t)e->ldL * e->kp;
+    const int nch = (e->L + e->rows_L - 1) / e->rows_L;
+    const size_t np = (size_t)n * (n + 1) / 2;
+    CK(gram_ps(e, B, e->Y, sY, e->ldL, e->L, n, e->rows_L, 0, (size_t)nch * np));
+    ssa_chol_job *cj = (ssa_chol_job *)calloc((size_t)I, sizeof(ssa_chol_job));
+    ssa_rowmul_job *rj = (ssa_rowmul_job *)calloc((size_t)B, sizeof(ssa_rowmul_job));
+    if (!cj || !rj)
+    {
+        free(cj);
+        free(rj);
+        return (int)cudaErrorMemoryAllocation;
+    }
+    for (int i = 0; i < I; i++)
+    {
+        cj[i].part = e->part + (size_t)i * M * nch * np;
+        cj[i].Rinv = e->Rinv + (size_t)i * e->kp * e->kp;
+        cj[i].status = e->status + i;
+        cj[i].nchunks = M * nch;
+        cj[i].n = n;
+    }
+    const int nqb = (e->L + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS;
+    for (int c = 0; c < B; c++)
+    {
+        ssa_rowmul_job *J = &rj[c];
+        J->A = e->Y + (size_t)c * sY;
+        J->C = e->Y + (size_t)c * sY;
+        J->Bm64 = e->Rinv + (size_t)(c / M) * e->kp * e->kp;
+        J->colsum = colsum ? colsum + (size_t)c * nqb * n : NULL;
+        J->lda = e->ldL;
+        J->ldc = e->ldL;
+        J->m = e->L;
+        J->n = n;
+        J->p = n;
+        J->ldb = n;
+    }
+    void *dc = ssae_push_jobs(e, cj, sizeof(ssa_chol_job) * I);
+    void *dr = dc ? ssae_push_jobs(e, rj, sizeof(ssa_rowmul_job) * B) : NULL;
+    free(cj);
+    free(rj);
+    if (!dc || !dr)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_CHOL);
+    int rc = ssad_chol((const ssa_chol_job *)dc, I, e->st);
+    ssae_prof_end(e);
+    CK(rc);
+    ssae_prof_begin(e, SSAK_ROWMUL);
+    rc = ssad_rowmul((const ssa_rowmul_job *)dr, B, e->L, n, e->st);
+    ssae_prof_end(e);
+    return rc;
+}
+
+/* Z_{i M} = sum_m H_{i,m}^T Y_{i,m} for every instance (per-channel adjoints into their Z slots,
+ * then a fixed-order channel sum per instance into its first channel's slot). */
+static int mssab_adjoint(ssa_engine *e, int I, int M, int n)
+{
+    const size_t sY = (size_t)e->ldL * e->kp, sZ = (size_t)e->ldK * e->kp;
+    CK(corr_io(e, I * M, n, 1, e->Y, sY, e->ldL, e->Z, sZ, e->ldK));
+    return ssad_slabsum_batch(e->Z, e->Z, (long long)sZ, M, (long long)e->ldK * n, I, (long long)M * sZ, e->st);
+}
+
+/* Y_{i,m} = H_{i,m} Z_{i M}: every channel of an instance reads the instance's block. */
+static int mssab_forward(ssa_engine *e, int I, int M, int n)
+{
+    const size_t sY = (size_t)e->ldL * e->kp, sZ = (size_t)e->ldK * e->kp;
+    const int B = I * M;
+    ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)B, sizeof(ssa_col_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    for (int c = 0; c < B; c++)
+    {
+        ssa_col_job *J = &jobs[c];
+        J->in = e->Z + (size_t)(c / M) * M * sZ;
+        J->ld_in = e->ldK;
+        J->n_in = e->K;
+        J->out = e->Y + (size_t)c * sY;
+        J->ld_out = e->ldL;
+        J->n_out = e->L;
+        J->X = e->X + (size_t)c * e->ldS;
+        J->ncols = n;
+        J->N = e->N;
+        J->L = e->L;
+        J->K = e->K;
+    }
+    void *d = ssae_push_jobs(e, jobs, sizeof(ssa_col_job) * B);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_CORR);
+    int rc = ssad_corr((const ssa_col_job *)d, B, n, e->logh, e->st);
+    ssae_prof_end(e);
+    return rc;
+}
+
+int ssae_mssa_batch_decompose(ssa_engine *e, int I, int M, int kp, int k, int q, unsigned long long seed)
+{
+    const int B = I * M;
+    if (I < 1 || M < 1 || B > e->B || kp < 1 || kp > e->kp || k < 1 || k > imin(kp, e->k))
+        return (int)cudaErrorInvalidValue;
+    const size_t sY = (size_t)e->ldL * e->kp, sZ = (size_t)e->ldK * e->kp;
+    const int K = e->K;
+    CK(cudaMemsetAsync(e->status, 0, sizeof(int) * I, e->st));
+    /* start block of instance i (the device generator, seed mixed with the instance) in Z_{i M} */
+    for (int i = 0; i < I; i++)
+        CK(ssad_gaussian(e->Z + (size_t)i * M * sZ, e->ldK, K, kp, 0,
+                         seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1)), e->st));
+    CK(mssab_forward(e, I, M, kp));
+    for (int it = 0; it < q; it++)
+    {
+        CK(mssab_cholqr(e, I, M, kp, NULL));
+        CK(mssab_adjoint(e, I, M, kp));
+        CK(cholqr_pass(e, I, e->Z, (size_t)M * sZ, e->ldK, K, kp, e->rows_K, NULL));
+        CK(mssab_forward(e, I, M, kp));
+    }
+    CK(mssab_cholqr(e, I, M, kp, NULL));
+    CK(mssab_cholqr(e, I, M, kp, e->qsum));
+    CK(mssab_adjoint(e, I, M, kp));
+    /* Rayleigh-Ritz per instance on B_i = Z_{i M} (its Gram partials at part + i * nchmax * np) */
+    CK(gram(e, I, e->Z, (size_t)M * sZ, e->ldK, K, kp, e->rows_K, 0));
+    {
+        const int nchmax = imax(e->nch_L, imax(e->nch_K, e->nch_N));
+        const size_t np = (size_t)e->kp * (e->kp + 1) / 2;
+        const int nqb = (e->L + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS;
+        ssa_rr_job *J = (ssa_rr_job *)calloc((size_t)I, sizeof(ssa_rr_job));
+        if (!J)
+            return (int)cudaErrorMemoryAllocation;
+        for (int i = 0; i < I; i++)
+        {
+            J[i].part = e->part + (size_t)i * nchmax * np;
+            J[i].qsum = e->qsum + (size_t)i * M * nqb * kp;
+            J[i].sigma = e->sigma + (size_t)i * M * e->k;
+            J[i].Zu = e->Zu + (size_t)i * e->kp * e->k;
+            J[i].Zv = e->Zv + (size_t)i * e->kp * e->k;
+            J[i].status = e->status + i;
+            J[i].nchunks = (K + e->rows_K - 1) / e->rows_K;
+            J[i].nchunks_q = M * nqb;
+            J[i].kp = kp;
+            J[i].k = k;
+        }
+        void *d = ssae_push_jobs(e, J, sizeof(ssa_rr_job) * I);
+        free(J);
+        if (!d)
+            return (int)cudaErrorMemoryAllocation;
+        ssae_prof_begin(e, SSAK_RR);
+        int rc = ssad_rr((const ssa_rr_job *)d, I, e->st);
+        ssae_prof_end(e);
+        CK(rc);
+    }
+    /* U_{i,m} = Q_{i,m} Zu_i for every channel; V_i = B_i Zv_i */
+    {
+        ssa_rowmul_job *rj = (ssa_rowmul_job *)calloc((size_t)(B + I), sizeof(ssa_rowmul_job));
+        if (!rj)
+            return (int)cudaErrorMemoryAllocation;
+        for (int c = 0; c < B; c++)
+        {
+            ssa_rowmul_job *R = &rj[c];
+            R->A = e->Y + (size_t)c * sY;
+            R->C = e->Y + (size_t)c * sY;
+            R->Bm = e->Zu + (size_t)(c / M) * e->kp * e->k;
+            R->lda = R->ldc = e->ldL;
+            R->m = e->L;
+            R->n = kp;
+            R->p = k;
+            R->ldb = kp;
+        }
+        void *d = ssae_push_jobs(e, rj, sizeof(ssa_rowmul_job) * B);
+        if (!d)
+        {
+            free(rj);
+            return (int)cudaErrorMemoryAllocation;
+        }
+        ssae_prof_begin(e, SSAK_ROWMUL);
+        int rc = ssad_rowmul((const ssa_rowmul_job *)d, B, e->L, kp, e->st);
+        ssae_prof_end(e);
+        CK(rc);
+        for (int i = 0; i < I; i++)
+        {
+            ssa_rowmul_job *R = &rj[B + i];
+            R->A = e->Z + (size_t)i * M * sZ;
+            R->C = e->Z + (size_t)i * M * sZ;
+            R->Bm = e->Zv + (size_t)i * e->kp * e->k;
+            R->lda = R->ldc = e->ldK;
+            R->m = K;
+            R->n = kp;
+            R->p = k;
+            R->ldb = kp;
+        }
+        d = ssae_push_jobs(e, rj + B, sizeof(ssa_rowmul_job) * I);
+        free(rj);
+        if (!d)
+            return (int)cudaErrorMemoryAllocation;
+        ssae_prof_begin(e, SSAK_ROWMUL);
+        rc = ssad_rowmul((const ssa_rowmul_job *)d, I, K, kp, e->st);
+        ssae_prof_end(e);
+        CK(rc);
+    }
+    return 0;
+}
+
 int ssae_mssa_decompose(ssa_engine *e, int M, int kp, int k, int q, const float *d_omega, unsigned long long seed)
 {
     if (M < 1 || M > e->B || kp < 1 || kp > e->kp || k < 1 || k > imin(kp, e->k))

@@ -145,6 +145,12 @@ int ssae_extend(ssa_engine *e, int k_old, int k_new, int max_iter, unsigned long
  * test matrix (ld ldK) or NULL for the generator with `seed`. Results: U_m in Y_m (L x k per
  * channel), V in every Z_m, sigma in series 0's slot. */
 int ssae_mssa_decompose(ssa_engine *e, int M, int kp, int k, int q, const float *d_omega, unsigned long long seed);
+/* Block power of I stacked operators at once (series i M .. i M + M - 1 are the M channels of
+ * instance i): subspace iteration of one block of kp columns from a generated Gaussian start
+ * (instance seed: seed ^ golden (i + 1)), q iterations, CholQR of the stacked block after every
+ * half step, Rayleigh-Ritz on the last adjoint. Results: U_{i,m} in channel (i, m)'s Y slot,
+ * V_i in channel (i, 0)'s Z slot, sigma_i at sigma + i M k, status per instance. */
+int ssae_mssa_batch_decompose(ssa_engine *e, int I, int M, int kp, int k, int q, unsigned long long seed);
 /* Grouped reconstruction of series s from cached spectra into d_out (double, N). */
 int ssae_recon_group(ssa_engine *e, int s, int k, const int *d_group, int n_group, double *d_out);
 

@@ -59,6 +59,8 @@ static inline int launched(cudaError_t e) {
 }
 
 extern "C" unsigned long long ssad_launch_count(void) { return g_launches.load(); }
+// Kernels launched by a CUDA-graph replay (the launches the graph captured).
+extern "C" void ssad_count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 // ---------------------------------------------------------------------------------------------
 // Device-side helpers
@@ -173,7 +175,7 @@ __device__ __forceinline__ ColPts col_pts(const ssa_col_job& J, int c) {
     p.f64 = (!J.in && J.in64) ? J.in64 + (long long)c * J.ld_in : nullptr;
     p.sc = (J.in && J.scale) ? (float)J.scale[c] : 1.0f;
     p.n = J.n_in;
-    p.seed = J.seed;
+    p.seed = J.seedp ? *J.seedp : J.seed;
     p.col = J.col0 + c;
     return p;
 }
@@ -213,11 +215,12 @@ __device__ __forceinline__ void load_column(float2* s, const ssa_col_job& J, int
     } else {
         const int n = J.n_in;
         const int col = J.col0 + c;
+        const unsigned long long seed = J.seedp ? *J.seedp : J.seed;
         for (int i = threadIdx.x; i < H; i += blockDim.x) {
             const int r = 2 * i;
             float2 v = make_float2(0.f, 0.f);
             if (r < n) {
-                v = gauss_pair(J.seed, col, i);
+                v = gauss_pair(seed, col, i);
                 if (r + 1 >= n) v.y = 0.f;
             }
             s[spad(i)] = v;
@@ -1432,7 +1435,10 @@ __global__ void k_permcols(const ssa_permcols_job* __restrict__ jobs) {
 // Small elementwise / reduction kernels (MSSA channel sums, contributions, Cadzow)
 // ---------------------------------------------------------------------------------------------
 
-__global__ void k_slabsum(float* out, const float* in, long long stride, int nslab, long long n) {
+__global__ void k_slabsum(float* out, const float* in, long long stride, int nslab, long long n, long long inst_stride) {
+    // instance blockIdx.y: its nslab slabs start at in + y * inst_stride, its sum at out + y * inst_stride
+    out += (long long)blockIdx.y * inst_stride;
+    in += (long long)blockIdx.y * inst_stride;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         float acc = 0.f;
         for (int sl = 0; sl < nslab; ++sl) acc += in[(long long)sl * stride + i];
@@ -1451,6 +1457,10 @@ __global__ void k_colnorm2(const float* A, long long sstride, long long ld, int 
 }
 
 __global__ void k_diffnorm(const double* a, const double* b, long long n, double* out2) {
+    // one CTA per vector: vector blockIdx.x at a + x n, b + x n, its two sums at out2 + 2 x
+    a += (long long)blockIdx.x * n;
+    b += (long long)blockIdx.x * n;
+    out2 += 2 * (long long)blockIdx.x;
     __shared__ double red[32];
     double d2 = 0.0, a2 = 0.0;
     for (long long i = threadIdx.x; i < n; i += blockDim.x) {
@@ -1905,11 +1915,16 @@ extern "C" int ssad_permcols(const ssa_permcols_job* d_jobs, int njobs, int maxr
     return launched(cudaGetLastError());
 }
 
-extern "C" int ssad_slabsum(float* out, const float* in, long long stride, int nslab, long long n, void* stream) {
-    if (n <= 0 || nslab <= 0) return 0;
+extern "C" int ssad_slabsum_batch(float* out, const float* in, long long stride, int nslab, long long n, int ninst,
+                                  long long inst_stride, void* stream) {
+    if (n <= 0 || nslab <= 0 || ninst <= 0) return 0;
     const long long blocks = (n + 255) / 256;
-    k_slabsum<<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0, (cudaStream_t)stream>>>(out, in, stride, nslab, n);
+    const unsigned bx = (unsigned)(blocks < 4096 ? blocks : 4096);
+    k_slabsum<<<dim3(bx, (unsigned)ninst), 256, 0, (cudaStream_t)stream>>>(out, in, stride, nslab, n, inst_stride);
     return launched(cudaGetLastError());
+}
+extern "C" int ssad_slabsum(float* out, const float* in, long long stride, int nslab, long long n, void* stream) {
+    return ssad_slabsum_batch(out, in, stride, nslab, n, 1, 0, stream);
 }
 
 extern "C" int ssad_colnorm2(const float* A, long long sstride, long long ld, int m, int k, int nb, double* out,
@@ -1933,6 +1948,12 @@ extern "C" int ssad_copy_segments(const ssa_copy_seg* d_segs, int nseg, void* st
 
 extern "C" int ssad_diffnorm(const double* a, const double* b, long long n, double* out2, void* stream) {
     k_diffnorm<<<1, 1024, 0, (cudaStream_t)stream>>>(a, b, n, out2);
+    return launched(cudaGetLastError());
+}
+extern "C" int ssad_diffnorm_batch(const double* a, const double* b, long long n, int nvec, double* out2,
+                                   void* stream) {
+    if (nvec <= 0 || n <= 0) return 0;
+    k_diffnorm<<<nvec, 1024, 0, (cudaStream_t)stream>>>(a, b, n, out2);
     return launched(cudaGetLastError());
 }
 

@@ -59,6 +59,7 @@ typedef struct
     int n_in, n_out, ncols, n_in2;
     int col0;             /* first generated column index (RNG counter offset) */
     int N, L, K;          /* series dims, used for the diagonal-averaging weights */
+    const unsigned long long *seedp; /* device: the generator seed, read at run time (NULL: seed) */
 } ssa_col_job;
 
 /* Gram job: part[chunk] = A_chunk^T W A_chunk (n x n, FP64) over rows of A (m x n, ld). */
@@ -259,10 +260,16 @@ int ssad_sortsign(const ssa_sortsign_job *d_jobs, int njobs, void *stream);
 int ssad_permcols(const ssa_permcols_job *d_jobs, int njobs, int maxrows, void *stream);
 /* out[i] = sum_{s < nslab} in[s * stride + i] for i < n (fixed order; out may alias slab 0). */
 int ssad_slabsum(float *out, const float *in, long long stride, int nslab, long long n, void *stream);
+/* The same for ninst instances: instance j sums its nslab slabs at in + j * inst_stride into
+ * out + j * inst_stride. */
+int ssad_slabsum_batch(float *out, const float *in, long long stride, int nslab, long long n, int ninst,
+                       long long inst_stride, void *stream);
 /* out[s * k + j] = sum_r A[s][r][j]^2 (FP64) for nb column blocks A_s = A + s * sstride (m x k, ld). */
 int ssad_colnorm2(const float *A, long long sstride, long long ld, int m, int k, int nb, double *out, void *stream);
 /* out2[0] = sum (a - b)^2, out2[1] = sum a^2 over n doubles (FP64, one CTA, fixed order). */
 int ssad_diffnorm(const double *a, const double *b, long long n, double *out2, void *stream);
+/* The same for nvec vectors of n doubles laid end to end: out2[2 v], out2[2 v + 1]. */
+int ssad_diffnorm_batch(const double *a, const double *b, long long n, int nvec, double *out2, void *stream);
 /* Segment copies dst[i] = src[i], i < n, one CTA per segment: dst may be page-locked host memory
  * mapped into the device address space, so one launch writes many small outputs straight to the
  * host instead of one copy call each. */
@@ -343,6 +350,8 @@ int ssad_gaussian(float *out, long long ld, int rows, int ncols, int col0, unsig
 /* Read (and optionally reset) the device self-check record {violations, kernel, block, code,
  * value} of the current device. */
 int ssad_read_checks(unsigned int *out5, int reset);
+/* Add n kernel launches to the count (a CUDA-graph replay launches the kernels it captured). */
+void ssad_count_launches(unsigned long long n);
 /* Count of kernel launches issued by this library since load (all devices). */
 unsigned long long ssad_launch_count(void);
 

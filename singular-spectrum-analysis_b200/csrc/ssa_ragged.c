@@ -112,6 +112,23 @@ struct ssa_rbatch
     int lrf_slot, n_lrf_group, lrf_gmax;
     int *d_lrf_group;
     int *lrf_status;
+    /* CUDA graphs of whole runs: a run whose launch signature was also the previous run's is
+     * captured, and later runs with that signature replay the graph (job tables restored into
+     * the staging areas, seeds through d_seeds) */
+    struct rgraph
+    {
+        unsigned long long sig, stamp;
+        unsigned long long kernels; /* kernel launches the graph holds */
+        cudaGraphExec_t exec;
+        char *snap[RB_NB];
+        size_t snap_n[RB_NB];
+    } graphs[4];
+    unsigned long long last_sig, gstamp;
+    int graphs_on, graph_pending;
+    cudaEvent_t ev_graph;
+    long long n_captures, n_replays;
+    unsigned long long *h_seeds, *d_seeds;
+    size_t c_seeds;
     /* follow-up runs (ssar_run_followup): given factors, per-series groups, no decomposition */
     int followup;
     const float *const *fu_U, *const *fu_V;
@@ -139,16 +156,55 @@ static int g_multi = 1;
 void ssa_b200_set_multi_length(int on) { g_multi = on != 0; }
 int ssa_b200_multi_length(void) { return g_multi; }
 
+struct rgraph;
+static void graph_free(struct rgraph *g);
+
 static int bucket_of(int code)
 {
     return (g_multi && code >= SSA_MULTI_MIN_LOGH && code <= SSA_MULTI_MAX_LOGH) ? SSA_MULTI_MAX_LOGH : code;
 }
 static long long round4(long long v) { return (v + 3) & ~3LL; }
 
-static int gram_rows(int m, int nb)
+/* Per-bucket launch parameters chosen by the autotuner (0 = the built-in heuristic): the CTA count
+ * the Gram partial launches aim at for each FFT size code, and the CTAs per SM of the persistent
+ * multi-length sweep. Host state only; set through ssa_b200_tune_set. */
+static struct
 {
-    /* about 1184 CTAs (eight per SM) over the bucket's series */
-    int target = 1184 / (nb > 0 ? nb : 1);
+    int gram_ctas[RB_NB];
+    int multi_ctas_per_sm;
+} g_tune;
+
+int ssa_b200_tune_set(const int *gram_ctas, int n, int multi_ctas_per_sm)
+{
+    if (n < 0 || n > RB_NB || multi_ctas_per_sm < 0 || multi_ctas_per_sm > 2)
+        return -1;
+    for (int i = 0; i < RB_NB; i++)
+    {
+        const int v = (gram_ctas && i < n) ? gram_ctas[i] : 0;
+        if (v < 0 || v > 65536)
+            return -1;
+        g_tune.gram_ctas[i] = v;
+    }
+    g_tune.multi_ctas_per_sm = multi_ctas_per_sm;
+    return 0;
+}
+
+int ssa_b200_tune_get(int *gram_ctas, int n, int *multi_ctas_per_sm)
+{
+    for (int i = 0; i < n && i < RB_NB; i++)
+        gram_ctas[i] = g_tune.gram_ctas[i];
+    if (multi_ctas_per_sm)
+        *multi_ctas_per_sm = g_tune.multi_ctas_per_sm;
+    return RB_NB;
+}
+
+/* Rows per Gram partial for a block of m rows in a bucket of nb series with FFT size code
+ * `code` (code < 0: the heuristic). */
+static int gram_rows_for(int m, int nb, int code)
+{
+    /* about 1184 CTAs (eight per SM) over the bucket's series, or the tuned count */
+    const int ctas = (code >= 0 && code < RB_NB && g_tune.gram_ctas[code] > 0) ? g_tune.gram_ctas[code] : 1184;
+    int target = ctas / (nb > 0 ? nb : 1);
     if (target < 1)
         target = 1;
     int rows = (m + target - 1) / target;
@@ -157,6 +213,8 @@ static int gram_rows(int m, int nb)
      * (their latency) when a launch holds few series */
     return imax(rows, 4 * SSA_GRAM_CHUNK);
 }
+
+static int gram_rows(int m, int nb) { return gram_rows_for(m, nb, -1); }
 
 /* The library's stream-ordered memory pool on the current device: freed blocks stay cached in
  * it (release threshold at its maximum), so re-growing buffers costs no driver allocation. */
@@ -234,6 +292,14 @@ void ssa_rbatch_destroy(ssa_rbatch *rb)
             cudaFree(bufs[i]);
     if (rb->ev_in)
         cudaEventDestroy(rb->ev_in);
+    for (int i = 0; i < 4; i++)
+        graph_free(&rb->graphs[i]);
+    if (rb->ev_graph)
+        cudaEventDestroy(rb->ev_graph);
+    if (rb->h_seeds)
+        cudaFreeHost(rb->h_seeds);
+    if (rb->d_seeds)
+        cudaFree(rb->d_seeds);
     if (rb->main)
         cudaStreamDestroy(rb->main);
     free(rb->h_off);
@@ -256,8 +322,10 @@ int ssa_rbatch_create(ssa_rbatch **out, int oversampling, int power_iters, const
     rb->p = oversampling <= 0 ? 8 : oversampling;
     rb->q = power_iters;
     rb->n_groups = n_groups;
+    rb->graphs_on = 1;
     if (ssad_init_device() != 0 || cudaStreamCreateWithFlags(&rb->main, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&rb->ev_in, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&rb->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&rb->ev_graph, cudaEventDisableTiming) != cudaSuccess)
     {
         ssa_rbatch_destroy(rb);
         return -1;
@@ -416,7 +484,7 @@ static int r_spectrum(rbucket *b, const double *d_x)
 
 /* adjoint 0: Y = H (Omega | Z); adjoint 1: Z = H^T Y. generate: Omega from the device generator,
  * series seed seeds[src] when given, else seed mixed with the batch position. */
-static int r_sweep(rbucket *b, int adjoint, int generate, unsigned long long seed, const unsigned long long *seeds)
+static int r_sweep(rbucket *b, int adjoint, int generate, const unsigned long long *d_seeds)
 {
     ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)b->nb, sizeof(ssa_col_job));
     if (!jobs)
@@ -432,7 +500,7 @@ static int r_sweep(rbucket *b, int adjoint, int generate, unsigned long long see
             if (generate)
             {
                 J->in = NULL;
-                J->seed = seeds ? seeds[S->src] : seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(S->src + 1));
+                J->seedp = d_seeds + S->src; /* read by the kernel: job tables stay run-invariant */
             }
             else
             {
@@ -499,8 +567,16 @@ static int r_sweep(rbucket *b, int adjoint, int generate, unsigned long long see
         if (!dt)
             return (int)cudaErrorMemoryAllocation;
         ssae_prof_begin(&b->e, SSAK_CORR);
+        int nctas = 0;
+        if (g_tune.multi_ctas_per_sm > 0)
+        {
+            int dev = 0, nsm = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            nctas = g_tune.multi_ctas_per_sm * nsm;
+        }
         int rc = ssad_corr_multi((const ssa_col_job *)d, (const ssa_tile *)dt, nt, (int *)((ssa_tile *)dt + nt),
-                                 0, b->e.st);
+                                 nctas, b->e.st);
         ssae_prof_end(&b->e);
         return rc;
     }
@@ -887,17 +963,17 @@ static int r_lrf(rbucket *b, ssa_rbatch *rb)
 static int bucket_run(rbucket *b, ssa_rbatch *rb, const double *d_x, unsigned long long seed)
 {
     CK(r_spectrum(b, d_x));
-    CK(r_sweep(b, 0, 1, seed, rb->cur_seeds));
+    CK(r_sweep(b, 0, 1, rb->d_seeds));
     for (int it = 0; it < rb->q; it++)
     {
         CK(r_cholqr(b, SIDE_L, 0, rb->status));
-        CK(r_sweep(b, 1, 0, 0, NULL));
+        CK(r_sweep(b, 1, 0, NULL));
         CK(r_cholqr(b, SIDE_K, 0, rb->status));
-        CK(r_sweep(b, 0, 0, 0, NULL));
+        CK(r_sweep(b, 0, 0, NULL));
     }
     CK(r_cholqr(b, SIDE_L, 0, rb->status));
     CK(r_cholqr(b, SIDE_L, 1, rb->status));
-    CK(r_sweep(b, 1, 0, 0, NULL));
+    CK(r_sweep(b, 1, 0, NULL));
     CK(r_gram(b, SIDE_K));
     CK(r_rr(b, rb->sigma, rb->status));
     CK(r_rowmul(b, SIDE_L, 0, 0));
@@ -921,6 +997,8 @@ static int bucket_followup(rbucket *b, ssa_rbatch *rb)
         CK(r_lrf(b, rb));
     return 0;
 }
+
+int ssa_b200_fft_size_code(int N) { return N >= 1 ? ssad_fft_code_for(N) : -1; }
 
 int ssa_b200_fft_length(int N)
 {
@@ -1045,9 +1123,9 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
             S->ldL = round4(S->L);
             S->ldK = round4(S->K);
             S->ldN = round4(S->N);
-            S->rows_L = gram_rows(S->L, b->nb);
-            S->rows_K = gram_rows(S->K, b->nb);
-            S->rows_N = gram_rows(S->N, b->nb);
+            S->rows_L = gram_rows_for(S->L, b->nb, g);
+            S->rows_K = gram_rows_for(S->K, b->nb, g);
+            S->rows_N = gram_rows_for(S->N, b->nb, g);
             S->nch_L = (S->L + S->rows_L - 1) / S->rows_L;
             S->nch_K = (S->K + S->rows_K - 1) / S->rows_K;
             S->nch_N = (S->N + S->rows_N - 1) / S->rows_N;
@@ -1177,6 +1255,12 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
 static int quiesce(ssa_rbatch *rb)
 {
     int rc = 0;
+    if (rb->graph_pending)
+    {
+        /* the graph's copy nodes read the staging areas and the seeds when they execute */
+        rc |= cudaEventSynchronize(rb->ev_graph) != cudaSuccess;
+        rb->graph_pending = 0;
+    }
     for (int g = 0; g < RB_NB; g++)
         if (rb->bk[g].live)
         {
@@ -1195,13 +1279,14 @@ static int ensure_hoff(ssa_rbatch *rb, int B)
     return 0;
 }
 
-/* Enqueue a run whose packed input d_x is ready at the main stream's current position. */
-static int run_enqueue(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k, const double *d_x,
-                       unsigned long long seed)
+/* The work of a run after plan(): seeds, output clears, every bucket's pipeline on its stream,
+ * joined back into the main stream. */
+static int enqueue_body(ssa_rbatch *rb, int B, const double *d_x, unsigned long long seed)
 {
-    if (ensure_hoff(rb, B) != 0 || plan(rb, B, N, L, k) != 0)
+    if (!rb->followup &&
+        cudaMemcpyAsync(rb->d_seeds, rb->h_seeds, sizeof(unsigned long long) * B, cudaMemcpyHostToDevice, rb->main) !=
+            cudaSuccess)
         return -1;
-    rb->B = B;
     if (rb->cur_wmask && rb->n_W > 0 &&
         cudaMemsetAsync(rb->W, 0, sizeof(double) * rb->n_W, rb->main) != cudaSuccess)
         return -1;
@@ -1225,6 +1310,181 @@ static int run_enqueue(ssa_rbatch *rb, int B, const int *N, const int *L, const 
             return -1;
         prev = b->done;
     }
+    return 0;
+}
+
+/* FNV-1a over the bytes of everything a captured run bakes in: shapes, per-series options,
+ * device addresses (input, arena, job tables, seeds) and the global switches. */
+static unsigned long long fnv(unsigned long long h, const void *p, size_t n)
+{
+    const unsigned char *c = (const unsigned char *)p;
+    for (size_t i = 0; i < n; i++)
+        h = (h ^ c[i]) * 0x100000001B3ull;
+    return h;
+}
+
+static unsigned long long run_signature(const ssa_rbatch *rb, int B, const int *N, const int *L, const int *k,
+                                        const double *d_x)
+{
+    unsigned long long h = 0xCBF29CE484222325ull;
+    const int head[8] = {B, rb->p, rb->q, rb->n_groups, rb->lrf_slot, rb->n_lrf_group, g_multi, ssad_wcorr_tc()};
+    h = fnv(h, head, sizeof(head));
+    h = fnv(h, N, sizeof(int) * B);
+    h = fnv(h, L, sizeof(int) * B);
+    h = fnv(h, k, sizeof(int) * B);
+    const void *ptrs[4] = {d_x, rb->arena, rb->d_seeds, rb->d_lrf_group};
+    h = fnv(h, ptrs, sizeof(ptrs));
+    for (int s = 0; s < B; s++)
+    {
+        const unsigned char w = rb->cur_wmask ? rb->cur_wmask[s] : 1;
+        const void *lp = rb->cur_lrf ? (const void *)rb->cur_lrf[s] : NULL;
+        h = fnv(h, &w, 1);
+        h = fnv(h, &lp, sizeof(lp));
+    }
+    for (int g = 0; g < RB_NB; g++)
+        if (rb->bk[g].nb)
+        {
+            const void *jd = rb->bk[g].e.ja.d;
+            h = fnv(h, &g, sizeof(g));
+            h = fnv(h, &jd, sizeof(jd));
+        }
+    return h;
+}
+
+static void graph_free(struct rgraph *g)
+{
+    if (g->exec)
+        cudaGraphExecDestroy(g->exec);
+    for (int i = 0; i < RB_NB; i++)
+        free(g->snap[i]);
+    memset(g, 0, sizeof(*g));
+}
+
+/* replay != 0: the graph's kernels join the launch count (a capture counted them already). */
+static int graph_launch(ssa_rbatch *rb, struct rgraph *g, int replay)
+{
+    g->stamp = ++rb->gstamp;
+    if (replay)
+        ssad_count_launches(g->kernels);
+    if (cudaGraphLaunch(g->exec, rb->main) != cudaSuccess || cudaEventRecord(rb->ev_graph, rb->main) != cudaSuccess)
+        return -1;
+    rb->graph_pending = 1;
+    return 0;
+}
+
+/* Enqueue a run whose packed input d_x is ready at the main stream's current position. */
+static int run_enqueue(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k, const double *d_x,
+                       unsigned long long seed)
+{
+    if (ensure_hoff(rb, B) != 0 || plan(rb, B, N, L, k) != 0)
+        return -1;
+    rb->B = B;
+    if (!rb->followup)
+    {
+        if ((size_t)B > rb->c_seeds)
+        {
+            if (rb->h_seeds)
+                cudaFreeHost(rb->h_seeds);
+            if (rb->d_seeds)
+                cudaFree(rb->d_seeds);
+            rb->h_seeds = NULL;
+            rb->d_seeds = NULL;
+            rb->c_seeds = 0;
+            const size_t c = (size_t)B + (size_t)B / 2 + 64;
+            if (cudaMallocHost((void **)&rb->h_seeds, sizeof(unsigned long long) * c) != cudaSuccess ||
+                cudaMalloc((void **)&rb->d_seeds, sizeof(unsigned long long) * c) != cudaSuccess)
+                return -1;
+            rb->c_seeds = c;
+        }
+        for (int s = 0; s < B; s++)
+            rb->h_seeds[s] = rb->cur_seeds ? rb->cur_seeds[s]
+                                           : seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(s + 1));
+    }
+    const int use = rb->graphs_on && !rb->prof && !rb->followup;
+    const unsigned long long sig = use ? run_signature(rb, B, N, L, k, d_x) : 0;
+    if (use)
+        for (int i = 0; i < 4; i++)
+        {
+            struct rgraph *g = &rb->graphs[i];
+            if (!g->exec || g->sig != sig)
+                continue;
+            /* replay: the job tables of the captured run back into the staging areas */
+            for (int b = 0; b < RB_NB; b++)
+                if (g->snap_n[b])
+                {
+                    memcpy(rb->bk[b].e.ja.h, g->snap[b], g->snap_n[b]);
+                    rb->bk[b].e.ja.used = g->snap_n[b];
+                }
+            rb->n_replays++;
+            return graph_launch(rb, g, 1);
+        }
+    const int capture = use && sig == rb->last_sig;
+    rb->last_sig = sig;
+    if (!capture)
+        return enqueue_body(rb, B, d_x, seed);
+    if (cudaStreamBeginCapture(rb->main, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+        return -1;
+    const unsigned long long k0 = ssad_launch_count();
+    const int rc = enqueue_body(rb, B, d_x, seed);
+    const unsigned long long nk = ssad_launch_count() - k0;
+    cudaGraph_t graph = NULL;
+    const cudaError_t ec = cudaStreamEndCapture(rb->main, &graph);
+    cudaGraphExec_t exec = NULL;
+    if (rc != 0 || ec != cudaSuccess || !graph || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+    {
+        if (graph)
+            cudaGraphDestroy(graph);
+        cudaGetLastError();
+        /* nothing of the captured work ran: run it directly, and leave graphs off for this batch */
+        rb->graphs_on = 0;
+        for (int b = 0; b < RB_NB; b++)
+            rb->bk[b].e.ja.used = 0;
+        return enqueue_body(rb, B, d_x, seed);
+    }
+    cudaGraphDestroy(graph);
+    int slot = 0;
+    for (int i = 1; i < 4; i++)
+        if (rb->graphs[i].stamp < rb->graphs[slot].stamp)
+            slot = i;
+    struct rgraph *g = &rb->graphs[slot];
+    graph_free(g);
+    g->sig = sig;
+    g->exec = exec;
+    g->kernels = nk;
+    for (int b = 0; b < RB_NB; b++)
+    {
+        const size_t n = rb->bk[b].nb ? rb->bk[b].e.ja.used : 0;
+        if (n && (g->snap[b] = (char *)malloc(n)) != NULL)
+        {
+            memcpy(g->snap[b], rb->bk[b].e.ja.h, n);
+            g->snap_n[b] = n;
+        }
+        else if (n)
+        {
+            graph_free(g);
+            return -1;
+        }
+    }
+    rb->n_captures++;
+    return graph_launch(rb, g, 0);
+}
+
+int ssa_rbatch_set_graphs(ssa_rbatch *rb, int on)
+{
+    if (!rb)
+        return -1;
+    rb->graphs_on = on != 0;
+    return 0;
+}
+
+int ssa_rbatch_graph_stats(const ssa_rbatch *rb, long long *captures, long long *replays)
+{
+    if (!rb)
+        return -1;
+    if (captures)
+        *captures = rb->n_captures;
+    if (replays)
+        *replays = rb->n_replays;
     return 0;
 }
 

@@ -903,6 +903,15 @@ class SSARaggedBatch:
             raise RuntimeError("ssa_rbatch_device_results failed")
         return {"sigma": r.sigma, "W": r.W, "groups": r.groups, "status": r.status, "stream": r.stream}
 
+    def set_graphs(self, on: bool) -> None:
+        """CUDA-graph capture and replay of runs with a repeated launch signature (default on)."""
+        _lib.ssa_rbatch_set_graphs(self._h, 1 if on else 0)
+
+    def graph_stats(self) -> dict:
+        c, r = ctypes.c_longlong(), ctypes.c_longlong()
+        _lib.ssa_rbatch_graph_stats(self._h, ctypes.byref(c), ctypes.byref(r))
+        return {"captures": c.value, "replays": r.value}
+
     def series_result(self, s: int, N: int, L: int, k: int, factors: bool = False) -> dict:
         """Outputs of series s of the last run (waits for it): sigma, W, groups and, with
         factors=True, U (L x k') and V (K x k')."""
@@ -920,6 +929,70 @@ class SSARaggedBatch:
         if factors:
             out["U"], out["V"] = U.T, V.T
         return out
+
+
+_sig("ssa_mbatch_create", _I, ctypes.POINTER(ctypes.c_void_p), _I, _I, _I, _I, _I, _I, _I)
+_sig("ssa_mbatch_destroy", _V, ctypes.c_void_p)
+_sig("ssa_mbatch_run_device", _I, ctypes.c_void_p, ctypes.c_void_p, _I, ctypes.c_uint64, ctypes.c_void_p,
+     ctypes.c_void_p)
+_sig("ssa_mbatch_sync", _I, ctypes.c_void_p)
+_sig("ssa_mbatch_diffs", _I, ctypes.c_void_p, _I, c_double_p)
+_sig("ssa_mbatch_run", _I, ctypes.c_void_p, c_double_p, _I, ctypes.c_uint64, c_double_p, c_double_p, c_double_p)
+_sig("ssa_mbatch_dims", _I, ctypes.c_void_p, c_int_p, c_int_p)
+_sig("ssa_mbatch_stream", ctypes.c_void_p, ctypes.c_void_p)
+
+
+class SSAMultiBatch:
+    """Batched multichannel SSA with Cadzow iterations (ssa_mbatch_* C ABI): I instances of M
+    channels of length N, block power of every stacked operator and `iters` multivariate Cadzow
+    iterations, all instances together."""
+
+    def __init__(self, instances: int, M: int, N: int, L: int, k: int, oversampling: int = 10,
+                 power_iters: int = 2):
+        self.I, self.M, self.N, self.L = instances, M, N, L
+        self._h = ctypes.c_void_p()
+        if _lib.ssa_mbatch_create(ctypes.byref(self._h), instances, M, N, L, k, oversampling, power_iters) != 0:
+            raise ValueError("ssa_mbatch_create failed")
+        kk, kp = ctypes.c_int(), ctypes.c_int()
+        _lib.ssa_mbatch_dims(self._h, ctypes.byref(kk), ctypes.byref(kp))
+        self.k, self.kp = kk.value, kp.value
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.ssa_mbatch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def run(self, X: np.ndarray, iters: int, seed: int = 0):
+        """X: (I, M, N). Returns (channels after the iterations (I, M, N), sigma (I, k), relative
+        change per iteration (I, iters))."""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        if X.shape != (self.I, self.M, self.N):
+            raise ValueError(f"X must have shape {(self.I, self.M, self.N)}")
+        out = np.zeros_like(X)
+        sig = np.zeros((self.I, self.k))
+        diff = np.zeros((self.I, iters))
+        if _lib.ssa_mbatch_run(self._h, _dp(X), iters, seed, _dp(out), _dp(sig), _dp(diff)) != 0:
+            raise RuntimeError("ssa_mbatch_run failed")
+        return out, sig, diff
+
+    def run_device(self, d_x_ptr: int, iters: int, seed: int = 0, d_out_ptr: int = 0, d_sigma_ptr: int = 0) -> None:
+        if _lib.ssa_mbatch_run_device(self._h, ctypes.c_void_p(d_x_ptr), iters, seed,
+                                      ctypes.c_void_p(d_out_ptr or None), ctypes.c_void_p(d_sigma_ptr or None)) != 0:
+            raise RuntimeError("ssa_mbatch_run_device failed")
+
+    def sync(self) -> None:
+        if _lib.ssa_mbatch_sync(self._h) != 0:
+            raise RuntimeError("an instance of the multichannel batch failed")
+
+    def diffs(self, iters: int) -> np.ndarray:
+        d = np.zeros((self.I, iters))
+        if _lib.ssa_mbatch_diffs(self._h, iters, _dp(d)) != 0:
+            raise RuntimeError("ssa_mbatch_diffs failed")
+        return d
+
+    @property
+    def stream(self) -> int:
+        return int(_lib.ssa_mbatch_stream(self._h) or 0)
 
 
 class _Request(ctypes.Structure):
@@ -945,6 +1018,8 @@ class _ServerStats(ctypes.Structure):
 
 _sig("ssa_b200_set_multi_length", _V, _I)
 _sig("ssa_b200_multi_length", _I)
+_sig("ssa_rbatch_set_graphs", _I, ctypes.c_void_p, _I)
+_sig("ssa_rbatch_graph_stats", _I, ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong))
 _sig("ssa_rbatch_series_result", _I, ctypes.c_void_p, _I, c_double_p, c_double_p, c_double_p, c_double_p,
      c_double_p)
 _sig("ssa_server_create", _I, ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t, _I, _I, _I, _I)

@@ -237,3 +237,34 @@ def test_cadzow_inplace(gpu, oracle):
     # the context stays usable: a fresh decomposition of its (updated) signal works
     s.decompose(rank, oversampling=8)
     assert len(s.singular_values) == rank
+
+
+def _mbatch_check(gpu, oracle, I, M, N, L, k, iters, seed, check=None):
+    rng = np.random.default_rng(seed)
+    X = np.stack([oracle.config4_instance(rng, Mch=M, N=N) for _ in range(I)])
+    mb = gpu.SSAMultiBatch(I, M, N, L, k, oversampling=10, power_iters=2)
+    out, sig, diff = mb.run(X, iters, seed=seed)
+    K = N - L + 1
+    for i in (range(I) if check is None else check):
+        Om = oracle.device_gaussian(oracle.series_seed(seed, i), K, mb.kp)
+        y_ref, s_ref, d_ref = oracle.mssa_cadzow(X[i], L, mb.k, iters, 10, Om, q=2)
+        lead = min(5, mb.k)
+        assert np.max(np.abs(sig[i][:lead] - s_ref[:lead]) / s_ref[:lead]) <= 1e-5, i
+        assert rel_l2(out[i], y_ref) <= CADZOW_TOL, (i, rel_l2(out[i], y_ref))
+        assert np.max(np.abs(diff[i] - d_ref)) <= 1e-5, (i, diff[i], d_ref)
+    return out, diff
+
+
+def test_multichannel_batch_cadzow_vs_oracle(gpu, oracle):
+    """Batched multichannel SSA with Cadzow iterations (ssa_mbatch): three instances of four
+    channels, block power of each stacked operator (one block of kp columns, two subspace
+    iterations, generated start block per instance), three multivariate Cadzow iterations; every
+    instance against the oracle's restatement with the same start block."""
+    out, diff = _mbatch_check(gpu, oracle, I=3, M=4, N=3000, L=750, k=12, iters=3, seed=21)
+    assert np.all(diff[:, -1] < diff[:, 0])  # the iteration contracts
+
+
+def test_multichannel_batch_full_shape(gpu, oracle):
+    """The multichannel workload's shape (16 channels of N = 20000, L = 5000, rank 50): two
+    instances, two Cadzow iterations, instance 1 against the oracle."""
+    _mbatch_check(gpu, oracle, I=2, M=16, N=20000, L=5000, k=50, iters=2, seed=3, check=[1])

@@ -219,3 +219,27 @@ def test_multi_length_sweeps_equal_per_length_buckets(gpu, oracle):
         check_sigma(s_m[i], d.sigma)
         for gi, g in enumerate(([0], [1, 2])):
             assert rel_l2(G_m[i][gi], oracle.reconstruct(d, g, N, L)) <= rec_tol(d.sigma, g)
+
+
+def test_graph_replays_equal_direct_runs(gpu, oracle):
+    """A run with the previous run's launch signature is captured as a CUDA graph and later runs
+    replay it (job tables restored, the generator seed read from device memory): the outputs are
+    bit-identical to direct launches with graphs off, for every seed."""
+    mix = oracle.config3_batch(10, seed=33, nmin=500, nmax=40000)
+    xs, Ls, ks = [m[0] for m in mix], [m[1] for m in mix], [m[2] for m in mix]
+    seeds = [11, 12, 13, 14]
+    g = gpu.SSARaggedBatch(oversampling=10, power_iters=2)
+    outs = [g.run(xs, Ls, ks, seed=sd) for sd in seeds]
+    st = g.graph_stats()
+    assert st == {"captures": 1, "replays": 2}, st
+    d = gpu.SSARaggedBatch(oversampling=10, power_iters=2)
+    d.set_graphs(False)
+    for sd, out in zip(seeds, outs):
+        ref = d.run(xs, Ls, ks, seed=sd)
+        for a, b in zip(out, ref):
+            for s in range(len(xs)):
+                assert np.array_equal(a[s], b[s]), (sd, s)
+    assert d.graph_stats() == {"captures": 0, "replays": 0}
+    # a different shape list is a new signature: direct launch, no replay of the old graph
+    g.run(xs[:5], Ls[:5], ks[:5], seed=1)
+    assert g.graph_stats()["replays"] == 2
