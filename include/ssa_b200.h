@@ -147,6 +147,12 @@ int ssa_b200_multi_length(void);
  * the number of size codes. No counterpart in the reference. */
 int ssa_b200_tune_set(const int *gram_ctas, int n, int multi_ctas_per_sm);
 int ssa_b200_tune_get(int *gram_ctas, int n, int *multi_ctas_per_sm);
+/* Transforms of real length 32768 (series of 16385 <= N <= 32768) on thread-block clusters of
+ * two 8192-point CTAs exchanging through distributed shared memory (on != 0) or on one CTA of 1024
+ * threads each (0, the default): a per-bucket choice of the autotuner. The same values either way
+ * up to FP32 rounding. */
+void ssa_b200_set_cluster32k(int on);
+int ssa_b200_cluster32k(void);
 /* Size code of the FFT length for a series of length N (the bucket index the tuning table uses):
  * log2 of the complex length for powers of two, other values for the mixed lengths; -1 beyond
  * N = 131072. */

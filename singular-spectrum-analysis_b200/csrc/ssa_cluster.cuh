@@ -408,10 +408,10 @@ static int launch_cl_recon(const ssa_recon_job* jobs, int njobs, cudaStream_t st
     return launched(e != cudaSuccess ? e : cudaGetLastError());
 }
 
-// logh 15 or 16 (callers check)
-// CTAs per cluster of a size code: 15 -> 4, 16 -> 8, SSA_FFT_3x13 -> 3, SSA_FFT_3x14 -> 6.
+// CTAs per cluster of a size code: 14 -> 2 (when the 2-CTA form of that length is selected),
+// 15 -> 4, 16 -> 8, SSA_FFT_3x13 -> 3, SSA_FFT_3x14 -> 6.
 static int cl_ctas(int code) {
-    return code == 15 ? 4 : code == 16 ? 8 : code == SSA_FFT_3x13 ? 3 : code == SSA_FFT_3x14 ? 6 : 0;
+    return code == 14 ? 2 : code == 15 ? 4 : code == 16 ? 8 : code == SSA_FFT_3x13 ? 3 : code == SSA_FFT_3x14 ? 6 : 0;
 }
 
 static int cl_col_dispatch(int kind, const ssa_col_job* jobs, int njobs, int maxcols, int code, cudaStream_t st) {
@@ -421,6 +421,7 @@ static int cl_col_dispatch(int kind, const ssa_col_job* jobs, int njobs, int max
         if (kind == CL_CORR) return launch_cl_col<C, CL_CORR>(jobs, njobs, maxcols, st);     \
         return launch_cl_col<C, CL_ELEM>(jobs, njobs, maxcols, st);                           \
     }
+    SSA_CL_CASE(2)
     SSA_CL_CASE(3)
     SSA_CL_CASE(4)
     SSA_CL_CASE(6)

@@ -1732,6 +1732,12 @@ static int launch_recon(const ssa_recon_job* jobs, int njobs, cudaStream_t st) {
     return launched(cudaGetLastError());
 }
 
+// Real FFT length 32768 (logh 14) on 2-CTA clusters of 8192-point CTAs (1) instead of one CTA of
+// 1024 threads (0, the default); a per-bucket choice of the autotuner.
+static int g_cl14 = 0;
+extern "C" void ssad_set_cl14(int on) { g_cl14 = on != 0; }
+extern "C" int ssad_cl14(void) { return g_cl14; }
+
 #include "ssa_cluster.cuh"
 #include "ssa_tc.cuh"
 
@@ -1754,7 +1760,8 @@ extern "C" int ssad_gram_tc(const ssa_wgram_job* d_jobs, int njobs, int maxchunk
 
 extern "C" int ssad_spectrum(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
     if (njobs <= 0 || maxcols <= 0) return 0;
-    if (logh > SSA_MAX_LOGH) return cl_col_dispatch(CL_SPEC, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);  // 15-18
+    if (logh > SSA_MAX_LOGH || (logh == 14 && g_cl14))  // 15-18, and 14 on 2-CTA clusters when selected
+        return cl_col_dispatch(CL_SPEC, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);
 #define CALL(L) return launch_spectrum<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
     SSA_LOGH_DISPATCH(logh, CALL)
 #undef CALL
@@ -1781,7 +1788,8 @@ extern "C" int ssad_corr_multi(const ssa_col_job* d_jobs, const ssa_tile* d_tile
 }
 extern "C" int ssad_corr(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
     if (njobs <= 0 || maxcols <= 0) return 0;
-    if (logh > SSA_MAX_LOGH) return cl_col_dispatch(CL_CORR, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);
+    if (logh > SSA_MAX_LOGH || (logh == 14 && g_cl14))  // 15-18, and 14 on 2-CTA clusters when selected
+        return cl_col_dispatch(CL_CORR, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);
 #define CALL(L) return launch_corr<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
     SSA_LOGH_DISPATCH(logh, CALL)
 #undef CALL
@@ -1796,7 +1804,8 @@ extern "C" int ssad_elem_recon(const ssa_col_job* d_jobs, int njobs, int maxcols
 }
 extern "C" int ssad_elem_recon1(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
     if (njobs <= 0 || maxcols <= 0) return 0;
-    if (logh > SSA_MAX_LOGH) return cl_col_dispatch(CL_ELEM, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);
+    if (logh > SSA_MAX_LOGH || (logh == 14 && g_cl14))  // 15-18, and 14 on 2-CTA clusters when selected
+        return cl_col_dispatch(CL_ELEM, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);
 #define CALL(L) return launch_elem1<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
     SSA_LOGH_DISPATCH(logh, CALL)
 #undef CALL

@@ -350,6 +350,10 @@ int ssad_gaussian(float *out, long long ld, int rows, int ncols, int col0, unsig
 /* Read (and optionally reset) the device self-check record {violations, kernel, block, code,
  * value} of the current device. */
 int ssad_read_checks(unsigned int *out5, int reset);
+/* Real FFT length 32768 on 2-CTA clusters of 8192-point CTAs (on != 0) or one CTA of 1024
+ * threads per transform (0, the default). */
+void ssad_set_cl14(int on);
+int ssad_cl14(void);
 /* Add n kernel launches to the count (a CUDA-graph replay launches the kernels it captured). */
 void ssad_count_launches(unsigned long long n);
 /* Count of kernel launches issued by this library since load (all devices). */

@@ -999,6 +999,8 @@ static int bucket_followup(rbucket *b, ssa_rbatch *rb)
 }
 
 int ssa_b200_fft_size_code(int N) { return N >= 1 ? ssad_fft_code_for(N) : -1; }
+void ssa_b200_set_cluster32k(int on) { ssad_set_cl14(on); }
+int ssa_b200_cluster32k(void) { return ssad_cl14(); }
 
 int ssa_b200_fft_length(int N)
 {
@@ -1327,7 +1329,8 @@ static unsigned long long run_signature(const ssa_rbatch *rb, int B, const int *
                                         const double *d_x)
 {
     unsigned long long h = 0xCBF29CE484222325ull;
-    const int head[8] = {B, rb->p, rb->q, rb->n_groups, rb->lrf_slot, rb->n_lrf_group, g_multi, ssad_wcorr_tc()};
+    const int head[9] = {B, rb->p, rb->q, rb->n_groups, rb->lrf_slot, rb->n_lrf_group, g_multi, ssad_wcorr_tc(),
+                         ssad_cl14()};
     h = fnv(h, head, sizeof(head));
     h = fnv(h, N, sizeof(int) * B);
     h = fnv(h, L, sizeof(int) * B);

@@ -4,7 +4,9 @@ Per FFT-length bucket it measures the Gram partial launches of a synthetic batch
 bucket's lengths under candidate CTA counts, with the batch's serialized profiler (every launch's
 CUDA-event interval its own), and keeps the fastest; then it chooses the multi-length sweep
 setting (one persistent launch for real FFT lengths 512..16384 at one or two CTAs per SM, or one
-bucket per length) by the wall time of a mixed batch. A candidate replaces the built-in heuristic
+bucket per length) by the wall time of a mixed batch, and the FFT form of the real length 32768
+(one 1024-thread CTA or a cluster of two 8192-point CTAs per transform) by the wall time of a
+batch of that bucket. A candidate replaces the built-in heuristic
 only when it is faster by more than `margin` (default 3 %), so that run-to-run noise does not flip
 choices. The chosen table is written to a JSON cache keyed by the GPU name, its SM count and a
 digest of the library; a later call with the same key applies the cached table without measuring.
@@ -35,6 +37,9 @@ _lib.ssa_b200_tune_get.restype = ctypes.c_int
 _lib.ssa_b200_tune_get.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
 _lib.ssa_b200_fft_size_code.restype = ctypes.c_int
 _lib.ssa_b200_fft_size_code.argtypes = [ctypes.c_int]
+_lib.ssa_b200_set_cluster32k.restype = None
+_lib.ssa_b200_set_cluster32k.argtypes = [ctypes.c_int]
+_lib.ssa_b200_cluster32k.restype = ctypes.c_int
 
 NCODES = 19
 GRAM_CANDIDATES = (296, 592, 1184, 2368)  # 2, 4, 8 (the heuristic) and 16 CTAs per SM
@@ -54,19 +59,22 @@ def current() -> dict:
     g = (ctypes.c_int * NCODES)()
     m = ctypes.c_int()
     _lib.ssa_b200_tune_get(g, NCODES, ctypes.byref(m))
-    return {"gram_ctas": list(g), "multi": ssa_gpu.multi_length(), "multi_ctas_per_sm": m.value}
+    return {"gram_ctas": list(g), "multi": ssa_gpu.multi_length(), "multi_ctas_per_sm": m.value,
+            "cluster32k": bool(_lib.ssa_b200_cluster32k())}
 
 
 def apply(table: dict) -> None:
-    """Set the tuning table (gram_ctas per size code, multi on/off, multi CTAs per SM)."""
+    """Set the tuning table (gram_ctas per size code, multi on/off, multi CTAs per SM, the FFT form
+    of the real length 32768)."""
     g = (ctypes.c_int * NCODES)(*[int(v) for v in table.get("gram_ctas", [0] * NCODES)][:NCODES])
     if _lib.ssa_b200_tune_set(g, NCODES, int(table.get("multi_ctas_per_sm", 0))) != 0:
         raise ValueError("invalid tuning table")
     ssa_gpu.set_multi_length(bool(table.get("multi", True)))
+    _lib.ssa_b200_set_cluster32k(1 if table.get("cluster32k", False) else 0)
 
 
 def reset() -> None:
-    apply({"gram_ctas": [0] * NCODES, "multi": True, "multi_ctas_per_sm": 0})
+    apply({"gram_ctas": [0] * NCODES, "multi": True, "multi_ctas_per_sm": 0, "cluster32k": False})
 
 
 def cache_key() -> dict:
@@ -165,6 +173,18 @@ def autotune(cache: Optional[Path] = None, buckets=None, series: int = 96, reps:
     gram = [0] * NCODES
     meas = {}
     t_start = time.perf_counter()
+    # the FFT form of real length 32768: one 1024-thread CTA or a 2-CTA cluster per transform
+    cl32 = False
+    if buckets is None or 14 in buckets:
+        xs, Ls, ks = _series(rng, series, *BUCKET_N[14])
+        rb = ssa_gpu.SSARaggedBatch(oversampling=10, power_iters=2)
+        forms = {}
+        for on in (False, True):
+            apply({"gram_ctas": gram, "multi": True, "multi_ctas_per_sm": 0, "cluster32k": on})
+            forms[on] = _wall_ms(rb, xs, Ls, ks, reps)
+        cl32 = forms[True] < (1.0 - margin) * forms[False]
+        meas["cluster32k_wall_ms"] = {"single_cta": round(forms[False], 3), "cluster2": round(forms[True], 3)}
+        del rb
     for code in (buckets if buckets is not None else list(BUCKET_N)):
         lo, hi = BUCKET_N[code]
         n = 2 * series if code == 13 else series if code == 14 else max(12, series // 4)
@@ -174,7 +194,7 @@ def autotune(cache: Optional[Path] = None, buckets=None, series: int = 96, reps:
         for cand in GRAM_CANDIDATES:
             g = list(gram)
             g[code] = cand
-            apply({"gram_ctas": g, "multi": True, "multi_ctas_per_sm": 0})
+            apply({"gram_ctas": g, "multi": True, "multi_ctas_per_sm": 0, "cluster32k": cl32})
             times[cand] = _gram_ms(rb, xs, Ls, ks, reps)
         base = times[HEURISTIC_GRAM]
         best = min(times, key=lambda c: (times[c], GRAM_CANDIDATES.index(c)))
@@ -187,12 +207,12 @@ def autotune(cache: Optional[Path] = None, buckets=None, series: int = 96, reps:
     opts = {"off": (False, 0), "on_2": (True, 0), "on_1": (True, 1)}
     wall = {}
     for name, (on, cps) in opts.items():
-        apply({"gram_ctas": gram, "multi": on, "multi_ctas_per_sm": cps})
+        apply({"gram_ctas": gram, "multi": on, "multi_ctas_per_sm": cps, "cluster32k": cl32})
         wall[name] = _wall_ms(rb, xs, Ls, ks, reps)
     best = min(wall, key=lambda k: (wall[k], list(opts).index(k)))
     if wall[best] >= (1.0 - margin) * wall["on_2"]:
         best = "on_2"
-    table = {"gram_ctas": gram, "multi": opts[best][0], "multi_ctas_per_sm": opts[best][1]}
+    table = {"gram_ctas": gram, "multi": opts[best][0], "multi_ctas_per_sm": opts[best][1], "cluster32k": cl32}
     apply(table)
     out = {"key": cache_key(), "table": table, "measurements": {"buckets": meas, "multi_wall_ms": wall},
            "seconds": round(time.perf_counter() - t_start, 1), "margin": margin}

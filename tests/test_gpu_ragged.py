@@ -243,3 +243,47 @@ def test_graph_replays_equal_direct_runs(gpu, oracle):
     # a different shape list is a new signature: direct launch, no replay of the old graph
     g.run(xs[:5], Ls[:5], ks[:5], seed=1)
     assert g.graph_stats()["replays"] == 2
+
+
+def test_cluster32k_form_equals_single_cta_form(gpu, oracle):
+    """Real FFT length 32768 on 2-CTA clusters (8192 points per CTA, exchange through distributed
+    shared memory) or on one 1024-thread CTA: the uneven batch (sweeps, spectra, elementary
+    reconstructions, W) and the single-series API (cached-spectra reconstruction) agree with each
+    other and with the oracle."""
+    import ctypes
+
+    lib = gpu._lib
+    lib.ssa_b200_set_cluster32k.argtypes = [ctypes.c_int]
+    lib.ssa_b200_cluster32k.restype = ctypes.c_int
+    rng = np.random.default_rng(51)
+    Ns = [16500, 20000, 24000, 30000, 32768]
+    xs = [oracle.walk_sines(rng, N) for N in Ns]
+    Ls = [N // 4 for N in Ns]
+    ks = [12, 20, 30, 16, 25]
+    rb = gpu.SSARaggedBatch(oversampling=10, power_iters=2)
+    assert lib.ssa_b200_cluster32k() == 0
+    outs = {}
+    try:
+        for on in (0, 1):
+            lib.ssa_b200_set_cluster32k(on)
+            outs[on] = rb.run(xs, Ls, ks, seed=6)
+            s = gpu.SSA(xs[1], Ls[1])
+            s.decompose(20, oversampling=10, power_iters=2)
+            outs[on] = outs[on] + (s.reconstruct([1, 2]), s.wcorr_matrix())
+    finally:
+        lib.ssa_b200_set_cluster32k(0)
+    (s0, W0, G0, r0, w0), (s1, W1, G1, r1, w1) = outs[0], outs[1]
+    for i in range(len(Ns)):
+        check_sigma(s1[i], s0[i])
+        for gi, g in enumerate(([0], [1, 2])):
+            assert rel_l2(G1[i][gi], G0[i][gi]) <= rec_tol(s0[i], g)
+        blk = leading_block(s0[i])
+        assert np.max(np.abs(W1[i][np.ix_(blk, blk)] - W0[i][np.ix_(blk, blk)])) < 1e-4
+        N, L, k = Ns[i], Ls[i], ks[i]
+        K = N - L + 1
+        kk, kp = oracle.clamp_kp(L, K, k, 10)
+        d = oracle.decompose_randomized(xs[i], L, kk, 10, oracle.device_gaussian(oracle.series_seed(6, i), K, kp), q=2)
+        check_sigma(s1[i], d.sigma)
+        for gi, g in enumerate(([0], [1, 2])):
+            assert rel_l2(G1[i][gi], oracle.reconstruct(d, g, N, L)) <= rec_tol(d.sigma, g)
+    assert rel_l2(r1, r0) <= 1e-5 and np.max(np.abs(w1[:3, :3] - w0[:3, :3])) < 1e-4
