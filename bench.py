@@ -603,8 +603,12 @@ def server_runs(gpu, torch, a, rank: int, world: int) -> dict:
     return out
 
 
-def plain_path(gpu, a, n: int = 120) -> dict:
-    """The stream's first n requests one per call through the reference-compatible API."""
+def plain_path(gpu, a, n: int = 120, recycle: bool = True) -> dict:
+    """The stream's first n requests one per call through the reference-compatible API, a context
+    created and freed per decomposition as the reference's wrapper does; with `recycle` the
+    library's context recycling (streams, pooled buffers, page-locked staging of freed contexts)
+    is on, as by default, else every context allocates afresh."""
+    gpu.set_context_recycling(recycle)
     specs = make_stream(n, a.seed, a.nmin, a.nmax)
     objs, lat, failed = {}, [], 0
     t0 = time.perf_counter()
@@ -626,10 +630,13 @@ def plain_path(gpu, a, n: int = 120) -> dict:
             failed += 1
         lat.append((time.perf_counter() - ts) * 1e3)
     el = time.perf_counter() - t0
+    objs.clear()
+    gpu.set_context_recycling(True)
     return {"value": n / el, "unit": "SSA/s", "p50_ms": float(np.percentile(lat, 50)),
-            "p99_ms": float(np.percentile(lat, 99)), "failed": failed,
+            "p99_ms": float(np.percentile(lat, 99)), "failed": failed, "context_recycling": recycle,
             "what": f"first {n} requests of the stream, one per call (SSA() + decompose(q={a.q}) + reconstruct x2 "
-                    "/ wcorr_matrix / forecast on the kept context) through libssa.so's reference API, host wall clock"}
+                    "/ wcorr_matrix / forecast on the kept context) through libssa.so's reference API, host wall "
+                    "clock; " + ("contexts recycled (default)" if recycle else "every context allocated afresh")}
 
 
 def uniform_batch(gpu, torch, a, B: int = 4096, N: int = 10000, L: int = 2500, k: int = 50, steps: int = 3) -> dict:
@@ -763,7 +770,9 @@ def main():
     if not a.no_e2e:
         line.update(server_runs(ssa_gpu, torch, a, rank, world))
     if rank == 0 and world == 1 and not a.no_plain:
+        plain_path(ssa_gpu, a, n=8)  # warm-up: library, pool and recycled contexts in place
         line["plain_gpu_path"] = plain_path(ssa_gpu, a)
+        line["plain_gpu_path_fresh_contexts"] = plain_path(ssa_gpu, a, recycle=False)
         if "e2e" in line:
             line["e2e_over_plain"] = line["e2e"]["value"] / line["plain_gpu_path"]["value"]
     if rank == 0 and world == 1 and not a.no_uniform:

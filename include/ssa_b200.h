@@ -96,6 +96,16 @@ int mssa_opt_copy_factors(const MSSA_Opt *mssa, double *U, double *V, double *si
 void ssa_b200_set_wcorr_tensor_cores(int on);
 int ssa_b200_wcorr_tensor_cores(void);
 
+/* Context recycling (default on): contexts that own their stream (SSA_Opt, MSSA_Opt, uniform
+ * and multichannel batches) take the stream from a per-device stack that freed contexts return
+ * it to, their device buffers from the library's stream-ordered memory pool (freed blocks stay
+ * cached), and their page-locked staging from a per-device free list, so that creating and
+ * freeing a context per series costs no device-wide synchronisation or page pinning. 0 restores
+ * plain cudaMalloc / cudaMallocHost / stream creation for contexts created afterwards. No
+ * counterpart in the reference (a CPU library). */
+void ssa_b200_set_context_recycling(int on);
+int ssa_b200_context_recycling(void);
+
 /* ---- Uneven batches ------------------------------------------------------------------------
  * B series of different lengths N[s], windows L[s] and ranks k[s] (common oversampling p and
  * power iterations q) through the same pipeline as ssa_batch_*: randomized decomposition with

@@ -43,19 +43,17 @@ static void gpu_free(struct ssa_gpu_ctx *g)
     if (!g)
         return;
     if (g->engine_ok)
+    {
+        /* the context's buffers come from the engine's allocator (recycled or plain) */
+        cudaStreamSynchronize(g->e.st);
+        ssae_dfree(&g->e, g->d_group);
+        ssae_dfree(&g->e, g->d_out);
+        ssae_dfree(&g->e, g->d_lrf);
+        ssae_dfree(&g->e, g->d_status);
+        ssae_dfree(&g->e, g->d_omega);
+        ssae_pinned_free(&g->e, g->h_stage, g->stage_cap * sizeof(float));
         ssae_destroy(&g->e);
-    if (g->d_group)
-        cudaFree(g->d_group);
-    if (g->d_out)
-        cudaFree(g->d_out);
-    if (g->d_lrf)
-        cudaFree(g->d_lrf);
-    if (g->d_status)
-        cudaFree(g->d_status);
-    if (g->d_omega)
-        cudaFree(g->d_omega);
-    if (g->h_stage)
-        cudaFreeHost(g->h_stage);
+    }
     free(g);
 }
 
@@ -70,11 +68,10 @@ static int ensure_group(struct ssa_gpu_ctx *g, const int *group, int n)
 {
     if (n > g->group_cap)
     {
-        if (g->d_group)
-            cudaFree(g->d_group);
+        ssae_dfree(&g->e, g->d_group);
         g->d_group = NULL;
         int cap = n < 64 ? 64 : n;
-        if (cudaMalloc((void **)&g->d_group, sizeof(int) * cap) != cudaSuccess)
+        if (ssae_dalloc(&g->e, (void **)&g->d_group, sizeof(int) * cap) != 0)
         {
             g->group_cap = 0;
             return -1;
@@ -89,12 +86,20 @@ static int ensure_stage(struct ssa_gpu_ctx *g, size_t floats)
     if (floats <= g->stage_cap)
         return 0;
     if (g->h_stage)
-        cudaFreeHost(g->h_stage);
+    {
+        if (cudaStreamSynchronize(g->e.st) != cudaSuccess)
+            return -1;
+        ssae_pinned_free(&g->e, g->h_stage, g->stage_cap * sizeof(float));
+    }
     g->h_stage = NULL;
     g->stage_cap = 0;
-    if (cudaMallocHost((void **)&g->h_stage, floats * sizeof(float)) != cudaSuccess)
+    size_t cap = 0;
+    if (ssae_pinned(&g->e, floats * sizeof(float), (void **)&g->h_stage, &cap) != 0)
+    {
+        g->h_stage = NULL;
         return -1;
-    g->stage_cap = floats;
+    }
+    g->stage_cap = cap / sizeof(float);
     return 0;
 }
 
@@ -146,7 +151,7 @@ int ssa_opt_init(SSA_Opt *ssa, const ssa_real *x, int N, int L)
     ssa->ws_complex = (double *)malloc(sizeof(double) * 2 * ssa->r2c_len);
     ssa->inv_diag_count = (double *)malloc(sizeof(double) * N);
     if (!ssa->fft_x || !ssa->ws_real || !ssa->ws_complex || !ssa->inv_diag_count ||
-        cudaMalloc((void **)&g->d_out, sizeof(double) * (size_t)N) != cudaSuccess)
+        ssae_dalloc(&g->e, (void **)&g->d_out, sizeof(double) * (size_t)N) != 0)
     {
         ssa_opt_free(ssa);
         return -1;
@@ -545,13 +550,12 @@ static int ensure_lrf(struct ssa_gpu_ctx *g, size_t doubles)
 {
     if (doubles <= g->lrf_cap)
         return 0;
-    if (g->d_lrf)
-        cudaFree(g->d_lrf);
+    ssae_dfree(&g->e, g->d_lrf);
     g->d_lrf = NULL;
     g->lrf_cap = 0;
-    if (cudaMalloc((void **)&g->d_lrf, sizeof(double) * doubles) != cudaSuccess)
+    if (ssae_dalloc(&g->e, (void **)&g->d_lrf, sizeof(double) * doubles) != 0)
         return -1;
-    if (!g->d_status && cudaMalloc((void **)&g->d_status, sizeof(int)) != cudaSuccess)
+    if (!g->d_status && ssae_dalloc(&g->e, (void **)&g->d_status, sizeof(int)) != 0)
         return -1;
     g->lrf_cap = doubles;
     return 0;
@@ -1173,7 +1177,7 @@ int ssa_opt_parestimate(const SSA_Opt *ssa, const int *group, int n_group, SSA_P
     double *G = (double *)calloc((size_t)nc * nc * 2, sizeof(double));
     double *Z = (double *)malloc(sizeof(double) * (size_t)k * k * 3);
     double *wr = (double *)malloc(sizeof(double) * (size_t)k * 2);
-    int rc = !h_part || !G || !Z || !wr || cudaMalloc((void **)&d_part, sizeof(double) * 2 * np) != cudaSuccess;
+    int rc = !h_part || !G || !Z || !wr || ssae_dalloc(e, (void **)&d_part, sizeof(double) * 2 * np) != 0;
     if (!rc)
     {
         /* job 0: U_up^T U_up, job 1: U_up^T U_down (the same block one row further down) */
@@ -1195,8 +1199,7 @@ int ssa_opt_parestimate(const SSA_Opt *ssa, const int *group, int n_group, SSA_P
              cudaMemcpyAsync(h_part, d_part, sizeof(double) * 2 * np, cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
              sync_ok(g) != 0;
     }
-    if (d_part)
-        cudaFree(d_part);
+    ssae_dfree(e, d_part);
     if (!rc)
     {
         for (int q = 0; q < 2; q++)
@@ -1429,7 +1432,7 @@ static int cadzow_setup(struct ssa_gpu_ctx *g, int rank, double **d_aux, size_t 
     int rc = ensure_group(g, grp, rank);
     rc |= sync_ok(g);
     free(grp);
-    if (rc || cudaMalloc((void **)d_aux, sizeof(double) * aux_doubles) != cudaSuccess)
+    if (rc || ssae_dalloc(&g->e, (void **)d_aux, sizeof(double) * aux_doubles) != 0)
         return -1;
     return cudaMemsetAsync(*d_aux, 0, sizeof(double) * aux_doubles, g->e.st) == cudaSuccess ? 0 : -1;
 }
@@ -1540,7 +1543,7 @@ static int cadzow_run_from(const double *x, const double *y1, int N, int L, int 
     if (!rc && (cudaMemcpyAsync(output, e->x64, sizeof(double) * N, cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
                 sync_ok(g) != 0))
         rc = -1;
-    cudaFree(d_aux);
+    ssae_dfree(&g->e, d_aux);
     ssa_opt_free(&ssa);
     if (rc)
         return -1;
@@ -1655,7 +1658,7 @@ int ssa_opt_cadzow_inplace(SSA_Opt *ssa, int rank, int max_iter, ssa_real tol, S
             }
         }
     }
-    cudaFree(d_aux);
+    ssae_dfree(&g->e, d_aux);
     if (rc)
         return -1;
     /* mirror the last decomposition and the current signal's spectrum */
@@ -1808,7 +1811,7 @@ int ssa_opt_gapfill(ssa_real *x, int N, int L, int rank, int max_iter, ssa_real 
     if (!rc && (cudaMemcpyAsync(x, e->x64, sizeof(double) * (size_t)N, cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
                 sync_ok(g) != 0))
         rc = -1;
-    cudaFree(d_aux);
+    ssae_dfree(&g->e, d_aux);
     ssa_opt_free(&ssa);
     if (rc)
         return -1;

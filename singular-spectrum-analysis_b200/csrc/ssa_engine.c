@@ -12,6 +12,7 @@
  */
 #include "ssa_engine.h"
 
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -42,13 +43,176 @@ static int gram_rows(int m, int B)
     return imax(rows, 4 * SSA_GRAM_CHUNK);
 }
 
-static int dmalloc(void **p, size_t bytes)
+/* ---- Context recycling ---------------------------------------------------------------------
+ * A drop-in caller creates and frees a context per series (SSA(x, L) ... free), and every
+ * context needs a stream, a page-locked job arena and a dozen device buffers. Created fresh,
+ * that costs driver calls that synchronise the device (cudaFree, cudaFreeHost) or pin pages
+ * (cudaMallocHost) on every request. With recycling on (the default), engines that own their
+ * stream take it from a per-device stack of streams that earlier contexts returned, take device
+ * buffers from the library's stream-ordered memory pool on that stream (freed blocks stay cached
+ * in the pool) and take page-locked blocks from a per-device free list. ssa_b200_set_context_
+ * recycling(0) restores plain allocation for contexts created afterwards. */
+#define SSA_RECYCLE_STREAMS 64
+#define SSA_RECYCLE_PINNED 16
+#define SSA_RECYCLE_DEVICES 64
+
+static pthread_mutex_t g_recycle_mu = PTHREAD_MUTEX_INITIALIZER;
+static int g_recycle_on = 1;
+static cudaStream_t g_free_streams[SSA_RECYCLE_DEVICES][SSA_RECYCLE_STREAMS];
+static int g_n_free_streams[SSA_RECYCLE_DEVICES];
+static struct
+{
+    void *p;
+    size_t cap;
+} g_free_pinned[SSA_RECYCLE_DEVICES][SSA_RECYCLE_PINNED];
+static int g_n_free_pinned[SSA_RECYCLE_DEVICES];
+
+void ssa_b200_set_context_recycling(int on)
+{
+    pthread_mutex_lock(&g_recycle_mu);
+    g_recycle_on = on != 0;
+    pthread_mutex_unlock(&g_recycle_mu);
+}
+
+int ssa_b200_context_recycling(void) { return g_recycle_on; }
+
+static int recycle_dev(int device) { return device >= 0 && device < SSA_RECYCLE_DEVICES; }
+
+static int stream_take(int device, cudaStream_t *st)
+{
+    *st = NULL;
+    if (recycle_dev(device))
+    {
+        pthread_mutex_lock(&g_recycle_mu);
+        if (g_n_free_streams[device] > 0)
+            *st = g_free_streams[device][--g_n_free_streams[device]];
+        pthread_mutex_unlock(&g_recycle_mu);
+    }
+    if (*st)
+        return 0;
+    return (int)cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
+}
+
+static void stream_return(int device, cudaStream_t st)
+{
+    int kept = 0;
+    if (recycle_dev(device))
+    {
+        pthread_mutex_lock(&g_recycle_mu);
+        if (g_n_free_streams[device] < SSA_RECYCLE_STREAMS)
+        {
+            g_free_streams[device][g_n_free_streams[device]++] = st;
+            kept = 1;
+        }
+        pthread_mutex_unlock(&g_recycle_mu);
+    }
+    if (!kept)
+        cudaStreamDestroy(st);
+}
+
+/* Smallest free page-locked block of at least `bytes` (its capacity in *cap), else a new one. */
+static int pinned_take(int device, size_t bytes, void **p, size_t *cap)
+{
+    *p = NULL;
+    if (recycle_dev(device))
+    {
+        pthread_mutex_lock(&g_recycle_mu);
+        int best = -1;
+        for (int i = 0; i < g_n_free_pinned[device]; i++)
+            if (g_free_pinned[device][i].cap >= bytes &&
+                (best < 0 || g_free_pinned[device][i].cap < g_free_pinned[device][best].cap))
+                best = i;
+        if (best >= 0)
+        {
+            *p = g_free_pinned[device][best].p;
+            *cap = g_free_pinned[device][best].cap;
+            g_free_pinned[device][best] = g_free_pinned[device][--g_n_free_pinned[device]];
+        }
+        pthread_mutex_unlock(&g_recycle_mu);
+    }
+    if (*p)
+        return 0;
+    *cap = bytes;
+    return (int)cudaMallocHost(p, bytes);
+}
+
+/* Back to the free list (the block's users have finished with it); beyond the list's length
+ * the smallest block is released. */
+static void pinned_return(int device, void *p, size_t cap)
+{
+    void *drop = p;
+    if (recycle_dev(device))
+    {
+        pthread_mutex_lock(&g_recycle_mu);
+        if (g_n_free_pinned[device] < SSA_RECYCLE_PINNED)
+        {
+            g_free_pinned[device][g_n_free_pinned[device]].p = p;
+            g_free_pinned[device][g_n_free_pinned[device]].cap = cap;
+            g_n_free_pinned[device]++;
+            drop = NULL;
+        }
+        else
+        {
+            int small = 0;
+            for (int i = 1; i < SSA_RECYCLE_PINNED; i++)
+                if (g_free_pinned[device][i].cap < g_free_pinned[device][small].cap)
+                    small = i;
+            if (g_free_pinned[device][small].cap < cap)
+            {
+                drop = g_free_pinned[device][small].p;
+                g_free_pinned[device][small].p = p;
+                g_free_pinned[device][small].cap = cap;
+            }
+        }
+        pthread_mutex_unlock(&g_recycle_mu);
+    }
+    if (drop)
+        cudaFreeHost(drop);
+}
+
+int ssae_dalloc(ssa_engine *e, void **p, size_t bytes)
 {
     *p = NULL;
     if (bytes == 0)
         return 0;
+    if (e->recycle)
+    {
+        cudaMemPool_t pool = ssar_pool();
+        if (pool)
+            return (int)cudaMallocFromPoolAsync(p, bytes, pool, e->st);
+    }
     return (int)cudaMalloc(p, bytes);
 }
+
+void ssae_dfree(ssa_engine *e, void *p)
+{
+    if (!p)
+        return;
+    if (e->recycle)
+        cudaFreeAsync(p, e->st);
+    else
+        cudaFree(p);
+}
+
+int ssae_pinned(ssa_engine *e, size_t bytes, void **p, size_t *cap)
+{
+    if (e->recycle)
+        return pinned_take(e->device, bytes, p, cap);
+    *cap = bytes;
+    return (int)cudaMallocHost(p, bytes);
+}
+
+void ssae_pinned_free(ssa_engine *e, void *p, size_t cap)
+{
+    if (!p)
+        return;
+    if (e->recycle)
+        pinned_return(e->device, p, cap);
+    else
+        cudaFreeHost(p);
+}
+
+#define dmalloc(pp, bytes) ssae_dalloc(e, (pp), (bytes))
 
 int ssae_create(ssa_engine *e, int B, int N, int L, int kp, int k, cudaStream_t stream)
 {
@@ -90,7 +254,11 @@ int ssae_create(ssa_engine *e, int B, int N, int L, int kp, int k, cudaStream_t 
     }
     else
     {
-        CK(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+        e->recycle = g_recycle_on;
+        if (e->recycle)
+            CK(stream_take(e->device, &e->st));
+        else
+            CK(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
         e->own_stream = 1;
     }
     const size_t Bs = (size_t)B;
@@ -115,13 +283,14 @@ int ssae_create(ssa_engine *e, int B, int N, int L, int kp, int k, cudaStream_t 
         ssae_destroy(e);
         return (int)cudaErrorMemoryAllocation;
     }
-    e->ja.cap = (size_t)B * 8192 + (1 << 20);
-    if (cudaMallocHost((void **)&e->ja.h, e->ja.cap) != cudaSuccess ||
-        cudaMalloc((void **)&e->ja.d, e->ja.cap) != cudaSuccess)
+    const size_t jbytes = (size_t)B * 8192 + (1 << 20);
+    if (ssae_pinned(e, jbytes, (void **)&e->ja.h, &e->ja.hcap) != 0 ||
+        ssae_dalloc(e, (void **)&e->ja.d, jbytes) != 0)
     {
         ssae_destroy(e);
         return (int)cudaErrorMemoryAllocation;
     }
+    e->ja.cap = jbytes;
     CK(cudaMemsetAsync(e->status, 0, Bs * sizeof(int), e->st));
     return 0;
 }
@@ -163,16 +332,15 @@ int ssae_grow_arena(ssa_engine *e, size_t bytes)
     }
     if (e->st)
         CK(cudaStreamSynchronize(e->st));
-    if (e->ja.h)
-        cudaFreeHost(e->ja.h);
-    if (e->ja.d)
-        cudaFree(e->ja.d);
+    ssae_pinned_free(e, e->ja.h, e->ja.hcap);
+    ssae_dfree(e, e->ja.d);
     e->ja.h = NULL;
     e->ja.d = NULL;
     e->ja.cap = 0;
+    e->ja.hcap = 0;
     e->ja.used = 0;
-    CK(cudaMallocHost((void **)&e->ja.h, bytes));
-    CK(cudaMalloc((void **)&e->ja.d, bytes));
+    CK(ssae_pinned(e, bytes, (void **)&e->ja.h, &e->ja.hcap));
+    CK(ssae_dalloc(e, (void **)&e->ja.d, bytes));
     e->ja.cap = bytes;
     return 0;
 }
@@ -257,12 +425,15 @@ void ssae_destroy(ssa_engine *e)
                     e->Ub, e->Vb, e->xpart, e->xC, e->sUs, e->sVs, e->sDinv, e->perm, e->sgn,
                     e->Ut, e->Vt};
     for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
-        if (bufs[i])
-            cudaFree(bufs[i]);
-    if (e->ja.h)
-        cudaFreeHost(e->ja.h);
+        ssae_dfree(e, bufs[i]);
+    ssae_pinned_free(e, e->ja.h, e->ja.hcap);
     if (e->own_stream && e->st)
-        cudaStreamDestroy(e->st);
+    {
+        if (e->recycle)
+            stream_return(e->device, e->st);
+        else
+            cudaStreamDestroy(e->st);
+    }
     memset(e, 0, sizeof(*e));
 }
 
@@ -793,8 +964,7 @@ int ssae_ensure_block(ssa_engine *e, int bcap)
     void *old[] = {e->Ub, e->Vb, e->xpart, e->xC, e->sUs, e->sVs, e->sDinv, e->perm, e->sgn, e->Ut, e->Vt};
     cudaStreamSynchronize(e->st);
     for (size_t i = 0; i < sizeof(old) / sizeof(old[0]); i++)
-        if (old[i])
-            cudaFree(old[i]);
+        ssae_dfree(e, old[i]);
     const size_t Bs = (size_t)e->B;
     const int nchx = imax(e->nch_L, e->nch_K);
     int r = 0;

@@ -48,6 +48,7 @@ typedef struct
     char *d;    /* device copy */
     size_t cap;
     size_t used;
+    size_t hcap; /* capacity of the pinned block (>= cap when it was recycled) */
 } ssa_job_arena;
 
 typedef struct
@@ -60,6 +61,7 @@ typedef struct
     int device;
     cudaStream_t st;
     int own_stream;
+    int recycle;                 /* stream, buffers and pinned arena recycled (own-stream engines) */
     /* device buffers */
     double *x64;
     float *X;
@@ -113,6 +115,15 @@ int ssae_create_light(ssa_engine *e, size_t arena_bytes, cudaStream_t stream);
 /* Enlarge the job arena to at least `bytes` (waits for the stream first). */
 int ssae_grow_arena(ssa_engine *e, size_t bytes);
 void ssae_destroy(ssa_engine *e);
+/* Device buffers and page-locked blocks of an engine: from the library's stream-ordered pool on
+ * the engine's stream and from the recycled page-locked blocks when the engine recycles, else
+ * plain cudaMalloc / cudaMallocHost. Return 0 or a cudaError_t value. */
+int ssae_dalloc(ssa_engine *e, void **p, size_t bytes);
+void ssae_dfree(ssa_engine *e, void *p);
+int ssae_pinned(ssa_engine *e, size_t bytes, void **p, size_t *cap);
+void ssae_pinned_free(ssa_engine *e, void *p, size_t cap);
+/* The library's stream-ordered memory pool on the current device (freed blocks stay cached). */
+cudaMemPool_t ssar_pool(void);
 int ssae_ensure_recon(ssa_engine *e);
 int ssae_ensure_spectra(ssa_engine *e);
 

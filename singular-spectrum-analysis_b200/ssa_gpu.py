@@ -131,6 +131,8 @@ _sig("ssa_batch_profile", _I, ctypes.c_void_p, c_double_p, ctypes.POINTER(ctypes
 
 _sig("ssa_b200_set_wcorr_tensor_cores", _V, _I)
 _sig("ssa_b200_wcorr_tensor_cores", _I)
+_sig("ssa_b200_set_context_recycling", _V, _I)
+_sig("ssa_b200_context_recycling", _I)
 _sig("ssa_b200_device_checks", _I, ctypes.POINTER(ctypes.c_uint), _I)
 _sig("ssa_b200_fft_length", _I, _I)
 
@@ -142,6 +144,16 @@ def set_wcorr_tensor_cores(on: bool) -> None:
 
 def wcorr_tensor_cores() -> bool:
     return bool(_lib.ssa_b200_wcorr_tensor_cores())
+
+
+def set_context_recycling(on: bool) -> None:
+    """Contexts created afterwards recycle streams, pooled device buffers and page-locked staging
+    of freed contexts (default) or allocate them afresh."""
+    _lib.ssa_b200_set_context_recycling(1 if on else 0)
+
+
+def context_recycling() -> bool:
+    return bool(_lib.ssa_b200_context_recycling())
 
 
 def device_checks(reset: bool = True) -> List[int]:

@@ -383,3 +383,46 @@ def test_sequential_and_block_agree_with_exact(gpu, oracle):
     assert np.all(np.diff(sb) <= 0)
     U, V, _ = b.factors()
     assert np.all(U.sum(axis=0) >= 0)
+
+
+def test_context_recycling_same_results_and_bounded_memory(gpu, oracle):
+    """Contexts created with recycling (streams, pooled device buffers and page-locked staging of
+    freed contexts) give bit-identical results to freshly allocated ones, and creating and freeing
+    contexts per series keeps device memory bounded (the pool reuses its cached blocks)."""
+    import torch
+
+    x, _, Om = oracle.config1(seed=2)
+    d = oracle.decompose_randomized(x, 250, 20, 10, Om, q=2)
+    got = []
+    try:
+        for on in (False, True, True, False):
+            gpu.set_context_recycling(on)
+            s = gpu.SSA(x, 250)
+            s.decompose(20, oversampling=10, power_iters=2, omega=Om)
+            got.append((s.singular_values.copy(), s.reconstruct([0, 1]), s.wcorr_matrix()))
+            del s
+        for sg, rec, W in got[1:]:
+            assert np.array_equal(sg, got[0][0]) and np.array_equal(rec, got[0][1]) and np.array_equal(W, got[0][2])
+        assert np.max(np.abs(got[0][0][:3] - d.sigma[:3]) / d.sigma[:3]) < 1e-5
+        gpu.set_context_recycling(True)
+        rng = np.random.default_rng(5)
+        shapes = [(1000, 250, 20), (7000, 1750, 40), (30000, 7500, 30)]
+        series = [(rng.standard_normal(N).cumsum(), L, k) for N, L, k in shapes]
+
+        def cycle(n):
+            for i in range(n):
+                xs, L, k = series[i % 3]
+                s = gpu.SSA(xs, L)
+                s.decompose(k, oversampling=10, power_iters=1)
+                s.reconstruct([0])
+                del s
+
+        cycle(6)
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        cycle(60)
+        torch.cuda.synchronize()
+        free1 = torch.cuda.mem_get_info()[0]
+        assert free0 - free1 < 64 << 20, (free0, free1)
+    finally:
+        gpu.set_context_recycling(True)
