@@ -666,6 +666,40 @@ def uniform_batch(gpu, torch, a, B: int = 4096, N: int = 10000, L: int = 2500, k
                         "reconstructions + W-correlation + groups [0],[1,2]; inputs resident in HBM"}
 
 
+def wgram_variants(gpu, a, B: int = 512, N: int = 10000, L: int = 2500, k: int = 50) -> dict:
+    """The W-correlation Gram in each of its arithmetics (FP64, split TF32 and split BF16 on the
+    tensor cores, FP32 on the CUDA cores) on the uniform batch (B series x N, k components): the
+    Gram stage's CUDA-event time, its algorithmic rate (k N floats read per series; k (k + 1) N
+    flops per series for the packed upper triangle) and the largest |W - W_fp64|."""
+    import ssa_oracle
+
+    X = ssa_oracle.config2_batch(B, seed=21, N=N)
+    out, ref = {}, None
+    try:
+        for mode in (gpu.WGRAM_FP64, gpu.WGRAM_TF32X3, gpu.WGRAM_BF16X3, gpu.WGRAM_FP32):
+            gpu.set_wcorr_gram(mode)
+            b = gpu.SSABatch(B, N, L, k, oversampling=a.p, power_iters=a.q, groups=[[0]])
+            b.run(X, seed=3)  # warm-up
+            b.set_profiling(True)
+            b.profile()
+            _, W, _ = b.run(X, seed=3)
+            ms, n = b.profile()["wcorr_gram"]
+            b.set_profiling(False)
+            del b
+            if ref is None:
+                ref = W
+            kk = W.shape[1]
+            byts, flops = 4.0 * kk * N * B, float(kk) * (kk + 1) * N * B
+            out[gpu.WGRAM_NAMES[mode]] = {"ms": ms, "launches": n, "GB_s": byts / (ms / 1e3) / 1e9,
+                                          "TFLOP_s": flops / (ms / 1e3) / 1e12,
+                                          "max_abs_dW_vs_fp64": float(np.max(np.abs(W - ref)))}
+    finally:
+        gpu.set_wcorr_gram(gpu.WGRAM_TF32X3)
+    out["workload"] = (f"W-correlation Gram of {B} series x N={N} (L={L}, k={k}): elementary reconstructions "
+                       f"{4 * k * N * B / 1e9:.2f} GB read per launch (> L2); CUDA events on the batch stream")
+    return out
+
+
 def config4(gpu, torch, a, I: int = 64, M: int = 16, N: int = 20000, L: int = 5000, k: int = 50,
             iters: int = 10) -> dict:
     """The multichannel workload: I instances of M correlated channels (random mixings of 4 shared
@@ -777,6 +811,7 @@ def main():
             line["e2e_over_plain"] = line["e2e"]["value"] / line["plain_gpu_path"]["value"]
     if rank == 0 and world == 1 and not a.no_uniform:
         line["uniform_batch"] = uniform_batch(ssa_gpu, torch, a)
+        line["wcorr_gram_variants"] = wgram_variants(ssa_gpu, a)
     if rank == 0 and world == 1 and not a.no_config4:
         line["config4"] = config4(ssa_gpu, torch, a)
     if rank == 0 and world == 1 and not a.no_cpu:

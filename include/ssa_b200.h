@@ -95,6 +95,21 @@ int mssa_opt_copy_factors(const MSSA_Opt *mssa, double *U, double *V, double *si
  * selects 0 at start-up. No counterpart in the reference (its W-correlation is FP64 dsyrk). */
 void ssa_b200_set_wcorr_tensor_cores(int on);
 int ssa_b200_wcorr_tensor_cores(void);
+/* The W-correlation Gram's arithmetic in full: SSA_WGRAM_FP64 (0) FP64 accumulation of FP32
+ * products on the CUDA cores; SSA_WGRAM_TF32X3 (1, the default) tensor cores, split TF32 as
+ * above; SSA_WGRAM_BF16X3 (2) tensor cores, split BF16 (hi, lo of 8 significant bits each, the
+ * same three products; ~16-bit products, for comparison); SSA_WGRAM_FP32 (3) FP32 products
+ * accumulated in FP32 per chunk of >= 1024 time steps on the CUDA cores, FP64 across chunks.
+ * Returns 0, or -1 for another mode. */
+enum
+{
+    SSA_WGRAM_FP64 = 0,
+    SSA_WGRAM_TF32X3 = 1,
+    SSA_WGRAM_BF16X3 = 2,
+    SSA_WGRAM_FP32 = 3
+};
+int ssa_b200_set_wcorr_gram(int mode);
+int ssa_b200_wcorr_gram(void);
 
 /* Context recycling (default on): contexts that own their stream (SSA_Opt, MSSA_Opt, uniform
  * and multichannel batches) take the stream from a per-device stack that freed contexts return

@@ -1935,8 +1935,16 @@ int ssa_opt_gapfill_simple(ssa_real *x, int N, int L, int rank, SSA_GapFillResul
 }
 
 
-void ssa_b200_set_wcorr_tensor_cores(int on) { ssad_set_wcorr_tc(on); }
-int ssa_b200_wcorr_tensor_cores(void) { return ssad_wcorr_tc(); }
+void ssa_b200_set_wcorr_tensor_cores(int on) { ssad_set_wcorr_tc(on ? 1 : 0); }
+int ssa_b200_wcorr_tensor_cores(void) { return ssad_wcorr_tc() != 0; }
+int ssa_b200_set_wcorr_gram(int mode)
+{
+    if (mode < 0 || mode > 3)
+        return -1;
+    ssad_set_wcorr_tc(mode);
+    return 0;
+}
+int ssa_b200_wcorr_gram(void) { return ssad_wcorr_tc(); }
 
 /* ---- library information ----------------------------------------------------------------- */
 unsigned long long ssa_b200_kernel_launches(void) { return ssad_launch_count(); }

@@ -243,7 +243,7 @@ int ssae_create(ssa_engine *e, int B, int N, int L, int kp, int k, cudaStream_t 
     e->ldS = round4(e->ldS);
     e->rows_L = gram_rows(L, B);
     e->rows_K = gram_rows(e->K, B);
-    e->rows_N = gram_rows(N, B);
+    e->rows_N = imin(gram_rows(N, B), SSA_W_MAX_ROWS);
     e->nch_L = (L + e->rows_L - 1) / e->rows_L;
     e->nch_K = (e->K + e->rows_K - 1) / e->rows_K;
     e->nch_N = (N + e->rows_N - 1) / e->rows_N;
@@ -366,7 +366,8 @@ int ssae_set_profiling(ssa_engine *e, int on)
 static const char *kind_name(int k)
 {
     static const char *names[SSAK_NKINDS] = {"spectrum", "corr", "gram", "chol", "rowmul", "rr",
-                                             "elem_recon", "wcorr_finish", "group_sum", "recon", "lrf"};
+                                             "elem_recon", "wcorr_finish", "group_sum", "recon", "lrf",
+                                             "wcorr_gram"};
     return (k >= 0 && k < SSAK_NKINDS) ? names[k] : "?";
 }
 
@@ -643,7 +644,7 @@ static int gram_ps(ssa_engine *e, int nb, const float *A, size_t sstride, long l
     free(jobs);
     if (!d)
         return (int)cudaErrorMemoryAllocation;
-    ssae_prof_begin(e, SSAK_GRAM);
+    ssae_prof_begin(e, weighted ? SSAK_WGRAM : SSAK_GRAM);
     int rc_ = ssad_gram((const ssa_gram_job *)d, nb, nch, weighted, e->st);
     ssae_prof_end(e);
     return rc_;
@@ -853,7 +854,7 @@ static int wgram_tc(ssa_engine *e, int nb, int k, int rows)
     free(jobs);
     if (!d)
         return (int)cudaErrorMemoryAllocation;
-    ssae_prof_begin(e, SSAK_GRAM);
+    ssae_prof_begin(e, SSAK_WGRAM);
     int rc_ = ssad_gram_tc((const ssa_wgram_job *)d, nb, (e->N + rows - 1) / rows, e->st);
     ssae_prof_end(e);
     return rc_;

@@ -38,6 +38,7 @@ enum
     SSAK_GSUM,
     SSAK_RECON,
     SSAK_LRF,
+    SSAK_WGRAM,                  /* the W-correlation Gram (SSAK_GRAM: the CholQR / Rayleigh-Ritz Grams) */
     SSAK_NKINDS
 };
 #define SSA_PROF_MAX 512

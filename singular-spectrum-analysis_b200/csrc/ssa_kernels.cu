@@ -1743,7 +1743,7 @@ extern "C" int ssad_cl14(void) { return g_cl14; }
 
 static int g_wcorr_tc = -1;  // -1: not yet read from the environment
 
-extern "C" void ssad_set_wcorr_tc(int on) { g_wcorr_tc = on ? 1 : 0; }
+extern "C" void ssad_set_wcorr_tc(int mode) { g_wcorr_tc = (mode >= 0 && mode <= 3) ? mode : 1; }
 
 extern "C" int ssad_wcorr_tc(void) {
     if (g_wcorr_tc < 0) {
@@ -1755,7 +1755,8 @@ extern "C" int ssad_wcorr_tc(void) {
 
 extern "C" int ssad_gram_tc(const ssa_wgram_job* d_jobs, int njobs, int maxchunks, void* stream) {
     if (njobs <= 0 || maxchunks <= 0) return 0;
-    return launch_gram_tc(d_jobs, njobs, maxchunks, (cudaStream_t)stream);
+    const int mode = ssad_wcorr_tc();
+    return launch_gram_tc(d_jobs, njobs, maxchunks, mode == 0 ? 1 : mode, (cudaStream_t)stream);
 }
 
 extern "C" int ssad_spectrum(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {

@@ -84,16 +84,23 @@ typedef struct
 } ssa_wgram_job;
 
 /* Weighted Gram of elementary reconstructions (n <= 64 rows of length m, time-contiguous, the
- * W-correlation input) on the tensor cores: split-TF32 products with FP32 accumulation in TMEM
- * per chunk of rows_per_cta time steps (a multiple of 32), FP64 partials in the same packed
- * layout as ssad_gram. */
+ * W-correlation input) per chunk of rows_per_cta time steps (a multiple of 32) in the arithmetic
+ * ssad_wcorr_tc selects (split-TF32 or split-BF16 products with FP32 accumulation in TMEM, or
+ * FP32 on the CUDA cores), FP64 partials in the same packed layout as ssad_gram. */
 int ssad_gram_tc(const ssa_wgram_job *d_jobs, int njobs, int maxchunks, void *stream);
-/* Which W-correlation Gram the pipelines use: 1 = tensor cores (split TF32, default), 0 = FP64
- * accumulation on the CUDA cores. The environment variable SSA_WCORR_FP64=1 sets 0 at load. */
-void ssad_set_wcorr_tc(int on);
+/* Which W-correlation Gram the pipelines use: 1 = tensor cores, split TF32 (default); 2 = tensor
+ * cores, split BF16; 3 = FP32 products and accumulation per chunk on the CUDA cores (modes 1-3
+ * run through ssad_gram_tc's chunked jobs); 0 = FP64 accumulation on the CUDA cores (ssad_gram).
+ * The environment variable SSA_WCORR_FP64=1 sets 0 at load. */
+void ssad_set_wcorr_tc(int mode);
 int ssad_wcorr_tc(void);
 /* Time steps per tensor-core W-Gram partial: chunks long enough to amortise a CTA's set-up. */
 #define SSA_TC_MIN_ROWS 1024
+/* Time steps per W-correlation Gram partial at most (multiple of SSA_GRAM_CHUNK): the partial
+ * sums of the tensor-core and FP32 forms accumulate in FP32 within a chunk, and their rounding
+ * grows with its length (a batch of few series would otherwise get chunks of thousands of
+ * steps). */
+#define SSA_W_MAX_ROWS 2048
 
 /* Cholesky job: G = sum of the partials; G = R^T R with R upper triangular; writes R^{-1}
  * (upper triangular, FP64) n x n column-major (X[r][c] at Rinv[r + c n], zeros below the

@@ -662,7 +662,7 @@ static int r_gram(rbucket *b, int side)
     free(wjobs);
     if (!d)
         return (int)cudaErrorMemoryAllocation;
-    ssae_prof_begin(&b->e, SSAK_GRAM);
+    ssae_prof_begin(&b->e, side == SIDE_N ? SSAK_WGRAM : SSAK_GRAM);
     int rc = tc ? ssad_gram_tc((const ssa_wgram_job *)d, nj, maxch, b->e.st)
                 : ssad_gram((const ssa_gram_job *)d, nj, maxch, side == SIDE_N, b->e.st);
     ssae_prof_end(&b->e);
@@ -1127,7 +1127,7 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
             S->ldN = round4(S->N);
             S->rows_L = gram_rows_for(S->L, b->nb, g);
             S->rows_K = gram_rows_for(S->K, b->nb, g);
-            S->rows_N = gram_rows_for(S->N, b->nb, g);
+            S->rows_N = imin(gram_rows_for(S->N, b->nb, g), SSA_W_MAX_ROWS);
             S->nch_L = (S->L + S->rows_L - 1) / S->rows_L;
             S->nch_K = (S->K + S->rows_K - 1) / S->rows_K;
             S->nch_N = (S->N + S->rows_N - 1) / S->rows_N;
@@ -1837,7 +1837,8 @@ size_t ssar_series_bytes(int N, int L, int k, int p, int n_groups)
     const int nb_est = 64; /* Gram chunking at moderate bucket sizes */
     const int nch = imax(imax((L + gram_rows(L, nb_est) - 1) / gram_rows(L, nb_est),
                               (K + gram_rows(K, nb_est) - 1) / gram_rows(K, nb_est)),
-                         (N + gram_rows(N, nb_est) - 1) / gram_rows(N, nb_est));
+                         (N + imin(gram_rows(N, nb_est), SSA_W_MAX_ROWS) - 1) /
+                             imin(gram_rows(N, nb_est), SSA_W_MAX_ROWS));
     size_t b = 0;
     b += 4 * ldS;                                               /* X */
     b += 4 * (size_t)(round4(L) + round4(K)) * kp;               /* Y, Z */

@@ -131,6 +131,8 @@ _sig("ssa_batch_profile", _I, ctypes.c_void_p, c_double_p, ctypes.POINTER(ctypes
 
 _sig("ssa_b200_set_wcorr_tensor_cores", _V, _I)
 _sig("ssa_b200_wcorr_tensor_cores", _I)
+_sig("ssa_b200_set_wcorr_gram", _I, _I)
+_sig("ssa_b200_wcorr_gram", _I)
 _sig("ssa_b200_set_context_recycling", _V, _I)
 _sig("ssa_b200_context_recycling", _I)
 _sig("ssa_b200_device_checks", _I, ctypes.POINTER(ctypes.c_uint), _I)
@@ -144,6 +146,23 @@ def set_wcorr_tensor_cores(on: bool) -> None:
 
 def wcorr_tensor_cores() -> bool:
     return bool(_lib.ssa_b200_wcorr_tensor_cores())
+
+
+# W-correlation Gram arithmetics (ssa_b200_set_wcorr_gram)
+WGRAM_FP64, WGRAM_TF32X3, WGRAM_BF16X3, WGRAM_FP32 = 0, 1, 2, 3
+WGRAM_NAMES = {WGRAM_FP64: "fp64", WGRAM_TF32X3: "split-tf32 (tensor cores)",
+               WGRAM_BF16X3: "split-bf16 (tensor cores)", WGRAM_FP32: "fp32 (cuda cores)"}
+
+
+def set_wcorr_gram(mode: int) -> None:
+    """The W-correlation Gram's arithmetic for the pipelines: WGRAM_FP64, WGRAM_TF32X3 (default),
+    WGRAM_BF16X3 or WGRAM_FP32."""
+    if _lib.ssa_b200_set_wcorr_gram(int(mode)) != 0:
+        raise ValueError(f"unknown W-correlation Gram mode {mode}")
+
+
+def wcorr_gram() -> int:
+    return int(_lib.ssa_b200_wcorr_gram())
 
 
 def set_context_recycling(on: bool) -> None:
@@ -164,7 +183,7 @@ def device_checks(reset: bool = True) -> List[int]:
 
 
 PROFILE_KINDS = ("spectrum", "corr", "gram", "chol", "rowmul", "rr", "elem_recon", "wcorr_finish", "group_sum",
-                 "recon", "lrf")
+                 "recon", "lrf", "wcorr_gram")
 
 
 def fft_length(N: int) -> int:

@@ -132,7 +132,8 @@ def _gram_ms(rb, xs, Ls, ks, reps: int) -> float:
         for r in range(reps + 1):
             rb.profile()
             rb.run(xs, Ls, ks, seed=r)
-            ms = rb.profile()["gram"][0]
+            prof = rb.profile()
+            ms = prof["gram"][0] + prof.get("wcorr_gram", (0.0, 0))[0]
             if r:
                 out.append(ms)
     finally:

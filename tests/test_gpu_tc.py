@@ -72,3 +72,56 @@ def test_tc_wcorr_in_batches(gpu, oracle):
         assert np.array_equal(a[3][s], b[3][s])
         assert np.max(np.abs(a[4][s] - b[4][s])) <= 5e-6, s
     assert gpu.device_checks(reset=True)[0] == 0
+
+
+@pytest.mark.parametrize("N,L,k", [(1000, 250, 50), (20000, 5000, 54)])
+def test_wcorr_gram_arithmetics_against_fp64(gpu, oracle, N, L, k):
+    """The four W-correlation Gram arithmetics on the same decomposition: split TF32 and FP32
+    within 5e-6 of the FP64 path (~21-22 bits per product, FP32 partial sums over chunks of
+    1024+ steps), split BF16 within 1e-4 (hi, lo of 8 significant bits each: ~16 bits per
+    product); every mode leaves sigma untouched and the diagonal at 1."""
+    rng = np.random.default_rng(N + 1)
+    x = oracle.walk_sines(rng, N)
+    K = N - L + 1
+    Om = rng.standard_normal((K, min(k + 10, L, K)))
+    Ws, sig = {}, {}
+    try:
+        for mode in (gpu.WGRAM_FP64, gpu.WGRAM_TF32X3, gpu.WGRAM_BF16X3, gpu.WGRAM_FP32):
+            gpu.set_wcorr_gram(mode)
+            assert gpu.wcorr_gram() == mode
+            s = gpu.SSA(x, L)
+            s.decompose(k, oversampling=10, power_iters=2, omega=Om)
+            Ws[mode], sig[mode] = s.wcorr_matrix(), s.singular_values.copy()
+    finally:
+        gpu.set_wcorr_gram(gpu.WGRAM_TF32X3)
+    assert gpu.device_checks(reset=True)[0] == 0
+    ref = Ws[gpu.WGRAM_FP64]
+    err = {m: float(np.max(np.abs(W - ref))) for m, W in Ws.items()}
+    print(f"\nN={N} k={k}: max |W - W_fp64|: " + ", ".join(f"{gpu.WGRAM_NAMES[m]} {e:.2e}" for m, e in err.items()))
+    for m in Ws:
+        assert np.array_equal(sig[m], sig[gpu.WGRAM_FP64])
+        assert np.max(np.abs(np.diag(Ws[m]) - 1.0)) < 1e-6
+    assert err[gpu.WGRAM_TF32X3] <= 5e-6 and err[gpu.WGRAM_FP32] <= 5e-6
+    assert err[gpu.WGRAM_BF16X3] <= 1e-4
+    with pytest.raises(ValueError):
+        gpu.set_wcorr_gram(7)
+
+
+def test_wcorr_gram_arithmetics_in_uneven_batch(gpu, oracle):
+    """The same comparison through the uneven batch, series across single-CTA and cluster
+    lengths."""
+    mix = oracle.config3_batch(6, seed=17, nmin=500, nmax=70000)
+    out = {}
+    try:
+        for mode in (gpu.WGRAM_FP64, gpu.WGRAM_TF32X3, gpu.WGRAM_BF16X3, gpu.WGRAM_FP32):
+            gpu.set_wcorr_gram(mode)
+            rb = gpu.SSARaggedBatch(oversampling=10, power_iters=2)
+            out[mode] = rb.run([m[0] for m in mix], [m[1] for m in mix], [m[2] for m in mix], seed=9)
+    finally:
+        gpu.set_wcorr_gram(gpu.WGRAM_TF32X3)
+    ref = out[gpu.WGRAM_FP64]
+    for mode, bar in ((gpu.WGRAM_TF32X3, 5e-6), (gpu.WGRAM_FP32, 5e-6), (gpu.WGRAM_BF16X3, 1e-4)):
+        for s in range(len(mix)):
+            assert np.array_equal(out[mode][0][s], ref[0][s])
+            assert np.max(np.abs(out[mode][1][s] - ref[1][s])) <= bar, (mode, s)
+    assert gpu.device_checks(reset=True)[0] == 0
