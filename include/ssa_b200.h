@@ -110,6 +110,15 @@ enum
 };
 int ssa_b200_set_wcorr_gram(int mode);
 int ssa_b200_wcorr_gram(void);
+/* Row products of the randomized pipelines (Q = Y R^{-1} of every CholQR pass, U = Q Z_u,
+ * V = B Z_v; single series, batches, MSSA, the server) on the tensor cores (1): both operands
+ * split into three TF32 parts and the six part products down to 2^-22 relative accumulated in
+ * FP32 in TMEM, i.e. FP32-level rounding (results within ~1e-7 of the CUDA-core form); 0 (the
+ * default, faster on the mixed stream) = FP32 on the CUDA cores. Block power (decompose_block,
+ * extend, the multichannel batch) always uses the CUDA-core form. SSA_ROWMUL_TC=1 in the
+ * environment selects 1 at start-up. */
+void ssa_b200_set_rowmul_tensor_cores(int on);
+int ssa_b200_rowmul_tensor_cores(void);
 
 /* Context recycling (default on): contexts that own their stream (SSA_Opt, MSSA_Opt, uniform
  * and multichannel batches) take the stream from a per-device stack that freed contexts return

@@ -1945,6 +1945,8 @@ int ssa_b200_set_wcorr_gram(int mode)
     return 0;
 }
 int ssa_b200_wcorr_gram(void) { return ssad_wcorr_tc(); }
+void ssa_b200_set_rowmul_tensor_cores(int on) { ssad_set_rowmul_tc(on); }
+int ssa_b200_rowmul_tensor_cores(void) { return ssad_rowmul_tc_on(); }
 
 /* ---- library information ----------------------------------------------------------------- */
 unsigned long long ssa_b200_kernel_launches(void) { return ssad_launch_count(); }

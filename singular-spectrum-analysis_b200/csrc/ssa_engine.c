@@ -424,7 +424,7 @@ void ssae_destroy(ssa_engine *e)
     void *bufs[] = {e->x64, e->X, e->Y, e->Z, e->part, e->qsum, e->Rinv, e->Zu, e->Zv,
                     e->sigma, e->status, e->recon, e->norm2, e->W, e->Us, e->Vs, e->ja.d,
                     e->Ub, e->Vb, e->xpart, e->xC, e->sUs, e->sVs, e->sDinv, e->perm, e->sgn,
-                    e->Ut, e->Vt};
+                    e->Ut, e->Vt, e->bsplit};
     for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
         ssae_dfree(e, bufs[i]);
     ssae_pinned_free(e, e->ja.h, e->ja.hcap);
@@ -701,12 +701,29 @@ static int rowmul(ssa_engine *e, int nb, const float *A, size_t astride, long lo
         J->p = p;
         J->ldb = ldb;
     }
+    const int tc = !e->rowmul_simt && ssad_rowmul_tc_on();
+    if (tc && (size_t)nb > e->bsplit_cap)
+    {
+        ssae_dfree(e, e->bsplit);
+        e->bsplit = NULL;
+        e->bsplit_cap = 0;
+        if (ssae_dalloc(e, (void **)&e->bsplit, sizeof(float) * SSA_ROWMUL_BSPLIT_FLOATS * (size_t)nb) != 0)
+        {
+            free(jobs);
+            return (int)cudaErrorMemoryAllocation;
+        }
+        e->bsplit_cap = (size_t)nb;
+    }
+    if (tc)
+        for (int s = 0; s < nb; s++)
+            jobs[s].Bsplit = e->bsplit + (size_t)s * SSA_ROWMUL_BSPLIT_FLOATS;
     void *d = ssae_push_jobs(e, jobs, sizeof(ssa_rowmul_job) * nb);
     free(jobs);
     if (!d)
         return (int)cudaErrorMemoryAllocation;
     ssae_prof_begin(e, SSAK_ROWMUL);
-    int rc_ = ssad_rowmul((const ssa_rowmul_job *)d, nb, m, n, e->st);
+    int rc_ = tc ? ssad_rowmul_tc((const ssa_rowmul_job *)d, nb, m, n, e->st)
+                 : ssad_rowmul((const ssa_rowmul_job *)d, nb, m, n, e->st);
     ssae_prof_end(e);
     return rc_;
 }
@@ -1092,8 +1109,23 @@ static int deflate(ssa_engine *e, int nb, float *Xm, size_t xs, long long ldx, i
 
 /* Block power iteration for components [comp0, k); components [0, comp0) are already in Y, Z
  * and sigma (deflated against, re-sorted with the new ones, their signs kept). */
+static int block_power_run(ssa_engine *e, int nb, int k, int comp0, int bsize, int max_iter, const float *d_V0,
+                           long long v0_ld, unsigned long long seed);
+
+/* Block power keeps its row products on the CUDA cores: it orthonormalises only every few
+ * iterations, and amplifies the rounding of the products in between by (sigma_1 / sigma_k)^(2j). */
 static int block_power(ssa_engine *e, int nb, int k, int comp0, int bsize, int max_iter, const float *d_V0,
                        long long v0_ld, unsigned long long seed)
+{
+    const int saved = e->rowmul_simt;
+    e->rowmul_simt = 1;
+    const int rc = block_power_run(e, nb, k, comp0, bsize, max_iter, d_V0, v0_ld, seed);
+    e->rowmul_simt = saved;
+    return rc;
+}
+
+static int block_power_run(ssa_engine *e, int nb, int k, int comp0, int bsize, int max_iter, const float *d_V0,
+                           long long v0_ld, unsigned long long seed)
 {
     const int L = e->L, K = e->K;
     if (nb < 1 || nb > e->B || k < 1 || bsize < 1 || max_iter < 0 || comp0 < 0)

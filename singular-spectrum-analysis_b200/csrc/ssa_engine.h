@@ -63,6 +63,9 @@ typedef struct
     cudaStream_t st;
     int own_stream;
     int recycle;                 /* stream, buffers and pinned arena recycled (own-stream engines) */
+    int rowmul_simt;             /* row products on the CUDA cores even when the tensor-core form is on */
+    float *bsplit;               /* tensor-core row products: split parts of the small factor per series */
+    size_t bsplit_cap;           /* series the scratch holds */
     /* device buffers */
     double *x64;
     float *X;

@@ -1753,6 +1753,26 @@ extern "C" int ssad_wcorr_tc(void) {
     return g_wcorr_tc;
 }
 
+// Row products of the randomized pipelines on the tensor cores (1) or on the CUDA cores (0, the
+// default: measured faster on the mixed stream, the tensor-core form being bound by the latency
+// of its register-staged row loads).
+// SSA_ROWMUL_TC=1 in the environment selects the tensor-core form at start-up.
+static int g_rowmul_tc = -1;  // -1: not yet read from the environment
+extern "C" void ssad_set_rowmul_tc(int on) { g_rowmul_tc = on != 0; }
+extern "C" int ssad_rowmul_tc_on(void) {
+    if (g_rowmul_tc < 0) {
+        const char* v = getenv("SSA_ROWMUL_TC");
+        g_rowmul_tc = (v && v[0] == '1') ? 1 : 0;
+    }
+    return g_rowmul_tc;
+}
+
+extern "C" int ssad_rowmul_tc(const ssa_rowmul_job* d_jobs, int njobs, int maxrows, int maxn, void* stream) {
+    if (njobs <= 0 || maxrows <= 0) return 0;
+    if (maxn > SSA_MAX_KP) return (int)cudaErrorInvalidValue;
+    return launch_rowmul_tc(d_jobs, njobs, maxrows, (cudaStream_t)stream);
+}
+
 extern "C" int ssad_gram_tc(const ssa_wgram_job* d_jobs, int njobs, int maxchunks, void* stream) {
     if (njobs <= 0 || maxchunks <= 0) return 0;
     const int mode = ssad_wcorr_tc();

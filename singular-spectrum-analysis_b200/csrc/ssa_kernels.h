@@ -128,7 +128,11 @@ typedef struct
     const float *sub;     /* optional: C = sub - A * Bm (sub may alias C), ld = ldsub */
     long long lda, ldc, ldsub;
     int m, n, p, ldb;
+    float *Bsplit;        /* tensor-core form: SSA_ROWMUL_BSPLIT_FLOATS of scratch for Bm's split parts */
 } ssa_rowmul_job;
+/* Scratch floats per job of the tensor-core row products: two phases of 32 inner elements x three
+ * TF32 parts x 64 output columns. */
+#define SSA_ROWMUL_BSPLIT_FLOATS (2 * 3 * 32 * 64)
 
 /* Cross Gram partials: part[chunk][i * nb + j] = sum over the chunk's rows r of A[r][i] B[r][j]
  * (FP64 accumulation), A m x na (lda), B m x nb (ldb), na, nb <= SSA_MAX_KP. */
@@ -335,6 +339,13 @@ int ssad_elem_recon(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh,
 int ssad_gram(const ssa_gram_job *d_jobs, int njobs, int maxchunks, int weighted, void *stream);
 int ssad_chol(const ssa_chol_job *d_jobs, int njobs, void *stream);
 int ssad_rowmul(const ssa_rowmul_job *d_jobs, int njobs, int maxrows, int maxn, void *stream);
+/* The same products on the 5th-generation tensor cores: both operands split into three TF32
+ * parts, the six part products down to 2^-22 relative accumulated in FP32 in TMEM (FP32-level
+ * rounding). ssad_rowmul_tc_on() says whether the randomized pipelines use it (default 0;
+ * block power always keeps the CUDA-core form). */
+int ssad_rowmul_tc(const ssa_rowmul_job *d_jobs, int njobs, int maxrows, int maxn, void *stream);
+void ssad_set_rowmul_tc(int on);
+int ssad_rowmul_tc_on(void);
 int ssad_rr(const ssa_rr_job *d_jobs, int njobs, void *stream);
 int ssad_recon(const ssa_recon_job *d_jobs, int njobs, int logh, void *stream);
 int ssad_wfin(const ssa_wfin_job *d_jobs, int njobs, void *stream);

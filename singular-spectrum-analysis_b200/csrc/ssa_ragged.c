@@ -84,6 +84,8 @@ typedef struct
     size_t sz[11]; /* bytes of X, Y, Z, part, qsum, R, Zu, Zv, recon, norm2, Us for the run */
     int *status_base; /* the batch's status words (indexed by series) */
     cudaEvent_t done;
+    float *bsplit;     /* tensor-core row products: split parts of the small factors, per series */
+    size_t bsplit_cap; /* floats */
 } rbucket;
 
 struct ssa_rbatch
@@ -267,6 +269,8 @@ static void bucket_free(rbucket *b)
 {
     if (!b->live)
         return;
+    if (b->bsplit)
+        cudaFreeAsync(b->bsplit, b->e.st);
     ssae_destroy(&b->e); /* stream, job arena, profiler events */
     if (b->done)
         cudaEventDestroy(b->done);
@@ -730,12 +734,26 @@ static int r_rowmul(rbucket *b, int side, int trsm, int colsum)
         maxm = imax(maxm, m);
         maxn = imax(maxn, S->kp);
     }
+    const int tc = ssad_rowmul_tc_on();
+    if (tc)
+    {
+        const int rc = grow((void **)&b->bsplit, &b->bsplit_cap, (size_t)b->nb * SSA_ROWMUL_BSPLIT_FLOATS, sizeof(float),
+                            b->e.st);
+        if (rc)
+        {
+            free(jobs);
+            return rc;
+        }
+        for (int i = 0; i < b->nb; i++)
+            jobs[i].Bsplit = b->bsplit + (size_t)i * SSA_ROWMUL_BSPLIT_FLOATS;
+    }
     void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_rowmul_job) * b->nb);
     free(jobs);
     if (!d)
         return (int)cudaErrorMemoryAllocation;
     ssae_prof_begin(&b->e, SSAK_ROWMUL);
-    int rc = ssad_rowmul((const ssa_rowmul_job *)d, b->nb, maxm, maxn, b->e.st);
+    int rc = tc ? ssad_rowmul_tc((const ssa_rowmul_job *)d, b->nb, maxm, maxn, b->e.st)
+                : ssad_rowmul((const ssa_rowmul_job *)d, b->nb, maxm, maxn, b->e.st);
     ssae_prof_end(&b->e);
     return rc;
 }
@@ -1329,8 +1347,8 @@ static unsigned long long run_signature(const ssa_rbatch *rb, int B, const int *
                                         const double *d_x)
 {
     unsigned long long h = 0xCBF29CE484222325ull;
-    const int head[9] = {B, rb->p, rb->q, rb->n_groups, rb->lrf_slot, rb->n_lrf_group, g_multi, ssad_wcorr_tc(),
-                         ssad_cl14()};
+    const int head[10] = {B, rb->p, rb->q, rb->n_groups, rb->lrf_slot, rb->n_lrf_group, g_multi, ssad_wcorr_tc(),
+                          ssad_cl14(), ssad_rowmul_tc_on()};
     h = fnv(h, head, sizeof(head));
     h = fnv(h, N, sizeof(int) * B);
     h = fnv(h, L, sizeof(int) * B);

@@ -395,3 +395,257 @@ static int launch_gram_tc(const ssa_wgram_job* jobs, int njobs, int maxchunks, i
     }
     return launch_gram_tc_p<TcTF32>(jobs, njobs, maxchunks, st);
 }
+
+// ---------------------------------------------------------------------------------------------
+// Row products on the tensor cores: C = A Bm (or sub - A Bm) for A (m x n, column-major, n <= 64)
+// and a small Bm (n x p, p <= 64), the operation of k_rowmul.
+//
+// Both operands are split into three TF32 parts, x = x1 + x2 + x3, by truncation (x1 = x with its
+// low 13 mantissa bits cleared, x2 the same of x - x1, x3 = x - x1 - x2: exact for FP32 values,
+// ~33 significant bits of an FP64 Bm), and the product is the sum of the six part products down
+// to relative size 2^-22: a1 b1 + a1 b2 + a2 b1 + a1 b3 + a2 b2 + a3 b1 (the dropped ones are
+// ~2^-33), accumulated in FP32 in TMEM: the rounding of an FP32 product with FP32 accumulation,
+// on the tensor pipe.
+//   k_split_b (one CTA per job) writes Bm's three parts once, as the shared-memory image of the
+//   B operand (N = 64 output columns x K, canonical K-major layout of 8-row x 16-byte core
+//   matrices, no swizzle), per phase of 32 inner elements, into the job's Bsplit buffer.
+//   k_rowmul_tc: CTAs of 256 threads, each over several 128-row tiles of one job (tile t of the
+//   job at blockIdx.x + i gridDim.x; 128 = SSA_ROWMUL_ROWS, so the column-sum partials have the
+//   layout of k_rowmul). The B image is copied in once; TMEM (64 columns) is allocated once. Per
+//   phase of 32 inner elements two threads per row split 16 values each and store the three A
+//   parts (K-major core matrices); one elected thread issues 6 x 4 tcgen05.mma.kind::tf32
+//   (M = 128, N = 64, K = 8) and commits them to an mbarrier, and the threads load the next
+//   phase's (or the next tile's) values while the MMAs run. Epilogue per tile: tcgen05.ld of
+//   the accumulators (warp w: TMEM lanes 32 (w % 4).., columns 32 (w / 4)..) into shared memory
+//   as a [column][row] tile, then a warp per column stores 128 consecutive rows (16 bytes per
+//   lane) and reduces the column's partial sum.
+// Every mbarrier wait is bounded; on a timeout the CTA stops issuing, waits (bounded) for its
+// own MMAs, frees its TMEM, records the failure in the self-check word and writes nothing more.
+#define RT_THREADS 256
+#define RT_KH 32                                 // inner elements per phase
+#define RT_TPC 4                                 // row tiles per CTA
+#define RT_A_PART (RT_KH / 4 * TC_A_LBO)         // 16 KB: 128 rows x 32 TF32
+#define RT_B_PART (RT_KH / 4 * TC_B_LBO)         // 8 KB: 64 columns x 32 TF32
+#define RT_B_PHASE (3 * RT_B_PART)               // one phase's B image: 24 KB
+#define RT_SMEM (3 * RT_A_PART + 2 * RT_B_PHASE) // 96 KB
+
+__device__ __forceinline__ float rt_trunc(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
+
+// x = a + b + c exactly (FP32 input): every subtraction is exact, c has at most 2 significant bits
+__device__ __forceinline__ void rt_split3f(float x, float& a, float& b, float& c) {
+    a = rt_trunc(x);
+    const float r = x - a;
+    b = rt_trunc(r);
+    c = r - b;
+}
+
+__device__ __forceinline__ void rt_split3d(double x, float& a, float& b, float& c) {
+    a = rt_trunc((float)x);
+    const double r1 = x - (double)a;
+    b = rt_trunc((float)r1);
+    c = rt_trunc((float)(r1 - (double)b));
+}
+
+__global__ void __launch_bounds__(256) k_split_b(const ssa_rowmul_job* __restrict__ jobs) {
+    const ssa_rowmul_job J = jobs[blockIdx.x];
+    const int n = J.n, p = J.p;
+    if (!J.Bsplit || n < 1 || p < 1 || n > SSA_MAX_KP || p > SSA_MAX_KP) return;
+    const int nph = (n + RT_KH - 1) / RT_KH;
+    unsigned char* img = reinterpret_cast<unsigned char*>(J.Bsplit);
+    // element (output column j, inner k): phase k / 32, 4 consecutive k per 16-byte slot
+    for (int e = threadIdx.x; e < nph * SSA_MAX_KP * (RT_KH / 4); e += blockDim.x) {
+        const int ph = e / (SSA_MAX_KP * (RT_KH / 4));
+        const int rem = e - ph * SSA_MAX_KP * (RT_KH / 4);
+        const int j = rem % SSA_MAX_KP, s4 = rem / SSA_MAX_KP;
+        float b1[4], b2[4], b3[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = ph * RT_KH + 4 * s4 + u;
+            double b = 0.0;
+            if (j < p && k < n) b = J.Bm64 ? J.Bm64[k + (long long)j * J.ldb] : (double)J.Bm[k + (long long)j * J.ldb];
+            rt_split3d(b, b1[u], b2[u], b3[u]);
+        }
+        unsigned char* base = img + (size_t)ph * RT_B_PHASE + tc_off<TcTF32>(j, 4 * s4, TC_B_LBO);
+        *reinterpret_cast<float4*>(base) = make_float4(b1[0], b1[1], b1[2], b1[3]);
+        *reinterpret_cast<float4*>(base + RT_B_PART) = make_float4(b2[0], b2[1], b2[2], b2[3]);
+        *reinterpret_cast<float4*>(base + 2 * RT_B_PART) = make_float4(b3[0], b3[1], b3[2], b3[3]);
+    }
+}
+
+__global__ void __launch_bounds__(RT_THREADS) k_rowmul_tc(const ssa_rowmul_job* __restrict__ jobs) {
+    extern __shared__ __align__(1024) unsigned char rts[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_base;
+    __shared__ int failed;
+    const ssa_rowmul_job J = jobs[blockIdx.y];
+    const int n = J.n, p = J.p;
+    const int ntiles = (J.m + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS;
+    if ((int)blockIdx.x >= ntiles || !J.Bsplit || n < 1 || p < 1 || n > SSA_MAX_KP || p > SSA_MAX_KP) return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    unsigned char* sA = rts;                  // parts a1, a2, a3 of the phase (the epilogue tile too)
+    unsigned char* sB = rts + 3 * RT_A_PART;  // parts b1, b2, b3 of every phase
+    const int nph = (n + RT_KH - 1) / RT_KH;
+
+    if (tid == 0) {
+        tc_mbar_init(&bar, 1);
+        failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem_u32(&tmem_base)),
+                     "r"(64)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(J.Bsplit);
+        uint4* dst = reinterpret_cast<uint4*>(sB);
+        for (int u = tid; u < nph * (RT_B_PHASE / 16); u += RT_THREADS) dst[u] = src[u];
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base;
+    const uint32_t idesc = tc_idesc<TcTF32::FMT>();
+
+    const int r = tid & (SSA_ROWMUL_ROWS - 1), half = tid >> 7;  // row in the tile, inner half
+    constexpr int QH = RT_KH / 2;
+    float v[QH];
+    auto load_a = [&](int t, int ph) {
+        const int row = t * SSA_ROWMUL_ROWS + r;
+        const bool rok = row < J.m;
+        const float* arow = J.A + (long long)row;
+#pragma unroll
+        for (int q = 0; q < QH; ++q) {
+            const int c = ph * RT_KH + half * QH + q;
+            v[q] = (rok && c < n) ? arow[(long long)c * J.lda] : 0.f;
+        }
+    };
+    bool ok = true;
+    int ncommit = 0;  // commits issued; the mbarrier phase of commit c has parity c & 1
+    auto wait_last = [&]() {
+        if (ncommit > 0 && ok && !tc_mbar_wait(&bar, (uint32_t)((ncommit - 1) & 1))) ok = false;
+    };
+    constexpr int CT_LD = SSA_ROWMUL_ROWS + 4;
+    float* ct = reinterpret_cast<float*>(rts);  // 64 x CT_LD floats (33.8 KB) over the A stages
+    const int sub4 = warp & 3, chalf = warp >> 2;
+    const int rl = 4 * lane;
+    load_a(blockIdx.x, 0);
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int r0 = t * SSA_ROWMUL_ROWS;
+        const int rows = min(SSA_ROWMUL_ROWS, J.m - r0);
+        for (int ph = 0; ph < nph; ++ph) {
+            wait_last();  // the A stages are free again
+#pragma unroll
+            for (int s4 = 0; s4 < QH / 4; ++s4) {
+                float4 a1, a2, a3;
+                rt_split3f(v[4 * s4 + 0], a1.x, a2.x, a3.x);
+                rt_split3f(v[4 * s4 + 1], a1.y, a2.y, a3.y);
+                rt_split3f(v[4 * s4 + 2], a1.z, a2.z, a3.z);
+                rt_split3f(v[4 * s4 + 3], a1.w, a2.w, a3.w);
+                const uint32_t off = tc_off<TcTF32>(r, half * QH + 4 * s4, TC_A_LBO);
+                *reinterpret_cast<float4*>(sA + off) = a1;
+                *reinterpret_cast<float4*>(sA + RT_A_PART + off) = a2;
+                *reinterpret_cast<float4*>(sA + 2 * RT_A_PART + off) = a3;
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tc_fence_before();
+            if (!ok) failed = 1;
+            __syncthreads();
+            if (tid == 0 && !failed) {
+                tc_fence_after();
+                const uint32_t a0 = tc_smem_u32(sA), b0 = tc_smem_u32(sB) + (uint32_t)(ph * RT_B_PHASE);
+                const int live = min(RT_KH, n - ph * RT_KH);
+                const int nks = (live + TcTF32::MMA_K - 1) / TcTF32::MMA_K;
+                // part products (A part, B part), largest first
+                auto product = [&](int ia, int ib, bool first) {
+                    for (int ks = 0; ks < nks; ++ks) {
+                        const uint64_t da = tc_desc(a0 + ia * RT_A_PART + ks * 2 * TC_A_LBO, TC_A_LBO, 128);
+                        const uint64_t db = tc_desc(b0 + ib * RT_B_PART + ks * 2 * TC_B_LBO, TC_B_LBO, 128);
+                        tc_mma<TcTF32>(tmem, da, db, idesc, (!first || ks > 0) ? 1u : 0u);
+                    }
+                };
+                product(0, 0, ph == 0);
+                product(0, 1, false);
+                product(1, 0, false);
+                product(0, 2, false);
+                product(1, 1, false);
+                product(2, 0, false);
+                tc_commit(&bar);
+            }
+            if (failed) break;
+            ++ncommit;
+            // the next phase's values, or the next tile's first, in flight while the MMAs run
+            if (ph + 1 < nph) load_a(t, ph + 1);
+            else if (t + (int)gridDim.x < ntiles) load_a(t + gridDim.x, 0);
+        }
+        if (failed) break;
+        wait_last();  // the tile's MMAs are done: TMEM and the A stages may be read
+        if (!ok) failed = 1;
+        __syncthreads();
+        if (failed) break;
+        tc_fence_after();
+        {
+            const uint32_t lane_base = (uint32_t)(sub4 * 32) << 16;
+            const int rr = sub4 * 32 + lane;
+            for (int cb = chalf * 32; cb < min(p, chalf * 32 + 32); cb += 8) {
+                float x[8];
+                tc_ld8(tmem + lane_base + (uint32_t)cb, x);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int q = 0; q < 8; ++q) ct[(cb + q) * CT_LD + rr] = x[q];
+            }
+        }
+        tc_fence_before();  // the accumulator reads are complete before the next tile's MMAs
+        __syncthreads();
+        const bool vecC = rl + 4 <= rows && ((reinterpret_cast<uintptr_t>(J.C) & 15) == 0) && ((J.ldc & 3) == 0) &&
+                          (!J.sub || (((reinterpret_cast<uintptr_t>(J.sub) & 15) == 0) && ((J.ldsub & 3) == 0)));
+        for (int col = warp; col < p; col += RT_THREADS / 32) {
+            float4 y = *reinterpret_cast<const float4*>(ct + col * CT_LD + rl);
+            const long long cbase = (long long)(r0 + rl) + (long long)col * J.ldc;
+            double cs = 0.0;
+            if (vecC) {
+                if (J.sub) {
+                    const float4 sv =
+                        *reinterpret_cast<const float4*>(J.sub + (long long)(r0 + rl) + (long long)col * J.ldsub);
+                    y = make_float4(sv.x - y.x, sv.y - y.y, sv.z - y.z, sv.w - y.w);
+                }
+                *reinterpret_cast<float4*>(J.C + cbase) = y;
+                cs = (double)y.x + (double)y.y + (double)y.z + (double)y.w;
+            } else {
+                float yv[4] = {y.x, y.y, y.z, y.w};
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (rl + u < rows) {
+                        if (J.sub) yv[u] = J.sub[(long long)(r0 + rl + u) + (long long)col * J.ldsub] - yv[u];
+                        J.C[cbase + u] = yv[u];
+                        cs += (double)yv[u];
+                    }
+            }
+            if (J.colsum) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, o);
+                if (lane == 0) J.colsum[(long long)t * p + col] = cs;
+            }
+        }
+        __syncthreads();  // every warp is done with the tile before the next tile's A parts overwrite it
+    }
+    if (failed) {
+        tc_mbar_wait(&bar, (uint32_t)((ncommit - 1) & 1));  // bounded: own MMAs done
+        if (tid == 0) check_fail(10, 1, (unsigned)blockIdx.x);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64) : "memory");
+}
+
+static int launch_rowmul_tc(const ssa_rowmul_job* jobs, int njobs, int maxrows, cudaStream_t st) {
+    cudaError_t e = cudaFuncSetAttribute(k_rowmul_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, RT_SMEM);
+    if (e != cudaSuccess) return (int)e;
+    k_split_b<<<njobs, 256, 0, st>>>(jobs);
+    if ((e = cudaGetLastError()) != cudaSuccess) return launched(e);
+    launched(e);
+    const int tiles = (maxrows + SSA_ROWMUL_ROWS - 1) / SSA_ROWMUL_ROWS;
+    k_rowmul_tc<<<dim3((tiles + RT_TPC - 1) / RT_TPC, njobs), RT_THREADS, RT_SMEM, st>>>(jobs);
+    return launched(cudaGetLastError());
+}

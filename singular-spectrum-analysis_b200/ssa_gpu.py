@@ -133,6 +133,8 @@ _sig("ssa_b200_set_wcorr_tensor_cores", _V, _I)
 _sig("ssa_b200_wcorr_tensor_cores", _I)
 _sig("ssa_b200_set_wcorr_gram", _I, _I)
 _sig("ssa_b200_wcorr_gram", _I)
+_sig("ssa_b200_set_rowmul_tensor_cores", _V, _I)
+_sig("ssa_b200_rowmul_tensor_cores", _I)
 _sig("ssa_b200_set_context_recycling", _V, _I)
 _sig("ssa_b200_context_recycling", _I)
 _sig("ssa_b200_device_checks", _I, ctypes.POINTER(ctypes.c_uint), _I)
@@ -163,6 +165,16 @@ def set_wcorr_gram(mode: int) -> None:
 
 def wcorr_gram() -> int:
     return int(_lib.ssa_b200_wcorr_gram())
+
+
+def set_rowmul_tensor_cores(on: bool) -> None:
+    """Row products of the randomized pipelines on the tensor cores (three-part TF32 split, six
+    products) or in FP32 on the CUDA cores (default)."""
+    _lib.ssa_b200_set_rowmul_tensor_cores(1 if on else 0)
+
+
+def rowmul_tensor_cores() -> bool:
+    return bool(_lib.ssa_b200_rowmul_tensor_cores())
 
 
 def set_context_recycling(on: bool) -> None:

@@ -125,3 +125,43 @@ def test_wcorr_gram_arithmetics_in_uneven_batch(gpu, oracle):
             assert np.array_equal(out[mode][0][s], ref[0][s])
             assert np.max(np.abs(out[mode][1][s] - ref[1][s])) <= bar, (mode, s)
     assert gpu.device_checks(reset=True)[0] == 0
+
+
+def test_rowmul_tensor_cores_match_cuda_cores(gpu, oracle):
+    """Row products on the tensor cores (three-part TF32 split, six products, FP32 accumulation in
+    TMEM) against the FP32 CUDA-core form, in the single-series API and the uneven batch: both
+    round like an FP32 product, so sigma and the group reconstructions agree to ~1e-6 relative,
+    and each stays within 1e-5 of the FP64 oracle (same device test matrices, q = 2)."""
+    x, _, Om = oracle.config1(seed=3)
+    N, L, k = 1000, 250, 50
+    mix = oracle.config3_batch(8, seed=19, nmin=500, nmax=100000)
+    res = {}
+    try:
+        for on in (False, True):
+            gpu.set_rowmul_tensor_cores(on)
+            assert gpu.rowmul_tensor_cores() == on
+            s = gpu.SSA(x, L)
+            s.decompose(k, oversampling=10, power_iters=2, omega=Om)
+            rb = gpu.SSARaggedBatch(oversampling=10, power_iters=2, groups=[[0], [1, 2]])
+            sig, W, G = rb.run([m[0] for m in mix], [m[1] for m in mix], [m[2] for m in mix], seed=5)
+            res[on] = (s.singular_values.copy(), s.reconstruct([0]), s.reconstruct([1, 2]), sig, G)
+    finally:
+        gpu.set_rowmul_tensor_cores(False)
+    assert gpu.device_checks(reset=True)[0] == 0
+    a, b = res[True], res[False]
+    d = oracle.decompose_randomized(x, L, k, 10, Om, q=2)
+    rel = lambda u, v: float(np.linalg.norm(u - v) / np.linalg.norm(v))  # noqa: E731
+    assert np.max(np.abs(a[0][:3] - b[0][:3]) / b[0][:3]) < 2e-6
+    assert rel(a[1], b[1]) < 5e-6 and rel(a[2], b[2]) < 5e-6
+    assert np.max(np.abs(a[0][:3] - d.sigma[:3]) / d.sigma[:3]) < 1e-5
+    assert rel(a[1], oracle.reconstruct(d, [0], N, L)) < 1e-5
+    assert rel(a[2], oracle.reconstruct(d, [1, 2], N, L)) < 1e-5
+    worst = 0.0
+    for i, (xs, Ls, ks) in enumerate(mix):
+        kk = min(ks, len(a[3][i]))
+        e = np.max(np.abs(a[3][i][:3] - b[3][i][:3]) / b[3][i][:3])
+        worst = max(worst, e)
+        assert e < 2e-6, (i, e)
+        for g in range(2):
+            assert rel(a[4][i][g], b[4][i][g]) < 5e-6, (i, g)
+    print(f"\nrow products tensor vs CUDA cores: sigma 0-2 max rel {worst:.2e}")
