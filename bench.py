@@ -160,6 +160,16 @@ def corr_flops(N: int, L: int, k: int, p: int, q: int, M: int) -> float:
     return (2 * q + 2) * kp * (10.0 * H * math.log2(H) + 12.0 * H)
 
 
+def elem_bytes(N: int, L: int, k: int, p: int, want_w: bool) -> int:
+    """Algorithmic FP32 bytes of the elementary reconstructions of one series: per computed
+    component its sigma u (L) and v (K) columns read and its N-point reconstruction written (all k
+    components for a W-correlation request, components 0..2 for groups [0], [1, 2])."""
+    K = N - L + 1
+    kk = min(k, k + p, L, K)
+    n = kk if want_w else min(kk, 3)
+    return 4 * n * (L + K + N)
+
+
 def corr_bytes(N: int, L: int, k: int, p: int, q: int) -> int:
     """Algorithmic FP32 bytes of the correlation sweeps of one series: the generated first sweep
     writes Y (L x kp); every other sweep reads one block and writes the other."""
@@ -516,12 +526,19 @@ def device_steps(gpu, torch, a, rank: int, world: int) -> dict:
         total_ms = float(t.item())
     cb = sum(corr_bytes(N, L, k, a.p, a.q) for N, L, k in zip(Ns, Ls, ks))
     cf = sum(corr_flops(N, L, k, a.p, a.q, gpu.fft_length(N)) for N, L, k in zip(Ns, Ls, ks))
+    # the same flops at the shortest transform a linear correlation of N points needs (M = N,
+    # rounded to even): padding to the FFT lengths the kernels use does not count as work
+    cf_min = sum(corr_flops(N, L, k, a.p, a.q, N + (N & 1)) for N, L, k in zip(Ns, Ls, ks))
+    eb = sum(elem_bytes(N, L, k, a.p, bool(w)) for N, L, k, w in zip(Ns, Ls, ks, want_w))
+    elem_ms, elem_n = prof.get("elem_recon", (0.0, 0))
     corr_ms, corr_n = prof["corr"]
     peak, peak_kind = measured_peak_hbm()
     per_launch = cb / max(corr_n, 1)
     avg_ms = corr_ms / max(corr_n, 1)
     achieved = per_launch / (avg_ms / 1e3) / 1e9
     tflops = cf / (corr_ms / 1e3) / 1e12 if corr_ms > 0 else 0.0
+    tflops_min = cf_min / (corr_ms / 1e3) / 1e12 if corr_ms > 0 else 0.0
+    elem_gbs = eb / (elem_ms / 1e3) / 1e9 if elem_ms > 0 else 0.0
     tot = max(sum(v[0] for v in prof.values()), 1e-9)
     out = {"value": a.batch * a.steps * world / (total_ms / 1e3), "ms_per_step": total_ms / a.steps,
            "step_ms": step_ms, "launches": launches, "acc_jobs": acc_jobs,
@@ -534,12 +551,22 @@ def device_steps(gpu, torch, a, rank: int, world: int) -> dict:
                         "traffic_source": "ncu dram__bytes_read+write / algorithmic bytes of captured launches "
                                           "(k_corr<13> 0.985, k_cl_col<6,1> 1.002 / 0.980) x this launch's bytes",
                         "avg_launch_ms": avg_ms, "algorithmic_bytes_per_launch": per_launch,
-                        "compute": {"bound": "fp32 issue", "achieved_tflops": tflops,
+                        "compute": {"bound": "fp32 issue", "achieved_tflops": tflops_min,
+                                    "achieved_tflops_at_used_lengths": tflops,
                                     "peak_tflops": FP32_NOMINAL_TFLOPS,
                                     "peak_source": "nominal FP32 SIMT peak (148 SMs x 128 lanes x 2 x 1.965 GHz)",
-                                    "frac": tflops / FP32_NOMINAL_TFLOPS},
+                                    "frac": tflops_min / FP32_NOMINAL_TFLOPS,
+                                    "what": "FFT flops (10 H log2 H + 12 H per probe column and sweep) counted at "
+                                            "H = N/2, the shortest linear-correlation length, over the correlation "
+                                            "launches' CUDA-event time; at the padded lengths the kernels use: "
+                                            "achieved_tflops_at_used_lengths"},
                         "note": "per-launch CUDA-event times of one extra step with the FFT-length buckets "
-                                "run one after another (the timed steps overlap them)"}}
+                                "run one after another (the timed steps overlap them)"},
+           "roofline_elem_recon": {"bound": "hbm", "kernel": "k_elem_recon / k_elem_recon1 / k_cl_col<C,CL_ELEM>",
+                                   "achieved": elem_gbs, "peak": peak, "unit": "GB/s", "frac": elem_gbs / peak,
+                                   "peak_source": peak_kind, "launches": elem_n, "ms": elem_ms,
+                                   "what": "4 n (L + K + N) bytes per series (n computed components: k for W, else 3) "
+                                           "over the elementary-reconstruction launches' CUDA-event time"}}
     del rb, d_x
     torch.cuda.empty_cache()
     return out
@@ -795,7 +822,7 @@ def main():
             "warmup": a.warmup, "ms_per_step": dev["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32 (FP64 Gram/Cholesky/Rayleigh-Ritz/LRF)", "data": "synthetic",
             "config": cfg, "gpu_launches": dev["launches"], "kernel_share": dev["share"],
-            "roofline": dev["roofline"], "clocks": dev["clocks"],
+            "roofline": dev["roofline"], "roofline_elem_recon": dev["roofline_elem_recon"], "clocks": dev["clocks"],
             "value_what": f"series/s of the uneven-batch pipeline (ssa_rbatch_run_device) over {a.batch} stream "
                           f"decompositions per step (mean N {dev['mean_N']:.0f}), each with the outputs of its "
                           "request type in the stream's 50:20 ratio: decompose + reconstruct -> sigma and groups "

@@ -310,7 +310,13 @@ int ssae_create_light(ssa_engine *e, size_t arena_bytes, cudaStream_t stream)
     }
     else
     {
-        CK(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+        /* recycled like a full engine: a growing job arena then frees in stream order and keeps
+         * its old page-locked block for reuse, instead of synchronising the device */
+        e->recycle = g_recycle_on;
+        if (e->recycle)
+            CK(stream_take(e->device, &e->st));
+        else
+            CK(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
         e->own_stream = 1;
     }
     return ssae_grow_arena(e, arena_bytes);
@@ -320,15 +326,16 @@ int ssae_grow_arena(ssa_engine *e, size_t bytes)
 {
     if (bytes <= e->ja.cap)
         return 0;
-    /* freeing page-locked and device memory waits for the whole device: grow by at least half
-     * again, so that a slowly growing workload pays that wait a few times, not once per batch */
-    if (e->ja.cap > 0 && bytes < e->ja.cap + e->ja.cap / 2)
-        bytes = e->ja.cap + e->ja.cap / 2;
+    /* growing waits for this engine's stream (and, without recycling, frees that wait for the
+     * whole device): at least double, so that a growing workload pays it a few times, not once
+     * per batch */
+    if (e->ja.cap > 0 && bytes < 2 * e->ja.cap)
+        bytes = 2 * e->ja.cap;
     {
         const char *ev = getenv("SSA_SERVER_TRACE");
         if (ev && ev[0] == '1' && e->ja.cap > 0)
-            fprintf(stderr, "ssa_engine: job arena grows %zu -> %zu bytes (frees synchronise the device)\n",
-                    e->ja.cap, bytes);
+            fprintf(stderr, "ssa_engine: job arena grows %zu -> %zu bytes%s\n", e->ja.cap, bytes,
+                    e->recycle ? "" : " (frees synchronise the device)");
     }
     if (e->st)
         CK(cudaStreamSynchronize(e->st));

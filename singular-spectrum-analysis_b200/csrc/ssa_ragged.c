@@ -1181,8 +1181,17 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
         size_t arena = ((size_t)b->nb * sizeof(ssa_col_job) + 16 * 6) * (size_t)(16 + 6 * rb->q) + (1 << 16);
         if (b->multi)
             arena += (size_t)(2 * rb->q + 2) * ((size_t)SSA_MAX_KP * b->nb + 2) * sizeof(ssa_tile);
+        const void *ja_old = b->e.ja.d;
         if (ssae_grow_arena(&b->e, arena) != 0)
             return -1;
+        if (ja_old && b->e.ja.d != ja_old)
+        {
+            /* captured graphs copy from and read the old staging areas: drop them (the previous
+             * run, graphs included, has completed: quiesce waited for it) */
+            for (int i = 0; i < 4; i++)
+                graph_free(&rb->graphs[i]);
+            rb->last_sig = 0;
+        }
         b->sz[0] = oX * sizeof(float); /* X */
         b->sz[1] = oY * sizeof(float);
         b->sz[2] = oZ * sizeof(float);

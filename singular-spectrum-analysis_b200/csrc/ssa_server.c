@@ -660,10 +660,10 @@ static int slot_launch(ssa_server *s, slot_t *sl)
             cudaFreeHost(sl->h_seg);
         sl->h_seg = sl->h_seg_d = NULL;
         sl->c_seg = 0;
-        if (cudaMallocHost((void **)&sl->h_seg, sizeof(ssa_copy_seg) * (nseg + nseg / 2)) != cudaSuccess ||
+        if (cudaMallocHost((void **)&sl->h_seg, sizeof(ssa_copy_seg) * (2 * nseg + 1024)) != cudaSuccess ||
             !(sl->h_seg_d = (ssa_copy_seg *)mapped(sl->h_seg)))
             return -1;
-        sl->c_seg = nseg + nseg / 2;
+        sl->c_seg = 2 * nseg + 1024;
     }
     /* inputs: one gather launch reading the callers' page-locked buffers, and the staging area
      * that the pageable ones are copied into */
