@@ -30,6 +30,7 @@
 #include <cuda_runtime_api.h>
 
 #include "ssa_engine.h"
+#include "ssa_ragged_int.h"
 #include "../../include/ssa_opt.h"
 
 #define CK(x)                  \
@@ -44,6 +45,7 @@
  * 3 * 2^13, 3 * 2^14 between the cluster powers of two */
 #define RB_MIN_LOGH 4
 #define RB_NB SSA_FFT_NCODES
+_Static_assert(RB_NB == SSAR_NB, "bucket count of the internal header");
 
 typedef struct
 {
@@ -220,6 +222,13 @@ static int gram_rows(int m, int nb) { return gram_rows_for(m, nb, -1); }
 
 /* The library's stream-ordered memory pool on the current device: freed blocks stay cached in
  * it (release threshold at its maximum), so re-growing buffers costs no driver allocation. */
+int ssar_bucket_index(int N) { return bucket_of(ssad_fft_code_for(N)); }
+
+cudaStream_t ssar_bucket_stream(const ssa_rbatch *rb, int g)
+{
+    return (rb && g >= 0 && g < RB_NB && rb->bk[g].live && rb->bk[g].nb) ? rb->bk[g].e.st : NULL;
+}
+
 cudaMemPool_t ssar_pool(void)
 {
     static cudaMemPool_t pools[64];

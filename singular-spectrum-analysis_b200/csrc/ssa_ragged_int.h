@@ -42,6 +42,13 @@ int ssar_series_factors(const ssa_rbatch *rb, int s, const float **U, const floa
 int ssab_cadzow_from(const double *x, const double *y1, int N, int L, int rank, int max_iter, double tol,
                      double *output, SSA_CadzowResult *result);
 cudaStream_t ssar_main_stream(const ssa_rbatch *rb);
+/* FFT-length bucket a series of length N runs in (0 .. SSAR_NB - 1), and a bucket's stream after
+ * a run (NULL for a bucket the run did not use). Outside graph replays, work a caller enqueues
+ * on a bucket's stream after ssar_run_enqueue_ex follows that bucket's part of the run and
+ * nothing else. */
+#define SSAR_NB 19
+int ssar_bucket_index(int N);
+cudaStream_t ssar_bucket_stream(const ssa_rbatch *rb, int g);
 const int *ssar_status(const ssa_rbatch *rb);
 const int *ssar_lrf_status(const ssa_rbatch *rb);
 const double *ssar_sigma(const ssa_rbatch *rb);

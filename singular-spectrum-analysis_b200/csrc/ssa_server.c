@@ -6,7 +6,9 @@
  * and taken in arrival order. Decompositions are gathered into uneven batches (ssa_ragged.c),
  * each batch bounded by a device-memory share of the HBM budget; up to `max_inflight` batches
  * run at once on their own streams, so requests that arrive while others are on the GPU start
- * as soon as a batch slot is free and overlap with the running ones. A decomposition request
+ * as soon as a batch slot is free and overlap with the running ones. A batch is ordered by
+ * FFT-length bucket, and each bucket's requests complete when that bucket's part of the run and
+ * its output copies are done, ahead of the batch's longer buckets. A decomposition request
  * leaves its series resident: its factors U, V, sigma, its signal, the LRF coefficients of the
  * forecast group [0, 1, 2] and the last L - 1 values of that group's reconstruction stay in
  * device memory (stream-ordered pool, least recently used entries evicted beyond the resident
@@ -93,6 +95,12 @@ typedef struct
     size_t c_dx;
     size_t bytes, in_used, out_used;
     cudaEvent_t done;
+    /* per-bucket completion: the batch is ordered by FFT-length bucket; range r holds requests
+     * rlo[r] .. rhi[r] - 1 of one bucket, whose outputs and status words are copied on that
+     * bucket's stream and which complete when rev[r] has fired, ahead of the rest of the batch */
+    int nrange;
+    int rlo[SSAR_NB], rhi[SSAR_NB], rdone[SSAR_NB];
+    cudaEvent_t rev[SSAR_NB];
 } slot_t;
 
 typedef struct
@@ -619,10 +627,78 @@ static int slot_reserve(slot_t *sl, int n)
     return 0;
 }
 
+/* Order the gathered batch by FFT-length bucket (arrival order kept within a bucket) and record
+ * the bucket ranges. Every request carries its own seed and buffers, so the order changes no
+ * result. */
+static int slot_order(slot_t *sl)
+{
+    const int n = sl->n;
+    int cnt[SSAR_NB + 1] = {0};
+    int *bk = (int *)malloc(sizeof(int) * (size_t)n), *pos = (int *)malloc(sizeof(int) * (size_t)n);
+    void *tmp = malloc((sizeof(void *) * 4 + sizeof(size_t)) * (size_t)n);
+    if (!bk || !pos || !tmp)
+    {
+        free(bk);
+        free(pos);
+        free(tmp);
+        return -1;
+    }
+    for (int i = 0; i < n; i++)
+    {
+        bk[i] = ssar_bucket_index(sl->N[i]);
+        cnt[bk[i] + 1]++;
+    }
+    for (int g = 0; g < SSAR_NB; g++)
+        cnt[g + 1] += cnt[g];
+    sl->nrange = 0;
+    for (int g = 0; g < SSAR_NB; g++)
+        if (cnt[g + 1] > cnt[g])
+        {
+            sl->rlo[sl->nrange] = cnt[g];
+            sl->rhi[sl->nrange] = cnt[g + 1];
+            sl->rdone[sl->nrange] = 0;
+            sl->nrange++;
+        }
+    for (int i = 0; i < n; i++)
+        pos[i] = cnt[bk[i]]++;
+#define SRV_PERMUTE(arr, T)                                 \
+    do                                                      \
+    {                                                       \
+        T *t_ = (T *)tmp;                                   \
+        for (int i_ = 0; i_ < n; i_++)                      \
+            t_[pos[i_]] = (arr)[i_];                        \
+        memcpy((arr), t_, sizeof(T) * (size_t)n);           \
+    } while (0)
+    SRV_PERMUTE(sl->req, ssa_request *);
+    SRV_PERMUTE(sl->N, int);
+    SRV_PERMUTE(sl->L, int);
+    SRV_PERMUTE(sl->k, int);
+    SRV_PERMUTE(sl->seeds, unsigned long long);
+    SRV_PERMUTE(sl->lrf_dst, double *);
+    SRV_PERMUTE(sl->res, res_entry *);
+    SRV_PERMUTE(sl->wantw, unsigned char);
+    SRV_PERMUTE(sl->sin, size_t);
+    SRV_PERMUTE(sl->sout, size_t);
+#undef SRV_PERMUTE
+    {
+        double **t4 = (double **)tmp;
+        for (int i = 0; i < n; i++)
+            memcpy(t4 + 4 * (size_t)pos[i], sl->hp + 4 * (size_t)i, sizeof(double *) * 4);
+        memcpy(sl->hp, t4, sizeof(double *) * 4 * (size_t)n);
+    }
+    free(bk);
+    free(pos);
+    free(tmp);
+    return 0;
+}
+
 /* Launch the batch gathered in sl (sl->n requests, dims and staging offsets filled). */
 static int slot_launch(ssa_server *s, slot_t *sl)
 {
     const double t0 = ssa_server_now();
+    sl->nrange = 0;
+    if (slot_order(sl) != 0)
+        return -1;
     size_t nx = 0;
     for (int i = 0; i < sl->n; i++)
     {
@@ -686,45 +762,56 @@ static int slot_launch(ssa_server *s, slot_t *sl)
     if (ssar_run_enqueue_ex(sl->rb, sl->n, sl->N, sl->L, sl->k, sl->d_x, sl->seeds, sl->lrf_dst, sl->wantw) != 0)
         return -1;
     const double t2 = ssa_server_now();
-    /* outputs the requests ask for: one scatter launch writing the callers' page-locked buffers,
-     * or the staging area slot_finish copies from */
+    /* outputs the requests ask for, per FFT-length bucket on its stream: one scatter launch writing
+     * the callers' page-locked buffers, or the staging area finish_range copies from */
     const size_t *off = ssar_offsets(sl->rb);
     const double *dsig = ssar_sigma(sl->rb), *dW = ssar_W(sl->rb), *dg = ssar_groups(sl->rb);
-    for (int i = 0; i < sl->n; i++)
+    const int *dst = ssar_status(sl->rb), *dlst = ssar_lrf_status(sl->rb);
+    for (int rg = 0; rg < sl->nrange; rg++)
     {
-        ssa_request *r = sl->req[i];
-        const size_t ke = (size_t)req_kout(s, r);
-        const int direct = sl->sout[i] == SRV_DIRECT;
-        size_t so = sl->sout[i];
-        if (r->sigma)
+        const int lo = sl->rlo[rg], hi = sl->rhi[rg];
+        cudaStream_t bs = ssar_bucket_stream(sl->rb, ssar_bucket_index(sl->N[lo]));
+        if (!bs)
+            return -1;
+        const size_t seg0 = ns;
+        for (int i = lo; i < hi; i++)
         {
-            seg_add(sl->h_seg, &ns, dsig + off[4 * i + 1], direct ? sl->hp[4 * i + 1] : sl->h_out_d + so, ke);
-            so += ke;
+            ssa_request *r = sl->req[i];
+            const size_t ke = (size_t)req_kout(s, r);
+            const int direct = sl->sout[i] == SRV_DIRECT;
+            size_t so = sl->sout[i];
+            if (r->sigma)
+            {
+                seg_add(sl->h_seg, &ns, dsig + off[4 * i + 1], direct ? sl->hp[4 * i + 1] : sl->h_out_d + so, ke);
+                so += ke;
+            }
+            if (r->type == SSA_REQ_DECOMPOSE_RECON && r->groups)
+                seg_add(sl->h_seg, &ns, dg + off[4 * i + 3], direct ? sl->hp[4 * i + 2] : sl->h_out_d + so,
+                        2 * (size_t)r->N);
+            if (r->type == SSA_REQ_DECOMPOSE_WCORR && r->W)
+                seg_add(sl->h_seg, &ns, dW + off[4 * i + 2], direct ? sl->hp[4 * i + 3] : sl->h_out_d + so, ke * ke);
+            /* the series stays resident: sigma, signal and the factor blocks (floats copied as pairs;
+             * both leading dimensions are multiples of 4) */
+            res_entry *e = sl->res[i];
+            const float *U = NULL, *V = NULL;
+            if (e && e->d && ssar_series_factors(sl->rb, i, &U, &V) == e->k)
+            {
+                seg_add(sl->h_seg, &ns, dsig + off[4 * i + 1], e->sig, (size_t)e->k);
+                seg_add(sl->h_seg, &ns, sl->d_x + sl->xoff[i], e->x, (size_t)e->N);
+                seg_add(sl->h_seg, &ns, (const double *)U, (double *)e->U, (size_t)(e->ldL * e->k / 2));
+                seg_add(sl->h_seg, &ns, (const double *)V, (double *)e->V, (size_t)(e->ldK * e->k / 2));
+            }
         }
-        if (r->type == SSA_REQ_DECOMPOSE_RECON && r->groups)
-            seg_add(sl->h_seg, &ns, dg + off[4 * i + 3], direct ? sl->hp[4 * i + 2] : sl->h_out_d + so,
-                    2 * (size_t)r->N);
-        if (r->type == SSA_REQ_DECOMPOSE_WCORR && r->W)
-            seg_add(sl->h_seg, &ns, dW + off[4 * i + 2], direct ? sl->hp[4 * i + 3] : sl->h_out_d + so, ke * ke);
-        /* the series stays resident: sigma, signal and the factor blocks (floats copied as pairs;
-         * both leading dimensions are multiples of 4) */
-        res_entry *e = sl->res[i];
-        const float *U = NULL, *V = NULL;
-        if (e && e->d && ssar_series_factors(sl->rb, i, &U, &V) == e->k)
-        {
-            seg_add(sl->h_seg, &ns, dsig + off[4 * i + 1], e->sig, (size_t)e->k);
-            seg_add(sl->h_seg, &ns, sl->d_x + sl->xoff[i], e->x, (size_t)e->N);
-            seg_add(sl->h_seg, &ns, (const double *)U, (double *)e->U, (size_t)(e->ldL * e->k / 2));
-            seg_add(sl->h_seg, &ns, (const double *)V, (double *)e->V, (size_t)(e->ldK * e->k / 2));
-        }
+        /* the bucket's outputs and status words, on its stream right after its part of the run */
+        if (ssad_copy_segments(sl->h_seg_d + seg0, (int)(ns - seg0), bs) != 0 ||
+            cudaMemcpyAsync(sl->h_st + lo, dst + lo, sizeof(int) * (size_t)(hi - lo), cudaMemcpyDeviceToHost, bs) !=
+                cudaSuccess ||
+            cudaMemcpyAsync(sl->h_lst + lo, dlst + lo, sizeof(int) * (size_t)(hi - lo), cudaMemcpyDeviceToHost, bs) !=
+                cudaSuccess ||
+            cudaEventRecord(sl->rev[rg], bs) != cudaSuccess || cudaStreamWaitEvent(ms, sl->rev[rg], 0) != cudaSuccess)
+            return -1;
     }
-    if (ssad_copy_segments(sl->h_seg_d + nin, (int)(ns - nin), ms) != 0)
-        return -1;
-    if (cudaMemcpyAsync(sl->h_st, ssar_status(sl->rb), sizeof(int) * sl->n, cudaMemcpyDeviceToHost, ms) !=
-            cudaSuccess ||
-        cudaMemcpyAsync(sl->h_lst, ssar_lrf_status(sl->rb), sizeof(int) * sl->n, cudaMemcpyDeviceToHost, ms) !=
-            cudaSuccess ||
-        cudaEventRecord(sl->done, ms) != cudaSuccess)
+    if (cudaEventRecord(sl->done, ms) != cudaSuccess)
         return -1;
     sl->busy = 1;
     s->stats.batches++;
@@ -741,10 +828,12 @@ static int slot_launch(ssa_server *s, slot_t *sl)
     return 0;
 }
 
-static void slot_finish(ssa_server *s, slot_t *sl, int launch_ok)
+/* Complete requests lo .. hi - 1 of the slot's batch (their outputs and status words are on
+ * the host). */
+static void finish_range(ssa_server *s, slot_t *sl, int lo, int hi, int launch_ok)
 {
     const double t0 = ssa_server_now();
-    for (int i = 0; i < sl->n; i++)
+    for (int i = lo; i < hi; i++)
     {
         ssa_request *r = sl->req[i];
         int ok = launch_ok && sl->h_st[i] == 0;
@@ -775,10 +864,29 @@ static void slot_finish(ssa_server *s, slot_t *sl, int launch_ok)
         }
         finish_request(s, r, ok ? 0 : -1);
     }
+    s->stats.host_finish_s += ssa_server_now() - t0;
+}
+
+static void slot_release(slot_t *sl)
+{
     sl->n = 0;
+    sl->nrange = 0;
     sl->busy = 0;
     sl->in_used = sl->out_used = 0;
-    s->stats.host_finish_s += ssa_server_now() - t0;
+}
+
+/* Complete every request of the batch not completed yet and free the slot. */
+static void slot_finish(ssa_server *s, slot_t *sl, int launch_ok)
+{
+    if (sl->nrange == 0)
+        finish_range(s, sl, 0, sl->n, launch_ok);
+    for (int r = 0; r < sl->nrange; r++)
+        if (!sl->rdone[r])
+        {
+            finish_range(s, sl, sl->rlo[r], sl->rhi[r], launch_ok);
+            sl->rdone[r] = 1;
+        }
+    slot_release(sl);
 }
 
 /* ---- forecast batches ------------------------------------------------------------------- */
@@ -1162,6 +1270,24 @@ static int poll_done(ssa_server *s)
         slot_t *sl = &s->slots[i];
         if (!sl->busy)
             continue;
+        /* buckets that are done complete their requests now */
+        int open = 0;
+        for (int r = 0; r < sl->nrange; r++)
+        {
+            if (sl->rdone[r])
+                continue;
+            const cudaError_t qr = cudaEventQuery(sl->rev[r]);
+            if (qr == cudaErrorNotReady)
+            {
+                open++;
+                continue;
+            }
+            finish_range(s, sl, sl->rlo[r], sl->rhi[r], qr == cudaSuccess);
+            sl->rdone[r] = 1;
+            progressed = 1;
+        }
+        if (open)
+            continue;
         cudaError_t q = cudaEventQuery(sl->done);
         if (q == cudaErrorNotReady)
             continue;
@@ -1206,9 +1332,9 @@ static void take_queue(ssa_server *s)
 }
 
 /* Size class of a decomposition: series whose transforms run on thread-block clusters (real FFT
- * length above 32768) take several times longer than the rest, and a batch completes as a whole,
- * so they are batched apart: a short series never waits for a long one's batch. Within a class
- * requests keep their arrival order. */
+ * length above 32768) take several times longer than the rest, and a batch slot is busy until
+ * its last bucket is done, so they are batched apart: a short series never waits for a long
+ * one's slot. Within a class requests keep their arrival order. */
 #define SRV_LONG_N 32768
 static int srv_class(const ssa_request *r) { return r->N > SRV_LONG_N; }
 
@@ -1540,6 +1666,7 @@ int ssa_server_create(ssa_server **out, size_t hbm_budget_bytes, int max_infligh
         if (ssa_rbatch_create(&sl->rb, s->p, power_iters, g_group_idx, g_group_sizes, SRV_GROUPS) != 0 ||
             ssar_set_lrf_group(sl->rb, 2, g_fc_group, 3) != 0 ||
             cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming) != cudaSuccess ||
+            ssa_rbatch_set_graphs(sl->rb, 0) != 0 || /* outputs follow each bucket on its stream */
             cudaMallocHost((void **)&sl->h_in, SRV_STAGE_IN) != cudaSuccess ||
             cudaMallocHost((void **)&sl->h_out, SRV_STAGE_OUT) != cudaSuccess ||
             cudaMallocHost((void **)&sl->h_st, sizeof(int) * (size_t)max_batch) != cudaSuccess ||
@@ -1552,6 +1679,12 @@ int ssa_server_create(ssa_server **out, size_t hbm_budget_bytes, int max_infligh
             ssa_server_destroy(s);
             return -1;
         }
+        for (int r = 0; r < SSAR_NB; r++)
+            if (cudaEventCreateWithFlags(&sl->rev[r], cudaEventDisableTiming) != cudaSuccess)
+            {
+                ssa_server_destroy(s);
+                return -1;
+            }
     }
     {
         /* forecast batches: tables for max_batch jobs and 4 MB of outputs up front (grown if a
@@ -1734,6 +1867,9 @@ void ssa_server_destroy(ssa_server *s)
             ssa_rbatch_destroy(sl->rb);
         if (sl->done)
             cudaEventDestroy(sl->done);
+        for (int r = 0; r < SSAR_NB; r++)
+            if (sl->rev[r])
+                cudaEventDestroy(sl->rev[r]);
         void *hp[] = {sl->h_in, sl->h_out, sl->h_st, sl->h_lst, sl->h_seg};
         for (size_t j = 0; j < sizeof(hp) / sizeof(hp[0]); j++)
             if (hp[j])

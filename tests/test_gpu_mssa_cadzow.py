@@ -264,7 +264,32 @@ def test_multichannel_batch_cadzow_vs_oracle(gpu, oracle):
     assert np.all(diff[:, -1] < diff[:, 0])  # the iteration contracts
 
 
+def _oracle_instance(args):
+    import ssa_oracle
+
+    x, L, k, iters, Om = args
+    return ssa_oracle.mssa_cadzow(x, L, k, iters, 10, Om, q=2)
+
+
 def test_multichannel_batch_full_shape(gpu, oracle):
-    """The multichannel workload's shape (16 channels of N = 20000, L = 5000, rank 50): two
-    instances, two Cadzow iterations, instance 1 against the oracle."""
-    _mbatch_check(gpu, oracle, I=2, M=16, N=20000, L=5000, k=50, iters=2, seed=3, check=[1])
+    """The multichannel workload's shape (16 channels of N = 20000, L = 5000, rank 50): four
+    instances in one batch, two Cadzow iterations, every instance against the oracle (computed in
+    four spawned processes)."""
+    import multiprocessing as mp
+    import os
+
+    I, M, N, L, k, iters, seed = 4, 16, 20000, 5000, 50, 2, 3
+    rng = np.random.default_rng(seed)
+    X = np.stack([oracle.config4_instance(rng, Mch=M, N=N) for _ in range(I)])
+    mb = gpu.SSAMultiBatch(I, M, N, L, k, oversampling=10, power_iters=2)
+    out, sig, diff = mb.run(X, iters, seed=seed)
+    K = N - L + 1
+    jobs = [(X[i], L, mb.k, iters, oracle.device_gaussian(oracle.series_seed(seed, i), K, mb.kp)) for i in range(I)]
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "4")
+    with mp.get_context("spawn").Pool(I) as pool:
+        refs = pool.map(_oracle_instance, jobs)
+    lead = min(5, mb.k)
+    for i, (y_ref, s_ref, d_ref) in enumerate(refs):
+        assert np.max(np.abs(sig[i][:lead] - s_ref[:lead]) / s_ref[:lead]) <= 1e-5, i
+        assert rel_l2(out[i], y_ref) <= CADZOW_TOL, (i, rel_l2(out[i], y_ref))
+        assert np.max(np.abs(diff[i] - d_ref)) <= 1e-5, (i, diff[i], d_ref)

@@ -303,3 +303,36 @@ def test_server_cadzow_new_series_and_followup_rejections(gpu, oracle):
     assert r["iterations"] == ref.iterations
     assert rel_l2(r["out"], ref.signal) <= 1e-6
     srv.close()
+
+
+def test_server_short_bucket_completes_ahead_of_batch(gpu, oracle):
+    """One batch of short series (N = 1000, real FFT length 1024) and longer ones (N = 30000,
+    length 32768), offered together: the batch is ordered by FFT-length bucket and each bucket's
+    requests complete when that bucket is done, so every short one finishes before any long one
+    of the same batch; results against the oracle for one of each."""
+    rng = np.random.default_rng(21)
+    short = [oracle.walk_sines(rng, 1000) for _ in range(160)]
+    long_ = [oracle.walk_sines(rng, 30000) for _ in range(24)]
+    srv = gpu.SSAServer(max_inflight=1, oversampling=P, power_iters=Q)
+    R = gpu.Requests(len(short) + len(long_) + 1)
+    # a long-class series first holds the only batch slot, so that the others, submitted
+    # meanwhile, form one batch
+    R.add_decompose(oracle.walk_sines(rng, 90000), 22500, 40, series_id=4999, seed=1)
+    idx_s, idx_l = [], []
+    for j in range(max(len(short), len(long_))):  # interleaved arrival order
+        if j < len(long_):
+            idx_l.append(R.add_decompose(long_[j], 7500, 30, series_id=5000 + j, seed=900 + j))
+        if j < len(short):
+            idx_s.append(R.add_decompose(short[j], 250, 20, series_id=6000 + j, seed=700 + j))
+    srv.run(R, np.zeros(R.n))
+    assert np.all(R.statuses() == 0)
+    assert srv.stats()["batches"] == 2
+    _, td = R.times()
+    assert td[idx_s].max() < td[idx_l].min(), (td[idx_s].max(), td[idx_l].min())
+    for i, x, L, k, sd in ((idx_s[3], short[3], 250, 20, 703), (idx_l[2], long_[2], 7500, 30, 902)):
+        d = oracle_dec(oracle, x, L, k, sd)
+        res = R.result(i)
+        check_sigma(res["sigma"], d.sigma)
+        for gi, g in enumerate(([0], [1, 2])):
+            assert rel_l2(res["groups"][gi], oracle.reconstruct(d, g, len(x), L)) <= rec_tol(d.sigma, g)
+    srv.close()
