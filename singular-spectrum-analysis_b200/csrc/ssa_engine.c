@@ -431,7 +431,7 @@ void ssae_destroy(ssa_engine *e)
     void *bufs[] = {e->x64, e->X, e->Y, e->Z, e->part, e->qsum, e->Rinv, e->Zu, e->Zv,
                     e->sigma, e->status, e->recon, e->norm2, e->W, e->Us, e->Vs, e->ja.d,
                     e->Ub, e->Vb, e->xpart, e->xC, e->sUs, e->sVs, e->sDinv, e->perm, e->sgn,
-                    e->Ut, e->Vt, e->bsplit};
+                    e->Ut, e->Vt, e->bsplit, e->Zs};
     for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
         ssae_dfree(e, bufs[i]);
     ssae_pinned_free(e, e->ja.h, e->ja.hcap);
@@ -1441,20 +1441,114 @@ static int mssab_cholqr(ssa_engine *e, int I, int M, int n, double *colsum)
     return rc;
 }
 
-/* Z_{i M} = sum_m H_{i,m}^T Y_{i,m} for every instance (per-channel adjoints into their Z slots,
- * then a fixed-order channel sum per instance into its first channel's slot). */
+/* Scratch of the stacked forward sweeps: one spectrum of ldS floats per block column of every
+ * instance. */
+static int mssab_scratch(ssa_engine *e, int I)
+{
+    const size_t need = (size_t)I * e->kp * (size_t)e->ldS;
+    if (need <= e->zs_cap)
+        return 0;
+    ssae_dfree(e, e->Zs);
+    e->Zs = NULL;
+    e->zs_cap = 0;
+    CK(ssae_dalloc(e, (void **)&e->Zs, sizeof(float) * need));
+    e->zs_cap = need;
+    return 0;
+}
+
+/* The stacked forward sweeps run fused for the single-CTA transform lengths: each block column
+ * is transformed once for all channels. */
+static int mssab_fused(const ssa_engine *e, int M) { return M > 1 && e->logh <= SSA_ONE_CTA_MAX_LOGH && !ssad_cl14(); }
+
+/* Z_{i M} = sum_m H_{i,m}^T Y_{i,m} for every instance. Fused: the channels' conj-products added
+ * into one accumulator per instance column (a launch per channel, in channel order), then one
+ * inverse transform per column; else per-channel adjoints into their Z slots and a fixed-order
+ * channel sum per instance into its first channel's slot. */
 static int mssab_adjoint(ssa_engine *e, int I, int M, int n)
 {
     const size_t sY = (size_t)e->ldL * e->kp, sZ = (size_t)e->ldK * e->kp;
-    CK(corr_io(e, I * M, n, 1, e->Y, sY, e->ldL, e->Z, sZ, e->ldK));
-    return ssad_slabsum_batch(e->Z, e->Z, (long long)sZ, M, (long long)e->ldK * n, I, (long long)M * sZ, e->st);
+    if (!mssab_fused(e, M))
+    {
+        CK(corr_io(e, I * M, n, 1, e->Y, sY, e->ldL, e->Z, sZ, e->ldK));
+        return ssad_slabsum_batch(e->Z, e->Z, (long long)sZ, M, (long long)e->ldK * n, I, (long long)M * sZ, e->st);
+    }
+    CK(mssab_scratch(e, I));
+    ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)(M + 1) * I, sizeof(ssa_col_job));
+    if (!jobs)
+        return (int)cudaErrorMemoryAllocation;
+    for (int m = 0; m <= M; m++)
+        for (int i = 0; i < I; i++)
+        {
+            ssa_col_job *J = &jobs[(size_t)m * I + i];
+            J->spec = e->Zs + (size_t)i * e->kp * e->ldS;
+            J->ld_spec = e->ldS;
+            J->ncols = n;
+            J->N = e->N;
+            J->L = e->L;
+            J->K = e->K;
+            if (m < M)
+            {
+                J->in = e->Y + (size_t)(i * M + m) * sY;
+                J->ld_in = e->ldL;
+                J->n_in = e->L;
+                J->X = e->X + (size_t)(i * M + m) * e->ldS;
+            }
+            else
+            {
+                J->out = e->Z + (size_t)i * M * sZ;
+                J->ld_out = e->ldK;
+                J->n_out = e->K;
+            }
+        }
+    ssa_col_job *d = (ssa_col_job *)ssae_push_jobs(e, jobs, sizeof(ssa_col_job) * (size_t)(M + 1) * I);
+    free(jobs);
+    if (!d)
+        return (int)cudaErrorMemoryAllocation;
+    ssae_prof_begin(e, SSAK_CORR);
+    int rc = 0;
+    for (int m = 0; m < M && !rc; m++)
+        rc = ssad_corr_acc(d + (size_t)m * I, I, n, e->logh, m == 0, e->st);
+    if (!rc)
+        rc = ssad_corr_spec(d + (size_t)M * I, I, n, e->logh, e->st);
+    ssae_prof_end(e);
+    return rc;
 }
 
-/* Y_{i,m} = H_{i,m} Z_{i M}: every channel of an instance reads the instance's block. */
+/* Y_{i,m} = H_{i,m} Z_{i M}: every channel of an instance reads the instance's block (fused: the
+ * block's columns transformed once, then every channel's product and inverse transform). */
 static int mssab_forward(ssa_engine *e, int I, int M, int n)
 {
     const size_t sY = (size_t)e->ldL * e->kp, sZ = (size_t)e->ldK * e->kp;
     const int B = I * M;
+    const int fused = mssab_fused(e, M);
+    if (fused)
+    {
+        CK(mssab_scratch(e, I));
+        ssa_col_job *sj = (ssa_col_job *)calloc((size_t)I, sizeof(ssa_col_job));
+        if (!sj)
+            return (int)cudaErrorMemoryAllocation;
+        for (int i = 0; i < I; i++)
+        {
+            ssa_col_job *J = &sj[i];
+            J->in = e->Z + (size_t)i * M * sZ;
+            J->ld_in = e->ldK;
+            J->n_in = e->K;
+            J->spec = e->Zs + (size_t)i * e->kp * e->ldS;
+            J->ld_spec = e->ldS;
+            J->ncols = n;
+            J->N = e->N;
+            J->L = e->L;
+            J->K = e->K;
+        }
+        void *d = ssae_push_jobs(e, sj, sizeof(ssa_col_job) * I);
+        free(sj);
+        if (!d)
+            return (int)cudaErrorMemoryAllocation;
+        ssae_prof_begin(e, SSAK_CORR);
+        int rc = ssad_spectrum((const ssa_col_job *)d, I, n, e->logh, e->st);
+        ssae_prof_end(e);
+        CK(rc);
+    }
     ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)B, sizeof(ssa_col_job));
     if (!jobs)
         return (int)cudaErrorMemoryAllocation;
@@ -1468,6 +1562,8 @@ static int mssab_forward(ssa_engine *e, int I, int M, int n)
         J->ld_out = e->ldL;
         J->n_out = e->L;
         J->X = e->X + (size_t)c * e->ldS;
+        J->spec = fused ? e->Zs + (size_t)(c / M) * e->kp * e->ldS : NULL;
+        J->ld_spec = e->ldS;
         J->ncols = n;
         J->N = e->N;
         J->L = e->L;
@@ -1478,7 +1574,8 @@ static int mssab_forward(ssa_engine *e, int I, int M, int n)
     if (!d)
         return (int)cudaErrorMemoryAllocation;
     ssae_prof_begin(e, SSAK_CORR);
-    int rc = ssad_corr((const ssa_col_job *)d, B, n, e->logh, e->st);
+    int rc = fused ? ssad_corr_spec((const ssa_col_job *)d, B, n, e->logh, e->st)
+                   : ssad_corr((const ssa_col_job *)d, B, n, e->logh, e->st);
     ssae_prof_end(e);
     return rc;
 }

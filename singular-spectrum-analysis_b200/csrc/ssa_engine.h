@@ -64,6 +64,8 @@ typedef struct
     int own_stream;
     int recycle;                 /* stream, buffers and pinned arena recycled (own-stream engines) */
     int rowmul_simt;             /* row products on the CUDA cores even when the tensor-core form is on */
+    float *Zs;                   /* stacked sweeps: spectra / accumulators of block columns */
+    size_t zs_cap;               /* floats */
     float *bsplit;               /* tensor-core row products: split parts of the small factor per series */
     size_t bsplit_cap;           /* series the scratch holds */
     /* device buffers */

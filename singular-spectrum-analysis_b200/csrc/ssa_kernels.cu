@@ -292,6 +292,80 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k
                              tw);
 }
 
+// The correlation of k_corr from the input column's real spectrum A (H + 1 bins: A[0], A[H] real,
+// as k_spectrum writes it): P = conj-product with the signal spectrum, packed and transformed
+// back. Bit-identical to k_corr on the same column (the spectrum holds the same FP32 values k_corr
+// forms in registers).
+template <int LOGH>
+__global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k_corr_spec(const ssa_col_job* __restrict__ jobs) {
+    constexpr int H = 1 << LOGH;
+    extern __shared__ float2 smem[];
+    const ssa_col_job J = jobs[blockIdx.y];
+    const int c = blockIdx.x;
+    if (c >= J.ncols) return;
+    float2* tw = smem + spad_size(H);
+    load_twiddles<LOGH + 1>(tw);
+    __syncthreads();
+    const float2* X = reinterpret_cast<const float2*>(J.X);
+    const float2* A = reinterpret_cast<const float2*>(J.spec + (long long)c * J.ld_spec);
+    for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
+        float2 zk, zm;
+        if (k == 0) {
+            if (X) pack_pair(cscale(X[0], A[0].x), cscale(X[H], A[H].x), make_float2(1.f, 0.f), zk, zm);
+            else pack_pair(A[0], A[H], make_float2(1.f, 0.f), zk, zm);
+            smem[spad(0)] = zk;
+        } else {
+            const float2 w = wm<LOGH>(tw, k);
+            if (X) pack_pair(cmulc(X[k], A[k]), cmulc(X[H - k], A[H - k]), w, zk, zm);
+            else pack_pair(A[k], A[H - k], w, zk, zm);
+            smem[spad(k)] = zk;
+            smem[spad(H - k)] = zm;
+        }
+    }
+    __syncthreads();
+    fft_block_io<LOGH, true>(smem, SmemPts{smem}, RealOut{J.out + (long long)c * J.ld_out, J.n_out, 1.0f / (float)H},
+                             tw);
+}
+
+// One channel's term of a stacked adjoint sweep: the forward transform of input column c and its
+// conj-product with the channel's signal spectrum, written (first channel) or added into the
+// column's product accumulator (spec + c ld_spec, H + 1 bins). The channels of one accumulator
+// run as consecutive launches on one stream.
+template <int LOGH>
+__global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k_corr_acc(const ssa_col_job* __restrict__ jobs,
+                                                                                           int first) {
+    constexpr int H = 1 << LOGH;
+    extern __shared__ float2 smem[];
+    const ssa_col_job J = jobs[blockIdx.y];
+    const int c = blockIdx.x;
+    if (c >= J.ncols) return;
+    float2* tw = smem + spad_size(H);
+    load_twiddles<LOGH + 1>(tw);
+    fft_block_io<LOGH, false>(smem, col_pts(J, c), SmemPts{smem}, tw);
+    const float2* X = reinterpret_cast<const float2*>(J.X);
+    float2* acc = reinterpret_cast<float2*>(J.spec + (long long)c * J.ld_spec);
+    for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
+        float2 pk, pm;
+        if (k == 0) {
+            const float2 z0 = smem[spad(0)];
+            pk = cscale(X[0], z0.x + z0.y);
+            pm = cscale(X[H], z0.x - z0.y);
+        } else {
+            float2 ak, am;
+            unpack_pair<LOGH>(smem[spad(k)], smem[spad(H - k)], wm<LOGH>(tw, k), ak, am);
+            pk = cmulc(X[k], ak);
+            pm = cmulc(X[H - k], am);
+        }
+        const int km = k == 0 ? H : H - k;  // k = H / 2 is its own mirror: pk == pm there
+        if (!first) {
+            pk = cadd(pk, acc[k]);
+            pm = cadd(pm, acc[km]);
+        }
+        acc[k] = pk;
+        acc[km] = pm;
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Multi-length persistent correlation sweep
 // ---------------------------------------------------------------------------------------------
@@ -1707,6 +1781,22 @@ static int launch_corr(const ssa_col_job* jobs, int njobs, int maxcols, cudaStre
     return launched(cudaGetLastError());
 }
 template <int LOGH>
+static int launch_corr_spec(const ssa_col_job* jobs, int njobs, int maxcols, cudaStream_t st) {
+    const int sm = smem_bytes<LOGH>(1);
+    cudaError_t e = set_smem(k_corr_spec<LOGH>, sm);
+    if (e != cudaSuccess) return (int)e;
+    k_corr_spec<LOGH><<<dim3(maxcols, njobs), FftShape<LOGH>::BLOCK, sm, st>>>(jobs);
+    return launched(cudaGetLastError());
+}
+template <int LOGH>
+static int launch_corr_acc(const ssa_col_job* jobs, int njobs, int maxcols, int first, cudaStream_t st) {
+    const int sm = smem_bytes<LOGH>(1);
+    cudaError_t e = set_smem(k_corr_acc<LOGH>, sm);
+    if (e != cudaSuccess) return (int)e;
+    k_corr_acc<LOGH><<<dim3(maxcols, njobs), FftShape<LOGH>::BLOCK, sm, st>>>(jobs, first);
+    return launched(cudaGetLastError());
+}
+template <int LOGH>
 static int launch_elem(const ssa_col_job* jobs, int njobs, int maxcols, cudaStream_t st) {
     const int sm = smem_bytes<LOGH>(2);
     if (sm > 227 * 1024) return (int)cudaErrorInvalidValue;
@@ -1812,6 +1902,20 @@ extern "C" int ssad_corr(const ssa_col_job* d_jobs, int njobs, int maxcols, int 
     if (logh > SSA_MAX_LOGH || (logh == 14 && g_cl14))  // 15-18, and 14 on 2-CTA clusters when selected
         return cl_col_dispatch(CL_CORR, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);
 #define CALL(L) return launch_corr<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
+    SSA_LOGH_DISPATCH(logh, CALL)
+#undef CALL
+    return 0;
+}
+extern "C" int ssad_corr_spec(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
+    if (njobs <= 0 || maxcols <= 0) return 0;
+#define CALL(L) return launch_corr_spec<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
+    SSA_LOGH_DISPATCH(logh, CALL)
+#undef CALL
+    return 0;
+}
+extern "C" int ssad_corr_acc(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, int first, void* stream) {
+    if (njobs <= 0 || maxcols <= 0) return 0;
+#define CALL(L) return launch_corr_acc<L>(d_jobs, njobs, maxcols, first, (cudaStream_t)stream)
     SSA_LOGH_DISPATCH(logh, CALL)
 #undef CALL
     return 0;

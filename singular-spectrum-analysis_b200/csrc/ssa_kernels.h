@@ -42,6 +42,8 @@ int ssad_fft_code_for(int N);   /* smallest size code with 2H >= N; -1 beyond N 
 /* Largest bucket: logh 16 (M = 131072, series up to N = 131072). Buckets up to 14 run one CTA
  * per transform, 15 and 16 a thread-block cluster of 4 or 8 CTAs. */
 #define SSA_MAX_LOGH_ALL 16
+/* Largest logh one CTA transforms (H = 16384 points, real length 32768). */
+#define SSA_ONE_CTA_MAX_LOGH 14
 
 /* Column job for the FFT kernels (signal spectrum, correlation matvec, reconstruction). */
 typedef struct
@@ -319,6 +321,15 @@ int ssad_elem_recon1(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh
 #define SSA_ELEM2_MAX_LOGH 13
 int ssad_spectrum(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);
 int ssad_corr(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);
+/* The correlation of ssad_corr from a precomputed real spectrum of each input column (spec +
+ * c ld_spec, H + 1 bins, as ssad_spectrum writes them), single-CTA lengths (logh <= 14): the
+ * forward sweep of every channel of a multichannel operator from one transform of the shared
+ * block column. With X == NULL the spectrum is taken as the product itself (the inverse step of
+ * a stacked adjoint sweep). */
+int ssad_corr_spec(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);
+/* One channel of a stacked adjoint sweep: forward transform of each input column, conj-product
+ * with X, written (first != 0) or added into the column's accumulator at spec + c ld_spec. */
+int ssad_corr_acc(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, int first, void *stream);
 /* Correlation sweeps of series of different FFT lengths in one persistent launch: every CTA
  * (512 threads) pops tiles from tiles[0 .. ntiles) through the counter *head (zero before the
  * launch), largest lengths first. A tile is (job, first column c0, logh): the CTA runs the columns
