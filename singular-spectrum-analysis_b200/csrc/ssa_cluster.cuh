@@ -40,7 +40,6 @@ struct ClShape {
     static constexpr int H = C * H1;
     static constexpr int BLOCK = FftShape<LOGH1>::BLOCK;
     static constexpr int MINB = BLOCK >= 1024 ? 1 : 2;  // CTAs per SM the kernels are built for
-    static constexpr int NITEM = H1 / 2 + 1;  // k1 = 0 .. H1/2, each with its mirror
     static constexpr bool POW2 = (C & (C - 1)) == 0;
     static_assert(POW2 || C % 3 == 0, "cluster sizes are 2^a or 3 * 2^a");
     // twiddle table of resolution M = 2H: 2^LOGM, or 3 * 2^A3
@@ -104,11 +103,11 @@ __device__ __forceinline__ void cl_pair(const ClOp& op, int k, float2& zk, float
             op.spec[H - k] = am;
             return;
         } else if constexpr (KIND == CL_CORR) {
-            pk = cmulc(op.X[k], ak);
-            pm = cmulc(op.X[H - k], am);
+            pk = cmulc(__ldg(op.X + k), ak);
+            pm = cmulc(__ldg(op.X + (H - k)), am);
         } else {
-            pk = cmul(op.us[k], ak);
-            pm = cmul(op.us[H - k], am);
+            pk = cmul(__ldg(op.us + k), ak);
+            pm = cmul(__ldg(op.us + (H - k)), am);
         }
     }
     pack_pair(pk, pm, w, zk, zm);
@@ -124,7 +123,7 @@ __device__ __forceinline__ void cl_dc(const ClOp& op, float2& z0) {
         op.spec[H] = make_float2(z0.x - z0.y, 0.f);
         return;
     } else if constexpr (KIND == CL_CORR) {
-        pack_pair(cscale(op.X[0], z0.x + z0.y), cscale(op.X[H], z0.x - z0.y), make_float2(1.f, 0.f), zk, zm);
+        pack_pair(cscale(__ldg(op.X), z0.x + z0.y), cscale(__ldg(op.X + H), z0.x - z0.y), make_float2(1.f, 0.f), zk, zm);
     } else if constexpr (KIND == CL_ELEM) {
         const float p0 = op.us[0].x * (z0.x + z0.y);
         const float ph = op.us[H].x * (z0.x - z0.y);
@@ -142,9 +141,13 @@ __device__ __forceinline__ uint32_t cl_map(uint32_t local, int q) {
     asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(q));
     return r;
 }
+// The loads carry no memory clobber, so that the compiler may move the independent global loads
+// of the spectral operation (signal spectrum bins) ahead of them; they stay ordered with the
+// volatile stores below, and the cluster barriers around the exchange order them with every
+// other access of the buffers.
 __device__ __forceinline__ float2 cl_ld(uint32_t a) {
     float2 v;
-    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a) : "memory");
+    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
     return v;
 }
 __device__ __forceinline__ void cl_st(uint32_t a, float2 v) {
@@ -171,7 +174,13 @@ template <int C_, int KIND>
 __device__ __forceinline__ void cl_exchange(uint32_t sbase, const float2* twM, int rank, const ClOp& op) {
     using S = ClShape<C_>;
     constexpr int C = S::C, H1 = S::H1, H = S::H;
-    for (int g = rank * S::BLOCK + (int)threadIdx.x; g < S::NITEM; g += C * S::BLOCK) {
+    // Work units u < H1/2, one item each, except that unit 0 takes both items whose bins are
+    // their own mirrors (k1 = 0 and k1 = H1/2), which cost half an item each: H1/2 units of equal
+    // cost, so that with C * BLOCK a divisor of H1/2 (C = 2, 4, 8) no thread runs one item more
+    // than the rest while the cluster waits at its barrier.
+    for (int u = rank * S::BLOCK + (int)threadIdx.x; u < H1 / 2; u += C * S::BLOCK)
+    for (int it = 0; it < (u == 0 ? 2 : 1); ++it) {
+        const int g = it ? H1 / 2 : u;
         const int ka = g, kb = (H1 - g) & (H1 - 1);
         const bool self = ka == kb;  // k1 = 0 or H1/2
         const uint32_t aa = sbase + 8u * (uint32_t)spad(ka), ab = sbase + 8u * (uint32_t)spad(kb);
@@ -246,6 +255,12 @@ struct ClDecim {
     P p;
     int rank;
     static constexpr bool kSmem = false;
+    // local points that can be nonzero, for a reader that knows its global count
+    template <class Q = P>
+    __device__ __forceinline__ auto nz() const -> decltype(std::declval<const Q&>().nz()) {
+        const int t = p.nz() - rank;
+        return t <= 0 ? 0 : (t + C - 1) / C;
+    }
     __device__ __forceinline__ float2 operator()(int m) const { return p(m * C + rank); }
     __device__ __forceinline__ void operator()(int m, float2 v) const { p(m * C + rank, v); }
 };

@@ -3,17 +3,20 @@
 // One CTA transforms one real sequence of length M = 2H (H = 2^LOGH complex points) that is
 // packed as z[n] = a[2n] + i a[2n+1]. The complex FFT of length H runs as a Stockham
 // auto-sort FFT (Govindaraju et al., "High performance discrete Fourier transforms on
-// graphics processors", SC'08) with radix-16 passes held in registers: every thread owns
-// 16 points per pass, loads them, waits at a barrier, applies twiddles and the in-register
-// DFT, and stores them at their auto-sorted positions, so the transform runs in place in one
-// buffer of H points. The buffer is padded by one point per 16 (spad) so that both the
-// strided loads and the auto-sort stores of a half-warp touch 16 distinct 8-byte bank pairs.
+// graphics processors", SC'08) with radix-16 (and lane-pair radix-32) passes held in
+// registers: every thread owns 16 points per pass, loads them, applies twiddles and the
+// in-register DFT, waits at a barrier and stores them at their auto-sorted positions, so the
+// transform runs in place in one buffer of H points. The buffer is padded by one point per 16
+// (spad) so that both the strided loads and the auto-sort stores of a half-warp touch 16
+// distinct 8-byte bank pairs.
 //
 // Twiddles come from one table g_tw[t] = exp(-2 pi i t / TW_N), computed on the host in FP64
 // and rounded to FP32 once per device.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <utility>
 
 #define SSA_TW_LOG 17
 #define SSA_TW_N (1 << SSA_TW_LOG)
@@ -166,14 +169,34 @@ __device__ __forceinline__ void dft8(float2* a) {
     }
 }
 
+// Inner stage of the 16-point DFT below for inputs of which only a[0 .. NZ) may be nonzero
+// (NZ = 4, 8 or 16; a[NZ ..] are not read): DFT4 over a[j + 4l] (l) for each j < 4, with the
+// terms of the zero inputs left out. Equal to the full stage on such inputs (up to the sign of
+// zero results).
+template <bool INV, int NZ>
+__device__ __forceinline__ void dft16_inner(float2* a) {
+    static_assert(NZ == 4 || NZ == 8 || NZ == 16, "inner stage for 4, 8 or 16 nonzero inputs");
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if constexpr (NZ == 16) {
+            dft4s<INV>(a[j], a[j + 4], a[j + 8], a[j + 12]);
+        } else if constexpr (NZ == 8) {
+            const float2 x0 = a[j], x1 = a[j + 4], m1 = mul_mi<INV>(x1);
+            a[j] = cadd(x0, x1);
+            a[j + 4] = cadd(x0, m1);
+            a[j + 8] = csub(x0, x1);
+            a[j + 12] = csub(x0, m1);
+        } else {
+            a[j + 4] = a[j + 8] = a[j + 12] = a[j];
+        }
+    }
+}
+
 // 16 = 4 x 4: inner DFT4 over a[j + 4l] (l), twiddle W16^{jm}, outer DFT4 over j,
-// output index m + 4n.
-template <bool INV>
+// output index m + 4n. With NZ < 16, only a[0 .. NZ) may be nonzero (dft16_inner).
+template <bool INV, int NZ = 16>
 __device__ __forceinline__ void dft16(float2* a) {
-    dft4s<INV>(a[0], a[4], a[8], a[12]);
-    dft4s<INV>(a[1], a[5], a[9], a[13]);
-    dft4s<INV>(a[2], a[6], a[10], a[14]);
-    dft4s<INV>(a[3], a[7], a[11], a[15]);
+    dft16_inner<INV, NZ>(a);
     // b[j][m] sits at a[j + 4m]
     a[5] = w16<INV, 1>(a[5]);
     a[9] = w16<INV, 2>(a[9]);
@@ -259,6 +282,17 @@ struct SmemPts {
     __device__ __forceinline__ void operator()(int i, float2 v) const { s[spad(i)] = v; }
 };
 
+// Point readers that know how many leading points can be nonzero (nz()): the first pass skips
+// the rest.
+template <class P, class = void>
+struct HasNz {
+    static constexpr bool value = false;
+};
+template <class P>
+struct HasNz<P, decltype((void)std::declval<const P&>().nz())> {
+    static constexpr bool value = true;
+};
+
 // One Stockham pass of radix 2^RLOG after 2^LOGNS points have been combined.
 template <int RLOG, int LOGNS, int LOGH, bool INV, class In, class Out>
 __device__ __forceinline__ void fft_pass(const In& in, const Out& out, const float2* tw, int tid) {
@@ -270,55 +304,91 @@ __device__ __forceinline__ void fft_pass(const In& in, const Out& out, const flo
     constexpr int NS = 1 << LOGNS;
     const bool active = tid < T;
     float2 a[16];
-    if (active) {
+    if constexpr (LOGNS == 0 && R == 16 && HasNz<In>::value) {
+        // First pass over a zero-padded column: only the points below in.nz() are nonzero, so a
+        // warp whose points j + r STR (j >= jw, its first thread) are zero from r = 4 or r = 8
+        // on loads and transforms only those (the adjoint sweeps' inputs fill about a fifth of
+        // the transform, the forward sweeps' half to three quarters). The choice is uniform
+        // over the warp; points beyond a thread's own bound read as zero.
+        const int nz = in.nz();
+        const int jw = tid & ~31;
+        const int rmax = nz <= jw ? 0 : (nz - jw + STR - 1) / STR;
+        if (active) {
+            if (rmax <= 4) {
 #pragma unroll
-        for (int b = 0; b < NB; ++b) {
-            const int j = tid + b * T;
+                for (int r = 0; r < 4; ++r) a[r] = in(tid + r * STR);
+                dft16<INV, 4>(a);
+            } else if (rmax <= 8) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) a[b * R + r] = in(j + r * STR);
+                for (int r = 0; r < 8; ++r) a[r] = in(tid + r * STR);
+                dft16<INV, 8>(a);
+            } else {
+#pragma unroll
+                for (int r = 0; r < 16; ++r) a[r] = in(tid + r * STR);
+                dft16<INV>(a);
+            }
+        }
+    } else {
+        if (active) {
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const int j = tid + b * T;
+#pragma unroll
+                for (int r = 0; r < R; ++r) a[b * R + r] = in(j + r * STR);
+            }
+        }
+        if (active) {
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const int j = tid + b * T;
+                const int k = j & (NS - 1);
+                if constexpr (LOGNS > 0) {
+                    // W_{NS R}^{r k} = W_M^{(r k) << (LOGM - LOGNS - RLOG)}, M = 2H
+                    constexpr int SH = LOGH + 1 - LOGNS - RLOG;
+                    if constexpr (R == 16) {
+                        // Two table lookups (w^1, w^4) and at most three complex products for the
+                        // other powers: 4 shared loads instead of 30, ~4 ulp per twiddle.
+                        float2* x = a + b * R;
+                        const float2 w1 = twiddle<LOGH + 1, INV>(tw, k << SH);
+                        const float2 w4 = twiddle<LOGH + 1, INV>(tw, (4 * k) << SH);
+                        const float2 w2 = cmul(w1, w1);
+                        const float2 w3 = cmul(w2, w1);
+                        x[1] = cmul(x[1], w1);
+                        x[2] = cmul(x[2], w2);
+                        x[3] = cmul(x[3], w3);
+                        x[4] = cmul(x[4], w4);
+                        x[5] = cmul(x[5], cmul(w4, w1));
+                        x[6] = cmul(x[6], cmul(w4, w2));
+                        x[7] = cmul(x[7], cmul(w4, w3));
+                        const float2 w8 = cmul(w4, w4);
+                        x[8] = cmul(x[8], w8);
+                        x[9] = cmul(x[9], cmul(w8, w1));
+                        x[10] = cmul(x[10], cmul(w8, w2));
+                        x[11] = cmul(x[11], cmul(w8, w3));
+                        const float2 w12 = cmul(w8, w4);
+                        x[12] = cmul(x[12], w12);
+                        x[13] = cmul(x[13], cmul(w12, w1));
+                        x[14] = cmul(x[14], cmul(w12, w2));
+                        x[15] = cmul(x[15], cmul(w12, w3));
+                    } else {
+#pragma unroll
+                        for (int r = 1; r < R; ++r)
+                            a[b * R + r] = cmul(a[b * R + r], twiddle<LOGH + 1, INV>(tw, (r * k) << SH));
+                    }
+                }
+                dftR<R, INV>(a + b * R);
+            }
         }
     }
+    // an in-place pass overwrites points other threads read: every load is done before any
+    // store (the arithmetic above runs before this barrier, so early warps compute while late
+    // ones are still loading)
     if constexpr (In::kSmem && Out::kSmem) __syncthreads();
     if (active) {
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
             const int j = tid + b * T;
             const int k = j & (NS - 1);
-            if constexpr (LOGNS > 0) {
-                // W_{NS R}^{r k} = W_M^{(r k) << (LOGM - LOGNS - RLOG)}, M = 2H
-                constexpr int SH = LOGH + 1 - LOGNS - RLOG;
-                if constexpr (R == 16) {
-                    // Two table lookups (w^1, w^4) and at most three complex products for the
-                    // other powers: 4 shared loads instead of 30, ~4 ulp per twiddle.
-                    float2* x = a + b * R;
-                    const float2 w1 = twiddle<LOGH + 1, INV>(tw, k << SH);
-                    const float2 w4 = twiddle<LOGH + 1, INV>(tw, (4 * k) << SH);
-                    const float2 w2 = cmul(w1, w1);
-                    const float2 w3 = cmul(w2, w1);
-                    x[1] = cmul(x[1], w1);
-                    x[2] = cmul(x[2], w2);
-                    x[3] = cmul(x[3], w3);
-                    x[4] = cmul(x[4], w4);
-                    x[5] = cmul(x[5], cmul(w4, w1));
-                    x[6] = cmul(x[6], cmul(w4, w2));
-                    x[7] = cmul(x[7], cmul(w4, w3));
-                    const float2 w8 = cmul(w4, w4);
-                    x[8] = cmul(x[8], w8);
-                    x[9] = cmul(x[9], cmul(w8, w1));
-                    x[10] = cmul(x[10], cmul(w8, w2));
-                    x[11] = cmul(x[11], cmul(w8, w3));
-                    const float2 w12 = cmul(w8, w4);
-                    x[12] = cmul(x[12], w12);
-                    x[13] = cmul(x[13], cmul(w12, w1));
-                    x[14] = cmul(x[14], cmul(w12, w2));
-                    x[15] = cmul(x[15], cmul(w12, w3));
-                } else {
-#pragma unroll
-                    for (int r = 1; r < R; ++r)
-                        a[b * R + r] = cmul(a[b * R + r], twiddle<LOGH + 1, INV>(tw, (r * k) << SH));
-                }
-            }
-            dftR<R, INV>(a + b * R);
             const int base = (j - k) * R + k;
 #pragma unroll
             for (int r = 0; r < R; ++r) out(base + r * NS, a[b * R + r]);
@@ -338,88 +408,125 @@ __device__ __forceinline__ float2 w32c() {
     return make_float2(c[I], INV ? c[8 - I] : -c[8 - I]);
 }
 
-// The last Stockham pass as one radix-32 step (LOGNS = LOGH - 5) instead of a radix-16 pass
-// followed by a radix-2 pass: one shared-memory round trip and one barrier fewer per transform.
-// The two lanes e = 0, 1 of a pair (group j = tid / 2) hold the even and odd inputs
-// x_{2r+e} (r < 16) of the group's 32 points. With u = W_H^{2k} (k = j, the group's twiddle
-// index) lane e forms D_e = DFT16(x_{2r+e} u^r), and the 32 outputs are
-//     X[q] = D_0[q] + c_q D_1[q],  X[q + 16] = D_0[q] - c_q D_1[q],  c_q = W_H^k W_32^q,  q < 16,
-// the odd half's own twiddle W_H^{k} folded into c_q. Lane e keeps q in [8e, 8e + 8): it trades
-// the eight D values it does not combine for the partner's eight it does (one shuffle each).
+// One Stockham pass of radix 32 after NS = 2^LOGNS points have been combined, computed by lane
+// pairs: one radix-32 step costs a single shared-memory round trip where a radix-16 and a radix-2
+// (or radix-4) pass cost two. The two lanes e = 0, 1 of a pair (group j, twiddle index
+// k = j mod NS) hold the even and odd inputs x_{2r+e} (r < 16, input stride H / 32) of the
+// group's 32 points. With u = W_{16 NS}^k lane e forms D_e = DFT16(x_{2r+e} u^r), and the 32
+// outputs are
+//     X[q] = D_0[q] + c_q D_1[q],  X[q + 16] = D_0[q] - c_q D_1[q],  c_q = W_{32 NS}^k W_32^q,  q < 16,
+// the odd half's own twiddle W_{32 NS}^k folded into c_q; they go to (j - k) 32 + k + q NS. Lane
+// e keeps q in [8e, 8e + 8): it trades the eight D values it does not combine for the partner's
+// eight it does (one shuffle each). The partners are lanes l and l ^ 16 (e = bit 4 of the lane,
+// j = the other bits), so the sixteen lanes of a half-warp share e and read and write sixteen
+// consecutive points of one row: no shared-memory bank conflicts.
 template <int LOGNS, int LOGH, bool INV, class In, class Out>
 __device__ __forceinline__ void fft_pass32(const In& in, const Out& out, const float2* tw, int tid) {
     constexpr int H = 1 << LOGH;
     constexpr int T = H / 16;
-    constexpr int NS = 1 << LOGNS;  // = H / 32 = the input stride
-    static_assert(LOGNS + 5 == LOGH && LOGNS >= 4, "radix-32 last pass after at least one radix-16 pass");
+    constexpr int NS = 1 << LOGNS;
+    constexpr int STR = H / 32;
+    static_assert(LOGNS + 5 <= LOGH, "radix-32 pass within the transform");
     static_assert(T % 32 == 0, "whole warps of lane pairs");
+    // u = W_{16 NS}^k = W_M^{k << SU}, W_{32 NS}^k = W_M^{k << (SU - 1)}, M = 2H
+    constexpr int SU = LOGH + 1 - LOGNS - 4;
     const bool active = tid < T;
-    const int j = tid >> 1, e = tid & 1;
+    const int e = (tid >> 4) & 1;
+    const int j = (tid & 15) | ((tid >> 5) << 4);
+    const int k = j & (NS - 1);
     float2 a[16];
     if (active) {
 #pragma unroll
-        for (int r = 0; r < 16; ++r) a[r] = in(j + (2 * r + e) * NS);
+        for (int r = 0; r < 16; ++r) a[r] = in(j + (2 * r + e) * STR);
     }
-    if constexpr (In::kSmem && Out::kSmem) __syncthreads();
     if (active) {
-        // u^r by the radix-16 pass's scheme: two table values (u, u^4) and products
-        const float2 u1 = twiddle<LOGH + 1, INV>(tw, 4 * j);
-        const float2 u4 = twiddle<LOGH + 1, INV>(tw, 16 * j);
-        const float2 u2 = cmul(u1, u1);
-        const float2 u3 = cmul(u2, u1);
-        a[1] = cmul(a[1], u1);
-        a[2] = cmul(a[2], u2);
-        a[3] = cmul(a[3], u3);
-        a[4] = cmul(a[4], u4);
-        a[5] = cmul(a[5], cmul(u4, u1));
-        a[6] = cmul(a[6], cmul(u4, u2));
-        a[7] = cmul(a[7], cmul(u4, u3));
-        const float2 u8 = cmul(u4, u4);
-        a[8] = cmul(a[8], u8);
-        a[9] = cmul(a[9], cmul(u8, u1));
-        a[10] = cmul(a[10], cmul(u8, u2));
-        a[11] = cmul(a[11], cmul(u8, u3));
-        const float2 u12 = cmul(u8, u4);
-        a[12] = cmul(a[12], u12);
-        a[13] = cmul(a[13], cmul(u12, u1));
-        a[14] = cmul(a[14], cmul(u12, u2));
-        a[15] = cmul(a[15], cmul(u12, u3));
+        if constexpr (LOGNS > 0) {
+            // u^r by the radix-16 pass's scheme: two table values (u, u^4) and products
+            const float2 u1 = twiddle<LOGH + 1, INV>(tw, k << SU);
+            const float2 u4 = twiddle<LOGH + 1, INV>(tw, (4 * k) << SU);
+            const float2 u2 = cmul(u1, u1);
+            const float2 u3 = cmul(u2, u1);
+            a[1] = cmul(a[1], u1);
+            a[2] = cmul(a[2], u2);
+            a[3] = cmul(a[3], u3);
+            a[4] = cmul(a[4], u4);
+            a[5] = cmul(a[5], cmul(u4, u1));
+            a[6] = cmul(a[6], cmul(u4, u2));
+            a[7] = cmul(a[7], cmul(u4, u3));
+            const float2 u8 = cmul(u4, u4);
+            a[8] = cmul(a[8], u8);
+            a[9] = cmul(a[9], cmul(u8, u1));
+            a[10] = cmul(a[10], cmul(u8, u2));
+            a[11] = cmul(a[11], cmul(u8, u3));
+            const float2 u12 = cmul(u8, u4);
+            a[12] = cmul(a[12], u12);
+            a[13] = cmul(a[13], cmul(u12, u1));
+            a[14] = cmul(a[14], cmul(u12, u2));
+            a[15] = cmul(a[15], cmul(u12, u3));
+        }
         dft16<INV>(a);
-        // lane 0 keeps D_0[0..7] and receives D_1[0..7]; lane 1 keeps D_1[8..15] and receives
-        // D_0[8..15]: afterwards a[i] = D_0[8e + i], a[8 + i] = D_1[8e + i]
+        // lane e = 0 keeps D_0[0..7] and receives D_1[0..7]; lane e = 1 keeps D_1[8..15] and
+        // receives D_0[8..15]: afterwards a[i] = D_0[8e + i], a[8 + i] = D_1[8e + i]
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const float2 snd = e ? a[i] : a[8 + i];
             float2 rcv;
-            rcv.x = __shfl_xor_sync(0xffffffffu, snd.x, 1);
-            rcv.y = __shfl_xor_sync(0xffffffffu, snd.y, 1);
+            rcv.x = __shfl_xor_sync(0xffffffffu, snd.x, 16);
+            rcv.y = __shfl_xor_sync(0xffffffffu, snd.y, 16);
             if (e) a[i] = rcv;
             else a[8 + i] = rcv;
         }
-        // c_{8e} = W_M^{2k + 8e (H / 16)} = W_M^{2k + e H / 2}, M = 2H; c_{8e + i} = c_{8e} W_32^i
-        const float2 c0 = twiddle<LOGH + 1, INV>(tw, 2 * j + e * (H / 2));
+        // c_{8e} = W_{32 NS}^k W_32^{8e} = W_M^{(k << (SU - 1)) + e H / 2}; c_{8e + i} = c_{8e} W_32^i.
+        // A first pass (k = 0) reads no table: c_{8e} = W_4^e, and a caller may still be filling
+        // the table while it runs.
+        float2 c0;
+        if constexpr (LOGNS == 0) c0 = e ? make_float2(0.f, INV ? 1.f : -1.f) : make_float2(1.f, 0.f);
+        else c0 = twiddle<LOGH + 1, INV>(tw, (k << (SU - 1)) + e * (H / 2));
         const float2 cs[8] = {c0,
                               cmul(c0, w32c<INV, 1>()), cmul(c0, w32c<INV, 2>()), cmul(c0, w32c<INV, 3>()),
                               cmul(c0, w32c<INV, 4>()), cmul(c0, w32c<INV, 5>()), cmul(c0, w32c<INV, 6>()),
                               cmul(c0, w32c<INV, 7>())};
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            const int q = 8 * e + i;
             const float2 t = cmul(a[8 + i], cs[i]);
-            out(j + q * NS, cadd(a[i], t));
-            out(j + (q + 16) * NS, csub(a[i], t));
+            const float2 lo = cadd(a[i], t);
+            a[8 + i] = csub(a[i], t);
+            a[i] = lo;
+        }
+    }
+    if constexpr (In::kSmem && Out::kSmem) __syncthreads();  // in place: all loads before any store
+    if (active) {
+        const int base = (j - k) * 32 + k;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int q = 8 * e + i;
+            out(base + q * NS, a[i]);
+            out(base + (q + 16) * NS, a[8 + i]);
         }
     }
     if constexpr (Out::kSmem) __syncthreads();
+}
+
+// Radix (as log2) of the pass after 2^LOGNS of 2^LOGH points have been combined: radix 32 where
+// the rest is 5 or 10 bits (one pass fewer than radix 16 + 2 or 16 + 16 + 4), else radix 16,
+// else what is left.
+template <int LOGH, int LOGNS>
+__host__ __device__ constexpr int fft_rlog() {
+    return (LOGH >= 9 && (LOGH - LOGNS == 5 || LOGH - LOGNS == 10)) ? 5 : (LOGNS + 4 <= LOGH) ? 4 : LOGH - LOGNS;
 }
 
 // Passes from LOGNS on; the first one reads through `in`, the last one writes through `out`.
 template <int LOGH, bool INV, int LOGNS, class In, class Out>
 __device__ __forceinline__ void fft_passes(float2* s, const In& in, const Out& out, const float2* tw, int tid) {
     const SmemPts sp{s};
-    constexpr int RLOG = (LOGNS + 4 <= LOGH) ? 4 : LOGH - LOGNS;
-    if constexpr (LOGNS >= 4 && LOGH - LOGNS == 5) {
-        fft_pass32<LOGNS, LOGH, INV>(in, out, tw, tid);
+    constexpr int RLOG = fft_rlog<LOGH, LOGNS>();
+    if constexpr (RLOG == 5) {
+        if constexpr (LOGNS + 5 == LOGH) {
+            fft_pass32<LOGNS, LOGH, INV>(in, out, tw, tid);
+        } else {
+            fft_pass32<LOGNS, LOGH, INV>(in, sp, tw, tid);
+            fft_passes<LOGH, INV, LOGNS + 5>(s, sp, out, tw, tid);
+        }
     } else if constexpr (LOGNS + RLOG == LOGH) {
         fft_pass<RLOG, LOGNS, LOGH, INV>(in, out, tw, tid);
     } else {

@@ -142,6 +142,8 @@ struct ColPts {
     unsigned long long seed;
     int col;
     static constexpr bool kSmem = false;
+    // packed points that can be nonzero
+    __device__ __forceinline__ int nz() const { return (n + 1) >> 1; }
     __device__ __forceinline__ float2 operator()(int i) const {
         const int t = 2 * i;
         float2 v = make_float2(0.f, 0.f);
@@ -257,6 +259,57 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k
     }
 }
 
+// Spectral product stage of a correlation sweep on the packed transform Z of one column held in
+// s (H points, NT threads, thread tid): unpack the real spectrum A, form P = X conj(A) with the
+// signal spectrum X (H + 1 bins, A[0] and A[H] real) and pack P for the inverse transform, in
+// place. Thread tid takes the bin pairs (k, H - k), k = tid + i NT; the spectrum bins of four
+// such pairs are read (read-only path) before any of them is used, so that their L2 latency
+// overlaps. Bin H/2, its own mirror, goes to thread 0 last.
+template <int LOGH, int NT>
+__device__ __forceinline__ void corr_product(float2* s, const float2* __restrict__ X, const float2* tw, int tid) {
+    constexpr int H = 1 << LOGH;
+    constexpr int NI = (H / 2 + NT - 1) / NT;
+    constexpr int G = NI < 4 ? NI : 4;
+#pragma unroll
+    for (int i0 = 0; i0 < NI; i0 += G) {
+        float2 xk[G], xm[G];
+#pragma unroll
+        for (int i = 0; i < G; ++i) {
+            const int k = tid + (i0 + i) * NT;
+            if (i0 + i < NI && k < H / 2) {
+                xk[i] = __ldg(X + k);
+                xm[i] = __ldg(X + (H - k));  // k = 0: the Nyquist bin X[H]
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < G; ++i) {
+            const int k = tid + (i0 + i) * NT;
+            if (i0 + i >= NI || k >= H / 2) continue;
+            float2 zk, zm;
+            if (k == 0) {
+                const float2 z0 = s[spad(0)];
+                pack_pair(cscale(xk[i], z0.x + z0.y), cscale(xm[i], z0.x - z0.y), make_float2(1.f, 0.f), zk, zm);
+                s[spad(0)] = zk;
+            } else {
+                const float2 w = wm<LOGH>(tw, k);
+                float2 ak, am;
+                unpack_pair<LOGH>(s[spad(k)], s[spad(H - k)], w, ak, am);
+                pack_pair(cmulc(xk[i], ak), cmulc(xm[i], am), w, zk, zm);
+                s[spad(k)] = zk;
+                s[spad(H - k)] = zm;
+            }
+        }
+    }
+    if (tid == 0) {
+        constexpr int k = H / 2;
+        const float2 x = __ldg(X + k), w = wm<LOGH>(tw, k), z = s[spad(k)];
+        float2 ak, am, zk, zm;
+        unpack_pair<LOGH>(z, z, w, ak, am);
+        pack_pair(cmulc(x, ak), cmulc(x, am), w, zk, zm);
+        s[spad(k)] = zm;  // the pair's mirror slot is the same slot
+    }
+}
+
 template <int LOGH>
 __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k_corr(const ssa_col_job* __restrict__ jobs) {
     constexpr int H = 1 << LOGH;
@@ -267,26 +320,7 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k
     float2* tw = smem + spad_size(H);
     load_twiddles<LOGH + 1>(tw);
     fft_block_io<LOGH, false>(smem, col_pts(J, c), SmemPts{smem}, tw);
-    const float2* X = reinterpret_cast<const float2*>(J.X);
-    for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
-        float2 zk, zm;
-        if (k == 0) {
-            const float2 z0 = smem[spad(0)];
-            const float2 p0 = cscale(X[0], z0.x + z0.y);
-            const float2 ph = cscale(X[H], z0.x - z0.y);
-            pack_pair(p0, ph, make_float2(1.f, 0.f), zk, zm);
-            smem[spad(0)] = zk;
-        } else {
-            const float2 w = wm<LOGH>(tw, k);
-            float2 ak, am;
-            unpack_pair<LOGH>(smem[spad(k)], smem[spad(H - k)], w, ak, am);
-            const float2 pk = cmulc(X[k], ak);
-            const float2 pm = cmulc(X[H - k], am);
-            pack_pair(pk, pm, w, zk, zm);
-            smem[spad(k)] = zk;
-            smem[spad(H - k)] = zm;
-        }
-    }
+    corr_product<LOGH, FftShape<LOGH>::BLOCK>(smem, reinterpret_cast<const float2*>(J.X), tw, threadIdx.x);
     __syncthreads();
     fft_block_io<LOGH, true>(smem, SmemPts{smem}, RealOut{J.out + (long long)c * J.ld_out, J.n_out, 1.0f / (float)H},
                              tw);
@@ -311,12 +345,12 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k
     for (int k = threadIdx.x; k <= H / 2; k += blockDim.x) {
         float2 zk, zm;
         if (k == 0) {
-            if (X) pack_pair(cscale(X[0], A[0].x), cscale(X[H], A[H].x), make_float2(1.f, 0.f), zk, zm);
+            if (X) pack_pair(cscale(__ldg(X), A[0].x), cscale(__ldg(X + H), A[H].x), make_float2(1.f, 0.f), zk, zm);
             else pack_pair(A[0], A[H], make_float2(1.f, 0.f), zk, zm);
             smem[spad(0)] = zk;
         } else {
             const float2 w = wm<LOGH>(tw, k);
-            if (X) pack_pair(cmulc(X[k], A[k]), cmulc(X[H - k], A[H - k]), w, zk, zm);
+            if (X) pack_pair(cmulc(__ldg(X + k), A[k]), cmulc(__ldg(X + (H - k)), A[H - k]), w, zk, zm);
             else pack_pair(A[k], A[H - k], w, zk, zm);
             smem[spad(k)] = zk;
             smem[spad(H - k)] = zm;
@@ -348,13 +382,13 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k
         float2 pk, pm;
         if (k == 0) {
             const float2 z0 = smem[spad(0)];
-            pk = cscale(X[0], z0.x + z0.y);
-            pm = cscale(X[H], z0.x - z0.y);
+            pk = cscale(__ldg(X), z0.x + z0.y);
+            pm = cscale(__ldg(X + H), z0.x - z0.y);
         } else {
             float2 ak, am;
             unpack_pair<LOGH>(smem[spad(k)], smem[spad(H - k)], wm<LOGH>(tw, k), ak, am);
-            pk = cmulc(X[k], ak);
-            pm = cmulc(X[H - k], am);
+            pk = cmulc(__ldg(X + k), ak);
+            pm = cmulc(__ldg(X + (H - k)), am);
         }
         const int km = k == 0 ? H : H - k;  // k = H / 2 is its own mirror: pk == pm there
         if (!first) {
@@ -406,27 +440,7 @@ __device__ __forceinline__ void corr_tile(float2* smem, const ssa_col_job* __res
     load_twiddles<LOGH + 1>(tw);  // published by the first pass's closing barrier
     const SmemPts sp{s};
     fft_passes<LOGH, false, 0>(s, valid ? col_pts(J, c) : idle_pts(), sp, tw, tid);
-    const float2* X = reinterpret_cast<const float2*>(J.X);
-    for (int k = tid; k <= H / 2; k += T) {
-        if (!valid) break;
-        float2 zk, zm;
-        if (k == 0) {
-            const float2 z0 = s[spad(0)];
-            const float2 p0 = cscale(X[0], z0.x + z0.y);
-            const float2 ph = cscale(X[H], z0.x - z0.y);
-            pack_pair(p0, ph, make_float2(1.f, 0.f), zk, zm);
-            s[spad(0)] = zk;
-        } else {
-            const float2 w = wm<LOGH>(tw, k);
-            float2 ak, am;
-            unpack_pair<LOGH>(s[spad(k)], s[spad(H - k)], w, ak, am);
-            const float2 pk = cmulc(X[k], ak);
-            const float2 pm = cmulc(X[H - k], am);
-            pack_pair(pk, pm, w, zk, zm);
-            s[spad(k)] = zk;
-            s[spad(H - k)] = zm;
-        }
-    }
+    if (valid) corr_product<LOGH, T>(s, reinterpret_cast<const float2*>(J.X), tw, tid);
     __syncthreads();
     const RealOut ro{valid ? J.out + (long long)c * J.ld_out : nullptr, valid ? J.n_out : 0, 1.0f / (float)H};
     fft_passes<LOGH, true, 0>(s, sp, ro, tw, tid);
