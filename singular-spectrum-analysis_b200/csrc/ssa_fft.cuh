@@ -508,11 +508,15 @@ __device__ __forceinline__ void fft_pass32(const In& in, const Out& out, const f
 }
 
 // Radix (as log2) of the pass after 2^LOGNS of 2^LOGH points have been combined: radix 32 where
-// the rest is 5 or 10 bits (one pass fewer than radix 16 + 2 or 16 + 16 + 4), else radix 16,
-// else what is left.
+// the rest is 5 bits, or 10 bits after a first radix-16 pass (16 + 32 + 32 instead of
+// 16 + 16 + 16 + 4 for 2^14 points), else radix 16, else what is left. (2^10 points keep
+// 16 + 16 + 4: as 32 + 32 its code is larger, which the persistent multi-length kernel, holding
+// every short length at once, pays for in instruction fetch.)
 template <int LOGH, int LOGNS>
 __host__ __device__ constexpr int fft_rlog() {
-    return (LOGH >= 9 && (LOGH - LOGNS == 5 || LOGH - LOGNS == 10)) ? 5 : (LOGNS + 4 <= LOGH) ? 4 : LOGH - LOGNS;
+    return (LOGH >= 9 && (LOGH - LOGNS == 5 || (LOGNS > 0 && LOGH - LOGNS == 10))) ? 5
+           : (LOGNS + 4 <= LOGH)                                                 ? 4
+                                                                                 : LOGH - LOGNS;
 }
 
 // Passes from LOGNS on; the first one reads through `in`, the last one writes through `out`.

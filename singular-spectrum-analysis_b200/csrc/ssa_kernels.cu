@@ -262,15 +262,15 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k
 // Spectral product stage of a correlation sweep on the packed transform Z of one column held in
 // s (H points, NT threads, thread tid): unpack the real spectrum A, form P = X conj(A) with the
 // signal spectrum X (H + 1 bins, A[0] and A[H] real) and pack P for the inverse transform, in
-// place. Thread tid takes the bin pairs (k, H - k), k = tid + i NT; the spectrum bins of four
+// place. Thread tid takes the bin pairs (k, H - k), k = tid + i NT; the spectrum bins of GMAX
 // such pairs are read (read-only path) before any of them is used, so that their L2 latency
 // overlaps. Bin H/2, its own mirror, goes to thread 0 last.
-template <int LOGH, int NT>
+template <int LOGH, int NT, int GMAX>
 __device__ __forceinline__ void corr_product(float2* s, const float2* __restrict__ X, const float2* tw, int tid) {
     constexpr int H = 1 << LOGH;
     constexpr int NI = (H / 2 + NT - 1) / NT;
-    constexpr int G = NI < 4 ? NI : 4;
-#pragma unroll
+    constexpr int G = NI < GMAX ? NI : GMAX;
+#pragma unroll 1
     for (int i0 = 0; i0 < NI; i0 += G) {
         float2 xk[G], xm[G];
 #pragma unroll
@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k
     float2* tw = smem + spad_size(H);
     load_twiddles<LOGH + 1>(tw);
     fft_block_io<LOGH, false>(smem, col_pts(J, c), SmemPts{smem}, tw);
-    corr_product<LOGH, FftShape<LOGH>::BLOCK>(smem, reinterpret_cast<const float2*>(J.X), tw, threadIdx.x);
+    corr_product<LOGH, FftShape<LOGH>::BLOCK, 4>(smem, reinterpret_cast<const float2*>(J.X), tw, threadIdx.x);
     __syncthreads();
     fft_block_io<LOGH, true>(smem, SmemPts{smem}, RealOut{J.out + (long long)c * J.ld_out, J.n_out, 1.0f / (float)H},
                              tw);
@@ -416,6 +416,15 @@ __device__ __forceinline__ ColPts idle_pts() {
     return p;
 }
 
+// A column reader that does not announce its nonzero count, so that the first pass transforms
+// every point: the persistent kernel, which inlines every transform length, keeps one form of
+// the first pass per length (the pruned forms cost it registers).
+struct DensePts {
+    ColPts p;
+    static constexpr bool kSmem = false;
+    __device__ __forceinline__ float2 operator()(int i) const { return p(i); }
+};
+
 // Shared-memory floats2 of the multi-length kernel: the largest data region over the lengths
 // (2^(13 - logh) padded buffers of H points, largest at the smallest length) plus the twiddle
 // table of the largest length.
@@ -439,8 +448,8 @@ __device__ __forceinline__ void corr_tile(float2* smem, const ssa_col_job* __res
     float2* tw = smem + multi_data_f2();
     load_twiddles<LOGH + 1>(tw);  // published by the first pass's closing barrier
     const SmemPts sp{s};
-    fft_passes<LOGH, false, 0>(s, valid ? col_pts(J, c) : idle_pts(), sp, tw, tid);
-    if (valid) corr_product<LOGH, T>(s, reinterpret_cast<const float2*>(J.X), tw, tid);
+    fft_passes<LOGH, false, 0>(s, DensePts{valid ? col_pts(J, c) : idle_pts()}, sp, tw, tid);
+    if (valid) corr_product<LOGH, T, 1>(s, reinterpret_cast<const float2*>(J.X), tw, tid);
     __syncthreads();
     const RealOut ro{valid ? J.out + (long long)c * J.ld_out : nullptr, valid ? J.n_out : 0, 1.0f / (float)H};
     fft_passes<LOGH, true, 0>(s, sp, ro, tw, tid);
