@@ -103,11 +103,11 @@ __device__ __forceinline__ void cl_pair(const ClOp& op, int k, float2& zk, float
             op.spec[H - k] = am;
             return;
         } else if constexpr (KIND == CL_CORR) {
-            pk = cmulc(__ldg(op.X + k), ak);
-            pm = cmulc(__ldg(op.X + (H - k)), am);
+            pk = cmulc(op.X[k], ak);
+            pm = cmulc(op.X[H - k], am);
         } else {
-            pk = cmul(__ldg(op.us + k), ak);
-            pm = cmul(__ldg(op.us + (H - k)), am);
+            pk = cmul(op.us[k], ak);
+            pm = cmul(op.us[H - k], am);
         }
     }
     pack_pair(pk, pm, w, zk, zm);
@@ -123,7 +123,7 @@ __device__ __forceinline__ void cl_dc(const ClOp& op, float2& z0) {
         op.spec[H] = make_float2(z0.x - z0.y, 0.f);
         return;
     } else if constexpr (KIND == CL_CORR) {
-        pack_pair(cscale(__ldg(op.X), z0.x + z0.y), cscale(__ldg(op.X + H), z0.x - z0.y), make_float2(1.f, 0.f), zk, zm);
+        pack_pair(cscale(op.X[0], z0.x + z0.y), cscale(op.X[H], z0.x - z0.y), make_float2(1.f, 0.f), zk, zm);
     } else if constexpr (KIND == CL_ELEM) {
         const float p0 = op.us[0].x * (z0.x + z0.y);
         const float ph = op.us[H].x * (z0.x - z0.y);
@@ -174,13 +174,7 @@ template <int C_, int KIND>
 __device__ __forceinline__ void cl_exchange(uint32_t sbase, const float2* twM, int rank, const ClOp& op) {
     using S = ClShape<C_>;
     constexpr int C = S::C, H1 = S::H1, H = S::H;
-    // Work units u < H1/2, one item each, except that unit 0 takes both items whose bins are
-    // their own mirrors (k1 = 0 and k1 = H1/2), which cost half an item each: H1/2 units of equal
-    // cost, so that with C * BLOCK a divisor of H1/2 (C = 2, 4, 8) no thread runs one item more
-    // than the rest while the cluster waits at its barrier.
-    for (int u = rank * S::BLOCK + (int)threadIdx.x; u < H1 / 2; u += C * S::BLOCK)
-    for (int it = 0; it < (u == 0 ? 2 : 1); ++it) {
-        const int g = it ? H1 / 2 : u;
+    for (int g = rank * S::BLOCK + (int)threadIdx.x; g <= H1 / 2; g += C * S::BLOCK) {
         const int ka = g, kb = (H1 - g) & (H1 - 1);
         const bool self = ka == kb;  // k1 = 0 or H1/2
         const uint32_t aa = sbase + 8u * (uint32_t)spad(ka), ab = sbase + 8u * (uint32_t)spad(kb);

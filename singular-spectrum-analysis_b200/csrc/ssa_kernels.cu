@@ -416,15 +416,6 @@ __device__ __forceinline__ ColPts idle_pts() {
     return p;
 }
 
-// A column reader that does not announce its nonzero count, so that the first pass transforms
-// every point: the persistent kernel, which inlines every transform length, keeps one form of
-// the first pass per length (the pruned forms cost it registers).
-struct DensePts {
-    ColPts p;
-    static constexpr bool kSmem = false;
-    __device__ __forceinline__ float2 operator()(int i) const { return p(i); }
-};
-
 // Shared-memory floats2 of the multi-length kernel: the largest data region over the lengths
 // (2^(13 - logh) padded buffers of H points, largest at the smallest length) plus the twiddle
 // table of the largest length.
@@ -448,8 +439,8 @@ __device__ __forceinline__ void corr_tile(float2* smem, const ssa_col_job* __res
     float2* tw = smem + multi_data_f2();
     load_twiddles<LOGH + 1>(tw);  // published by the first pass's closing barrier
     const SmemPts sp{s};
-    fft_passes<LOGH, false, 0>(s, DensePts{valid ? col_pts(J, c) : idle_pts()}, sp, tw, tid);
-    if (valid) corr_product<LOGH, T, 1>(s, reinterpret_cast<const float2*>(J.X), tw, tid);
+    fft_passes<LOGH, false, 0>(s, valid ? col_pts(J, c) : idle_pts(), sp, tw, tid);
+    if (valid) corr_product<LOGH, T, 4>(s, reinterpret_cast<const float2*>(J.X), tw, tid);
     __syncthreads();
     const RealOut ro{valid ? J.out + (long long)c * J.ld_out : nullptr, valid ? J.n_out : 0, 1.0f / (float)H};
     fft_passes<LOGH, true, 0>(s, sp, ro, tw, tid);
