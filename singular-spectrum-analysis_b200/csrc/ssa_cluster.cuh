@@ -262,7 +262,8 @@ struct ClDecim {
 // Spectrum (CL_SPEC), correlation sweep (CL_CORR) and one-buffer elementary reconstruction
 // (CL_ELEM) on clusters; grid (C x columns, jobs), one cluster per column.
 template <int C, int KIND>
-__global__ void __launch_bounds__(ClShape<C>::BLOCK, ClShape<C>::MINB) k_cl_col(const ssa_col_job* __restrict__ jobs) {
+__global__ void __launch_bounds__(ClShape<C>::BLOCK, ClShape<C>::MINB) k_cl_col(const ssa_col_job* __restrict__ jobs,
+                                                                                  const ssa_tile* __restrict__ tiles) {
     using S = ClShape<C>;
     extern __shared__ float2 smem[];
     __shared__ double red[32];
@@ -272,8 +273,9 @@ __global__ void __launch_bounds__(ClShape<C>::BLOCK, ClShape<C>::MINB) k_cl_col(
     float2* twM = tw1 + TwSplit<S::LOGH1 + 1>::N;
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
-    const ssa_col_job J = jobs[blockIdx.y];
-    const int c = blockIdx.x / S::C;
+    int jb, c;
+    sweep_column(tiles, blockIdx.x / S::C, jb, c);
+    const ssa_col_job J = jobs[jb];
     if (c >= J.ncols) return;  // the whole cluster shares c
     load_twiddles<S::LOGH1 + 1>(tw1);
     cl_load_twM<C>(twM);
@@ -374,13 +376,14 @@ __global__ void __launch_bounds__(ClShape<C>::BLOCK, ClShape<C>::MINB) k_cl_reco
 }
 
 template <int C, int KIND>
-static int launch_cl_col(const ssa_col_job* jobs, int njobs, int maxcols, cudaStream_t st) {
+static int launch_cl_col(const ssa_col_job* jobs, int njobs, int maxcols, cudaStream_t st, const ssa_tile* tiles) {
     using S = ClShape<C>;
     const int sm = cl_smem_f2<C>() * (int)sizeof(float2);
     cudaError_t e = cudaFuncSetAttribute(k_cl_col<C, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return (int)e;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(S::C * maxcols, njobs, 1);
+    // with a column list, njobs is its tile count: one cluster per listed column
+    cfg.gridDim = tiles ? dim3(S::C * njobs, 1, 1) : dim3(S::C * maxcols, njobs, 1);
     cfg.blockDim = dim3(S::BLOCK, 1, 1);
     cfg.dynamicSmemBytes = sm;
     cfg.stream = st;
@@ -391,7 +394,7 @@ static int launch_cl_col(const ssa_col_job* jobs, int njobs, int maxcols, cudaSt
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, k_cl_col<C, KIND>, jobs);
+    e = cudaLaunchKernelEx(&cfg, k_cl_col<C, KIND>, jobs, tiles);
     return launched(e != cudaSuccess ? e : cudaGetLastError());
 }
 
@@ -423,12 +426,13 @@ static int cl_ctas(int code) {
     return code == 14 ? 2 : code == 15 ? 4 : code == 16 ? 8 : code == SSA_FFT_3x13 ? 3 : code == SSA_FFT_3x14 ? 6 : 0;
 }
 
-static int cl_col_dispatch(int kind, const ssa_col_job* jobs, int njobs, int maxcols, int code, cudaStream_t st) {
-#define SSA_CL_CASE(C)                                                                        \
-    if (cl_ctas(code) == C) {                                                                 \
-        if (kind == CL_SPEC) return launch_cl_col<C, CL_SPEC>(jobs, njobs, maxcols, st);     \
-        if (kind == CL_CORR) return launch_cl_col<C, CL_CORR>(jobs, njobs, maxcols, st);     \
-        return launch_cl_col<C, CL_ELEM>(jobs, njobs, maxcols, st);                           \
+static int cl_col_dispatch(int kind, const ssa_col_job* jobs, int njobs, int maxcols, int code, cudaStream_t st,
+                           const ssa_tile* tiles = nullptr) {
+#define SSA_CL_CASE(C)                                                                          \
+    if (cl_ctas(code) == C) {                                                                   \
+        if (kind == CL_SPEC) return launch_cl_col<C, CL_SPEC>(jobs, njobs, maxcols, st, tiles); \
+        if (kind == CL_CORR) return launch_cl_col<C, CL_CORR>(jobs, njobs, maxcols, st, tiles); \
+        return launch_cl_col<C, CL_ELEM>(jobs, njobs, maxcols, st, tiles);                      \
     }
     SSA_CL_CASE(2)
     SSA_CL_CASE(3)

@@ -310,12 +310,27 @@ __device__ __forceinline__ void corr_product(float2* s, const float2* __restrict
     }
 }
 
+// Grid of a correlation sweep: (columns, jobs), or with a column list one CTA per listed
+// (job, column) tile, so that no CTA is spent on the columns beyond a job's ncols.
+__device__ __forceinline__ void sweep_column(const ssa_tile* __restrict__ tiles, int unit, int& job, int& c) {
+    if (tiles) {
+        const ssa_tile t = tiles[unit];
+        job = t.job;
+        c = t.c0;
+    } else {
+        job = blockIdx.y;
+        c = unit;
+    }
+}
+
 template <int LOGH>
-__global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k_corr(const ssa_col_job* __restrict__ jobs) {
+__global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k_corr(const ssa_col_job* __restrict__ jobs,
+                                                                                       const ssa_tile* __restrict__ tiles) {
     constexpr int H = 1 << LOGH;
     extern __shared__ float2 smem[];
-    const ssa_col_job J = jobs[blockIdx.y];
-    const int c = blockIdx.x;
+    int jb, c;
+    sweep_column(tiles, blockIdx.x, jb, c);
+    const ssa_col_job J = jobs[jb];
     if (c >= J.ncols) return;
     float2* tw = smem + spad_size(H);
     load_twiddles<LOGH + 1>(tw);
@@ -1787,11 +1802,13 @@ static int launch_spectrum(const ssa_col_job* jobs, int njobs, int maxcols, cuda
     return launched(cudaGetLastError());
 }
 template <int LOGH>
-static int launch_corr(const ssa_col_job* jobs, int njobs, int maxcols, cudaStream_t st) {
+static int launch_corr(const ssa_col_job* jobs, int njobs, int maxcols, cudaStream_t st,
+                       const ssa_tile* tiles = nullptr) {
     const int sm = smem_bytes<LOGH>(1);
     cudaError_t e = set_smem(k_corr<LOGH>, sm);
     if (e != cudaSuccess) return (int)e;
-    k_corr<LOGH><<<dim3(maxcols, njobs), FftShape<LOGH>::BLOCK, sm, st>>>(jobs);
+    const dim3 grid = tiles ? dim3(njobs, 1) : dim3(maxcols, njobs);  // tiles: njobs = tile count
+    k_corr<LOGH><<<grid, FftShape<LOGH>::BLOCK, sm, st>>>(jobs, tiles);
     return launched(cudaGetLastError());
 }
 template <int LOGH>
@@ -1916,6 +1933,15 @@ extern "C" int ssad_corr(const ssa_col_job* d_jobs, int njobs, int maxcols, int 
     if (logh > SSA_MAX_LOGH || (logh == 14 && g_cl14))  // 15-18, and 14 on 2-CTA clusters when selected
         return cl_col_dispatch(CL_CORR, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);
 #define CALL(L) return launch_corr<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
+    SSA_LOGH_DISPATCH(logh, CALL)
+#undef CALL
+    return 0;
+}
+extern "C" int ssad_corr_tiles(const ssa_col_job* d_jobs, const ssa_tile* d_tiles, int ntiles, int logh, void* stream) {
+    if (ntiles <= 0) return 0;
+    if (logh > SSA_MAX_LOGH || (logh == 14 && g_cl14))
+        return cl_col_dispatch(CL_CORR, d_jobs, ntiles, 1, logh, (cudaStream_t)stream, d_tiles);
+#define CALL(L) return launch_corr<L>(d_jobs, ntiles, 1, (cudaStream_t)stream, d_tiles)
     SSA_LOGH_DISPATCH(logh, CALL)
 #undef CALL
     return 0;

@@ -343,6 +343,9 @@ typedef struct
 } ssa_tile;
 int ssad_corr_multi(const ssa_col_job *d_jobs, const ssa_tile *d_tiles, int ntiles, int *d_head, int nctas,
                     void *stream);
+/* The sweep of ssad_corr over a column list: one CTA (cluster) per tile (job, column c0; logh
+ * unused), so that the grid holds no columns beyond a job's ncols. */
+int ssad_corr_tiles(const ssa_col_job *d_jobs, const ssa_tile *d_tiles, int ntiles, int logh, void *stream);
 /* Columns one tile of the multi-length sweep covers at logh. */
 int ssad_multi_tile_cols(int logh);
 int ssad_elem_recon(const ssa_col_job *d_jobs, int njobs, int maxcols, int logh, void *stream);

@@ -502,7 +502,6 @@ static int r_sweep(rbucket *b, int adjoint, int generate, const unsigned long lo
     ssa_col_job *jobs = (ssa_col_job *)calloc((size_t)b->nb, sizeof(ssa_col_job));
     if (!jobs)
         return (int)cudaErrorMemoryAllocation;
-    int maxc = 0;
     for (int i = 0; i < b->nb; i++)
     {
         const rser *S = &b->sd[i];
@@ -539,7 +538,6 @@ static int r_sweep(rbucket *b, int adjoint, int generate, const unsigned long lo
         J->N = S->N;
         J->L = S->L;
         J->K = S->K;
-        maxc = imax(maxc, S->kp);
     }
     void *d = ssae_push_jobs(&b->e, jobs, sizeof(ssa_col_job) * b->nb);
     free(jobs);
@@ -593,8 +591,29 @@ static int r_sweep(rbucket *b, int adjoint, int generate, const unsigned long lo
         ssae_prof_end(&b->e);
         return rc;
     }
+    /* one CTA (cluster) per live column: the series' kp differ (k + p), so a (columns, series)
+     * grid would hold a third of its CTAs for columns beyond a series' kp */
+    int nt = 0;
+    for (int i = 0; i < b->nb; i++)
+        nt += b->sd[i].kp;
+    ssa_tile *tiles = (ssa_tile *)calloc((size_t)nt + 1, sizeof(ssa_tile));
+    if (!tiles)
+        return (int)cudaErrorMemoryAllocation;
+    int t = 0;
+    for (int i = 0; i < b->nb; i++)
+        for (int c = 0; c < b->sd[i].kp; c++)
+        {
+            tiles[t].job = i;
+            tiles[t].c0 = c;
+            tiles[t].logh = b->logh;
+            t++;
+        }
+    void *dt = ssae_push_jobs(&b->e, tiles, sizeof(ssa_tile) * (size_t)nt);
+    free(tiles);
+    if (!dt)
+        return (int)cudaErrorMemoryAllocation;
     ssae_prof_begin(&b->e, SSAK_CORR);
-    int rc = ssad_corr((const ssa_col_job *)d, b->nb, maxc, b->logh, b->e.st);
+    int rc = ssad_corr_tiles((const ssa_col_job *)d, (const ssa_tile *)dt, nt, b->logh, b->e.st);
     ssae_prof_end(&b->e);
     return rc;
 }
@@ -1186,10 +1205,10 @@ static int plan(ssa_rbatch *rb, int B, const int *N, const int *L, const int *k)
         }
         /* one run pushes 13 + 6 q job tables of at most sizeof(ssa_col_job) bytes per series,
          * each 16-byte aligned (a multi-length bucket pushes the per-code stages in up to six
-         * parts, and a tile table of at most 64 tiles per series per sweep) */
+         * parts), and per sweep a column list or tile table of at most SSA_MAX_KP entries per
+         * series */
         size_t arena = ((size_t)b->nb * sizeof(ssa_col_job) + 16 * 6) * (size_t)(16 + 6 * rb->q) + (1 << 16);
-        if (b->multi)
-            arena += (size_t)(2 * rb->q + 2) * ((size_t)SSA_MAX_KP * b->nb + 2) * sizeof(ssa_tile);
+        arena += (size_t)(2 * rb->q + 2) * ((size_t)SSA_MAX_KP * b->nb + 2) * sizeof(ssa_tile);
         const void *ja_old = b->e.ja.d;
         if (ssae_grow_arena(&b->e, arena) != 0)
             return -1;
