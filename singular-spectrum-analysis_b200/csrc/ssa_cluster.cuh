@@ -1,7 +1,7 @@
 // FFT lengths beyond one CTA's shared memory: each transform runs on a thread-block cluster of
 // C CTAs of H1 = 8192 points, H = C H1 complex points (real length M = 2H): C = 4 and 8 for
-// M = 2^16 and 2^17, C = 3 and 6 for M = 3 * 2^14 and 3 * 2^15, which cut the padding of the
-// series between the powers of two (series up to N = 131072).
+// M = 2^16 and 2^17, C = 3, 5 and 6 for M = 3 * 2^14, 5 * 2^14 and 3 * 2^15, which cut the
+// padding of the series between the powers of two (series up to N = 131072).
 //
 // Packed sequence z[n] = a[2n] + i a[2n+1], n < H = C H1 (H1 = 8192). CTA r of the cluster holds
 // the decimated sequence z_r[m] = z[C m + r] and transforms it locally (fft_block, H1 points):
@@ -41,11 +41,15 @@ struct ClShape {
     static constexpr int BLOCK = FftShape<LOGH1>::BLOCK;
     static constexpr int MINB = BLOCK >= 1024 ? 1 : 2;  // CTAs per SM the kernels are built for
     static constexpr bool POW2 = (C & (C - 1)) == 0;
-    static_assert(POW2 || C % 3 == 0, "cluster sizes are 2^a or 3 * 2^a");
-    // twiddle table of resolution M = 2H: 2^LOGM, or 3 * 2^A3
+    static constexpr bool FIVE = C == 5;
+    static_assert(POW2 || C % 3 == 0 || FIVE, "cluster sizes are 2^a, 3 * 2^a or 5");
+    // twiddle table of resolution M = 2H: 2^LOGM, 3 * 2^A3 or 5 * 2^A5
     static constexpr int LOGM = cl_ilog2(2 * H);
     static constexpr int A3 = cl_ilog2(2 * H / 3);
-    using Tw = typename std::conditional<POW2, TwSplit<(POW2 ? LOGM : 1)>, TwSplit3<(POW2 ? 9 : A3)>>::type;
+    static constexpr int A5 = cl_ilog2(2 * H / 5);
+    using Tw = typename std::conditional<
+        POW2, TwSplit<(POW2 ? LOGM : 1)>,
+        typename std::conditional<FIVE, TwSplit5<(FIVE ? A5 : 9)>, TwSplit3<(POW2 || FIVE ? 9 : A3)>>::type>::type;
 };
 
 template <int C>
@@ -53,6 +57,8 @@ __device__ __forceinline__ void cl_load_twM(float2* tab) {
     using S = ClShape<C>;
     if constexpr (S::POW2)
         load_twiddles<S::LOGM>(tab);
+    else if constexpr (S::FIVE)
+        load_twiddles5<S::A5>(tab);
     else
         load_twiddles3<S::A3>(tab);
 }
@@ -424,9 +430,10 @@ static int launch_cl_recon(const ssa_recon_job* jobs, int njobs, cudaStream_t st
 }
 
 // CTAs per cluster of a size code: 14 -> 2 (when the 2-CTA form of that length is selected),
-// 15 -> 4, 16 -> 8, SSA_FFT_3x13 -> 3, SSA_FFT_3x14 -> 6.
+// 15 -> 4, 16 -> 8, SSA_FFT_3x13 -> 3, SSA_FFT_3x14 -> 6, SSA_FFT_5x13 -> 5.
 static int cl_ctas(int code) {
-    return code == 14 ? 2 : code == 15 ? 4 : code == 16 ? 8 : code == SSA_FFT_3x13 ? 3 : code == SSA_FFT_3x14 ? 6 : 0;
+    return code == 14 ? 2 : code == 15 ? 4 : code == 16 ? 8 : code == SSA_FFT_3x13 ? 3 : code == SSA_FFT_3x14 ? 6
+         : code == SSA_FFT_5x13 ? 5 : 0;
 }
 
 static int cl_col_dispatch(int kind, const ssa_col_job* jobs, int njobs, int maxcols, int code, cudaStream_t st,
@@ -440,6 +447,7 @@ static int cl_col_dispatch(int kind, const ssa_col_job* jobs, int njobs, int max
     SSA_CL_CASE(2)
     SSA_CL_CASE(3)
     SSA_CL_CASE(4)
+    SSA_CL_CASE(5)
     SSA_CL_CASE(6)
     SSA_CL_CASE(8)
 #undef SSA_CL_CASE

@@ -30,6 +30,10 @@ __device__ float2 g_tw[SSA_TW_N];
 #define SSA_TW3_LOG 15
 #define SSA_TW3_N (3 << SSA_TW3_LOG)
 __device__ float2 g_tw3[SSA_TW3_N];
+// Twiddles of the length 5 * 2^14: g_tw5[t] = exp(-2 pi i t / (5 * 2^14)), FP64 on the host.
+#define SSA_TW5_LOG 14
+#define SSA_TW5_N (5 << SSA_TW5_LOG)
+__device__ float2 g_tw5[SSA_TW5_N];
 
 namespace ssa {
 
@@ -94,6 +98,25 @@ __device__ __forceinline__ void load_twiddles3(float2* tab) {
     for (int i = threadIdx.x; i < S::N; i += blockDim.x) {
         const int t = i < S::NLO ? i : (i - S::NLO) << S::LO;
         tab[i] = g_tw3[t << (SSA_TW3_LOG - A)];
+    }
+}
+
+// The same for the resolution M = 5 * 2^14: lo W_M^j for j < 512, hi W_M^(512 i) for i < M / 512.
+template <int A>
+struct TwSplit5 {
+    static constexpr int LO = 9;
+    static constexpr int NLO = 1 << LO;
+    static constexpr int NHI = 5 << (A - LO);
+    static constexpr int N = NLO + NHI;
+};
+
+template <int A>
+__device__ __forceinline__ void load_twiddles5(float2* tab) {
+    using S = TwSplit5<A>;
+    static_assert(A >= S::LO && A <= SSA_TW5_LOG, "twiddle resolution outside the 5 * 2^A table");
+    for (int i = threadIdx.x; i < S::N; i += blockDim.x) {
+        const int t = i < S::NLO ? i : (i - S::NLO) << S::LO;
+        tab[i] = g_tw5[t << (SSA_TW5_LOG - A)];
     }
 }
 
@@ -250,10 +273,32 @@ __device__ __forceinline__ void dft6(float2* a) {
     }
 }
 
+// 5 points from the definition, pairing n with 5 - n: with s_n = a_n + a_{5-n}, d_n = a_n - a_{5-n},
+// X_0 = a_0 + s_1 + s_2, X_{1,4} = a_0 + c_1 s_1 + c_2 s_2 -/+ i (g_1 d_1 + g_2 d_2),
+// X_{2,3} = a_0 + c_2 s_1 + c_1 s_2 -/+ i (g_2 d_1 - g_1 d_2), c_j = cos(2 pi j / 5),
+// g_j = sin(2 pi j / 5) (signs of i flipped for INV).
+template <bool INV>
+__device__ __forceinline__ void dft5(float2* a) {
+    constexpr float C1 = 0.30901699437494742f, C2 = -0.80901699437494742f;
+    constexpr float G1 = 0.95105651629515357f, G2 = 0.58778525229247313f;
+    const float2 s1 = cadd(a[1], a[4]), d1 = csub(a[1], a[4]);
+    const float2 s2 = cadd(a[2], a[3]), d2 = csub(a[2], a[3]);
+    const float2 t1 = make_float2(a[0].x + C1 * s1.x + C2 * s2.x, a[0].y + C1 * s1.y + C2 * s2.y);
+    const float2 t2 = make_float2(a[0].x + C2 * s1.x + C1 * s2.x, a[0].y + C2 * s1.y + C1 * s2.y);
+    const float2 u1 = mul_mi<INV>(make_float2(G1 * d1.x + G2 * d2.x, G1 * d1.y + G2 * d2.y));
+    const float2 u2 = mul_mi<INV>(make_float2(G2 * d1.x - G1 * d2.x, G2 * d1.y - G1 * d2.y));
+    a[0] = cadd(a[0], cadd(s1, s2));
+    a[1] = cadd(t1, u1);
+    a[4] = csub(t1, u1);
+    a[2] = cadd(t2, u2);
+    a[3] = csub(t2, u2);
+}
+
 template <int R, bool INV>
 __device__ __forceinline__ void dftR(float2* a) {
     if constexpr (R == 2) dft2<INV>(a);
     else if constexpr (R == 3) dft3<INV>(a);
+    else if constexpr (R == 5) dft5<INV>(a);
     else if constexpr (R == 4) dft4<INV>(a);
     else if constexpr (R == 6) dft6<INV>(a);
     else if constexpr (R == 8) dft8<INV>(a);

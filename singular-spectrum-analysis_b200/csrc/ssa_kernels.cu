@@ -1739,6 +1739,7 @@ extern "C" int ssad_fft_h(int code) {
     if (code >= 4 && code <= SSA_MAX_LOGH_ALL) return 1 << code;
     if (code == SSA_FFT_3x13) return 3 << 13;
     if (code == SSA_FFT_3x14) return 3 << 14;
+    if (code == SSA_FFT_5x13) return 5 << 13;
     return 0;
 }
 
@@ -1747,6 +1748,7 @@ extern "C" int ssad_fft_code_for(int N) {
     if (logh > SSA_MAX_LOGH_ALL) return -1;  // beyond the largest length
     // between the cluster powers of two, the 3 * 2^a length when it suffices
     if (logh == 15 && N <= 2 * (3 << 13)) return SSA_FFT_3x13;
+    if (logh == 16 && N <= 2 * (5 << 13)) return SSA_FFT_5x13;
     if (logh == 16 && N <= 2 * (3 << 14)) return SSA_FFT_3x14;
     return logh;
 }
@@ -1775,6 +1777,13 @@ extern "C" int ssad_init_device(void) {
         tw3[t] = make_float2((float)cos(a), (float)sin(a));
     }
     e = cudaMemcpyToSymbol(g_tw3, tw3.data(), sizeof(float2) * SSA_TW3_N);
+    if (e != cudaSuccess) return (int)e;
+    std::vector<float2> tw5(SSA_TW5_N);
+    for (int t = 0; t < SSA_TW5_N; ++t) {
+        const double a = -2.0 * M_PI * (double)t / (double)SSA_TW5_N;
+        tw5[t] = make_float2((float)cos(a), (float)sin(a));
+    }
+    e = cudaMemcpyToSymbol(g_tw5, tw5.data(), sizeof(float2) * SSA_TW5_N);
     if (e != cudaSuccess) return (int)e;
     if (dev < 64) done[dev] = true;
     return 0;
@@ -1924,7 +1933,7 @@ extern "C" int ssad_gram_tc(const ssa_wgram_job* d_jobs, int njobs, int maxchunk
 
 extern "C" int ssad_spectrum(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
     if (njobs <= 0 || maxcols <= 0) return 0;
-    if (logh > SSA_MAX_LOGH || (logh == 14 && g_cl14))  // 15-18, and 14 on 2-CTA clusters when selected
+    if (logh > SSA_MAX_LOGH || (logh == 14 && g_cl14))  // 15-19, and 14 on 2-CTA clusters when selected
         return cl_col_dispatch(CL_SPEC, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);
 #define CALL(L) return launch_spectrum<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
     SSA_LOGH_DISPATCH(logh, CALL)
@@ -1952,7 +1961,7 @@ extern "C" int ssad_corr_multi(const ssa_col_job* d_jobs, const ssa_tile* d_tile
 }
 extern "C" int ssad_corr(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
     if (njobs <= 0 || maxcols <= 0) return 0;
-    if (logh > SSA_MAX_LOGH || (logh == 14 && g_cl14))  // 15-18, and 14 on 2-CTA clusters when selected
+    if (logh > SSA_MAX_LOGH || (logh == 14 && g_cl14))  // 15-19, and 14 on 2-CTA clusters when selected
         return cl_col_dispatch(CL_CORR, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);
 #define CALL(L) return launch_corr<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
     SSA_LOGH_DISPATCH(logh, CALL)
@@ -1991,7 +2000,7 @@ extern "C" int ssad_elem_recon(const ssa_col_job* d_jobs, int njobs, int maxcols
 }
 extern "C" int ssad_elem_recon1(const ssa_col_job* d_jobs, int njobs, int maxcols, int logh, void* stream) {
     if (njobs <= 0 || maxcols <= 0) return 0;
-    if (logh > SSA_MAX_LOGH || (logh == 14 && g_cl14))  // 15-18, and 14 on 2-CTA clusters when selected
+    if (logh > SSA_MAX_LOGH || (logh == 14 && g_cl14))  // 15-19, and 14 on 2-CTA clusters when selected
         return cl_col_dispatch(CL_ELEM, d_jobs, njobs, maxcols, logh, (cudaStream_t)stream);
 #define CALL(L) return launch_elem1<L>(d_jobs, njobs, maxcols, (cudaStream_t)stream)
     SSA_LOGH_DISPATCH(logh, CALL)

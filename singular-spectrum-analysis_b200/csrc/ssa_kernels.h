@@ -31,12 +31,13 @@ extern "C" {
 /* FFT-length bucket: real length M = 2^(logh + 1). */
 int ssad_logh_for(int N);
 /* FFT size codes of the uneven batches: a logh (4..16, H = 2^logh complex points), or one of the
- * two lengths between the cluster powers of two, H = 3 * 2^13 (real length 49152) and
- * H = 3 * 2^14 (98304), which run on clusters of 3 and 6 CTAs. ssad_spectrum / ssad_corr /
- * ssad_elem_recon1 accept every code. */
+ * three lengths between the cluster powers of two, H = 3 * 2^13 (real length 49152),
+ * H = 5 * 2^13 (81920) and H = 3 * 2^14 (98304), which run on clusters of 3, 5 and 6 CTAs.
+ * ssad_spectrum / ssad_corr / ssad_elem_recon1 accept every code. */
 #define SSA_FFT_3x13 17
 #define SSA_FFT_3x14 18
-#define SSA_FFT_NCODES 19
+#define SSA_FFT_5x13 19
+#define SSA_FFT_NCODES 20
 int ssad_fft_h(int code);       /* complex points H of a size code (0 for an unknown code) */
 int ssad_fft_code_for(int N);   /* smallest size code with 2H >= N; -1 beyond N = 131072 */
 /* Largest bucket: logh 16 (M = 131072, series up to N = 131072). Buckets up to 14 run one CTA

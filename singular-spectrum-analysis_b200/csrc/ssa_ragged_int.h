@@ -46,7 +46,7 @@ cudaStream_t ssar_main_stream(const ssa_rbatch *rb);
  * a run (NULL for a bucket the run did not use). Outside graph replays, work a caller enqueues
  * on a bucket's stream after ssar_run_enqueue_ex follows that bucket's part of the run and
  * nothing else. */
-#define SSAR_NB 19
+#define SSAR_NB 20
 int ssar_bucket_index(int N);
 cudaStream_t ssar_bucket_stream(const ssa_rbatch *rb, int g);
 const int *ssar_status(const ssa_rbatch *rb);

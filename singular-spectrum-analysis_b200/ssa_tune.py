@@ -41,14 +41,14 @@ _lib.ssa_b200_set_cluster32k.restype = None
 _lib.ssa_b200_set_cluster32k.argtypes = [ctypes.c_int]
 _lib.ssa_b200_cluster32k.restype = ctypes.c_int
 
-NCODES = 19
+NCODES = 20
 GRAM_CANDIDATES = (296, 592, 1184, 2368)  # 2, 4, 8 (the heuristic) and 16 CTAs per SM
 HEURISTIC_GRAM = 1184
 # representative series lengths per tuned bucket (size code): the buckets a mixed stream of N in
 # [500, 1e5] uses. With the multi-length sweep on, lengths 513..16384 share the bucket of code 13,
 # whose table entry then holds for all of them, so that bucket is tuned on the mixed range.
 BUCKET_N = {13: (513, 16384), 14: (16385, 32768), 17: (32769, 49152), 15: (49153, 65536),
-            18: (65537, 98304), 16: (98305, 131072)}
+            19: (65537, 81920), 18: (81921, 98304), 16: (98305, 131072)}
 
 
 def size_code(N: int) -> int:

@@ -110,12 +110,13 @@ def test_uneven_batch_across_cluster_lengths(gpu, oracle):
 
 
 def test_uneven_batch_mixed_radix_boundaries(gpu, oracle):
-    """Both sides of the two 3 * 2^a FFT lengths (real lengths 49152 and 98304, clusters of 3 and
-    6 CTAs) against the oracle: 32769 and 49152 run at 49152, 49153 at 65536, 98304 at 98304,
-    98305 at 131072."""
+    """Both sides of the mixed-radix FFT lengths (real lengths 49152, 81920 and 98304, clusters of
+    3, 5 and 6 CTAs) against the oracle: 32769 and 49152 run at 49152, 49153 at 65536, 65537 and
+    81920 at 81920, 81921 and 98304 at 98304, 98305 at 131072."""
     rng = np.random.default_rng(11)
     mix = [(oracle.walk_sines(rng, N), N // 4, k) for N, k in
-           ((32769, 14), (49152, 22), (49153, 10), (98304, 18), (98305, 9))]
+           ((32769, 14), (49152, 22), (49153, 10), (65537, 12), (81920, 16), (81921, 11), (98304, 18),
+            (98305, 9))]
     p, q, seed = 10, 2, 23
     rb = gpu.SSARaggedBatch(oversampling=p, power_iters=q, groups=[[0], [1, 2]])
     sig, W, G = rb.run([m[0] for m in mix], [m[1] for m in mix], [m[2] for m in mix], seed=seed)

@@ -126,15 +126,15 @@ def test_host_eigen_solver_vs_numpy():
 
 
 def test_fft_size_codes():
-    """FFT lengths of the uneven batches: powers of two, and 49152 / 98304 between the cluster
-    powers of two (ssa_b200_fft_length)."""
+    """FFT lengths of the uneven batches: powers of two, and 49152 / 81920 / 98304 between the
+    cluster powers of two (ssa_b200_fft_length)."""
     import ssa_gpu
 
     f = ssa_gpu._lib.ssa_b200_fft_length
     f.restype = ctypes.c_int
     f.argtypes = [ctypes.c_int]
     cases = {500: 512, 32768: 32768, 32769: 49152, 49152: 49152, 49153: 65536, 65536: 65536,
-             65537: 98304, 98304: 98304, 98305: 131072, 131072: 131072}
+             65537: 81920, 81920: 81920, 81921: 98304, 98304: 98304, 98305: 131072, 131072: 131072}
     for N, M in cases.items():
         assert f(N) == M, (N, f(N))
     assert f(131073) == -1 and f(0) == -1

@@ -34,6 +34,7 @@ def test_table_round_trip_and_validation(tune):
 def test_size_codes(tune):
     assert tune.size_code(1000) == 9 and tune.size_code(16384) == 13 and tune.size_code(16385) == 14
     assert tune.size_code(40000) == 17 and tune.size_code(60000) == 15 and tune.size_code(90000) == 18
+    assert tune.size_code(70000) == 19 and tune.size_code(81920) == 19 and tune.size_code(81921) == 18
     assert tune.size_code(131073) == -1
 
 
