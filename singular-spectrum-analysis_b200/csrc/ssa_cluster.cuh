@@ -280,8 +280,8 @@ __global__ void __launch_bounds__(ClShape<C>::BLOCK, ClShape<C>::MINB) k_cl_col(
     float2* twM = tw1 + TwSplit<S::LOGH1 + 1>::N;
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
-    // one cluster per column, or per tile of a column list (a persistent form that loops over the
-    // list with the resident clusters measured 44% slower per launch: 10.5 vs 7.3 ms)
+    // one cluster per column, or per tile of a column list (a persistent form, the resident
+    // clusters looping over the list, measured 44% slower per launch: 10.5 vs 7.3 ms)
     int jb, c;
     if (!sweep_column(tiles, ntiles, blockIdx.x / S::C, jb, c)) return;
     const ssa_col_job J = jobs[jb];

@@ -21,7 +21,6 @@
 #include "ssa_fft.cuh"
 #include "ssa_kernels.h"
 
-#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -311,10 +310,9 @@ __device__ __forceinline__ void corr_product(float2* s, const float2* __restrict
     }
 }
 
-// Work of a correlation sweep: the grid (columns, jobs), one CTA per column; or, with a column
-// list of ntiles (job, column) tiles, the tile of work unit u (the single-CTA sweep runs units
-// u = blockIdx.x, blockIdx.x + gridDim.x, ... on a grid of resident CTAs, which stage their
-// twiddle table once). Returns the unit's (job, column), or false past the end.
+// Work unit of a correlation sweep: the grid (columns, jobs), one CTA per column; or, with a
+// column list of ntiles (job, column) tiles, one CTA (cluster) per tile, so that no CTA is spent
+// on the columns beyond a job's ncols. Returns the unit's (job, column), or false past the end.
 __device__ __forceinline__ bool sweep_column(const ssa_tile* __restrict__ tiles, int ntiles, int unit, int& job,
                                              int& c) {
     if (tiles) {
@@ -329,28 +327,26 @@ __device__ __forceinline__ bool sweep_column(const ssa_tile* __restrict__ tiles,
     return true;
 }
 
+// (A persistent form of this kernel, resident CTAs looping over the column list, measured 0.9%
+// faster on real length 32768 but made the one-pass form of the (columns, jobs) grid 20% slower
+// on the uniform batches: not kept.)
 template <int LOGH>
 __global__ void __launch_bounds__(FftShape<LOGH>::BLOCK, FftShape<LOGH>::MINB) k_corr(const ssa_col_job* __restrict__ jobs,
                                                                                        const ssa_tile* __restrict__ tiles,
                                                                                        int ntiles) {
     constexpr int H = 1 << LOGH;
     extern __shared__ float2 smem[];
+    int jb, c;
+    if (!sweep_column(tiles, ntiles, blockIdx.x, jb, c)) return;
+    const ssa_col_job J = jobs[jb];
+    if (c >= J.ncols) return;
     float2* tw = smem + spad_size(H);
-    load_twiddles<LOGH + 1>(tw);  // published by the first pass's closing barrier
-    const int stride = tiles ? (int)gridDim.x : 1 << 30;
-    for (int u = blockIdx.x;; u += stride) {
-        int jb, c;
-        if (!sweep_column(tiles, ntiles, u, jb, c)) return;
-        const ssa_col_job J = jobs[jb];
-        if (c >= J.ncols) return;
-        if (u != (int)blockIdx.x) __syncthreads();  // the previous column's last pass has read the buffer
-        fft_block_io<LOGH, false>(smem, col_pts(J, c), SmemPts{smem}, tw);
-        corr_product<LOGH, FftShape<LOGH>::BLOCK, 4>(smem, reinterpret_cast<const float2*>(J.X), tw, threadIdx.x);
-        __syncthreads();
-        fft_block_io<LOGH, true>(smem, SmemPts{smem},
-                                 RealOut{J.out + (long long)c * J.ld_out, J.n_out, 1.0f / (float)H}, tw);
-        if (!tiles) return;
-    }
+    load_twiddles<LOGH + 1>(tw);
+    fft_block_io<LOGH, false>(smem, col_pts(J, c), SmemPts{smem}, tw);
+    corr_product<LOGH, FftShape<LOGH>::BLOCK, 4>(smem, reinterpret_cast<const float2*>(J.X), tw, threadIdx.x);
+    __syncthreads();
+    fft_block_io<LOGH, true>(smem, SmemPts{smem}, RealOut{J.out + (long long)c * J.ld_out, J.n_out, 1.0f / (float)H},
+                             tw);
 }
 
 // The correlation of k_corr from the input column's real spectrum A (H + 1 bins: A[0], A[H] real,
@@ -1828,17 +1824,7 @@ static int launch_corr(const ssa_col_job* jobs, int njobs, int maxcols, cudaStre
     const int sm = smem_bytes<LOGH>(1);
     cudaError_t e = set_smem(k_corr<LOGH>, sm);
     if (e != cudaSuccess) return (int)e;
-    dim3 grid(maxcols, njobs);
-    if (tiles) {
-        // a column list of njobs tiles: as many CTAs as stay resident, each looping over the list
-        int dev = 0, nsm = 0, per_sm = 0;
-        if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
-            (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
-            (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_corr<LOGH>, FftShape<LOGH>::BLOCK, sm)) !=
-                cudaSuccess)
-            return (int)e;
-        grid = dim3(std::max(1, std::min(njobs, std::max(1, per_sm) * nsm)), 1);
-    }
+    const dim3 grid = tiles ? dim3(njobs, 1) : dim3(maxcols, njobs);  // tiles: njobs = tile count
     k_corr<LOGH><<<grid, FftShape<LOGH>::BLOCK, sm, st>>>(jobs, tiles, njobs);
     return launched(cudaGetLastError());
 }

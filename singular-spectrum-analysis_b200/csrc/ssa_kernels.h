@@ -344,10 +344,8 @@ typedef struct
 } ssa_tile;
 int ssad_corr_multi(const ssa_col_job *d_jobs, const ssa_tile *d_tiles, int ntiles, int *d_head, int nctas,
                     void *stream);
-/* The sweep of ssad_corr over a column list of tiles (job, column c0; logh unused), so that no
- * CTA is spent on columns beyond a job's ncols: single-CTA lengths run as many CTAs as stay
- * resident, each taking every gridDim.x-th tile and staging its twiddle table once; cluster
- * lengths one cluster per tile. */
+/* The sweep of ssad_corr over a column list of tiles (job, column c0; logh unused): one CTA
+ * (cluster) per tile, so that no CTA is spent on columns beyond a job's ncols. */
 int ssad_corr_tiles(const ssa_col_job *d_jobs, const ssa_tile *d_tiles, int ntiles, int logh, void *stream);
 /* Columns one tile of the multi-length sweep covers at logh. */
 int ssad_multi_tile_cols(int logh);
