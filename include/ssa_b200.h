@@ -137,7 +137,7 @@ int ssa_b200_context_recycling(void);
  * all k[s] elementary reconstructions, W-correlation and group sums. Series are bucketed by FFT
  * length (N <= 131072); each bucket runs one launch per
  * stage on its own stream and the buckets overlap on the device. (M is the FFT length
- * ssa_b200_fft_length(N): a power of two or one of the mixed lengths 49152 / 98304.) No
+ * ssa_b200_fft_length(N): a power of two or one of the mixed lengths 49152 / 81920 / 98304.) No
  * counterpart in the reference, whose API takes one series per context.
  *
  * Inputs and outputs are packed in series order: x holds N[s] doubles at sum_{t<s} N[t];
@@ -192,7 +192,7 @@ int ssa_b200_cluster32k(void);
  * N = 131072. */
 int ssa_b200_fft_size_code(int N);
 /* Real FFT length an uneven batch (and the server) uses for a series of length N: the smallest
- * of 2^a (a <= 17), 49152 and 98304 that is >= N (at least 32), or -1 beyond N = 131072. The
+ * of 2^a (a <= 17), 49152, 81920 and 98304 that is >= N (at least 32), or -1 beyond N = 131072. The
  * single-series API and the uniform batch use the power of two. No counterpart in the reference
  * (whose FFT length is the power of two >= N + K - 1). */
 int ssa_b200_fft_length(int N);

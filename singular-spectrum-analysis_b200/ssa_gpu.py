@@ -200,7 +200,7 @@ PROFILE_KINDS = ("spectrum", "corr", "gram", "chol", "rowmul", "rr", "elem_recon
 
 def fft_length(N: int) -> int:
     """Real FFT length the uneven batches use for a series of length N (a power of two, or 49152 /
-    98304 between the cluster powers of two); -1 beyond 131072."""
+    81920 / 98304 between the cluster powers of two); -1 beyond 131072."""
     return int(_lib.ssa_b200_fft_length(int(N)))
 
 
